@@ -1,0 +1,233 @@
+/*
+ * lsd_b200.h -- C ABI of the B200-native Leeds Spherical Dynamo timestep hot path.
+ *
+ * The reference (Leeds-Spherical-Dynamo/leeds-code v3.6.0, Fortran 90) has no runtime
+ * plugin API: its seam is the module interface of `transform`, `nonlinear`, `timestep`
+ * and the field modules, selected at build time by `TRANSFORM = fftw3`
+ * (Scripts/Makefile_template:9,194-196) or `#define _SHTNS`
+ * (Scripts/parallel.h_template:17).  Every entry point below replaces one module
+ * procedure (cited per function) and is callable from Fortran through ISO_C_BINDING:
+ * plain pointers, plain sizes, int status, no C++ or torch types.
+ *
+ * Array layouts at this boundary are the reference's own Fortran (column-major) ones:
+ *   coll  Re(i_N, 0:i_H1)            re[(n-1) + N*nh]            (variables.F90:76-81)
+ *   spec  Re(0:i_H1, i_N)            re[nh + H*(n-1)]            (variables.F90:65-70)
+ *   phys  Re(i_Th, 0:i_Ph-1, i_N)    p[(j-1) + Th*(i + Ph*(n-1))] (variables.F90:84-86)
+ * with the harmonic index nh in the reference's folded order (parallel.h_template:54-80).
+ *
+ * Status codes: 0 = success; >0 = error class (LSD_E*); lsd_last_error() gives text.
+ * No entry point aborts, traps or exits; the reference's `stop 'msg'` becomes a status.
+ * A context is single-threaded: one host thread and one CUDA stream per context.
+ */
+#ifndef LSD_B200_H
+#define LSD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define LSD_OK            0
+#define LSD_EARG          1   /* bad argument or parameter combination (par_precompute) */
+#define LSD_ECUDA         2   /* CUDA runtime error, or no CUDA device                   */
+#define LSD_ESINGULAR     3   /* zero pivot in a banded factorisation (mes_lu_find)      */
+#define LSD_ENOTCONVERGED 4   /* corrector loop gave up (tim_check_cgce)                 */
+#define LSD_ENONFINITE    5   /* NaN/Inf detected in the state                           */
+#define LSD_ESTATE        6   /* call out of order (e.g. corrector before predictor)     */
+#define LSD_ENOMEM        7   /* device allocation failed                                */
+
+/* ---- fields (coll variables held by the context) ---------------------------------- */
+#define LSD_VEL_TOR   0   /* vel_Tor  (velocity.F90)    */
+#define LSD_VEL_POL   1   /* vel_Pol                    */
+#define LSD_COD_C     2   /* cod_C    (codensity.F90)   */
+#define LSD_MAG_TOR   3   /* mag_Tor  (magnetic.F90)    */
+#define LSD_MAG_POL   4   /* mag_Pol                    */
+#define LSD_COMP_C    5   /* comp_C   (composition.F90) */
+#define LSD_NFIELD    6
+
+/* nonlinear terms (outputs of nonlinear.F90), readable with lsd_get_nonlinear */
+#define LSD_N_VEL_TOR 0   /* vel_NTor  nonlinear.F90:188 */
+#define LSD_N_VEL_POL 1   /* vel_NPol  nonlinear.F90:190 */
+#define LSD_N_COD     2   /* cod_NC    nonlinear.F90:276-288 */
+#define LSD_N_MAG_TOR 3   /* mag_NTor  nonlinear.F90:443 */
+#define LSD_N_MAG_POL 4   /* mag_NPol  nonlinear.F90:441 */
+#define LSD_N_COMP    5   /* comp_NC   nonlinear.F90:339-356 */
+
+/* Legendre tables readable with lsd_legendre_table (legendre.F90:41-56), (Th2, H) each */
+#define LSD_LEG_P          0
+#define LSD_LEG_P_         1
+#define LSD_LEG_SIN1MP     2
+#define LSD_LEG_LLP_       3
+#define LSD_LEG_LLSIN1MP   4
+#define LSD_LEG_GWP        5
+#define LSD_LEG_GWLLP_     6
+#define LSD_LEG_GWLLSIN1MP 7
+
+/* precision of the Legendre contraction */
+#define LSD_PREC_FP64   0   /* plain FP64 on the CUDA cores                              */
+#define LSD_PREC_OZAKI  1   /* FP64 emulated by int8 slices on tcgen05 tensor cores      */
+
+/* energy diagnostics written by lsd_energies (io.F90:1739-2024 column order) */
+#define LSD_E_TIME     0   /* tim_t                                                      */
+#define LSD_E_KE       1   /* vel_energy.dat col 2: kinetic energy                       */
+#define LSD_E_KE_TOR   2   /* col 3: total toroidal                                      */
+#define LSD_E_KE_SYM   3   /* col 4: E_eq_sym                                            */
+#define LSD_E_KE_L1    4   /* col 5: E_l=1 (m=0, l even part; variables.F90:837-901)     */
+#define LSD_E_KE_TM0   5   /* col 6: E_tor_m=0                                           */
+#define LSD_E_KE_DIS   6   /* col 7: viscous dissipation                                 */
+#define LSD_E_KE_AX    7   /* col 8: axisymmetric KE                                     */
+#define LSD_E_ME       8   /* mag_energy.dat col 2: magnetic energy                      */
+#define LSD_E_ME_TOR   9   /* col 3                                                      */
+#define LSD_E_ME_SYM  10   /* col 4                                                      */
+#define LSD_E_ME_L1   11   /* col 5                                                      */
+#define LSD_E_ME_TM0  12   /* col 6                                                      */
+#define LSD_E_ME_DIS  13   /* col 7: ohmic dissipation                                   */
+#define LSD_E_DIP     14   /* col 8: axial dipole g10                                    */
+#define LSD_E_QUAD    15   /* col 9: axial quadrupole g20                                */
+#define LSD_E_ME_AX   16   /* col 10: axisymmetric ME                                    */
+#define LSD_E_TOPFLX  17   /* top heat flux (io.F90:1773-1783)                           */
+#define LSD_E_BOTFLX  18   /* bottom heat flux (io.F90:1785-1794)                        */
+#define LSD_NENERGY   19
+
+/* ---- configuration: the compile-time `parameters` module as a runtime struct --------- */
+typedef struct lsd_config {
+  /* resolution (parameters.F90_template:19-23,250) */
+  int L, M, Mp, N, Nic, KL;
+  /* boundary conditions and switches (parameters.F90_template:45-190) */
+  int vel_bc, cod_bc, comp_bc, time_step_control;
+  int boussinesq, vel_tstep, cod_tstep, comp_tstep, mag_tstep;
+  int precision;            /* LSD_PREC_* for the Legendre contraction                */
+  int device;               /* CUDA device ordinal                                    */
+  int ozaki_slices;         /* int8 slices per operand for LSD_PREC_OZAKI (0 = default)*/
+  /* physics (parameters.F90_template:29-44) */
+  double rratio, alpha, Ra, Ra_comp, Pr, Sc, Pm, E, Hyp;
+  /* time integration (parameters.F90_template:229-243) */
+  double implicit, timestep, dterr, courant, corr_upper, corr_lower;
+  /* sources and fluxes (parameters.F90_template:134-171) */
+  double source, source_comp, qi, qo, qi_comp, qo_comp;
+  int reserved[8];
+} lsd_config;
+
+/* derived sizes (parameters.F90_template:251-262; parallel.h_template:54-62) */
+typedef struct lsd_sizes {
+  int H, Th, Th2, Ph, Ma, Hc, Hr, N, L, M, Mp, KL;
+} lsd_sizes;
+
+/* per-call statistics of lsd_step */
+typedef struct lsd_stats {
+  int steps_done;           /* completed timesteps                                      */
+  int correctors;           /* corrector iterations taken in total                      */
+  int evaluations;          /* nonlinear evaluations (transforms + products)            */
+  int kernel_launches;      /* device kernels launched by this call                     */
+  double last_dterr;        /* tim_dterr of the last corrector                          */
+  double t, dt;             /* tim_t, tim_dt after the call                             */
+} lsd_stats;
+
+typedef struct lsd_ctx lsd_ctx;
+
+/* Fill cfg with the template parameter values of Scripts/parameters.F90_template. */
+int lsd_config_default(lsd_config* cfg);
+
+/* Create a context on cfg->device: radial mesh and FD weights (meshs.F90:116-419),
+ * Gauss points (auxiliary/gauwts.f), Schmidt P_l^m tables (legendre.F90:63-128,
+ * auxiliary/schnla.f), harmonic layout (variables.F90:103-194) and, at cfg->timestep,
+ * the banded operators and their LU factors (velocity/codensity/magnetic *_matrices),
+ * all computed in FP64 on the device.  Replaces `initialise` (main.F90:220-380) up to
+ * the state load.  Checks par_precompute (parameters.F90_template:274-288). */
+int lsd_create(const lsd_config* cfg, lsd_ctx** out);
+int lsd_destroy(lsd_ctx* ctx);
+const char* lsd_last_error(const lsd_ctx* ctx);
+int lsd_get_sizes(const lsd_ctx* ctx, lsd_sizes* out);
+
+/* Layout and table queries (for bit-identical layout checks).
+ * lsd_harmonics: var_H%l, var_H%m, var_H%s (variables.F90:124-152), H ints each.
+ * lsd_theta_map: var_Th%m (variables.F90:159-194), 2*Hc ints.
+ * lsd_radial_grid: mes_oc%r(:,1) (meshs.F90:135-143), N doubles.
+ * lsd_radial_weights: mes_oc%intr2dr (meshs.F90:311-336), N doubles.
+ * lsd_gauss: leg_gp, leg_gw (legendre.F90:73), Th doubles each.
+ * lsd_legendre_table: one of the LSD_LEG_* tables, (Th2, H) column-major. */
+int lsd_harmonics(const lsd_ctx* ctx, int* l, int* m, int* s);
+int lsd_theta_map(const lsd_ctx* ctx, int* thm);
+int lsd_radial_grid(const lsd_ctx* ctx, double* r);
+int lsd_radial_weights(const lsd_ctx* ctx, double* intr2dr);
+int lsd_gauss(const lsd_ctx* ctx, double* gp, double* gw);
+int lsd_legendre_table(const lsd_ctx* ctx, int which, double* out);
+
+/* ---- state ---------------------------------------------------------------------- */
+/* Copy a coll field (Fortran layout) to / from the device.  Replaces the state load
+ * (io_load_state, io.F90:349-483) and the refresh before output (io_write2files). */
+int lsd_set_coll(lsd_ctx* ctx, int field, const double* re, const double* im);
+int lsd_get_coll(lsd_ctx* ctx, int field, double* re, double* im);
+/* Nonlinear term of the last evaluation (LSD_N_*), coll layout. */
+int lsd_get_nonlinear(lsd_ctx* ctx, int which, double* re, double* im);
+/* tim_t, tim_dt; setting dt rebuilds the operators (vel/cod/mag_matrices). */
+int lsd_set_time(lsd_ctx* ctx, double t, double dt);
+int lsd_get_time(const lsd_ctx* ctx, double* t, double* dt, int* step);
+
+/* ---- transforms on host buffers (unit parity with transform.fftw3.F90) --------------
+ * Each works on all N shells of the context. */
+/* tra_spec2phys (transform.fftw3.F90:472-520) */
+int lsd_tra_spec2phys(lsd_ctx* ctx, const double* s_re, const double* s_im, double* p);
+/* tra_phys2spec (transform.fftw3.F90:527-583, 586-602) */
+int lsd_tra_phys2spec(lsd_ctx* ctx, const double* p, double* s_re, double* s_im);
+/* tra_qst2rtp (transform.fftw3.F90:719-818) */
+int lsd_tra_qst2rtp(lsd_ctx* ctx,
+                    const double* q_re, const double* q_im,
+                    const double* s_re, const double* s_im,
+                    const double* t_re, const double* t_im,
+                    double* r, double* th, double* ph);
+/* tra_rtp2qst (transform.fftw3.F90:825-949) */
+int lsd_tra_rtp2qst(lsd_ctx* ctx, const double* r, const double* th, const double* ph,
+                    double* q_re, double* q_im, double* s_re, double* s_im,
+                    double* t_re, double* t_im);
+/* tra_grad (transform.fftw3.F90:955-1000) */
+int lsd_tra_grad(lsd_ctx* ctx, const double* s_re, const double* s_im, double* th, double* ph);
+
+/* ---- device-resident batched transforms (inputs already in HBM) ----------------------
+ * d_spec: nbatch spectral fields, interleaved complex, [batch][N][H] (harmonic fastest).
+ * d_phys: nbatch physical fields, [batch][N][Ph][Th] (the Fortran phys layout per field).
+ * Asynchronous on the context stream. */
+int lsd_sht_synth_device(lsd_ctx* ctx, int nbatch, const double* d_spec, double* d_phys);
+int lsd_sht_analys_device(lsd_ctx* ctx, int nbatch, const double* d_phys, double* d_spec);
+
+/* ---- time stepping ----------------------------------------------------------------- */
+/* vel_matrices + cod_matrices + comp_matrices + mag_matrices at the current dt
+ * (velocity.F90:56-168, codensity.F90:37-79, magnetic.F90:62-133). */
+int lsd_matrices(lsd_ctx* ctx);
+/* One nonlinear evaluation from the current state: *_transform + non_velocity,
+ * non_codensity, non_composition, non_magnetic (main.F90:101-124). */
+int lsd_nonlinear(lsd_ctx* ctx);
+/* vel/cod/comp/mag _predictor (main.F90:136-146) using the last evaluation. */
+int lsd_predictor(lsd_ctx* ctx);
+/* vel/cod/comp/mag _corrector (main.F90:148-154); *dterr gets tim_dterr. */
+int lsd_corrector(lsd_ctx* ctx, double* dterr);
+/* nsteps full timesteps (main loop main.F90:100-164: evaluation, predictor, evaluations
+ * and correctors until tim_check_cgce converges), captured as one CUDA graph. */
+int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats);
+/* Energy diagnostics (io_write_vel_energy / io_write_mag_energy), LSD_NENERGY doubles. */
+int lsd_energies(lsd_ctx* ctx, double* out);
+
+/* ---- batched banded radial solves (timestep.F90:566-588 over every (l,m)) -----------
+ * Factorise nmat banded operators A_k (LAPACK band storage with ldab = 3*kl+1, columns
+ * of length n, k = 0..nmat-1, overwritten by their LU factors and pivots like dgbtrf,
+ * meshs.F90:447-456) and solve nrhs right-hand sides, rhs r using matrix map[r]
+ * (dgbtrs, timestep.F90:578-586).  All device pointers; one launch each.
+ * d_ab: [nmat][n][3*kl+1] (column-major per matrix), d_ipiv: [nmat][n],
+ * d_b: [n][nrhs] (rhs index fastest), d_info: [nmat]. */
+int lsd_banded_factor_device(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab,
+                             int* d_ipiv, int* d_info);
+int lsd_banded_solve_device(lsd_ctx* ctx, int n, int kl, int nmat, const double* d_ab,
+                            const int* d_ipiv, int nrhs, const int* d_map, double* d_b);
+
+/* ---- synchronisation and timing ------------------------------------------------------ */
+int lsd_synchronize(lsd_ctx* ctx);
+/* Device-side elapsed milliseconds of the last lsd_step / transform call, measured with
+ * CUDA events on the context stream. */
+int lsd_last_elapsed_ms(const lsd_ctx* ctx, double* ms);
+/* Number of device kernels this context has launched so far. */
+int lsd_kernel_launches(const lsd_ctx* ctx, long long* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LSD_B200_H */

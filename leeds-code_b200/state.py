@@ -1,0 +1,113 @@
+"""Host-side state-file I/O in the reference's classic netCDF layout.
+
+Reads and writes the `state.cdf` files of program/io.F90 (io_load_state :349-483,
+io_save_state :1502-1621) with scipy.io.netcdf_file.  Coefficients are stored in the
+file in plain m-major harmonic order (io_state_nh, io.F90:1258-1272) and in memory in
+the reference's folded order (parallel.h_template:54-80); this module maps between the
+two.  Radial interpolation onto a different grid (io_interp, io.F90:1360-1431) is not
+supported: the radial grid in the file must match (io.F90:407-412 tolerance 1e-8).
+"""
+import numpy as np
+
+from . import capi
+
+STATE_VARS = ("uT", "uP", "C", "BT", "BP")
+FIELD_OF_VAR = {"uT": capi.VEL_TOR, "uP": capi.VEL_POL, "C": capi.COD_C,
+                "BT": capi.MAG_TOR, "BP": capi.MAG_POL, "Comp": capi.COMP_C}
+
+
+def folded_harmonics(L, M, Mp):
+    """(l, m_, s) of every nh in the folded order of _loop_setlm (parallel.h_template:54-80)."""
+    sz = capi.derived_sizes(L, M, Mp)
+    Hc, Hr, H = sz["Hc"], sz["Hr"], sz["H"]
+    l_ = np.zeros(H, np.int64)
+    m_ = np.zeros(H, np.int64)
+    nh = 0
+    for j in range(1, Hc + 1):
+        for i in range(1, Hr + 1):
+            m = j - 1
+            l = m * Mp + i - 1
+            if l >= L:
+                m = 2 * Hc - j
+                l = L - Hr + i - 1
+            l_[nh], m_[nh] = l, m * Mp
+            nh += 1
+    return l_, m_, (l_ + m_) % 2
+
+
+def state_nh(l, m_, L, M, Mp):
+    """io_state_nh (io.F90:1258-1272): file index of (l, m_), -1 when absent."""
+    l = np.asarray(l)
+    m_ = np.asarray(m_)
+    ok = (m_ % Mp == 0) & (l < L) & (m_ < M * Mp)
+    m = m_ // Mp
+    nh = L * m - Mp * (m - 1) * m // 2 + l - m_
+    return np.where(ok, nh, -1)
+
+
+def load_state(path, L, M, Mp, N, r_expected=None):
+    """Return dict(field -> (re, im) arrays of shape (H, N)), t, dt, r.
+
+    Modes of the run that are not in the file are zero (the reference fills them with
+    uniform noise of amplitude d_init_pert from an unseeded generator, io.F90:1316-1324,
+    which no run can reproduce)."""
+    from scipy.io import netcdf_file
+    f = netcdf_file(path, "r", mmap=False)
+    r = np.array(f.variables["r"].data, dtype=np.float64)
+    if len(r) != N:
+        raise ValueError("state has %d radial points, run has %d (interpolation unsupported)" % (len(r), N))
+    if r_expected is not None and np.max(np.abs(r - r_expected)) > 1e-8:
+        raise ValueError("state radial grid differs from the run's grid")
+    l, m_, _ = folded_harmonics(L, M, Mp)
+    out = {}
+    for name, var in f.variables.items():
+        if name not in FIELD_OF_VAR:
+            continue
+        a = var._attributes
+        Lf, Mf, Mpf = int(a["L"]), int(a["M"]), int(a["Mp"])
+        data = np.array(var.data, dtype=np.float64)  # (2, Hfile, N)
+        idx = state_nh(l, m_, Lf, Mf, Mpf)
+        re = np.zeros((len(l), N))
+        im = np.zeros((len(l), N))
+        ok = idx >= 0
+        re[ok] = data[0, idx[ok], :]
+        im[ok] = data[1, idx[ok], :]
+        out[FIELD_OF_VAR[name]] = (re, im)
+    t = float(f._attributes.get("t", 0.0))
+    dt = float(f.variables["dt"].data) if "dt" in f.variables else 0.0
+    f.close()
+    return out, t, dt, r
+
+
+def save_state(path, fields, L, M, Mp, r, ric, t, dt, attrs):
+    """Write a state file in the current layout of io_save_state (dims r, icr, H, ReIm)."""
+    from scipy.io import netcdf_file
+    l, m_, _ = folded_harmonics(L, M, Mp)
+    H = len(l)
+    idx = state_nh(l, m_, L, M, Mp)
+    f = netcdf_file(path, "w", version=1)
+    f.t = t
+    for k, v in attrs.items():
+        setattr(f, k, v)
+    N = len(r)
+    f.createDimension("r", N)
+    f.createDimension("icr", len(ric))
+    f.createDimension("H", H)
+    f.createDimension("ReIm", 2)
+    vr = f.createVariable("r", "d", ("r",))
+    vr[:] = r
+    vic = f.createVariable("icr", "d", ("icr",))
+    vic[:] = ric
+    vdt = f.createVariable("dt", "d", ())
+    vdt.assignValue(dt)
+    vom = f.createVariable("icOmega", "d", ())
+    vom.assignValue(0.0)
+    inv = {v: k for k, v in FIELD_OF_VAR.items()}
+    for fld, (re, im) in fields.items():
+        v = f.createVariable(inv[fld], "d", ("ReIm", "H", "r"))
+        data = np.zeros((2, H, N))
+        data[0, idx, :] = re
+        data[1, idx, :] = im
+        v[:] = data
+        v.L, v.M, v.Mp = np.int32(L), np.int32(M), np.int32(Mp)
+    f.close()

@@ -1,0 +1,85 @@
+"""Seeded synthetic initial states and workload configurations.
+
+No public dataset or checkpoint exists for these workloads; the states are drawn from a
+fixed seed with the shapes and amplitude spectra of the named configurations:
+complex FP64 coefficients ~ N(0,1) for every (l, m), scaled by 1e-3 * l^-2 and by the
+radial profile sin(pi (r - ri)) on the reference's Chebyshev grid (meshs.F90:135-143);
+l = 0 coefficients are zero (the l = 0 velocity and magnetic modes are not stepped,
+timestep.F90:579, and the codensity's l = 0 profile comes from its boundary condition,
+codensity.F90:165-181); m = 0 imaginary parts are zero.
+"""
+import numpy as np
+
+from . import capi
+from .state import folded_harmonics, state_nh
+
+SEED = 20261203
+
+
+def chebyshev_grid(N, rratio, alpha=-1.0):
+    """mes_oc%r(:,1) of meshs.F90:135-143."""
+    n = np.arange(1, N + 1)
+    if alpha > 0:
+        r = 0.5 * (1.0 + np.arcsin(alpha * np.cos(np.pi * (N - n) / (N - 1))) / np.arcsin(alpha))
+    else:
+        r = 0.5 * (1.0 + np.cos(np.pi * (N - n) / (N - 1)))
+    return r + rratio / (1.0 - rratio)
+
+
+def boussinesq_state(cfg, seed=SEED, amplitude=1e-3, fields=(capi.VEL_TOR, capi.VEL_POL, capi.COD_C,
+                                                             capi.MAG_TOR, capi.MAG_POL)):
+    """dict field -> (re, im), each (H, N) == Fortran coll (N, H).
+
+    Draw order: for each field in (uT, uP, C, BT, BP), one (H_file, 2) standard-normal
+    block in the state-file (m-major) harmonic order of io_state_nh."""
+    L, M, Mp, N = cfg.L, cfg.M, cfg.Mp, cfg.N
+    l, m_, _ = folded_harmonics(L, M, Mp)
+    H = len(l)
+    idx = state_nh(l, m_, L, M, Mp)
+    r = chebyshev_grid(N, cfg.rratio, cfg.alpha)
+    ri = cfg.rratio / (1.0 - cfg.rratio)
+    prof = np.sin(np.pi * (r - ri))
+    rng = np.random.Generator(np.random.PCG64(seed))
+    amp = np.zeros(H)
+    amp[l > 0] = amplitude / l[l > 0].astype(np.float64) ** 2
+    out = {}
+    for f in (capi.VEL_TOR, capi.VEL_POL, capi.COD_C, capi.MAG_TOR, capi.MAG_POL):
+        z = rng.standard_normal((H, 2))[idx]  # file order -> folded order
+        re = (z[:, 0] * amp)[:, None] * prof[None, :]
+        im = (z[:, 1] * amp)[:, None] * prof[None, :]
+        im[m_ == 0, :] = 0.0
+        if f in fields:
+            out[f] = (np.ascontiguousarray(re), np.ascontiguousarray(im))
+    return out
+
+
+def random_spectral(L, M, Mp, nshell, nfield, seed=SEED, power=1.0):
+    """Random complex coefficients ~ N(0,1) * l^-power (l = 0 -> 1), m = 0 imaginary zero.
+    Returns interleaved complex array [field][shell][H] (harmonic fastest)."""
+    l, m_, _ = folded_harmonics(L, M, Mp)
+    H = len(l)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    a = np.ones(H)
+    a[l > 0] = 1.0 / l[l > 0].astype(np.float64) ** power
+    z = rng.standard_normal((nfield, nshell, H, 2)) * a[None, None, :, None]
+    z[:, :, m_ == 0, 1] = 0.0
+    return z  # (..., 2) = (re, im)
+
+
+# ---- named workloads ------------------------------------------------------------------
+def config_parity(**kw):
+    """Plain FP64 Boussinesq MHD shell at L = M = 32 (lmax = mmax = 31; Th = 48, Ph = 96),
+    N = 33, E = 3e-4, Ra = 200, Pr = 1, Pm = 3, dt = 1e-5, no-slip, fixed T, insulating."""
+    base = dict(L=32, M=32, Mp=1, N=33, Nic=1, KL=3, rratio=0.35, E=3e-4, Ra=200.0, Pr=1.0,
+                Pm=3.0, vel_bc=1, cod_bc=1, timestep=1e-5, implicit=0.6, time_step_control=2)
+    base.update(kw)
+    return capi.template_config(**base)
+
+
+def config_dynamo128(**kw):
+    """Full Boussinesq dynamo step at lmax = mmax = 127 (L = M = 128; Th = 192, Ph = 384),
+    N = 129, parameters of config_parity, dt = 2e-6."""
+    base = dict(L=128, M=128, Mp=1, N=129, Nic=1, KL=3, rratio=0.35, E=3e-4, Ra=200.0, Pr=1.0,
+                Pm=3.0, vel_bc=1, cod_bc=1, timestep=2e-6, implicit=0.6, time_step_control=2)
+    base.update(kw)
+    return capi.template_config(**base)
