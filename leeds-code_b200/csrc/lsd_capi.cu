@@ -1,0 +1,723 @@
+// lsd_capi.cu -- the extern "C" entry points of include/lsd_b200.h.
+//
+// Host-side control mirrors the reference's driver: initialise (main.F90:220-400),
+// the main loop (main.F90:100-164) with tim_check_cgce (timestep.F90:744-830), and the
+// state refresh for output.  Every entry point returns a status; nothing aborts.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "lsd_common.cuh"
+
+int lsd_fail(lsd_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+namespace {
+
+
+void free_ctx(lsd_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->dev >= 0) cudaSetDevice(ctx->dev);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->g_pred) cudaGraphExecDestroy(ctx->g_pred);
+  if (ctx->g_corr) cudaGraphExecDestroy(ctx->g_corr);
+  void* ptrs[] = {ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_lm2nh,
+                  ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,
+                  ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y,
+                  ctx->d_ipiv, ctx->d_ipivs, ctx->d_info, ctx->d_gre, ctx->d_invg, ctx->d_state, ctx->d_nl,
+                  ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
+  if (ctx->h_red) cudaFreeHost(ctx->h_red);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream && ctx->owns_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+template <class T>
+int dalloc(lsd_ctx* ctx, T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return LSD_OK;
+}
+
+template <class T>
+int upload(lsd_ctx* ctx, T* d, const std::vector<T>& h) {
+  CUDA_TRY(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+  return LSD_OK;
+}
+
+// harmonic layout: _loop_setlm (parallel.h_template:54-80), _loop_sumth (:85-100)
+void build_layout(lsd_ctx* c) {
+  c->hl.assign(c->H, 0); c->hm.assign(c->H, 0); c->hs.assign(c->H, 0); c->mcount.assign(c->H, 0);
+  int nh = -1;
+  for (int j = 1; j <= c->Hc; ++j)
+    for (int i = 1; i <= c->Hr; ++i) {
+      int m = j - 1, l = m * c->Mp + i - 1;
+      if (l >= c->L) { m = 2 * c->Hc - j; l = c->L - c->Hr + i - 1; }
+      ++nh;
+      c->hl[nh] = l; c->hm[nh] = m * c->Mp; c->hs[nh] = (l + m * c->Mp) % 2;
+    }
+  c->thm.assign(c->NM, 0);
+  c->mstart.assign(c->NM, 0);
+  c->mlen.assign(c->NM, 0);
+  int m = -1, m_ = -1;
+  for (nh = 0; nh < c->H; ++nh) {
+    int m__ = m_;
+    m_ = c->hm[nh];
+    if (m_ != m__) { ++m; c->thm[m] = m_ / c->Mp; c->mstart[m] = nh; }
+    c->mcount[nh] = m;
+    c->mlen[m]++;
+  }
+}
+
+// radix plan for the complex FFT of length P2 = 3^a 2^b
+bool plan_radices(lsd_ctx* c) {
+  int p = c->P2, n = 0;
+  while (p % 4 == 0 && n < 16) { c->radices[n++] = 4; p /= 4; }
+  while (p % 2 == 0 && n < 16) { c->radices[n++] = 2; p /= 2; }
+  while (p % 3 == 0 && n < 16) { c->radices[n++] = 3; p /= 3; }
+  c->nrad = n;
+  return p == 1;
+}
+
+// packing between Fortran split (re, im) arrays and device interleaved [n][nh]
+void pack_coll(const lsd_ctx* c, const double* re, const double* im, double* out) {  // coll (N,H)
+  for (int n = 0; n < c->N; ++n)
+    for (int nh = 0; nh < c->H; ++nh) {
+      size_t src = (size_t)n + (size_t)c->N * nh, dst = ((size_t)n * c->H + nh) * 2;
+      out[dst] = re[src];
+      out[dst + 1] = im[src];
+    }
+}
+void unpack_coll(const lsd_ctx* c, const double* in, double* re, double* im) {
+  for (int n = 0; n < c->N; ++n)
+    for (int nh = 0; nh < c->H; ++nh) {
+      size_t dst = (size_t)n + (size_t)c->N * nh, src = ((size_t)n * c->H + nh) * 2;
+      re[dst] = in[src];
+      im[dst] = in[src + 1];
+    }
+}
+void pack_spec(const lsd_ctx* c, const double* re, const double* im, double* out) {  // spec (H,N)
+  size_t T = (size_t)c->N * c->H;
+  for (size_t i = 0; i < T; ++i) { out[2 * i] = re[i]; out[2 * i + 1] = im[i]; }
+}
+void unpack_spec(const lsd_ctx* c, const double* in, double* re, double* im) {
+  size_t T = (size_t)c->N * c->H;
+  for (size_t i = 0; i < T; ++i) { re[i] = in[2 * i]; im[i] = in[2 * i + 1]; }
+}
+
+int ensure_phys(lsd_ctx* ctx, int nslots) {
+  if (ctx->nphys >= nslots) return LSD_OK;
+  if (ctx->d_phys) { cudaFree(ctx->d_phys); ctx->d_phys = nullptr; }
+  int rc = dalloc(ctx, &ctx->d_phys, (size_t)nslots * ctx->N * ctx->Ph * ctx->Th);
+  if (rc) return rc;
+  ctx->nphys = nslots;
+  return LSD_OK;
+}
+
+int time_begin(lsd_ctx* ctx) {
+  CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
+  return LSD_OK;
+}
+int time_end(lsd_ctx* ctx) {
+  CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
+  CUDA_TRY(cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->last_ms = ms;
+  return LSD_OK;
+}
+
+// tim_check_cgce (timestep.F90:744-830); returns LSD_ENOTCONVERGED when it gives up.
+int check_cgce(lsd_ctx* c) {
+  int fail = 0;
+  const double dterr = c->dterr;
+  if (c->cfg.time_step_control == 1) {
+    if (c->it == 1) { c->corr_dt = dterr; c->lasterr = 1e99; }
+    if (c->dt < 1e-12 && c->step > 30) { c->it = 0; fail = 1; }
+    else if (c->it > 10) { c->it = 0; fail = 1; }
+    else if (dterr > c->lasterr) { if (dterr > 1.0) fail = 1; c->it = 0; }
+    else if (dterr > 1.0) { c->lasterr = dterr; c->it = c->it + 1; }
+    else c->it = 0;
+  } else {
+    if (c->it == 1) { c->corr_dt = c->dt * std::sqrt(c->cfg.dterr / dterr); c->lasterr = 1e99; }
+    if (c->dt < 1e-12 && c->step > 30) { c->it = 0; fail = 1; }
+    else if (c->it == c->tim_pcn) c->it = 0;
+    else if (c->it > 10) { c->it = 0; fail = 1; }
+    else if (dterr > c->lasterr) {
+      if (dterr > 2.0 * c->cfg.dterr) fail = 1;
+      if (dterr < 2.0 * c->cfg.dterr) c->corr_dt = c->dt / (1e1 * c->cfg.courant);
+      c->it = 0;
+    } else if (dterr > c->cfg.dterr) { c->lasterr = dterr; c->it = c->it + 1; }
+    else c->it = 0;
+  }
+  c->dterr = 0.0;
+  return fail ? LSD_ENOTCONVERGED : LSD_OK;
+}
+
+// read the corrector's sums of squares and form tim_dterr (timestep.F90:715-737)
+int finish_corrector(lsd_ctx* ctx) {
+  CUDA_TRY(cudaMemcpyAsync(ctx->h_red, ctx->d_red, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  const double* r = ctx->h_red;
+  double d = ctx->dterr;
+  d = d + std::sqrt(r[0]);  // vel Tor
+  d = d + std::sqrt(r[1]);  // vel Pol
+  d = d + std::sqrt(r[2]);  // codensity
+  if (ctx->cfg.comp_tstep) d = d + std::sqrt(r[3]);
+  d = d + std::sqrt(r[4]);  // mag Tor
+  d = d + std::sqrt(r[5]);  // inner-core Tor
+  d = d + std::sqrt(r[6]);  // mag Pol
+  d = d + std::sqrt(r[7]);  // inner-core Pol
+  ctx->dterr = d;
+  if (!std::isfinite(d)) return lsd_fail(ctx, LSD_ENONFINITE, "non-finite corrector norm (state diverged)");
+  return LSD_OK;
+}
+
+int capture(lsd_ctx* ctx, bool pred, cudaGraphExec_t* out, long long* nkernels) {
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+  long long before = ctx->launches;
+  int rc = lsd_eval(ctx);
+  if (!rc) rc = pred ? lsd_pred(ctx) : lsd_corr(ctx);
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  *nkernels = ctx->launches - before;
+  ctx->launches = before;
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return LSD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lsd_config_default(lsd_config* c) {
+  if (!c) return LSD_EARG;
+  std::memset(c, 0, sizeof(*c));
+  c->L = 64; c->M = 16; c->Mp = 4; c->N = 64; c->Nic = 1; c->KL = 3;
+  c->vel_bc = 1; c->cod_bc = 1; c->comp_bc = 1; c->time_step_control = 2;
+  c->boussinesq = 1; c->vel_tstep = 1; c->cod_tstep = 1; c->comp_tstep = 0; c->mag_tstep = 1;
+  c->precision = LSD_PREC_FP64; c->device = 0; c->ozaki_slices = 0;
+  c->rratio = 0.35; c->alpha = -1.0; c->Ra = 6.5e4; c->Ra_comp = 1.0; c->Pr = 1.0; c->Sc = 1.0;
+  c->Pm = 5.0; c->E = 1.0e-3; c->Hyp = 0.0;
+  c->implicit = 0.6; c->timestep = -5e-5; c->dterr = 0.025; c->courant = (double)0.8f;
+  c->corr_upper = 0.020; c->corr_lower = 0.00200;
+  c->source = 0.0; c->source_comp = 0.0; c->qi = 0.0; c->qo = -1.0; c->qi_comp = 0.0; c->qo_comp = -1.0;
+  return LSD_OK;
+}
+
+int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
+  if (!cfg || !out) return LSD_EARG;
+  *out = nullptr;
+  lsd_ctx* ctx = new (std::nothrow) lsd_ctx();
+  if (!ctx) return LSD_ENOMEM;
+  ctx->cfg = *cfg;
+  ctx->dev = -1;
+  const lsd_config& c = *cfg;
+  ctx->L = c.L; ctx->M = c.M; ctx->Mp = c.Mp; ctx->N = c.N; ctx->KL = c.KL;
+  // par_precompute (parameters.F90_template:274-288) and this library's scope
+  std::string why;
+  if (c.L < 2 || c.M < 2 || c.Mp < 1 || c.N < 2 * c.KL + 2 || c.KL < 2 || c.KL > LSD_MAX_KL) why = "bad resolution";
+  else if (c.L <= (c.M - 1) * c.Mp) why = "set L > (M-1)*Mp";
+  else if (c.M % 2 == 1) why = "if(M>1) set M even";
+  else if (c.Nic != 1) why = "only an insulating inner core (Nic = 1) is supported";
+  else if (!c.boussinesq) why = "only the Boussinesq equations are supported";
+  else if (c.timestep <= 0.0) why = "only a fixed timestep (d_timestep > 0) is supported";
+  else if (!c.vel_tstep || !c.cod_tstep || !c.mag_tstep) why = "velocity, codensity and field must all be stepped";
+  else if (c.comp_tstep) why = "composition stepping is not supported on the device yet";
+  else if (c.precision != LSD_PREC_FP64 && c.precision != LSD_PREC_OZAKI) why = "unknown precision";
+  if (!why.empty()) { int rc = lsd_fail(ctx, LSD_EARG, why); free_ctx(ctx); return rc; }
+  ctx->Ma = c.M * 3 / 2;
+  ctx->H = c.L * c.M - c.Mp * (c.M - 1) * c.M / 2;
+  ctx->Th = c.L * 3 / 2;
+  ctx->Th2 = (ctx->Th + 1) / 2;
+  ctx->Ph = ctx->Ma * 2;
+  ctx->Hc = (c.M + 1) / 2;
+  ctx->Hr = ctx->H / ctx->Hc;
+  ctx->NM = 2 * ctx->Hc;
+  ctx->P2 = ctx->Ma;
+  ctx->dt = c.timestep;
+  if (!plan_radices(ctx)) { free_ctx(ctx); return LSD_EARG; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || c.device < 0 || c.device >= ndev) {
+    free_ctx(ctx);
+    return LSD_ECUDA;
+  }
+  ctx->dev = c.device;
+  int rc = LSD_OK;
+#define TRY(x) do { rc = (x); if (rc) { free_ctx(ctx); return rc; } } while (0)
+#define CTRY(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { free_ctx(ctx); return LSD_ECUDA; } } while (0)
+  CTRY(cudaSetDevice(ctx->dev));
+  CTRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  ctx->owns_stream = true;
+  CTRY(cudaEventCreate(&ctx->ev0));
+  CTRY(cudaEventCreate(&ctx->ev1));
+  build_layout(ctx);
+  const int H = ctx->H, N = ctx->N, L = ctx->L, KL = ctx->KL, Th = ctx->Th, Th2 = ctx->Th2, NM = ctx->NM;
+  std::vector<int> lm2nh((size_t)ctx->M * L, -1);
+  for (int nh = 0; nh < H; ++nh) lm2nh[(size_t)(ctx->hm[nh] / ctx->Mp) * L + ctx->hl[nh]] = nh;
+  TRY(dalloc(ctx, &ctx->d_l, H)); TRY(upload(ctx, ctx->d_l, ctx->hl));
+  TRY(dalloc(ctx, &ctx->d_m, H)); TRY(upload(ctx, ctx->d_m, ctx->hm));
+  TRY(dalloc(ctx, &ctx->d_s, H)); TRY(upload(ctx, ctx->d_s, ctx->hs));
+  TRY(dalloc(ctx, &ctx->d_mc, H)); TRY(upload(ctx, ctx->d_mc, ctx->mcount));
+  TRY(dalloc(ctx, &ctx->d_mstart, NM)); TRY(upload(ctx, ctx->d_mstart, ctx->mstart));
+  TRY(dalloc(ctx, &ctx->d_mlen, NM)); TRY(upload(ctx, ctx->d_mlen, ctx->mlen));
+  TRY(dalloc(ctx, &ctx->d_thm, NM)); TRY(upload(ctx, ctx->d_thm, ctx->thm));
+  TRY(dalloc(ctx, &ctx->d_lm2nh, lm2nh.size())); TRY(upload(ctx, ctx->d_lm2nh, lm2nh));
+  // FFT twiddles (long double host trigonometry, rounded once)
+  {
+    std::vector<double2> tw2(ctx->P2), twh(ctx->Ph);
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < ctx->P2; ++k) {
+      long double a = 2.0L * PI * (long double)k / (long double)ctx->P2;
+      tw2[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    for (int k = 0; k < ctx->Ph; ++k) {
+      long double a = 2.0L * PI * (long double)k / (long double)ctx->Ph;
+      twh[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    TRY(dalloc(ctx, &ctx->d_tw2, tw2.size())); TRY(upload(ctx, ctx->d_tw2, tw2));
+    TRY(dalloc(ctx, &ctx->d_twh, twh.size())); TRY(upload(ctx, ctx->d_twh, twh));
+  }
+  TRY(dalloc(ctx, &ctx->d_leg, (size_t)8 * H * Th2));
+  TRY(dalloc(ctx, &ctx->d_gp, Th)); TRY(dalloc(ctx, &ctx->d_gw, Th));
+  TRY(dalloc(ctx, &ctx->d_sn, Th)); TRY(dalloc(ctx, &ctx->d_sn1, Th));
+  TRY(dalloc(ctx, &ctx->d_r, (size_t)7 * N));
+  TRY(dalloc(ctx, &ctx->d_dr, (size_t)KL * (2 * KL + 1) * N));
+  TRY(dalloc(ctx, &ctx->d_r1dr, (size_t)(2 * KL + 1) * N));
+  TRY(dalloc(ctx, &ctx->d_radlap, (size_t)(2 * KL + 1) * N));
+  TRY(dalloc(ctx, &ctx->d_intr2dr, N));
+  const size_t lus = (size_t)OP_NFAM * L * N * (3 * KL + 1);
+  TRY(dalloc(ctx, &ctx->d_lu, lus)); TRY(dalloc(ctx, &ctx->d_lus, lus));
+  TRY(dalloc(ctx, &ctx->d_y, (size_t)OP_NFAM * N * (2 * KL + 1) * L));
+  TRY(dalloc(ctx, &ctx->d_ipiv, (size_t)OP_NFAM * L * N)); TRY(dalloc(ctx, &ctx->d_ipivs, (size_t)OP_NFAM * L * N));
+  TRY(dalloc(ctx, &ctx->d_info, (size_t)OP_NFAM * L));
+  TRY(dalloc(ctx, &ctx->d_gre, (size_t)L * 2 * N)); TRY(dalloc(ctx, &ctx->d_invg, (size_t)L * 4));
+  const size_t F = (size_t)N * H;
+  TRY(dalloc(ctx, &ctx->d_state, LSD_NFIELD * F)); TRY(dalloc(ctx, &ctx->d_nl, LSD_NFIELD * F));
+  TRY(dalloc(ctx, &ctx->d_sv, LSD_NFIELD * F));
+  CTRY(cudaMemset(ctx->d_state, 0, sizeof(cplx) * LSD_NFIELD * F));
+  CTRY(cudaMemset(ctx->d_nl, 0, sizeof(cplx) * LSD_NFIELD * F));
+  CTRY(cudaMemset(ctx->d_sv, 0, sizeof(cplx) * LSD_NFIELD * F));
+  ctx->nspec = 13;
+  TRY(dalloc(ctx, &ctx->d_spec, (size_t)ctx->nspec * F));
+  ctx->nfour = 15;
+  TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * NM * Th));
+  TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
+  CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));
+  ctx->h_pin_bytes = std::max(sizeof(cplx) * F * 3, sizeof(double) * 16);
+  CTRY(cudaMallocHost((void**)&ctx->h_pin, ctx->h_pin_bytes));
+  TRY(lsd_build_tables(ctx));
+  TRY(lsd_build_operators(ctx));
+#undef TRY
+#undef CTRY
+  *out = ctx;
+  return LSD_OK;
+}
+
+int lsd_destroy(lsd_ctx* ctx) {
+  free_ctx(ctx);
+  return LSD_OK;
+}
+
+const char* lsd_last_error(const lsd_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int lsd_get_sizes(const lsd_ctx* c, lsd_sizes* s) {
+  if (!c || !s) return LSD_EARG;
+  s->H = c->H; s->Th = c->Th; s->Th2 = c->Th2; s->Ph = c->Ph; s->Ma = c->Ma; s->Hc = c->Hc; s->Hr = c->Hr;
+  s->N = c->N; s->L = c->L; s->M = c->M; s->Mp = c->Mp; s->KL = c->KL;
+  return LSD_OK;
+}
+
+int lsd_harmonics(const lsd_ctx* c, int* l, int* m, int* s) {
+  if (!c || !l || !m || !s) return LSD_EARG;
+  for (int i = 0; i < c->H; ++i) { l[i] = c->hl[i]; m[i] = c->hm[i]; s[i] = c->hs[i]; }
+  return LSD_OK;
+}
+int lsd_theta_map(const lsd_ctx* c, int* thm) {
+  if (!c || !thm) return LSD_EARG;
+  for (int i = 0; i < c->NM; ++i) thm[i] = c->thm[i];
+  return LSD_OK;
+}
+
+static int d2h(lsd_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return LSD_OK;
+}
+
+int lsd_radial_grid(const lsd_ctx* c, double* r) {
+  if (!c || !r) return LSD_EARG;
+  return d2h(const_cast<lsd_ctx*>(c), r, c->d_r + (size_t)4 * c->N, sizeof(double) * c->N);
+}
+int lsd_radial_weights(const lsd_ctx* c, double* w) {
+  if (!c || !w) return LSD_EARG;
+  return d2h(const_cast<lsd_ctx*>(c), w, c->d_intr2dr, sizeof(double) * c->N);
+}
+int lsd_gauss(const lsd_ctx* c, double* gp, double* gw) {
+  if (!c || !gp || !gw) return LSD_EARG;
+  int rc = d2h(const_cast<lsd_ctx*>(c), gp, c->d_gp, sizeof(double) * c->Th);
+  if (rc) return rc;
+  return d2h(const_cast<lsd_ctx*>(c), gw, c->d_gw, sizeof(double) * c->Th);
+}
+int lsd_legendre_table(const lsd_ctx* c, int which, double* out) {
+  if (!c || !out || which < 0 || which > 7) return LSD_EARG;
+  size_t T = (size_t)c->H * c->Th2;
+  return d2h(const_cast<lsd_ctx*>(c), out, c->d_leg + (size_t)which * T, sizeof(double) * T);
+}
+
+int lsd_set_coll(lsd_ctx* ctx, int field, const double* re, const double* im) {
+  if (!ctx || !re || !im || field < 0 || field >= LSD_NFIELD) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  const size_t F = (size_t)ctx->N * ctx->H;
+  pack_coll(ctx, re, im, ctx->h_pin);
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_state + field * F, ctx->h_pin, sizeof(cplx) * F, cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->have_eval = false;
+  return LSD_OK;
+}
+int lsd_get_coll(lsd_ctx* ctx, int field, double* re, double* im) {
+  if (!ctx || !re || !im || field < 0 || field >= LSD_NFIELD) return LSD_EARG;
+  const size_t F = (size_t)ctx->N * ctx->H;
+  int rc = d2h(ctx, ctx->h_pin, ctx->d_state + field * F, sizeof(cplx) * F);
+  if (rc) return rc;
+  unpack_coll(ctx, ctx->h_pin, re, im);
+  return LSD_OK;
+}
+int lsd_get_nonlinear(lsd_ctx* ctx, int which, double* re, double* im) {
+  if (!ctx || !re || !im || which < 0 || which >= LSD_NFIELD) return LSD_EARG;
+  const size_t F = (size_t)ctx->N * ctx->H;
+  int rc = d2h(ctx, ctx->h_pin, ctx->d_nl + which * F, sizeof(cplx) * F);
+  if (rc) return rc;
+  unpack_coll(ctx, ctx->h_pin, re, im);
+  return LSD_OK;
+}
+
+int lsd_set_time(lsd_ctx* ctx, double t, double dt) {
+  if (!ctx || !(dt > 0.0)) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  ctx->t = t;
+  if (dt != ctx->dt) {
+    ctx->dt = dt;
+    int rc = lsd_build_operators(ctx);
+    if (rc) return rc;
+    if (ctx->g_pred) { cudaGraphExecDestroy(ctx->g_pred); ctx->g_pred = nullptr; }
+    if (ctx->g_corr) { cudaGraphExecDestroy(ctx->g_corr); ctx->g_corr = nullptr; }
+  }
+  return LSD_OK;
+}
+int lsd_get_time(const lsd_ctx* ctx, double* t, double* dt, int* step) {
+  if (!ctx) return LSD_EARG;
+  if (t) *t = ctx->t;
+  if (dt) *dt = ctx->dt;
+  if (step) *step = ctx->step;
+  return LSD_OK;
+}
+
+// ---- host-buffer transforms ------------------------------------------------------------
+static int spec_in(lsd_ctx* ctx, int slot, const double* re, const double* im) {
+  const size_t F = (size_t)ctx->N * ctx->H;
+  double* buf = ctx->h_pin + (size_t)slot * 2 * F;
+  pack_spec(ctx, re, im, buf);
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_spec + slot * F, buf, sizeof(cplx) * F, cudaMemcpyHostToDevice, ctx->stream));
+  return LSD_OK;
+}
+static int spec_out(lsd_ctx* ctx, int slot, double* re, double* im) {
+  const size_t F = (size_t)ctx->N * ctx->H;
+  double* buf = ctx->h_pin + (size_t)slot * 2 * F;
+  CUDA_TRY(cudaMemcpyAsync(buf, ctx->d_spec + slot * F, sizeof(cplx) * F, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  unpack_spec(ctx, buf, re, im);
+  return LSD_OK;
+}
+static size_t phys_count(const lsd_ctx* c) { return (size_t)c->N * c->Ph * c->Th; }
+
+int lsd_tra_spec2phys(lsd_ctx* ctx, const double* s_re, const double* s_im, double* p) {
+  if (!ctx || !s_re || !s_im || !p) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc;
+  if ((rc = ensure_phys(ctx, 3))) return rc;
+  if ((rc = spec_in(ctx, 0, s_re, s_im))) return rc;
+  const size_t F = (size_t)ctx->N * ctx->H;
+  (void)F;
+  SynthGroup g;
+  g.kind = SK_SCALAR;
+  g.in[0] = ctx->d_spec; g.in[1] = g.in[2] = nullptr;
+  g.out[0] = ctx->d_four; g.out[1] = g.out[2] = nullptr;
+  if ((rc = time_begin(ctx))) return rc;
+  if ((rc = lsd_launch_synth(ctx, &g, 1))) return rc;
+  if ((rc = lsd_launch_c2r(ctx, ctx->d_four, ctx->d_phys, 1))) return rc;
+  if ((rc = time_end(ctx))) return rc;
+  CUDA_TRY(cudaMemcpy(p, ctx->d_phys, sizeof(double) * phys_count(ctx), cudaMemcpyDeviceToHost));
+  return LSD_OK;
+}
+
+int lsd_tra_phys2spec(lsd_ctx* ctx, const double* p, double* s_re, double* s_im) {
+  if (!ctx || !s_re || !s_im || !p) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc;
+  if ((rc = ensure_phys(ctx, 3))) return rc;
+  CUDA_TRY(cudaMemcpy(ctx->d_phys, p, sizeof(double) * phys_count(ctx), cudaMemcpyHostToDevice));
+  AnalGroup g;
+  g.kind = AK_SCALAR;
+  g.in[0] = ctx->d_four; g.in[1] = g.in[2] = nullptr;
+  g.out[0] = ctx->d_spec; g.out[1] = g.out[2] = nullptr;
+  if ((rc = time_begin(ctx))) return rc;
+  if ((rc = lsd_launch_r2c(ctx, ctx->d_phys, ctx->d_four, 1))) return rc;
+  if ((rc = lsd_launch_anal(ctx, &g, 1))) return rc;
+  if ((rc = time_end(ctx))) return rc;
+  return spec_out(ctx, 0, s_re, s_im);
+}
+
+int lsd_tra_qst2rtp(lsd_ctx* ctx, const double* q_re, const double* q_im, const double* s_re, const double* s_im,
+                    const double* t_re, const double* t_im, double* r, double* th, double* ph) {
+  if (!ctx || !q_re || !q_im || !s_re || !s_im || !t_re || !t_im || !r || !th || !ph) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc;
+  if ((rc = ensure_phys(ctx, 3))) return rc;
+  if ((rc = spec_in(ctx, 0, q_re, q_im)) || (rc = spec_in(ctx, 1, s_re, s_im)) || (rc = spec_in(ctx, 2, t_re, t_im))) return rc;
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * ctx->Th;
+  SynthGroup g;
+  g.kind = SK_VECTOR;
+  for (int k = 0; k < 3; ++k) { g.in[k] = ctx->d_spec + k * F; g.out[k] = ctx->d_four + k * FF; }
+  if ((rc = time_begin(ctx))) return rc;
+  if ((rc = lsd_launch_synth(ctx, &g, 1))) return rc;
+  if ((rc = lsd_launch_c2r(ctx, ctx->d_four, ctx->d_phys, 3))) return rc;
+  if ((rc = time_end(ctx))) return rc;
+  size_t P = phys_count(ctx);
+  CUDA_TRY(cudaMemcpy(r, ctx->d_phys, sizeof(double) * P, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(th, ctx->d_phys + P, sizeof(double) * P, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(ph, ctx->d_phys + 2 * P, sizeof(double) * P, cudaMemcpyDeviceToHost));
+  return LSD_OK;
+}
+
+int lsd_tra_rtp2qst(lsd_ctx* ctx, const double* r, const double* th, const double* ph, double* q_re, double* q_im,
+                    double* s_re, double* s_im, double* t_re, double* t_im) {
+  if (!ctx || !q_re || !q_im || !s_re || !s_im || !t_re || !t_im || !r || !th || !ph) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc;
+  if ((rc = ensure_phys(ctx, 3))) return rc;
+  size_t P = phys_count(ctx);
+  CUDA_TRY(cudaMemcpy(ctx->d_phys, r, sizeof(double) * P, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(ctx->d_phys + P, th, sizeof(double) * P, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(ctx->d_phys + 2 * P, ph, sizeof(double) * P, cudaMemcpyHostToDevice));
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * ctx->Th;
+  AnalGroup g;
+  g.kind = AK_VECTOR;
+  for (int k = 0; k < 3; ++k) { g.in[k] = ctx->d_four + k * FF; g.out[k] = ctx->d_spec + k * F; }
+  if ((rc = time_begin(ctx))) return rc;
+  if ((rc = lsd_launch_r2c(ctx, ctx->d_phys, ctx->d_four, 3))) return rc;
+  if ((rc = lsd_launch_anal(ctx, &g, 1))) return rc;
+  if ((rc = time_end(ctx))) return rc;
+  if ((rc = spec_out(ctx, 0, q_re, q_im)) || (rc = spec_out(ctx, 1, s_re, s_im)) || (rc = spec_out(ctx, 2, t_re, t_im))) return rc;
+  return LSD_OK;
+}
+
+int lsd_tra_grad(lsd_ctx* ctx, const double* s_re, const double* s_im, double* th, double* ph) {
+  if (!ctx || !s_re || !s_im || !th || !ph) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc;
+  if ((rc = ensure_phys(ctx, 3))) return rc;
+  if ((rc = spec_in(ctx, 0, s_re, s_im))) return rc;
+  const size_t FF = (size_t)ctx->N * ctx->NM * ctx->Th;
+  SynthGroup g;
+  g.kind = SK_GRAD2;
+  g.in[0] = ctx->d_spec; g.in[1] = g.in[2] = nullptr;
+  g.out[0] = ctx->d_four; g.out[1] = ctx->d_four + FF; g.out[2] = nullptr;
+  if ((rc = time_begin(ctx))) return rc;
+  if ((rc = lsd_launch_synth(ctx, &g, 1))) return rc;
+  if ((rc = lsd_launch_c2r(ctx, ctx->d_four, ctx->d_phys, 2))) return rc;
+  if ((rc = time_end(ctx))) return rc;
+  size_t P = phys_count(ctx);
+  CUDA_TRY(cudaMemcpy(th, ctx->d_phys, sizeof(double) * P, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(ph, ctx->d_phys + P, sizeof(double) * P, cudaMemcpyDeviceToHost));
+  return LSD_OK;
+}
+
+// ---- device-resident batched transforms --------------------------------------------------
+int lsd_sht_synth_device(lsd_ctx* ctx, int nbatch, const double* d_spec, double* d_phys) {
+  if (!ctx || !d_spec || !d_phys || nbatch < 1) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * ctx->Th, P = phys_count(ctx);
+  const cplx* in = (const cplx*)d_spec;
+  for (int b0 = 0; b0 < nbatch; b0 += ctx->nfour) {
+    int nb = std::min(ctx->nfour, nbatch - b0);
+    for (int g0 = 0; g0 < nb; g0 += 6) {
+      SynthGroup g[6];
+      int ng = std::min(6, nb - g0);
+      for (int i = 0; i < ng; ++i) {
+        g[i].kind = SK_SCALAR;
+        g[i].in[0] = in + (size_t)(b0 + g0 + i) * F; g[i].in[1] = g[i].in[2] = nullptr;
+        g[i].out[0] = ctx->d_four + (size_t)(g0 + i) * FF; g[i].out[1] = g[i].out[2] = nullptr;
+      }
+      int rc = lsd_launch_synth(ctx, g, ng);
+      if (rc) return rc;
+    }
+    int rc = lsd_launch_c2r(ctx, ctx->d_four, d_phys + (size_t)b0 * P, nb);
+    if (rc) return rc;
+  }
+  return LSD_OK;
+}
+
+int lsd_sht_analys_device(lsd_ctx* ctx, int nbatch, const double* d_phys, double* d_spec) {
+  if (!ctx || !d_spec || !d_phys || nbatch < 1) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * ctx->Th, P = phys_count(ctx);
+  cplx* out = (cplx*)d_spec;
+  for (int b0 = 0; b0 < nbatch; b0 += ctx->nfour) {
+    int nb = std::min(ctx->nfour, nbatch - b0);
+    int rc = lsd_launch_r2c(ctx, d_phys + (size_t)b0 * P, ctx->d_four, nb);
+    if (rc) return rc;
+    for (int g0 = 0; g0 < nb; g0 += 4) {
+      AnalGroup g[4];
+      int ng = std::min(4, nb - g0);
+      for (int i = 0; i < ng; ++i) {
+        g[i].kind = AK_SCALAR;
+        g[i].in[0] = ctx->d_four + (size_t)(g0 + i) * FF; g[i].in[1] = g[i].in[2] = nullptr;
+        g[i].out[0] = out + (size_t)(b0 + g0 + i) * F; g[i].out[1] = g[i].out[2] = nullptr;
+      }
+      rc = lsd_launch_anal(ctx, g, ng);
+      if (rc) return rc;
+    }
+  }
+  return LSD_OK;
+}
+
+// ---- time stepping ---------------------------------------------------------------------
+int lsd_matrices(lsd_ctx* ctx) {
+  if (!ctx) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  return lsd_build_operators(ctx);
+}
+
+int lsd_nonlinear(lsd_ctx* ctx) {
+  if (!ctx) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc;
+  if ((rc = time_begin(ctx))) return rc;
+  if ((rc = lsd_eval(ctx))) return rc;
+  if ((rc = time_end(ctx))) return rc;
+  ctx->have_eval = true;
+  return LSD_OK;
+}
+
+int lsd_predictor(lsd_ctx* ctx) {
+  if (!ctx) return LSD_EARG;
+  if (!ctx->have_eval) return lsd_fail(ctx, LSD_ESTATE, "predictor needs a nonlinear evaluation first");
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc = lsd_pred(ctx);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->it = 1;
+  ctx->have_eval = false;
+  return LSD_OK;
+}
+
+int lsd_corrector(lsd_ctx* ctx, double* dterr) {
+  if (!ctx) return LSD_EARG;
+  if (!ctx->have_eval || ctx->it == 0) return lsd_fail(ctx, LSD_ESTATE, "corrector needs a predictor and an evaluation");
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  ctx->dterr = 0.0;
+  int rc = lsd_corr(ctx);
+  if (!rc) rc = finish_corrector(ctx);
+  if (rc) return rc;
+  if (dterr) *dterr = ctx->dterr;
+  ctx->have_eval = false;
+  return LSD_OK;
+}
+
+int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats) {
+  if (!ctx || nsteps < 0) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc;
+  long long l0 = ctx->launches;
+  if (!ctx->g_pred) {
+    if ((rc = capture(ctx, true, &ctx->g_pred, &ctx->g_pred_kernels))) return rc;
+    if ((rc = capture(ctx, false, &ctx->g_corr, &ctx->g_corr_kernels))) return rc;
+  }
+  const long long per_pred = ctx->g_pred_kernels, per_corr = ctx->g_corr_kernels;
+  int done = 0, corr = 0, evals = 0;
+  double last = 0.0;
+  if ((rc = time_begin(ctx))) return rc;
+  while (done < nsteps) {
+    if (ctx->it == 0) {
+      CUDA_TRY(cudaGraphLaunch(ctx->g_pred, ctx->stream));
+      ctx->launches += per_pred;
+      ++evals;
+      ctx->it = 1;
+    } else {
+      ctx->dterr = 0.0;
+      CUDA_TRY(cudaGraphLaunch(ctx->g_corr, ctx->stream));
+      ctx->launches += per_corr;
+      ++evals;
+      ++corr;
+      if ((rc = finish_corrector(ctx))) return rc;
+      last = ctx->dterr;
+      if ((rc = check_cgce(ctx))) return lsd_fail(ctx, rc, "tim_check_cgce: corrector iterations did not converge");
+    }
+    if (ctx->it == 0) {
+      ctx->t = ctx->t + ctx->dt;
+      ctx->step = ctx->step + 1;
+      ++done;
+    }
+  }
+  if ((rc = time_end(ctx))) return rc;
+  ctx->have_eval = false;
+  if (stats) {
+    stats->steps_done = done; stats->correctors = corr; stats->evaluations = evals;
+    stats->kernel_launches = (int)(ctx->launches - l0); stats->last_dterr = last;
+    stats->t = ctx->t; stats->dt = ctx->dt;
+  }
+  return LSD_OK;
+}
+
+int lsd_energies(lsd_ctx* ctx, double* out) {
+  if (!ctx || !out) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  return lsd_energy_device(ctx, out);
+}
+
+int lsd_banded_factor_device(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info) {
+  if (!ctx || n < 1 || kl < 1 || kl > LSD_MAX_KL || nmat < 1 || !d_ab || !d_ipiv || !d_info) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  return lsd_factor_batch(ctx, n, kl, nmat, d_ab, d_ipiv, d_info);
+}
+int lsd_banded_solve_device(lsd_ctx* ctx, int n, int kl, int nmat, const double* d_ab, const int* d_ipiv, int nrhs,
+                            const int* d_map, double* d_b) {
+  if (!ctx || n < 1 || kl < 1 || kl > LSD_MAX_KL || nmat < 1 || nrhs < 1 || !d_ab || !d_ipiv || !d_map || !d_b) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  return lsd_solve_batch(ctx, n, kl, nmat, d_ab, d_ipiv, nrhs, d_map, d_b);
+}
+
+int lsd_synchronize(lsd_ctx* ctx) {
+  if (!ctx) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return LSD_OK;
+}
+int lsd_last_elapsed_ms(const lsd_ctx* ctx, double* ms) {
+  if (!ctx || !ms) return LSD_EARG;
+  *ms = ctx->last_ms;
+  return LSD_OK;
+}
+int lsd_kernel_launches(const lsd_ctx* ctx, long long* count) {
+  if (!ctx || !count) return LSD_EARG;
+  *count = ctx->launches;
+  return LSD_OK;
+}
+
+}  // extern "C"

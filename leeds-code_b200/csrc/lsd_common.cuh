@@ -1,0 +1,147 @@
+// lsd_common.cuh -- shared declarations of the B200 dynamo-step library.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/lsd_b200.h"
+
+#define LSD_MAX_KL 8
+
+// complex FP64 stored as double2 (x = re, y = im)
+typedef double2 cplx;
+
+#define CUDA_TRY(expr)                                                               \
+  do {                                                                               \
+    cudaError_t e__ = (expr);                                                        \
+    if (e__ != cudaSuccess) {                                                        \
+      return lsd_fail(ctx, LSD_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e__)); \
+    }                                                                                \
+  } while (0)
+
+// Kernel families counted for lsd_kernel_launches
+#define LSD_LAUNCH(ctx) ((ctx)->launches++)
+
+// operator families (one banded LU + one band Y per l)
+enum OpFamily {
+  OP_VTOR = 0,  // velocity toroidal  (XTor/YTor, velocity.F90:72-103)
+  OP_VPOL = 1,  // velocity poloidal  (XPol/YPol, velocity.F90:104-131)
+  OP_VGRE = 2,  // Green's operator   (XGre, velocity.F90:134-146)
+  OP_COD = 3,   // codensity          (XC/YC, codensity.F90:37-79)
+  OP_COMP = 4,  // composition        (composition.F90:31-54)
+  OP_MTOR = 5,  // magnetic toroidal  (magnetic.F90:72-103)
+  OP_MPOL = 6,  // magnetic poloidal  (magnetic.F90:104-133)
+  OP_NFAM = 7
+};
+
+// synthesis group kinds (one CTA group = one output triple)
+enum SynthKind {
+  SK_VECTOR = 0,  // (q,s,t) -> (r,th,ph)                 tra_qst2rtp  :719-818
+  SK_SCALAR = 1,  // a -> a(th,ph)                         tra_spec2phys :472-520
+  SK_GRAD3 = 2,   // (dC, C) -> (P dC, P_ C/r, sin1mP iC/r) cod_transform+tra_grad
+  SK_GRAD2 = 3,   // C -> (P_ C/r, sin1mP iC/r)            tra_grad :955-1000
+};
+enum AnalKind {
+  AK_VECTOR = 0,  // (r,th,ph) -> (q,s,t)                 tra_rtp2qst :825-949
+  AK_SCALAR = 1,  // a -> a                                tra_phys2spec :527-602
+};
+
+struct SynthGroup {
+  int kind;
+  const cplx* in[3];   // spectral inputs [n][H]
+  cplx* out[3];        // theta-Fourier outputs [n][NM][Th]
+};
+struct AnalGroup {
+  int kind;
+  const cplx* in[3];   // theta-Fourier inputs [n][NM][Th]
+  cplx* out[3];        // spectral outputs [n][H]
+};
+
+struct lsd_ctx {
+  lsd_config cfg;
+  int L, M, Mp, N, KL, H, Th, Th2, Ph, Ma, Hc, Hr, NM, P2;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0;
+  long long launches = 0;
+  std::string err;
+  bool owns_stream = false;
+
+  // host layout
+  std::vector<int> hl, hm, hs, thm, mcount, mstart, mlen;
+  // device layout
+  int *d_l = nullptr, *d_m = nullptr, *d_s = nullptr, *d_mc = nullptr;
+  int *d_mstart = nullptr, *d_mlen = nullptr, *d_thm = nullptr, *d_lm2nh = nullptr;
+  // device Legendre tables, each [H][Th2] (== Fortran (Th2, H))
+  double *d_leg = nullptr;  // 8 tables contiguous, LSD_LEG_* order
+  double *d_gp = nullptr, *d_gw = nullptr, *d_sn = nullptr, *d_sn1 = nullptr;
+  // FFT twiddles
+  double2 *d_tw2 = nullptr;  // e^{+2 pi i k / P2}, k < P2
+  double2 *d_twh = nullptr;  // e^{+2 pi i k / Ph}, k < Ph
+  int nrad = 0;
+  int radices[16];
+  // radial mesh
+  double *d_r = nullptr;       // [7][N]: r^p, p = -3..3
+  double *d_dr = nullptr;      // [KL][N][2KL+1] bands (column-major per band, like Fortran)
+  double *d_r1dr = nullptr;    // [N][2KL+1]
+  double *d_radlap = nullptr;  // [N][2KL+1]
+  double *d_intr2dr = nullptr; // [N]
+  // operators: LAPACK band LU [fam][L][N][3KL+1] + ipiv [fam][L][N];
+  // solve layout [fam][N][3KL+1][L] + ipiv [fam][N][L]; Y bands [fam][N][2KL+1][L]
+  double *d_lu = nullptr, *d_lus = nullptr, *d_y = nullptr;
+  int *d_ipiv = nullptr, *d_ipivs = nullptr, *d_info = nullptr;
+  double *d_gre = nullptr;   // [L][2][N]
+  double *d_invg = nullptr;  // [L][4]
+  bool have_ops = false;
+  double op_dt = 0.0;
+  // state, nonlinear terms, saved nonlinear terms: [field][N][H] complex
+  cplx *d_state = nullptr, *d_nl = nullptr, *d_sv = nullptr;
+  // spectral scratch: qst etc. [slot][N][H]
+  cplx *d_spec = nullptr;
+  int nspec = 0;
+  // theta-Fourier scratch: [slot][N][NM][Th]
+  cplx *d_four = nullptr;
+  int nfour = 0;
+  // physical scratch for host-buffer transforms: [slot][N][Ph][Th]
+  double *d_phys = nullptr;
+  int nphys = 0;
+  // host staging (pinned)
+  double *h_pin = nullptr;
+  size_t h_pin_bytes = 0;
+  // reductions
+  double *d_red = nullptr;   // small reduction area
+  double *h_red = nullptr;   // pinned mirror
+  // time
+  double t = 0.0, dt = 0.0, dterr = 0.0, corr_dt = 0.0, lasterr = 1e99;
+  int it = 0, step = 0;
+  bool have_eval = false;
+  int tim_pcn = -1;
+  // CUDA graph of one (evaluation + predictor/corrector) pass
+  cudaGraphExec_t g_pred = nullptr, g_corr = nullptr;
+  long long g_pred_kernels = 0, g_corr_kernels = 0;
+};
+
+int lsd_fail(lsd_ctx* ctx, int code, const std::string& msg);
+
+// ---- tables (lsd_tables.cu) ----
+int lsd_build_tables(lsd_ctx* ctx);
+int lsd_build_operators(lsd_ctx* ctx);
+// ---- transforms (lsd_sht.cu, lsd_fft.cu) ----
+int lsd_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups);
+int lsd_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups);
+int lsd_launch_c2r(lsd_ctx* ctx, const cplx* four, double* phys, int nfields);
+int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields);
+int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out);
+// ---- spectral algebra and solves (lsd_solve.cu) ----
+int lsd_eval(lsd_ctx* ctx);            // one nonlinear evaluation (device)
+int lsd_pred(lsd_ctx* ctx);            // predictor solves (device)
+int lsd_corr(lsd_ctx* ctx);            // corrector solves + dterr (device)
+int lsd_energy_device(lsd_ctx* ctx, double* out);
+int lsd_factor_batch(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info);
+int lsd_solve_batch(lsd_ctx* ctx, int n, int kl, int nmat, const double* d_ab, const int* d_ipiv,
+                    int nrhs, const int* d_map, double* d_b);
+
+// small helpers
+static inline int ceil_div(int a, int b) { return (a + b - 1) / b; }

@@ -1,0 +1,436 @@
+// lsd_tables.cu -- FP64 device construction of the static tables of one context:
+// Gauss-Legendre points and weights (auxiliary/gauwts.f), Schmidt P_l^m and dP/dtheta
+// with the derived transform tables (legendre.F90:63-128, auxiliary/schnla.f and helpers),
+// the radial Chebyshev grid with finite-difference weights and integration weights
+// (meshs.F90:116-419), and the banded time-stepping operators with their LU factors
+// (timestep.F90:47-546, velocity.F90:56-273, codensity.F90:37-119, magnetic.F90:62-282).
+#include <cmath>
+#include <cstdio>
+
+#include "lsd_banded.cuh"
+#include "lsd_common.cuh"
+
+namespace {
+
+// ---------------------------------------------------------------------------------------
+// Gauss-Legendre nodes on [-1, 1], ascending (gauwts.f:43-71)
+// ---------------------------------------------------------------------------------------
+__global__ void k_gauss(int nth, double* gp, double* gw, int* fail) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int m = (nth + 1) / 2;
+  if (i > m) return;
+  const double EPS = 1.0e-13, PI = 3.14159265358979312;
+  const double xm = 0.0, xl = 1.0;  // 0.5*(x2+x1), 0.5*(x2-x1) with x1=-1, x2=1
+  double z = cos(PI * ((double)i - 0.25) / ((double)nth + 0.5));
+  double z1, pp;
+  int iter = 0;
+  do {
+    double p1 = 1.0, p2 = 0.0, p3;
+    for (int j = 1; j <= nth; ++j) {
+      p3 = p2; p2 = p1;
+      p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / (double)j;
+    }
+    pp = nth * (z * p1 - p2) / (z * z - 1.0);
+    z1 = z;
+    z = z1 - p1 / pp;
+    if (++iter > 200) { atomicExch(fail, 1); break; }  // bounded Newton loop
+  } while (fabs(z - z1) > EPS);
+  gp[i - 1] = xm - xl * z;
+  gp[nth - i] = xm + xl * z;
+  gw[i - 1] = 2.0 * xl / ((1.0 - z * z) * pp * pp);
+  gw[nth - i] = gw[i - 1];
+}
+
+__global__ void k_trig(int nth, const double* gp, double* sn, double* sn1) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nth) return;
+  double th = acos(gp[j]);
+  sn[j] = sin(th);
+  sn1[j] = 1.0 / sn[j];
+}
+
+// Schmidt helpers (pmm.f, pmm1.f, plm.f, dpmm.f, dpmm1.f, dplm.f)
+__device__ double d_pmm(int m, double s) {
+  if (m == 0) return 1.0;
+  double p = sqrt(2.0);
+  for (int i = 1; i <= m; ++i) { double twoi = 2.0 * i; p = p * s * sqrt((twoi - 1.0) / twoi); }
+  return p;
+}
+__device__ double d_dpmm(int m, double c, double s) {
+  if (m == 0) return 0.0;
+  double d = sqrt(2.0) * (double)m * c / s;
+  for (int i = 1; i <= m; ++i) { double twoi = 2.0 * i; d = d * s * sqrt((twoi - 1.0) / twoi); }
+  return d;
+}
+
+// One thread per (theta point j of the southern half grid, order index m): the
+// three-term recurrences in l of schnla.f:66-109 for m_ = m*Mp, then the eight tables.
+// Tables are stored [table][nh][Th2] (Fortran leg_*(Th2, 0:H-1)).
+__global__ void k_legendre(int L, int M, int Mp, int H, int Th2, const double* gp, const double* gw,
+                           const double* sn1, const int* lm2nh, double* leg, int* fail) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  int m = blockIdx.y;
+  if (j >= Th2 || m >= M) return;
+  const double x = gp[j];
+  const double sine = sqrt((1.0 + x) * (1.0 - x));
+  if (sine < 1.0e-6) { atomicExch(fail, 2); return; }
+  const int m_ = m * Mp;
+  const size_t T = (size_t)H * Th2;
+  double p2 = 0.0, p1 = 0.0, d2 = 0.0, d1 = 0.0;
+  for (int l = m_; l < L; ++l) {
+    double pa, dpa;
+    if (l == m_) {
+      pa = d_pmm(m_, sine);
+      dpa = d_dpmm(m_, x, sine);
+    } else if (l == m_ + 1) {
+      pa = x * p1 * sqrt(2.0 * m_ + 1.0);
+      dpa = sqrt(2.0 * m_ + 1.0) * (x * d1 - sine * p1);
+    } else {
+      double rm = m_, rl = l;
+      pa = (2.0 * rl - 1.0) * x * p1;
+      pa = pa - p2 * sqrt((rl + rm - 1.0) * (rl - rm - 1.0));
+      pa = pa / sqrt((rl + rm) * (rl - rm));
+      dpa = (2.0 * rl - 1.0) * (x * d1 - sine * p1);
+      dpa = dpa - d2 * sqrt((rl + rm - 1.0) * (rl - rm - 1.0));
+      dpa = dpa / sqrt((rl + rm) * (rl - rm));
+    }
+    p2 = p1; p1 = pa; d2 = d1; d1 = dpa;
+    int nh = lm2nh[m * L + l];
+    if (nh < 0) continue;
+    size_t id = (size_t)nh * Th2 + j;
+    double s1 = sn1[j];
+    leg[LSD_LEG_P * T + id] = pa;
+    leg[LSD_LEG_P_ * T + id] = dpa;
+    leg[LSD_LEG_SIN1MP * T + id] = pa * m_ * s1;
+    double w = gw[j] * ((2.0 * l + 1.0) / 4.0);
+    if (m == 0) w = 2.0 * w;
+    leg[LSD_LEG_GWP * T + id] = pa * w;
+    if (l == 0) {
+      leg[LSD_LEG_LLP_ * T + id] = 0.0;
+      leg[LSD_LEG_LLSIN1MP * T + id] = 0.0;
+      leg[LSD_LEG_GWLLP_ * T + id] = 0.0;
+      leg[LSD_LEG_GWLLSIN1MP * T + id] = 0.0;
+    } else {
+      double w1 = 1.0 / sqrt((double)(l * (l + 1)));
+      leg[LSD_LEG_LLP_ * T + id] = dpa * w1;
+      leg[LSD_LEG_LLSIN1MP * T + id] = pa * w1 * m_ * s1;
+      double w2 = w / sqrt((double)(l * (l + 1)));
+      leg[LSD_LEG_GWLLP_ * T + id] = dpa * w2;
+      leg[LSD_LEG_GWLLSIN1MP * T + id] = pa * w2 * m_ * s1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Radial mesh (meshs.F90:135-143, 228-419), Boussinesq profile (rho = 0, eta = 1)
+// ---------------------------------------------------------------------------------------
+__global__ void k_grid(int N, double rratio, double alpha, double* r) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (n > N) return;
+  const double PI = 3.1415926535897931;
+  double x;
+  if (alpha > 0)
+    x = 0.5 * (1.0 + asin(alpha * cos(PI * (N - n) / (double)(N - 1))) / asin(alpha));
+  else
+    x = 0.5 * (1.0 + cos(PI * (N - n) / (double)(N - 1)));
+  double ri = rratio / (1.0 - rratio);
+  x = x + ri;
+  for (int p = -3; p <= 3; ++p) {  // integer powers as products, like gfortran's r**p
+    double y = 1.0;
+    int ap = p < 0 ? -p : p;
+    for (int k = 0; k < ap; ++k) y = (k == 0) ? x : y * x;
+    r[(size_t)(p + 3) * N + (n - 1)] = p < 0 ? 1.0 / y : (p == 1 ? x : y);
+  }
+}
+
+// FD weights at point n by inverting the local Taylor matrix; integration-weight
+// contributions w(n, i, j) kept for an ordered sum.
+__global__ void k_fdweights(int N, int KL, const double* r, double* dr, double* wcontrib, int* fail) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (n > N) return;
+  const int lda = 2 * KL + 1;
+  double A[(2 * LSD_MAX_KL + 1) * (2 * LSD_MAX_KL + 1)];
+  const double* r1 = r + (size_t)4 * N;  // r^1
+  const double* r2 = r + (size_t)5 * N;  // r^2
+#define Aa(i, j) A[((i) - 1) + lda * ((j) - 1)]
+  int l = max(1, n - KL), rr = min(n + KL, N), nn = rr - l + 1;
+  for (int i = 1; i <= nn; ++i) Aa(i, 1) = 1.0;
+  for (int j = 2; j <= nn; ++j)
+    for (int i = 1; i <= nn; ++i) Aa(i, j) = Aa(i, j - 1) * (r1[l + i - 2] - r1[n - 1]) / (double)(j - 1);
+  if (dev_mat_invert(nn, A, lda) != 0) { atomicExch(fail, 3); return; }
+  const size_t band = (size_t)(2 * KL + 1) * N;
+  for (int i = 1; i <= KL; ++i)
+    for (int j = l; j <= rr; ++j) dr[(i - 1) * band + (size_t)(KL + n - j) + (size_t)(2 * KL + 1) * (j - 1)] = Aa(i + 1, j - l + 1);
+  double c = 1.0, e = 1.0;
+  for (int i = 1; i <= nn; ++i) {
+    c = c * (r1[min(n + 1, N) - 1] - r1[n - 1]) / (double)i;
+    e = e * (r1[max(1, n - 1) - 1] - r1[n - 1]) / (double)i;
+    for (int j = l; j <= rr; ++j) {
+      double w = 0.5 * (c - e) * Aa(i, j - l + 1) * r2[n - 1];
+      wcontrib[((size_t)(n - 1) * lda + (i - 1)) * lda + (j - l)] = w;
+    }
+  }
+#undef Aa
+}
+
+// intr2dr(j) = sum over n ascending, i ascending of the contributions (meshs.F90:311-336)
+__global__ void k_intr2dr(int N, int KL, const double* wcontrib, double* intr2dr) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (j > N) return;
+  const int lda = 2 * KL + 1;
+  double s = 0.0;
+  for (int n = max(1, j - KL); n <= min(j + KL, N); ++n) {
+    int l = max(1, n - KL), rr = min(n + KL, N), nn = rr - l + 1;
+    for (int i = 1; i <= nn; ++i) s = s + wcontrib[((size_t)(n - 1) * lda + (i - 1)) * lda + (j - l)];
+  }
+  intr2dr[j - 1] = s;
+}
+
+// radLap = dr2 + dr1*2/r ; r1dr = dr1 + diag(1/r)   (meshs.F90:339-415)
+__global__ void k_bands(int N, int KL, const double* r, const double* dr, double* radlap, double* r1dr) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (j > N) return;
+  const size_t band = (size_t)(2 * KL + 1) * N;
+  const double* rm1 = r + (size_t)2 * N;
+  for (int row = 1; row <= 2 * KL + 1; ++row) {
+    size_t id = (size_t)(row - 1) + (size_t)(2 * KL + 1) * (j - 1);
+    int n = row - KL - 1 + j;
+    double v = 0.0;
+    if (n >= 1 && n <= N) v = dr[band + id] + dr[id] * 2.0 * rm1[n - 1];
+    radlap[id] = v;
+    double w = dr[id];
+    if (row == KL + 1) w = w + rm1[j - 1];
+    r1dr[id] = w;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Operators.  One thread per (family, l): build X in LAPACK band storage, apply the
+// boundary rows, factorise; build Y in the solve layout [fam][N][2KL+1][L].
+// ---------------------------------------------------------------------------------------
+struct OpParams {
+  double c1_[OP_NFAM], c2_[OP_NFAM], c2y[OP_NFAM];
+  double Hyp;
+  int vel_bc, cod_bc, comp_bc;
+};
+
+__global__ void k_build_ops(int N, int KL, int L, const double* r, const double* dr, const double* radlap,
+                            OpParams P, double* lu, int* ipiv, double* y, int* info) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  int fam = blockIdx.y;
+  if (l >= L) return;
+  const int ld = 3 * KL + 1, ldm = 2 * KL + 1;
+  double* A = lu + ((size_t)fam * L + l) * (size_t)ld * N;
+  int* ip = ipiv + ((size_t)fam * L + l) * N;
+  const double* rm1 = r + (size_t)2 * N;
+  const double* rm2 = r + (size_t)1 * N;
+  const size_t band = (size_t)ldm * N;
+#define AX(i, j) A[(size_t)((i) - 1) + (size_t)ld * ((j) - 1)]
+#define MB(B, i, j) (B)[(size_t)((i) - 1) + (size_t)ldm * ((j) - 1)]
+  for (size_t i = 0; i < (size_t)ld * N; ++i) A[i] = 0.0;
+  bool skip_l0 = (fam != OP_COD && fam != OP_COMP);
+  if (l == 0 && skip_l0) {  // never solved: keep an identity so the factors are defined
+    for (int j = 1; j <= N; ++j) AX(2 * KL + 1, j) = 1.0;
+    info[fam * L + l] = dev_dgbtf2(N, KL, A, ld, ip);
+    return;
+  }
+  const double c1_ = P.c1_[fam], c2_ = P.c2_[fam], c2y = P.c2y[fam];
+  const double ll1 = (double)(l * (l + 1));
+  // A(KL+1:, :) = -c2_ * Lap  (radLap == radLap_flayer == GreLap == MagTorLap == MagPolLap
+  // bit for bit in the Boussinesq case: f_factor = 1, xi = 0, eta = 1, deta = 0)
+  for (int j = 1; j <= N; ++j)
+    for (int row = 1; row <= ldm; ++row) {
+      double v = MB(radlap, row, j);
+      AX(KL + row, j) = (fam == OP_MTOR || fam == OP_MPOL) ? 0.0 - c2_ * v : -c2_ * v;
+    }
+  for (int n = 1; n <= N; ++n) {
+    double t = ll1 * rm2[n - 1];
+    if (fam == OP_MTOR || fam == OP_MPOL)
+      AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * ll1 * rm2[n - 1];
+    else
+      AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * (t + P.Hyp * t * t);
+  }
+  for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = 0.0;
+  for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = 0.0;
+  // boundary rows
+  switch (fam) {
+    case OP_VTOR:  // vel_bc_Tor (velocity.F90:177-201)
+      if (P.vel_bc == 1 || P.vel_bc == 2) AX(2 * KL + 1, 1) = 1.0;
+      else {
+        for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
+        AX(2 * KL + 1, 1) = AX(2 * KL + 1, 1) - rm1[0];
+      }
+      if (P.vel_bc == 1 || P.vel_bc == 3) AX(2 * KL + 1, N) = 1.0;
+      else {
+        for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
+        AX(2 * KL + 1, N) = AX(2 * KL + 1, N) - rm1[N - 1];
+      }
+      break;
+    case OP_VPOL:  // vel_bc_Pol (velocity.F90:207-254), Boussinesq
+      if (P.vel_bc == 1 || P.vel_bc == 2)
+        for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
+      else
+        for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr + band, KL + 1 + 1 - j, j);
+      if (P.vel_bc == 1 || P.vel_bc == 3)
+        for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
+      else
+        for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr + band, KL + 1 + N - j, j);
+      break;
+    case OP_VGRE:  // vel_bc_Gre (velocity.F90:260-267)
+      AX(2 * KL + 1, 1) = 1.0;
+      AX(2 * KL + 1, N) = 1.0;
+      break;
+    case OP_COD:
+    case OP_COMP: {  // cod_bc_C (codensity.F90:85-112)
+      int bc = fam == OP_COD ? P.cod_bc : P.comp_bc;
+      if (bc == 1 || bc == 2) AX(2 * KL + 1, 1) = 1.0;
+      else for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
+      if (bc == 1 || bc == 3) AX(2 * KL + 1, N) = 1.0;
+      else for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
+      break;
+    }
+    case OP_MTOR:  // mag_bc_Tor (magnetic.F90:137-192), Ni = 1
+      AX(2 * KL + 1, 1) = 1.0;
+      AX(2 * KL + 1, N) = 1.0;
+      break;
+    case OP_MPOL:  // mag_bc_Pol (magnetic.F90:198-282), insulating, Ni = 1
+      for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
+      AX(2 * KL + 1, 1) = AX(2 * KL + 1, 1) - rm1[0] * l;
+      for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
+      AX(2 * KL + 1, N) = AX(2 * KL + 1, N) + rm1[N - 1] * (l + 1);
+      break;
+  }
+  info[fam * L + l] = dev_dgbtf2(N, KL, A, ld, ip);
+  // Y = c2y*Lap ; diag += c1_ - c2y*(l(l+1)/r^2 + Hyp (.)^2)   (tim_mesh_Y / _flayer_Y)
+  if (fam != OP_VGRE) {
+    for (int j = 1; j <= N; ++j)
+      for (int row = 1; row <= ldm; ++row) {
+        double v = c2y * MB(radlap, row, j);
+        if (row == KL + 1) {
+          double t = (double)(l * (l + 1)) * rm2[j - 1];
+          v = v + c1_ - c2y * (t + P.Hyp * t * t);
+        }
+        y[(((size_t)fam * N + (j - 1)) * ldm + (row - 1)) * L + l] = v;
+      }
+  }
+#undef AX
+#undef MB
+}
+
+// LAPACK layout [fam][L][N][3KL+1] -> solve layout [fam][N][3KL+1][L]
+__global__ void k_lu_transpose(int N, int KL, int L, const double* lu, const int* ipiv, double* lus, int* ipivs) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y;
+  int fam = blockIdx.z;
+  if (l >= L) return;
+  const int ld = 3 * KL + 1;
+  const double* A = lu + (((size_t)fam * L + l) * N + j) * ld;
+  for (int row = 0; row < ld; ++row) lus[(((size_t)fam * N + j) * ld + row) * L + l] = A[row];
+  ipivs[((size_t)fam * N + j) * L + l] = ipiv[((size_t)fam * L + l) * N + j];
+}
+
+// Green's functions and influence matrices (velocity.F90:148-168)
+__global__ void k_greens(int N, int KL, int L, const double* lu, const int* ipiv, double* gre, double* invg, int* fail) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l < 1 || l >= L) return;
+  const int ld = 3 * KL + 1;
+  const double* Agre = lu + ((size_t)OP_VGRE * L + l) * (size_t)ld * N;
+  const int* pgre = ipiv + ((size_t)OP_VGRE * L + l) * N;
+  const double* Apol = lu + ((size_t)OP_VPOL * L + l) * (size_t)ld * N;
+  const int* ppol = ipiv + ((size_t)OP_VPOL * L + l) * N;
+  double* g1 = gre + (size_t)l * 2 * N;
+  double* g2 = g1 + N;
+  for (int n = 0; n < N; ++n) { g1[n] = 0.0; g2[n] = 0.0; }
+  g1[0] = 1.0;
+  g2[N - 1] = 1.0;
+  dev_dgbtrs1(N, KL, Agre, ld, pgre, g1);
+  dev_dgbtrs1(N, KL, Agre, ld, pgre, g2);
+  g1[0] = 0.0; g1[N - 1] = 0.0; g2[0] = 0.0; g2[N - 1] = 0.0;
+  dev_dgbtrs1(N, KL, Apol, ld, ppol, g1);
+  dev_dgbtrs1(N, KL, Apol, ld, ppol, g2);
+  double a[4] = {g1[0], g1[N - 1], g2[0], g2[N - 1]};  // invG(i,j) at a[(i-1)+2(j-1)]
+  if (dev_mat_invert(2, a, 2) != 0) atomicExch(fail, 4);
+  for (int k = 0; k < 4; ++k) invg[(size_t)l * 4 + k] = a[k];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+int lsd_build_tables(lsd_ctx* ctx) {
+  const int Th = ctx->Th, Th2 = ctx->Th2, H = ctx->H, N = ctx->N, KL = ctx->KL, L = ctx->L, M = ctx->M;
+  cudaStream_t s = ctx->stream;
+  int* d_fail = nullptr;
+  CUDA_TRY(cudaMalloc(&d_fail, sizeof(int)));
+  CUDA_TRY(cudaMemsetAsync(d_fail, 0, sizeof(int), s));
+  k_gauss<<<ceil_div((Th + 1) / 2, 128), 128, 0, s>>>(Th, ctx->d_gp, ctx->d_gw, d_fail);
+  k_trig<<<ceil_div(Th, 128), 128, 0, s>>>(Th, ctx->d_gp, ctx->d_sn, ctx->d_sn1);
+  dim3 gl(ceil_div(Th2, 64), M);
+  k_legendre<<<gl, 64, 0, s>>>(L, M, ctx->Mp, H, Th2, ctx->d_gp, ctx->d_gw, ctx->d_sn1, ctx->d_lm2nh, ctx->d_leg, d_fail);
+  k_grid<<<ceil_div(N, 128), 128, 0, s>>>(N, ctx->cfg.rratio, ctx->cfg.alpha, ctx->d_r);
+  double* wc = nullptr;
+  size_t lda = 2 * KL + 1;
+  CUDA_TRY(cudaMalloc(&wc, sizeof(double) * N * lda * lda));
+  CUDA_TRY(cudaMemsetAsync(ctx->d_dr, 0, sizeof(double) * KL * lda * N, s));
+  k_fdweights<<<ceil_div(N, 64), 64, 0, s>>>(N, KL, ctx->d_r, ctx->d_dr, wc, d_fail);
+  k_intr2dr<<<ceil_div(N, 128), 128, 0, s>>>(N, KL, wc, ctx->d_intr2dr);
+  k_bands<<<ceil_div(N, 128), 128, 0, s>>>(N, KL, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_r1dr);
+  ctx->launches += 7;
+  CUDA_TRY(cudaGetLastError());
+  int fail = 0;
+  CUDA_TRY(cudaMemcpyAsync(&fail, d_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(wc);
+  cudaFree(d_fail);
+  if (fail == 2) return lsd_fail(ctx, LSD_EARG, "schnla: sin(theta) too small (legendre)");
+  if (fail) return lsd_fail(ctx, LSD_ESINGULAR, "table construction failed (code " + std::to_string(fail) + ")");
+  return LSD_OK;
+}
+
+int lsd_build_operators(lsd_ctx* ctx) {
+  const int N = ctx->N, KL = ctx->KL, L = ctx->L;
+  const lsd_config& c = ctx->cfg;
+  cudaStream_t s = ctx->stream;
+  OpParams P;
+  const double dt = ctx->dt;
+  const double impl = c.implicit;
+  auto setf = [&](int fam, double c1, double c2) {
+    P.c1_[fam] = c1 / dt;
+    P.c2_[fam] = (impl == 0.0) ? 1.0 : c2 * impl;
+    P.c2y[fam] = c2 * (1.0 - impl);
+  };
+  setf(OP_VTOR, 1.0, c.Pm);
+  setf(OP_VPOL, 1.0, c.Pm);
+  setf(OP_VGRE, 0.0, 1.0 / impl);
+  setf(OP_COD, c.Pr / c.Pm, 1.0);
+  setf(OP_COMP, c.Sc / c.Pm, 1.0);
+  setf(OP_MTOR, 1.0, 1.0);
+  setf(OP_MPOL, 1.0, 1.0);
+  P.Hyp = c.Hyp;
+  P.vel_bc = c.vel_bc; P.cod_bc = c.cod_bc; P.comp_bc = c.comp_bc;
+  int* d_fail = nullptr;
+  CUDA_TRY(cudaMalloc(&d_fail, sizeof(int)));
+  CUDA_TRY(cudaMemsetAsync(d_fail, 0, sizeof(int), s));
+  CUDA_TRY(cudaMemsetAsync(ctx->d_y, 0, sizeof(double) * OP_NFAM * N * (2 * KL + 1) * L, s));
+  dim3 g(ceil_div(L, 32), OP_NFAM);
+  k_build_ops<<<g, 32, 0, s>>>(N, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap, P, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_info);
+  dim3 gt(ceil_div(L, 64), N, OP_NFAM);
+  k_lu_transpose<<<gt, 64, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_lus, ctx->d_ipivs);
+  k_greens<<<ceil_div(L, 32), 32, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_gre, ctx->d_invg, d_fail);
+  ctx->launches += 3;
+  CUDA_TRY(cudaGetLastError());
+  std::vector<int> info((size_t)OP_NFAM * L);
+  int fail = 0;
+  CUDA_TRY(cudaMemcpyAsync(info.data(), ctx->d_info, sizeof(int) * info.size(), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(&fail, d_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(d_fail);
+  for (int fam = 0; fam < OP_NFAM; ++fam)
+    for (int l = 0; l < L; ++l)
+      if (info[(size_t)fam * L + l] != 0)
+        return lsd_fail(ctx, LSD_ESINGULAR, "mes_lu_find: zero pivot in operator family " + std::to_string(fam) +
+                                                " l=" + std::to_string(l));
+  if (fail) return lsd_fail(ctx, LSD_ESINGULAR, "influence matrix inversion failed (vel_matrices)");
+  ctx->have_ops = true;
+  ctx->op_dt = dt;
+  return LSD_OK;
+}
