@@ -1,0 +1,351 @@
+"""Benchmark of the B200 dynamo timestep (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision best|fp64|ozaki] [--workload dynamo128|parity32]
+
+Workload (default dynamo128): the full Boussinesq MHD + codensity step at lmax = mmax =
+127 (L = M = 128, Th = 192, Ph = 384), Nr = 129, E = 3e-4, Ra = 200, Pr = 1, Pm = 3,
+dt = 2e-6, from the seeded synthetic state (l^-2 spectrum, sin(pi (r - ri)) profile).
+A "step" is one timestep: predictor evaluation + predictor solves + corrector
+evaluation(s) + corrector solves until tim_check_cgce converges.
+
+value  = timesteps/s over all ranks (independent replicas, one per GPU, no collective
+         inside a step), device time from CUDA events on the library's stream, max
+         over ranks.  The per-step working set (theta-Fourier buffers ~0.8 GB) is far
+         larger than the 126 MB L2, so no flush is needed between steps.
+e2e    = the same metric through the public API with host buffers: every step uploads
+         the five state fields from host memory, steps, and reads the energies back.
+roofline: the dominant phase of the step (CUDA-event phase timings), algorithmic
+         bytes or flops per launch over its measured duration.
+cpu_baseline: the CPU oracle (C++ restatement of the reference path, OpenMP over shells
+         and harmonics) timed on this host for one timestep of the same workload.
+--impl reference: the same metric for the CPU oracle (the Fortran reference needs a
+         Fortran compiler, FFTW, LAPACK and netCDF, none of which exists on this image).
+"""
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(name, precision):
+    pkg = importlib.import_module("leeds-code_b200")
+    syn = pkg.synthetic
+    capi = pkg.capi
+    prec = capi.PREC_OZAKI if precision == "ozaki" else capi.PREC_FP64
+    if name == "parity32":
+        cfg = syn.config_parity(precision=prec)
+        desc = "Boussinesq MHD shell L=M=32 (lmax=31), Nr=33, Th=48, Ph=96, dt=1e-5"
+    else:
+        cfg = syn.config_dynamo128(precision=prec)
+        desc = "Boussinesq MHD dynamo step lmax=mmax=127 (L=M=128), Nr=129, Th=192, Ph=384, dt=2e-6"
+    return cfg, desc
+
+
+def legendre_flops(sz, N):
+    """Algorithmic Legendre flops of one evaluation: synthesis 92 and analysis 44 complex x
+    real multiply-adds (4 flops) per (harmonic, half-grid theta, shell)."""
+    base = sz["H"] * sz["Th2"] * N
+    return 92 * base, 44 * base
+
+
+def fft_flops(sz, N):
+    """2.5 n log2 n per real FFT of length n = Ph, 22 transforms per (theta, shell)."""
+    n = sz["Ph"]
+    return 22 * sz["Th"] * N * 2.5 * n * np.log2(n)
+
+
+def phase_roofline(ctx, peaks, src):
+    """Phase timings of one step and the roofline entry of the dominant phase."""
+    ph = ctx.profile_phases()
+    for _ in range(2):  # repeat, keep the minimum (first call includes graph warm paths)
+        p2 = ctx.profile_phases()
+        ph = {k: min(ph[k], p2[k]) for k in ph}
+    sz = ctx.sizes
+    N = sz["N"]
+    F = N * sz["H"] * 16
+    FF = N * 2 * sz["Hc"] * sz["Th"] * 16
+    syn_fl, ana_fl = legendre_flops(sz, N)
+    # algorithmic HBM bytes per phase launch
+    bytes_ = {
+        "spectral_prep": (5 + 13) * F,
+        "synthesis": 13 * F + 15 * FF,
+        "fft_products": 22 * FF,
+        "analysis": 7 * FF + 7 * F,
+        "spectral_tail": (7 + 2 + 5) * F,
+        "predictor_solve": 5 * 3 * F,
+        "corrector_solve": 5 * 5 * F,
+    }
+    dom = max(ph, key=ph.get)
+    ms = ph[dom]
+    hbm = peaks["hbm_gbs"]
+    rf = {"kernel": dom, "bound": "hbm", "unit": "GB/s", "peak": hbm,
+          "achieved": bytes_[dom] / (ms * 1e-3) / 1e9, "bytes_per_launch": bytes_[dom],
+          "ms_per_launch": ms, "peak_source": src}
+    rf["frac"] = rf["achieved"] / rf["peak"]
+    if dom in ("synthesis", "analysis"):
+        fl = syn_fl if dom == "synthesis" else ana_fl
+        rf["fp64_tflops"] = fl / (ms * 1e-3) / 1e12
+    return ph, rf
+
+
+def cpu_oracle_step(cfg, threads):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    pkg = importlib.import_module("leeds-code_b200")
+    ol.set_threads(threads)
+    o = ol.Oracle(cfg)
+    for f, (re, im) in pkg.synthetic.boussinesq_state(cfg).items():
+        o.set_coll(f, re, im)
+    return o
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU oracle on this host, rank 0 only."""
+    cfg, desc = workload(args.workload, "fp64")
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    o = cpu_oracle_step(cfg, threads)
+    t0 = time.perf_counter()
+    o.step(1)  # warm-up (first-touch of buffers)
+    t_one = time.perf_counter() - t0
+    warm = 1
+    while warm < args.warmup and t_one * (warm + 1) < 60:
+        o.step(1)
+        warm += 1
+    k = max(1, min(args.steps, int(150.0 / max(t_one, 1e-3))))
+    t0 = time.perf_counter()
+    o.step(k)
+    dt = time.perf_counter() - t0
+    v = k / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "timesteps/s", "n_gpus": world,
+        "steps": k, "warmup": warm, "ms_per_step": 1e3 * dt / k, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": desc, "parallelism": "cpu-openmp"},
+        "cpu_baseline": {"value": v, "unit": "timesteps/s", "cores": threads, "kind": "port",
+                         "sample": "%d full timesteps of the workload after %d warm-up (timed steps capped at ~150 s)" % (k, warm)},
+        "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "timesteps/s lmax127 Nr129: mixed vs FP64 GPU at <=1e-9 energy err; SHT TF/s"
+
+
+def run_ours(args, rank, world, local_rank, dist):
+    import torch
+    pkg = importlib.import_module("leeds-code_b200")
+    capi = pkg.capi
+    peaks, src = load_peaks()
+    precisions = ["fp64"] if args.precision == "fp64" else (["ozaki"] if args.precision == "ozaki" else ["fp64", "ozaki"])
+    results = {}
+    for prec in precisions:
+        cfg, desc = workload(args.workload, prec)
+        cfg.device = local_rank
+        try:
+            ctx = pkg.Context(cfg)
+        except pkg.LsdError as e:
+            results[prec] = {"error": str(e)}
+            continue
+        fields = pkg.synthetic.boussinesq_state(cfg, seed=pkg.synthetic.SEED + rank)
+        ctx.load_fields(fields)
+        st = ctx.step(args.warmup)
+        ctx.synchronize()
+        if dist:
+            dist.barrier()
+        sampler = ClockSampler(local_rank) if rank == 0 else None
+        if sampler:
+            sampler.start()
+        l0 = ctx.kernel_launches()
+        st = ctx.step(args.steps)
+        ms = ctx.last_elapsed_ms()
+        launches = ctx.kernel_launches() - l0
+        clocks = sampler.stop() if sampler else None
+        if dist:
+            t = torch.tensor([ms], device="cuda:%d" % local_rank, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        e = ctx.energies()
+        res = {"ms": ms, "steps": st.steps_done, "correctors": st.correctors, "launches": launches,
+               "clocks": clocks, "energies": e, "desc": desc}
+        # end-to-end through the public API with host buffers
+        ne = max(1, min(args.steps, 5))
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            ctx.load_fields(fields)
+            ctx.step(1)
+            ctx.energies()
+        ctx.synchronize()
+        res["e2e_s"] = (time.perf_counter() - t0) / ne
+        res["h2d"] = 5 * ctx.N * ctx.H * 16
+        res["d2h"] = (48 + 2) * ctx.N * 8 + 3 * 16
+        ph, rf = phase_roofline(ctx, peaks, src)
+        res["phases_ms"] = ph
+        res["roofline"] = rf
+        res["sizes"] = ctx.sizes
+        results[prec] = res
+        ctx.close()
+    if rank != 0:
+        return
+    good = {k: v for k, v in results.items() if "ms" in v}
+    best = "fp64"
+    if "ozaki" in good:
+        best = "ozaki"
+    r = good[best]
+    steps_per_s = world * r["steps"] / (r["ms"] * 1e-3)
+    sz = r["sizes"]
+    syn_fl, ana_fl = legendre_flops(sz, sz["N"])
+    sht_flops = (syn_fl + ana_fl + fft_flops(sz, sz["N"]))
+    evals_per_step = (r["steps"] + r["correctors"]) / r["steps"]
+    ph = r["phases_ms"]
+    sht_ms = ph["synthesis"] + ph["fft_products"] + ph["analysis"]
+    line = {
+        "metric": METRIC, "value": steps_per_s, "unit": "timesteps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / r["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded l^-2 state)",
+        "config": {"workload": r["desc"], "precision": best, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "per-step working set ~1.9 GB >> 126 MB L2 (no flush)"},
+        "e2e": {"value": world / r["e2e_s"], "unit": "timesteps/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"]},
+        "gpu_launches": r["launches"],
+        "roofline": {k: r["roofline"][k] for k in ("bound", "achieved", "peak", "unit", "frac")},
+        "roofline_detail": r["roofline"],
+        "sht_tflops": sht_flops / (sht_ms * 1e-3) / 1e12,
+        "evaluations_per_step": evals_per_step,
+        "phases_ms": ph,
+        "energies_after": {k: r["energies"][k] for k in ("KE", "ME")},
+    }
+    line["roofline"]["traffic"] = None
+    if "fp64" in good and best != "fp64":
+        f = good["fp64"]
+        line["fp64_timesteps_per_s"] = world * f["steps"] / (f["ms"] * 1e-3)
+        line["speedup_vs_fp64"] = steps_per_s / line["fp64_timesteps_per_s"]
+    for k, v in results.items():
+        if "error" in v:
+            line.setdefault("errors", {})[k] = v["error"]
+    if r["clocks"]:
+        line["clocks"] = r["clocks"]
+    if world == 1 and not args.no_cpu:
+        cfg, _ = workload(args.workload, "fp64")
+        threads = os.cpu_count() or 1
+        o = cpu_oracle_step(cfg, threads)
+        t0 = time.perf_counter()
+        o.step(1)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "timesteps/s", "cores": threads, "kind": "port",
+                                "sample": "1 full timestep of the same workload (cold buffers)"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="best", choices=["best", "fp64", "ozaki"])
+    ap.add_argument("--workload", default="dynamo128", choices=["dynamo128", "parity32"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup) if args.impl == "ours" else args.warmup
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    run_ours(args, rank, world, local_rank, dist)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

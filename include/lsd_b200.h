@@ -220,10 +220,23 @@ int lsd_banded_solve_device(lsd_ctx* ctx, int n, int kl, int nmat, const double*
                             const int* d_ipiv, int nrhs, const int* d_map, double* d_b);
 
 /* ---- synchronisation and timing ------------------------------------------------------ */
+/* Phase timings (CUDA events on the context stream) of one predictor pass and one
+ * corrector solve from the current state; the state advances by that step.  ms[]:
+ * 0 spectral q,s,t and curls, 1 Legendre synthesis, 2 phi-FFT + products + FFT,
+ * 3 Legendre analysis, 4 spectral tail (curls of N, buoyancy), 5 predictor solves,
+ * 6 corrector solves.  *nphase >= LSD_NPHASE on input, = LSD_NPHASE on output.
+ * Tracing aid; the reference has only its wall-clock get_time (dyn_mpi.F90:80-93). */
+#define LSD_NPHASE 7
+int lsd_profile_phases(lsd_ctx* ctx, double* ms, int* nphase);
+
 int lsd_synchronize(lsd_ctx* ctx);
 /* Device-side elapsed milliseconds of the last lsd_step / transform call, measured with
  * CUDA events on the context stream. */
 int lsd_last_elapsed_ms(const lsd_ctx* ctx, double* ms);
+/* Device self-tests of the tensor-core path (diagnostics).  which = 0: one tcgen05 int8
+ * product D(128x32) = A(128x64) B(32x64)^T checked against the host product;
+ * *result = largest absolute difference (0 expected). */
+int lsd_selftest(lsd_ctx* ctx, int which, double* result);
 /* Number of device kernels this context has launched so far. */
 int lsd_kernel_launches(const lsd_ctx* ctx, long long* count);
 

@@ -27,10 +27,10 @@ void free_ctx(lsd_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->g_pred) cudaGraphExecDestroy(ctx->g_pred);
   if (ctx->g_corr) cudaGraphExecDestroy(ctx->g_corr);
-  void* ptrs[] = {ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_lm2nh,
+  void* ptrs[] = {ctx->d_sblk_l, ctx->d_sblk_nh, ctx->d_aperm, ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_lm2nh,
                   ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,
                   ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y,
-                  ctx->d_ipiv, ctx->d_ipivs, ctx->d_info, ctx->d_gre, ctx->d_invg, ctx->d_state, ctx->d_nl,
+                  ctx->d_ipiv, ctx->d_ipivs, ctx->d_info, ctx->d_gre, ctx->d_gret, ctx->d_invg, ctx->d_state, ctx->d_nl,
                   ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -238,7 +238,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   else if (c.timestep <= 0.0) why = "only a fixed timestep (d_timestep > 0) is supported";
   else if (!c.vel_tstep || !c.cod_tstep || !c.mag_tstep) why = "velocity, codensity and field must all be stepped";
   else if (c.comp_tstep) why = "composition stepping is not supported on the device yet";
-  else if (c.precision != LSD_PREC_FP64 && c.precision != LSD_PREC_OZAKI) why = "unknown precision";
+  else if (c.precision != LSD_PREC_FP64) why = "the tensor-core Legendre path is not available in this build";
   if (!why.empty()) { int rc = lsd_fail(ctx, LSD_EARG, why); free_ctx(ctx); return rc; }
   ctx->Ma = c.M * 3 / 2;
   ctx->H = c.L * c.M - c.Mp * (c.M - 1) * c.M / 2;
@@ -277,6 +277,32 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   TRY(dalloc(ctx, &ctx->d_mlen, NM)); TRY(upload(ctx, ctx->d_mlen, ctx->mlen));
   TRY(dalloc(ctx, &ctx->d_thm, NM)); TRY(upload(ctx, ctx->d_thm, ctx->thm));
   TRY(dalloc(ctx, &ctx->d_lm2nh, lm2nh.size())); TRY(upload(ctx, ctx->d_lm2nh, lm2nh));
+  {  // analysis thread order per folded column: (m-counter, parity)-sorted harmonics
+    std::vector<int> perm((size_t)ctx->Hc * ctx->Hr);
+    for (int col = 0; col < ctx->Hc; ++col) {
+      int base = col * ctx->Hr, len0 = ctx->mlen[2 * col], t = 0;
+      for (int cl = 0; cl < 2; ++cl)
+        for (int par = 0; par < 2; ++par)
+          for (int k = 0; k < ctx->Hr; ++k)
+            if ((k < len0 ? 0 : 1) == cl && ctx->hs[base + k] == par) perm[(size_t)col * ctx->Hr + t++] = k;
+    }
+    TRY(dalloc(ctx, &ctx->d_aperm, perm.size())); TRY(upload(ctx, ctx->d_aperm, perm));
+  }
+  {  // solve blocks: one degree l, up to 16 orders m (all (l, m) share the factors of l)
+    std::vector<int> bl, bnh;
+    for (int l = 0; l < L; ++l) {
+      std::vector<int> nhs;
+      for (int mi = 0; mi < ctx->M; ++mi)
+        if (lm2nh[(size_t)mi * L + l] >= 0) nhs.push_back(lm2nh[(size_t)mi * L + l]);
+      for (size_t i0 = 0; i0 < nhs.size(); i0 += 16) {
+        bl.push_back(l);
+        for (size_t i = i0; i < i0 + 16; ++i) bnh.push_back(i < nhs.size() ? nhs[i] : -1);
+      }
+    }
+    ctx->nsblk = (int)bl.size();
+    TRY(dalloc(ctx, &ctx->d_sblk_l, bl.size())); TRY(upload(ctx, ctx->d_sblk_l, bl));
+    TRY(dalloc(ctx, &ctx->d_sblk_nh, bnh.size())); TRY(upload(ctx, ctx->d_sblk_nh, bnh));
+  }
   // FFT twiddles (long double host trigonometry, rounded once)
   {
     std::vector<double2> tw2(ctx->P2), twh(ctx->Ph);
@@ -306,6 +332,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   TRY(dalloc(ctx, &ctx->d_ipiv, (size_t)OP_NFAM * L * N)); TRY(dalloc(ctx, &ctx->d_ipivs, (size_t)OP_NFAM * L * N));
   TRY(dalloc(ctx, &ctx->d_info, (size_t)OP_NFAM * L));
   TRY(dalloc(ctx, &ctx->d_gre, (size_t)L * 2 * N)); TRY(dalloc(ctx, &ctx->d_invg, (size_t)L * 4));
+  TRY(dalloc(ctx, &ctx->d_gret, (size_t)L * 2 * N));
   const size_t F = (size_t)N * H;
   TRY(dalloc(ctx, &ctx->d_state, LSD_NFIELD * F)); TRY(dalloc(ctx, &ctx->d_nl, LSD_NFIELD * F));
   TRY(dalloc(ctx, &ctx->d_sv, LSD_NFIELD * F));
@@ -703,6 +730,39 @@ int lsd_banded_solve_device(lsd_ctx* ctx, int n, int kl, int nmat, const double*
   return lsd_solve_batch(ctx, n, kl, nmat, d_ab, d_ipiv, nrhs, d_map, d_b);
 }
 
+int lsd_profile_phases(lsd_ctx* ctx, double* ms, int* nphase) {
+  if (!ctx || !ms || !nphase || *nphase < LSD_NPHASE) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  // ev[0] start, ev[1..5] after the five evaluation phases, ev[6] after the predictor,
+  // ev[7], ev[8] around the corrector solve of the second evaluation
+  cudaEvent_t ev[9];
+  for (int i = 0; i < 9; ++i) CUDA_TRY(cudaEventCreate(&ev[i]));
+  CUDA_TRY(cudaEventRecord(ev[0], ctx->stream));
+  int rc = lsd_eval_marked(ctx, ev + 1);
+  if (!rc) rc = lsd_pred(ctx);
+  if (!rc) { cudaEventRecord(ev[6], ctx->stream); rc = lsd_eval(ctx); }
+  if (!rc) { cudaEventRecord(ev[7], ctx->stream); rc = lsd_corr(ctx); }
+  if (!rc) cudaEventRecord(ev[8], ctx->stream);
+  if (!rc) rc = finish_corrector(ctx);
+  if (!rc) {
+    float t = 0.f;
+    for (int i = 0; i < 6; ++i) {
+      cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+      ms[i] = t;
+    }
+    cudaEventElapsedTime(&t, ev[7], ev[8]);
+    ms[6] = t;
+    *nphase = LSD_NPHASE;
+  }
+  for (int i = 0; i < 9; ++i) cudaEventDestroy(ev[i]);
+  ctx->it = 0;
+  ctx->dterr = 0.0;
+  ctx->have_eval = false;
+  ctx->t = ctx->t + ctx->dt;
+  ctx->step = ctx->step + 1;
+  return rc;
+}
+
 int lsd_synchronize(lsd_ctx* ctx) {
   if (!ctx) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
@@ -714,6 +774,13 @@ int lsd_last_elapsed_ms(const lsd_ctx* ctx, double* ms) {
   *ms = ctx->last_ms;
   return LSD_OK;
 }
+int lsd_selftest(lsd_ctx* ctx, int which, double* result) {
+  if (!ctx || !result) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  if (which == 0) return lsd_umma_selftest(ctx, result);
+  return LSD_EARG;
+}
+
 int lsd_kernel_launches(const lsd_ctx* ctx, long long* count) {
   if (!ctx || !count) return LSD_EARG;
   *count = ctx->launches;

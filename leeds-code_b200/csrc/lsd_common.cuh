@@ -74,6 +74,9 @@ struct lsd_ctx {
   // device layout
   int *d_l = nullptr, *d_m = nullptr, *d_s = nullptr, *d_mc = nullptr;
   int *d_mstart = nullptr, *d_mlen = nullptr, *d_thm = nullptr, *d_lm2nh = nullptr;
+  int *d_aperm = nullptr;  // [Hc][Hr] analysis thread order
+  int *d_sblk_l = nullptr, *d_sblk_nh = nullptr;  // solve blocks: degree, [16] harmonics
+  int nsblk = 0;
   // device Legendre tables, each [H][Th2] (== Fortran (Th2, H))
   double *d_leg = nullptr;  // 8 tables contiguous, LSD_LEG_* order
   double *d_gp = nullptr, *d_gw = nullptr, *d_sn = nullptr, *d_sn1 = nullptr;
@@ -88,11 +91,12 @@ struct lsd_ctx {
   double *d_r1dr = nullptr;    // [N][2KL+1]
   double *d_radlap = nullptr;  // [N][2KL+1]
   double *d_intr2dr = nullptr; // [N]
-  // operators: LAPACK band LU [fam][L][N][3KL+1] + ipiv [fam][L][N];
-  // solve layout [fam][N][3KL+1][L] + ipiv [fam][N][L]; Y bands [fam][N][2KL+1][L]
+  // operators: LAPACK band LU [fam][L][N][3KL+1] + ipiv [fam][L][N]; Y bands
+  // [fam][L][N][2KL+1]; (d_lus / d_ipivs: [fam][N][3KL+1][L] copies, l fastest)
   double *d_lu = nullptr, *d_lus = nullptr, *d_y = nullptr;
   int *d_ipiv = nullptr, *d_ipivs = nullptr, *d_info = nullptr;
   double *d_gre = nullptr;   // [L][2][N]
+  double *d_gret = nullptr;  // [N][2][L]
   double *d_invg = nullptr;  // [L][4]
   bool have_ops = false;
   double op_dt = 0.0;
@@ -136,12 +140,15 @@ int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields);
 int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out);
 // ---- spectral algebra and solves (lsd_solve.cu) ----
 int lsd_eval(lsd_ctx* ctx);            // one nonlinear evaluation (device)
+int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks);
 int lsd_pred(lsd_ctx* ctx);            // predictor solves (device)
 int lsd_corr(lsd_ctx* ctx);            // corrector solves + dterr (device)
 int lsd_energy_device(lsd_ctx* ctx, double* out);
 int lsd_factor_batch(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info);
 int lsd_solve_batch(lsd_ctx* ctx, int n, int kl, int nmat, const double* d_ab, const int* d_ipiv,
                     int nrhs, const int* d_map, double* d_b);
+
+int lsd_umma_selftest(lsd_ctx* ctx, double* maxerr);
 
 // small helpers
 static inline int ceil_div(int a, int b) { return (a + b - 1) / b; }

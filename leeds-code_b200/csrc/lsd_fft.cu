@@ -290,6 +290,7 @@ int lsd_launch_c2r(lsd_ctx* ctx, const cplx* four, double* phys, int nfields) {
   if (TJ == 0) return lsd_fail(ctx, LSD_EARG, "FFT row does not fit in shared memory");
   size_t smem = (size_t)2 * TJ * ctx->P2 * sizeof(double2);
   cudaFuncSetAttribute(k_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_c2r, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   dim3 grid(ceil_div(ctx->Th, TJ), ctx->N, nfields);
   k_c2r<<<grid, 256, smem, ctx->stream>>>(pl, ctx->N, four, phys, TJ);
   ctx->launches++;
@@ -304,6 +305,7 @@ int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields) {
   if (TJ == 0) return lsd_fail(ctx, LSD_EARG, "FFT row does not fit in shared memory");
   size_t smem = (size_t)2 * TJ * ctx->P2 * sizeof(double2);
   cudaFuncSetAttribute(k_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_r2c, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   dim3 grid(ceil_div(ctx->Th, TJ), ctx->N, nfields);
   k_r2c<<<grid, 256, smem, ctx->stream>>>(pl, ctx->N, phys, four, TJ);
   ctx->launches++;
@@ -326,6 +328,7 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.sn = ctx->d_sn;
   pc.gp = ctx->d_gp;
   cudaFuncSetAttribute(k_products, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_products, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   dim3 grid(ceil_div(ctx->Th, TJ), ctx->N);
   k_products<<<grid, 512, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out, TJ);
   ctx->launches++;

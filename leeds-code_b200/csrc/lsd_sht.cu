@@ -24,6 +24,7 @@ constexpr int S_NT = 4;   // shells per synthesis CTA
 constexpr int S_KC = 16;  // harmonics per synthesis k-chunk
 constexpr int A_NT = 8;   // shells per analysis CTA
 constexpr int A_JC = 16;  // theta rows per analysis j-chunk
+constexpr int DROW = A_JC * A_NT + 1;  // padded analysis data row (double2)
 
 struct SynthArgs {
   int N, H, Th, Th2, NM, ngroup;
@@ -51,6 +52,63 @@ __device__ __forceinline__ int synth_table(int t) {
   if (KIND == SK_SCALAR) return LSD_LEG_P;
   if (KIND == SK_GRAD3) return t == 0 ? LSD_LEG_P : (t == 1 ? LSD_LEG_P_ : LSD_LEG_SIN1MP);
   return t == 0 ? LSD_LEG_P_ : LSD_LEG_SIN1MP;  // SK_GRAD2
+}
+
+// One harmonic k of the current chunk: accumulate into the even (E) / odd (O) sums of
+// the outputs; S = parity of (l + m) of this harmonic.
+template <int KIND, int S, int NOUT>
+__device__ __forceinline__ void synth_accum(double2 (&acc)[NOUT][2][S_NT], const double* tab,
+                                            const double2* coef, int kk, int j, int Th2) {
+  constexpr int O = 1 - S;
+  if (KIND == SK_VECTOR) {
+    const double P = tab[(0 * S_KC + kk) * Th2 + j];
+    const double A1 = tab[(1 * S_KC + kk) * Th2 + j];
+    const double A2 = tab[(2 * S_KC + kk) * Th2 + j];
+#pragma unroll
+    for (int q = 0; q < S_NT; ++q) {
+      const double2 cq = coef[(0 * S_KC + kk) * S_NT + q];
+      const double2 cs = coef[(1 * S_KC + kk) * S_NT + q];
+      const double2 ct = coef[(2 * S_KC + kk) * S_NT + q];
+      const double2 c2 = cmul_mi(ct);  // (t.Im, -t.Re)
+      const double2 c3 = cmul_i(cs);   // (-s.Im, s.Re)
+      // r: P on parity S ; th: llP_ on 1-S, llsin1mP on S ; ph: llsin1mP on S, llP_ on 1-S
+      acc[0][S][q].x += cq.x * P;  acc[0][S][q].y += cq.y * P;
+      acc[1][O][q].x += cs.x * A1; acc[1][O][q].y += cs.y * A1;
+      acc[1][S][q].x += c2.x * A2; acc[1][S][q].y += c2.y * A2;
+      acc[2][S][q].x += c3.x * A2; acc[2][S][q].y += c3.y * A2;
+      acc[2][O][q].x += ct.x * A1; acc[2][O][q].y += ct.y * A1;
+    }
+  } else if (KIND == SK_SCALAR) {
+    const double P = tab[kk * Th2 + j];
+#pragma unroll
+    for (int q = 0; q < S_NT; ++q) {
+      const double2 cq = coef[kk * S_NT + q];
+      acc[0][S][q].x += cq.x * P; acc[0][S][q].y += cq.y * P;
+    }
+  } else if (KIND == SK_GRAD3) {
+    const double P = tab[(0 * S_KC + kk) * Th2 + j];
+    const double D = tab[(1 * S_KC + kk) * Th2 + j];
+    const double S1 = tab[(2 * S_KC + kk) * Th2 + j];
+#pragma unroll
+    for (int q = 0; q < S_NT; ++q) {
+      const double2 cd = coef[(0 * S_KC + kk) * S_NT + q];
+      const double2 cc = coef[(1 * S_KC + kk) * S_NT + q];
+      const double2 ci = cmul_i(cc);
+      acc[0][S][q].x += cd.x * P;  acc[0][S][q].y += cd.y * P;
+      acc[1][O][q].x += cc.x * D;  acc[1][O][q].y += cc.y * D;
+      acc[2 % NOUT][S][q].x += ci.x * S1; acc[2 % NOUT][S][q].y += ci.y * S1;
+    }
+  } else {  // SK_GRAD2
+    const double D = tab[(0 * S_KC + kk) * Th2 + j];
+    const double S1 = tab[(1 * S_KC + kk) * Th2 + j];
+#pragma unroll
+    for (int q = 0; q < S_NT; ++q) {
+      const double2 cc = coef[kk * S_NT + q];
+      const double2 ci = cmul_i(cc);
+      acc[0][O][q].x += cc.x * D;  acc[0][O][q].y += cc.y * D;
+      acc[1 % NOUT][S][q].x += ci.x * S1; acc[1 % NOUT][S][q].y += ci.y * S1;
+    }
+  }
 }
 
 template <int KIND>
@@ -98,61 +156,12 @@ __global__ void __launch_bounds__(256) k_synth(SynthArgs a) {
     __syncthreads();
     if (j < Th2) {
       for (int kk = 0; kk < kc; ++kk) {
-        const int s = spar[kk];
-        if (KIND == SK_VECTOR) {
-          const double P = tab[(0 * S_KC + kk) * Th2 + j];
-          const double A1 = tab[(1 * S_KC + kk) * Th2 + j];
-          const double A2 = tab[(2 * S_KC + kk) * Th2 + j];
-#pragma unroll
-          for (int q = 0; q < S_NT; ++q) {
-            const double2 cq = coef[(0 * S_KC + kk) * S_NT + q];
-            const double2 cs = coef[(1 * S_KC + kk) * S_NT + q];
-            const double2 ct = coef[(2 * S_KC + kk) * S_NT + q];
-            const double2 c2 = cmul_mi(ct);  // (t.Im, -t.Re)
-            const double2 c3 = cmul_i(cs);   // (-s.Im, s.Re)
-            // r: parity s ; th: llP_ on 1-s, llsin1mP on s ; ph: llsin1mP on s, llP_ on 1-s
-            double2& r_s = acc[0][s][q];
-            r_s.x += cq.x * P; r_s.y += cq.y * P;
-            double2& th_o = acc[1][1 - s][q];
-            th_o.x += cs.x * A1; th_o.y += cs.y * A1;
-            double2& th_s = acc[1][s][q];
-            th_s.x += c2.x * A2; th_s.y += c2.y * A2;
-            double2& ph_s = acc[2][s][q];
-            ph_s.x += c3.x * A2; ph_s.y += c3.y * A2;
-            double2& ph_o = acc[2][1 - s][q];
-            ph_o.x += ct.x * A1; ph_o.y += ct.y * A1;
-          }
-        } else if (KIND == SK_SCALAR) {
-          const double P = tab[kk * Th2 + j];
-#pragma unroll
-          for (int q = 0; q < S_NT; ++q) {
-            const double2 cq = coef[kk * S_NT + q];
-            acc[0][s][q].x += cq.x * P; acc[0][s][q].y += cq.y * P;
-          }
-        } else if (KIND == SK_GRAD3) {
-          const double P = tab[(0 * S_KC + kk) * Th2 + j];
-          const double D = tab[(1 * S_KC + kk) * Th2 + j];
-          const double S1 = tab[(2 * S_KC + kk) * Th2 + j];
-#pragma unroll
-          for (int q = 0; q < S_NT; ++q) {
-            const double2 cd = coef[(0 * S_KC + kk) * S_NT + q];
-            const double2 cc = coef[(1 * S_KC + kk) * S_NT + q];
-            const double2 ci = cmul_i(cc);
-            acc[0][s][q].x += cd.x * P; acc[0][s][q].y += cd.y * P;
-            acc[1][1 - s][q].x += cc.x * D; acc[1][1 - s][q].y += cc.y * D;
-            acc[2][s][q].x += ci.x * S1; acc[2][s][q].y += ci.y * S1;
-          }
-        } else {  // SK_GRAD2
-          const double D = tab[(0 * S_KC + kk) * Th2 + j];
-          const double S1 = tab[(1 * S_KC + kk) * Th2 + j];
-#pragma unroll
-          for (int q = 0; q < S_NT; ++q) {
-            const double2 cc = coef[kk * S_NT + q];
-            const double2 ci = cmul_i(cc);
-            acc[0][1 - s][q].x += cc.x * D; acc[0][1 - s][q].y += cc.y * D;
-            acc[1][s][q].x += ci.x * S1; acc[1][s][q].y += ci.y * S1;
-          }
-        }
+        // parity is uniform across the block for a given k: branch so that every
+        // accumulator index is a compile-time constant (registers, no local memory)
+        if (spar[kk] == 0)
+          synth_accum<KIND, 0>(acc, tab, coef, kk, j, Th2);
+        else
+          synth_accum<KIND, 1>(acc, tab, coef, kk, j, Th2);
       }
     }
   }
@@ -173,6 +182,7 @@ __global__ void __launch_bounds__(256) k_synth(SynthArgs a) {
 
 struct AnalArgs {
   int N, H, Th, Th2, NM, Hr, ngroup;
+  const int* perm;     // [Hc][Hr]: thread -> harmonic of the column, sorted by (m-counter, parity)
   const int* mstart;   // per m-counter
   const int* mlen;
   const int* hs;
@@ -194,9 +204,11 @@ __global__ void __launch_bounds__(288) k_anal(AnalArgs a) {
   const int len0 = a.mlen[c0];
   const int kbeg = a.mstart[c0];     // the column's harmonics are contiguous
   double* tab = smem;                                         // [NTAB][A_JC][Hr]
-  double2* dat = (double2*)(smem + NTAB * A_JC * Hr);         // [2 cnt][NF][2 par][A_JC][A_NT]
-  const int k = threadIdx.x;
-  const bool active = k < Hr;
+  double2* dat = (double2*)(smem + NTAB * A_JC * Hr);         // [2 cnt][NF][2 par][A_JC*A_NT + 1]
+  // threads are ordered by (m-counter, parity) so that a warp reads one data row (a smem
+  // broadcast); rows are padded by one element so that neighbouring rows use other banks
+  const bool active = threadIdx.x < Hr;
+  const int k = active ? a.perm[(size_t)col * Hr + threadIdx.x] : 0;
   const int cl = (k < len0) ? 0 : 1;
   const int s = active ? a.hs[kbeg + k] : 0;
   double2 acc[NF][A_NT];
@@ -225,8 +237,8 @@ __global__ void __launch_bounds__(288) k_anal(AnalArgs a) {
         o = make_double2(x.x - y.x, x.y - y.y);
         if ((Th & 1) && j == Th2 - 1) { e.x *= 0.5; e.y *= 0.5; }
       }
-      dat[(((cc * NF + f) * 2 + 0) * A_JC + jj) * A_NT + q] = e;
-      dat[(((cc * NF + f) * 2 + 1) * A_JC + jj) * A_NT + q] = o;
+      dat[((cc * NF + f) * 2 + 0) * DROW + jj * A_NT + q] = e;
+      dat[((cc * NF + f) * 2 + 1) * DROW + jj * A_NT + q] = o;
     }
     __syncthreads();
     if (active) {
@@ -235,11 +247,11 @@ __global__ void __launch_bounds__(288) k_anal(AnalArgs a) {
           const double gP = tab[(0 * A_JC + jj) * Hr + k];
           const double A1 = tab[(1 * A_JC + jj) * Hr + k];
           const double A2 = tab[(2 * A_JC + jj) * Hr + k];
-          const double2* Yr_s = dat + (((cl * NF + 0) * 2 + s) * A_JC + jj) * A_NT;
-          const double2* Yt_s = dat + (((cl * NF + 1) * 2 + s) * A_JC + jj) * A_NT;
-          const double2* Yt_o = dat + (((cl * NF + 1) * 2 + (1 - s)) * A_JC + jj) * A_NT;
-          const double2* Yp_s = dat + (((cl * NF + 2) * 2 + s) * A_JC + jj) * A_NT;
-          const double2* Yp_o = dat + (((cl * NF + 2) * 2 + (1 - s)) * A_JC + jj) * A_NT;
+          const double2* Yr_s = dat + ((cl * NF + 0) * 2 + s) * DROW + jj * A_NT;
+          const double2* Yt_s = dat + ((cl * NF + 1) * 2 + s) * DROW + jj * A_NT;
+          const double2* Yt_o = dat + ((cl * NF + 1) * 2 + (1 - s)) * DROW + jj * A_NT;
+          const double2* Yp_s = dat + ((cl * NF + 2) * 2 + s) * DROW + jj * A_NT;
+          const double2* Yp_o = dat + ((cl * NF + 2) * 2 + (1 - s)) * DROW + jj * A_NT;
 #pragma unroll
           for (int q = 0; q < A_NT; ++q) {
             const double2 yr = Yr_s[q], yts = Yt_s[q], yto = Yt_o[q], yps = Yp_s[q], ypo = Yp_o[q];
@@ -252,7 +264,7 @@ __global__ void __launch_bounds__(288) k_anal(AnalArgs a) {
           }
         } else {
           const double gP = tab[jj * Hr + k];
-          const double2* Y = dat + (((cl * NF + 0) * 2 + s) * A_JC + jj) * A_NT;
+          const double2* Y = dat + ((cl * NF + 0) * 2 + s) * DROW + jj * A_NT;
 #pragma unroll
           for (int q = 0; q < A_NT; ++q) {
             acc[0][q].x += Y[q].x * gP;
@@ -294,6 +306,7 @@ int launch_synth_kind(lsd_ctx* ctx, const SynthGroup* groups, int ngroups) {
   constexpr int NIN = SK<KIND>::nin, NTAB = SK<KIND>::ntab;
   size_t smem = sizeof(double) * NTAB * S_KC * ctx->Th2 + sizeof(double2) * NIN * S_KC * S_NT;
   cudaFuncSetAttribute(k_synth<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_synth<KIND>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   int threads = ((ctx->Th2 + 31) / 32) * 32;
   dim3 grid(ctx->NM, ceil_div(ctx->N, S_NT), ng);
   k_synth<KIND><<<grid, threads, smem, ctx->stream>>>(a);
@@ -314,8 +327,10 @@ int launch_anal_kind(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
   if (ng == 0) return LSD_OK;
   a.ngroup = ng;
   constexpr int NF = (KIND == AK_VECTOR) ? 3 : 1;
-  size_t smem = sizeof(double) * NF * A_JC * ctx->Hr + sizeof(double2) * 2 * NF * 2 * A_JC * A_NT;
+  size_t smem = sizeof(double) * NF * A_JC * ctx->Hr + sizeof(double2) * 2 * NF * 2 * DROW;
+  a.perm = ctx->d_aperm;
   cudaFuncSetAttribute(k_anal<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_anal<KIND>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   int threads = ((ctx->Hr + 31) / 32) * 32;
   if (threads > 1024) return lsd_fail(ctx, LSD_EARG, "analysis: folded column longer than 1024 harmonics");
   dim3 grid(ctx->Hc, ceil_div(ctx->N, A_NT), ng);

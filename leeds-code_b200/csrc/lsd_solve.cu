@@ -152,99 +152,75 @@ __global__ void k_tail(TailArgs a) {
 // Column solves.  One thread per harmonic nh; the column x(n) = X[(n-1)*H + nh].
 // LU factors in solve layout [N][3KL+1][L], pivots [N][L]; Y bands [N][2KL+1][L].
 // ---------------------------------------------------------------------------------------
-struct OpView {
-  const double* lu;   // [N][3KL+1][L]
-  const int* ipiv;    // [N][L]
-  const double* y;    // [N][2KL+1][L]
-};
+// ---- real column kernels ------------------------------------------------------------
+// A thread owns one real column (the Re or the Im part of one harmonic): the reference
+// solves them with separate dgbtrs calls (timestep.F90:580-585) with the same factors.
+// A block handles one degree l (up to SBM orders m), so the factors of l are staged once
+// in shared memory and read as broadcasts; columns are x(n) = col[n * CW].
 
-__device__ __forceinline__ double luat(const OpView& o, int KL, int L, int row, int col, int l) {
-  return o.lu[((size_t)(col - 1) * (3 * KL + 1) + (row - 1)) * L + l];
-}
-
-// dgbtrs on a complex column (Re and Im solved with the same real factors)
-__device__ void col_lu_solve(const OpView& o, int KL, int L, int N, int l, cplx* x, size_t st) {
-  const int kd = 2 * KL + 1;
-  for (int j = 1; j <= N - 1; ++j) {
-    int lm = min(KL, N - j);
-    int p = o.ipiv[(size_t)(j - 1) * L + l];
-    double2 xj = x[(size_t)(j - 1) * st];
-    if (p != j) {
-      double2 xp = x[(size_t)(p - 1) * st];
-      x[(size_t)(p - 1) * st] = xj;
-      xj = xp;
-      x[(size_t)(j - 1) * st] = xj;
-    }
-    double2 temp = make_double2(-xj.x, -xj.y);
-    for (int i = 1; i <= lm; ++i) {
-      double a = luat(o, KL, L, kd + i, j, l);
-      double2 v = x[(size_t)(j + i - 1) * st];
-      v.x = v.x + a * temp.x;
-      v.y = v.y + a * temp.y;
-      x[(size_t)(j + i - 1) * st] = v;
-    }
+// dgbtrs: forward sweep with row interchanges and the unit-lower band, backward dtbsv
+// with the upper band of width 2KL (LAPACK loop order).  ab: LAPACK band (3KL+1, N).
+template <int KL, int CW>
+__device__ void rcol_lu_solve(const double* ab, const int* piv, const double* rdiag, int N, double* x) {
+  constexpr int LD = 3 * KL + 1, KD = 2 * KL + 1, K2 = 2 * KL;
+#define LU(row, col) ab[(col) * LD + ((row) - 1)]  /* 1-based band row, 0-based column */
+  for (int c = 0; c < N - 1; ++c) {
+    const int p = piv[c] - 1;
+    double xc = x[p * CW];
+    if (p != c) { x[p * CW] = x[c * CW]; x[c * CW] = xc; }
+    const double temp = -xc;
+    const int lm = min(KL, N - 1 - c);
+#pragma unroll
+    for (int i = 1; i <= KL; ++i)
+      if (i <= lm) x[(c + i) * CW] = x[(c + i) * CW] + LU(KD + i, c) * temp;
   }
-  const int k = 2 * KL, kplus1 = k + 1;
-  for (int j = N; j >= 1; --j) {
-    double2 xj = x[(size_t)(j - 1) * st];
-    double d = luat(o, KL, L, kplus1, j, l);
-    xj.x = xj.x / d;
-    xj.y = xj.y / d;
-    x[(size_t)(j - 1) * st] = xj;
-    int lo = kplus1 - j;
-    for (int i = j - 1; i >= max(1, j - k); --i) {
-      double a = luat(o, KL, L, lo + i, j, l);
-      double2 v = x[(size_t)(i - 1) * st];
-      v.x = v.x - xj.x * a;
-      v.y = v.y - xj.y * a;
-      x[(size_t)(i - 1) * st] = v;
-    }
+  for (int c = N - 1; c >= 0; --c) {
+    const double xc = x[c * CW] * rdiag[c];  // dtbsv divides; the reciprocal is taken once per block
+    x[c * CW] = xc;
+#pragma unroll
+    for (int t = 1; t <= K2; ++t)
+      if (c - t >= 0) x[(c - t) * CW] = x[(c - t) * CW] - xc * LU(K2 + 1 - t, c);
   }
+#undef LU
 }
 
-// d = Y b + c  (tim_multY, timestep.F90:640-670), written to d (may alias c, not b)
-__device__ void col_multY(const OpView& o, int KL, int L, int N, int l, const cplx* b, const cplx* c, cplx* d, size_t st) {
-  const int ldm = 2 * KL + 1;
-  for (int n = 1; n <= N; ++n) {
-    double2 acc = c[(size_t)(n - 1) * st];
-    for (int j = max(1, n - KL); j <= min(n + KL, N); ++j) {
-      double a = o.y[((size_t)(j - 1) * ldm + (KL + n - j)) * L + l];
-      double2 bv = b[(size_t)(j - 1) * st];
-      acc.x = acc.x + a * bv.x;
-      acc.y = acc.y + a * bv.y;
-    }
-    d[(size_t)(n - 1) * st] = acc;
-  }
-}
-
-__device__ __forceinline__ void col_zero_ends(cplx* x, size_t st, int N) {
-  x[0] = make_double2(0.0, 0.0);
-  x[(size_t)(N - 1) * st] = make_double2(0.0, 0.0);
-}
-
-// vel_gre_adjust (velocity.F90:445-465)
-__device__ void col_gre_adjust(const double* gre, const double* invg, int N, int l, cplx* x, size_t st) {
-  const double* g1 = gre + (size_t)l * 2 * N;
-  const double* g2 = g1 + N;
-  const double* iG = invg + (size_t)l * 4;
-  double2 bi = x[0], bo = x[(size_t)(N - 1) * st];
-  double ar = iG[0] * bi.x + iG[2] * bo.x, br = iG[1] * bi.x + iG[3] * bo.x;
-  double ai = iG[0] * bi.y + iG[2] * bo.y, bim = iG[1] * bi.y + iG[3] * bo.y;
+// d(n) = c(n) + sum_j Y(KL+1+n-j, j) b(j), j ascending (tim_multY); Y band (2KL+1, N) in
+// shared memory, b in global memory with element stride bst, c and d in shared memory.
+template <int KL, int CW>
+__device__ void rcol_multY(const double* y, int N, const double* __restrict__ b, size_t bst,
+                           const double* c, double* d) {
+  constexpr int LDM = 2 * KL + 1;
+#pragma unroll 4
   for (int n = 0; n < N; ++n) {
-    double2 v = x[(size_t)n * st];
-    v.x = v.x - ar * g1[n] - br * g2[n];
-    v.y = v.y - ai * g1[n] - bim * g2[n];
-    x[(size_t)n * st] = v;
+    double acc = c[n * CW];
+#pragma unroll
+    for (int t = 0; t < LDM; ++t) {
+      const int j = n - KL + t;
+      if (j >= 0 && j < N) acc = acc + y[j * LDM + (LDM - 1 - t)] * __ldg(b + (size_t)j * bst);
+    }
+    d[n * CW] = acc;
   }
+}
+
+// vel_gre_adjust (velocity.F90:445-465); g: Green's functions (N, 2), iG: invG (2, 2)
+template <int CW>
+__device__ void rcol_gre_adjust(const double* g, const double* iG, int N, double* x) {
+  const double bi = x[0], bo = x[(N - 1) * CW];
+  const double a = iG[0] * bi + iG[2] * bo, b = iG[1] * bi + iG[3] * bo;
+  for (int n = 0; n < N; ++n) x[n * CW] = x[n * CW] - a * g[n] - b * g[N + n];
 }
 
 struct StepArgs {
-  int N, H, KL, L;
+  int N, H, KL, L, nblk;
   const int* hl;
   const int* hm;
-  OpView op[OP_NFAM];
-  const double* gre;
-  const double* invg;
+  const int* blk_l;    // [nblk] degree of each solve block
+  const int* blk_nh;   // [nblk][SBM] harmonics of the block (-1 = none)
+  const double* lu;    // [fam][L][N][3KL+1] LAPACK factors
+  const int* ipiv;     // [fam][L][N]
+  const double* y;     // [fam][L][N][2KL+1]
+  const double* gre;   // [L][2][N]
+  const double* invg;  // [L][4]
   cplx* state;  // [field][N][H]
   cplx* nl;
   cplx* sv;
@@ -256,63 +232,189 @@ struct StepArgs {
   double* red;  // corrector: [8] sums of squares
 };
 
+// Batched column I/O between global memory (element stride gst) and a shared column
+// (stride CW): IOB loads are issued before any store so that they overlap.
+constexpr int IOB = 8;
+template <int CW>
+__device__ __forceinline__ void col_load_save(const double* __restrict__ src, double* __restrict__ save, size_t gst,
+                                              double* col, int N) {
+  for (int n0 = 0; n0 < N; n0 += IOB) {
+    double v[IOB];
+#pragma unroll
+    for (int u = 0; u < IOB; ++u) v[u] = (n0 + u < N) ? src[(size_t)(n0 + u) * gst] : 0.0;
+#pragma unroll
+    for (int u = 0; u < IOB; ++u)
+      if (n0 + u < N) { col[(n0 + u) * CW] = v[u]; save[(size_t)(n0 + u) * gst] = v[u]; }
+  }
+}
+// col = c (src - save) ; save = src
+template <int CW>
+__device__ __forceinline__ void col_load_diff(const double* __restrict__ src, double* __restrict__ save, size_t gst,
+                                              double c, double* col, int N) {
+  for (int n0 = 0; n0 < N; n0 += IOB) {
+    double v[IOB], p[IOB];
+#pragma unroll
+    for (int u = 0; u < IOB; ++u) {
+      v[u] = (n0 + u < N) ? src[(size_t)(n0 + u) * gst] : 0.0;
+      p[u] = (n0 + u < N) ? save[(size_t)(n0 + u) * gst] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < IOB; ++u)
+      if (n0 + u < N) { col[(n0 + u) * CW] = c * (v[u] - p[u]); save[(size_t)(n0 + u) * gst] = v[u]; }
+  }
+}
+template <int CW>
+__device__ __forceinline__ void col_store(double* __restrict__ dst, size_t gst, const double* col, int N) {
+  for (int n0 = 0; n0 < N; n0 += IOB) {
+    double v[IOB];
+#pragma unroll
+    for (int u = 0; u < IOB; ++u) v[u] = (n0 + u < N) ? col[(n0 + u) * CW] : 0.0;
+#pragma unroll
+    for (int u = 0; u < IOB; ++u)
+      if (n0 + u < N) dst[(size_t)(n0 + u) * gst] = v[u];
+  }
+}
+// x += col, returning sum of col^2 (tim_addcorr order within the column)
+template <int CW>
+__device__ __forceinline__ double col_addcorr(double* __restrict__ x, size_t gst, const double* col, int N) {
+  double ss = 0.0;
+  for (int n0 = 0; n0 < N; n0 += IOB) {
+    double v[IOB], d[IOB];
+#pragma unroll
+    for (int u = 0; u < IOB; ++u) {
+      v[u] = (n0 + u < N) ? x[(size_t)(n0 + u) * gst] : 0.0;
+      d[u] = (n0 + u < N) ? col[(n0 + u) * CW] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < IOB; ++u)
+      if (n0 + u < N) {
+        ss = ss + d[u] * d[u];
+        x[(size_t)(n0 + u) * gst] = v[u] + d[u];
+      }
+  }
+  return ss;
+}
+
 // which solve this CTA row performs
 enum SolveJob { J_VTOR = 0, J_VPOL, J_COD, J_MTOR, J_MPOL, J_COMP, J_NJOB };
 
-// Predictor (velocity.F90:369-395, codensity.F90:224-234, magnetic.F90:370-408)
-__global__ void k_predictor(StepArgs a) {
-  int nh = blockIdx.x * blockDim.x + threadIdx.x;
-  int job = blockIdx.y;
-  if (nh >= a.H) return;
-  if (job == J_COMP && !a.comp) return;
-  const size_t F = (size_t)a.N * a.H, st = a.H;
-  const int l = a.hl[nh], N = a.N, KL = a.KL, L = a.L;
-  int fld = 0;
-  switch (job) {
-    case J_VTOR: fld = LSD_VEL_TOR; break;
-    case J_VPOL: fld = LSD_VEL_POL; break;
-    case J_COD: fld = LSD_COD_C; break;
-    case J_MTOR: fld = LSD_MAG_TOR; break;
-    case J_MPOL: fld = LSD_MAG_POL; break;
-    case J_COMP: fld = LSD_COMP_C; break;
+constexpr int SBM = 16;        // orders m per solve block
+constexpr int SCW = 2 * SBM;   // real columns per block (Re, Im)
+
+__device__ __forceinline__ int job_field(int job) {
+  return job == J_VTOR ? LSD_VEL_TOR : job == J_VPOL ? LSD_VEL_POL : job == J_COD ? LSD_COD_C
+       : job == J_MTOR ? LSD_MAG_TOR : job == J_MPOL ? LSD_MAG_POL : LSD_COMP_C;
+}
+__device__ __forceinline__ int job_family(int job) {
+  return job == J_VTOR ? OP_VTOR : job == J_VPOL ? OP_VPOL : job == J_COD ? OP_COD : job == J_COMP ? OP_COMP
+       : job == J_MTOR ? OP_MTOR : OP_MPOL;
+}
+
+// shared-memory plan of a solve block: columns [N][SCW], then the factors of degree l
+struct SolveSmem {
+  double* col;
+  double* lu1; int* piv1;   // main operator (XTor / XPol / XC / ...)
+  double* lu2; int* piv2;   // Green's operator (vel Pol only)
+  double* y;                // Y band of the main family
+  double* g;                // Green's functions (N, 2) + invG (4)
+  double* rd1; double* rd2;  // reciprocals of the U diagonals
+};
+
+template <int KL>
+__device__ SolveSmem solve_smem(double* base, int N) {
+  SolveSmem m;
+  const int LD = 3 * KL + 1, LDM = 2 * KL + 1;
+  m.col = base;
+  m.lu1 = m.col + (size_t)N * SCW;
+  m.lu2 = m.lu1 + (size_t)N * LD;
+  m.y = m.lu2 + (size_t)N * LD;
+  m.g = m.y + (size_t)N * LDM;
+  m.rd1 = m.g + 2 * N + 4;
+  m.rd2 = m.rd1 + N;
+  m.piv1 = (int*)(m.rd2 + N);
+  m.piv2 = m.piv1 + N;
+  return m;
+}
+
+// stage the factors of degree l for this job into shared memory (whole block)
+template <int KL>
+__device__ void stage_factors(const StepArgs& a, const SolveSmem& m, int job, int l, bool with_y) {
+  const int N = a.N, L = a.L, LD = 3 * KL + 1, LDM = 2 * KL + 1;
+  const int fam = job_family(job);
+  const double* lu = a.lu + ((size_t)fam * L + l) * N * LD;
+  for (int i = threadIdx.x; i < N * LD; i += blockDim.x) m.lu1[i] = lu[i];
+  const int* pv = a.ipiv + ((size_t)fam * L + l) * N;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) m.piv1[i] = pv[i];
+  if (with_y) {
+    const double* y = a.y + ((size_t)fam * L + l) * N * LDM;
+    for (int i = threadIdx.x; i < N * LDM; i += blockDim.x) m.y[i] = y[i];
   }
-  cplx* X = a.state + fld * F + nh;
-  const cplx* Nn = a.nl + fld * F + nh;
-  cplx* S = a.sv + fld * F + nh;
-  cplx* W = a.work + (size_t)job * F + nh;
-  for (int n = 0; n < N; ++n) S[(size_t)n * st] = Nn[(size_t)n * st];  // save N
+  for (int i = threadIdx.x; i < N; i += blockDim.x) m.rd1[i] = 1.0 / lu[(size_t)i * LD + 2 * KL];
+  if (job == J_VPOL) {
+    const double* lu2 = a.lu + ((size_t)OP_VGRE * L + l) * N * LD;
+    for (int i = threadIdx.x; i < N * LD; i += blockDim.x) m.lu2[i] = lu2[i];
+    for (int i = threadIdx.x; i < N; i += blockDim.x) m.rd2[i] = 1.0 / lu2[(size_t)i * LD + 2 * KL];
+    const int* pv2 = a.ipiv + ((size_t)OP_VGRE * L + l) * N;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) m.piv2[i] = pv2[i];
+    const double* g = a.gre + (size_t)l * 2 * N;
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) m.g[i] = g[i];
+    if (threadIdx.x < 4) m.g[2 * N + threadIdx.x] = a.invg[(size_t)l * 4 + threadIdx.x];
+  }
+}
+
+// Predictor (velocity.F90:369-395, codensity.F90:224-234, magnetic.F90:370-408).
+template <int KL>
+__global__ void __launch_bounds__(SCW) k_predictor(StepArgs a) {
+  extern __shared__ double smem_raw[];
+  const int job = blockIdx.y;
+  if (job == J_COMP && !a.comp) return;
+  const int b = blockIdx.x;
+  const int l = a.blk_l[b];
+  const bool zero = (job == J_COD || job == J_COMP);
+  if (l == 0 && !zero) {
+    // l = 0 of velocity / field: the predictor leaves N (zero) with zeroed boundary rows
+  }
+  const SolveSmem m = solve_smem<KL>(smem_raw, a.N);
+  stage_factors<KL>(a, m, job, l, true);
+  __syncthreads();
+  const int t = threadIdx.x;
+  const int nh = a.blk_nh[b * SBM + t / 2], part = t & 1;
+  if (nh < 0) return;
+  const size_t F = (size_t)a.N * a.H;
+  const int N = a.N;
+  const int fld = job_field(job);
+  const size_t off = 2 * (size_t)nh + part, rst = 2 * (size_t)a.H;
+  double* X = (double*)(a.state + fld * F) + off;
+  const double* Nn = (const double*)(a.nl + fld * F) + off;
+  double* S = (double*)(a.sv + fld * F) + off;
+  double* W = m.col + t;
+  col_load_save<SCW>(Nn, S, rst, W, N);  // W = N ; save N
   if (job == J_VPOL) {
     // Pol := NPol ; zerobc ; invX(XGre) ; Pol := YPol vel_Pol + Pol ; zerobc ; invX(XPol) ; adjust
-    for (int n = 0; n < N; ++n) W[(size_t)n * st] = Nn[(size_t)n * st];
-    col_zero_ends(W, st, N);
+    W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
     if (l != 0) {
-      col_lu_solve(a.op[OP_VGRE], KL, L, N, l, W, st);
-      col_multY(a.op[OP_VPOL], KL, L, N, l, X, W, W, st);
+      rcol_lu_solve<KL, SCW>(m.lu2, m.piv2, m.rd2, N, W);
+      rcol_multY<KL, SCW>(m.y, N, X, rst, W, W);
     }
-    col_zero_ends(W, st, N);
+    W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
     if (l != 0) {
-      col_lu_solve(a.op[OP_VPOL], KL, L, N, l, W, st);
-      col_gre_adjust(a.gre, a.invg, N, l, W, st);
+      rcol_lu_solve<KL, SCW>(m.lu1, m.piv1, m.rd1, N, W);
+      rcol_gre_adjust<SCW>(m.g, m.g + 2 * N, N, W);
     }
-    for (int n = 0; n < N; ++n) X[(size_t)n * st] = W[(size_t)n * st];
-    return;
+  } else {
+    if (l != 0 || zero) rcol_multY<KL, SCW>(m.y, N, X, rst, W, W);
+    W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
+    if (zero && nh == 0 && part == 0) {  // cod_setbc / comp_setbc (codensity.F90:126-184)
+      int bc = job == J_COD ? a.cod_bc : a.comp_bc;
+      double qi = job == J_COD ? a.qi : a.qi_comp, qo = job == J_COD ? a.qo : a.qo_comp;
+      if (bc == 1 || bc == 2) W[0] = 1.0;
+      else if (bc == 3 || bc == 4) W[0] = qi;
+      W[(N - 1) * SCW] = (bc == 2 || bc == 4) ? qo : 0.0;
+    }
+    // vel_setbc_Tor: the l=1, m=0 inner value rot_omega*r_i is 0 (no inner-core rotation)
+    if (l != 0 || zero) rcol_lu_solve<KL, SCW>(m.lu1, m.piv1, m.rd1, N, W);
   }
-  const bool zero = (job == J_COD || job == J_COMP);
-  const int fam = job == J_VTOR ? OP_VTOR : job == J_COD ? OP_COD : job == J_COMP ? OP_COMP
-                : job == J_MTOR ? OP_MTOR : OP_MPOL;
-  if (l != 0 || zero) col_multY(a.op[fam], KL, L, N, l, X, Nn, W, st);
-  else for (int n = 0; n < N; ++n) W[(size_t)n * st] = Nn[(size_t)n * st];
-  col_zero_ends(W, st, N);
-  if (zero && nh == 0) {  // cod_setbc / comp_setbc (codensity.F90:126-184)
-    int bc = job == J_COD ? a.cod_bc : a.comp_bc;
-    double qi = job == J_COD ? a.qi : a.qi_comp, qo = job == J_COD ? a.qo : a.qo_comp;
-    if (bc == 1 || bc == 2) W[0].x = 1.0;
-    else if (bc == 3 || bc == 4) W[0].x = qi;
-    W[(size_t)(N - 1) * st].x = (bc == 2 || bc == 4) ? qo : 0.0;
-  }
-  // vel_setbc_Tor: l=1, m=0 inner value rot_omega*r_i with rot_omega = 0 -> 0
-  if (l != 0 || zero) col_lu_solve(a.op[fam], KL, L, N, l, W, st);
-  for (int n = 0; n < N; ++n) X[(size_t)n * st] = W[(size_t)n * st];
+  col_store<SCW>(X, rst, W, N);
 }
 
 __device__ __forceinline__ void warp_block_add(double v, double* target) {
@@ -322,53 +424,46 @@ __device__ __forceinline__ void warp_block_add(double v, double* target) {
 
 // Corrector (velocity.F90:413-439, codensity.F90:240-259, magnetic.F90:414-461)
 // red[] slots: 0 vTor, 1 vPol, 2 cod, 3 comp, 4 bTor, 5 bicTor, 6 bPol, 7 bicPol
-__global__ void k_corrector(StepArgs a) {
-  int nh = blockIdx.x * blockDim.x + threadIdx.x;
-  int job = blockIdx.y;
-  bool live = nh < a.H && !(job == J_COMP && !a.comp);
+template <int KL>
+__global__ void __launch_bounds__(SCW) k_corrector(StepArgs a) {
+  extern __shared__ double smem_raw[];
+  const int job = blockIdx.y;
+  if (job == J_COMP && !a.comp) return;
+  const int b = blockIdx.x;
+  const int l = a.blk_l[b];
+  const SolveSmem m = solve_smem<KL>(smem_raw, a.N);
+  stage_factors<KL>(a, m, job, l, false);
+  __syncthreads();
+  const int t = threadIdx.x;
+  const int nh = a.blk_nh[b * SBM + t / 2], part = t & 1;
   double ss = 0.0, ssic = 0.0;
-  if (live) {
-    const size_t F = (size_t)a.N * a.H, st = a.H;
-    const int l = a.hl[nh], N = a.N, KL = a.KL, L = a.L;
-    int fld = job == J_VTOR ? LSD_VEL_TOR : job == J_VPOL ? LSD_VEL_POL : job == J_COD ? LSD_COD_C
-            : job == J_MTOR ? LSD_MAG_TOR : job == J_MPOL ? LSD_MAG_POL : LSD_COMP_C;
-    cplx* X = a.state + fld * F + nh;
-    const cplx* Nn = a.nl + fld * F + nh;
-    cplx* S = a.sv + fld * F + nh;
-    cplx* W = a.work + (size_t)job * F + nh;
+  if (nh >= 0) {
+    const size_t F = (size_t)a.N * a.H;
+    const int N = a.N;
+    const int fld = job_field(job);
+    const size_t off = 2 * (size_t)nh + part, rst = 2 * (size_t)a.H;
+    double* X = (double*)(a.state + fld * F) + off;
+    const double* Nn = (const double*)(a.nl + fld * F) + off;
+    double* S = (double*)(a.sv + fld * F) + off;
+    double* W = m.col + t;
     const double c = a.implicit;
-    for (int n = 0; n < N; ++n) {  // nc = c (N - N_saved) ; N_saved = N
-      double2 v = Nn[(size_t)n * st], p = S[(size_t)n * st];
-      W[(size_t)n * st] = make_double2(c * (v.x - p.x), c * (v.y - p.y));
-      S[(size_t)n * st] = v;
-    }
-    double2 x0 = X[0];
-    col_zero_ends(W, st, N);
-    if (job == J_VTOR && l == 1 && a.hm[nh] == 0) W[0].x = 0.0 - x0.x;  // vel_setbc_Tor, tim_it /= 0
+    col_load_diff<SCW>(Nn, S, rst, c, W, N);  // nc = c (N - N_saved) ; N_saved = N
+    W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
+    if (job == J_VTOR && l == 1 && a.hm[nh] == 0 && part == 0) W[0] = 0.0 - X[0];  // vel_setbc_Tor, tim_it /= 0
     if (job == J_VPOL) {
-      if (l != 0) col_lu_solve(a.op[OP_VGRE], KL, L, N, l, W, st);
-      col_zero_ends(W, st, N);
+      if (l != 0) rcol_lu_solve<KL, SCW>(m.lu2, m.piv2, m.rd2, N, W);
+      W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
       if (l != 0) {
-        col_lu_solve(a.op[OP_VPOL], KL, L, N, l, W, st);
-        col_gre_adjust(a.gre, a.invg, N, l, W, st);
+        rcol_lu_solve<KL, SCW>(m.lu1, m.piv1, m.rd1, N, W);
+        rcol_gre_adjust<SCW>(m.g, m.g + 2 * N, N, W);
       }
     } else {
       const bool zero = (job == J_COD || job == J_COMP);
-      const int fam = job == J_VTOR ? OP_VTOR : job == J_COD ? OP_COD : job == J_COMP ? OP_COMP
-                    : job == J_MTOR ? OP_MTOR : OP_MPOL;
-      if (l != 0 || zero) col_lu_solve(a.op[fam], KL, L, N, l, W, st);
+      if (l != 0 || zero) rcol_lu_solve<KL, SCW>(m.lu1, m.piv1, m.rd1, N, W);
     }
-    for (int n = 0; n < N; ++n) {  // tim_addcorr
-      double2 d = W[(size_t)n * st];
-      ss = ss + d.x * d.x;
-      ss = ss + d.y * d.y;
-      double2 v = X[(size_t)n * st];
-      X[(size_t)n * st] = make_double2(v.x + d.x, v.y + d.y);
-    }
-    if ((job == J_MTOR || job == J_MPOL) && l != 0) {  // inner-core copy (Ni = 1)
-      double2 d = W[0];
-      ssic = d.x * d.x + d.y * d.y;
-    }
+    const double x0 = W[0];
+    ss = col_addcorr<SCW>(X, rst, W, N);  // tim_addcorr
+    if ((job == J_MTOR || job == J_MPOL) && l != 0) ssic = x0 * x0;  // inner-core copy (Ni = 1)
   }
   int slot = job == J_VTOR ? 0 : job == J_VPOL ? 1 : job == J_COD ? 2 : job == J_COMP ? 3 : job == J_MTOR ? 4 : 6;
   warp_block_add(ss, a.red + slot);
@@ -450,19 +545,13 @@ SpecArgs spec_args(lsd_ctx* ctx) {
 
 StepArgs step_args(lsd_ctx* ctx) {
   StepArgs a;
-  a.N = ctx->N; a.H = ctx->H; a.KL = ctx->KL; a.L = ctx->L;
+  a.N = ctx->N; a.H = ctx->H; a.KL = ctx->KL; a.L = ctx->L; a.nblk = ctx->nsblk;
   a.hl = ctx->d_l; a.hm = ctx->d_m;
-  const size_t lus = (size_t)ctx->N * (3 * ctx->KL + 1) * ctx->L;
-  const size_t ys = (size_t)ctx->N * (2 * ctx->KL + 1) * ctx->L;
-  const size_t ps = (size_t)ctx->N * ctx->L;
-  for (int f = 0; f < OP_NFAM; ++f) {
-    a.op[f].lu = ctx->d_lus + f * lus;
-    a.op[f].ipiv = ctx->d_ipivs + f * ps;
-    a.op[f].y = ctx->d_y + f * ys;
-  }
+  a.blk_l = ctx->d_sblk_l; a.blk_nh = ctx->d_sblk_nh;
+  a.lu = ctx->d_lu; a.ipiv = ctx->d_ipiv; a.y = ctx->d_y;
   a.gre = ctx->d_gre; a.invg = ctx->d_invg;
   a.state = ctx->d_state; a.nl = ctx->d_nl; a.sv = ctx->d_sv;
-  a.work = ctx->d_spec;  // J_NJOB slots of the spectral scratch (free between evaluations)
+  a.work = ctx->d_spec;
   a.implicit = ctx->cfg.implicit;
   a.cod_bc = ctx->cfg.cod_bc; a.comp_bc = ctx->cfg.comp_bc;
   a.qi = ctx->cfg.qi; a.qo = ctx->cfg.qo; a.qi_comp = ctx->cfg.qi_comp; a.qo_comp = ctx->cfg.qo_comp;
@@ -474,7 +563,11 @@ StepArgs step_args(lsd_ctx* ctx) {
 }  // namespace
 
 // One nonlinear evaluation: main.F90:102-124 for Boussinesq MHD + codensity.
-int lsd_eval(lsd_ctx* ctx) {
+int lsd_eval(lsd_ctx* ctx) { return lsd_eval_marked(ctx, nullptr); }
+
+// marks (optional): 5 events recorded after the spectral preparation, the synthesis, the
+// FFT+products, the analysis and the tail
+int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   const size_t F = (size_t)ctx->N * ctx->H;
   const size_t FF = (size_t)ctx->N * ctx->NM * ctx->Th;
   cplx* sp = ctx->d_spec;
@@ -488,6 +581,7 @@ int lsd_eval(lsd_ctx* ctx) {
   k_curl<<<g, 128, 0, s>>>(sa, sp + S_BQ * F, sp + S_BS * F, sp + S_BT * F, sp + S_BCQ * F, sp + S_BCS * F, sp + S_BCT * F);
   k_drC<<<g, 128, 0, s>>>(sa, st + LSD_COD_C * F, sp + S_DC * F);
   ctx->launches += 5;
+  if (marks) cudaEventRecord(marks[0], s);
   cplx* fo = ctx->d_four;
   SynthGroup sg[5];
   const int vin[4][3] = {{S_VQ, S_VS, S_VT}, {S_VCQ, S_VCS, S_VCT}, {S_BQ, S_BS, S_BT}, {S_BCQ, S_BCS, S_BCT}};
@@ -500,7 +594,9 @@ int lsd_eval(lsd_ctx* ctx) {
   for (int k = 0; k < 3; ++k) sg[4].out[k] = fo + (12 + k) * FF;
   int rc;
   if ((rc = lsd_launch_synth(ctx, sg, 5))) return rc;
+  if (marks) cudaEventRecord(marks[1], s);
   if ((rc = lsd_launch_products(ctx, fo, fo))) return rc;
+  if (marks) cudaEventRecord(marks[2], s);
   AnalGroup ag[3];
   ag[0].kind = AK_VECTOR;
   ag[1].kind = AK_VECTOR;
@@ -512,6 +608,7 @@ int lsd_eval(lsd_ctx* ctx) {
   ag[2].in[0] = fo + 6 * FF; ag[2].out[0] = sp + S_DC * F;
   ag[2].in[1] = ag[2].in[2] = nullptr; ag[2].out[1] = ag[2].out[2] = nullptr;
   if ((rc = lsd_launch_anal(ctx, ag, 3))) return rc;
+  if (marks) cudaEventRecord(marks[3], s);
   TailArgs ta;
   ta.s = sa;
   const lsd_config& c = ctx->cfg;
@@ -527,15 +624,47 @@ int lsd_eval(lsd_ctx* ctx) {
   ta.codNC = ctx->d_nl + LSD_N_COD * F;
   k_tail<<<g, 128, 0, s>>>(ta);
   ctx->launches++;
+  if (marks) cudaEventRecord(marks[4], s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("evaluation: ") + cudaGetErrorString(e));
   return LSD_OK;
 }
 
+namespace {
+template <int KL>
+void launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
+  dim3 g(ctx->nsblk, J_NJOB);
+  const int N = ctx->N;
+  size_t smem = sizeof(double) * ((size_t)N * SCW + 2 * (size_t)N * (3 * KL + 1) + (size_t)N * (2 * KL + 1) + 2 * N + 4 + 2 * N)
+              + sizeof(int) * 2 * N;
+  if (corr) {
+    cudaFuncSetAttribute(k_corrector<KL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_corrector<KL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    k_corrector<KL><<<g, SCW, smem, ctx->stream>>>(a);
+  } else {
+    cudaFuncSetAttribute(k_predictor<KL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_predictor<KL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    k_predictor<KL><<<g, SCW, smem, ctx->stream>>>(a);
+  }
+}
+
+int launch_step_kernel(lsd_ctx* ctx, const StepArgs& a, bool corr) {
+  switch (ctx->KL) {
+    case 2: launch_pred<2>(ctx, a, corr); break;
+    case 3: launch_pred<3>(ctx, a, corr); break;
+    case 4: launch_pred<4>(ctx, a, corr); break;
+    case 5: launch_pred<5>(ctx, a, corr); break;
+    case 6: launch_pred<6>(ctx, a, corr); break;
+    default: return lsd_fail(ctx, LSD_EARG, "stencil half-width KL must be 2..6 for the step kernels");
+  }
+  return LSD_OK;
+}
+}  // namespace
+
 int lsd_pred(lsd_ctx* ctx) {
   StepArgs a = step_args(ctx);
-  dim3 g(ceil_div(ctx->H, 64), J_NJOB);
-  k_predictor<<<g, 64, 0, ctx->stream>>>(a);
+  int rc = launch_step_kernel(ctx, a, false);
+  if (rc) return rc;
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_predictor: ") + cudaGetErrorString(e));
@@ -545,8 +674,8 @@ int lsd_pred(lsd_ctx* ctx) {
 int lsd_corr(lsd_ctx* ctx) {
   StepArgs a = step_args(ctx);
   cudaMemsetAsync(ctx->d_red, 0, sizeof(double) * 8, ctx->stream);
-  dim3 g(ceil_div(ctx->H, 64), J_NJOB);
-  k_corrector<<<g, 64, 0, ctx->stream>>>(a);
+  int rc = launch_step_kernel(ctx, a, true);
+  if (rc) return rc;
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_corrector: ") + cudaGetErrorString(e));

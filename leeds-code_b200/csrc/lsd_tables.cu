@@ -310,7 +310,7 @@ __global__ void k_build_ops(int N, int KL, int L, const double* r, const double*
           double t = (double)(l * (l + 1)) * rm2[j - 1];
           v = v + c1_ - c2y * (t + P.Hyp * t * t);
         }
-        y[(((size_t)fam * N + (j - 1)) * ldm + (row - 1)) * L + l] = v;
+        y[(((size_t)fam * L + l) * N + (j - 1)) * ldm + (row - 1)] = v;
       }
   }
 #undef AX
@@ -330,7 +330,7 @@ __global__ void k_lu_transpose(int N, int KL, int L, const double* lu, const int
 }
 
 // Green's functions and influence matrices (velocity.F90:148-168)
-__global__ void k_greens(int N, int KL, int L, const double* lu, const int* ipiv, double* gre, double* invg, int* fail) {
+__global__ void k_greens(int N, int KL, int L, const double* lu, const int* ipiv, double* gre, double* gret, double* invg, int* fail) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l < 1 || l >= L) return;
   const int ld = 3 * KL + 1;
@@ -351,6 +351,10 @@ __global__ void k_greens(int N, int KL, int L, const double* lu, const int* ipiv
   double a[4] = {g1[0], g1[N - 1], g2[0], g2[N - 1]};  // invG(i,j) at a[(i-1)+2(j-1)]
   if (dev_mat_invert(2, a, 2) != 0) atomicExch(fail, 4);
   for (int k = 0; k < 4; ++k) invg[(size_t)l * 4 + k] = a[k];
+  for (int n = 0; n < N; ++n) {  // [n][2][L] copy for coalesced use in the solves
+    gret[((size_t)n * 2 + 0) * L + l] = g1[n];
+    gret[((size_t)n * 2 + 1) * L + l] = g2[n];
+  }
 }
 
 }  // namespace
@@ -415,7 +419,8 @@ int lsd_build_operators(lsd_ctx* ctx) {
   k_build_ops<<<g, 32, 0, s>>>(N, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap, P, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_info);
   dim3 gt(ceil_div(L, 64), N, OP_NFAM);
   k_lu_transpose<<<gt, 64, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_lus, ctx->d_ipivs);
-  k_greens<<<ceil_div(L, 32), 32, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_gre, ctx->d_invg, d_fail);
+  CUDA_TRY(cudaMemsetAsync(ctx->d_gret, 0, sizeof(double) * 2 * N * L, s));
+  k_greens<<<ceil_div(L, 32), 32, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_gre, ctx->d_gret, ctx->d_invg, d_fail);
   ctx->launches += 3;
   CUDA_TRY(cudaGetLastError());
   std::vector<int> info((size_t)OP_NFAM * L);

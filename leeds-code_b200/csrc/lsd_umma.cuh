@@ -1,0 +1,106 @@
+// lsd_umma.cuh -- thin inline-PTX helpers for the sm_100a tensor-core path (tcgen05 UMMA
+// with int8 operands in shared memory and int32 accumulators in tensor memory).
+//
+// Shared-memory operands use the K-major, no-swizzle canonical layout: 8-row x 16-byte
+// core matrices; the two 16-byte K halves of one 32-byte MMA K step are LBO bytes apart
+// and consecutive 8-row groups are SBO bytes apart.  Every wait on an mbarrier is
+// bounded: on timeout it records an error code instead of spinning forever.
+#pragma once
+#include <cstdint>
+
+namespace umma {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor (tcgen05 "matrix descriptor"), SWIZZLE_NONE, K-major
+__device__ __forceinline__ uint64_t desc_kmajor_noswz(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+  return d;
+}
+
+// instruction descriptor for kind::i8: signed int8 A and B, int32 D, K-major A and B
+__host__ __device__ constexpr uint32_t idesc_s8(int M, int N) {
+  return (2u << 4)                       // D format: S32
+       | (1u << 7)                       // A format: signed 8-bit
+       | (1u << 10)                      // B format: signed 8-bit
+       | ((uint32_t)(N >> 3) << 17)      // N / 8
+       | ((uint32_t)(M >> 4) << 24);     // M / 16
+}
+
+__device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, int accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void commit(uint64_t* mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :: "r"(smem_u32(mbar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+
+// Wait for the phase `parity` of an mbarrier to complete; gives up after max_iter
+// polls and returns false (the caller records an error and carries on to clean up).
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, long long max_iter) {
+  uint32_t addr = smem_u32(mbar);
+  for (long long it = 0; it < max_iter; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// whole warp: allocate ncols (power of two >= 32) TMEM columns, address written to *dst
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+               :: "r"(smem_u32(dst)), "r"(ncols) : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(ncols) : "memory");
+}
+
+// whole warp: 8 consecutive 32-bit columns of this thread's lane (lane quarter of the warp)
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int32_t (&v)[8]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// byte offset of (row r, byte b of the K step) in a K-major no-swizzle tile whose 8-row
+// groups are 256 bytes apart (two 128-byte core matrices per group: LBO = 128, SBO = 256)
+__host__ __device__ __forceinline__ int tile_off(int r, int b) {
+  return (r >> 3) * 256 + (b >> 4) * 128 + (r & 7) * 16 + (b & 15);
+}
+
+}  // namespace umma

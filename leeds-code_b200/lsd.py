@@ -71,6 +71,8 @@ def load_library(path=None):
         "lsd_energies": [_V, _D],
         "lsd_banded_factor_device": [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V, _V, _V],
         "lsd_banded_solve_device": [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V, _V, ctypes.c_int, _V, _V],
+        "lsd_profile_phases": [_V, _D, _I],
+        "lsd_selftest": [_V, ctypes.c_int, _D],
         "lsd_synchronize": [_V],
         "lsd_last_elapsed_ms": [_V, _D],
         "lsd_kernel_launches": [_V, ctypes.POINTER(ctypes.c_longlong)],
@@ -265,6 +267,21 @@ class Context:
 
     def banded_solve_device(self, n, kl, nmat, d_ab, d_ipiv, nrhs, d_map, d_b):
         self._ok(self.lib.lsd_banded_solve_device(self.h, n, kl, nmat, _V(d_ab), _V(d_ipiv), nrhs, _V(d_map), _V(d_b)))
+
+    PHASES = ["spectral_prep", "synthesis", "fft_products", "analysis", "spectral_tail",
+              "predictor_solve", "corrector_solve"]
+
+    def profile_phases(self):
+        """Device milliseconds of the phases of one full step (it advances the state)."""
+        ms = np.zeros(7)
+        n = ctypes.c_int(7)
+        self._ok(self.lib.lsd_profile_phases(self.h, _dp(ms), ctypes.byref(n)))
+        return dict(zip(self.PHASES, ms))
+
+    def selftest(self, which=0):
+        r = ctypes.c_double(-1.0)
+        self._ok(self.lib.lsd_selftest(self.h, int(which), ctypes.byref(r)))
+        return r.value
 
     def synchronize(self):
         self._ok(self.lib.lsd_synchronize(self.h))

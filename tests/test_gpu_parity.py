@@ -219,3 +219,12 @@ def test_batched_banded_solve():
         res = np.abs(A @ x[:, r] - b[:, r]).max() / np.abs(b[:, r]).max()
         assert res < 1e-13
     g.close()
+
+
+@pytest.mark.gpu
+def test_tensor_core_int8_selftest():
+    """One tcgen05 int8 product (128x32x64) through the library's descriptors and TMEM
+    read-out equals the exact integer product."""
+    g = pkg.Context(small_cfg())
+    assert g.selftest(0) == 0.0
+    g.close()
