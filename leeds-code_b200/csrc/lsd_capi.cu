@@ -342,7 +342,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   ctx->nspec = 13;
   TRY(dalloc(ctx, &ctx->d_spec, (size_t)ctx->nspec * F));
   ctx->nfour = 15;
-  TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * NM * Th));
+  TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * NM * 2 * Th2));
   TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));
   ctx->h_pin_bytes = std::max(sizeof(cplx) * F * 3, sizeof(double) * 16);
@@ -517,7 +517,7 @@ int lsd_tra_qst2rtp(lsd_ctx* ctx, const double* q_re, const double* q_im, const 
   int rc;
   if ((rc = ensure_phys(ctx, 3))) return rc;
   if ((rc = spec_in(ctx, 0, q_re, q_im)) || (rc = spec_in(ctx, 1, s_re, s_im)) || (rc = spec_in(ctx, 2, t_re, t_im))) return rc;
-  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * ctx->Th;
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2;
   SynthGroup g;
   g.kind = SK_VECTOR;
   for (int k = 0; k < 3; ++k) { g.in[k] = ctx->d_spec + k * F; g.out[k] = ctx->d_four + k * FF; }
@@ -542,7 +542,7 @@ int lsd_tra_rtp2qst(lsd_ctx* ctx, const double* r, const double* th, const doubl
   CUDA_TRY(cudaMemcpy(ctx->d_phys, r, sizeof(double) * P, cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(ctx->d_phys + P, th, sizeof(double) * P, cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(ctx->d_phys + 2 * P, ph, sizeof(double) * P, cudaMemcpyHostToDevice));
-  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * ctx->Th;
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2;
   AnalGroup g;
   g.kind = AK_VECTOR;
   for (int k = 0; k < 3; ++k) { g.in[k] = ctx->d_four + k * FF; g.out[k] = ctx->d_spec + k * F; }
@@ -560,7 +560,7 @@ int lsd_tra_grad(lsd_ctx* ctx, const double* s_re, const double* s_im, double* t
   int rc;
   if ((rc = ensure_phys(ctx, 3))) return rc;
   if ((rc = spec_in(ctx, 0, s_re, s_im))) return rc;
-  const size_t FF = (size_t)ctx->N * ctx->NM * ctx->Th;
+  const size_t FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2;
   SynthGroup g;
   g.kind = SK_GRAD2;
   g.in[0] = ctx->d_spec; g.in[1] = g.in[2] = nullptr;
@@ -579,7 +579,7 @@ int lsd_tra_grad(lsd_ctx* ctx, const double* s_re, const double* s_im, double* t
 int lsd_sht_synth_device(lsd_ctx* ctx, int nbatch, const double* d_spec, double* d_phys) {
   if (!ctx || !d_spec || !d_phys || nbatch < 1) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
-  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * ctx->Th, P = phys_count(ctx);
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2, P = phys_count(ctx);
   const cplx* in = (const cplx*)d_spec;
   for (int b0 = 0; b0 < nbatch; b0 += ctx->nfour) {
     int nb = std::min(ctx->nfour, nbatch - b0);
@@ -603,7 +603,7 @@ int lsd_sht_synth_device(lsd_ctx* ctx, int nbatch, const double* d_spec, double*
 int lsd_sht_analys_device(lsd_ctx* ctx, int nbatch, const double* d_phys, double* d_spec) {
   if (!ctx || !d_spec || !d_phys || nbatch < 1) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
-  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * ctx->Th, P = phys_count(ctx);
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2, P = phys_count(ctx);
   cplx* out = (cplx*)d_spec;
   for (int b0 = 0; b0 < nbatch; b0 += ctx->nfour) {
     int nb = std::min(ctx->nfour, nbatch - b0);

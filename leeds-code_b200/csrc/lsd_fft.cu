@@ -22,7 +22,7 @@
 namespace {
 
 struct FFTPlanDev {
-  int P2, Ph, M, NM, Th, nrad;
+  int P2, Ph, M, NM, Th, Th2, nrad;
   int rad[16];
   const double2* tw2;  // e^{+2 pi i k/P2}
   const double2* twh;  // e^{+2 pi i k/Ph}
@@ -129,58 +129,85 @@ __device__ __forceinline__ double2 r2c_unpack(int k, const double2* Z, const FFT
   return make_double2(A.x + wb.x, A.y + wb.y);
 }
 
-// ---- standalone c2r: theta-Fourier [f][n][NM][Th] -> phys [f][n][Ph][Th] ---------------
-__global__ void k_c2r(FFTPlanDev pl, int N, const cplx* four, double* phys, int TJ) {
+// The theta-Fourier arrays hold the even/odd half-grid sums of the reference's
+// Legendre loops, [f][n][m-counter][p][Th2] with p = 0 (E) and 1 (O): a southern row
+// h < Th2 is E + O, its northern mirror Th-1-h is E - O.  A CTA therefore owns TH
+// half-rows h and transforms both full rows of each (row 2hh: south, 2hh+1: north);
+// for odd Th the equator row is its own mirror and is written once.
+__device__ __forceinline__ int row_theta(int h, int side, int Th) { return side ? Th - 1 - h : h; }
+
+// ---- standalone c2r: theta-Fourier -> phys [f][n][Ph][Th] -------------------------------
+__global__ void k_c2r(FFTPlanDev pl, int N, const cplx* four, double* phys, int TH) {
   extern __shared__ double2 sm[];
-  const int f = blockIdx.z, n = blockIdx.y, j0 = blockIdx.x * TJ;
-  const int P2 = pl.P2, Th = pl.Th;
-  const int tj = min(TJ, Th - j0);
+  const int f = blockIdx.z, n = blockIdx.y, h0 = blockIdx.x * TH;
+  const int P2 = pl.P2, Th = pl.Th, Th2 = pl.Th2, M = pl.M;
+  const int th = min(TH, Th2 - h0);
+  const int rows = 2 * th;
   double2* A = sm;
-  double2* B = sm + (size_t)TJ * P2;
-  double2* Ybuf = B;  // bins staged in B first: [TJ][M]
-  const cplx* src = four + ((size_t)f * N + n) * pl.NM * Th;
-  for (int i = threadIdx.x; i < pl.NM * tj; i += blockDim.x) {
-    int c = i / tj, jj = i % tj;
-    Ybuf[jj * pl.M + pl.thm[c]] = src[(size_t)c * Th + j0 + jj];
+  double2* B = sm + (size_t)2 * TH * P2;
+  double2* Ybuf = B;  // bins staged in B first: [row][M]
+  const cplx* src = four + ((size_t)f * N + n) * pl.NM * 2 * Th2;
+  for (int i = threadIdx.x; i < pl.NM * th; i += blockDim.x) {
+    int c = i / th, hh = i % th;
+    double2 e = src[((size_t)c * 2 + 0) * Th2 + h0 + hh], o = src[((size_t)c * 2 + 1) * Th2 + h0 + hh];
+    int b = pl.thm[c];
+    Ybuf[(2 * hh + 0) * M + b] = make_double2(e.x + o.x, e.y + o.y);
+    Ybuf[(2 * hh + 1) * M + b] = make_double2(e.x - o.x, e.y - o.y);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < tj * P2; i += blockDim.x) {
-    int jj = i / P2, k = i % P2;
-    const double2* Y = Ybuf + jj * pl.M;
-    A[jj * P2 + k] = c2r_pack(k, pl, [&](int b) { return b < pl.M ? Y[b] : make_double2(0.0, 0.0); });
+  for (int i = threadIdx.x; i < rows * P2; i += blockDim.x) {
+    int r = i / P2, k = i % P2;
+    const double2* Y = Ybuf + r * M;
+    A[r * P2 + k] = c2r_pack(k, pl, [&](int b) { return b < M ? Y[b] : make_double2(0.0, 0.0); });
   }
   __syncthreads();
-  double2* R = block_fft(A, B, tj, pl, +1);
+  double2* R = block_fft(A, B, rows, pl, +1);
   double* dst = phys + ((size_t)f * N + n) * (size_t)pl.Ph * Th;
-  for (int i = threadIdx.x; i < tj * P2; i += blockDim.x) {
-    int t = i / tj, jj = i % tj;
-    double2 z = R[jj * P2 + t];
-    dst[(size_t)(2 * t) * Th + j0 + jj] = z.x;
-    dst[(size_t)(2 * t + 1) * Th + j0 + jj] = z.y;
+  for (int i = threadIdx.x; i < rows * P2; i += blockDim.x) {
+    int t = i / rows, r = i % rows;
+    int hh = r >> 1, side = r & 1, h = h0 + hh;
+    int j = row_theta(h, side, Th);
+    if (side && j == h) continue;
+    double2 z = R[r * P2 + t];
+    dst[(size_t)(2 * t) * Th + j] = z.x;
+    dst[(size_t)(2 * t + 1) * Th + j] = z.y;
   }
 }
 
-// ---- standalone r2c: phys [f][n][Ph][Th] -> theta-Fourier [f][n][NM][Th] ---------------
-__global__ void k_r2c(FFTPlanDev pl, int N, const double* phys, cplx* four, int TJ) {
+// fold two transformed rows (south, north) of half-row h into E and O bins
+__device__ __forceinline__ void fold_store(cplx* dst, int c, int Th2, int h, double2 xs, double2 xn, bool equator) {
+  double2 e = make_double2(xs.x + xn.x, xs.y + xn.y);
+  double2 o = make_double2(xs.x - xn.x, xs.y - xn.y);
+  if (equator) { e.x *= 0.5; e.y *= 0.5; }  // odd Th: the equator row is counted once
+  dst[((size_t)c * 2 + 0) * Th2 + h] = e;
+  dst[((size_t)c * 2 + 1) * Th2 + h] = o;
+}
+
+// ---- standalone r2c: phys [f][n][Ph][Th] -> theta-Fourier (folded E/O) ---------------------
+__global__ void k_r2c(FFTPlanDev pl, int N, const double* phys, cplx* four, int TH) {
   extern __shared__ double2 sm[];
-  const int f = blockIdx.z, n = blockIdx.y, j0 = blockIdx.x * TJ;
-  const int P2 = pl.P2, Th = pl.Th;
-  const int tj = min(TJ, Th - j0);
+  const int f = blockIdx.z, n = blockIdx.y, h0 = blockIdx.x * TH;
+  const int P2 = pl.P2, Th = pl.Th, Th2 = pl.Th2;
+  const int th = min(TH, Th2 - h0);
+  const int rows = 2 * th;
   double2* A = sm;
-  double2* B = sm + (size_t)TJ * P2;
+  double2* B = sm + (size_t)2 * TH * P2;
   const double* src = phys + ((size_t)f * N + n) * (size_t)pl.Ph * Th;
   const double scale = 1.0 / (double)pl.Ph;
-  for (int i = threadIdx.x; i < tj * P2; i += blockDim.x) {
-    int t = i / tj, jj = i % tj;
-    A[jj * P2 + t] = make_double2(src[(size_t)(2 * t) * Th + j0 + jj] * scale,
-                                  src[(size_t)(2 * t + 1) * Th + j0 + jj] * scale);
+  for (int i = threadIdx.x; i < rows * P2; i += blockDim.x) {
+    int t = i / rows, r = i % rows;
+    int j = row_theta(h0 + (r >> 1), r & 1, Th);
+    A[r * P2 + t] = make_double2(src[(size_t)(2 * t) * Th + j] * scale, src[(size_t)(2 * t + 1) * Th + j] * scale);
   }
   __syncthreads();
-  double2* R = block_fft(A, B, tj, pl, -1);
-  cplx* dst = four + ((size_t)f * N + n) * pl.NM * Th;
-  for (int i = threadIdx.x; i < pl.NM * tj; i += blockDim.x) {
-    int c = i / tj, jj = i % tj;
-    dst[(size_t)c * Th + j0 + jj] = r2c_unpack(pl.thm[c], R + (size_t)jj * P2, pl);
+  double2* R = block_fft(A, B, rows, pl, -1);
+  cplx* dst = four + ((size_t)f * N + n) * pl.NM * 2 * Th2;
+  for (int i = threadIdx.x; i < pl.NM * th; i += blockDim.x) {
+    int c = i / th, hh = i % th, h = h0 + hh;
+    int b = pl.thm[c];
+    double2 xs = r2c_unpack(b, R + (size_t)(2 * hh) * P2, pl);
+    double2 xn = r2c_unpack(b, R + (size_t)(2 * hh + 1) * P2, pl);
+    fold_store(dst, c, Th2, h, xs, xn, (Th & 1) && h == Th2 - 1);
   }
 }
 
@@ -193,19 +220,24 @@ struct ProdConst {
 
 constexpr int NF_IN = 15, NF_OUT = 7;
 
-__global__ void k_products(FFTPlanDev pl, int N, ProdConst pc, const cplx* four_in, cplx* four_out, int TJ) {
+__global__ void k_products(FFTPlanDev pl, int N, ProdConst pc, const cplx* four_in, cplx* four_out, int TH) {
   extern __shared__ double2 sm[];
-  const int n = blockIdx.y, j0 = blockIdx.x * TJ;
-  const int P2 = pl.P2, Th = pl.Th, M = pl.M, NM = pl.NM;
-  const int tj = min(TJ, Th - j0);
-  const int rows = NF_IN * tj;
+  const int n = blockIdx.y, h0 = blockIdx.x * TH;
+  const int P2 = pl.P2, Th = pl.Th, Th2 = pl.Th2, M = pl.M, NM = pl.NM;
+  const int th = min(TH, Th2 - h0);
+  const int rpf = 2 * th;            // rows per field
+  const int rows = NF_IN * rpf;
   double2* A = sm;
-  double2* B = sm + (size_t)NF_IN * TJ * P2;
-  const size_t fstride = (size_t)N * NM * Th;
-  // stage bins into B as [row][M], row = f*tj + jj
-  for (int i = threadIdx.x; i < NF_IN * NM * tj; i += blockDim.x) {
-    int jj = i % tj, rem = i / tj, c = rem % NM, f = rem / NM;
-    B[(f * tj + jj) * M + pl.thm[c]] = four_in[f * fstride + ((size_t)n * NM + c) * Th + j0 + jj];
+  double2* B = sm + (size_t)NF_IN * 2 * TH * P2;
+  const size_t fstride = (size_t)N * NM * 2 * Th2;
+  // stage bins into B as [row][M], row = f*rpf + 2*hh + side
+  for (int i = threadIdx.x; i < NF_IN * NM * th; i += blockDim.x) {
+    int hh = i % th, rem = i / th, c = rem % NM, f = rem / NM;
+    const cplx* src = four_in + f * fstride + ((size_t)n * NM + c) * 2 * Th2 + h0 + hh;
+    double2 e = src[0], o = src[Th2];
+    int b = pl.thm[c];
+    B[(f * rpf + 2 * hh + 0) * M + b] = make_double2(e.x + o.x, e.y + o.y);
+    B[(f * rpf + 2 * hh + 1) * M + b] = make_double2(e.x - o.x, e.y - o.y);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < rows * P2; i += blockDim.x) {
@@ -216,14 +248,14 @@ __global__ void k_products(FFTPlanDev pl, int N, ProdConst pc, const cplx* four_
   __syncthreads();
   double2* X = block_fft(A, B, rows, pl, +1);
   double2* W = (X == A) ? B : A;  // the other buffer receives the products
-  // products at every point (row jj, sample t, part re/im)
-  for (int i = threadIdx.x; i < tj * P2; i += blockDim.x) {
-    int jj = i / P2, t = i % P2;
-    int j = j0 + jj;
+  // products at every point (row r, sample t, part re/im)
+  for (int i = threadIdx.x; i < rpf * P2; i += blockDim.x) {
+    int r = i / P2, t = i % P2;
+    int j = row_theta(h0 + (r >> 1), r & 1, Th);
     double sn = pc.sn[j], cs = pc.gp[j];
     double2 v[NF_IN];
 #pragma unroll
-    for (int f = 0; f < NF_IN; ++f) v[f] = X[(size_t)(f * tj + jj) * P2 + t];
+    for (int f = 0; f < NF_IN; ++f) v[f] = X[(size_t)(f * rpf + r) * P2 + t];
     double2 out[NF_OUT];
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
@@ -256,27 +288,30 @@ __global__ void k_products(FFTPlanDev pl, int N, ProdConst pc, const cplx* four_
     const double scale = 1.0 / (double)pl.Ph;
 #pragma unroll
     for (int q = 0; q < NF_OUT; ++q)
-      W[(size_t)(q * tj + jj) * P2 + t] = make_double2(out[q].x * scale, out[q].y * scale);
+      W[(size_t)(q * rpf + r) * P2 + t] = make_double2(out[q].x * scale, out[q].y * scale);
   }
   __syncthreads();
-  double2* Z = block_fft(W, X, NF_OUT * tj, pl, -1);
-  for (int i = threadIdx.x; i < NF_OUT * NM * tj; i += blockDim.x) {
-    int jj = i % tj, rem = i / tj, c = rem % NM, q = rem / NM;
-    four_out[q * fstride + ((size_t)n * NM + c) * Th + j0 + jj] = r2c_unpack(pl.thm[c], Z + (size_t)(q * tj + jj) * P2, pl);
+  double2* Z = block_fft(W, X, NF_OUT * rpf, pl, -1);
+  for (int i = threadIdx.x; i < NF_OUT * NM * th; i += blockDim.x) {
+    int hh = i % th, rem = i / th, c = rem % NM, q = rem / NM;
+    int h = h0 + hh, b = pl.thm[c];
+    double2 xs = r2c_unpack(b, Z + (size_t)(q * rpf + 2 * hh) * P2, pl);
+    double2 xn = r2c_unpack(b, Z + (size_t)(q * rpf + 2 * hh + 1) * P2, pl);
+    fold_store(four_out + q * fstride + (size_t)n * NM * 2 * Th2, c, Th2, h, xs, xn, (Th & 1) && h == Th2 - 1);
   }
 }
 
 FFTPlanDev make_plan(lsd_ctx* ctx) {
   FFTPlanDev pl;
-  pl.P2 = ctx->P2; pl.Ph = ctx->Ph; pl.M = ctx->M; pl.NM = ctx->NM; pl.Th = ctx->Th;
+  pl.P2 = ctx->P2; pl.Ph = ctx->Ph; pl.M = ctx->M; pl.NM = ctx->NM; pl.Th = ctx->Th; pl.Th2 = ctx->Th2;
   pl.nrad = ctx->nrad;
   for (int i = 0; i < 16; ++i) pl.rad[i] = ctx->radices[i];
   pl.tw2 = ctx->d_tw2; pl.twh = ctx->d_twh; pl.thm = ctx->d_thm;
   return pl;
 }
 
-int pick_tj(int rows_per_j, int P2, size_t budget) {
-  size_t per = (size_t)2 * rows_per_j * P2 * sizeof(double2);
+int pick_tj(int rows_per_j, int P2, size_t budget) {  // half-rows per CTA (2 full rows each)
+  size_t per = (size_t)2 * 2 * rows_per_j * P2 * sizeof(double2);
   int tj = (int)(budget / per);
   if (tj > 16) tj = 16;
   return tj < 1 ? 0 : tj;
@@ -288,10 +323,10 @@ int lsd_launch_c2r(lsd_ctx* ctx, const cplx* four, double* phys, int nfields) {
   FFTPlanDev pl = make_plan(ctx);
   int TJ = pick_tj(1, ctx->P2, 200 * 1024);
   if (TJ == 0) return lsd_fail(ctx, LSD_EARG, "FFT row does not fit in shared memory");
-  size_t smem = (size_t)2 * TJ * ctx->P2 * sizeof(double2);
+  size_t smem = (size_t)2 * 2 * TJ * ctx->P2 * sizeof(double2);
   cudaFuncSetAttribute(k_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_c2r, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  dim3 grid(ceil_div(ctx->Th, TJ), ctx->N, nfields);
+  dim3 grid(ceil_div(ctx->Th2, TJ), ctx->N, nfields);
   k_c2r<<<grid, 256, smem, ctx->stream>>>(pl, ctx->N, four, phys, TJ);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
@@ -303,10 +338,10 @@ int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields) {
   FFTPlanDev pl = make_plan(ctx);
   int TJ = pick_tj(1, ctx->P2, 200 * 1024);
   if (TJ == 0) return lsd_fail(ctx, LSD_EARG, "FFT row does not fit in shared memory");
-  size_t smem = (size_t)2 * TJ * ctx->P2 * sizeof(double2);
+  size_t smem = (size_t)2 * 2 * TJ * ctx->P2 * sizeof(double2);
   cudaFuncSetAttribute(k_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_r2c, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  dim3 grid(ceil_div(ctx->Th, TJ), ctx->N, nfields);
+  dim3 grid(ceil_div(ctx->Th2, TJ), ctx->N, nfields);
   k_r2c<<<grid, 256, smem, ctx->stream>>>(pl, ctx->N, phys, four, TJ);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
@@ -318,7 +353,7 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   FFTPlanDev pl = make_plan(ctx);
   int TJ = pick_tj(NF_IN, ctx->P2, 220 * 1024);
   if (TJ == 0) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
-  size_t smem = (size_t)2 * NF_IN * TJ * ctx->P2 * sizeof(double2);
+  size_t smem = (size_t)2 * NF_IN * 2 * TJ * ctx->P2 * sizeof(double2);
   // the bin staging area [rows][M] must fit in one buffer
   ProdConst pc;
   const lsd_config& c = ctx->cfg;
@@ -329,7 +364,7 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.gp = ctx->d_gp;
   cudaFuncSetAttribute(k_products, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_products, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  dim3 grid(ceil_div(ctx->Th, TJ), ctx->N);
+  dim3 grid(ceil_div(ctx->Th2, TJ), ctx->N);
   k_products<<<grid, 512, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out, TJ);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();

@@ -166,17 +166,15 @@ __global__ void __launch_bounds__(256) k_synth(SynthArgs a) {
     }
   }
   if (j >= Th2) return;
-  const int Th = a.Th, Thh = a.Th / 2;
 #pragma unroll
   for (int o = 0; o < NOUT; ++o)
 #pragma unroll
     for (int q = 0; q < S_NT; ++q) {
       int n = n0 + q;
       if (n >= a.N) continue;
-      cplx* out = G.out[o] + ((size_t)n * a.NM + c) * Th;
-      double2 e = acc[o][0][q], od = acc[o][1][q];
-      out[j] = make_double2(e.x + od.x, e.y + od.y);
-      if (j < Thh) out[Th - 1 - j] = make_double2(e.x - od.x, e.y - od.y);
+      cplx* out = G.out[o] + ((size_t)n * a.NM + c) * 2 * Th2;  // [p][Th2]: E then O
+      out[j] = acc[o][0][q];
+      out[Th2 + j] = acc[o][1][q];
     }
 }
 
@@ -229,13 +227,11 @@ __global__ void __launch_bounds__(288) k_anal(AnalArgs a) {
       int jj = i % jc, rem = i / jc, q = rem % A_NT, rem2 = rem / A_NT, f = rem2 % NF, cc = rem2 / NF;
       int n = n0 + q;
       double2 e = make_double2(0.0, 0.0), o = e;
-      if (n < a.N) {
-        const cplx* src = G.in[f] + ((size_t)n * a.NM + (cc ? c1 : c0)) * Th;
+      if (n < a.N) {  // folded E/O data (the FFT stage folded the two hemispheres)
+        const cplx* src = G.in[f] + ((size_t)n * a.NM + (cc ? c1 : c0)) * 2 * Th2;
         int j = j0 + jj;
-        double2 x = src[j], y = src[Th - 1 - j];
-        e = make_double2(x.x + y.x, x.y + y.y);
-        o = make_double2(x.x - y.x, x.y - y.y);
-        if ((Th & 1) && j == Th2 - 1) { e.x *= 0.5; e.y *= 0.5; }
+        e = src[j];
+        o = src[Th2 + j];
       }
       dat[((cc * NF + f) * 2 + 0) * DROW + jj * A_NT + q] = e;
       dat[((cc * NF + f) * 2 + 1) * DROW + jj * A_NT + q] = o;
