@@ -27,6 +27,7 @@ void free_ctx(lsd_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->g_pred) cudaGraphExecDestroy(ctx->g_pred);
   if (ctx->g_corr) cudaGraphExecDestroy(ctx->g_corr);
+  lsd_ozaki_free(ctx);
   void* ptrs[] = {ctx->d_sblk_l, ctx->d_sblk_nh, ctx->d_aperm, ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_lm2nh,
                   ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,
                   ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y,
@@ -134,6 +135,7 @@ int time_end(lsd_ctx* ctx) {
   float ms = 0.f;
   CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   ctx->last_ms = ms;
+  if (ctx->oz) return lsd_ozaki_check(ctx);
   return LSD_OK;
 }
 
@@ -167,7 +169,11 @@ int check_cgce(lsd_ctx* c) {
 // read the corrector's sums of squares and form tim_dterr (timestep.F90:715-737)
 int finish_corrector(lsd_ctx* ctx) {
   CUDA_TRY(cudaMemcpyAsync(ctx->h_red, ctx->d_red, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  int* oz_err = (int*)(ctx->h_red + 16);
+  *oz_err = 0;
+  if (ctx->oz) CUDA_TRY(cudaMemcpyAsync(oz_err, lsd_ozaki_err_flag(ctx), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (*oz_err) return lsd_fail(ctx, LSD_ECUDA, "tensor-core Legendre contraction: an mbarrier wait timed out");
   const double* r = ctx->h_red;
   double d = ctx->dterr;
   d = d + std::sqrt(r[0]);  // vel Tor
@@ -238,7 +244,9 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   else if (c.timestep <= 0.0) why = "only a fixed timestep (d_timestep > 0) is supported";
   else if (!c.vel_tstep || !c.cod_tstep || !c.mag_tstep) why = "velocity, codensity and field must all be stepped";
   else if (c.comp_tstep) why = "composition stepping is not supported on the device yet";
-  else if (c.precision != LSD_PREC_FP64) why = "the tensor-core Legendre path is not available in this build";
+  else if (c.precision != LSD_PREC_FP64 && c.precision != LSD_PREC_OZAKI) why = "unknown precision";
+  else if (c.precision == LSD_PREC_OZAKI && c.ozaki_slices != 0 && (c.ozaki_slices < 2 || c.ozaki_slices > 8))
+    why = "ozaki_slices must be 0 (default) or 2..8";
   if (!why.empty()) { int rc = lsd_fail(ctx, LSD_EARG, why); free_ctx(ctx); return rc; }
   ctx->Ma = c.M * 3 / 2;
   ctx->H = c.L * c.M - c.Mp * (c.M - 1) * c.M / 2;
@@ -349,6 +357,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   CTRY(cudaMallocHost((void**)&ctx->h_pin, ctx->h_pin_bytes));
   TRY(lsd_build_tables(ctx));
   TRY(lsd_build_operators(ctx));
+  if (c.precision == LSD_PREC_OZAKI) TRY(lsd_ozaki_setup(ctx));
 #undef TRY
 #undef CTRY
   *out = ctx;
@@ -767,6 +776,7 @@ int lsd_synchronize(lsd_ctx* ctx) {
   if (!ctx) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (ctx->oz) return lsd_ozaki_check(ctx);
   return LSD_OK;
 }
 int lsd_last_elapsed_ms(const lsd_ctx* ctx, double* ms) {

@@ -125,6 +125,7 @@ struct lsd_ctx {
   // CUDA graph of one (evaluation + predictor/corrector) pass
   cudaGraphExec_t g_pred = nullptr, g_corr = nullptr;
   long long g_pred_kernels = 0, g_corr_kernels = 0;
+  void* oz = nullptr;  // tensor-core path state (lsd_ozaki.cu)
 };
 
 int lsd_fail(lsd_ctx* ctx, int code, const std::string& msg);
@@ -149,6 +150,21 @@ int lsd_solve_batch(lsd_ctx* ctx, int n, int kl, int nmat, const double* d_ab, c
                     int nrhs, const int* d_map, double* d_b);
 
 int lsd_umma_selftest(lsd_ctx* ctx, double* maxerr);
+// ---- tensor-core (Ozaki) Legendre path (lsd_ozaki.cu) ----
+struct OzSynthGroupH { const cplx* in0; const cplx* in1; cplx* out0; cplx* out1; const int* e0; const int* e1; };
+struct OzAnalGroupH { const cplx* in0; const cplx* in1; cplx* out0; cplx* out1; const int* e0; const int* e1; int zero_m0_im; };
+enum { OZS_VEC = 0, OZS_P = 1, OZS_GRAD = 2, OZA_ST = 3, OZA_Q = 4 };
+int lsd_ozaki_setup(lsd_ctx* ctx);
+void lsd_ozaki_free(lsd_ctx* ctx);
+int lsd_ozaki_exp_spec(lsd_ctx* ctx, const cplx* in, const double* rinv, int slot);
+int lsd_ozaki_exp_four(lsd_ctx* ctx, const cplx* in, int slot);
+const int* lsd_ozaki_exp(lsd_ctx* ctx, int slot);
+int lsd_ozaki_synth(lsd_ctx* ctx, int type, const OzSynthGroupH* g, int ng);
+int lsd_ozaki_anal(lsd_ctx* ctx, int type, const OzAnalGroupH* g, int ng);
+int lsd_ozaki_check(lsd_ctx* ctx);
+int* lsd_ozaki_err_flag(lsd_ctx* ctx);
+int lsd_ozaki_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups);
+int lsd_ozaki_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups);
 
 // small helpers
 static inline int ceil_div(int a, int b) { return (a + b - 1) / b; }

@@ -340,6 +340,7 @@ int launch_anal_kind(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
 }  // namespace
 
 int lsd_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups) {
+  if (ctx->oz) return lsd_ozaki_launch_synth(ctx, groups, ngroups);  // LSD_PREC_OZAKI
   int rc;
   if ((rc = launch_synth_kind<SK_VECTOR>(ctx, groups, ngroups))) return rc;
   if ((rc = launch_synth_kind<SK_SCALAR>(ctx, groups, ngroups))) return rc;
@@ -349,6 +350,7 @@ int lsd_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups) {
 }
 
 int lsd_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
+  if (ctx->oz) return lsd_ozaki_launch_anal(ctx, groups, ngroups);  // LSD_PREC_OZAKI
   int rc;
   if ((rc = launch_anal_kind<AK_VECTOR>(ctx, groups, ngroups))) return rc;
   if ((rc = launch_anal_kind<AK_SCALAR>(ctx, groups, ngroups))) return rc;
