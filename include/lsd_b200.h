@@ -206,6 +206,14 @@ int lsd_corrector(lsd_ctx* ctx, double* dterr);
 int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats);
 /* Energy diagnostics (io_write_vel_energy / io_write_mag_energy), LSD_NENERGY doubles. */
 int lsd_energies(lsd_ctx* ctx, double* out);
+/* lsd_energies without any allocation: no counterpart in the reference.  For host codes
+ * that cannot allocate when they write diagnostics (device memory fully committed to the
+ * state, or work still queued on the stream that a cudaMalloc/cudaFree would stall).  The
+ * norm scratch is a static device array sized for N <= 1024 shells (larger N returns
+ * LSD_EARG); it is cleared by each call, shared by all contexts of a device, so overlapping
+ * calls race.  The first call on a device does the set-up (symbol lookup): make it before
+ * any stream capture. */
+int lsd_energies_static(lsd_ctx* ctx, double* out);
 
 /* ---- batched banded radial solves (timestep.F90:566-588 over every (l,m)) -----------
  * Factorise nmat banded operators A_k (LAPACK band storage with ldab = 3*kl+1, columns

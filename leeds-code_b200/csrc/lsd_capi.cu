@@ -727,6 +727,12 @@ int lsd_energies(lsd_ctx* ctx, double* out) {
   return lsd_energy_device(ctx, out);
 }
 
+int lsd_energies_static(lsd_ctx* ctx, double* out) {
+  if (!ctx || !out) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  return lsd_energy_static(ctx, out);
+}
+
 int lsd_banded_factor_device(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info) {
   if (!ctx || n < 1 || kl < 1 || kl > LSD_MAX_KL || nmat < 1 || !d_ab || !d_ipiv || !d_info) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));

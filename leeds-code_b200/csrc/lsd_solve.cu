@@ -9,6 +9,8 @@
 #include <cmath>
 
 #include "lsd_banded.cuh"
+#include <cstdio>
+
 #include "lsd_common.cuh"
 
 namespace {
@@ -682,9 +684,13 @@ int lsd_corr(lsd_ctx* ctx) {
   return LSD_OK;
 }
 
-// Energy diagnostics (io_write_vel_energy io.F90:1739-1926, io_write_mag_energy
-// io.F90:1933-2024): device norms, host radial dot products in the reference's order.
-int lsd_energy_device(lsd_ctx* ctx, double* out) {
+namespace {
+
+// The derived fields (q, s, t and curl of velocity and field), their per-(field,
+// category, shell) norms summed into d_out (48 N doubles, zeroed here first), and host
+// copies of all that the radial sums need.  d_arrs: device room for 12 pointers.
+int energy_partials(lsd_ctx* ctx, const cplx** d_arrs, double* d_out, double* Fh, double* wts, double* cod0,
+                    double* bpolN, double* r, double* dr1) {
   const int N = ctx->N, H = ctx->H, KL = ctx->KL;
   const size_t F = (size_t)N * H;
   cplx* sp = ctx->d_spec;
@@ -698,23 +704,27 @@ int lsd_energy_device(lsd_ctx* ctx, double* out) {
   k_curl<<<g, 128, 0, s>>>(sa, sp + 6 * F, sp + 7 * F, sp + 8 * F, sp + 9 * F, sp + 10 * F, sp + 11 * F);
   const cplx* arrs[12];
   for (int k = 0; k < 12; ++k) arrs[k] = sp + k * F;
-  const cplx** d_arrs = (const cplx**)(ctx->d_red + 64);  // 12 pointers after the sums
-  double* d_out = ctx->d_red + 128;
   CUDA_TRY(cudaMemcpyAsync(d_arrs, arrs, sizeof(arrs), cudaMemcpyHostToDevice, s));
   CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(double) * 48 * N, s));
   dim3 gn(ceil_div(H, 128), N, 12);
   k_norms<<<gn, 128, 0, s>>>(N, H, ctx->d_l, ctx->d_m, d_arrs, 12, d_out);
   ctx->launches += 5;
-  std::vector<double> Fh((size_t)48 * N), wts(N), cod0(N), bpolN(3 * 2), r(N * 7), dr1((size_t)(2 * KL + 1) * N);
-  CUDA_TRY(cudaMemcpyAsync(Fh.data(), d_out, sizeof(double) * 48 * N, cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(wts.data(), ctx->d_intr2dr, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(r.data(), ctx->d_r, sizeof(double) * 7 * N, cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(dr1.data(), ctx->d_dr, sizeof(double) * dr1.size(), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpy2DAsync(cod0.data(), sizeof(double), st + LSD_COD_C * F, sizeof(cplx) * H, sizeof(double), N,
+  CUDA_TRY(cudaMemcpyAsync(Fh, d_out, sizeof(double) * 48 * N, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(wts, ctx->d_intr2dr, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(r, ctx->d_r, sizeof(double) * 7 * N, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(dr1, ctx->d_dr, sizeof(double) * (2 * KL + 1) * N, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpy2DAsync(cod0, sizeof(double), st + LSD_COD_C * F, sizeof(cplx) * H, sizeof(double), N,
                              cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(bpolN.data(), st + LSD_MAG_POL * F + (size_t)(N - 1) * H, sizeof(cplx) * 3,
+  CUDA_TRY(cudaMemcpyAsync(bpolN, st + LSD_MAG_POL * F + (size_t)(N - 1) * H, sizeof(cplx) * 3,
                            cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
+  return LSD_OK;
+}
+
+// The radial dot products and the energy combinations, on the host in the reference's order.
+int energy_finish(lsd_ctx* ctx, const double* Fh, const double* wts, const double* cod0, const double* bpolN,
+                  const double* r, const double* dr1, double* out) {
+  const int N = ctx->N, KL = ctx->KL;
   auto norm = [&](int k, double& Eo, double& Ee, double& E1, double& E0) {
     double v[4];
     for (int q = 0; q < 4; ++q) {
@@ -775,6 +785,71 @@ int lsd_energy_device(lsd_ctx* ctx, double* out) {
     out[LSD_E_ME_AX] = ME * Etas + ME * Epas;
   }
   return LSD_OK;
+}
+
+}  // namespace
+
+// Energy diagnostics (io_write_vel_energy io.F90:1739-1926, io_write_mag_energy
+// io.F90:1933-2024): device norms, host radial dot products in the reference's order.
+int lsd_energy_device(lsd_ctx* ctx, double* out) {
+  const int N = ctx->N, KL = ctx->KL;
+  std::vector<double> Fh((size_t)48 * N), wts(N), cod0(N), bpolN(3 * 2), r(N * 7), dr1((size_t)(2 * KL + 1) * N);
+  int rc = energy_partials(ctx, (const cplx**)(ctx->d_red + 64), ctx->d_red + 128, Fh.data(), wts.data(),
+                           cod0.data(), bpolN.data(), r.data(), dr1.data());
+  if (rc) return rc;
+  return energy_finish(ctx, Fh.data(), wts.data(), cod0.data(), bpolN.data(), r.data(), dr1.data(), out);
+}
+
+// ---- energies with no allocation -------------------------------------------------------
+// lsd_energy_static: the energies of lsd_energy_device for callers that must not allocate
+// when they ask for diagnostics -- a host code whose device memory is fully committed to
+// its state arrays (cudaMalloc would fail), or one that keeps work queued on its stream
+// while it writes output (cudaMalloc / cudaFree synchronise the device and would stall that
+// pipeline).  The norm partial sums and the 12 field pointers live in a file-scope device
+// array instead of context memory; host staging uses the context's pinned buffer.  The
+// partial sums are accumulated with atomics, so they must start at zero: every call clears
+// them on the context's stream before the norm kernel.  Nothing else needs clearing.  The
+// array is shared by every context on a device, so overlapping calls (two threads, or two
+// streams) race on it.  The first call on a device looks the array up (set-up, which may
+// load this module): make that first call before any stream capture.
+namespace {
+constexpr int ESTATIC_MAX_N = 1024;  // shells
+constexpr int ESTATIC_PTRS = 16;     // 12 field pointers, padded to 128 bytes
+constexpr int ESTATIC_MAX_DEV = 64;
+}  // namespace
+static __device__ __align__(256) double g_energy_scratch[ESTATIC_PTRS + 48 * ESTATIC_MAX_N];  // 384 KiB + 128 B
+static double* g_energy_scratch_ptr[ESTATIC_MAX_DEV] = {};  // per device, filled by the first call
+
+int lsd_energy_static(lsd_ctx* ctx, double* out) {
+  const int N = ctx->N, KL = ctx->KL;
+  char msg[160];
+  if (N > ESTATIC_MAX_N) {
+    snprintf(msg, sizeof(msg), "lsd_energies_static: N = %d shells exceeds the static scratch maximum of %d", N,
+             ESTATIC_MAX_N);
+    return lsd_fail(ctx, LSD_EARG, msg);
+  }
+  const size_t stage = (size_t)(48 + 1 + 1 + 7 + 2 * KL + 1) * N + 6;
+  if (sizeof(double) * stage > ctx->h_pin_bytes)
+    return lsd_fail(ctx, LSD_EARG, "lsd_energies_static: the context's pinned staging buffer is too small");
+  if (ctx->dev < 0 || ctx->dev >= ESTATIC_MAX_DEV) return lsd_fail(ctx, LSD_EARG, "lsd_energies_static: device index");
+  double*& dscr = g_energy_scratch_ptr[ctx->dev];
+  if (!dscr) {  // set-up, once per device, with that device current
+    cudaError_t e = cudaGetSymbolAddress((void**)&dscr, g_energy_scratch);
+    if (e != cudaSuccess) {
+      dscr = nullptr;
+      snprintf(msg, sizeof(msg), "lsd_energies_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      return lsd_fail(ctx, LSD_ECUDA, msg);
+    }
+  }
+  double* Fh = ctx->h_pin;
+  double* wts = Fh + (size_t)48 * N;
+  double* cod0 = wts + N;
+  double* bpolN = cod0 + N;
+  double* r = bpolN + 6;
+  double* dr1 = r + (size_t)7 * N;
+  int rc = energy_partials(ctx, (const cplx**)dscr, dscr + ESTATIC_PTRS, Fh, wts, cod0, bpolN, r, dr1);
+  if (rc) return rc;
+  return energy_finish(ctx, Fh, wts, cod0, bpolN, r, dr1, out);
 }
 
 int lsd_factor_batch(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info) {

@@ -69,6 +69,7 @@ def load_library(path=None):
         "lsd_corrector": [_V, _D],
         "lsd_step": [_V, ctypes.c_int, ctypes.POINTER(capi.LsdStats)],
         "lsd_energies": [_V, _D],
+        "lsd_energies_static": [_V, _D],
         "lsd_banded_factor_device": [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V, _V, _V],
         "lsd_banded_solve_device": [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V, _V, ctypes.c_int, _V, _V],
         "lsd_profile_phases": [_V, _D, _I],
@@ -253,6 +254,12 @@ class Context:
     def energies(self):
         e = np.zeros(capi.NENERGY)
         self._ok(self.lib.lsd_energies(self.h, _dp(e)))
+        return dict(zip(capi.ENERGY_NAMES, e))
+
+    def energies_static(self):
+        """lsd_energies_static: the same diagnostics with a static device scratch (no allocation)."""
+        e = np.zeros(capi.NENERGY)
+        self._ok(self.lib.lsd_energies_static(self.h, _dp(e)))
         return dict(zip(capi.ENERGY_NAMES, e))
 
     # ---- device-resident work (pointers from torch / cuda-python allocations)
