@@ -28,7 +28,7 @@ void free_ctx(lsd_ctx* ctx) {
   if (ctx->g_pred) cudaGraphExecDestroy(ctx->g_pred);
   if (ctx->g_corr) cudaGraphExecDestroy(ctx->g_corr);
   lsd_ozaki_free(ctx);
-  void* ptrs[] = {ctx->d_sblk_l, ctx->d_sblk_nh, ctx->d_aperm, ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_lm2nh,
+  void* ptrs[] = {ctx->d_sblk_l, ctx->d_sblk_nh, ctx->d_aperm, ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_bin2c, ctx->d_lm2nh,
                   ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,
                   ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y,
                   ctx->d_ipiv, ctx->d_ipivs, ctx->d_info, ctx->d_gre, ctx->d_gret, ctx->d_invg, ctx->d_state, ctx->d_nl,
@@ -81,14 +81,6 @@ void build_layout(lsd_ctx* c) {
 }
 
 // radix plan for the complex FFT of length P2 = 3^a 2^b
-bool plan_radices(lsd_ctx* c) {
-  int p = c->P2, n = 0;
-  while (p % 4 == 0 && n < 16) { c->radices[n++] = 4; p /= 4; }
-  while (p % 2 == 0 && n < 16) { c->radices[n++] = 2; p /= 2; }
-  while (p % 3 == 0 && n < 16) { c->radices[n++] = 3; p /= 3; }
-  c->nrad = n;
-  return p == 1;
-}
 
 // packing between Fortran split (re, im) arrays and device interleaved [n][nh]
 void pack_coll(const lsd_ctx* c, const double* re, const double* im, double* out) {  // coll (N,H)
@@ -258,7 +250,8 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   ctx->NM = 2 * ctx->Hc;
   ctx->P2 = ctx->Ma;
   ctx->dt = c.timestep;
-  if (!plan_radices(ctx)) { free_ctx(ctx); return LSD_EARG; }
+  ctx->HB = (ctx->Th2 + 1) / 2;
+  if (!lsd_fft_plan(ctx)) { int rc = lsd_fail(ctx, LSD_EARG, "phi FFT length 3M/2 not supported"); free_ctx(ctx); return rc; }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || c.device < 0 || c.device >= ndev) {
     free_ctx(ctx);
@@ -284,6 +277,12 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   TRY(dalloc(ctx, &ctx->d_mstart, NM)); TRY(upload(ctx, ctx->d_mstart, ctx->mstart));
   TRY(dalloc(ctx, &ctx->d_mlen, NM)); TRY(upload(ctx, ctx->d_mlen, ctx->mlen));
   TRY(dalloc(ctx, &ctx->d_thm, NM)); TRY(upload(ctx, ctx->d_thm, ctx->thm));
+  {  // FFT bin -> m-counter (var_Th%m is a permutation of the bins 0..M-1)
+    std::vector<int> b2c(ctx->M, 0);
+    for (int c = 0; c < NM; ++c)
+      if (ctx->thm[c] >= 0 && ctx->thm[c] < ctx->M) b2c[ctx->thm[c]] = c;
+    TRY(dalloc(ctx, &ctx->d_bin2c, b2c.size())); TRY(upload(ctx, ctx->d_bin2c, b2c));
+  }
   TRY(dalloc(ctx, &ctx->d_lm2nh, lm2nh.size())); TRY(upload(ctx, ctx->d_lm2nh, lm2nh));
   {  // analysis thread order per folded column: (m-counter, parity)-sorted harmonics
     std::vector<int> perm((size_t)ctx->Hc * ctx->Hr);
@@ -350,7 +349,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   ctx->nspec = 13;
   TRY(dalloc(ctx, &ctx->d_spec, (size_t)ctx->nspec * F));
   ctx->nfour = 15;
-  TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * NM * 2 * Th2));
+  TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * ctx->HB * NM * 4));
   TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));
   ctx->h_pin_bytes = std::max(sizeof(cplx) * F * 3, sizeof(double) * 16);
@@ -526,7 +525,7 @@ int lsd_tra_qst2rtp(lsd_ctx* ctx, const double* q_re, const double* q_im, const 
   int rc;
   if ((rc = ensure_phys(ctx, 3))) return rc;
   if ((rc = spec_in(ctx, 0, q_re, q_im)) || (rc = spec_in(ctx, 1, s_re, s_im)) || (rc = spec_in(ctx, 2, t_re, t_im))) return rc;
-  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2;
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
   SynthGroup g;
   g.kind = SK_VECTOR;
   for (int k = 0; k < 3; ++k) { g.in[k] = ctx->d_spec + k * F; g.out[k] = ctx->d_four + k * FF; }
@@ -551,7 +550,7 @@ int lsd_tra_rtp2qst(lsd_ctx* ctx, const double* r, const double* th, const doubl
   CUDA_TRY(cudaMemcpy(ctx->d_phys, r, sizeof(double) * P, cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(ctx->d_phys + P, th, sizeof(double) * P, cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(ctx->d_phys + 2 * P, ph, sizeof(double) * P, cudaMemcpyHostToDevice));
-  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2;
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
   AnalGroup g;
   g.kind = AK_VECTOR;
   for (int k = 0; k < 3; ++k) { g.in[k] = ctx->d_four + k * FF; g.out[k] = ctx->d_spec + k * F; }
@@ -569,7 +568,7 @@ int lsd_tra_grad(lsd_ctx* ctx, const double* s_re, const double* s_im, double* t
   int rc;
   if ((rc = ensure_phys(ctx, 3))) return rc;
   if ((rc = spec_in(ctx, 0, s_re, s_im))) return rc;
-  const size_t FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2;
+  const size_t FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
   SynthGroup g;
   g.kind = SK_GRAD2;
   g.in[0] = ctx->d_spec; g.in[1] = g.in[2] = nullptr;
@@ -588,7 +587,7 @@ int lsd_tra_grad(lsd_ctx* ctx, const double* s_re, const double* s_im, double* t
 int lsd_sht_synth_device(lsd_ctx* ctx, int nbatch, const double* d_spec, double* d_phys) {
   if (!ctx || !d_spec || !d_phys || nbatch < 1) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
-  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2, P = phys_count(ctx);
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4, P = phys_count(ctx);
   const cplx* in = (const cplx*)d_spec;
   for (int b0 = 0; b0 < nbatch; b0 += ctx->nfour) {
     int nb = std::min(ctx->nfour, nbatch - b0);
@@ -612,7 +611,7 @@ int lsd_sht_synth_device(lsd_ctx* ctx, int nbatch, const double* d_spec, double*
 int lsd_sht_analys_device(lsd_ctx* ctx, int nbatch, const double* d_phys, double* d_spec) {
   if (!ctx || !d_spec || !d_phys || nbatch < 1) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
-  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2, P = phys_count(ctx);
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4, P = phys_count(ctx);
   cplx* out = (cplx*)d_spec;
   for (int b0 = 0; b0 < nbatch; b0 += ctx->nfour) {
     int nb = std::min(ctx->nfour, nbatch - b0);

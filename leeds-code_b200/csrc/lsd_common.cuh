@@ -47,6 +47,12 @@ enum AnalKind {
   AK_SCALAR = 1,  // a -> a                                tra_phys2spec :527-602
 };
 
+// theta-Fourier rows: [n][h/2][m-counter c][p = E/O][h%2] per field (complex); a field
+// holds N * HB * NM * 4 values.  Half-row pairs keep the rows one FFT block needs together.
+__host__ __device__ __forceinline__ size_t four_off(int n, int c, int p, int h, int NM, int HB) {
+  return ((((size_t)n * HB + (h >> 1)) * NM + c) * 2 + p) * 2 + (h & 1);
+}
+
 struct SynthGroup {
   int kind;
   const cplx* in[3];   // spectral inputs [n][H]
@@ -61,6 +67,7 @@ struct AnalGroup {
 struct lsd_ctx {
   lsd_config cfg;
   int L, M, Mp, N, KL, H, Th, Th2, Ph, Ma, Hc, Hr, NM, P2;
+  int HB = 0;                // theta-Fourier half-row pairs, ceil(Th2 / 2)
   int dev = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -73,7 +80,7 @@ struct lsd_ctx {
   std::vector<int> hl, hm, hs, thm, mcount, mstart, mlen;
   // device layout
   int *d_l = nullptr, *d_m = nullptr, *d_s = nullptr, *d_mc = nullptr;
-  int *d_mstart = nullptr, *d_mlen = nullptr, *d_thm = nullptr, *d_lm2nh = nullptr;
+  int *d_mstart = nullptr, *d_mlen = nullptr, *d_thm = nullptr, *d_lm2nh = nullptr, *d_bin2c = nullptr;
   int *d_aperm = nullptr;  // [Hc][Hr] analysis thread order
   int *d_sblk_l = nullptr, *d_sblk_nh = nullptr;  // solve blocks: degree, [16] harmonics
   int nsblk = 0;
@@ -83,8 +90,7 @@ struct lsd_ctx {
   // FFT twiddles
   double2 *d_tw2 = nullptr;  // e^{+2 pi i k / P2}, k < P2
   double2 *d_twh = nullptr;  // e^{+2 pi i k / Ph}, k < Ph
-  int nrad = 0;
-  int radices[16];
+  int fftG = 1, fftE = 1;     // phi FFT: P2 = fftE * fftG (lanes x registers)
   // radial mesh
   double *d_r = nullptr;       // [7][N]: r^p, p = -3..3
   double *d_dr = nullptr;      // [KL][N][2KL+1] bands (column-major per band, like Fortran)
@@ -138,6 +144,7 @@ int lsd_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups);
 int lsd_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups);
 int lsd_launch_c2r(lsd_ctx* ctx, const cplx* four, double* phys, int nfields);
 int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields);
+bool lsd_fft_plan(lsd_ctx* c);
 int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out);
 // ---- spectral algebra and solves (lsd_solve.cu) ----
 int lsd_eval(lsd_ctx* ctx);            // one nonlinear evaluation (device)
@@ -152,16 +159,8 @@ int lsd_solve_batch(lsd_ctx* ctx, int n, int kl, int nmat, const double* d_ab, c
 
 int lsd_umma_selftest(lsd_ctx* ctx, double* maxerr);
 // ---- tensor-core (Ozaki) Legendre path (lsd_ozaki.cu) ----
-struct OzSynthGroupH { const cplx* in0; const cplx* in1; cplx* out0; cplx* out1; const int* e0; const int* e1; };
-struct OzAnalGroupH { const cplx* in0; const cplx* in1; cplx* out0; cplx* out1; const int* e0; const int* e1; int zero_m0_im; };
-enum { OZS_VEC = 0, OZS_P = 1, OZS_GRAD = 2, OZA_ST = 3, OZA_Q = 4 };
 int lsd_ozaki_setup(lsd_ctx* ctx);
 void lsd_ozaki_free(lsd_ctx* ctx);
-int lsd_ozaki_exp_spec(lsd_ctx* ctx, const cplx* in, const double* rinv, int slot);
-int lsd_ozaki_exp_four(lsd_ctx* ctx, const cplx* in, int slot);
-const int* lsd_ozaki_exp(lsd_ctx* ctx, int slot);
-int lsd_ozaki_synth(lsd_ctx* ctx, int type, const OzSynthGroupH* g, int ng);
-int lsd_ozaki_anal(lsd_ctx* ctx, int type, const OzAnalGroupH* g, int ng);
 int lsd_ozaki_check(lsd_ctx* ctx);
 int* lsd_ozaki_err_flag(lsd_ctx* ctx);
 int lsd_ozaki_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups);

@@ -5,210 +5,176 @@
 //  * synthesis (c2r, unnormalised): bins 0..M-1 come from the m-counter map var_Th%m,
 //    bins M..Ph/2 are zero, the imaginary part of bin 0 is ignored;
 //  * analysis (r2c): input scaled by 1/Ph first, bins 0..M-1 kept, bin 0 exactly real.
-// A real transform of length Ph = 2*P2 is done as one complex FFT of length P2 of the
-// even/odd-interleaved samples z[t] = x[2t] + i x[2t+1], with the usual split
-// pre-/post-processing.  The complex FFT is a shared-memory Stockham autosort with
-// radix-4/2/3 passes; P2 = 3M/2 = 3^a 2^b for every supported M.
+// A real row of length Ph = 2 P2 is transformed as one complex FFT of length P2 of the
+// interleaved samples z[t] = x[2t] + i x[2t+1], with the usual split pre-/post-processing.
 //
-// The fused kernel (one CTA per shell n and TJ theta rows) reads the 15 synthesised
-// theta-Fourier rows of u, curl u, B, curl B and grad C, transforms them, forms
+// Each complex FFT of length P2 = E G (G a power of two <= 32) runs in the registers of
+// G lanes: lane l holds E values.  The inverse is a lane-parallel radix-2 DIF over the G
+// lanes (shuffles), a twiddle w^(g k1) and an E-point DFT in registers; the forward
+// transform is its mirror (E-point DFT, twiddle, radix-2 DIT over the lanes).  Physical
+// samples come out of the inverse in a lane-permuted order and the forward transform
+// takes them back in that order, so the point-wise products never need a reordering.
+// Every shuffle runs with all 32 lanes of the warp: task loops advance warp by warp and
+// lanes without a task compute a dummy row whose results are dropped.
+//
+// The theta-Fourier rows are stored in half-row pairs ([n][h/2][m-counter][E/O][h%2],
+// four_off); one CTA of the fused kernel owns one pair (four full theta rows: the
+// southern and northern row of each half-row), reads the 15 synthesised fields of u,
+// curl u, B, curl B and grad C as contiguous 8 KB blocks, transforms them, forms
 //   u x (curl u) + Coriolis + Lorentz      (nonlinear.F90:70-146, Boussinesq)
 //   -(Pr/Pm) u . grad C                     (nonlinear.F90:269-272)
 //   u x B                                   (nonlinear.F90:421-430)
 // at every grid point in shared memory, transforms the 7 results back and writes their
-// theta-Fourier rows.  Physical-space fields never touch HBM.
+// folded theta-Fourier rows.  Physical-space fields never touch HBM.
+#include <type_traits>
+
 #include "lsd_common.cuh"
 
 namespace {
 
+constexpr unsigned FULL = 0xffffffffu;
+
 struct FFTPlanDev {
-  int P2, Ph, M, NM, Th, Th2, nrad;
-  int rad[16];
-  const double2* tw2;  // e^{+2 pi i k/P2}
-  const double2* twh;  // e^{+2 pi i k/Ph}
+  int P2, Ph, M, NM, Th, Th2, HB, G, lgG;
+  const double2* tw2;  // e^{+2 pi i k/P2}, k < P2
+  const double2* twh;  // e^{+2 pi i k/Ph}, k < Ph
   const int* thm;      // m-counter -> bin
+  const int* bin2c;    // bin b < M -> m-counter
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
 __device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 sub2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 shfl_xor2(double2 v, int m) {
+  return make_double2(__shfl_xor_sync(FULL, v.x, m), __shfl_xor_sync(FULL, v.y, m));
+}
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+  return make_double2(__shfl_sync(FULL, v.x, src), __shfl_sync(FULL, v.y, src));
+}
+__device__ __forceinline__ int brev_bits(int l, int bits) {
+  return bits ? (int)(__brev((unsigned)l) >> (32 - bits)) : 0;
+}
 
-// In-place (ping-pong) Stockham FFT of nrows rows of length P stored contiguously in a
-// (row stride P).  sign = +1: e^{+i...} (inverse, unnormalised), -1: forward.
-// Returns the buffer holding the result.  All threads of the block must call it.
-__device__ double2* block_fft(double2* a, double2* b, int nrows, const FFTPlanDev& pl, int sign) {
-  const int P = pl.P2;
-  int Ns = 1;
-  for (int pass = 0; pass < pl.nrad; ++pass) {
-    const int R = pl.rad[pass];
-    const int PR = P / R;
-    const int tstep = P / (Ns * R);
-    const int total = nrows * PR;
-    for (int g = threadIdx.x; g < total; g += blockDim.x) {
-      const int row = g / PR, t = g - row * PR;
-      const int k = t % Ns;
-      const double2* src = a + (size_t)row * P;
-      double2 v[4];
+// Inverse (e^{+i}) FFT of length E*G.  In: v[k1] = Z[k1 + E l].  Out: v[e] = x[brev(l) + G e].
+template <int E>
+__device__ __forceinline__ void wfft_inv(double2 (&v)[E], int l, const FFTPlanDev& pl) {
+  const int G = pl.G;
+  for (int h = G >> 1; h >= 1; h >>= 1) {  // radix-2 DIF over the lanes (natural -> bit-reversed)
+    const bool up = l & h;
+    const double2 w = __ldg(&pl.tw2[E * (l & (h - 1)) * (G / (2 * h))]);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (q < R) {
-          double2 x = src[t + q * PR];
-          if (q > 0) {
-            double2 w = pl.tw2[(q * k * tstep) % P];
-            if (sign < 0) w.y = -w.y;
-            x = cmul(x, w);
-          }
-          v[q] = x;
-        }
-      }
-      double2 o[4];
-      if (R == 2) {
-        o[0] = make_double2(v[0].x + v[1].x, v[0].y + v[1].y);
-        o[1] = make_double2(v[0].x - v[1].x, v[0].y - v[1].y);
-      } else if (R == 4) {
-        double2 s02 = make_double2(v[0].x + v[2].x, v[0].y + v[2].y);
-        double2 d02 = make_double2(v[0].x - v[2].x, v[0].y - v[2].y);
-        double2 s13 = make_double2(v[1].x + v[3].x, v[1].y + v[3].y);
-        double2 d13 = make_double2(v[1].x - v[3].x, v[1].y - v[3].y);
-        // i*sign*d13
-        double2 jd13 = sign > 0 ? make_double2(-d13.y, d13.x) : make_double2(d13.y, -d13.x);
-        o[0] = make_double2(s02.x + s13.x, s02.y + s13.y);
-        o[1] = make_double2(d02.x + jd13.x, d02.y + jd13.y);
-        o[2] = make_double2(s02.x - s13.x, s02.y - s13.y);
-        o[3] = make_double2(d02.x - jd13.x, d02.y - jd13.y);
-      } else {  // R == 3
-        const double h = 0.86602540378443864676;  // sqrt(3)/2
-        double2 t1 = make_double2(v[1].x + v[2].x, v[1].y + v[2].y);
-        double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-        double2 t3 = make_double2(sign * h * (v[1].x - v[2].x), sign * h * (v[1].y - v[2].y));
-        o[0] = make_double2(v[0].x + t1.x, v[0].y + t1.y);
-        o[1] = make_double2(t2.x - t3.y, t2.y + t3.x);  // t2 + i t3
-        o[2] = make_double2(t2.x + t3.y, t2.y - t3.x);  // t2 - i t3
-      }
-      double2* dst = b + (size_t)row * P;
-      const int base = (t / Ns) * Ns * R + k;
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (q < R) dst[base + q * Ns] = o[q];
+    for (int k = 0; k < E; ++k) {
+      const double2 p = shfl_xor2(v[k], h);
+      v[k] = up ? cmul(sub2(p, v[k]), w) : add2(v[k], p);
     }
-    __syncthreads();
-    double2* tmp = a; a = b; b = tmp;
-    Ns *= R;
   }
-  return a;
+  const int g = brev_bits(l, pl.lgG);
+#pragma unroll
+  for (int k = 1; k < E; ++k) v[k] = cmul(v[k], __ldg(&pl.tw2[g * k]));
+  double2 x[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {  // E-point DFT in registers, w_E = w_P2^G
+    double2 s = v[0];
+#pragma unroll
+    for (int k = 1; k < E; ++k) s = add2(s, cmul(v[k], __ldg(&pl.tw2[G * ((e * k) % E)])));
+    x[e] = s;
+  }
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = x[e];
 }
 
-// Pack the Hermitian half-spectrum Y (bins 0..M-1, rest zero) of one row into the
-// half-length complex array Z whose inverse FFT gives z[t] = x[2t] + i x[2t+1].
-// Y is read through a lambda ybin(b) returning bin b (b < M) or 0.
-template <class YF>
-__device__ __forceinline__ double2 c2r_pack(int k, const FFTPlanDev& pl, YF ybin) {
-  const int P2 = pl.P2;
-  double2 yk = ybin(k);
-  double2 yc = conj2(ybin(k == 0 ? P2 : P2 - k));  // conj(Y[P2-k]); Y[P2] = Nyquist = 0
-  if (k == 0) yk.y = 0.0;                           // DC imaginary ignored
-  double2 s = make_double2(yk.x + yc.x, yk.y + yc.y);
-  double2 d = make_double2(yk.x - yc.x, yk.y - yc.y);
-  double2 w = pl.twh[k];                            // e^{+2 pi i k/Ph}
-  double2 wd = cmul(w, d);
-  return make_double2(s.x - wd.y, s.y + wd.x);      // s + i*w*d
+// Forward (e^{-i}) FFT, the mirror of wfft_inv.  In: v[e] = x[brev(l) + G e].
+// Out: v[k1] = X[k1 + E l].
+template <int E>
+__device__ __forceinline__ void wfft_fwd(double2 (&v)[E], int l, const FFTPlanDev& pl) {
+  const int G = pl.G;
+  double2 u[E];
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    double2 s = v[0];
+#pragma unroll
+    for (int e = 1; e < E; ++e) s = add2(s, cmulc(v[e], __ldg(&pl.tw2[G * ((e * k) % E)])));
+    u[k] = s;
+  }
+  const int g = brev_bits(l, pl.lgG);
+#pragma unroll
+  for (int k = 0; k < E; ++k) v[k] = k ? cmulc(u[k], __ldg(&pl.tw2[g * k])) : u[0];
+  for (int h = 1; h < G; h <<= 1) {  // radix-2 DIT over the lanes (bit-reversed -> natural)
+    const bool up = l & h;
+    const double2 w = __ldg(&pl.tw2[E * (l & (h - 1)) * (G / (2 * h))]);
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      const double2 send = up ? cmulc(v[k], w) : v[k];
+      const double2 recv = shfl_xor2(send, h);
+      v[k] = up ? sub2(recv, send) : add2(send, recv);
+    }
+  }
 }
 
-// From Z = FFT_-(z), bin k < M of the real spectrum (k < P2)
-__device__ __forceinline__ double2 r2c_unpack(int k, const double2* Z, const FFTPlanDev& pl) {
-  const int P2 = pl.P2;
-  double2 zk = Z[k];
-  double2 zc = conj2(Z[k == 0 ? 0 : P2 - k]);
+// Half-spectrum packing for the c2r: Z[k] from Y[k] and conj(Y[P2-k]) (Y[P2] = Nyquist = 0;
+// the imaginary part of the DC bin is ignored).
+__device__ __forceinline__ double2 c2r_pack(int k, double2 yk, double2 ymk, const FFTPlanDev& pl) {
+  const double2 yc = conj2(ymk);
+  if (k == 0) yk.y = 0.0;
+  const double2 s = add2(yk, yc), d = sub2(yk, yc);
+  const double2 wd = cmul(__ldg(&pl.twh[k]), d);
+  return make_double2(s.x - wd.y, s.y + wd.x);  // s + i w d
+}
+// Bin k < P2 of the real spectrum from Z[k] and Z[P2-k] (Z[0] for k = 0).
+__device__ __forceinline__ double2 r2c_unpack(int k, double2 zk, double2 zmk, const FFTPlanDev& pl) {
   if (k == 0) return make_double2(zk.x + zk.y, 0.0);
-  double2 A = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
-  double2 Bi = make_double2(0.5 * (zk.x - zc.x), 0.5 * (zk.y - zc.y));  // (Z - conj Z')/2 = i B
-  double2 B = make_double2(Bi.y, -Bi.x);                                 // divide by i
-  double2 w = conj2(pl.twh[k]);                                          // e^{-2 pi i k/Ph}
-  double2 wb = cmul(w, B);
-  return make_double2(A.x + wb.x, A.y + wb.y);
+  const double2 zc = conj2(zmk);
+  const double2 A = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+  const double2 Bi = make_double2(0.5 * (zk.x - zc.x), 0.5 * (zk.y - zc.y));  // i B
+  const double2 B = make_double2(Bi.y, -Bi.x);
+  return add2(A, cmulc(B, __ldg(&pl.twh[k])));
 }
 
-// The theta-Fourier arrays hold the even/odd half-grid sums of the reference's
-// Legendre loops, [f][n][m-counter][p][Th2] with p = 0 (E) and 1 (O): a southern row
-// h < Th2 is E + O, its northern mirror Th-1-h is E - O.  A CTA therefore owns TH
-// half-rows h and transforms both full rows of each (row 2hh: south, 2hh+1: north);
-// for odd Th the equator row is its own mirror and is written once.
+// theta row of half-row h on side 0 (south) / 1 (north)
 __device__ __forceinline__ int row_theta(int h, int side, int Th) { return side ? Th - 1 - h : h; }
 
-// ---- standalone c2r: theta-Fourier -> phys [f][n][Ph][Th] -------------------------------
-__global__ void k_c2r(FFTPlanDev pl, int N, const cplx* four, double* phys, int TH) {
-  extern __shared__ double2 sm[];
-  const int f = blockIdx.z, n = blockIdx.y, h0 = blockIdx.x * TH;
-  const int P2 = pl.P2, Th = pl.Th, Th2 = pl.Th2, M = pl.M;
-  const int th = min(TH, Th2 - h0);
-  const int rows = 2 * th;
-  double2* A = sm;
-  double2* B = sm + (size_t)2 * TH * P2;
-  double2* Ybuf = B;  // bins staged in B first: [row][M]
-  const cplx* src = four + ((size_t)f * N + n) * pl.NM * 2 * Th2;
-  for (int i = threadIdx.x; i < pl.NM * th; i += blockDim.x) {
-    int c = i / th, hh = i % th;
-    double2 e = src[((size_t)c * 2 + 0) * Th2 + h0 + hh], o = src[((size_t)c * 2 + 1) * Th2 + h0 + hh];
-    int b = pl.thm[c];
-    Ybuf[(2 * hh + 0) * M + b] = make_double2(e.x + o.x, e.y + o.y);
-    Ybuf[(2 * hh + 1) * M + b] = make_double2(e.x - o.x, e.y - o.y);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < rows * P2; i += blockDim.x) {
-    int r = i / P2, k = i % P2;
-    const double2* Y = Ybuf + r * M;
-    A[r * P2 + k] = c2r_pack(k, pl, [&](int b) { return b < M ? Y[b] : make_double2(0.0, 0.0); });
-  }
-  __syncthreads();
-  double2* R = block_fft(A, B, rows, pl, +1);
-  double* dst = phys + ((size_t)f * N + n) * (size_t)pl.Ph * Th;
-  for (int i = threadIdx.x; i < rows * P2; i += blockDim.x) {
-    int t = i / rows, r = i % rows;
-    int hh = r >> 1, side = r & 1, h = h0 + hh;
-    int j = row_theta(h, side, Th);
-    if (side && j == h) continue;
-    double2 z = R[r * P2 + t];
-    dst[(size_t)(2 * t) * Th + j] = z.x;
-    dst[(size_t)(2 * t + 1) * Th + j] = z.y;
-  }
+// Spectrum Y[b] of one full theta row from the folded rows of counter bin2c[b] in a
+// half-row-pair block: south E + O, north E - O.
+__device__ __forceinline__ double2 row_bin(const cplx* blk, int b, int jj, int side, const FFTPlanDev& pl) {
+  if (b >= pl.M) return make_double2(0.0, 0.0);
+  const int c = __ldg(&pl.bin2c[b]);
+  const double2 e = __ldg(&blk[(c * 2 + 0) * 2 + jj]), o = __ldg(&blk[(c * 2 + 1) * 2 + jj]);
+  return side ? sub2(e, o) : add2(e, o);
 }
 
-// fold two transformed rows (south, north) of half-row h into E and O bins
-__device__ __forceinline__ void fold_store(cplx* dst, int c, int Th2, int h, double2 xs, double2 xn, bool equator) {
-  double2 e = make_double2(xs.x + xn.x, xs.y + xn.y);
-  double2 o = make_double2(xs.x - xn.x, xs.y - xn.y);
-  if (equator) { e.x *= 0.5; e.y *= 0.5; }  // odd Th: the equator row is counted once
-  dst[((size_t)c * 2 + 0) * Th2 + h] = e;
-  dst[((size_t)c * 2 + 1) * Th2 + h] = o;
+// Load + pack + inverse FFT of one row; blk = the (n, h/2) block of one field.
+template <int E>
+__device__ __forceinline__ void row_c2r(double2 (&v)[E], const cplx* blk, int jj, int side, int l, const FFTPlanDev& pl) {
+  const int P2 = pl.P2;
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) {
+    const int k = k1 + E * l;
+    v[k1] = c2r_pack(k, row_bin(blk, k, jj, side, pl), row_bin(blk, k == 0 ? P2 : P2 - k, jj, side, pl), pl);
+  }
+  wfft_inv<E>(v, l, pl);
 }
 
-// ---- standalone r2c: phys [f][n][Ph][Th] -> theta-Fourier (folded E/O) ---------------------
-__global__ void k_r2c(FFTPlanDev pl, int N, const double* phys, cplx* four, int TH) {
-  extern __shared__ double2 sm[];
-  const int f = blockIdx.z, n = blockIdx.y, h0 = blockIdx.x * TH;
-  const int P2 = pl.P2, Th = pl.Th, Th2 = pl.Th2;
-  const int th = min(TH, Th2 - h0);
-  const int rows = 2 * th;
-  double2* A = sm;
-  double2* B = sm + (size_t)2 * TH * P2;
-  const double* src = phys + ((size_t)f * N + n) * (size_t)pl.Ph * Th;
-  const double scale = 1.0 / (double)pl.Ph;
-  for (int i = threadIdx.x; i < rows * P2; i += blockDim.x) {
-    int t = i / rows, r = i % rows;
-    int j = row_theta(h0 + (r >> 1), r & 1, Th);
-    A[r * P2 + t] = make_double2(src[(size_t)(2 * t) * Th + j] * scale, src[(size_t)(2 * t + 1) * Th + j] * scale);
+// Forward FFT of one row of physical samples (lane order) + unpack of bins b = k1 + E l.
+// The partner Z[P2 - k] lives in lane (G - l) % G (k1 = 0) or G - 1 - l (register E - k1).
+template <int E>
+__device__ __forceinline__ void row_r2c(double2 (&v)[E], int l, int lane0, const FFTPlanDev& pl) {
+  const int G = pl.G;
+  wfft_fwd<E>(v, l, pl);
+  double2 out[E];
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) {
+    const int src = k1 == 0 ? (G - l) % G : G - 1 - l;
+    const double2 zm = shfl2(v[k1 == 0 ? 0 : E - k1], lane0 + src);
+    out[k1] = r2c_unpack(k1 + E * l, v[k1], zm, pl);
   }
-  __syncthreads();
-  double2* R = block_fft(A, B, rows, pl, -1);
-  cplx* dst = four + ((size_t)f * N + n) * pl.NM * 2 * Th2;
-  for (int i = threadIdx.x; i < pl.NM * th; i += blockDim.x) {
-    int c = i / th, hh = i % th, h = h0 + hh;
-    int b = pl.thm[c];
-    double2 xs = r2c_unpack(b, R + (size_t)(2 * hh) * P2, pl);
-    double2 xn = r2c_unpack(b, R + (size_t)(2 * hh + 1) * P2, pl);
-    fold_store(dst, c, Th2, h, xs, xn, (Th & 1) && h == Th2 - 1);
-  }
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) v[k1] = out[k1];
 }
 
 // ---- fused: 15 theta-Fourier inputs -> products -> 7 theta-Fourier outputs -------------
@@ -220,52 +186,57 @@ struct ProdConst {
 
 constexpr int NF_IN = 15, NF_OUT = 7;
 
-__global__ void k_products(FFTPlanDev pl, int N, ProdConst pc, const cplx* four_in, cplx* four_out, int TH) {
-  extern __shared__ double2 sm[];
-  const int n = blockIdx.y, h0 = blockIdx.x * TH;
-  const int P2 = pl.P2, Th = pl.Th, Th2 = pl.Th2, M = pl.M, NM = pl.NM;
-  const int th = min(TH, Th2 - h0);
-  const int rpf = 2 * th;            // rows per field
-  const int rows = NF_IN * rpf;
-  double2* A = sm;
-  double2* B = sm + (size_t)NF_IN * 2 * TH * P2;
-  const size_t fstride = (size_t)N * NM * 2 * Th2;
-  // stage bins into B as [row][M], row = f*rpf + 2*hh + side
-  for (int i = threadIdx.x; i < NF_IN * NM * th; i += blockDim.x) {
-    int hh = i % th, rem = i / th, c = rem % NM, f = rem / NM;
-    const cplx* src = four_in + f * fstride + ((size_t)n * NM + c) * 2 * Th2 + h0 + hh;
-    double2 e = src[0], o = src[Th2];
-    int b = pl.thm[c];
-    B[(f * rpf + 2 * hh + 0) * M + b] = make_double2(e.x + o.x, e.y + o.y);
-    B[(f * rpf + 2 * hh + 1) * M + b] = make_double2(e.x - o.x, e.y - o.y);
+// grid (HB or 2 HB, N); RPC = 4 rows (both half-rows of the pair) or 2 (one half-row,
+// blockIdx.x = h, for long rows).  smem: [NF_IN][RPC][P2] double2.
+template <int E>
+__global__ void __launch_bounds__(512) k_products(FFTPlanDev pl, int N, ProdConst pc, const cplx* four_in,
+                                                  cplx* four_out, int RPC) {
+  extern __shared__ double2 phys[];
+  const int n = blockIdx.y;
+  const int hb = RPC == 4 ? blockIdx.x : blockIdx.x >> 1;
+  const int jj0 = RPC == 4 ? 0 : (blockIdx.x & 1);
+  const int P2 = pl.P2, G = pl.G, NM = pl.NM, Th = pl.Th, Th2 = pl.Th2;
+  const size_t fstride = (size_t)N * pl.HB * NM * 4;
+  const size_t boff = ((size_t)n * pl.HB + hb) * NM * 4;  // the CTA's block in every field
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int sgw = 32 / G, l = lane % G, lane0 = lane - l;
+  // ---- inverse transforms: task = (field, row), G lanes per task
+  for (int t0 = warp * sgw; t0 < NF_IN * RPC; t0 += nw * sgw) {
+    const int t = t0 + lane / G;
+    const int tt = t < NF_IN * RPC ? t : t0;  // lanes without a task redo a valid one
+    const int f = tt / RPC, r = tt % RPC;
+    const int jj = jj0 + (r >> 1), side = r & 1;
+    const bool act = t < NF_IN * RPC && 2 * hb + jj < Th2;
+    double2 v[E];
+    row_c2r<E>(v, four_in + f * fstride + boff, jj, side, l, pl);
+    if (act) {
+      double2* dst = phys + ((size_t)f * RPC + r) * P2;
+#pragma unroll
+      for (int e = 0; e < E; ++e) dst[e * G + l] = v[e];
+    }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < rows * P2; i += blockDim.x) {
-    int row = i / P2, k = i % P2;
-    const double2* Y = B + (size_t)row * M;
-    A[(size_t)row * P2 + k] = c2r_pack(k, pl, [&](int b) { return b < M ? Y[b] : make_double2(0.0, 0.0); });
-  }
-  __syncthreads();
-  double2* X = block_fft(A, B, rows, pl, +1);
-  double2* W = (X == A) ? B : A;  // the other buffer receives the products
-  // products at every point (row r, sample t, part re/im)
-  for (int i = threadIdx.x; i < rpf * P2; i += blockDim.x) {
-    int r = i / P2, t = i % P2;
-    int j = row_theta(h0 + (r >> 1), r & 1, Th);
-    double sn = pc.sn[j], cs = pc.gp[j];
+  // ---- products at every point (row r, position i, part re/im), in place into slots 0..6
+  const double scale = 1.0 / (double)pl.Ph;
+  for (int i = threadIdx.x; i < RPC * P2; i += blockDim.x) {
+    const int r = i / P2, pos = i - r * P2;
+    const int h = 2 * hb + jj0 + (r >> 1);
+    if (h >= Th2) continue;
+    const int j = row_theta(h, r & 1, Th);
+    const double sn = pc.sn[j], cs = pc.gp[j];
     double2 v[NF_IN];
 #pragma unroll
-    for (int f = 0; f < NF_IN; ++f) v[f] = X[(size_t)(f * rpf + r) * P2 + t];
+    for (int f = 0; f < NF_IN; ++f) v[f] = phys[((size_t)f * RPC + r) * P2 + pos];
     double2 out[NF_OUT];
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
-#define G(f) (part == 0 ? v[f].x : v[f].y)
-      double vr = G(0), vt = G(1), vp = G(2);
-      double wr = G(3), wt = G(4), wp = G(5);
-      double br = G(6), bt = G(7), bp = G(8);
-      double jr = G(9), jt = G(10), jp = G(11);
-      double cr = G(12), ct = G(13), cp = G(14);
-#undef G
+#define G_(f) (part == 0 ? v[f].x : v[f].y)
+      const double vr = G_(0), vt = G_(1), vp = G_(2);
+      const double wr = G_(3), wt = G_(4), wp = G_(5);
+      const double br = G_(6), bt = G_(7), bp = G_(8);
+      const double jr = G_(9), jt = G_(10), jp = G_(11);
+      const double cr = G_(12), ct = G_(13), cp = G_(14);
+#undef G_
       double a = vt * wp - vp * wt;
       double b = vp * wr - vr * wp;
       double c = vr * wt - vt * wr;
@@ -275,59 +246,164 @@ __global__ void k_products(FFTPlanDev pl, int N, ProdConst pc, const cplx* four_
       a = a + pc.Cmag * (jt * bp - jp * bt);
       b = b + pc.Cmag * (jp * br - jr * bp);
       c = c + pc.Cmag * (jr * bt - jt * br);
-      double e0 = vt * bp - vp * bt;
-      double e1 = vp * br - vr * bp;
-      double e2 = vr * bt - vt * br;
-      double cod = -pc.d_qm1 * vr * cr - pc.d_qm1 * vt * ct - pc.d_qm1 * vp * cp;
-      double o[NF_OUT] = {a, b, c, e0, e1, e2, cod};
+      const double e0 = vt * bp - vp * bt;
+      const double e1 = vp * br - vr * bp;
+      const double e2 = vr * bt - vt * br;
+      const double cod = -pc.d_qm1 * vr * cr - pc.d_qm1 * vt * ct - pc.d_qm1 * vp * cp;
+      const double o[NF_OUT] = {a, b, c, e0, e1, e2, cod};
 #pragma unroll
       for (int q = 0; q < NF_OUT; ++q) {
-        if (part == 0) out[q].x = o[q]; else out[q].y = o[q];
+        if (part == 0) out[q].x = o[q] * scale; else out[q].y = o[q] * scale;
       }
     }
-    const double scale = 1.0 / (double)pl.Ph;
 #pragma unroll
-    for (int q = 0; q < NF_OUT; ++q)
-      W[(size_t)(q * rpf + r) * P2 + t] = make_double2(out[q].x * scale, out[q].y * scale);
+    for (int q = 0; q < NF_OUT; ++q) phys[((size_t)q * RPC + r) * P2 + pos] = out[q];
   }
   __syncthreads();
-  double2* Z = block_fft(W, X, NF_OUT * rpf, pl, -1);
-  for (int i = threadIdx.x; i < NF_OUT * NM * th; i += blockDim.x) {
-    int hh = i % th, rem = i / th, c = rem % NM, q = rem / NM;
-    int h = h0 + hh, b = pl.thm[c];
-    double2 xs = r2c_unpack(b, Z + (size_t)(q * rpf + 2 * hh) * P2, pl);
-    double2 xn = r2c_unpack(b, Z + (size_t)(q * rpf + 2 * hh + 1) * P2, pl);
-    fold_store(four_out + q * fstride + (size_t)n * NM * 2 * Th2, c, Th2, h, xs, xn, (Th & 1) && h == Th2 - 1);
+  // ---- forward transforms: task = (output, row); bins b < M back into the row's slot
+  for (int t0 = warp * sgw; t0 < NF_OUT * RPC; t0 += nw * sgw) {
+    const int t = t0 + lane / G;
+    const int tt = t < NF_OUT * RPC ? t : t0;
+    const int q = tt / RPC, r = tt % RPC;
+    const bool act = t < NF_OUT * RPC && 2 * hb + jj0 + (r >> 1) < Th2;
+    double2* slot = phys + ((size_t)q * RPC + r) * P2;
+    double2 v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = slot[e * G + l];
+    row_r2c<E>(v, l, lane0, pl);
+    __syncwarp();
+    if (act) {
+#pragma unroll
+      for (int k1 = 0; k1 < E; ++k1) {
+        const int b = k1 + E * l;
+        if (b < pl.M) slot[b] = v[k1];
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // ---- fold south/north into E/O and store the output blocks (contiguous per field)
+  const int njj = RPC / 2;
+  for (int i = threadIdx.x; i < NF_OUT * NM * 2 * njj; i += blockDim.x) {
+    const int q = i / (NM * 2 * njj), rem = i % (NM * 2 * njj);
+    const int c = rem / (2 * njj), p = (rem / njj) % 2, jr = rem % njj;
+    const int jj = jj0 + jr, h = 2 * hb + jj;
+    if (h >= Th2) continue;
+    const int b = pl.thm[c];
+    const double2 xs = phys[((size_t)q * RPC + 2 * jr) * P2 + b];
+    const double2 xn = phys[((size_t)q * RPC + 2 * jr + 1) * P2 + b];
+    double2 val = p == 0 ? add2(xs, xn) : sub2(xs, xn);
+    if (p == 0 && (Th & 1) && h == Th2 - 1) { val.x *= 0.5; val.y *= 0.5; }  // odd Th: equator once
+    four_out[q * fstride + boff + (c * 2 + p) * 2 + jj] = val;
+  }
+}
+
+// ---- standalone c2r: theta-Fourier -> phys [f][n][Ph][Th] -------------------------------
+// grid (Th2, N, nfields), 64 threads: the two theta rows of half-row h, G lanes each.
+template <int E>
+__global__ void __launch_bounds__(64) k_c2r(FFTPlanDev pl, int N, const cplx* four, double* phys) {
+  const int h = blockIdx.x, n = blockIdx.y, f = blockIdx.z;
+  const int G = pl.G, Th = pl.Th;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int l = lane % G;
+  const int grp = warp * (32 / G) + lane / G;  // groups 0, 1 take the rows; others redo row 0
+  const int side = grp & 1;
+  const cplx* blk = four + (((size_t)f * N + n) * pl.HB + (h >> 1)) * pl.NM * 4;
+  double2 v[E];
+  row_c2r<E>(v, blk, h & 1, side, l, pl);
+  const int j = row_theta(h, side, Th);
+  if (grp > 1 || (side && j == h)) return;  // odd Th: the equator row is written once
+  double* dst = phys + ((size_t)f * N + n) * (size_t)pl.Ph * Th;
+  const int g = brev_bits(l, pl.lgG);
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int t = g + G * e;
+    dst[(size_t)(2 * t) * Th + j] = v[e].x;
+    dst[(size_t)(2 * t + 1) * Th + j] = v[e].y;
+  }
+}
+
+// ---- standalone r2c: phys [f][n][Ph][Th] -> folded theta-Fourier --------------------------
+template <int E>
+__global__ void __launch_bounds__(64) k_r2c(FFTPlanDev pl, int N, const double* phys, cplx* four) {
+  __shared__ double2 bins[2][512];
+  const int h = blockIdx.x, n = blockIdx.y, f = blockIdx.z;
+  const int G = pl.G, Th = pl.Th, Th2 = pl.Th2, M = pl.M;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int l = lane % G, lane0 = lane - l;
+  const int grp = warp * (32 / G) + lane / G;
+  const int side = grp & 1;
+  const double scale = 1.0 / (double)pl.Ph;
+  const int j = row_theta(h, side, Th);
+  const double* src = phys + ((size_t)f * N + n) * (size_t)pl.Ph * Th;
+  const int g = brev_bits(l, pl.lgG);
+  double2 v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int t = g + G * e;
+    v[e] = make_double2(src[(size_t)(2 * t) * Th + j] * scale, src[(size_t)(2 * t + 1) * Th + j] * scale);
+  }
+  row_r2c<E>(v, l, lane0, pl);
+  if (grp <= 1) {
+#pragma unroll
+    for (int k1 = 0; k1 < E; ++k1) {
+      const int b = k1 + E * l;
+      if (b < M) bins[side][b] = v[k1];
+    }
+  }
+  __syncthreads();
+  cplx* blk = four + (((size_t)f * N + n) * pl.HB + (h >> 1)) * pl.NM * 4;
+  for (int i = threadIdx.x; i < pl.NM * 2; i += blockDim.x) {
+    const int c = i >> 1, p = i & 1, b = pl.thm[c];
+    double2 val = p == 0 ? add2(bins[0][b], bins[1][b]) : sub2(bins[0][b], bins[1][b]);
+    if (p == 0 && (Th & 1) && h == Th2 - 1) { val.x *= 0.5; val.y *= 0.5; }
+    blk[(c * 2 + p) * 2 + (h & 1)] = val;
   }
 }
 
 FFTPlanDev make_plan(lsd_ctx* ctx) {
   FFTPlanDev pl;
   pl.P2 = ctx->P2; pl.Ph = ctx->Ph; pl.M = ctx->M; pl.NM = ctx->NM; pl.Th = ctx->Th; pl.Th2 = ctx->Th2;
-  pl.nrad = ctx->nrad;
-  for (int i = 0; i < 16; ++i) pl.rad[i] = ctx->radices[i];
-  pl.tw2 = ctx->d_tw2; pl.twh = ctx->d_twh; pl.thm = ctx->d_thm;
+  pl.HB = ctx->HB; pl.G = ctx->fftG; pl.lgG = 0;
+  while ((1 << pl.lgG) < pl.G) ++pl.lgG;
+  pl.tw2 = ctx->d_tw2; pl.twh = ctx->d_twh; pl.thm = ctx->d_thm; pl.bin2c = ctx->d_bin2c;
   return pl;
 }
 
-int pick_tj(int rows_per_j, int P2, size_t budget) {  // half-rows per CTA (2 full rows each)
-  size_t per = (size_t)2 * 2 * rows_per_j * P2 * sizeof(double2);
-  int tj = (int)(budget / per);
-  if (tj > 16) tj = 16;
-  return tj < 1 ? 0 : tj;
+template <class F>
+int dispatch_E(int E, F&& f) {
+  switch (E) {
+    case 3: return f(std::integral_constant<int, 3>());
+    case 6: return f(std::integral_constant<int, 6>());
+    case 9: return f(std::integral_constant<int, 9>());
+    case 12: return f(std::integral_constant<int, 12>());
+    case 18: return f(std::integral_constant<int, 18>());
+    case 24: return f(std::integral_constant<int, 24>());
+  }
+  return -1;
 }
 
 }  // namespace
 
+// P2 = E G with G the power-of-two part of P2 capped at 32; E must be one of the
+// instantiated register-DFT lengths.
+bool lsd_fft_plan(lsd_ctx* c) {
+  int G = 1;
+  while (G < 32 && c->P2 % (2 * G) == 0) G *= 2;
+  const int E = c->P2 / G;
+  c->fftG = G;
+  c->fftE = E;
+  return E == 3 || E == 6 || E == 9 || E == 12 || E == 18 || E == 24;
+}
+
 int lsd_launch_c2r(lsd_ctx* ctx, const cplx* four, double* phys, int nfields) {
   FFTPlanDev pl = make_plan(ctx);
-  int TJ = pick_tj(1, ctx->P2, 200 * 1024);
-  if (TJ == 0) return lsd_fail(ctx, LSD_EARG, "FFT row does not fit in shared memory");
-  size_t smem = (size_t)2 * 2 * TJ * ctx->P2 * sizeof(double2);
-  cudaFuncSetAttribute(k_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_c2r, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  dim3 grid(ceil_div(ctx->Th2, TJ), ctx->N, nfields);
-  k_c2r<<<grid, 256, smem, ctx->stream>>>(pl, ctx->N, four, phys, TJ);
+  dim3 grid(ctx->Th2, ctx->N, nfields);
+  int rc = dispatch_E(ctx->fftE, [&](auto e) {
+    k_c2r<decltype(e)::value><<<grid, 64, 0, ctx->stream>>>(pl, ctx->N, four, phys);
+    return 0;
+  });
+  if (rc) return lsd_fail(ctx, LSD_EARG, "FFT length not supported");
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_c2r: ") + cudaGetErrorString(e));
@@ -336,13 +412,13 @@ int lsd_launch_c2r(lsd_ctx* ctx, const cplx* four, double* phys, int nfields) {
 
 int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields) {
   FFTPlanDev pl = make_plan(ctx);
-  int TJ = pick_tj(1, ctx->P2, 200 * 1024);
-  if (TJ == 0) return lsd_fail(ctx, LSD_EARG, "FFT row does not fit in shared memory");
-  size_t smem = (size_t)2 * 2 * TJ * ctx->P2 * sizeof(double2);
-  cudaFuncSetAttribute(k_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_r2c, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  dim3 grid(ceil_div(ctx->Th2, TJ), ctx->N, nfields);
-  k_r2c<<<grid, 256, smem, ctx->stream>>>(pl, ctx->N, phys, four, TJ);
+  if (ctx->M > 512) return lsd_fail(ctx, LSD_EARG, "r2c: more than 512 bins");
+  dim3 grid(ctx->Th2, ctx->N, nfields);
+  int rc = dispatch_E(ctx->fftE, [&](auto e) {
+    k_r2c<decltype(e)::value><<<grid, 64, 0, ctx->stream>>>(pl, ctx->N, phys, four);
+    return 0;
+  });
+  if (rc) return lsd_fail(ctx, LSD_EARG, "FFT length not supported");
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_r2c: ") + cudaGetErrorString(e));
@@ -351,10 +427,6 @@ int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields) {
 
 int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   FFTPlanDev pl = make_plan(ctx);
-  int TJ = pick_tj(NF_IN, ctx->P2, 220 * 1024);
-  if (TJ == 0) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
-  size_t smem = (size_t)2 * NF_IN * 2 * TJ * ctx->P2 * sizeof(double2);
-  // the bin staging area [rows][M] must fit in one buffer
   ProdConst pc;
   const lsd_config& c = ctx->cfg;
   pc.d_Cor = 2.0 * c.Pm / c.E;
@@ -362,10 +434,19 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.d_qm1 = c.Pr / c.Pm;
   pc.sn = ctx->d_sn;
   pc.gp = ctx->d_gp;
-  cudaFuncSetAttribute(k_products, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_products, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  dim3 grid(ceil_div(ctx->Th2, TJ), ctx->N);
-  k_products<<<grid, 512, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out, TJ);
+  // four rows (a half-row pair) per CTA when they fit, else two (one half-row)
+  int RPC = 4;
+  size_t smem = sizeof(double2) * NF_IN * RPC * ctx->P2;
+  if (smem > 220 * 1024) { RPC = 2; smem /= 2; }
+  if (smem > 220 * 1024) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
+  dim3 grid(RPC == 4 ? ctx->HB : 2 * ctx->HB, ctx->N);
+  int rc = dispatch_E(ctx->fftE, [&](auto e) {
+    constexpr int E = decltype(e)::value;
+    cudaFuncSetAttribute(k_products<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_products<E><<<grid, 512, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out, RPC);
+    return 0;
+  });
+  if (rc) return lsd_fail(ctx, LSD_EARG, "FFT length not supported");
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_products: ") + cudaGetErrorString(e));

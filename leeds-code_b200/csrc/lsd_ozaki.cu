@@ -114,31 +114,51 @@ int lsd_umma_selftest(lsd_ctx* ctx, double* maxerr) {
 
 // =========================================================================================
 // Ozaki Legendre contractions
+//
+// Every contraction of one m-counter c and one output parity p is a real GEMM
+//   D[row, col] = sum_k A[row, k] B[k, col]
+// rows: the data (group, shell, component re/im of the inputs), 128 per CTA ("z-block");
+// columns: theta rows j of the half grid (synthesis) or the harmonics of (c, p) (analysis),
+// 32 per chunk; k: harmonics of c in two segments (synthesis) or the folded theta rows of
+// two parities (analysis), 32 per K step.  The sign/parity recipes of the reference's
+// accumulations (transform.fftw3.F90:746-774, 866-909) are folded into the A rows.
+//
+// Two kernels per contraction: a slicing pre-pass reads the FP64 data once, takes each
+// row's exponent and writes the int8 digits in the tcgen05 shared-memory tile layout; the
+// GEMM streams A and B tiles with bulk copies (a two-stage ring), issues the int8 MMAs of
+// the S(S+1)/2 digit pairs into S tensor-memory diagonals, and its epilogue warps recombine
+// the diagonals in FP64 and store through shared memory (coalesced).
 // =========================================================================================
 namespace {
 
-constexpr int OZ_MAXS = 8;      // slices per operand (TMEM: S x 64 columns <= 512)
-constexpr int OZ_NC = 32;       // synthesis: theta rows per N chunk
+constexpr int OZ_MAXS = 8;       // slices per operand
+constexpr int OZ_NC = 32;        // columns per chunk
+constexpr int OZ_STAGES = 2;     // bulk-copy ring
+constexpr int OZ_THREADS = 192;  // warps 0-3 epilogue (TMEM lane quarters), 4 copies, 5 MMA
+constexpr int OZ_STG = OZ_NC + 1;  // epilogue staging row (doubles)
 
-// per (table type, m-counter, parity) GEMM description
+enum { OZ_VEC = 0, OZ_P = 1, OZ_GRAD = 2, OZ_ST = 3, OZ_Q = 4, OZ_NTYPE = 5 };
+
+// per (type, m-counter, parity)
 struct OzProb {
-  int kofs;   // offset of the K-index list (harmonics nh, or theta rows for analysis)
-  int len1;   // length of segment 1 (segment 2 follows)
-  int K;      // total K
-  int nks;    // K steps of 32
-  long long bofs;  // byte offset of the table slices
-  int fofs;   // offset of the table column exponents
-  int npad;   // analysis: N (harmonics) padded to 16; synthesis: theta rows padded to 32
-  int nk;     // analysis: number of harmonics of this (counter, parity)
-  int nhofs;  // analysis: offset of the harmonic list (nh) of this (counter, parity)
+  int kofs;        // synthesis: offset of the K list (harmonics nh)
+  int len1;        // K length of segment 1 (segment 2 follows)
+  int K;           // total K
+  int nks;         // K steps of 32
+  int nchunk;      // column chunks of 32
+  int nk;          // analysis: harmonics of (c, p)
+  int nhofs;       // analysis: offset of their list
+  int fofs;        // column exponents (nchunk * 32)
+  long long bofs;  // table digits [chunk][ks][slice][32 x 32]
+  long long aofs;  // data digits of z-block 0 [zb][ks][slice][128 x 32]
 };
 
 // digits of x * 2^-e (|x| < 2^e): S signed 7-bit digits, most significant first
 __device__ __forceinline__ void oz_digits(double x, int e, int S, int8_t* d) {
-  double y = ldexp(x, -e);
-  long long X = (long long)ldexp(y, 7 * S);  // truncation, |X| < 2^(7S)
-  long long mag = X < 0 ? -X : X;
-  int sgn = X < 0 ? -1 : 1;
+  const double y = ldexp(x, -e);
+  const long long X = (long long)ldexp(y, 7 * S);  // truncation, |X| < 2^(7S)
+  const long long mag = X < 0 ? -X : X;
+  const int sgn = X < 0 ? -1 : 1;
 #pragma unroll
   for (int s = 0; s < OZ_MAXS; ++s)
     if (s < S) d[s] = (int8_t)(sgn * (int)((mag >> (7 * (S - 1 - s))) & 127));
@@ -151,29 +171,33 @@ __device__ __forceinline__ int oz_exponent(double maxabs) {
   return e;
 }
 
-// ---- table slicing at set-up -----------------------------------------------------------
-// Synthesis: B(N = theta row j, K = k') with column scale per j.  Tile layout per (chunk of
-// 32 rows, K step, slice): 32 x 32 bytes, K-major no swizzle.
+// (row r, K byte b) of the 4-byte word at byte `addr` of a 128 x 32 K-major tile
+__device__ __forceinline__ void oz_word_pos(int addr, int& r, int& b) {
+  r = (addr >> 8) * 8 + ((addr & 127) >> 4);
+  b = ((addr >> 7) & 1) * 16 + (addr & 15);
+}
+
+// ---- table digits, once at set-up --------------------------------------------------------
 struct OzTabArgs {
-  const double* leg; int H, Th2, S;
-  const OzProb* probs;  // [type][NM][2]
+  const double* leg; int H, Th2, S, NM;
+  const OzProb* probs;
   const int* kidx;
+  const int* nhlist;
   int8_t* B; int* fexp;
-  int tab1[5], tab2[5];  // per type: table of segment 1 / segment 2
-  int NM;
+  int tab1[OZ_NTYPE], tab2[OZ_NTYPE];  // per type: table of segment 1 / segment 2
 };
 
-__global__ void k_oz_slice_synth_tables(OzTabArgs a, int type, int nchunk) {
+// Synthesis: B(column = theta row j, K = harmonic k), column scale per j.
+__global__ void k_oz_tab_synth(OzTabArgs a, int type) {
   const int c = blockIdx.x, p = blockIdx.y;
   const OzProb pr = a.probs[(type * a.NM + c) * 2 + p];
-  for (int j = threadIdx.x; j < nchunk * OZ_NC; j += blockDim.x) {
-    double mx = 0.0;
+  for (int j = threadIdx.x; j < pr.nchunk * OZ_NC; j += blockDim.x) {
     const bool valid = j < a.Th2;
+    double mx = 0.0;
     if (valid)
       for (int k = 0; k < pr.K; ++k) {
-        int t = k < pr.len1 ? a.tab1[type] : a.tab2[type];
-        double v = a.leg[(size_t)t * a.H * a.Th2 + (size_t)a.kidx[pr.kofs + k] * a.Th2 + j];
-        mx = fmax(mx, fabs(v));
+        const int t = k < pr.len1 ? a.tab1[type] : a.tab2[type];
+        mx = fmax(mx, fabs(a.leg[((size_t)t * a.H + a.kidx[pr.kofs + k]) * a.Th2 + j]));
       }
     const int e = oz_exponent(mx);
     a.fexp[pr.fofs + j] = e;
@@ -182,424 +206,350 @@ __global__ void k_oz_slice_synth_tables(OzTabArgs a, int type, int nchunk) {
       int8_t d[OZ_MAXS];
       double v = 0.0;
       if (valid && k < pr.K) {
-        int t = k < pr.len1 ? a.tab1[type] : a.tab2[type];
-        v = a.leg[(size_t)t * a.H * a.Th2 + (size_t)a.kidx[pr.kofs + k] * a.Th2 + j];
+        const int t = k < pr.len1 ? a.tab1[type] : a.tab2[type];
+        v = a.leg[((size_t)t * a.H + a.kidx[pr.kofs + k]) * a.Th2 + j];
       }
       oz_digits(v, e, a.S, d);
-      for (int s = 0; s < a.S; ++s) {
-        size_t off = pr.bofs + ((((size_t)ch * pr.nks + k / 32) * a.S + s) * 1024) + umma::tile_off(r, k % 32);
-        a.B[off] = d[s];
-      }
+      for (int s = 0; s < a.S; ++s)
+        a.B[pr.bofs + (((size_t)ch * pr.nks + k / 32) * a.S + s) * 1024 + umma::tile_off(r, k % 32)] = d[s];
     }
   }
 }
 
-// Analysis: B(N = harmonic k of the (counter, parity), K = theta index j' of the two
-// segments) with column scale per k.  Tile per (K step, slice): npad x 32 bytes.
-__global__ void k_oz_slice_anal_tables(OzTabArgs a, int type, const int* nhlist) {
+// Analysis: B(column = harmonic k of (c, p), K = folded theta row jj), column scale per k.
+__global__ void k_oz_tab_anal(OzTabArgs a, int type) {
   const int c = blockIdx.x, p = blockIdx.y;
   const OzProb pr = a.probs[(type * a.NM + c) * 2 + p];
-  for (int k = threadIdx.x; k < pr.npad; k += blockDim.x) {
+  for (int k = threadIdx.x; k < pr.nchunk * OZ_NC; k += blockDim.x) {
     const bool valid = k < pr.nk;
-    const int nh = valid ? nhlist[pr.nhofs + k] : 0;
+    const int nh = valid ? a.nhlist[pr.nhofs + k] : 0;
     double mx = 0.0;
     if (valid)
       for (int jj = 0; jj < pr.K; ++jj) {
-        int t = jj < pr.len1 ? a.tab1[type] : a.tab2[type];
-        int j = jj < pr.len1 ? jj : jj - pr.len1;
-        mx = fmax(mx, fabs(a.leg[(size_t)t * a.H * a.Th2 + (size_t)nh * a.Th2 + j]));
+        const int t = jj < pr.len1 ? a.tab1[type] : a.tab2[type];
+        const int j = jj < pr.len1 ? jj : jj - pr.len1;
+        mx = fmax(mx, fabs(a.leg[((size_t)t * a.H + nh) * a.Th2 + j]));
       }
     const int e = oz_exponent(mx);
     a.fexp[pr.fofs + k] = e;
+    const int cb = k / OZ_NC, r = k % OZ_NC;
     for (int jj = 0; jj < pr.nks * 32; ++jj) {
       int8_t d[OZ_MAXS];
       double v = 0.0;
       if (valid && jj < pr.K) {
-        int t = jj < pr.len1 ? a.tab1[type] : a.tab2[type];
-        int j = jj < pr.len1 ? jj : jj - pr.len1;
-        v = a.leg[(size_t)t * a.H * a.Th2 + (size_t)nh * a.Th2 + j];
+        const int t = jj < pr.len1 ? a.tab1[type] : a.tab2[type];
+        const int j = jj < pr.len1 ? jj : jj - pr.len1;
+        v = a.leg[((size_t)t * a.H + nh) * a.Th2 + j];
       }
       oz_digits(v, e, a.S, d);
-      for (int s = 0; s < a.S; ++s) {
-        size_t off = pr.bofs + (((size_t)(jj / 32) * a.S + s) * (size_t)pr.npad * 32) + umma::tile_off(k, jj % 32);
-        a.B[off] = d[s];
-      }
+      for (int s = 0; s < a.S; ++s)
+        a.B[pr.bofs + (((size_t)cb * pr.nks + jj / 32) * a.S + s) * 1024 + umma::tile_off(r, jj % 32)] = d[s];
     }
   }
 }
 
-// ---- data exponents -----------------------------------------------------------------------
-// spectral input [n][H]: exponent of max |re|,|im| (times 1/r_n if rinv) over each counter
-__global__ void k_oz_exp_spec(int N, int H, int NM, const int* mstart, const int* mlen, const cplx* in,
-                              const double* rinv, int* out) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  int n = blockIdx.y;
-  if (c >= NM) return;
-  double mx = 0.0;
-  const double r1 = rinv ? rinv[n] : 1.0;
-  for (int k = 0; k < mlen[c]; ++k) {
-    double2 v = in[(size_t)n * H + mstart[c] + k];
-    if (rinv) { v.x *= r1; v.y *= r1; }
-    mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
-  }
-  out[n * NM + c] = oz_exponent(mx);
-}
-// folded theta-Fourier input [n][c][p][Th2]: exponent of max over p, j
-__global__ void k_oz_exp_four(int N, int NM, int Th2, const cplx* in, int* out) {
-  int c = blockIdx.x;
-  int n = blockIdx.y;
-  double mx = 0.0;
-  const cplx* src = in + ((size_t)n * NM + c) * 2 * Th2;
-  for (int i = threadIdx.x; i < 2 * Th2; i += blockDim.x) mx = fmax(mx, fmax(fabs(src[i].x), fabs(src[i].y)));
-  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  __shared__ double wm[8];
-  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = mx;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = fmax(mx, wm[w]);
-    out[n * NM + c] = oz_exponent(mx);
-  }
-}
-
-// ---- the GEMM kernels ---------------------------------------------------------------------
-enum { OZ_VEC = 0, OZ_P = 1, OZ_GRAD = 2 };   // synthesis table types
-enum { OZ_ST = 3, OZ_Q = 4 };                 // analysis table types
-
-struct OzSGroup {
-  const cplx* in0; const cplx* in1;   // VEC: s, t ; P: q ; GRAD: C
-  cplx* out0; cplx* out1;             // VEC/GRAD: theta, phi ; P: r
-  const int* e0; const int* e1;       // data exponents [n][NM]
-};
-struct OzSArgs {
-  int N, H, Th2, NM, S, nchunk, nrows, rows_per_group, tmem_cols;
-  const OzProb* probs; const int* kidx; const int8_t* B; const int* fexp;
+// ---- the slicing pre-pass ---------------------------------------------------------------
+struct OzPrepArgs {
+  int N, H, NM, Th2, HB, S, nrows, rows_per_group;
+  const OzProb* probs; const int* kidx; const int* mstart; const int* mlen;
   const double* rinv;
-  OzSGroup g[5];
-  int* err;
+  int8_t* A; int* erow;                  // erow [c][nrows]
+  const cplx* in0[5]; const cplx* in1[5];
 };
 
-// Synthesis GEMM: rows = data (group, shell, component), N = theta rows j (chunks of 32),
-// K = harmonics of the counter (two segments).  One CTA: (counter, parity, 128 rows).
+template <int TYPE> struct OzT {
+  static constexpr bool anal = TYPE >= OZ_ST;
+  static constexpr int per = (TYPE == OZ_P || TYPE == OZ_Q) ? 2 : 4;  // rows per shell
+  static constexpr int nin = (TYPE == OZ_VEC || TYPE == OZ_ST) ? 2 : 1;
+};
+
+// One CTA = (counter c, z-block of 128 rows); both parities.
 template <int TYPE>
-__global__ void __launch_bounds__(128, 1) k_oz_synth(OzSArgs a) {
-  extern __shared__ __align__(1024) uint8_t oz_smem[];
-  __shared__ __align__(8) uint64_t mbar;
-  __shared__ uint32_t tbase;
-  __shared__ int fexp_s[OZ_NC];
-  const int c = blockIdx.x, p = blockIdx.y;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int S = a.S;
-  const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
-  const int nks = pr.nks;
-  uint8_t* sA = oz_smem;                                 // [S][nks][4096]
-  uint8_t* sB = oz_smem + (size_t)S * nks * 4096;         // [S][nks][1024]
-  // ---- the row of this thread and its data
-  const int R = blockIdx.z * 128 + tid;
-  const bool live = R < a.nrows;
-  int g = 0, n = 0, comp = 0;
-  if (live) {
-    const int per = (TYPE == OZ_P) ? 2 : 4;
-    g = R / a.rows_per_group;
-    n = (R % a.rows_per_group) / per;
-    comp = R % per;
-  }
-  const OzSGroup G = a.g[g];
-  int erow = -1000;
-  if (live) {
-    if (TYPE == OZ_VEC) erow = max(G.e0[n * a.NM + c], G.e1[n * a.NM + c]);
-    else erow = G.e0[n * a.NM + c];
-  }
-  const double r1 = (TYPE == OZ_GRAD && live) ? a.rinv[n] : 1.0;
-  // ---- slice the data rows into A tiles (4 K-bytes at a time per slice)
-  for (int k0 = 0; k0 < nks * 32; k0 += 4) {
-    uint32_t w[OZ_MAXS];
+__global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
+  constexpr int PER = OzT<TYPE>::per, NIN = OzT<TYPE>::nin;
+  constexpr int NPAIR = 128 / PER;  // shells of the z-block
+  __shared__ int e_pair[NPAIR];
+  const int c = blockIdx.x, zb = blockIdx.y;
+  const int R0 = zb * 128;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int kbeg = a.mstart[c], klen = a.mlen[c];
+  // ---- exponents: one warp per shell of the block, max over the counter's data
+  for (int pi = warp; pi < NPAIR; pi += 8) {
+    const int R = R0 + pi * PER;
+    double mx = 0.0;
+    if (R < a.nrows) {
+      const int g = R / a.rows_per_group, n = (R % a.rows_per_group) / PER;
 #pragma unroll
-    for (int s = 0; s < OZ_MAXS; ++s) w[s] = 0;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int k = k0 + u;
-      double v = 0.0;
-      if (live && k < pr.K) {
-        const int nh = a.kidx[pr.kofs + k];
-        const bool seg1 = k < pr.len1;
-        if (TYPE == OZ_P) {
-          double2 q = G.in0[(size_t)n * a.H + nh];
-          v = comp ? q.y : q.x;
-        } else if (TYPE == OZ_VEC) {
-          double2 sv = G.in0[(size_t)n * a.H + nh], tv = G.in1[(size_t)n * a.H + nh];
-          if (seg1) v = comp == 0 ? sv.x : comp == 1 ? sv.y : comp == 2 ? tv.x : tv.y;
-          else v = comp == 0 ? tv.y : comp == 1 ? -tv.x : comp == 2 ? -sv.y : sv.x;
-        } else {  // OZ_GRAD: theta uses P_ (segment 1), phi uses sin1mP (segment 2)
-          double2 cv = G.in0[(size_t)n * a.H + nh];
-          cv.x *= r1; cv.y *= r1;
-          if (seg1) v = comp == 0 ? cv.x : comp == 1 ? cv.y : 0.0;
-          else v = comp == 2 ? -cv.y : comp == 3 ? cv.x : 0.0;
-        }
-      }
-      int8_t d[OZ_MAXS];
-      oz_digits(v, erow, S, d);
-#pragma unroll
-      for (int s = 0; s < OZ_MAXS; ++s) w[s] |= ((uint32_t)(uint8_t)d[s]) << (8 * u);
-    }
-    for (int s = 0; s < S; ++s)
-      *(uint32_t*)(sA + ((size_t)s * nks + k0 / 32) * 4096 + umma::tile_off(tid, k0 % 32)) = w[s];
-  }
-  if (tid == 0) umma::mbar_init(&mbar, 1);
-  const uint32_t tcols = a.tmem_cols;
-  if (warp == 0) umma::tmem_alloc(&tbase, tcols);
-  umma::fence_proxy_async_smem();
-  umma::fence_before_sync();
-  __syncthreads();
-  umma::fence_after_sync();
-  const uint32_t tmem = tbase;
-  const uint32_t idesc = umma::idesc_s8(128, OZ_NC);
-  bool ok = true;
-  uint32_t fail_par = 0;
-  for (int ch = 0; ch < a.nchunk; ++ch) {
-    // ---- table slices of this chunk (copied as 16-byte words)
-    const int4* src = (const int4*)(a.B + pr.bofs + (size_t)ch * nks * S * 1024);
-    int4* dst = (int4*)sB;
-    for (int i = tid; i < nks * S * 64; i += 128) dst[i] = src[i];
-    if (tid < OZ_NC) fexp_s[tid] = a.fexp[pr.fofs + ch * OZ_NC + tid];
-    umma::fence_proxy_async_smem();
-    umma::fence_before_sync();
-    __syncthreads();
-    umma::fence_after_sync();
-    if (tid == 0) {
-      for (int ks = 0; ks < nks; ++ks)
-        for (int d = 0; d < S; ++d)
-          for (int sa = 0; sa <= d; ++sa) {
-            const int sb = d - sa;
-            uint64_t ad = umma::desc_kmajor_noswz(umma::smem_u32(sA + ((size_t)sa * nks + ks) * 4096), 128, 256);
-            uint64_t bd = umma::desc_kmajor_noswz(umma::smem_u32(sB + ((size_t)ks * S + sb) * 1024), 128, 256);
-            umma::mma_s8(tmem + (uint32_t)(d * OZ_NC), ad, bd, idesc, (ks > 0 || sa > 0) ? 1 : 0);
+      for (int f = 0; f < NIN; ++f) {
+        const cplx* src = f == 0 ? a.in0[g] : a.in1[g];
+        if (!OzT<TYPE>::anal) {
+          const double r1 = (TYPE == OZ_GRAD) ? a.rinv[n] : 1.0;
+          for (int k = lane; k < klen; k += 32) {
+            double2 v = src[(size_t)n * a.H + kbeg + k];
+            if (TYPE == OZ_GRAD) { v.x *= r1; v.y *= r1; }
+            mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
           }
-      umma::commit(&mbar);
-    }
-    __syncwarp();
-    const bool mine = umma::mbar_wait(&mbar, ch & 1, WAIT_ITERS);
-    umma::fence_after_sync();
-    if (!__syncthreads_and(mine)) {  // uniform across the CTA
-      ok = false;
-      fail_par = ch & 1;
-      if (tid == 0) atomicExch(a.err, 1);
-    }
-    if (ok) {
-      // ---- epilogue: row tid, 8 theta rows at a time; sum the diagonals from the smallest
-      for (int c0 = 0; c0 < OZ_NC; c0 += 8) {
-        double acc[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] = 0.0;
-        for (int d = S - 1; d >= 0; --d) {
-          int32_t v[8];
-          umma::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * OZ_NC + c0), v);
-          umma::tmem_wait_ld();
-          const double wgt = ldexp(1.0, -7 * (d + 2));
-#pragma unroll
-          for (int q = 0; q < 8; ++q) acc[q] += (double)v[q] * wgt;
-        }
-        if (live) {
-          cplx* out = (TYPE == OZ_P || comp < 2) ? G.out0 : G.out1;
-          double* o = (double*)(out + (((size_t)n * a.NM + c) * 2 + p) * a.Th2) + (comp & 1);
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int j = ch * OZ_NC + c0 + q;
-            if (j < a.Th2) o[(size_t)j * 2] = ldexp(acc[q], erow + fexp_s[c0 + q]);
+        } else {
+          for (int i = lane; i < 2 * a.Th2; i += 32) {
+            const double2 y = src[four_off(n, c, i & 1, i >> 1, a.NM, a.HB)];
+            mx = fmax(mx, fmax(fabs(y.x), fabs(y.y)));
           }
         }
       }
     }
-    umma::fence_before_sync();
-    __syncthreads();
-    umma::fence_after_sync();
-    if (!ok) break;
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) e_pair[pi] = oz_exponent(mx);
   }
-  if (!ok) umma::mbar_wait(&mbar, fail_par, WAIT_ITERS);  // error path: let MMAs in flight drain (bounded)
-  if (warp == 0) umma::tmem_dealloc(tmem, tcols);
-}
-
-struct OzAGroup {
-  const cplx* in0; const cplx* in1;   // ST: Y_theta, Y_phi ; Q: Y
-  cplx* out0; cplx* out1;             // ST: s, t ; Q: q
-  const int* e0; const int* e1;       // data exponents [n][NM]
-  int zero_m0_im;                     // Q: zero the imaginary part of m = 0 (scalar analysis)
-};
-struct OzAArgs {
-  int N, H, Th2, NM, S, nrows, rows_per_group, tmem_cols;
-  const OzProb* probs; const int* nhlist; const int8_t* B; const int* fexp; const int* hm;
-  OzAGroup g[3];
-  int* err;
-};
-
-// Analysis GEMM: rows = data (group, shell, component), N = harmonics of the (counter,
-// parity), K = folded theta rows of the two segments.  Streams K steps through smem.
-template <int TYPE>
-__global__ void __launch_bounds__(128, 1) k_oz_anal(OzAArgs a) {
-  extern __shared__ __align__(1024) uint8_t oz_smem[];
-  __shared__ __align__(8) uint64_t mbar;
-  __shared__ uint32_t tbase;
-  __shared__ int fexp_s[64];
-  __shared__ int nh_s[64];
-  const int c = blockIdx.x, p = blockIdx.y;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int S = a.S;
-  const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
-  const int npad = pr.npad;
-  uint8_t* sA = oz_smem;                    // [S][4096]
-  uint8_t* sB = oz_smem + (size_t)S * 4096;  // [S][npad * 32]
-  const int R = blockIdx.z * 128 + tid;
-  const bool live = R < a.nrows;
-  int g = 0, n = 0, comp = 0;
-  if (live) {
-    const int per = (TYPE == OZ_Q) ? 2 : 4;
-    g = R / a.rows_per_group;
-    n = (R % a.rows_per_group) / per;
-    comp = R % per;
-  }
-  const OzAGroup G = a.g[g];
-  int erow = -1000;
-  if (live) erow = (TYPE == OZ_ST) ? max(G.e0[n * a.NM + c], G.e1[n * a.NM + c]) : G.e0[n * a.NM + c];
-  if (tid < 64) {
-    fexp_s[tid] = tid < npad ? a.fexp[pr.fofs + tid] : 0;
-    nh_s[tid] = tid < pr.nk ? a.nhlist[pr.nhofs + tid] : 0;
-  }
-  if (tid == 0) umma::mbar_init(&mbar, 1);
-  const uint32_t tcols = a.tmem_cols;
-  if (warp == 0) umma::tmem_alloc(&tbase, tcols);
-  umma::fence_before_sync();
   __syncthreads();
-  umma::fence_after_sync();
-  const uint32_t tmem = tbase;
-  const uint32_t idesc = umma::idesc_s8(128, npad);
-  // data pointers of this row: folded E/O rows of the counter at shell n
-  const size_t base = ((size_t)n * a.NM + c) * 2 * a.Th2;
-  bool ok = true;
-  uint32_t fail_par = 0;
-  for (int ks = 0; ks < pr.nks; ++ks) {
-    for (int k0 = 0; k0 < 32; k0 += 4) {
-      uint32_t w[OZ_MAXS];
+  for (int r = tid; r < 128; r += 256)
+    if (R0 + r < a.nrows) a.erow[(size_t)c * a.nrows + R0 + r] = e_pair[r / PER];
+  // ---- digits of both parities' A tiles
+  for (int p = 0; p < 2; ++p) {
+    const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+    if (pr.nchunk == 0) continue;
+    int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * a.S * 4096;
+    for (int w = tid; w < pr.nks * 1024; w += 256) {
+      const int ks = w >> 10, addr = (w & 1023) * 4;
+      int r, b;
+      oz_word_pos(addr, r, b);
+      const int R = R0 + r;
+      const bool live = R < a.nrows;
+      int g = 0, n = 0, comp = 0, e = -1000;
+      if (live) {
+        g = R / a.rows_per_group;
+        n = (R % a.rows_per_group) / PER;
+        comp = R % PER;
+        e = e_pair[r / PER];
+      }
+      uint32_t word[OZ_MAXS];
 #pragma unroll
-      for (int s = 0; s < OZ_MAXS; ++s) w[s] = 0;
+      for (int s = 0; s < OZ_MAXS; ++s) word[s] = 0;
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const int jj = ks * 32 + k0 + u;
+        const int k = ks * 32 + b + u;
         double v = 0.0;
-        if (live && jj < pr.K) {
-          if (TYPE == OZ_Q) {
-            double2 y = G.in0[base + (size_t)p * a.Th2 + jj];
+        if (live && k < pr.K) {
+          const bool seg1 = k < pr.len1;
+          if (TYPE == OZ_P) {
+            const double2 q = a.in0[g][(size_t)n * a.H + a.kidx[pr.kofs + k]];
+            v = comp ? q.y : q.x;
+          } else if (TYPE == OZ_VEC) {
+            const int nh = a.kidx[pr.kofs + k];
+            const double2 sv = a.in0[g][(size_t)n * a.H + nh], tv = a.in1[g][(size_t)n * a.H + nh];
+            // theta: s llP_ (segment 1) + (t.im, -t.re) llsin1mP (segment 2);
+            // phi:   t llP_ + (-s.im, s.re) llsin1mP        (transform.fftw3.F90:746-774)
+            if (seg1) v = comp == 0 ? sv.x : comp == 1 ? sv.y : comp == 2 ? tv.x : tv.y;
+            else v = comp == 0 ? tv.y : comp == 1 ? -tv.x : comp == 2 ? -sv.y : sv.x;
+          } else if (TYPE == OZ_GRAD) {
+            // theta: (C/r) P_ ; phi: i (C/r) sin1mP              (transform.fftw3.F90:955-1000)
+            double2 cv = a.in0[g][(size_t)n * a.H + a.kidx[pr.kofs + k]];
+            const double r1 = a.rinv[n];
+            cv.x *= r1; cv.y *= r1;
+            if (seg1) v = comp == 0 ? cv.x : comp == 1 ? cv.y : 0.0;
+            else v = comp == 2 ? -cv.y : comp == 3 ? cv.x : 0.0;
+          } else if (TYPE == OZ_Q) {
+            const double2 y = a.in0[g][four_off(n, c, p, k, a.NM, a.HB)];
             v = comp ? y.y : y.x;
-          } else {
-            const bool seg1 = jj < pr.len1;
-            const int j = seg1 ? jj : jj - pr.len1;
-            // segment 1 (gwllP_): theta/phi of parity 1-p ; segment 2 (gwllsin1mP): parity p
+          } else {  // OZ_ST: segment 1 (gwllP_) on parity 1-p, segment 2 (gwllsin1mP) on parity p
             const int pp = seg1 ? 1 - p : p;
-            double2 yt = G.in0[base + (size_t)pp * a.Th2 + j], yp = G.in1[base + (size_t)pp * a.Th2 + j];
+            const int j = seg1 ? k : k - pr.len1;
+            const size_t o = four_off(n, c, pp, j, a.NM, a.HB);
+            const double2 yt = a.in0[g][o], yp = a.in1[g][o];
+            // s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re) ...
+            // (transform.fftw3.F90:866-909)
             if (seg1) v = comp == 0 ? yt.x : comp == 1 ? yt.y : comp == 2 ? yp.x : yp.y;
             else v = comp == 0 ? yp.y : comp == 1 ? -yp.x : comp == 2 ? -yt.y : yt.x;
           }
         }
         int8_t d[OZ_MAXS];
-        oz_digits(v, erow, S, d);
+        oz_digits(v, e, a.S, d);
 #pragma unroll
-        for (int s = 0; s < OZ_MAXS; ++s) w[s] |= ((uint32_t)(uint8_t)d[s]) << (8 * u);
+        for (int s = 0; s < OZ_MAXS; ++s) word[s] |= ((uint32_t)(uint8_t)d[s]) << (8 * u);
       }
-      for (int s = 0; s < S; ++s) *(uint32_t*)(sA + (size_t)s * 4096 + umma::tile_off(tid, k0)) = w[s];
-    }
-    const int4* src = (const int4*)(a.B + pr.bofs + (size_t)ks * S * npad * 32);
-    int4* dst = (int4*)sB;
-    for (int i = tid; i < S * npad * 2; i += 128) dst[i] = src[i];
-    umma::fence_proxy_async_smem();
-    umma::fence_before_sync();
-    __syncthreads();
-    umma::fence_after_sync();
-    if (tid == 0) {
-      for (int d = 0; d < S; ++d)
-        for (int sa = 0; sa <= d; ++sa) {
-          const int sb = d - sa;
-          uint64_t ad = umma::desc_kmajor_noswz(umma::smem_u32(sA + (size_t)sa * 4096), 128, 256);
-          uint64_t bd = umma::desc_kmajor_noswz(umma::smem_u32(sB + (size_t)sb * npad * 32), 128, 256);
-          umma::mma_s8(tmem + (uint32_t)(d * npad), ad, bd, idesc, (ks > 0 || sa > 0) ? 1 : 0);
-        }
-      umma::commit(&mbar);
-    }
-    __syncwarp();
-    const bool mine = umma::mbar_wait(&mbar, ks & 1, WAIT_ITERS);
-    umma::fence_after_sync();
-    if (!__syncthreads_and(mine)) {  // uniform across the CTA
-      ok = false;
-      fail_par = ks & 1;
-      if (tid == 0) atomicExch(a.err, 1);
-      break;
+      for (int s = 0; s < a.S; ++s)
+        *(uint32_t*)(Ablk + ((size_t)ks * a.S + s) * 4096 + addr) = word[s];
     }
   }
-  if (ok) {
-    for (int c0 = 0; c0 < npad; c0 += 8) {
-      double acc[8];
+}
+
+// ---- the GEMM ---------------------------------------------------------------------------
+struct OzGemmArgs {
+  int N, H, NM, Th2, HB, S, nrows, rows_per_group;
+  const OzProb* probs; const int8_t* A; const int8_t* B; const int* fexp; const int* erow;
+  const int* nhlist; const int* hm;
+  cplx* out0[5]; cplx* out1[5]; int zero_m0_im[5];
+  int* err;
+};
+
+__device__ __forceinline__ bool oz_wait(uint64_t* mbar, uint32_t parity, int* err) {
+  if (umma::mbar_wait(mbar, parity, WAIT_ITERS)) return true;
+  atomicExch(err, 1);
+  return false;
+}
+
+// One CTA = (counter c, parity p, z-block of 128 rows); loops over the column chunks.
+template <int TYPE>
+__global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
+  constexpr int PER = OzT<TYPE>::per;
+  extern __shared__ __align__(1024) uint8_t oz_smem[];
+  __shared__ __align__(8) uint64_t full[OZ_STAGES], empty[OZ_STAGES], accf, tfree, fin;
+  __shared__ uint32_t tbase;
+  const int c = blockIdx.x, p = blockIdx.y, zb = blockIdx.z;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int S = a.S;
+  const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+  if (pr.nchunk == 0) return;  // no harmonics of this parity: nothing to write
+  const int nks = pr.nks, nch = pr.nchunk, total = nks * nch;
+  const uint32_t stage_bytes = (uint32_t)S * 5120;  // A: S x 4096, B: S x 1024
+  double* stg = (double*)(oz_smem + (size_t)OZ_STAGES * stage_bytes);  // [128][OZ_STG]
+  if (tid == 0) {
+    for (int i = 0; i < OZ_STAGES; ++i) { umma::mbar_init(&full[i], 1); umma::mbar_init(&empty[i], 1); }
+    umma::mbar_init(&accf, 1);
+    umma::mbar_init(&tfree, 128);
+    umma::mbar_init(&fin, 1);
+    umma::fence_mbar_init();
+  }
+  if (warp == 0) umma::tmem_alloc(&tbase, 256);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = tbase;
+
+  if (tid == 128) {
+    // ---- producer: A (this z-block, K step) and B (chunk, K step) tiles into the ring
+    const int8_t* Ablk = a.A + pr.aofs + (size_t)zb * nks * S * 4096;
+    const int8_t* Bblk = a.B + pr.bofs;
+    int it = 0;
+    for (; it < total; ++it) {
+      const int st = it % OZ_STAGES, use = it / OZ_STAGES;
+      if (use > 0 && !oz_wait(&empty[st], (use - 1) & 1, a.err)) break;
+      const int ch = it / nks, ks = it % nks;
+      uint8_t* sA = oz_smem + (size_t)st * stage_bytes;
+      umma::mbar_expect_tx(&full[st], stage_bytes);
+      umma::bulk_g2s(sA, Ablk + (size_t)ks * S * 4096, (uint32_t)S * 4096, &full[st]);
+      umma::bulk_g2s(sA + (size_t)S * 4096, Bblk + ((size_t)ch * nks + ks) * S * 1024, (uint32_t)S * 1024, &full[st]);
+    }
+    // drain: the copies of the last stages have landed before the CTA can exit
+    for (int j = (it > OZ_STAGES ? it - OZ_STAGES : 0); j < it; ++j)
+      umma::mbar_wait(&full[j % OZ_STAGES], (j / OZ_STAGES) & 1, WAIT_ITERS);
+  } else if (tid == 160) {
+    // ---- MMA issuer: S(S+1)/2 digit pairs per K step into S diagonals of 32 columns
+    const uint32_t idesc = umma::idesc_s8(128, OZ_NC);
+    bool ok = true;
+    for (int ch = 0; ch < nch && ok; ++ch) {
+      if (ch > 0 && !oz_wait(&tfree, (ch - 1) & 1, a.err)) { ok = false; break; }
+      umma::fence_after_sync();
+      for (int ks = 0; ks < nks; ++ks) {
+        const int it = ch * nks + ks, st = it % OZ_STAGES;
+        if (!oz_wait(&full[st], (it / OZ_STAGES) & 1, a.err)) { ok = false; break; }
+        umma::fence_after_sync();
+        const uint32_t sa0 = umma::smem_u32(oz_smem + (size_t)st * stage_bytes);
+        const uint32_t sb0 = sa0 + (uint32_t)S * 4096;
+        for (int d = 0; d < S; ++d)
+          for (int sa = 0; sa <= d; ++sa) {
+            const uint64_t ad = umma::desc_kmajor_noswz(sa0 + (uint32_t)sa * 4096, 128, 256);
+            const uint64_t bd = umma::desc_kmajor_noswz(sb0 + (uint32_t)(d - sa) * 1024, 128, 256);
+            umma::mma_s8(tmem + (uint32_t)(d * OZ_NC), ad, bd, idesc, (ks > 0 || sa > 0) ? 1 : 0);
+          }
+        umma::commit(&empty[st]);
+      }
+      if (ok) umma::commit(&accf);
+    }
+    umma::commit(&fin);  // arrives when every MMA issued above has completed
+    umma::mbar_wait(&fin, 0, WAIT_ITERS);
+  } else if (tid < 128) {
+    // ---- epilogue: row tid of the z-block
+    const int R = zb * 128 + tid;
+    const bool live = R < a.nrows;
+    const int erow = live ? a.erow[(size_t)c * a.nrows + R] : 0;
+    for (int ch = 0; ch < nch; ++ch) {
+      const bool got = umma::mbar_wait(&accf, ch & 1, WAIT_ITERS);
+      if (!umma::bar_and(1, 128, got)) {  // uniform over the 128 epilogue threads
+        if (tid == 0) atomicExch(a.err, 1);
+        break;
+      }
+      umma::fence_after_sync();
+      double acc[OZ_NC];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) acc[q] = 0.0;
-      for (int d = S - 1; d >= 0; --d) {
-        int32_t v[8];
-        umma::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * npad + c0), v);
+      for (int q = 0; q < OZ_NC; ++q) acc[q] = 0.0;
+      for (int d = S - 1; d >= 0; --d) {  // smallest diagonals first
+        int32_t v[OZ_NC];
+        umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * OZ_NC), v);
         umma::tmem_wait_ld();
         const double wgt = ldexp(1.0, -7 * (d + 2));
 #pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] += (double)v[q] * wgt;
+        for (int q = 0; q < OZ_NC; ++q) acc[q] += (double)v[q] * wgt;
       }
-      if (live) {
-        cplx* out = (TYPE == OZ_Q || comp < 2) ? G.out0 : G.out1;
+      umma::fence_before_sync();
+      umma::mbar_arrive(&tfree);  // tensor memory may take the next chunk
+      const int* fx = a.fexp + pr.fofs + ch * OZ_NC;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int k = c0 + q;
+      for (int q = 0; q < OZ_NC; ++q) stg[tid * OZ_STG + q] = live ? ldexp(acc[q], erow + fx[q]) : 0.0;
+      umma::bar_sync(1, 128);
+      // coalesced stores: row pairs (re, im) x 32 columns
+      for (int idx = tid; idx < 64 * OZ_NC; idx += 128) {
+        const int pair = idx / OZ_NC, q = idx % OZ_NC;
+        const int Rr = zb * 128 + 2 * pair;
+        if (Rr >= a.nrows) continue;
+        const int g = Rr / a.rows_per_group, n = (Rr % a.rows_per_group) / PER, comp = Rr % PER;
+        double2 val = make_double2(stg[(2 * pair) * OZ_STG + q], stg[(2 * pair + 1) * OZ_STG + q]);
+        cplx* out = (comp < 2) ? a.out0[g] : a.out1[g];
+        if (!OzT<TYPE>::anal) {
+          const int j = ch * OZ_NC + q;
+          if (j < a.Th2) out[four_off(n, c, p, j, a.NM, a.HB)] = val;
+        } else {
+          const int k = ch * OZ_NC + q;
           if (k < pr.nk) {
-            const int nh = nh_s[k];
-            double val = ldexp(acc[q], erow + fexp_s[k]);
-            const bool im = comp & 1;
-            // m = 0: s, t (and a scalar) have zero imaginary parts; q keeps its own
+            const int nh = a.nhlist[pr.nhofs + k];
+            // m = 0: s, t (and a scalar) keep no imaginary part; q keeps its own
             // (transform.fftw3.F90:599, 869, 902, 908)
-            if (im && a.hm[nh] == 0 && (TYPE == OZ_ST || G.zero_m0_im)) val = 0.0;
-            ((double*)(out + (size_t)n * a.H + nh))[im ? 1 : 0] = val;
+            if (a.hm[nh] == 0 && (TYPE == OZ_ST || a.zero_m0_im[g])) val.y = 0.0;
+            out[(size_t)n * a.H + nh] = val;
           }
         }
       }
+      umma::bar_sync(1, 128);
     }
   }
-  if (!ok) umma::mbar_wait(&mbar, fail_par, WAIT_ITERS);  // error path: let MMAs in flight drain (bounded)
   umma::fence_before_sync();
   __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tmem, tcols);
+  if (warp == 0) umma::tmem_dealloc(tmem, 256);
 }
 
 }  // namespace
 
 // =========================================================================================
-// host side: set-up of the sliced tables, and the launches
+// host side
 // =========================================================================================
-constexpr int OZ_EXP_SLOTS = 32;
-
 struct OzState {
-  int S = 0, nchunk = 0, max_nks_synth = 0;
+  int S = 0;
+  int nzb_max[OZ_NTYPE] = {};
   OzProb* d_probs = nullptr;
   int* d_kidx = nullptr;
   int* d_nh = nullptr;
   int8_t* d_B = nullptr;
   int* d_fexp = nullptr;
-  int* d_exp = nullptr;  // data exponents: [slot][N][NM], one slot per input of a launch call
+  int8_t* d_A = nullptr;  // data digits, shared by every launch (stream ordered)
+  int* d_erow = nullptr;  // row exponents [c][rows]
   int* d_err = nullptr;
-  std::vector<OzProb> probs;
+  size_t smem = 0;
 };
 
-static unsigned pow2cols(int n) {
-  unsigned c = 32;
-  while ((int)c < n) c <<= 1;
-  return c;
+namespace {
+constexpr int OZ_MAXG_SYNTH = 5, OZ_MAXG_ANAL = 3;  // groups per launch
+
+template <int TYPE>
+void oz_set_smem(size_t smem) {
+  cudaFuncSetAttribute(k_oz_gemm<TYPE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
+}  // namespace
 
 void lsd_ozaki_free(lsd_ctx* ctx) {
   OzState* o = (OzState*)ctx->oz;
   if (!o) return;
-  void* ptrs[] = {o->d_probs, o->d_kidx, o->d_nh, o->d_B, o->d_fexp, o->d_exp, o->d_err};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  void* ptrs[] = {o->d_probs, o->d_kidx, o->d_nh, o->d_B, o->d_fexp, o->d_A, o->d_erow, o->d_err};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
   delete o;
   ctx->oz = nullptr;
 }
@@ -607,23 +557,26 @@ void lsd_ozaki_free(lsd_ctx* ctx) {
 int lsd_ozaki_setup(lsd_ctx* ctx) {
   OzState* o = new OzState();
   ctx->oz = o;
-  int S = ctx->cfg.ozaki_slices > 0 ? ctx->cfg.ozaki_slices : 7;
+  const int S = ctx->cfg.ozaki_slices > 0 ? ctx->cfg.ozaki_slices : 7;
   if (S < 2 || S > OZ_MAXS) return lsd_fail(ctx, LSD_EARG, "ozaki_slices must be 2..8");
   o->S = S;
-  const int NM = ctx->NM, Th2 = ctx->Th2;
-  o->nchunk = ceil_div(Th2, OZ_NC);
-  // harmonic lists per (counter, parity)
-  std::vector<std::vector<int>> Kcp((size_t)NM * 2);
+  const int NM = ctx->NM, Th2 = ctx->Th2, N = ctx->N;
+  std::vector<std::vector<int>> Kcp((size_t)NM * 2);  // harmonics per (counter, parity)
   for (int c = 0; c < NM; ++c)
     for (int k = 0; k < ctx->mlen[c]; ++k) {
-      int nh = ctx->mstart[c] + k;
+      const int nh = ctx->mstart[c] + k;
       Kcp[(size_t)c * 2 + ctx->hs[nh]].push_back(nh);
     }
   std::vector<int> kidx, nhl;
-  o->probs.assign((size_t)5 * NM * 2, OzProb());
-  long long bytes = 0;
+  std::vector<OzProb> probs((size_t)OZ_NTYPE * NM * 2);
+  long long bbytes = 0, abytes_max = 0;
   int fofs = 0;
-  for (int type = 0; type < 5; ++type)
+  for (int type = 0; type < OZ_NTYPE; ++type) {
+    const bool anal = type >= OZ_ST;
+    const int per = (type == OZ_P || type == OZ_Q) ? 2 : 4;
+    const int maxg = anal ? OZ_MAXG_ANAL : OZ_MAXG_SYNTH;
+    o->nzb_max[type] = ceil_div(maxg * per * N, 128);
+    long long abytes = 0;
     for (int c = 0; c < NM; ++c)
       for (int p = 0; p < 2; ++p) {
         OzProb pr{};
@@ -633,7 +586,7 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
         pr.nk = (int)Kp.size();
         nhl.insert(nhl.end(), Kp.begin(), Kp.end());
         pr.kofs = (int)kidx.size();
-        if (type == OZ_VEC || type == OZ_GRAD) {  // segment 1 on K(1-p), segment 2 on K(p)
+        if (type == OZ_VEC || type == OZ_GRAD) {
           kidx.insert(kidx.end(), Kq.begin(), Kq.end());
           kidx.insert(kidx.end(), Kp.begin(), Kp.end());
           pr.len1 = (int)Kq.size();
@@ -648,137 +601,143 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
           pr.len1 = pr.K = Th2;
         }
         pr.nks = std::max(1, ceil_div(pr.K, 32));
-        pr.bofs = bytes;
+        // analysis: (c, p) without harmonics has no output (nchunk 0); a synthesis output
+        // without harmonics is still written (zeros)
+        const bool empty = anal && pr.nk == 0;
+        pr.nchunk = empty ? 0 : (anal ? ceil_div(pr.nk, OZ_NC) : ceil_div(Th2, OZ_NC));
         pr.fofs = fofs;
-        if (type <= OZ_GRAD) {
-          pr.npad = o->nchunk * OZ_NC;
-          bytes += (long long)o->nchunk * pr.nks * S * 1024;
-          fofs += pr.npad;
-          o->max_nks_synth = std::max(o->max_nks_synth, pr.nks);
-        } else {
-          pr.npad = std::max(16, ((pr.nk + 15) / 16) * 16);
-          if (pr.npad > 64) return lsd_fail(ctx, LSD_EARG, "tensor-core analysis supports at most 64 harmonics per (m, parity)");
-          bytes += (long long)pr.nks * S * pr.npad * 32;
-          fofs += pr.npad;
-        }
-        o->probs[((size_t)type * NM + c) * 2 + p] = pr;
+        fofs += pr.nchunk * OZ_NC;
+        pr.bofs = bbytes;
+        bbytes += (long long)pr.nchunk * pr.nks * S * 1024;
+        pr.aofs = abytes;
+        if (pr.nchunk) abytes += (long long)o->nzb_max[type] * pr.nks * S * 4096;
+        probs[((size_t)type * NM + c) * 2 + p] = pr;
       }
-  size_t smem_synth = std::max((size_t)5120 * S * o->max_nks_synth, (size_t)80 * 1024);
-  if (smem_synth > 220 * 1024)
-    return lsd_fail(ctx, LSD_EARG, "tensor-core synthesis: too many harmonics per m for the resident slices (reduce ozaki_slices or L)");
+    abytes_max = std::max(abytes_max, abytes);
+  }
+  o->smem = (size_t)OZ_STAGES * S * 5120 + sizeof(double) * 128 * OZ_STG;
   if (kidx.empty()) kidx.push_back(0);
   if (nhl.empty()) nhl.push_back(0);
-  CUDA_TRY(cudaMalloc(&o->d_probs, sizeof(OzProb) * o->probs.size()));
-  CUDA_TRY(cudaMemcpy(o->d_probs, o->probs.data(), sizeof(OzProb) * o->probs.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&o->d_probs, sizeof(OzProb) * probs.size()));
+  CUDA_TRY(cudaMemcpy(o->d_probs, probs.data(), sizeof(OzProb) * probs.size(), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMalloc(&o->d_kidx, sizeof(int) * kidx.size()));
   CUDA_TRY(cudaMemcpy(o->d_kidx, kidx.data(), sizeof(int) * kidx.size(), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMalloc(&o->d_nh, sizeof(int) * nhl.size()));
   CUDA_TRY(cudaMemcpy(o->d_nh, nhl.data(), sizeof(int) * nhl.size(), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMalloc(&o->d_B, bytes));
-  CUDA_TRY(cudaMalloc(&o->d_fexp, sizeof(int) * (size_t)fofs));
-  CUDA_TRY(cudaMalloc(&o->d_exp, sizeof(int) * (size_t)OZ_EXP_SLOTS * ctx->N * NM));
+  CUDA_TRY(cudaMalloc(&o->d_B, std::max<long long>(bbytes, 16)));
+  CUDA_TRY(cudaMalloc(&o->d_fexp, sizeof(int) * (size_t)std::max(fofs, 1)));
+  CUDA_TRY(cudaMalloc(&o->d_A, std::max<long long>(abytes_max, 16)));
+  int max_rows = 0;
+  for (int type = 0; type < OZ_NTYPE; ++type) max_rows = std::max(max_rows, o->nzb_max[type] * 128);
+  CUDA_TRY(cudaMalloc(&o->d_erow, sizeof(int) * (size_t)NM * max_rows));
   CUDA_TRY(cudaMalloc(&o->d_err, sizeof(int)));
   CUDA_TRY(cudaMemset(o->d_err, 0, sizeof(int)));
   OzTabArgs ta;
-  ta.leg = ctx->d_leg; ta.H = ctx->H; ta.Th2 = Th2; ta.S = S; ta.probs = o->d_probs; ta.kidx = o->d_kidx;
-  ta.B = o->d_B; ta.fexp = o->d_fexp; ta.NM = NM;
-  const int t1[5] = {LSD_LEG_LLP_, LSD_LEG_P, LSD_LEG_P_, LSD_LEG_GWLLP_, LSD_LEG_GWP};
-  const int t2[5] = {LSD_LEG_LLSIN1MP, LSD_LEG_P, LSD_LEG_SIN1MP, LSD_LEG_GWLLSIN1MP, LSD_LEG_GWP};
-  for (int i = 0; i < 5; ++i) { ta.tab1[i] = t1[i]; ta.tab2[i] = t2[i]; }
-  dim3 g(NM, 2);
-  for (int type = 0; type <= OZ_GRAD; ++type) k_oz_slice_synth_tables<<<g, 128, 0, ctx->stream>>>(ta, type, o->nchunk);
-  for (int type = OZ_ST; type <= OZ_Q; ++type) k_oz_slice_anal_tables<<<g, 64, 0, ctx->stream>>>(ta, type, o->d_nh);
+  ta.leg = ctx->d_leg; ta.H = ctx->H; ta.Th2 = Th2; ta.S = S; ta.NM = NM;
+  ta.probs = o->d_probs; ta.kidx = o->d_kidx; ta.nhlist = o->d_nh; ta.B = o->d_B; ta.fexp = o->d_fexp;
+  const int t1[OZ_NTYPE] = {LSD_LEG_LLP_, LSD_LEG_P, LSD_LEG_P_, LSD_LEG_GWLLP_, LSD_LEG_GWP};
+  const int t2[OZ_NTYPE] = {LSD_LEG_LLSIN1MP, LSD_LEG_P, LSD_LEG_SIN1MP, LSD_LEG_GWLLSIN1MP, LSD_LEG_GWP};
+  for (int i = 0; i < OZ_NTYPE; ++i) { ta.tab1[i] = t1[i]; ta.tab2[i] = t2[i]; }
+  const dim3 g(NM, 2);
+  for (int type = OZ_VEC; type <= OZ_GRAD; ++type) k_oz_tab_synth<<<g, 128, 0, ctx->stream>>>(ta, type);
+  for (int type = OZ_ST; type <= OZ_Q; ++type) k_oz_tab_anal<<<g, 64, 0, ctx->stream>>>(ta, type);
   ctx->launches += 5;
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  for (int type = 0; type <= OZ_GRAD; ++type) {
-    auto kern = type == OZ_VEC ? k_oz_synth<OZ_VEC> : type == OZ_P ? k_oz_synth<OZ_P> : k_oz_synth<OZ_GRAD>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_synth);
+  oz_set_smem<OZ_VEC>(o->smem); oz_set_smem<OZ_P>(o->smem); oz_set_smem<OZ_GRAD>(o->smem);
+  oz_set_smem<OZ_ST>(o->smem); oz_set_smem<OZ_Q>(o->smem);
+  CUDA_TRY(cudaGetLastError());
+  return LSD_OK;
+}
+
+namespace {
+
+struct OzLaunchGroup { const cplx* in0; const cplx* in1; cplx* out0; cplx* out1; int zero_m0_im; };
+
+template <int TYPE>
+int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
+  OzState* o = (OzState*)ctx->oz;
+  constexpr int PER = OzT<TYPE>::per;
+  const int rpg = PER * ctx->N, nrows = ng * rpg, nzb = ceil_div(nrows, 128);
+  if (nzb > o->nzb_max[TYPE]) return lsd_fail(ctx, LSD_EARG, "tensor-core contraction: too many groups in one launch");
+  OzPrepArgs pa;
+  pa.N = ctx->N; pa.H = ctx->H; pa.NM = ctx->NM; pa.Th2 = ctx->Th2; pa.HB = ctx->HB; pa.S = o->S; pa.nrows = nrows;
+  pa.rows_per_group = rpg; pa.probs = o->d_probs; pa.kidx = o->d_kidx; pa.mstart = ctx->d_mstart;
+  pa.mlen = ctx->d_mlen; pa.rinv = ctx->d_r + (size_t)2 * ctx->N; pa.A = o->d_A; pa.erow = o->d_erow;
+  OzGemmArgs ga;
+  ga.N = ctx->N; ga.H = ctx->H; ga.NM = ctx->NM; ga.Th2 = ctx->Th2; ga.HB = ctx->HB; ga.S = o->S; ga.nrows = nrows;
+  ga.rows_per_group = rpg; ga.probs = o->d_probs; ga.A = o->d_A; ga.B = o->d_B; ga.fexp = o->d_fexp;
+  ga.erow = o->d_erow; ga.nhlist = o->d_nh; ga.hm = ctx->d_m; ga.err = o->d_err;
+  for (int i = 0; i < 5; ++i) {
+    const bool on = i < ng;
+    pa.in0[i] = on ? gs[i].in0 : nullptr; pa.in1[i] = on ? gs[i].in1 : nullptr;
+    ga.out0[i] = on ? gs[i].out0 : nullptr; ga.out1[i] = on ? gs[i].out1 : nullptr;
+    ga.zero_m0_im[i] = on ? gs[i].zero_m0_im : 0;
   }
-  return LSD_OK;
-}
-
-// data exponents of a spectral input (slot < 14) or a theta-Fourier input (slot 14..20)
-static int oz_exp_spec(lsd_ctx* ctx, const cplx* in, const double* rinv, int slot) {
-  OzState* o = (OzState*)ctx->oz;
-  dim3 g(ceil_div(ctx->NM, 64), ctx->N);
-  k_oz_exp_spec<<<g, 64, 0, ctx->stream>>>(ctx->N, ctx->H, ctx->NM, ctx->d_mstart, ctx->d_mlen, in, rinv,
-                                            o->d_exp + (size_t)slot * ctx->N * ctx->NM);
-  ctx->launches++;
-  return LSD_OK;
-}
-static int oz_exp_four(lsd_ctx* ctx, const cplx* in, int slot) {
-  OzState* o = (OzState*)ctx->oz;
-  dim3 g(ctx->NM, ctx->N);
-  k_oz_exp_four<<<g, 128, 0, ctx->stream>>>(ctx->N, ctx->NM, ctx->Th2, in, o->d_exp + (size_t)slot * ctx->N * ctx->NM);
-  ctx->launches++;
-  return LSD_OK;
-}
-
-const int* lsd_ozaki_exp(lsd_ctx* ctx, int slot) {
-  OzState* o = (OzState*)ctx->oz;
-  return o->d_exp + (size_t)slot * ctx->N * ctx->NM;
-}
-int lsd_ozaki_exp_spec(lsd_ctx* ctx, const cplx* in, const double* rinv, int slot) { return oz_exp_spec(ctx, in, rinv, slot); }
-int lsd_ozaki_exp_four(lsd_ctx* ctx, const cplx* in, int slot) { return oz_exp_four(ctx, in, slot); }
-
-// groups: VEC {s, t -> theta, phi}, P {q -> r}, GRAD {C -> theta, phi}
-int lsd_ozaki_synth(lsd_ctx* ctx, int type, const OzSynthGroupH* gh, int ng) {
-  OzState* o = (OzState*)ctx->oz;
-  OzSArgs a;
-  a.N = ctx->N; a.H = ctx->H; a.Th2 = ctx->Th2; a.NM = ctx->NM; a.S = o->S; a.nchunk = o->nchunk;
-  const int per = (type == OZ_P) ? 2 : 4;
-  a.rows_per_group = per * ctx->N;
-  a.nrows = ng * a.rows_per_group;
-  a.tmem_cols = pow2cols(o->S * OZ_NC);
-  a.probs = o->d_probs; a.kidx = o->d_kidx; a.B = o->d_B; a.fexp = o->d_fexp;
-  a.rinv = ctx->d_r + (size_t)2 * ctx->N;
-  a.err = o->d_err;
-  for (int i = 0; i < ng; ++i) {
-    a.g[i].in0 = gh[i].in0; a.g[i].in1 = gh[i].in1; a.g[i].out0 = gh[i].out0; a.g[i].out1 = gh[i].out1;
-    a.g[i].e0 = gh[i].e0; a.g[i].e1 = gh[i].e1;
-  }
-  dim3 grid(ctx->NM, 2, ceil_div(a.nrows, 128));
-  // at most two CTAs (2 x 256 TMEM columns) per SM
-  size_t smem = std::max((size_t)5120 * o->S * o->max_nks_synth, (size_t)80 * 1024);
-  if (type == OZ_VEC) k_oz_synth<OZ_VEC><<<grid, 128, smem, ctx->stream>>>(a);
-  else if (type == OZ_P) k_oz_synth<OZ_P><<<grid, 128, smem, ctx->stream>>>(a);
-  else k_oz_synth<OZ_GRAD><<<grid, 128, smem, ctx->stream>>>(a);
-  ctx->launches++;
+  k_oz_prep<TYPE><<<dim3(ctx->NM, nzb), 256, 0, ctx->stream>>>(pa);
+  k_oz_gemm<TYPE><<<dim3(ctx->NM, 2, nzb), OZ_THREADS, o->smem, ctx->stream>>>(ga);
+  ctx->launches += 2;
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_oz_synth: ") + cudaGetErrorString(e));
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("tensor-core contraction: ") + cudaGetErrorString(e));
   return LSD_OK;
 }
 
-// groups: ST {Y_theta, Y_phi -> s, t}, Q {Y -> q}
-int lsd_ozaki_anal(lsd_ctx* ctx, int type, const OzAnalGroupH* gh, int ng) {
-  OzState* o = (OzState*)ctx->oz;
-  OzAArgs a;
-  a.N = ctx->N; a.H = ctx->H; a.Th2 = ctx->Th2; a.NM = ctx->NM; a.S = o->S;
-  const int per = (type == OZ_Q) ? 2 : 4;
-  a.rows_per_group = per * ctx->N;
-  a.nrows = ng * a.rows_per_group;
-  a.tmem_cols = pow2cols(o->S * 64);
-  a.probs = o->d_probs; a.nhlist = o->d_nh; a.B = o->d_B; a.fexp = o->d_fexp; a.hm = ctx->d_m;
-  a.err = o->d_err;
-  for (int i = 0; i < ng; ++i) {
-    a.g[i].in0 = gh[i].in0; a.g[i].in1 = gh[i].in1; a.g[i].out0 = gh[i].out0; a.g[i].out1 = gh[i].out1;
-    a.g[i].e0 = gh[i].e0; a.g[i].e1 = gh[i].e1; a.g[i].zero_m0_im = gh[i].zero_m0_im;
+template <int TYPE>
+int oz_run_all(lsd_ctx* ctx, const std::vector<OzLaunchGroup>& gs, int maxg) {
+  for (size_t i = 0; i < gs.size(); i += maxg) {
+    int rc = oz_run<TYPE>(ctx, gs.data() + i, (int)std::min<size_t>(maxg, gs.size() - i));
+    if (rc) return rc;
   }
-  dim3 grid(ctx->NM, 2, ceil_div(a.nrows, 128));
-  size_t smem = (size_t)o->S * (4096 + 64 * 32) + 1024;
-  // ask for more than half of an SM's shared memory: one CTA (one TMEM allocation) per SM
-  smem = std::max(smem, (size_t)120 * 1024);
-  if (type == OZ_ST) {
-    cudaFuncSetAttribute(k_oz_anal<OZ_ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_oz_anal<OZ_ST><<<grid, 128, smem, ctx->stream>>>(a);
-  } else {
-    cudaFuncSetAttribute(k_oz_anal<OZ_Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_oz_anal<OZ_Q><<<grid, 128, smem, ctx->stream>>>(a);
+  return LSD_OK;
+}
+
+}  // namespace
+
+// The FP64 group descriptions of the synthesis / analysis launchers, mapped onto the
+// tensor-core GEMM types: vector (q,s,t) = P(q) + VEC(s,t); scalar = P; grad3 (dC, C) =
+// P(dC) + GRAD(C); grad2 = GRAD; analysis vector (r,th,ph) = Q(r) + ST(th,ph); scalar = Q.
+int lsd_ozaki_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups) {
+  std::vector<OzLaunchGroup> gv, gp, gg;
+  for (int i = 0; i < ngroups; ++i) {
+    const SynthGroup& G = groups[i];
+    switch (G.kind) {
+      case SK_VECTOR:
+        gp.push_back({G.in[0], nullptr, G.out[0], nullptr, 0});
+        gv.push_back({G.in[1], G.in[2], G.out[1], G.out[2], 0});
+        break;
+      case SK_SCALAR:
+        gp.push_back({G.in[0], nullptr, G.out[0], nullptr, 0});
+        break;
+      case SK_GRAD3:
+        gp.push_back({G.in[0], nullptr, G.out[0], nullptr, 0});
+        gg.push_back({G.in[1], nullptr, G.out[1], G.out[2], 0});
+        break;
+      default:  // SK_GRAD2
+        gg.push_back({G.in[0], nullptr, G.out[0], G.out[1], 0});
+        break;
+    }
   }
-  ctx->launches++;
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_oz_anal: ") + cudaGetErrorString(e));
+  int rc;
+  if ((rc = oz_run_all<OZ_VEC>(ctx, gv, OZ_MAXG_SYNTH))) return rc;
+  if ((rc = oz_run_all<OZ_P>(ctx, gp, OZ_MAXG_SYNTH))) return rc;
+  if ((rc = oz_run_all<OZ_GRAD>(ctx, gg, OZ_MAXG_SYNTH))) return rc;
+  return LSD_OK;
+}
+
+int lsd_ozaki_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
+  std::vector<OzLaunchGroup> gs, gq;
+  for (int i = 0; i < ngroups; ++i) {
+    const AnalGroup& G = groups[i];
+    if (G.kind == AK_VECTOR) {
+      gq.push_back({G.in[0], nullptr, G.out[0], nullptr, 0});  // q keeps Im of m = 0
+      gs.push_back({G.in[1], G.in[2], G.out[1], G.out[2], 1});
+    } else {
+      gq.push_back({G.in[0], nullptr, G.out[0], nullptr, 1});
+    }
+  }
+  int rc;
+  if ((rc = oz_run_all<OZ_ST>(ctx, gs, OZ_MAXG_ANAL))) return rc;
+  if ((rc = oz_run_all<OZ_Q>(ctx, gq, OZ_MAXG_ANAL))) return rc;
   return LSD_OK;
 }
 
@@ -788,87 +747,6 @@ int lsd_ozaki_check(lsd_ctx* ctx) {
   OzState* o = (OzState*)ctx->oz;
   int err = 0;
   CUDA_TRY(cudaMemcpy(&err, o->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (err) return lsd_fail(ctx, LSD_ECUDA, "tensor-core contraction: an mbarrier wait timed out");
-  return LSD_OK;
-}
-
-// The FP64 group descriptions of the synthesis / analysis launchers, mapped onto the
-// tensor-core GEMM types: vector (q,s,t) = P(q) + VEC(s,t); scalar = P; grad3 (dC, C) =
-// P(dC) + GRAD(C); grad2 = GRAD; analysis vector (r,th,ph) = Q(r) + ST(th,ph); scalar = Q.
-int lsd_ozaki_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups) {
-  OzState* o = (OzState*)ctx->oz;
-  const double* rinv = ctx->d_r + (size_t)2 * ctx->N;
-  std::vector<OzSynthGroupH> gv, gp, gg;
-  int slot = 0;
-  auto ex = [&](const cplx* in, const double* ri) -> const int* {
-    if (slot >= OZ_EXP_SLOTS) return nullptr;
-    oz_exp_spec(ctx, in, ri, slot);
-    return o->d_exp + (size_t)(slot++) * ctx->N * ctx->NM;
-  };
-  for (int i = 0; i < ngroups; ++i) {
-    const SynthGroup& G = groups[i];
-    OzSynthGroupH h{};
-    switch (G.kind) {
-      case SK_VECTOR:
-        h = {G.in[0], nullptr, G.out[0], nullptr, ex(G.in[0], nullptr), nullptr};
-        gp.push_back(h);
-        h = {G.in[1], G.in[2], G.out[1], G.out[2], ex(G.in[1], nullptr), ex(G.in[2], nullptr)};
-        gv.push_back(h);
-        break;
-      case SK_SCALAR:
-        h = {G.in[0], nullptr, G.out[0], nullptr, ex(G.in[0], nullptr), nullptr};
-        gp.push_back(h);
-        break;
-      case SK_GRAD3:
-        h = {G.in[0], nullptr, G.out[0], nullptr, ex(G.in[0], nullptr), nullptr};
-        gp.push_back(h);
-        h = {G.in[1], nullptr, G.out[1], G.out[2], ex(G.in[1], rinv), nullptr};
-        gg.push_back(h);
-        break;
-      default:  // SK_GRAD2
-        h = {G.in[0], nullptr, G.out[0], G.out[1], ex(G.in[0], rinv), nullptr};
-        gg.push_back(h);
-        break;
-    }
-  }
-  if (slot >= OZ_EXP_SLOTS) return lsd_fail(ctx, LSD_EARG, "tensor-core synthesis: too many inputs in one call");
-  int rc;
-  for (size_t i = 0; i < gv.size(); i += 5)
-    if ((rc = lsd_ozaki_synth(ctx, OZ_VEC, gv.data() + i, (int)std::min<size_t>(5, gv.size() - i)))) return rc;
-  for (size_t i = 0; i < gp.size(); i += 5)
-    if ((rc = lsd_ozaki_synth(ctx, OZ_P, gp.data() + i, (int)std::min<size_t>(5, gp.size() - i)))) return rc;
-  for (size_t i = 0; i < gg.size(); i += 5)
-    if ((rc = lsd_ozaki_synth(ctx, OZ_GRAD, gg.data() + i, (int)std::min<size_t>(5, gg.size() - i)))) return rc;
-  return LSD_OK;
-}
-
-int lsd_ozaki_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
-  OzState* o = (OzState*)ctx->oz;
-  std::vector<OzAnalGroupH> gs, gq;
-  int slot = 0;
-  auto ex = [&](const cplx* in) -> const int* {
-    if (slot >= OZ_EXP_SLOTS) return nullptr;
-    oz_exp_four(ctx, in, slot);
-    return o->d_exp + (size_t)(slot++) * ctx->N * ctx->NM;
-  };
-  for (int i = 0; i < ngroups; ++i) {
-    const AnalGroup& G = groups[i];
-    OzAnalGroupH h{};
-    if (G.kind == AK_VECTOR) {
-      h = {G.in[0], nullptr, G.out[0], nullptr, ex(G.in[0]), nullptr, 0};  // q keeps Im of m = 0
-      gq.push_back(h);
-      h = {G.in[1], G.in[2], G.out[1], G.out[2], ex(G.in[1]), ex(G.in[2]), 1};
-      gs.push_back(h);
-    } else {
-      h = {G.in[0], nullptr, G.out[0], nullptr, ex(G.in[0]), nullptr, 1};
-      gq.push_back(h);
-    }
-  }
-  if (slot >= OZ_EXP_SLOTS) return lsd_fail(ctx, LSD_EARG, "tensor-core analysis: too many inputs in one call");
-  int rc;
-  for (size_t i = 0; i < gs.size(); i += 3)
-    if ((rc = lsd_ozaki_anal(ctx, OZ_ST, gs.data() + i, (int)std::min<size_t>(3, gs.size() - i)))) return rc;
-  for (size_t i = 0; i < gq.size(); i += 3)
-    if ((rc = lsd_ozaki_anal(ctx, OZ_Q, gq.data() + i, (int)std::min<size_t>(3, gq.size() - i)))) return rc;
+  if (err) return lsd_fail(ctx, LSD_ECUDA, "tensor-core Legendre contraction: an mbarrier wait timed out");
   return LSD_OK;
 }

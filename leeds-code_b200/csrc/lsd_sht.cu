@@ -8,7 +8,8 @@
 // (transform.fftw3.F90:527-602, 825-949).
 //
 // Data layouts: spectral [n][H] complex (harmonic fastest, the reference's `spec`
-// order); theta-Fourier [n][m-counter][Th] complex (the reference's a3c_Y3 per shell);
+// order); theta-Fourier rows folded into even/odd half-grid sums in half-row pairs
+// (four_off: [n][h/2][m-counter][E/O][h%2]);
 // tables [nh][Th2] (the reference's leg_*(Th2, 0:H-1)).
 //
 // Synthesis CTA = (m-counter, NT shells, group); thread = one theta row j of the half
@@ -27,7 +28,7 @@ constexpr int A_JC = 16;  // theta rows per analysis j-chunk
 constexpr int DROW = A_JC * A_NT + 1;  // padded analysis data row (double2)
 
 struct SynthArgs {
-  int N, H, Th, Th2, NM, ngroup;
+  int N, H, Th, Th2, NM, HB, ngroup;
   const int* mstart;
   const int* mlen;
   const int* hs;
@@ -172,14 +173,13 @@ __global__ void __launch_bounds__(256) k_synth(SynthArgs a) {
     for (int q = 0; q < S_NT; ++q) {
       int n = n0 + q;
       if (n >= a.N) continue;
-      cplx* out = G.out[o] + ((size_t)n * a.NM + c) * 2 * Th2;  // [p][Th2]: E then O
-      out[j] = acc[o][0][q];
-      out[Th2 + j] = acc[o][1][q];
+      G.out[o][four_off(n, c, 0, j, a.NM, a.HB)] = acc[o][0][q];  // E
+      G.out[o][four_off(n, c, 1, j, a.NM, a.HB)] = acc[o][1][q];  // O
     }
 }
 
 struct AnalArgs {
-  int N, H, Th, Th2, NM, Hr, ngroup;
+  int N, H, Th, Th2, NM, HB, Hr, ngroup;
   const int* perm;     // [Hc][Hr]: thread -> harmonic of the column, sorted by (m-counter, parity)
   const int* mstart;   // per m-counter
   const int* mlen;
@@ -228,10 +228,9 @@ __global__ void __launch_bounds__(288) k_anal(AnalArgs a) {
       int n = n0 + q;
       double2 e = make_double2(0.0, 0.0), o = e;
       if (n < a.N) {  // folded E/O data (the FFT stage folded the two hemispheres)
-        const cplx* src = G.in[f] + ((size_t)n * a.NM + (cc ? c1 : c0)) * 2 * Th2;
-        int j = j0 + jj;
-        e = src[j];
-        o = src[Th2 + j];
+        const int cn = cc ? c1 : c0, j = j0 + jj;
+        e = G.in[f][four_off(n, cn, 0, j, a.NM, a.HB)];
+        o = G.in[f][four_off(n, cn, 1, j, a.NM, a.HB)];
       }
       dat[((cc * NF + f) * 2 + 0) * DROW + jj * A_NT + q] = e;
       dat[((cc * NF + f) * 2 + 1) * DROW + jj * A_NT + q] = o;
@@ -291,7 +290,7 @@ __global__ void __launch_bounds__(288) k_anal(AnalArgs a) {
 template <int KIND>
 int launch_synth_kind(lsd_ctx* ctx, const SynthGroup* groups, int ngroups) {
   SynthArgs a;
-  a.N = ctx->N; a.H = ctx->H; a.Th = ctx->Th; a.Th2 = ctx->Th2; a.NM = ctx->NM;
+  a.N = ctx->N; a.H = ctx->H; a.Th = ctx->Th; a.Th2 = ctx->Th2; a.NM = ctx->NM; a.HB = ctx->HB;
   a.mstart = ctx->d_mstart; a.mlen = ctx->d_mlen; a.hs = ctx->d_s; a.leg = ctx->d_leg;
   a.rinv = ctx->d_r + (size_t)2 * ctx->N;
   int ng = 0;
@@ -315,7 +314,7 @@ int launch_synth_kind(lsd_ctx* ctx, const SynthGroup* groups, int ngroups) {
 template <int KIND>
 int launch_anal_kind(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
   AnalArgs a;
-  a.N = ctx->N; a.H = ctx->H; a.Th = ctx->Th; a.Th2 = ctx->Th2; a.NM = ctx->NM; a.Hr = ctx->Hr;
+  a.N = ctx->N; a.H = ctx->H; a.Th = ctx->Th; a.Th2 = ctx->Th2; a.NM = ctx->NM; a.HB = ctx->HB; a.Hr = ctx->Hr;
   a.mstart = ctx->d_mstart; a.mlen = ctx->d_mlen; a.hs = ctx->d_s; a.hm = ctx->d_m; a.leg = ctx->d_leg;
   int ng = 0;
   for (int i = 0; i < ngroups; ++i)

@@ -571,7 +571,7 @@ int lsd_eval(lsd_ctx* ctx) { return lsd_eval_marked(ctx, nullptr); }
 // FFT+products, the analysis and the tail
 int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   const size_t F = (size_t)ctx->N * ctx->H;
-  const size_t FF = (size_t)ctx->N * ctx->NM * 2 * ctx->Th2;
+  const size_t FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
   cplx* sp = ctx->d_spec;
   cplx* st = ctx->d_state;
   SpecArgs sa = spec_args(ctx);
