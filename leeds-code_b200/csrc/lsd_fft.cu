@@ -8,14 +8,15 @@
 // A real row of length Ph = 2 P2 is transformed as one complex FFT of length P2 of the
 // interleaved samples z[t] = x[2t] + i x[2t+1], with the usual split pre-/post-processing.
 //
-// Each complex FFT of length P2 = E G (G a power of two <= 32) runs in the registers of
-// G lanes: lane l holds E values.  The inverse is a lane-parallel radix-2 DIF over the G
-// lanes (shuffles), a twiddle w^(g k1) and an E-point DFT in registers; the forward
-// transform is its mirror (E-point DFT, twiddle, radix-2 DIT over the lanes).  Physical
-// samples come out of the inverse in a lane-permuted order and the forward transform
-// takes them back in that order, so the point-wise products never need a reordering.
-// Every shuffle runs with all 32 lanes of the warp: task loops advance warp by warp and
-// lanes without a task compute a dummy row whose results are dropped.
+// Each complex FFT of length P2 = E G (G a power of two <= 16) is two shared-memory
+// passes of in-register DFTs (the "four-step" split k = k1 + G k2, t = t1 + E t2):
+//   column pass: G threads per row, an E-point DFT over k2 and the twiddle w^(t1 k1);
+//   row pass:    E threads per row, a G-point DFT over k1.
+// Rows are padded by one complex per G values, so both passes read and write shared
+// memory without bank conflicts.  The inverse leaves the samples transposed (position
+// (G+1) t1 + t2 holds x[t1 + E t2]); the forward transform is the mirror image, takes
+// them back in that order and returns the spectrum in natural order, so the point-wise
+// products never need a reordering.
 //
 // The theta-Fourier rows are stored in half-row pairs ([n][h/2][m-counter][E/O][h%2],
 // four_off); one CTA of the fused kernel owns one pair (four full theta rows: the
@@ -33,14 +34,11 @@
 
 namespace {
 
-constexpr unsigned FULL = 0xffffffffu;
-
 struct FFTPlanDev {
-  int P2, Ph, M, NM, Th, Th2, HB, G, lgG;
+  int P2, Ph, M, NM, Th, Th2, HB;
   const double2* tw2;  // e^{+2 pi i k/P2}, k < P2
   const double2* twh;  // e^{+2 pi i k/Ph}, k < Ph
   const int* thm;      // m-counter -> bin
-  const int* bin2c;    // bin b < M -> m-counter
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -52,15 +50,6 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
 __device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 sub2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 shfl_xor2(double2 v, int m) {
-  return make_double2(__shfl_xor_sync(FULL, v.x, m), __shfl_xor_sync(FULL, v.y, m));
-}
-__device__ __forceinline__ double2 shfl2(double2 v, int src) {
-  return make_double2(__shfl_sync(FULL, v.x, src), __shfl_sync(FULL, v.y, src));
-}
-__device__ __forceinline__ int brev_bits(int l, int bits) {
-  return bits ? (int)(__brev((unsigned)l) >> (32 - bits)) : 0;
-}
 
 // In-register DFT of length N (mixed radix 2/3, decimation in time) with the twiddles of
 // the full length EF: w[j] = e^{+2 pi i j / EF} (a shared-memory table, read as
@@ -120,87 +109,80 @@ __device__ __forceinline__ void rdft(double2 (&x)[N], const double2* w) {
 }
 
 // Per-CTA shared tables of one transform length P2 = E G:
-//   wst[s][l] = e^{+2 pi i (l mod h) / (2h)}, h = 2^s    lane-stage twiddles, [s][lane]
-//   wlt[t][l] = e^{+2 pi i t l / P2}                     inter-step twiddles, [t][lane]
-//   twE[j]    = e^{+2 pi i j / E}                        register-DFT twiddles (broadcast)
-//   thm[c]    = FFT bin of m-counter c
-// Lane-indexed tables are read at consecutive addresses by consecutive lanes.
+//   tw[t1 G + k1] = e^{+2 pi i t1 k1 / P2}   column-pass twiddles (read by consecutive k1)
+//   twE[j] = e^{+2 pi i j / E},  twG[j] = e^{+2 pi i j / G}   register-DFT twiddles
+//   thm[c] = FFT bin of m-counter c
 struct FFTTabs {
-  double2* wst;
-  double2* wlt;
+  double2* tw;
   double2* twE;
+  double2* twG;
   int* thm;
 };
 
-__host__ __device__ __forceinline__ size_t fft_tab_bytes(int G, int E, int NM) {
-  return sizeof(double2) * ((size_t)5 * G + (size_t)E * G + E) + sizeof(int) * (size_t)((NM + 3) & ~3);
+__host__ __device__ __forceinline__ size_t fft_tab_bytes(int P2, int E, int G, int NM) {
+  return sizeof(double2) * ((size_t)P2 + E + G) + sizeof(int) * (size_t)((NM + 3) & ~3);
 }
 
 // carve the tables out of `base` (16-byte aligned) and fill them; ends with a barrier
-template <int E>
+template <int E, int G>
 __device__ __forceinline__ FFTTabs fft_tabs_init(unsigned char* base, const FFTPlanDev& pl) {
-  const int G = pl.G;
   FFTTabs t;
-  t.wst = (double2*)base;
-  t.wlt = t.wst + 5 * G;
-  t.twE = t.wlt + E * G;
-  t.thm = (int*)(t.twE + E);
-  for (int i = threadIdx.x; i < 5 * G; i += blockDim.x) {
-    const int s = i / G, l = i % G, h = 1 << s;
-    t.wst[i] = h < G ? __ldg(&pl.tw2[E * (l & (h - 1)) * (G / (2 * h))]) : make_double2(1.0, 0.0);
-  }
-  for (int i = threadIdx.x; i < E * G; i += blockDim.x) t.wlt[i] = __ldg(&pl.tw2[(i / G) * (i % G)]);
+  t.tw = (double2*)base;
+  t.twE = t.tw + E * G;
+  t.twG = t.twE + E;
+  t.thm = (int*)(t.twG + G);
+  for (int i = threadIdx.x; i < E * G; i += blockDim.x) t.tw[i] = __ldg(&pl.tw2[(i / G) * (i % G)]);
   for (int i = threadIdx.x; i < E; i += blockDim.x) t.twE[i] = __ldg(&pl.tw2[G * i]);
+  for (int i = threadIdx.x; i < G; i += blockDim.x) t.twG[i] = __ldg(&pl.tw2[E * i]);
   for (int i = threadIdx.x; i < pl.NM; i += blockDim.x) t.thm[i] = __ldg(&pl.thm[i]);
   __syncthreads();
   return t;
 }
 
-// Inverse (e^{+i}) FFT of length P2 = E G on G lanes.
-//   In:  v[k1] = Z[l + G k1]        (lane l holds every G-th bin from l)
-//   Out: v[t1] = x[t1 + E brev(l)]  (brev over log2 G bits)
-// x[t1 + E t2] = sum_k2 w_G^(t2 k2) w^(t1 k2) sum_k1 w_E^(t1 k1) Z[k2 + G k1].
-template <int E>
-__device__ __forceinline__ void wfft_inv(double2 (&v)[E], int l, const FFTPlanDev& pl, const FFTTabs& t) {
-  const int G = pl.G;
-  rdft<E, E, +1>(v, t.twE);
+// padded position of natural index k (one pad slot after every G values)
+template <int G>
+__device__ __forceinline__ int ppos(int k) { return k + k / G; }
+
+// Column pass over `nrows` rows of stride RS = E (G + 1).  SIGN +1 (inverse): E-point DFT
+// over k2 of Z[k1 + G k2], then the twiddle w^(t1 k1).  SIGN -1 (forward): the twiddle
+// w^(-t1 k1) first, then the E-point DFT.  In place.
+template <int E, int G, int SIGN>
+__device__ __forceinline__ void col_pass(double2* rows, int nrows, const FFTTabs& t) {
+  constexpr int RS = E * (G + 1);
+  for (int i = threadIdx.x; i < nrows * G; i += blockDim.x) {
+    const int r = i / G, k1 = i - r * G;
+    double2* col = rows + (size_t)r * RS + k1;
+    double2 v[E];
 #pragma unroll
-  for (int k = 1; k < E; ++k) v[k] = cmul(v[k], t.wlt[k * G + l]);
+    for (int k = 0; k < E; ++k) v[k] = col[k * (G + 1)];
+    if (SIGN < 0) {
 #pragma unroll
-  for (int s = 4; s >= 0; --s) {  // radix-2 DIF over the lanes (natural -> bit-reversed)
-    const int h = 1 << s;
-    if (h >= G) continue;
-    const bool up = l & h;
-    const double2 w = t.wst[s * G + l];
-#pragma unroll
-    for (int k = 0; k < E; ++k) {
-      const double2 p = shfl_xor2(v[k], h);
-      v[k] = up ? cmul(sub2(p, v[k]), w) : add2(v[k], p);
+      for (int k = 1; k < E; ++k) v[k] = cmulc(v[k], t.tw[k * G + k1]);
     }
+    rdft<E, E, SIGN>(v, t.twE);
+    if (SIGN > 0) {
+#pragma unroll
+      for (int k = 1; k < E; ++k) v[k] = cmul(v[k], t.tw[k * G + k1]);
+    }
+#pragma unroll
+    for (int k = 0; k < E; ++k) col[k * (G + 1)] = v[k];
   }
 }
 
-// Forward (e^{-i}) FFT, the mirror of wfft_inv.
-//   In:  v[t1] = x[t1 + E brev(l)]      Out: v[k1] = X[l + G k1]
-template <int E>
-__device__ __forceinline__ void wfft_fwd(double2 (&v)[E], int l, const FFTPlanDev& pl, const FFTTabs& t) {
-  const int G = pl.G;
+// Row pass: a G-point DFT over the G contiguous values of each (row, t1).  In place.
+template <int E, int G, int SIGN>
+__device__ __forceinline__ void row_pass(double2* rows, int nrows, const FFTTabs& t) {
+  constexpr int RS = E * (G + 1);
+  for (int i = threadIdx.x; i < nrows * E; i += blockDim.x) {
+    const int r = i / E, t1 = i - r * E;
+    double2* seg = rows + (size_t)r * RS + t1 * (G + 1);
+    double2 v[G];
 #pragma unroll
-  for (int s = 0; s <= 4; ++s) {  // radix-2 DIT over the lanes (bit-reversed -> natural)
-    const int h = 1 << s;
-    if (h >= G) continue;
-    const bool up = l & h;
-    const double2 w = t.wst[s * G + l];
+    for (int k = 0; k < G; ++k) v[k] = seg[k];
+    rdft<G, G, SIGN>(v, t.twG);
 #pragma unroll
-    for (int k = 0; k < E; ++k) {
-      const double2 send = up ? cmulc(v[k], w) : v[k];
-      const double2 recv = shfl_xor2(send, h);
-      v[k] = up ? sub2(recv, send) : add2(send, recv);
-    }
+    for (int k = 0; k < G; ++k) seg[k] = v[k];
   }
-#pragma unroll
-  for (int k = 1; k < E; ++k) v[k] = cmulc(v[k], t.wlt[k * G + l]);
-  rdft<E, E, -1>(v, t.twE);
 }
 
 // Half-spectrum packing for the c2r: Z[k] from Y[k] and conj(Y[P2-k]) (Y[P2] = Nyquist = 0;
@@ -240,34 +222,10 @@ __device__ __forceinline__ void stage_elem(double2* sp, const cplx* blk, const F
   sp[(p * 2 + jj) * M + t.thm[c]] = blk[i];
 }
 
-// Pack + inverse FFT of one row from a staged field.
-template <int E>
-__device__ __forceinline__ void row_c2r(double2 (&v)[E], const double2* sp, int jj, int side, int l,
-                                        const FFTPlanDev& pl, const FFTTabs& t) {
-  const int P2 = pl.P2, G = pl.G;
-#pragma unroll
-  for (int k1 = 0; k1 < E; ++k1) {
-    const int k = l + G * k1;
-    v[k1] = c2r_pack(k, row_bin(sp, k, jj, side, pl.M), row_bin(sp, P2 - k, jj, side, pl.M), pl);
-  }
-  wfft_inv<E>(v, l, pl, t);
-}
-
-// Forward FFT of one row of physical samples (lane order) + unpack of bins k = l + G k1.
-// Z[P2 - k] lives in lane G - l, register E - 1 - k1 (l > 0), or in lane 0, register E - k1.
-template <int E>
-__device__ __forceinline__ void row_r2c(double2 (&v)[E], int l, int lane0, const FFTPlanDev& pl, const FFTTabs& t) {
-  const int G = pl.G;
-  wfft_fwd<E>(v, l, pl, t);
-  double2 out[E];
-#pragma unroll
-  for (int k1 = 0; k1 < E; ++k1) {
-    const double2 za = shfl2(v[E - 1 - k1], lane0 + (G - l) % G);
-    const double2 zb = shfl2(v[(E - k1) % E], lane0);
-    out[k1] = r2c_unpack(l + G * k1, v[k1], l ? za : zb, pl);
-  }
-#pragma unroll
-  for (int k1 = 0; k1 < E; ++k1) v[k1] = out[k1];
+// bin b < M of a transformed row (natural order, padded) as a real-spectrum bin
+template <int G>
+__device__ __forceinline__ double2 row_unpack(const double2* row, int b, const FFTPlanDev& pl) {
+  return r2c_unpack(b, row[ppos<G>(b)], row[ppos<G>(b == 0 ? 0 : pl.P2 - b)], pl);
 }
 
 // ---- fused: 15 theta-Fourier inputs -> products -> 7 theta-Fourier outputs -------------
@@ -279,58 +237,65 @@ struct ProdConst {
 
 constexpr int NF_IN = 15, NF_OUT = 7;
 
-// grid (HB or 2 HB, N); RPC = 4 rows (both half-rows of the pair) or 2 (one half-row,
-// blockIdx.x = h, for long rows).  Shared memory: the physical rows [NF_IN][RPC][P2]
-// (double2, lane order), FPR staged fields [FPR][4][M], the FFT tables.
-template <int E>
-__global__ void __launch_bounds__(512) k_products(FFTPlanDev pl, int N, ProdConst pc, const cplx* four_in,
-                                                  cplx* four_out, int RPC, int FPR) {
+// grid (2 HB, N): one half-row h = blockIdx.x (its southern and northern theta row) per
+// CTA, 256 threads, two CTAs per SM so that one's memory waits overlap the other's work.
+// Every thread loads its share of all 15 input blocks into registers at the start (all
+// loads in flight at once); the blocks then pass through a double-buffered bin-order
+// stage into the padded rows [NF_IN][2][E (G+1)].
+constexpr int PROD_THREADS = 256;
+
+template <int E, int G>
+__global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int N, ProdConst pc,
+                                                              const cplx* four_in, cplx* four_out) {
+  constexpr int RS = E * (G + 1), P2 = E * G;
   extern __shared__ __align__(16) unsigned char psm[];
-  const int n = blockIdx.y;
-  const int hb = RPC == 4 ? blockIdx.x : blockIdx.x >> 1;
-  const int jj0 = RPC == 4 ? 0 : (blockIdx.x & 1);
-  const int P2 = pl.P2, G = pl.G, NM = pl.NM, M = pl.M, Th = pl.Th, Th2 = pl.Th2;
-  const int BLK = NM * 4;  // complex values of one field's (n, h/2) block
-  double2* phys = (double2*)psm;
-  double2* stage = phys + (size_t)NF_IN * RPC * P2;
-  const FFTTabs tabs = fft_tabs_init<E>((unsigned char*)(stage + (size_t)FPR * 4 * M), pl);
+  const int n = blockIdx.y, h = blockIdx.x, hb = h >> 1, jj = h & 1;
+  const int NM = pl.NM, M = pl.M, Th = pl.Th, Th2 = pl.Th2;
+  if (h >= Th2) return;  // padding half-row of an odd Th2
+  double2* rows = (double2*)psm;                 // [NF_IN][2][RS]
+  double2* stage = rows + (size_t)NF_IN * 2 * RS;  // [2 buffers][2 (E/O)][M]
+  const FFTTabs tabs = fft_tabs_init<E, G>((unsigned char*)(stage + (size_t)4 * M), pl);
+  const int BLK = NM * 4;                        // one field's (n, h/2) block
   const size_t fstride = (size_t)N * pl.HB * BLK;
-  const size_t boff = ((size_t)n * pl.HB + hb) * BLK;  // the CTA's block in every field
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int sgw = 32 / G, l = lane % G, lane0 = lane - l;
-  const int sg = warp * sgw + lane / G;
-  // ---- inverse transforms, FPR fields per round: stage their blocks (coalesced reads),
-  //      then sub-group sg takes (field f0 + sg / RPC, row sg % RPC)
-  for (int f0 = 0; f0 < NF_IN; f0 += FPR) {
-    const int nf = min(FPR, NF_IN - f0);
-    for (int i = threadIdx.x; i < nf * BLK; i += blockDim.x) {
-      const int fi = i / BLK;
-      stage_elem(stage + (size_t)fi * 4 * M, four_in + (size_t)(f0 + fi) * fstride + boff, tabs, M, i - fi * BLK);
-    }
-    __syncthreads();
-    const int fi = sg / RPC, r = sg % RPC;
-    const int jj = jj0 + (r >> 1), side = r & 1;
-    const bool act = fi < nf && 2 * hb + jj < Th2;
-    double2 v[E];
-    row_c2r<E>(v, stage + (size_t)(fi < nf ? fi : 0) * 4 * M, jj, side, l, pl, tabs);
-    if (act) {
-      double2* dst = phys + ((size_t)(f0 + fi) * RPC + r) * P2;
+  const size_t boff = ((size_t)n * pl.HB + hb) * BLK + jj;  // element (c, p) at boff + 2 (2c + p)
+  const int tid = threadIdx.x, NE = NM * 2;                 // (c, p) elements of this half-row
+  // ---- all loads first: element tid of every field (the rest, for NM > 128, later)
+  double2 pre[NF_IN];
 #pragma unroll
-      for (int e = 0; e < E; ++e) dst[e * G + l] = v[e];
+  for (int f = 0; f < NF_IN; ++f)
+    pre[f] = tid < NE ? four_in[(size_t)f * fstride + boff + 2 * tid] : make_double2(0.0, 0.0);
+  // ---- per field: bin-order stage (double buffer), then the packed half spectra
+#pragma unroll
+  for (int f = 0; f < NF_IN; ++f) {
+    double2* sp = stage + (size_t)(f & 1) * 2 * M;  // [p][M]
+    for (int i = tid; i < NE; i += PROD_THREADS) {
+      const double2 val = i == tid ? pre[f] : four_in[(size_t)f * fstride + boff + 2 * i];
+      sp[(i & 1) * M + tabs.thm[i >> 1]] = val;
     }
     __syncthreads();
+    for (int i = tid; i < 2 * P2; i += PROD_THREADS) {
+      const int side = i / P2, k = i - side * P2;
+      const double2 yk = k < M ? (side ? sub2(sp[k], sp[M + k]) : add2(sp[k], sp[M + k])) : make_double2(0.0, 0.0);
+      const int km = k == 0 ? P2 : P2 - k;
+      const double2 ym = km < M ? (side ? sub2(sp[km], sp[M + km]) : add2(sp[km], sp[M + km])) : make_double2(0.0, 0.0);
+      rows[(size_t)(f * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, yk, ym, pl);
+    }
   }
-  // ---- products at every point (row r, position i, part re/im), in place into slots 0..6
+  __syncthreads();
+  // ---- inverse FFTs of the 30 rows
+  col_pass<E, G, +1>(rows, NF_IN * 2, tabs);
+  __syncthreads();
+  row_pass<E, G, +1>(rows, NF_IN * 2, tabs);
+  __syncthreads();
+  // ---- products at every point (row side, sample position, part re/im), in place into 0..6
   const double scale = 1.0 / (double)pl.Ph;
-  for (int i = threadIdx.x; i < RPC * P2; i += blockDim.x) {
-    const int r = i / P2, pos = i - r * P2;
-    const int h = 2 * hb + jj0 + (r >> 1);
-    if (h >= Th2) continue;
-    const int j = row_theta(h, r & 1, Th);
+  for (int i = tid; i < 2 * P2; i += PROD_THREADS) {
+    const int r = i / P2, pos = ppos<G>(i - r * P2);
+    const int j = row_theta(h, r, Th);
     const double sn = pc.sn[j], cs = pc.gp[j];
     double2 v[NF_IN];
 #pragma unroll
-    for (int f = 0; f < NF_IN; ++f) v[f] = phys[((size_t)f * RPC + r) * P2 + pos];
+    for (int f = 0; f < NF_IN; ++f) v[f] = rows[(size_t)(f * 2 + r) * RS + pos];
     double2 out[NF_OUT];
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
@@ -361,165 +326,141 @@ __global__ void __launch_bounds__(512) k_products(FFTPlanDev pl, int N, ProdCons
       }
     }
 #pragma unroll
-    for (int q = 0; q < NF_OUT; ++q) phys[((size_t)q * RPC + r) * P2 + pos] = out[q];
+    for (int q = 0; q < NF_OUT; ++q) rows[(size_t)(q * 2 + r) * RS + pos] = out[q];
   }
   __syncthreads();
-  // ---- forward transforms: task = (output, row); bins b < M back into the row's slot
-  for (int t0 = warp * sgw; t0 < NF_OUT * RPC; t0 += nw * sgw) {
-    const int t = t0 + lane / G;
-    const int tt = t < NF_OUT * RPC ? t : t0;  // lanes without a task redo a valid one
-    const int q = tt / RPC, r = tt % RPC;
-    const bool act = t < NF_OUT * RPC && 2 * hb + jj0 + (r >> 1) < Th2;
-    double2* slot = phys + ((size_t)q * RPC + r) * P2;
-    double2 v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = slot[e * G + l];
-    row_r2c<E>(v, l, lane0, pl, tabs);
-    __syncwarp();
-    if (act) {
-#pragma unroll
-      for (int k1 = 0; k1 < E; ++k1) {
-        const int b = l + G * k1;
-        if (b < M) slot[b] = v[k1];
-      }
-    }
-    __syncwarp();
-  }
+  // ---- forward FFTs of the 14 product rows (spectrum back in natural order)
+  row_pass<E, G, -1>(rows, NF_OUT * 2, tabs);
   __syncthreads();
-  // ---- fold south/north into E/O and store the output blocks (contiguous per field)
-  const int njj = RPC / 2;
-  for (int i = threadIdx.x; i < NF_OUT * NM * 2 * njj; i += blockDim.x) {
-    const int q = i / (NM * 2 * njj), rem = i % (NM * 2 * njj);
-    const int c = rem / (2 * njj), p = (rem / njj) % 2, jr = rem % njj;
-    const int jj = jj0 + jr, h = 2 * hb + jj;
-    if (h >= Th2) continue;
+  col_pass<E, G, -1>(rows, NF_OUT * 2, tabs);
+  __syncthreads();
+  // ---- unpack bins, fold south/north into E/O, store
+  const bool equator = (Th & 1) && h == Th2 - 1;  // odd Th: the equator row is counted once
+  for (int i = tid; i < NF_OUT * NE; i += PROD_THREADS) {
+    const int q = i / NE, e = i - q * NE, c = e >> 1, p = e & 1;
     const int b = tabs.thm[c];
-    const double2 xs = phys[((size_t)q * RPC + 2 * jr) * P2 + b];
-    const double2 xn = phys[((size_t)q * RPC + 2 * jr + 1) * P2 + b];
+    const double2 xs = row_unpack<G>(rows + (size_t)(q * 2) * RS, b, pl);
+    const double2 xn = row_unpack<G>(rows + (size_t)(q * 2 + 1) * RS, b, pl);
     double2 val = p == 0 ? add2(xs, xn) : sub2(xs, xn);
-    if (p == 0 && (Th & 1) && h == Th2 - 1) { val.x *= 0.5; val.y *= 0.5; }  // odd Th: equator once
-    four_out[q * fstride + boff + (c * 2 + p) * 2 + jj] = val;
+    if (p == 0 && equator) { val.x *= 0.5; val.y *= 0.5; }
+    four_out[(size_t)q * fstride + boff + 2 * e] = val;
   }
 }
 
 // ---- standalone c2r: theta-Fourier -> phys [f][n][Ph][Th] -------------------------------
-// grid (HB, N, nfields), 128 threads: the four theta rows of a half-row pair, G lanes each
-// (sub-groups beyond the four rows redo row 0 and drop it).
-template <int E>
+// grid (HB, N, nfields), 128 threads: the four theta rows of a half-row pair.
+template <int E, int G>
 __global__ void __launch_bounds__(128) k_c2r(FFTPlanDev pl, int N, const cplx* four, double* phys) {
+  constexpr int RS = E * (G + 1), P2 = E * G;
   extern __shared__ __align__(16) unsigned char csm[];
   const int hb = blockIdx.x, n = blockIdx.y, f = blockIdx.z;
-  const int G = pl.G, Th = pl.Th, Th2 = pl.Th2, M = pl.M, NM = pl.NM;
-  double2* sp = (double2*)csm;  // [4][M]
-  const FFTTabs tabs = fft_tabs_init<E>((unsigned char*)(sp + 4 * M), pl);
+  const int Th = pl.Th, Th2 = pl.Th2, M = pl.M, NM = pl.NM;
+  double2* rows = (double2*)csm;    // [4][RS]
+  double2* sp = rows + 4 * RS;      // [4][M]
+  const FFTTabs tabs = fft_tabs_init<E, G>((unsigned char*)(sp + 4 * M), pl);
   const cplx* blk = four + (((size_t)f * N + n) * pl.HB + hb) * NM * 4;
   for (int i = threadIdx.x; i < NM * 4; i += blockDim.x) stage_elem(sp, blk, tabs, M, i);
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int l = lane % G;
-  const int grp = warp * (32 / G) + lane / G;
-  const int r = grp < 4 ? grp : 0;
-  const int jj = r >> 1, side = r & 1, h = 2 * hb + jj;
-  double2 v[E];
-  row_c2r<E>(v, sp, jj, side, l, pl, tabs);
-  const int j = row_theta(h, side, Th);
-  if (grp >= 4 || h >= Th2 || (side && j == h)) return;  // odd Th: the equator row is written once
+  for (int i = threadIdx.x; i < 4 * P2; i += blockDim.x) {
+    const int r = i / P2, k = i - r * P2;
+    rows[r * RS + ppos<G>(k)] = c2r_pack(k, row_bin(sp, k, r >> 1, r & 1, M), row_bin(sp, k == 0 ? P2 : P2 - k, r >> 1, r & 1, M), pl);
+  }
+  __syncthreads();
+  col_pass<E, G, +1>(rows, 4, tabs);
+  __syncthreads();
+  row_pass<E, G, +1>(rows, 4, tabs);
+  __syncthreads();
   double* dst = phys + ((size_t)f * N + n) * (size_t)pl.Ph * Th;
-  const int t2 = brev_bits(l, pl.lgG);
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const int t = e + E * t2;
-    dst[(size_t)(2 * t) * Th + j] = v[e].x;
-    dst[(size_t)(2 * t + 1) * Th + j] = v[e].y;
+  for (int i = threadIdx.x; i < 4 * P2; i += blockDim.x) {
+    const int r = i / P2, pos = i - r * P2;       // pos = (G+1) t1 + t2 without the pads
+    const int t1 = pos / G, t2 = pos - t1 * G, t = t1 + E * t2;
+    const int h = 2 * hb + (r >> 1), side = r & 1;
+    if (h >= Th2) continue;
+    const int j = row_theta(h, side, Th);
+    if (side && j == h) continue;  // odd Th: the equator row is written once
+    const double2 z = rows[r * RS + t1 * (G + 1) + t2];
+    dst[(size_t)(2 * t) * Th + j] = z.x;
+    dst[(size_t)(2 * t + 1) * Th + j] = z.y;
   }
 }
 
 // ---- standalone r2c: phys [f][n][Ph][Th] -> folded theta-Fourier --------------------------
-template <int E>
+template <int E, int G>
 __global__ void __launch_bounds__(128) k_r2c(FFTPlanDev pl, int N, const double* phys, cplx* four) {
+  constexpr int RS = E * (G + 1), P2 = E * G;
   extern __shared__ __align__(16) unsigned char rsm[];
   const int hb = blockIdx.x, n = blockIdx.y, f = blockIdx.z;
-  const int G = pl.G, Th = pl.Th, Th2 = pl.Th2, M = pl.M, NM = pl.NM;
-  double2* bins = (double2*)rsm;  // [4][M]
-  const FFTTabs tabs = fft_tabs_init<E>((unsigned char*)(bins + 4 * M), pl);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int l = lane % G, lane0 = lane - l;
-  const int grp = warp * (32 / G) + lane / G;
-  const int r = grp < 4 ? grp : 0;
-  const int jj = r >> 1, side = r & 1, h = 2 * hb + jj;
+  const int Th = pl.Th, Th2 = pl.Th2, NM = pl.NM;
+  double2* rows = (double2*)rsm;  // [4][RS]
+  const FFTTabs tabs = fft_tabs_init<E, G>((unsigned char*)(rows + 4 * RS), pl);
   const double scale = 1.0 / (double)pl.Ph;
-  const int j = row_theta(h < Th2 ? h : 2 * hb, side, Th);
   const double* src = phys + ((size_t)f * N + n) * (size_t)pl.Ph * Th;
-  const int t2 = brev_bits(l, pl.lgG);
-  double2 v[E];
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const int t = e + E * t2;
-    v[e] = make_double2(src[(size_t)(2 * t) * Th + j] * scale, src[(size_t)(2 * t + 1) * Th + j] * scale);
-  }
-  row_r2c<E>(v, l, lane0, pl, tabs);
-  if (grp < 4) {
-#pragma unroll
-    for (int k1 = 0; k1 < E; ++k1) {
-      const int b = l + G * k1;
-      if (b < M) bins[r * M + b] = v[k1];
-    }
+  for (int i = threadIdx.x; i < 4 * P2; i += blockDim.x) {
+    const int r = i / P2, pos = i - r * P2;
+    const int t1 = pos / G, t2 = pos - t1 * G, t = t1 + E * t2;
+    const int h = 2 * hb + (r >> 1);
+    const int j = row_theta(h < Th2 ? h : 2 * hb, r & 1, Th);
+    rows[r * RS + t1 * (G + 1) + t2] =
+        make_double2(src[(size_t)(2 * t) * Th + j] * scale, src[(size_t)(2 * t + 1) * Th + j] * scale);
   }
   __syncthreads();
+  row_pass<E, G, -1>(rows, 4, tabs);
+  __syncthreads();
+  col_pass<E, G, -1>(rows, 4, tabs);
+  __syncthreads();
   cplx* blk = four + (((size_t)f * N + n) * pl.HB + hb) * NM * 4;
-  for (int i = threadIdx.x; i < NM * 4; i += blockDim.x) {
-    const int c = i >> 2, p = (i >> 1) & 1, q = i & 1, hh = 2 * hb + q, b = tabs.thm[c];
+  for (int i = threadIdx.x; i < NM * 2; i += blockDim.x) {
+    const int c = i >> 1, q = i & 1, hh = 2 * hb + q, b = tabs.thm[c];
     if (hh >= Th2) continue;
-    const double2 xs = bins[(2 * q) * M + b], xn = bins[(2 * q + 1) * M + b];
-    double2 val = p == 0 ? add2(xs, xn) : sub2(xs, xn);
-    if (p == 0 && (Th & 1) && hh == Th2 - 1) { val.x *= 0.5; val.y *= 0.5; }
-    blk[i] = val;
+    const double2 xs = row_unpack<G>(rows + (2 * q) * RS, b, pl);
+    const double2 xn = row_unpack<G>(rows + (2 * q + 1) * RS, b, pl);
+    double2 ev = add2(xs, xn);
+    if ((Th & 1) && hh == Th2 - 1) { ev.x *= 0.5; ev.y *= 0.5; }
+    blk[(c * 2 + 0) * 2 + q] = ev;
+    blk[(c * 2 + 1) * 2 + q] = sub2(xs, xn);
   }
 }
 
 FFTPlanDev make_plan(lsd_ctx* ctx) {
   FFTPlanDev pl;
   pl.P2 = ctx->P2; pl.Ph = ctx->Ph; pl.M = ctx->M; pl.NM = ctx->NM; pl.Th = ctx->Th; pl.Th2 = ctx->Th2;
-  pl.HB = ctx->HB; pl.G = ctx->fftG; pl.lgG = 0;
-  while ((1 << pl.lgG) < pl.G) ++pl.lgG;
-  pl.tw2 = ctx->d_tw2; pl.twh = ctx->d_twh; pl.thm = ctx->d_thm; pl.bin2c = ctx->d_bin2c;
+  pl.HB = ctx->HB;
+  pl.tw2 = ctx->d_tw2; pl.twh = ctx->d_twh; pl.thm = ctx->d_thm;
   return pl;
 }
 
+// (E, G) pairs: P2 = 3 * 2^a or 9 * 2^a with the power of two split off up to 16
 template <class F>
-int dispatch_E(int E, F&& f) {
-  switch (E) {
-    case 3: return f(std::integral_constant<int, 3>());
-    case 6: return f(std::integral_constant<int, 6>());
-    case 9: return f(std::integral_constant<int, 9>());
-    case 12: return f(std::integral_constant<int, 12>());
-    case 18: return f(std::integral_constant<int, 18>());
-    case 24: return f(std::integral_constant<int, 24>());
-  }
+int dispatch_EG(int E, int G, F&& f) {
+#define LSD_EG(e, g) if (E == e && G == g) return f(std::integral_constant<int, e>(), std::integral_constant<int, g>());
+  LSD_EG(3, 1) LSD_EG(3, 2) LSD_EG(3, 4) LSD_EG(3, 8) LSD_EG(3, 16)
+  LSD_EG(9, 1) LSD_EG(9, 2) LSD_EG(9, 4) LSD_EG(9, 8) LSD_EG(9, 16)
+  LSD_EG(6, 16) LSD_EG(12, 16) LSD_EG(18, 16) LSD_EG(24, 16)
+#undef LSD_EG
   return -1;
 }
 
 }  // namespace
 
-// P2 = E G with G the power-of-two part of P2 capped at 32; E must be one of the
-// instantiated register-DFT lengths.
+// P2 = E G with G the power-of-two part of P2 capped at 16; (E, G) must be instantiated.
 bool lsd_fft_plan(lsd_ctx* c) {
   int G = 1;
-  while (G < 32 && c->P2 % (2 * G) == 0) G *= 2;
+  while (G < 16 && c->P2 % (2 * G) == 0) G *= 2;
   const int E = c->P2 / G;
   c->fftG = G;
   c->fftE = E;
-  return E == 3 || E == 6 || E == 9 || E == 12 || E == 18 || E == 24;
+  return dispatch_EG(E, G, [](auto, auto) { return 0; }) == 0;
 }
 
 int lsd_launch_c2r(lsd_ctx* ctx, const cplx* four, double* phys, int nfields) {
   FFTPlanDev pl = make_plan(ctx);
   dim3 grid(ctx->HB, ctx->N, nfields);
-  const size_t smem = sizeof(double2) * 4 * ctx->M + fft_tab_bytes(ctx->fftG, ctx->fftE, ctx->NM);
-  int rc = dispatch_E(ctx->fftE, [&](auto e) {
-    constexpr int E = decltype(e)::value;
-    cudaFuncSetAttribute(k_c2r<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_c2r<E><<<grid, 128, smem, ctx->stream>>>(pl, ctx->N, four, phys);
+  const size_t smem = sizeof(double2) * 4 * (ctx->fftE * (ctx->fftG + 1) + ctx->M) +
+                      fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
+  int rc = dispatch_EG(ctx->fftE, ctx->fftG, [&](auto e, auto g) {
+    constexpr int E = decltype(e)::value, G = decltype(g)::value;
+    cudaFuncSetAttribute(k_c2r<E, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_c2r<E, G><<<grid, 128, smem, ctx->stream>>>(pl, ctx->N, four, phys);
     return 0;
   });
   if (rc) return lsd_fail(ctx, LSD_EARG, "FFT length not supported");
@@ -532,11 +473,12 @@ int lsd_launch_c2r(lsd_ctx* ctx, const cplx* four, double* phys, int nfields) {
 int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields) {
   FFTPlanDev pl = make_plan(ctx);
   dim3 grid(ctx->HB, ctx->N, nfields);
-  const size_t smem = sizeof(double2) * 4 * ctx->M + fft_tab_bytes(ctx->fftG, ctx->fftE, ctx->NM);
-  int rc = dispatch_E(ctx->fftE, [&](auto e) {
-    constexpr int E = decltype(e)::value;
-    cudaFuncSetAttribute(k_r2c<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_r2c<E><<<grid, 128, smem, ctx->stream>>>(pl, ctx->N, phys, four);
+  const size_t smem = sizeof(double2) * 4 * ctx->fftE * (ctx->fftG + 1) +
+                      fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
+  int rc = dispatch_EG(ctx->fftE, ctx->fftG, [&](auto e, auto g) {
+    constexpr int E = decltype(e)::value, G = decltype(g)::value;
+    cudaFuncSetAttribute(k_r2c<E, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_r2c<E, G><<<grid, 128, smem, ctx->stream>>>(pl, ctx->N, phys, four);
     return 0;
   });
   if (rc) return lsd_fail(ctx, LSD_EARG, "FFT length not supported");
@@ -555,23 +497,14 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.d_qm1 = c.Pr / c.Pm;
   pc.sn = ctx->d_sn;
   pc.gp = ctx->d_gp;
-  // four rows (a half-row pair) per CTA when they fit, else two (one half-row); then as
-  // many staged input fields per round as the sub-groups can take and memory allows
-  const size_t budget = 224 * 1024, blk = sizeof(double2) * ctx->M * 4;
-  const size_t tabs = fft_tab_bytes(ctx->fftG, ctx->fftE, ctx->NM);
-  int RPC = 4;
-  size_t fixed = sizeof(double2) * NF_IN * RPC * ctx->P2 + tabs;
-  if (fixed + blk > budget) { RPC = 2; fixed = sizeof(double2) * NF_IN * RPC * ctx->P2 + tabs; }
-  if (fixed + blk > budget) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
-  const int nsg = 16 * (32 / ctx->fftG);
-  int FPR = std::min(NF_IN, nsg / RPC);
-  FPR = std::min<int>(FPR, (int)((budget - fixed) / blk));
-  const size_t smem = fixed + blk * FPR;
-  dim3 grid(RPC == 4 ? ctx->HB : 2 * ctx->HB, ctx->N);
-  int rc = dispatch_E(ctx->fftE, [&](auto e) {
-    constexpr int E = decltype(e)::value;
-    cudaFuncSetAttribute(k_products<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_products<E><<<grid, 512, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out, RPC, FPR);
+  const size_t smem = sizeof(double2) * ((size_t)NF_IN * 2 * ctx->fftE * (ctx->fftG + 1) + (size_t)4 * ctx->M) +
+                      fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
+  if (smem > 224 * 1024) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
+  dim3 grid(2 * ctx->HB, ctx->N);
+  int rc = dispatch_EG(ctx->fftE, ctx->fftG, [&](auto e, auto g) {
+    constexpr int E = decltype(e)::value, G = decltype(g)::value;
+    cudaFuncSetAttribute(k_products<E, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_products<E, G><<<grid, PROD_THREADS, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out);
     return 0;
   });
   if (rc) return lsd_fail(ctx, LSD_EARG, "FFT length not supported");
