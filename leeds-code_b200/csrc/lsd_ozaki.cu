@@ -153,10 +153,16 @@ struct OzProb {
   long long aofs;  // data digits of z-block 0 [zb][ks][slice][128 x 32]
 };
 
+// 2^e exactly (bit construction in the normal range)
+__device__ __forceinline__ double pow2i(int e) {
+  if (e >= -1022 && e <= 1023) return __longlong_as_double((long long)(e + 1023) << 52);
+  return ldexp(1.0, e);
+}
+
 // digits of x * 2^-e (|x| < 2^e): S signed 7-bit digits, most significant first
 __device__ __forceinline__ void oz_digits(double x, int e, int S, int8_t* d) {
-  const double y = ldexp(x, -e);
-  const long long X = (long long)ldexp(y, 7 * S);  // truncation, |X| < 2^(7S)
+  long long X = 0;
+  if (e > -1000) X = (long long)((x * pow2i(-e)) * pow2i(7 * S));  // exact scaling; truncation
   const long long mag = X < 0 ? -X : X;
   const int sgn = X < 0 ? -1 : 1;
 #pragma unroll
@@ -334,12 +340,12 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
             const double2 q = a.in0[g][(size_t)n * a.H + a.kidx[pr.kofs + k]];
             v = comp ? q.y : q.x;
           } else if (TYPE == OZ_VEC) {
-            const int nh = a.kidx[pr.kofs + k];
-            const double2 sv = a.in0[g][(size_t)n * a.H + nh], tv = a.in1[g][(size_t)n * a.H + nh];
             // theta: s llP_ (segment 1) + (t.im, -t.re) llsin1mP (segment 2);
             // phi:   t llP_ + (-s.im, s.re) llsin1mP        (transform.fftw3.F90:746-774)
-            if (seg1) v = comp == 0 ? sv.x : comp == 1 ? sv.y : comp == 2 ? tv.x : tv.y;
-            else v = comp == 0 ? tv.y : comp == 1 ? -tv.x : comp == 2 ? -sv.y : sv.x;
+            const bool use_t = seg1 ? comp >= 2 : comp < 2;
+            const double2 x = (use_t ? a.in1[g] : a.in0[g])[(size_t)n * a.H + a.kidx[pr.kofs + k]];
+            if (seg1) v = (comp & 1) ? x.y : x.x;
+            else v = comp == 0 ? x.y : comp == 1 ? -x.x : comp == 2 ? -x.y : x.x;
           } else if (TYPE == OZ_GRAD) {
             // theta: (C/r) P_ ; phi: i (C/r) sin1mP              (transform.fftw3.F90:955-1000)
             double2 cv = a.in0[g][(size_t)n * a.H + a.kidx[pr.kofs + k]];
@@ -353,12 +359,12 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
           } else {  // OZ_ST: segment 1 (gwllP_) on parity 1-p, segment 2 (gwllsin1mP) on parity p
             const int pp = seg1 ? 1 - p : p;
             const int j = seg1 ? k : k - pr.len1;
-            const size_t o = four_off(n, c, pp, j, a.NM, a.HB);
-            const double2 yt = a.in0[g][o], yp = a.in1[g][o];
             // s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re) ...
             // (transform.fftw3.F90:866-909)
-            if (seg1) v = comp == 0 ? yt.x : comp == 1 ? yt.y : comp == 2 ? yp.x : yp.y;
-            else v = comp == 0 ? yp.y : comp == 1 ? -yp.x : comp == 2 ? -yt.y : yt.x;
+            const bool use_ph = seg1 ? comp >= 2 : comp < 2;
+            const double2 y = (use_ph ? a.in1[g] : a.in0[g])[four_off(n, c, pp, j, a.NM, a.HB)];
+            if (seg1) v = (comp & 1) ? y.y : y.x;
+            else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
           }
         }
         int8_t d[OZ_MAXS];
@@ -394,6 +400,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
   extern __shared__ __align__(1024) uint8_t oz_smem[];
   __shared__ __align__(8) uint64_t full[OZ_STAGES], empty[OZ_STAGES], accf, tfree, fin;
   __shared__ uint32_t tbase;
+  __shared__ cplx* pbase[64];  // output base of each (re, im) row pair of the z-block
+  __shared__ int pzero[64];    // analysis: drop the imaginary part of m = 0 for this pair
   const int c = blockIdx.x, p = blockIdx.y, zb = blockIdx.z;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int S = a.S;
@@ -410,6 +418,19 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
     umma::fence_mbar_init();
   }
   if (warp == 0) umma::tmem_alloc(&tbase, 256);
+  if (tid < 64) {
+    const int Rr = zb * 128 + 2 * tid;
+    cplx* base = nullptr;
+    int zero = 0;
+    if (Rr < a.nrows) {
+      const int g = Rr / a.rows_per_group, n = (Rr % a.rows_per_group) / PER, comp = Rr % PER;
+      cplx* out = (comp < 2) ? a.out0[g] : a.out1[g];
+      base = OzT<TYPE>::anal ? out + (size_t)n * a.H : out + four_off(n, c, p, 0, a.NM, a.HB);
+      zero = TYPE == OZ_ST || a.zero_m0_im[g];
+    }
+    pbase[tid] = base;
+    pzero[tid] = zero;
+  }
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
@@ -469,42 +490,47 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
         break;
       }
       umma::fence_after_sync();
-      double acc[OZ_NC];
+      // diagonals d < 4 and 4 <= d < 8 combined exactly in int64 (Horner in 2^7):
+      //   sum_d D_d 2^(-7(d+2)) = G0 2^-35 + G1 2^-63; then the row and column scales
+      const int* fx = a.fexp + pr.fofs + ch * OZ_NC;
 #pragma unroll
-      for (int q = 0; q < OZ_NC; ++q) acc[q] = 0.0;
-      for (int d = S - 1; d >= 0; --d) {  // smallest diagonals first
-        int32_t v[OZ_NC];
-        umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * OZ_NC), v);
+      for (int c0 = 0; c0 < OZ_NC; c0 += 8) {
+        int32_t v[OZ_MAXS][8];
+#pragma unroll
+        for (int d = 0; d < OZ_MAXS; ++d)
+          if (d < S) umma::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * OZ_NC + c0), v[d]);
         umma::tmem_wait_ld();
-        const double wgt = ldexp(1.0, -7 * (d + 2));
 #pragma unroll
-        for (int q = 0; q < OZ_NC; ++q) acc[q] += (double)v[q] * wgt;
+        for (int q = 0; q < 8; ++q) {
+          long long g0 = 0, g1 = 0;
+#pragma unroll
+          for (int d = 0; d < 4; ++d) g0 = g0 * 128 + (d < S ? v[d][q] : 0);
+#pragma unroll
+          for (int d = 4; d < OZ_MAXS; ++d) g1 = g1 * 128 + (d < S ? v[d][q] : 0);
+          const double x = fma((double)g1, 0x1p-63, (double)g0 * 0x1p-35);
+          stg[tid * OZ_STG + c0 + q] = live ? x * pow2i(erow + fx[c0 + q]) : 0.0;
+        }
       }
       umma::fence_before_sync();
       umma::mbar_arrive(&tfree);  // tensor memory may take the next chunk
-      const int* fx = a.fexp + pr.fofs + ch * OZ_NC;
-#pragma unroll
-      for (int q = 0; q < OZ_NC; ++q) stg[tid * OZ_STG + q] = live ? ldexp(acc[q], erow + fx[q]) : 0.0;
       umma::bar_sync(1, 128);
       // coalesced stores: row pairs (re, im) x 32 columns
       for (int idx = tid; idx < 64 * OZ_NC; idx += 128) {
         const int pair = idx / OZ_NC, q = idx % OZ_NC;
-        const int Rr = zb * 128 + 2 * pair;
-        if (Rr >= a.nrows) continue;
-        const int g = Rr / a.rows_per_group, n = (Rr % a.rows_per_group) / PER, comp = Rr % PER;
+        cplx* base = pbase[pair];
+        if (!base) continue;
         double2 val = make_double2(stg[(2 * pair) * OZ_STG + q], stg[(2 * pair + 1) * OZ_STG + q]);
-        cplx* out = (comp < 2) ? a.out0[g] : a.out1[g];
         if (!OzT<TYPE>::anal) {
           const int j = ch * OZ_NC + q;
-          if (j < a.Th2) out[four_off(n, c, p, j, a.NM, a.HB)] = val;
+          if (j < a.Th2) base[(size_t)(j >> 1) * a.NM * 4 + (j & 1)] = val;
         } else {
           const int k = ch * OZ_NC + q;
           if (k < pr.nk) {
             const int nh = a.nhlist[pr.nhofs + k];
             // m = 0: s, t (and a scalar) keep no imaginary part; q keeps its own
             // (transform.fftw3.F90:599, 869, 902, 908)
-            if (a.hm[nh] == 0 && (TYPE == OZ_ST || a.zero_m0_im[g])) val.y = 0.0;
-            out[(size_t)n * a.H + nh] = val;
+            if (pzero[pair] && a.hm[nh] == 0) val.y = 0.0;
+            base[nh] = val;
           }
         }
       }
