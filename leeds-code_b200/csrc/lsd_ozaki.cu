@@ -170,6 +170,25 @@ __device__ __forceinline__ void oz_digits(double x, int e, int S, int8_t* d) {
     if (s < S) d[s] = (int8_t)(sgn * (int)((mag >> (7 * (S - 1 - s))) & 127));
 }
 
+// The same digits from 32-bit integers: y = x * sc (|y| < 1, exact power-of-two scaling),
+// the top S - L digits from trunc(|y| 2^(7(S-L))) and the low L = min(S, 4) digits from the
+// exact remainder scaled by 2^(7L); the sign is applied to every digit.
+__device__ __forceinline__ void oz_digits32(double x, double sc, int S, int (&d)[OZ_MAXS]) {
+  const double y = fabs(x) * sc;
+  const int L = S < 4 ? S : 4, SH = S - L;
+  const double yh = y * pow2i(7 * SH);
+  const int hi = (int)yh;                       // < 2^(7 SH) <= 2^28
+  const int lo = (int)((yh - (double)hi) * pow2i(7 * L));  // exact remainder, < 2^(7L)
+  const int m = x < 0.0 ? -1 : 0;               // conditional negation: (v ^ m) - m
+#pragma unroll
+  for (int s = 0; s < OZ_MAXS; ++s) {
+    int v = 0;
+    if (s < SH) v = (hi >> (7 * (SH - 1 - s))) & 127;
+    else if (s < S) v = (lo >> (7 * (S - 1 - s))) & 127;
+    d[s] = (v ^ m) - m;
+  }
+}
+
 __device__ __forceinline__ int oz_exponent(double maxabs) {
   if (!(maxabs > 0.0)) return -1000;
   int e;
@@ -177,11 +196,6 @@ __device__ __forceinline__ int oz_exponent(double maxabs) {
   return e;
 }
 
-// (row r, K byte b) of the 4-byte word at byte `addr` of a 128 x 32 K-major tile
-__device__ __forceinline__ void oz_word_pos(int addr, int& r, int& b) {
-  r = (addr >> 8) * 8 + ((addr & 127) >> 4);
-  b = ((addr >> 7) & 1) * 16 + (addr & 15);
-}
 
 // ---- table digits, once at set-up --------------------------------------------------------
 struct OzTabArgs {
@@ -309,30 +323,33 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
   __syncthreads();
   for (int r = tid; r < 128; r += 256)
     if (R0 + r < a.nrows) a.erow[(size_t)c * a.nrows + R0 + r] = e_pair[r / PER];
-  // ---- digits of both parities' A tiles
+  // ---- digits of both parities' A tiles: thread = (row r, K half kh), 16 values per K step
+  const int r = tid & 127, kh = tid >> 7;
+  const int R = R0 + r;
+  const bool live = R < a.nrows;
+  int g = 0, n = 0, comp = 0;
+  double sc = 0.0;
+  if (live) {
+    g = R / a.rows_per_group;
+    n = (R % a.rows_per_group) / PER;
+    comp = R % PER;
+    const int e = e_pair[r / PER];
+    sc = e > -1000 ? pow2i(-e) : 0.0;
+  }
+  const int toff = umma::tile_off(r, kh * 16);
   for (int p = 0; p < 2; ++p) {
     const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
     if (pr.nchunk == 0) continue;
     int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * a.S * 4096;
-    for (int w = tid; w < pr.nks * 1024; w += 256) {
-      const int ks = w >> 10, addr = (w & 1023) * 4;
-      int r, b;
-      oz_word_pos(addr, r, b);
-      const int R = R0 + r;
-      const bool live = R < a.nrows;
-      int g = 0, n = 0, comp = 0, e = -1000;
-      if (live) {
-        g = R / a.rows_per_group;
-        n = (R % a.rows_per_group) / PER;
-        comp = R % PER;
-        e = e_pair[r / PER];
-      }
-      uint32_t word[OZ_MAXS];
+    for (int ks = 0; ks < pr.nks; ++ks) {
+      uint32_t wd[OZ_MAXS][4];
 #pragma unroll
-      for (int s = 0; s < OZ_MAXS; ++s) word[s] = 0;
+      for (int s2 = 0; s2 < OZ_MAXS; ++s2)
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int k = ks * 32 + b + u;
+        for (int q = 0; q < 4; ++q) wd[s2][q] = 0u;
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const int k = ks * 32 + kh * 16 + u;
         double v = 0.0;
         if (live && k < pr.K) {
           const bool seg1 = k < pr.len1;
@@ -348,11 +365,12 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
             else v = comp == 0 ? x.y : comp == 1 ? -x.x : comp == 2 ? -x.y : x.x;
           } else if (TYPE == OZ_GRAD) {
             // theta: (C/r) P_ ; phi: i (C/r) sin1mP              (transform.fftw3.F90:955-1000)
-            double2 cv = a.in0[g][(size_t)n * a.H + a.kidx[pr.kofs + k]];
-            const double r1 = a.rinv[n];
-            cv.x *= r1; cv.y *= r1;
-            if (seg1) v = comp == 0 ? cv.x : comp == 1 ? cv.y : 0.0;
-            else v = comp == 2 ? -cv.y : comp == 3 ? cv.x : 0.0;
+            if (seg1 == (comp < 2)) {
+              double2 cv = a.in0[g][(size_t)n * a.H + a.kidx[pr.kofs + k]];
+              const double r1 = a.rinv[n];
+              cv.x *= r1; cv.y *= r1;
+              v = comp == 0 ? cv.x : comp == 1 ? cv.y : comp == 2 ? -cv.y : cv.x;
+            }
           } else if (TYPE == OZ_Q) {
             const double2 y = a.in0[g][four_off(n, c, p, k, a.NM, a.HB)];
             v = comp ? y.y : y.x;
@@ -367,13 +385,15 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
             else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
           }
         }
-        int8_t d[OZ_MAXS];
-        oz_digits(v, e, a.S, d);
+        int d[OZ_MAXS];
+        oz_digits32(v, sc, a.S, d);
 #pragma unroll
-        for (int s = 0; s < OZ_MAXS; ++s) word[s] |= ((uint32_t)(uint8_t)d[s]) << (8 * u);
+        for (int s2 = 0; s2 < OZ_MAXS; ++s2) wd[s2][u >> 2] |= ((uint32_t)d[s2] & 255u) << (8 * (u & 3));
       }
-      for (int s = 0; s < a.S; ++s)
-        *(uint32_t*)(Ablk + ((size_t)ks * a.S + s) * 4096 + addr) = word[s];
+#pragma unroll
+      for (int s2 = 0; s2 < OZ_MAXS; ++s2)
+        if (s2 < a.S)
+          *(uint4*)(Ablk + ((size_t)ks * a.S + s2) * 4096 + toff) = make_uint4(wd[s2][0], wd[s2][1], wd[s2][2], wd[s2][3]);
     }
   }
 }
@@ -402,6 +422,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
   __shared__ uint32_t tbase;
   __shared__ cplx* pbase[64];  // output base of each (re, im) row pair of the z-block
   __shared__ int pzero[64];    // analysis: drop the imaginary part of m = 0 for this pair
+  __shared__ double csc[OZ_NC];  // column scales 2^fexp of the current chunk
   const int c = blockIdx.x, p = blockIdx.y, zb = blockIdx.z;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int S = a.S;
@@ -482,17 +503,17 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
     // ---- epilogue: row tid of the z-block
     const int R = zb * 128 + tid;
     const bool live = R < a.nrows;
-    const int erow = live ? a.erow[(size_t)c * a.nrows + R] : 0;
+    // sum_d D_d 2^(-7(d+2)) = 2^(-7(S+1)) H with H = Horner over d in 2^7; the power of two
+    // and the row scale 2^erow are one factor
+    const double rsc = live ? pow2i(a.erow[(size_t)c * a.nrows + R] - 7 * (S + 1)) : 0.0;
     for (int ch = 0; ch < nch; ++ch) {
+      if (tid < OZ_NC) csc[tid] = pow2i(a.fexp[pr.fofs + ch * OZ_NC + tid]);
       const bool got = umma::mbar_wait(&accf, ch & 1, WAIT_ITERS);
       if (!umma::bar_and(1, 128, got)) {  // uniform over the 128 epilogue threads
         if (tid == 0) atomicExch(a.err, 1);
         break;
       }
       umma::fence_after_sync();
-      // diagonals d < 4 and 4 <= d < 8 combined exactly in int64 (Horner in 2^7):
-      //   sum_d D_d 2^(-7(d+2)) = G0 2^-35 + G1 2^-63; then the row and column scales
-      const int* fx = a.fexp + pr.fofs + ch * OZ_NC;
 #pragma unroll
       for (int c0 = 0; c0 < OZ_NC; c0 += 8) {
         int32_t v[OZ_MAXS][8];
@@ -502,13 +523,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
         umma::tmem_wait_ld();
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          long long g0 = 0, g1 = 0;
+          double hsum = (double)v[0][q];
 #pragma unroll
-          for (int d = 0; d < 4; ++d) g0 = g0 * 128 + (d < S ? v[d][q] : 0);
-#pragma unroll
-          for (int d = 4; d < OZ_MAXS; ++d) g1 = g1 * 128 + (d < S ? v[d][q] : 0);
-          const double x = fma((double)g1, 0x1p-63, (double)g0 * 0x1p-35);
-          stg[tid * OZ_STG + c0 + q] = live ? x * pow2i(erow + fx[c0 + q]) : 0.0;
+          for (int d = 1; d < OZ_MAXS; ++d)
+            if (d < S) hsum = fma(hsum, 128.0, (double)v[d][q]);
+          stg[tid * OZ_STG + c0 + q] = hsum * (rsc * csc[c0 + q]);
         }
       }
       umma::fence_before_sync();
