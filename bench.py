@@ -150,17 +150,49 @@ def phase_roofline(ctx, peaks, src):
         "predictor_solve": 5 * 3 * F,
         "corrector_solve": 5 * 5 * F,
     }
-    dom = max(ph, key=ph.get)
-    ms = ph[dom]
     hbm = peaks["hbm_gbs"]
+    per = {}
+    for k, ms in ph.items():
+        per[k] = {"ms": ms, "bytes": bytes_[k], "achieved_gbs": bytes_[k] / (ms * 1e-3) / 1e9,
+                  "frac": bytes_[k] / (ms * 1e-3) / 1e9 / hbm}
+    per["synthesis"]["fp64_equiv_tflops"] = syn_fl / (ph["synthesis"] * 1e-3) / 1e12
+    per["analysis"]["fp64_equiv_tflops"] = ana_fl / (ph["analysis"] * 1e-3) / 1e12
+    # the headline roofline is the largest single-kernel phase: the fused FFT + products
+    # kernel (synthesis and analysis are several launches each, listed in "phases")
+    dom = "fft_products"
+    ms = ph[dom]
     rf = {"kernel": dom, "bound": "hbm", "unit": "GB/s", "peak": hbm,
           "achieved": bytes_[dom] / (ms * 1e-3) / 1e9, "bytes_per_launch": bytes_[dom],
-          "ms_per_launch": ms, "peak_source": src}
+          "ms_per_launch": ms, "peak_source": src, "phases": per}
     rf["frac"] = rf["achieved"] / rf["peak"]
-    if dom in ("synthesis", "analysis"):
-        fl = syn_fl if dom == "synthesis" else ana_fl
-        rf["fp64_tflops"] = fl / (ms * 1e-3) / 1e12
     return ph, rf
+
+
+def energy_check(args, local_rank, nsteps):
+    """Energies of the tensor-core step against the plain FP64 step after nsteps steps from
+    the same seeded state (untimed); relative errors per energy."""
+    pkg = importlib.import_module("leeds-code_b200")
+    out = {}
+    for prec in ("fp64", "ozaki"):
+        cfg, _ = workload(args.workload, prec)
+        cfg.device = local_rank
+        ctx = pkg.Context(cfg)
+        ctx.load_fields(pkg.synthetic.boussinesq_state(cfg))
+        ctx.step(nsteps)
+        out[prec] = ctx.energies()
+        ctx.close()
+    f, o = out["fp64"], out["ozaki"]
+    keys = ("KE", "ME", "KE_ax", "ME_ax", "KE_dis", "ME_dis")
+    rel = {k: abs(o[k] - f[k]) / abs(f[k]) for k in keys}
+    return {"steps": nsteps, "max_rel_err": max(rel.values()), "rel_err": rel}
+
+
+# DRAM traffic per launch of the dominant kernel from an ncu capture of this benchmark
+# (dram__bytes_read.sum + dram__bytes_write.sum); see profiles/ for the command.
+NCU_TRAFFIC = {
+    "fft_products": {"kernel": "k_products<12,16>", "bytes": 761.12e6 + 313.09e6,
+                     "profile": "profiles/k_products_dynamo128.md"},
+}
 
 
 def cpu_oracle_step(cfg, threads):
@@ -294,7 +326,12 @@ def run_ours(args, rank, world, local_rank, dist):
         "phases_ms": ph,
         "energies_after": {k: r["energies"][k] for k in ("KE", "ME")},
     }
-    line["roofline"]["traffic"] = None
+    tr = NCU_TRAFFIC.get(r["roofline"]["kernel"]) if args.workload == "dynamo128" else None
+    line["roofline"]["traffic"] = tr["bytes"] if tr else None
+    if tr:
+        line["roofline_detail"]["traffic_source"] = tr
+    if world == 1 and "fp64" in good and "ozaki" in good and args.energy_steps > 0:
+        line["energy_check"] = energy_check(args, local_rank, args.energy_steps)
     if "fp64" in good and best != "fp64":
         f = good["fp64"]
         line["fp64_timesteps_per_s"] = world * f["steps"] / (f["ms"] * 1e-3)
@@ -325,6 +362,8 @@ def main():
     ap.add_argument("--precision", default="best", choices=["best", "fp64", "ozaki"])
     ap.add_argument("--workload", default="dynamo128", choices=["dynamo128", "parity32"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--energy-steps", type=int, default=1000,
+                    help="steps of the FP64 vs tensor-core energy comparison (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
