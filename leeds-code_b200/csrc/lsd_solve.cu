@@ -151,74 +151,22 @@ __global__ void k_tail(TailArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Column solves.  One thread per harmonic nh; the column x(n) = X[(n-1)*H + nh].
-// LU factors in solve layout [N][3KL+1][L], pivots [N][L]; Y bands [N][2KL+1][L].
+// Column solves.  A real column is the Re or the Im part of one harmonic nh of one field,
+// x(n) = X[(n * H + nh) * 2 + part]; the reference solves both parts with the same
+// factors (tim_invX, timestep.F90:566-588).  A warp owns one solve block: a degree l and
+// up to 16 orders m (32 real columns), so every factor it reads is a broadcast.  Columns
+// stream through register windows: KL + 1 values for the forward elimination with row
+// interchanges, 2 KL + 1 for the banded back substitution; intermediate columns go to
+// per-field scratch in global memory (L2 resident).  No shared memory, so every solve
+// block of a launch is resident at once.
 // ---------------------------------------------------------------------------------------
-// ---- real column kernels ------------------------------------------------------------
-// A thread owns one real column (the Re or the Im part of one harmonic): the reference
-// solves them with separate dgbtrs calls (timestep.F90:580-585) with the same factors.
-// A block handles one degree l (up to SBM orders m), so the factors of l are staged once
-// in shared memory and read as broadcasts; columns are x(n) = col[n * CW].
-
-// dgbtrs: forward sweep with row interchanges and the unit-lower band, backward dtbsv
-// with the upper band of width 2KL (LAPACK loop order).  ab: LAPACK band (3KL+1, N).
-template <int KL, int CW>
-__device__ void rcol_lu_solve(const double* ab, const int* piv, const double* rdiag, int N, double* x) {
-  constexpr int LD = 3 * KL + 1, KD = 2 * KL + 1, K2 = 2 * KL;
-#define LU(row, col) ab[(col) * LD + ((row) - 1)]  /* 1-based band row, 0-based column */
-  for (int c = 0; c < N - 1; ++c) {
-    const int p = piv[c] - 1;
-    double xc = x[p * CW];
-    if (p != c) { x[p * CW] = x[c * CW]; x[c * CW] = xc; }
-    const double temp = -xc;
-    const int lm = min(KL, N - 1 - c);
-#pragma unroll
-    for (int i = 1; i <= KL; ++i)
-      if (i <= lm) x[(c + i) * CW] = x[(c + i) * CW] + LU(KD + i, c) * temp;
-  }
-  for (int c = N - 1; c >= 0; --c) {
-    const double xc = x[c * CW] * rdiag[c];  // dtbsv divides; the reciprocal is taken once per block
-    x[c * CW] = xc;
-#pragma unroll
-    for (int t = 1; t <= K2; ++t)
-      if (c - t >= 0) x[(c - t) * CW] = x[(c - t) * CW] - xc * LU(K2 + 1 - t, c);
-  }
-#undef LU
-}
-
-// d(n) = c(n) + sum_j Y(KL+1+n-j, j) b(j), j ascending (tim_multY); Y band (2KL+1, N) in
-// shared memory, b in global memory with element stride bst, c and d in shared memory.
-template <int KL, int CW>
-__device__ void rcol_multY(const double* y, int N, const double* __restrict__ b, size_t bst,
-                           const double* c, double* d) {
-  constexpr int LDM = 2 * KL + 1;
-#pragma unroll 4
-  for (int n = 0; n < N; ++n) {
-    double acc = c[n * CW];
-#pragma unroll
-    for (int t = 0; t < LDM; ++t) {
-      const int j = n - KL + t;
-      if (j >= 0 && j < N) acc = acc + y[j * LDM + (LDM - 1 - t)] * __ldg(b + (size_t)j * bst);
-    }
-    d[n * CW] = acc;
-  }
-}
-
-// vel_gre_adjust (velocity.F90:445-465); g: Green's functions (N, 2), iG: invG (2, 2)
-template <int CW>
-__device__ void rcol_gre_adjust(const double* g, const double* iG, int N, double* x) {
-  const double bi = x[0], bo = x[(N - 1) * CW];
-  const double a = iG[0] * bi + iG[2] * bo, b = iG[1] * bi + iG[3] * bo;
-  for (int n = 0; n < N; ++n) x[n * CW] = x[n * CW] - a * g[n] - b * g[N + n];
-}
-
 struct StepArgs {
   int N, H, KL, L, nblk;
   const int* hl;
   const int* hm;
   const int* blk_l;    // [nblk] degree of each solve block
   const int* blk_nh;   // [nblk][SBM] harmonics of the block (-1 = none)
-  const double* lu;    // [fam][L][N][3KL+1] LAPACK factors
+  const double* lu;    // [fam][L][N][3KL+1] LAPACK band factors
   const int* ipiv;     // [fam][L][N]
   const double* y;     // [fam][L][N][2KL+1]
   const double* gre;   // [L][2][N]
@@ -226,7 +174,7 @@ struct StepArgs {
   cplx* state;  // [field][N][H]
   cplx* nl;
   cplx* sv;
-  cplx* work;   // [2][N][H] scratch columns
+  cplx* work;   // scratch: two columns sets per field, [2 field + k][N][H]
   double implicit;
   int cod_bc, comp_bc;
   double qi, qo, qi_comp, qo_comp;
@@ -234,74 +182,11 @@ struct StepArgs {
   double* red;  // corrector: [8] sums of squares
 };
 
-// Batched column I/O between global memory (element stride gst) and a shared column
-// (stride CW): IOB loads are issued before any store so that they overlap.
-constexpr int IOB = 8;
-template <int CW>
-__device__ __forceinline__ void col_load_save(const double* __restrict__ src, double* __restrict__ save, size_t gst,
-                                              double* col, int N) {
-  for (int n0 = 0; n0 < N; n0 += IOB) {
-    double v[IOB];
-#pragma unroll
-    for (int u = 0; u < IOB; ++u) v[u] = (n0 + u < N) ? src[(size_t)(n0 + u) * gst] : 0.0;
-#pragma unroll
-    for (int u = 0; u < IOB; ++u)
-      if (n0 + u < N) { col[(n0 + u) * CW] = v[u]; save[(size_t)(n0 + u) * gst] = v[u]; }
-  }
-}
-// col = c (src - save) ; save = src
-template <int CW>
-__device__ __forceinline__ void col_load_diff(const double* __restrict__ src, double* __restrict__ save, size_t gst,
-                                              double c, double* col, int N) {
-  for (int n0 = 0; n0 < N; n0 += IOB) {
-    double v[IOB], p[IOB];
-#pragma unroll
-    for (int u = 0; u < IOB; ++u) {
-      v[u] = (n0 + u < N) ? src[(size_t)(n0 + u) * gst] : 0.0;
-      p[u] = (n0 + u < N) ? save[(size_t)(n0 + u) * gst] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < IOB; ++u)
-      if (n0 + u < N) { col[(n0 + u) * CW] = c * (v[u] - p[u]); save[(size_t)(n0 + u) * gst] = v[u]; }
-  }
-}
-template <int CW>
-__device__ __forceinline__ void col_store(double* __restrict__ dst, size_t gst, const double* col, int N) {
-  for (int n0 = 0; n0 < N; n0 += IOB) {
-    double v[IOB];
-#pragma unroll
-    for (int u = 0; u < IOB; ++u) v[u] = (n0 + u < N) ? col[(n0 + u) * CW] : 0.0;
-#pragma unroll
-    for (int u = 0; u < IOB; ++u)
-      if (n0 + u < N) dst[(size_t)(n0 + u) * gst] = v[u];
-  }
-}
-// x += col, returning sum of col^2 (tim_addcorr order within the column)
-template <int CW>
-__device__ __forceinline__ double col_addcorr(double* __restrict__ x, size_t gst, const double* col, int N) {
-  double ss = 0.0;
-  for (int n0 = 0; n0 < N; n0 += IOB) {
-    double v[IOB], d[IOB];
-#pragma unroll
-    for (int u = 0; u < IOB; ++u) {
-      v[u] = (n0 + u < N) ? x[(size_t)(n0 + u) * gst] : 0.0;
-      d[u] = (n0 + u < N) ? col[(n0 + u) * CW] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < IOB; ++u)
-      if (n0 + u < N) {
-        ss = ss + d[u] * d[u];
-        x[(size_t)(n0 + u) * gst] = v[u] + d[u];
-      }
-  }
-  return ss;
-}
-
-// which solve this CTA row performs
+// which solve a warp row performs
 enum SolveJob { J_VTOR = 0, J_VPOL, J_COD, J_MTOR, J_MPOL, J_COMP, J_NJOB };
 
 constexpr int SBM = 16;        // orders m per solve block
-constexpr int SCW = 2 * SBM;   // real columns per block (Re, Im)
+constexpr int SOLVE_WARPS = 4; // solve blocks per CTA
 
 __device__ __forceinline__ int job_field(int job) {
   return job == J_VTOR ? LSD_VEL_TOR : job == J_VPOL ? LSD_VEL_POL : job == J_COD ? LSD_COD_C
@@ -312,111 +197,205 @@ __device__ __forceinline__ int job_family(int job) {
        : job == J_MTOR ? OP_MTOR : OP_MPOL;
 }
 
-// shared-memory plan of a solve block: columns [N][SCW], then the factors of degree l
-struct SolveSmem {
-  double* col;
-  double* lu1; int* piv1;   // main operator (XTor / XPol / XC / ...)
-  double* lu2; int* piv2;   // Green's operator (vel Pol only)
-  double* y;                // Y band of the main family
-  double* g;                // Green's functions (N, 2) + invG (4)
-  double* rd1; double* rd2;  // reciprocals of the U diagonals
+// dgbtrs forward part (LAPACK order): for c = 0..N-2 swap rows c and piv(c), then
+// x(c+i) -= L(c+i, c) x(c), i <= KL.  in(n) supplies right-hand-side rows in increasing
+// n (each once); out(c, y) receives the finished rows.  ab: band (3KL+1, N) per column.
+// rows fetched ahead of the elimination, so that their loads overlap
+constexpr int SPF = 8;
+
+template <int KL, class IN, class OUT>
+__device__ __forceinline__ void stream_forward(const double* __restrict__ ab, const int* __restrict__ piv, int N,
+                                               IN&& in, OUT&& out) {
+  constexpr int LD = 3 * KL + 1, KD = 2 * KL + 1;
+  double w[KL + 1];
+#pragma unroll
+  for (int i = 0; i <= KL; ++i) w[i] = i < N ? in(i) : 0.0;
+  for (int c0 = 0; c0 < N; c0 += SPF) {
+    double buf[SPF];  // rows c0 + KL + 1 + u, requested in increasing order
+#pragma unroll
+    for (int u = 0; u < SPF; ++u) buf[u] = c0 + KL + 1 + u < N ? in(c0 + KL + 1 + u) : 0.0;
+#pragma unroll
+    for (int u = 0; u < SPF; ++u) {
+      const int c = c0 + u;
+      if (c >= N) break;
+      if (c < N - 1) {
+        const int p = __ldg(piv + c) - 1 - c;  // 0..KL
+#pragma unroll
+        for (int i = 1; i <= KL; ++i)
+          if (p == i) { const double t = w[0]; w[0] = w[i]; w[i] = t; }
+        const double temp = -w[0];
+        const double* col = ab + (size_t)c * LD;
+#pragma unroll
+        for (int i = 1; i <= KL; ++i)
+          if (c + i < N) w[i] = w[i] + __ldg(col + KD + i - 1) * temp;
+      }
+      out(c, w[0]);
+#pragma unroll
+      for (int i = 0; i < KL; ++i) w[i] = w[i + 1];
+      w[KL] = buf[u];
+    }
+  }
+}
+
+// dtbsv (upper, non-unit, bandwidth 2KL; LAPACK column order) on the forward result:
+// for c = N-1..0: x(c) = y(c) / U(c, c); x(c-t) -= x(c) U(c-t, c), t <= 2KL.
+// in(n) supplies y rows in decreasing n; out(c, x) receives x(c) in decreasing c.
+template <int KL, class IN, class OUT>
+__device__ __forceinline__ void stream_backward(const double* __restrict__ ab, int N, IN&& in, OUT&& out) {
+  constexpr int LD = 3 * KL + 1, K2 = 2 * KL;
+  double w[K2 + 1];  // w[t] = pending y(c - t)
+#pragma unroll
+  for (int t = 0; t <= K2; ++t) w[t] = N - 1 - t >= 0 ? in(N - 1 - t) : 0.0;
+  for (int c0 = N - 1; c0 >= 0; c0 -= SPF) {
+    double buf[SPF];  // rows c0 - K2 - 1 - u
+#pragma unroll
+    for (int u = 0; u < SPF; ++u) buf[u] = c0 - K2 - 1 - u >= 0 ? in(c0 - K2 - 1 - u) : 0.0;
+#pragma unroll
+    for (int u = 0; u < SPF; ++u) {
+      const int c = c0 - u;
+      if (c < 0) break;
+      const double* col = ab + (size_t)c * LD;
+      double xc = w[0];
+      if (xc != 0.0) xc = xc / __ldg(col + K2);
+      out(c, xc);
+#pragma unroll
+      for (int t = 1; t <= K2; ++t) w[t] = w[t] - xc * __ldg(col + K2 - t);
+#pragma unroll
+      for (int t = 0; t < K2; ++t) w[t] = w[t + 1];
+      w[K2] = buf[u];
+    }
+  }
+}
+
+// (Y b)(n) + w(n) with the Y band (2KL+1, N) per column (tim_multY, timestep.F90:640-660),
+// b streamed through a window of 2KL+1 rows; rows are requested in increasing n.
+// Loads of right-hand-side inputs that a thread reads before it writes them (state,
+// nonlinear terms, the saved terms) go through the read-only path: no thread re-reads an
+// element after writing it, and the loads may then be hoisted above the saves.
+template <int KL>
+struct MultY {
+  const double* y;
+  const double* b;
+  size_t rst;
+  int N;
+  double win[2 * KL + 1];  // b(n - KL .. n + KL)
+  int next;                // next b row to load
+  __device__ void init(const double* y_, const double* b_, size_t rst_, int N_) {
+    y = y_; b = b_; rst = rst_; N = N_;
+#pragma unroll
+    for (int t = 0; t <= 2 * KL; ++t) {
+      const int j = t - KL;
+      win[t] = (j >= 0 && j < N) ? __ldg(b + (size_t)j * rst) : 0.0;
+    }
+    next = KL + 1;
+  }
+  // row n (called for n = 0, 1, 2, ... in order)
+  __device__ double apply(int n, double acc) {
+    constexpr int LDM = 2 * KL + 1;
+#pragma unroll
+    for (int t = 0; t < LDM; ++t) {
+      const int j = n - KL + t;
+      if (j >= 0 && j < N) acc = acc + __ldg(y + (size_t)j * LDM + (LDM - 1 - t)) * win[t];
+    }
+#pragma unroll
+    for (int t = 0; t < 2 * KL; ++t) win[t] = win[t + 1];
+    win[2 * KL] = next < N ? __ldg(b + (size_t)next * rst) : 0.0;
+    ++next;
+    return acc;
+  }
 };
 
-template <int KL>
-__device__ SolveSmem solve_smem(double* base, int N) {
-  SolveSmem m;
-  const int LD = 3 * KL + 1, LDM = 2 * KL + 1;
-  m.col = base;
-  m.lu1 = m.col + (size_t)N * SCW;
-  m.lu2 = m.lu1 + (size_t)N * LD;
-  m.y = m.lu2 + (size_t)N * LD;
-  m.g = m.y + (size_t)N * LDM;
-  m.rd1 = m.g + 2 * N + 4;
-  m.rd2 = m.rd1 + N;
-  m.piv1 = (int*)(m.rd2 + N);
-  m.piv2 = m.piv1 + N;
-  return m;
-}
-
-// stage the factors of degree l for this job into shared memory (whole block)
-template <int KL>
-__device__ void stage_factors(const StepArgs& a, const SolveSmem& m, int job, int l, bool with_y) {
-  const int N = a.N, L = a.L, LD = 3 * KL + 1, LDM = 2 * KL + 1;
-  const int fam = job_family(job);
-  const double* lu = a.lu + ((size_t)fam * L + l) * N * LD;
-  for (int i = threadIdx.x; i < N * LD; i += blockDim.x) m.lu1[i] = lu[i];
-  const int* pv = a.ipiv + ((size_t)fam * L + l) * N;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) m.piv1[i] = pv[i];
-  if (with_y) {
-    const double* y = a.y + ((size_t)fam * L + l) * N * LDM;
-    for (int i = threadIdx.x; i < N * LDM; i += blockDim.x) m.y[i] = y[i];
-  }
-  for (int i = threadIdx.x; i < N; i += blockDim.x) m.rd1[i] = 1.0 / lu[(size_t)i * LD + 2 * KL];
-  if (job == J_VPOL) {
-    const double* lu2 = a.lu + ((size_t)OP_VGRE * L + l) * N * LD;
-    for (int i = threadIdx.x; i < N * LD; i += blockDim.x) m.lu2[i] = lu2[i];
-    for (int i = threadIdx.x; i < N; i += blockDim.x) m.rd2[i] = 1.0 / lu2[(size_t)i * LD + 2 * KL];
-    const int* pv2 = a.ipiv + ((size_t)OP_VGRE * L + l) * N;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) m.piv2[i] = pv2[i];
-    const double* g = a.gre + (size_t)l * 2 * N;
-    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) m.g[i] = g[i];
-    if (threadIdx.x < 4) m.g[2 * N + threadIdx.x] = a.invg[(size_t)l * 4 + threadIdx.x];
-  }
-}
+__device__ __forceinline__ void warp_block_add(double v, double* target);
 
 // Predictor (velocity.F90:369-395, codensity.F90:224-234, magnetic.F90:370-408).
+// grid (ceil(nblk / SOLVE_WARPS), J_NJOB), SOLVE_WARPS warps per CTA.
 template <int KL>
-__global__ void __launch_bounds__(SCW) k_predictor(StepArgs a) {
-  extern __shared__ double smem_raw[];
+__global__ void __launch_bounds__(32 * SOLVE_WARPS) k_predictor(StepArgs a) {
   const int job = blockIdx.y;
   if (job == J_COMP && !a.comp) return;
-  const int b = blockIdx.x;
+  const int b = blockIdx.x * SOLVE_WARPS + (threadIdx.x >> 5);
+  if (b >= a.nblk) return;  // whole warps leave together
+  const int lane = threadIdx.x & 31;
   const int l = a.blk_l[b];
-  const bool zero = (job == J_COD || job == J_COMP);
-  if (l == 0 && !zero) {
-    // l = 0 of velocity / field: the predictor leaves N (zero) with zeroed boundary rows
-  }
-  const SolveSmem m = solve_smem<KL>(smem_raw, a.N);
-  stage_factors<KL>(a, m, job, l, true);
-  __syncthreads();
-  const int t = threadIdx.x;
-  const int nh = a.blk_nh[b * SBM + t / 2], part = t & 1;
+  const int nh = a.blk_nh[b * SBM + lane / 2], part = lane & 1;
   if (nh < 0) return;
-  const size_t F = (size_t)a.N * a.H;
-  const int N = a.N;
-  const int fld = job_field(job);
-  const size_t off = 2 * (size_t)nh + part, rst = 2 * (size_t)a.H;
+  const int N = a.N, L = a.L, fam = job_family(job), fld = job_field(job);
+  const bool zero = (job == J_COD || job == J_COMP);
+  const size_t F = (size_t)N * a.H, off = 2 * (size_t)nh + part, rst = 2 * (size_t)a.H;
+  constexpr int LD = 3 * KL + 1, LDM = 2 * KL + 1;
   double* X = (double*)(a.state + fld * F) + off;
   const double* Nn = (const double*)(a.nl + fld * F) + off;
   double* S = (double*)(a.sv + fld * F) + off;
-  double* W = m.col + t;
-  col_load_save<SCW>(Nn, S, rst, W, N);  // W = N ; save N
-  if (job == J_VPOL) {
-    // Pol := NPol ; zerobc ; invX(XGre) ; Pol := YPol vel_Pol + Pol ; zerobc ; invX(XPol) ; adjust
-    W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
-    if (l != 0) {
-      rcol_lu_solve<KL, SCW>(m.lu2, m.piv2, m.rd2, N, W);
-      rcol_multY<KL, SCW>(m.y, N, X, rst, W, W);
-    }
-    W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
-    if (l != 0) {
-      rcol_lu_solve<KL, SCW>(m.lu1, m.piv1, m.rd1, N, W);
-      rcol_gre_adjust<SCW>(m.g, m.g + 2 * N, N, W);
-    }
-  } else {
-    if (l != 0 || zero) rcol_multY<KL, SCW>(m.y, N, X, rst, W, W);
-    W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
-    if (zero && nh == 0 && part == 0) {  // cod_setbc / comp_setbc (codensity.F90:126-184)
-      int bc = job == J_COD ? a.cod_bc : a.comp_bc;
-      double qi = job == J_COD ? a.qi : a.qi_comp, qo = job == J_COD ? a.qo : a.qo_comp;
-      if (bc == 1 || bc == 2) W[0] = 1.0;
-      else if (bc == 3 || bc == 4) W[0] = qi;
-      W[(N - 1) * SCW] = (bc == 2 || bc == 4) ? qo : 0.0;
-    }
-    // vel_setbc_Tor: the l=1, m=0 inner value rot_omega*r_i is 0 (no inner-core rotation)
-    if (l != 0 || zero) rcol_lu_solve<KL, SCW>(m.lu1, m.piv1, m.rd1, N, W);
+  double* W1 = (double*)(a.work + (size_t)(2 * fld) * F) + off;
+  double* W2 = (double*)(a.work + (size_t)(2 * fld + 1) * F) + off;
+  const double* lu1 = a.lu + ((size_t)fam * L + l) * N * LD;
+  const int* pv1 = a.ipiv + ((size_t)fam * L + l) * N;
+  const double* y1 = a.y + ((size_t)fam * L + l) * N * LDM;
+  // boundary rows of the right-hand side (tim_zerobc; cod_setbc / comp_setbc for l = 0)
+  double bc0 = 0.0, bcN = 0.0;
+  if (zero && nh == 0 && part == 0) {
+    const int bc = job == J_COD ? a.cod_bc : a.comp_bc;
+    const double qi = job == J_COD ? a.qi : a.qi_comp, qo = job == J_COD ? a.qo : a.qo_comp;
+    if (bc == 1 || bc == 2) bc0 = 1.0;
+    else if (bc == 3 || bc == 4) bc0 = qi;
+    bcN = (bc == 2 || bc == 4) ? qo : 0.0;
   }
-  col_store<SCW>(X, rst, W, N);
+  auto rowbc = [&](int n, double v) { return n == 0 ? bc0 : (n == N - 1 ? bcN : v); };
+  if (job == J_VPOL) {
+    // Pol := NPol ; zerobc ; invX(XGre) ; Pol := YPol vel_Pol + Pol ; zerobc ; invX(XPol) ;
+    // vel_gre_adjust (velocity.F90:369-395, 445-465)
+    auto inA = [&](int n) {
+      const double v = __ldg(Nn + (size_t)n * rst);
+      S[(size_t)n * rst] = v;
+      return (n == 0 || n == N - 1) ? 0.0 : v;
+    };
+    if (l == 0) {
+      for (int n = 0; n < N; ++n) X[(size_t)n * rst] = inA(n);
+      return;
+    }
+    const double* lu2 = a.lu + ((size_t)OP_VGRE * L + l) * N * LD;
+    const int* pv2 = a.ipiv + ((size_t)OP_VGRE * L + l) * N;
+    stream_forward<KL>(lu2, pv2, N, inA, [&](int c, double v) { W1[(size_t)c * rst] = v; });
+    stream_backward<KL>(lu2, N, [&](int n) { return W1[(size_t)n * rst]; },
+                        [&](int c, double v) { W2[(size_t)c * rst] = v; });
+    MultY<KL> my;
+    my.init(y1, X, rst, N);
+    auto inB = [&](int n) {
+      const double v = my.apply(n, W2[(size_t)n * rst]);
+      return (n == 0 || n == N - 1) ? 0.0 : v;
+    };
+    double xN = 0.0, x0 = 0.0;
+    stream_forward<KL>(lu1, pv1, N, inB, [&](int c, double v) { W1[(size_t)c * rst] = v; });
+    stream_backward<KL>(lu1, N, [&](int n) { return W1[(size_t)n * rst]; }, [&](int c, double v) {
+      W2[(size_t)c * rst] = v;
+      if (c == N - 1) xN = v;
+      if (c == 0) x0 = v;
+    });
+    const double* g = a.gre + (size_t)l * 2 * N;
+    const double* iG = a.invg + (size_t)l * 4;
+    const double ca = iG[0] * x0 + iG[2] * xN, cb = iG[1] * x0 + iG[3] * xN;
+#pragma unroll 8
+    for (int n = 0; n < N; ++n) X[(size_t)n * rst] = W2[(size_t)n * rst] - ca * g[n] - cb * g[N + n];
+    return;
+  }
+  // other fields: X := Y X + N ; zerobc (+ setbc) ; invX
+  MultY<KL> my;
+  const bool solve = (l != 0 || zero);
+  if (solve) my.init(y1, X, rst, N);
+  auto inC = [&](int n) {
+    double v = __ldg(Nn + (size_t)n * rst);
+    S[(size_t)n * rst] = v;
+    if (solve) v = my.apply(n, v);
+    return rowbc(n, v);
+  };
+  // vel_setbc_Tor: the l = 1, m = 0 inner value rot_omega r_i is 0 (no inner-core rotation)
+  if (!solve) {
+    for (int n = 0; n < N; ++n) X[(size_t)n * rst] = inC(n);
+    return;
+  }
+  stream_forward<KL>(lu1, pv1, N, inC, [&](int c, double v) { W1[(size_t)c * rst] = v; });
+  stream_backward<KL>(lu1, N, [&](int n) { return W1[(size_t)n * rst]; },
+                      [&](int c, double v) { X[(size_t)c * rst] = v; });
 }
 
 __device__ __forceinline__ void warp_block_add(double v, double* target) {
@@ -427,44 +406,77 @@ __device__ __forceinline__ void warp_block_add(double v, double* target) {
 // Corrector (velocity.F90:413-439, codensity.F90:240-259, magnetic.F90:414-461)
 // red[] slots: 0 vTor, 1 vPol, 2 cod, 3 comp, 4 bTor, 5 bicTor, 6 bPol, 7 bicPol
 template <int KL>
-__global__ void __launch_bounds__(SCW) k_corrector(StepArgs a) {
-  extern __shared__ double smem_raw[];
+__global__ void __launch_bounds__(32 * SOLVE_WARPS) k_corrector(StepArgs a) {
   const int job = blockIdx.y;
   if (job == J_COMP && !a.comp) return;
-  const int b = blockIdx.x;
+  const int b = blockIdx.x * SOLVE_WARPS + (threadIdx.x >> 5);
+  if (b >= a.nblk) return;  // whole warps leave together
+  const int lane = threadIdx.x & 31;
   const int l = a.blk_l[b];
-  const SolveSmem m = solve_smem<KL>(smem_raw, a.N);
-  stage_factors<KL>(a, m, job, l, false);
-  __syncthreads();
-  const int t = threadIdx.x;
-  const int nh = a.blk_nh[b * SBM + t / 2], part = t & 1;
+  const int nh = a.blk_nh[b * SBM + lane / 2], part = lane & 1;
   double ss = 0.0, ssic = 0.0;
   if (nh >= 0) {
-    const size_t F = (size_t)a.N * a.H;
-    const int N = a.N;
-    const int fld = job_field(job);
-    const size_t off = 2 * (size_t)nh + part, rst = 2 * (size_t)a.H;
+    const int N = a.N, L = a.L, fam = job_family(job), fld = job_field(job);
+    const size_t F = (size_t)N * a.H, off = 2 * (size_t)nh + part, rst = 2 * (size_t)a.H;
+    constexpr int LD = 3 * KL + 1;
     double* X = (double*)(a.state + fld * F) + off;
     const double* Nn = (const double*)(a.nl + fld * F) + off;
     double* S = (double*)(a.sv + fld * F) + off;
-    double* W = m.col + t;
+    double* W1 = (double*)(a.work + (size_t)(2 * fld) * F) + off;
+    double* W2 = (double*)(a.work + (size_t)(2 * fld + 1) * F) + off;
+    const double* lu1 = a.lu + ((size_t)fam * L + l) * N * LD;
+    const int* pv1 = a.ipiv + ((size_t)fam * L + l) * N;
     const double c = a.implicit;
-    col_load_diff<SCW>(Nn, S, rst, c, W, N);  // nc = c (N - N_saved) ; N_saved = N
-    W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
-    if (job == J_VTOR && l == 1 && a.hm[nh] == 0 && part == 0) W[0] = 0.0 - X[0];  // vel_setbc_Tor, tim_it /= 0
+    // nc = c (N - N_saved) ; N_saved = N ; zerobc (tim_nlincorr, timestep.F90:696-715)
+    const bool tor10 = job == J_VTOR && l == 1 && a.hm[nh] == 0 && part == 0;  // vel_setbc_Tor
+    auto inC = [&](int n) {
+      const double v = __ldg(Nn + (size_t)n * rst), p = __ldg(S + (size_t)n * rst);
+      S[(size_t)n * rst] = v;
+      if (n == 0) return tor10 ? -X[0] : 0.0;
+      if (n == N - 1) return 0.0;
+      return c * (v - p);
+    };
+    // x += d ; dterr sum of d^2 (tim_addcorr, timestep.F90:717-737)
+    auto addcorr = [&](int n, double d) {
+      X[(size_t)n * rst] = X[(size_t)n * rst] + d;
+      ss = ss + d * d;
+    };
+    const bool zero = (job == J_COD || job == J_COMP);
+    double x0 = 0.0;
     if (job == J_VPOL) {
-      if (l != 0) rcol_lu_solve<KL, SCW>(m.lu2, m.piv2, m.rd2, N, W);
-      W[0] = 0.0; W[(N - 1) * SCW] = 0.0;
-      if (l != 0) {
-        rcol_lu_solve<KL, SCW>(m.lu1, m.piv1, m.rd1, N, W);
-        rcol_gre_adjust<SCW>(m.g, m.g + 2 * N, N, W);
+      if (l == 0) {
+        for (int n = 0; n < N; ++n) addcorr(n, inC(n));
+      } else {
+        const double* lu2 = a.lu + ((size_t)OP_VGRE * L + l) * N * LD;
+        const int* pv2 = a.ipiv + ((size_t)OP_VGRE * L + l) * N;
+        stream_forward<KL>(lu2, pv2, N, inC, [&](int cc, double v) { W1[(size_t)cc * rst] = v; });
+        stream_backward<KL>(lu2, N, [&](int n) { return W1[(size_t)n * rst]; },
+                            [&](int cc, double v) { W2[(size_t)cc * rst] = v; });
+        auto inD = [&](int n) { return (n == 0 || n == N - 1) ? 0.0 : W2[(size_t)n * rst]; };
+        double xN = 0.0;
+        stream_forward<KL>(lu1, pv1, N, inD, [&](int cc, double v) { W1[(size_t)cc * rst] = v; });
+        stream_backward<KL>(lu1, N, [&](int n) { return W1[(size_t)n * rst]; }, [&](int cc, double v) {
+          W2[(size_t)cc * rst] = v;
+          if (cc == N - 1) xN = v;
+          if (cc == 0) x0 = v;
+        });
+        const double* g = a.gre + (size_t)l * 2 * N;
+        const double* iG = a.invg + (size_t)l * 4;
+        const double ca = iG[0] * x0 + iG[2] * xN, cb = iG[1] * x0 + iG[3] * xN;
+#pragma unroll 8
+        for (int n = 0; n < N; ++n) addcorr(n, W2[(size_t)n * rst] - ca * g[n] - cb * g[N + n]);
       }
+    } else if (l != 0 || zero) {
+      stream_forward<KL>(lu1, pv1, N, inC, [&](int cc, double v) { W1[(size_t)cc * rst] = v; });
+      // the back substitution runs from n = N-1 down; tim_addcorr's sum runs up, so the
+      // corrections are kept and added in increasing n afterwards (same summation order)
+      stream_backward<KL>(lu1, N, [&](int n) { return W1[(size_t)n * rst]; },
+                          [&](int cc, double v) { W2[(size_t)cc * rst] = v; if (cc == 0) x0 = v; });
+#pragma unroll 8
+      for (int n = 0; n < N; ++n) addcorr(n, W2[(size_t)n * rst]);
     } else {
-      const bool zero = (job == J_COD || job == J_COMP);
-      if (l != 0 || zero) rcol_lu_solve<KL, SCW>(m.lu1, m.piv1, m.rd1, N, W);
+      for (int n = 0; n < N; ++n) addcorr(n, inC(n));
     }
-    const double x0 = W[0];
-    ss = col_addcorr<SCW>(X, rst, W, N);  // tim_addcorr
     if ((job == J_MTOR || job == J_MPOL) && l != 0) ssic = x0 * x0;  // inner-core copy (Ni = 1)
   }
   int slot = job == J_VTOR ? 0 : job == J_VPOL ? 1 : job == J_COD ? 2 : job == J_COMP ? 3 : job == J_MTOR ? 4 : 6;
@@ -635,19 +647,9 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
 namespace {
 template <int KL>
 void launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
-  dim3 g(ctx->nsblk, J_NJOB);
-  const int N = ctx->N;
-  size_t smem = sizeof(double) * ((size_t)N * SCW + 2 * (size_t)N * (3 * KL + 1) + (size_t)N * (2 * KL + 1) + 2 * N + 4 + 2 * N)
-              + sizeof(int) * 2 * N;
-  if (corr) {
-    cudaFuncSetAttribute(k_corrector<KL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_corrector<KL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    k_corrector<KL><<<g, SCW, smem, ctx->stream>>>(a);
-  } else {
-    cudaFuncSetAttribute(k_predictor<KL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_predictor<KL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    k_predictor<KL><<<g, SCW, smem, ctx->stream>>>(a);
-  }
+  dim3 g(ceil_div(ctx->nsblk, SOLVE_WARPS), J_NJOB);
+  if (corr) k_corrector<KL><<<g, 32 * SOLVE_WARPS, 0, ctx->stream>>>(a);
+  else k_predictor<KL><<<g, 32 * SOLVE_WARPS, 0, ctx->stream>>>(a);
 }
 
 int launch_step_kernel(lsd_ctx* ctx, const StepArgs& a, bool corr) {
