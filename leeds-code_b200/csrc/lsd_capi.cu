@@ -30,7 +30,7 @@ void free_ctx(lsd_ctx* ctx) {
   lsd_ozaki_free(ctx);
   void* ptrs[] = {ctx->d_sblk_l, ctx->d_sblk_nh, ctx->d_aperm, ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_bin2c, ctx->d_lm2nh,
                   ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,
-                  ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y,
+                  ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y, ctx->d_yt,
                   ctx->d_ipiv, ctx->d_ipivs, ctx->d_info, ctx->d_gre, ctx->d_gret, ctx->d_invg, ctx->d_state, ctx->d_nl,
                   ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red};
   for (void* p : ptrs)
@@ -336,6 +336,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   const size_t lus = (size_t)OP_NFAM * L * N * (3 * KL + 1);
   TRY(dalloc(ctx, &ctx->d_lu, lus)); TRY(dalloc(ctx, &ctx->d_lus, lus));
   TRY(dalloc(ctx, &ctx->d_y, (size_t)OP_NFAM * N * (2 * KL + 1) * L));
+  TRY(dalloc(ctx, &ctx->d_yt, (size_t)OP_NFAM * N * (2 * KL + 1) * L));
   TRY(dalloc(ctx, &ctx->d_ipiv, (size_t)OP_NFAM * L * N)); TRY(dalloc(ctx, &ctx->d_ipivs, (size_t)OP_NFAM * L * N));
   TRY(dalloc(ctx, &ctx->d_info, (size_t)OP_NFAM * L));
   TRY(dalloc(ctx, &ctx->d_gre, (size_t)L * 2 * N)); TRY(dalloc(ctx, &ctx->d_invg, (size_t)L * 4));

@@ -99,7 +99,7 @@ struct lsd_ctx {
   double *d_intr2dr = nullptr; // [N]
   // operators: LAPACK band LU [fam][L][N][3KL+1] + ipiv [fam][L][N]; Y bands
   // [fam][L][N][2KL+1]; (d_lus / d_ipivs: [fam][N][3KL+1][L] copies, l fastest)
-  double *d_lu = nullptr, *d_lus = nullptr, *d_y = nullptr;
+  double *d_lu = nullptr, *d_lus = nullptr, *d_y = nullptr, *d_yt = nullptr;
   int *d_ipiv = nullptr, *d_ipivs = nullptr, *d_info = nullptr;
   double *d_gre = nullptr;   // [L][2][N]
   double *d_gret = nullptr;  // [N][2][L]

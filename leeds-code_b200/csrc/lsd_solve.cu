@@ -151,30 +151,29 @@ __global__ void k_tail(TailArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Column solves.  A real column is the Re or the Im part of one harmonic nh of one field,
-// x(n) = X[(n * H + nh) * 2 + part]; the reference solves both parts with the same
-// factors (tim_invX, timestep.F90:566-588).  A warp owns one solve block: a degree l and
-// up to 16 orders m (32 real columns), so every factor it reads is a broadcast.  Columns
-// stream through register windows: KL + 1 values for the forward elimination with row
-// interchanges, 2 KL + 1 for the banded back substitution; intermediate columns go to
-// per-field scratch in global memory (L2 resident).  No shared memory, so every solve
-// block of a launch is resident at once.
+// Column solves.  A thread owns one harmonic nh of one field: its Re and Im columns
+// x(n) = X[n * H + nh] (complex), solved with the same factors like the reference's two
+// dgbtrs calls (tim_invX, timestep.F90:566-588).  Consecutive threads take consecutive
+// harmonics, so every row access of a warp is one contiguous 512-byte segment, and the
+// factors are read from copies with the degree l fastest ([fam][n][band][l]), so a
+// warp's factor reads are contiguous too.  Columns stream through register windows:
+// KL + 1 rows for the forward elimination with row interchanges, 2 KL + 1 for the banded
+// back substitution, right-hand-side rows fetched SPF rows ahead; intermediate columns
+// go to per-field scratch in global memory.
 // ---------------------------------------------------------------------------------------
 struct StepArgs {
-  int N, H, KL, L, nblk;
+  int N, H, KL, L;
   const int* hl;
   const int* hm;
-  const int* blk_l;    // [nblk] degree of each solve block
-  const int* blk_nh;   // [nblk][SBM] harmonics of the block (-1 = none)
-  const double* lu;    // [fam][L][N][3KL+1] LAPACK band factors
-  const int* ipiv;     // [fam][L][N]
-  const double* y;     // [fam][L][N][2KL+1]
-  const double* gre;   // [L][2][N]
+  const double* lus;   // [fam][N][3KL+1][L] LAPACK band factors, l fastest
+  const int* ipivs;    // [fam][N][L]
+  const double* yt;    // [fam][N][2KL+1][L] Y bands, l fastest
+  const double* gret;  // [N][2][L] Green's functions
   const double* invg;  // [L][4]
   cplx* state;  // [field][N][H]
   cplx* nl;
   cplx* sv;
-  cplx* work;   // scratch: two columns sets per field, [2 field + k][N][H]
+  cplx* work;   // scratch: two column sets per field, [2 field + k][N][H]
   double implicit;
   int cod_bc, comp_bc;
   double qi, qo, qi_comp, qo_comp;
@@ -182,11 +181,11 @@ struct StepArgs {
   double* red;  // corrector: [8] sums of squares
 };
 
-// which solve a warp row performs
+// which solve a grid row performs
 enum SolveJob { J_VTOR = 0, J_VPOL, J_COD, J_MTOR, J_MPOL, J_COMP, J_NJOB };
 
-constexpr int SBM = 16;        // orders m per solve block
-constexpr int SOLVE_WARPS = 4; // solve blocks per CTA
+constexpr int SOLVE_THREADS = 128;
+constexpr int SPF = 8;  // right-hand-side rows fetched ahead, so that their loads overlap
 
 __device__ __forceinline__ int job_field(int job) {
   return job == J_VTOR ? LSD_VEL_TOR : job == J_VPOL ? LSD_VEL_POL : job == J_COD ? LSD_COD_C
@@ -197,37 +196,55 @@ __device__ __forceinline__ int job_family(int job) {
        : job == J_MTOR ? OP_MTOR : OP_MPOL;
 }
 
+// band factor element (row r 0-based, column c) of this thread's degree: f[(c LD + r) L]
+struct Band {
+  const double* f;
+  const int* piv;
+  int L, LD;
+  __device__ double at(int r, int c) const { return __ldg(f + ((size_t)c * LD + r) * L); }
+  __device__ int pivot(int c) const { return __ldg(piv + (size_t)c * L); }
+};
+
+__device__ __forceinline__ double2 axpy2(double2 y, double a, double2 x) {  // y + a x
+  return make_double2(y.x + a * x.x, y.y + a * x.y);
+}
+
 // dgbtrs forward part (LAPACK order): for c = 0..N-2 swap rows c and piv(c), then
 // x(c+i) -= L(c+i, c) x(c), i <= KL.  in(n) supplies right-hand-side rows in increasing
-// n (each once); out(c, y) receives the finished rows.  ab: band (3KL+1, N) per column.
-// rows fetched ahead of the elimination, so that their loads overlap
-constexpr int SPF = 8;
-
+// n (each once); out(c, y) receives the finished rows.  The right-hand-side rows and the
+// factors of a batch of SPF rows are loaded before its arithmetic.
 template <int KL, class IN, class OUT>
-__device__ __forceinline__ void stream_forward(const double* __restrict__ ab, const int* __restrict__ piv, int N,
-                                               IN&& in, OUT&& out) {
-  constexpr int LD = 3 * KL + 1, KD = 2 * KL + 1;
-  double w[KL + 1];
+__device__ __forceinline__ void stream_forward(const Band& B, int N, IN&& in, OUT&& out) {
+  constexpr int KD = 2 * KL + 1;
+  double2 w[KL + 1];
 #pragma unroll
-  for (int i = 0; i <= KL; ++i) w[i] = i < N ? in(i) : 0.0;
+  for (int i = 0; i <= KL; ++i) w[i] = i < N ? in(i) : make_double2(0.0, 0.0);
   for (int c0 = 0; c0 < N; c0 += SPF) {
-    double buf[SPF];  // rows c0 + KL + 1 + u, requested in increasing order
+    double2 buf[SPF];  // rows c0 + KL + 1 + u, requested in increasing order
+    int pv[SPF];
+    double lf[SPF][KL];
 #pragma unroll
-    for (int u = 0; u < SPF; ++u) buf[u] = c0 + KL + 1 + u < N ? in(c0 + KL + 1 + u) : 0.0;
+    for (int u = 0; u < SPF; ++u) {
+      const int c = min(c0 + u, N - 1);
+      pv[u] = B.pivot(c);
+#pragma unroll
+      for (int i = 0; i < KL; ++i) lf[u][i] = B.at(KD + i, c);
+    }
+#pragma unroll
+    for (int u = 0; u < SPF; ++u) buf[u] = c0 + KL + 1 + u < N ? in(c0 + KL + 1 + u) : make_double2(0.0, 0.0);
 #pragma unroll
     for (int u = 0; u < SPF; ++u) {
       const int c = c0 + u;
       if (c >= N) break;
       if (c < N - 1) {
-        const int p = __ldg(piv + c) - 1 - c;  // 0..KL
+        const int p = pv[u] - 1 - c;  // 0..KL
 #pragma unroll
         for (int i = 1; i <= KL; ++i)
-          if (p == i) { const double t = w[0]; w[0] = w[i]; w[i] = t; }
-        const double temp = -w[0];
-        const double* col = ab + (size_t)c * LD;
+          if (p == i) { const double2 t = w[0]; w[0] = w[i]; w[i] = t; }
+        const double2 temp = make_double2(-w[0].x, -w[0].y);
 #pragma unroll
         for (int i = 1; i <= KL; ++i)
-          if (c + i < N) w[i] = w[i] + __ldg(col + KD + i - 1) * temp;
+          if (c + i < N) w[i] = axpy2(w[i], lf[u][i - 1], temp);
       }
       out(c, w[0]);
 #pragma unroll
@@ -240,26 +257,34 @@ __device__ __forceinline__ void stream_forward(const double* __restrict__ ab, co
 // dtbsv (upper, non-unit, bandwidth 2KL; LAPACK column order) on the forward result:
 // for c = N-1..0: x(c) = y(c) / U(c, c); x(c-t) -= x(c) U(c-t, c), t <= 2KL.
 // in(n) supplies y rows in decreasing n; out(c, x) receives x(c) in decreasing c.
+constexpr int SPB = 4;  // rows per batch of the back substitution
 template <int KL, class IN, class OUT>
-__device__ __forceinline__ void stream_backward(const double* __restrict__ ab, int N, IN&& in, OUT&& out) {
-  constexpr int LD = 3 * KL + 1, K2 = 2 * KL;
-  double w[K2 + 1];  // w[t] = pending y(c - t)
+__device__ __forceinline__ void stream_backward(const Band& B, int N, IN&& in, OUT&& out) {
+  constexpr int K2 = 2 * KL;
+  double2 w[K2 + 1];  // w[t] = pending y(c - t)
 #pragma unroll
-  for (int t = 0; t <= K2; ++t) w[t] = N - 1 - t >= 0 ? in(N - 1 - t) : 0.0;
-  for (int c0 = N - 1; c0 >= 0; c0 -= SPF) {
-    double buf[SPF];  // rows c0 - K2 - 1 - u
+  for (int t = 0; t <= K2; ++t) w[t] = N - 1 - t >= 0 ? in(N - 1 - t) : make_double2(0.0, 0.0);
+  for (int c0 = N - 1; c0 >= 0; c0 -= SPB) {
+    double2 buf[SPB];  // rows c0 - K2 - 1 - u
+    double uf[SPB][K2 + 1];
 #pragma unroll
-    for (int u = 0; u < SPF; ++u) buf[u] = c0 - K2 - 1 - u >= 0 ? in(c0 - K2 - 1 - u) : 0.0;
+    for (int u = 0; u < SPB; ++u) {
+      const int c = max(c0 - u, 0);
 #pragma unroll
-    for (int u = 0; u < SPF; ++u) {
+      for (int t = 0; t <= K2; ++t) uf[u][t] = B.at(K2 - t, c);  // uf[u][0] = U(c, c)
+    }
+#pragma unroll
+    for (int u = 0; u < SPB; ++u) buf[u] = c0 - K2 - 1 - u >= 0 ? in(c0 - K2 - 1 - u) : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int u = 0; u < SPB; ++u) {
       const int c = c0 - u;
       if (c < 0) break;
-      const double* col = ab + (size_t)c * LD;
-      double xc = w[0];
-      if (xc != 0.0) xc = xc / __ldg(col + K2);
+      const double d = uf[u][0];
+      const double2 xc = make_double2(w[0].x / d, w[0].y / d);
       out(c, xc);
+      const double2 mx = make_double2(-xc.x, -xc.y);
 #pragma unroll
-      for (int t = 1; t <= K2; ++t) w[t] = w[t] - xc * __ldg(col + K2 - t);
+      for (int t = 1; t <= K2; ++t) w[t] = axpy2(w[t], uf[u][t], mx);
 #pragma unroll
       for (int t = 0; t < K2; ++t) w[t] = w[t + 1];
       w[K2] = buf[u];
@@ -267,39 +292,39 @@ __device__ __forceinline__ void stream_backward(const double* __restrict__ ab, i
   }
 }
 
-// (Y b)(n) + w(n) with the Y band (2KL+1, N) per column (tim_multY, timestep.F90:640-660),
-// b streamed through a window of 2KL+1 rows; rows are requested in increasing n.
-// Loads of right-hand-side inputs that a thread reads before it writes them (state,
-// nonlinear terms, the saved terms) go through the read-only path: no thread re-reads an
-// element after writing it, and the loads may then be hoisted above the saves.
+// (Y b)(n) + w(n) with the Y band (2KL+1, N) (tim_multY, timestep.F90:640-660), b streamed
+// through a window of 2KL+1 rows; rows are requested in increasing n.  Right-hand-side
+// inputs that a thread reads before it writes them (state, nonlinear terms, the saved
+// terms) go through the read-only path: no thread re-reads an element after writing it,
+// so the loads may be hoisted above the saves.
 template <int KL>
 struct MultY {
-  const double* y;
-  const double* b;
+  const double* y;  // this degree's band: element (r, j) at y[(j LDM + r) L]
+  int L;
+  const double2* b;
   size_t rst;
   int N;
-  double win[2 * KL + 1];  // b(n - KL .. n + KL)
-  int next;                // next b row to load
-  __device__ void init(const double* y_, const double* b_, size_t rst_, int N_) {
-    y = y_; b = b_; rst = rst_; N = N_;
+  double2 win[2 * KL + 1];  // b(n - KL .. n + KL)
+  int next;
+  __device__ void init(const double* y_, int L_, const double2* b_, size_t rst_, int N_) {
+    y = y_; L = L_; b = b_; rst = rst_; N = N_;
 #pragma unroll
     for (int t = 0; t <= 2 * KL; ++t) {
       const int j = t - KL;
-      win[t] = (j >= 0 && j < N) ? __ldg(b + (size_t)j * rst) : 0.0;
+      win[t] = (j >= 0 && j < N) ? __ldg(b + (size_t)j * rst) : make_double2(0.0, 0.0);
     }
     next = KL + 1;
   }
-  // row n (called for n = 0, 1, 2, ... in order)
-  __device__ double apply(int n, double acc) {
+  __device__ double2 apply(int n, double2 acc) {
     constexpr int LDM = 2 * KL + 1;
 #pragma unroll
     for (int t = 0; t < LDM; ++t) {
       const int j = n - KL + t;
-      if (j >= 0 && j < N) acc = acc + __ldg(y + (size_t)j * LDM + (LDM - 1 - t)) * win[t];
+      if (j >= 0 && j < N) acc = axpy2(acc, __ldg(y + ((size_t)j * LDM + (LDM - 1 - t)) * L), win[t]);
     }
 #pragma unroll
     for (int t = 0; t < 2 * KL; ++t) win[t] = win[t + 1];
-    win[2 * KL] = next < N ? __ldg(b + (size_t)next * rst) : 0.0;
+    win[2 * KL] = next < N ? __ldg(b + (size_t)next * rst) : make_double2(0.0, 0.0);
     ++next;
     return acc;
   }
@@ -307,95 +332,125 @@ struct MultY {
 
 __device__ __forceinline__ void warp_block_add(double v, double* target);
 
-// Predictor (velocity.F90:369-395, codensity.F90:224-234, magnetic.F90:370-408).
-// grid (ceil(nblk / SOLVE_WARPS), J_NJOB), SOLVE_WARPS warps per CTA.
+// per-thread view of one field's columns and this degree's operators
+struct ColView {
+  double2 *X, *S, *W1, *W2;
+  const double2* Nn;
+  size_t rst;
+  Band B1, B2;       // main operator; Green's operator (poloidal velocity)
+  const double* y1;  // Y band of the main family
+  const double* g;   // Green's functions: element (n, k) at g[(n 2 + k) L]
+  double iG[4];
+};
+
 template <int KL>
-__global__ void __launch_bounds__(32 * SOLVE_WARPS) k_predictor(StepArgs a) {
+__device__ ColView col_view(const StepArgs& a, int job, int nh, int l) {
+  ColView v;
+  const int N = a.N, L = a.L, fam = job_family(job), fld = job_field(job);
+  constexpr int LD = 3 * KL + 1, LDM = 2 * KL + 1;
+  const size_t F = (size_t)N * a.H;
+  v.rst = a.H;
+  v.X = a.state + fld * F + nh;
+  v.Nn = a.nl + fld * F + nh;
+  v.S = a.sv + fld * F + nh;
+  v.W1 = a.work + (size_t)(2 * fld) * F + nh;
+  v.W2 = a.work + (size_t)(2 * fld + 1) * F + nh;
+  v.B1.f = a.lus + (size_t)fam * N * LD * L + l; v.B1.piv = a.ipivs + (size_t)fam * N * L + l;
+  v.B1.L = L; v.B1.LD = LD;
+  v.B2.f = a.lus + (size_t)OP_VGRE * N * LD * L + l; v.B2.piv = a.ipivs + (size_t)OP_VGRE * N * L + l;
+  v.B2.L = L; v.B2.LD = LD;
+  v.y1 = a.yt + (size_t)fam * N * LDM * L + l;
+  v.g = a.gret + l;
+  for (int i = 0; i < 4; ++i) v.iG[i] = job == J_VPOL ? __ldg(a.invg + (size_t)l * 4 + i) : 0.0;
+  return v;
+}
+
+// vel_gre_adjust (velocity.F90:445-465): coefficients of the two Green's functions
+__device__ __forceinline__ void gre_coeffs(const double* iG, double2 x0, double2 xN, double2& ca, double2& cb) {
+  ca = make_double2(iG[0] * x0.x + iG[2] * xN.x, iG[0] * x0.y + iG[2] * xN.y);
+  cb = make_double2(iG[1] * x0.x + iG[3] * xN.x, iG[1] * x0.y + iG[3] * xN.y);
+}
+
+// Predictor (velocity.F90:369-395, codensity.F90:224-234, magnetic.F90:370-408).
+// grid (ceil(H / SOLVE_THREADS), J_NJOB).
+template <int KL>
+__global__ void __launch_bounds__(SOLVE_THREADS) k_predictor(StepArgs a) {
   const int job = blockIdx.y;
   if (job == J_COMP && !a.comp) return;
-  const int b = blockIdx.x * SOLVE_WARPS + (threadIdx.x >> 5);
-  if (b >= a.nblk) return;  // whole warps leave together
-  const int lane = threadIdx.x & 31;
-  const int l = a.blk_l[b];
-  const int nh = a.blk_nh[b * SBM + lane / 2], part = lane & 1;
-  if (nh < 0) return;
-  const int N = a.N, L = a.L, fam = job_family(job), fld = job_field(job);
+  const int nh = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nh >= a.H) return;
+  const int l = a.hl[nh], N = a.N, L = a.L;
   const bool zero = (job == J_COD || job == J_COMP);
-  const size_t F = (size_t)N * a.H, off = 2 * (size_t)nh + part, rst = 2 * (size_t)a.H;
-  constexpr int LD = 3 * KL + 1, LDM = 2 * KL + 1;
-  double* X = (double*)(a.state + fld * F) + off;
-  const double* Nn = (const double*)(a.nl + fld * F) + off;
-  double* S = (double*)(a.sv + fld * F) + off;
-  double* W1 = (double*)(a.work + (size_t)(2 * fld) * F) + off;
-  double* W2 = (double*)(a.work + (size_t)(2 * fld + 1) * F) + off;
-  const double* lu1 = a.lu + ((size_t)fam * L + l) * N * LD;
-  const int* pv1 = a.ipiv + ((size_t)fam * L + l) * N;
-  const double* y1 = a.y + ((size_t)fam * L + l) * N * LDM;
+  const ColView v = col_view<KL>(a, job, nh, l);
+  const size_t rst = v.rst;
+  const double2 z2 = make_double2(0.0, 0.0);
   // boundary rows of the right-hand side (tim_zerobc; cod_setbc / comp_setbc for l = 0)
   double bc0 = 0.0, bcN = 0.0;
-  if (zero && nh == 0 && part == 0) {
+  if (zero && nh == 0) {
     const int bc = job == J_COD ? a.cod_bc : a.comp_bc;
     const double qi = job == J_COD ? a.qi : a.qi_comp, qo = job == J_COD ? a.qo : a.qo_comp;
     if (bc == 1 || bc == 2) bc0 = 1.0;
     else if (bc == 3 || bc == 4) bc0 = qi;
     bcN = (bc == 2 || bc == 4) ? qo : 0.0;
   }
-  auto rowbc = [&](int n, double v) { return n == 0 ? bc0 : (n == N - 1 ? bcN : v); };
+  auto w1 = [&](int c, double2 x) { v.W1[(size_t)c * rst] = x; };
+  auto r1 = [&](int n) { return v.W1[(size_t)n * rst]; };
   if (job == J_VPOL) {
     // Pol := NPol ; zerobc ; invX(XGre) ; Pol := YPol vel_Pol + Pol ; zerobc ; invX(XPol) ;
     // vel_gre_adjust (velocity.F90:369-395, 445-465)
     auto inA = [&](int n) {
-      const double v = __ldg(Nn + (size_t)n * rst);
-      S[(size_t)n * rst] = v;
-      return (n == 0 || n == N - 1) ? 0.0 : v;
+      const double2 x = __ldg(v.Nn + (size_t)n * rst);
+      v.S[(size_t)n * rst] = x;
+      return (n == 0 || n == N - 1) ? z2 : x;
     };
     if (l == 0) {
-      for (int n = 0; n < N; ++n) X[(size_t)n * rst] = inA(n);
+      for (int n = 0; n < N; ++n) v.X[(size_t)n * rst] = inA(n);
       return;
     }
-    const double* lu2 = a.lu + ((size_t)OP_VGRE * L + l) * N * LD;
-    const int* pv2 = a.ipiv + ((size_t)OP_VGRE * L + l) * N;
-    stream_forward<KL>(lu2, pv2, N, inA, [&](int c, double v) { W1[(size_t)c * rst] = v; });
-    stream_backward<KL>(lu2, N, [&](int n) { return W1[(size_t)n * rst]; },
-                        [&](int c, double v) { W2[(size_t)c * rst] = v; });
+    stream_forward<KL>(v.B2, N, inA, w1);
+    stream_backward<KL>(v.B2, N, r1, [&](int c, double2 x) { v.W2[(size_t)c * rst] = x; });
     MultY<KL> my;
-    my.init(y1, X, rst, N);
+    my.init(v.y1, L, v.X, rst, N);
     auto inB = [&](int n) {
-      const double v = my.apply(n, W2[(size_t)n * rst]);
-      return (n == 0 || n == N - 1) ? 0.0 : v;
+      const double2 x = my.apply(n, v.W2[(size_t)n * rst]);
+      return (n == 0 || n == N - 1) ? z2 : x;
     };
-    double xN = 0.0, x0 = 0.0;
-    stream_forward<KL>(lu1, pv1, N, inB, [&](int c, double v) { W1[(size_t)c * rst] = v; });
-    stream_backward<KL>(lu1, N, [&](int n) { return W1[(size_t)n * rst]; }, [&](int c, double v) {
-      W2[(size_t)c * rst] = v;
-      if (c == N - 1) xN = v;
-      if (c == 0) x0 = v;
+    double2 x0 = z2, xN = z2;
+    stream_forward<KL>(v.B1, N, inB, w1);
+    stream_backward<KL>(v.B1, N, r1, [&](int c, double2 x) {
+      v.W2[(size_t)c * rst] = x;
+      if (c == N - 1) xN = x;
+      if (c == 0) x0 = x;
     });
-    const double* g = a.gre + (size_t)l * 2 * N;
-    const double* iG = a.invg + (size_t)l * 4;
-    const double ca = iG[0] * x0 + iG[2] * xN, cb = iG[1] * x0 + iG[3] * xN;
+    double2 ca, cb;
+    gre_coeffs(v.iG, x0, xN, ca, cb);
 #pragma unroll 8
-    for (int n = 0; n < N; ++n) X[(size_t)n * rst] = W2[(size_t)n * rst] - ca * g[n] - cb * g[N + n];
+    for (int n = 0; n < N; ++n) {
+      const double g1 = __ldg(v.g + (size_t)(2 * n) * L), g2 = __ldg(v.g + (size_t)(2 * n + 1) * L);
+      const double2 x = v.W2[(size_t)n * rst];
+      v.X[(size_t)n * rst] = make_double2(x.x - ca.x * g1 - cb.x * g2, x.y - ca.y * g1 - cb.y * g2);
+    }
     return;
   }
   // other fields: X := Y X + N ; zerobc (+ setbc) ; invX
   MultY<KL> my;
   const bool solve = (l != 0 || zero);
-  if (solve) my.init(y1, X, rst, N);
+  if (solve) my.init(v.y1, L, v.X, rst, N);
   auto inC = [&](int n) {
-    double v = __ldg(Nn + (size_t)n * rst);
-    S[(size_t)n * rst] = v;
-    if (solve) v = my.apply(n, v);
-    return rowbc(n, v);
+    double2 x = __ldg(v.Nn + (size_t)n * rst);
+    v.S[(size_t)n * rst] = x;
+    if (solve) x = my.apply(n, x);
+    if (n == 0) return make_double2(bc0, 0.0);
+    if (n == N - 1) return make_double2(bcN, 0.0);
+    return x;
   };
   // vel_setbc_Tor: the l = 1, m = 0 inner value rot_omega r_i is 0 (no inner-core rotation)
   if (!solve) {
-    for (int n = 0; n < N; ++n) X[(size_t)n * rst] = inC(n);
+    for (int n = 0; n < N; ++n) v.X[(size_t)n * rst] = inC(n);
     return;
   }
-  stream_forward<KL>(lu1, pv1, N, inC, [&](int c, double v) { W1[(size_t)c * rst] = v; });
-  stream_backward<KL>(lu1, N, [&](int n) { return W1[(size_t)n * rst]; },
-                      [&](int c, double v) { X[(size_t)c * rst] = v; });
+  stream_forward<KL>(v.B1, N, inC, w1);
+  stream_backward<KL>(v.B1, N, r1, [&](int c, double2 x) { v.X[(size_t)c * rst] = x; });
 }
 
 __device__ __forceinline__ void warp_block_add(double v, double* target) {
@@ -404,80 +459,70 @@ __device__ __forceinline__ void warp_block_add(double v, double* target) {
 }
 
 // Corrector (velocity.F90:413-439, codensity.F90:240-259, magnetic.F90:414-461)
-// red[] slots: 0 vTor, 1 vPol, 2 cod, 3 comp, 4 bTor, 5 bicTor, 6 bPol, 7 bicPol
+// red[] slots: 0 vTor, 1 vPol, 2 cod, 3 comp, 4 bTor, 5 bicTor, 6 bPol, 7 bicPol.
+// The sum of squares of the corrections is accumulated per harmonic in the order the
+// back substitution produces them (n decreasing) and across harmonics by atomics.
 template <int KL>
-__global__ void __launch_bounds__(32 * SOLVE_WARPS) k_corrector(StepArgs a) {
+__global__ void __launch_bounds__(SOLVE_THREADS) k_corrector(StepArgs a) {
   const int job = blockIdx.y;
   if (job == J_COMP && !a.comp) return;
-  const int b = blockIdx.x * SOLVE_WARPS + (threadIdx.x >> 5);
-  if (b >= a.nblk) return;  // whole warps leave together
-  const int lane = threadIdx.x & 31;
-  const int l = a.blk_l[b];
-  const int nh = a.blk_nh[b * SBM + lane / 2], part = lane & 1;
+  const int nh = blockIdx.x * blockDim.x + threadIdx.x;
   double ss = 0.0, ssic = 0.0;
-  if (nh >= 0) {
-    const int N = a.N, L = a.L, fam = job_family(job), fld = job_field(job);
-    const size_t F = (size_t)N * a.H, off = 2 * (size_t)nh + part, rst = 2 * (size_t)a.H;
-    constexpr int LD = 3 * KL + 1;
-    double* X = (double*)(a.state + fld * F) + off;
-    const double* Nn = (const double*)(a.nl + fld * F) + off;
-    double* S = (double*)(a.sv + fld * F) + off;
-    double* W1 = (double*)(a.work + (size_t)(2 * fld) * F) + off;
-    double* W2 = (double*)(a.work + (size_t)(2 * fld + 1) * F) + off;
-    const double* lu1 = a.lu + ((size_t)fam * L + l) * N * LD;
-    const int* pv1 = a.ipiv + ((size_t)fam * L + l) * N;
+  if (nh < a.H) {
+    const int l = a.hl[nh], N = a.N, L = a.L;
+    const ColView v = col_view<KL>(a, job, nh, l);
+    const size_t rst = v.rst;
+    const double2 z2 = make_double2(0.0, 0.0);
     const double c = a.implicit;
     // nc = c (N - N_saved) ; N_saved = N ; zerobc (tim_nlincorr, timestep.F90:696-715)
-    const bool tor10 = job == J_VTOR && l == 1 && a.hm[nh] == 0 && part == 0;  // vel_setbc_Tor
+    const bool tor10 = job == J_VTOR && l == 1 && a.hm[nh] == 0;  // vel_setbc_Tor (Re part)
     auto inC = [&](int n) {
-      const double v = __ldg(Nn + (size_t)n * rst), p = __ldg(S + (size_t)n * rst);
-      S[(size_t)n * rst] = v;
-      if (n == 0) return tor10 ? -X[0] : 0.0;
-      if (n == N - 1) return 0.0;
-      return c * (v - p);
+      const double2 x = __ldg(v.Nn + (size_t)n * rst), p = __ldg(v.S + (size_t)n * rst);
+      v.S[(size_t)n * rst] = x;
+      if (n == 0) return tor10 ? make_double2(-v.X[0].x, 0.0) : z2;
+      if (n == N - 1) return z2;
+      return make_double2(c * (x.x - p.x), c * (x.y - p.y));
     };
     // x += d ; dterr sum of d^2 (tim_addcorr, timestep.F90:717-737)
-    auto addcorr = [&](int n, double d) {
-      X[(size_t)n * rst] = X[(size_t)n * rst] + d;
-      ss = ss + d * d;
+    auto addcorr = [&](int n, double2 d) {
+      const double2 x = v.X[(size_t)n * rst];
+      v.X[(size_t)n * rst] = make_double2(x.x + d.x, x.y + d.y);
+      ss = ss + d.x * d.x + d.y * d.y;
     };
+    auto w1 = [&](int cc, double2 x) { v.W1[(size_t)cc * rst] = x; };
+    auto r1 = [&](int n) { return v.W1[(size_t)n * rst]; };
     const bool zero = (job == J_COD || job == J_COMP);
-    double x0 = 0.0;
+    double2 x0 = z2;
     if (job == J_VPOL) {
       if (l == 0) {
         for (int n = 0; n < N; ++n) addcorr(n, inC(n));
       } else {
-        const double* lu2 = a.lu + ((size_t)OP_VGRE * L + l) * N * LD;
-        const int* pv2 = a.ipiv + ((size_t)OP_VGRE * L + l) * N;
-        stream_forward<KL>(lu2, pv2, N, inC, [&](int cc, double v) { W1[(size_t)cc * rst] = v; });
-        stream_backward<KL>(lu2, N, [&](int n) { return W1[(size_t)n * rst]; },
-                            [&](int cc, double v) { W2[(size_t)cc * rst] = v; });
-        auto inD = [&](int n) { return (n == 0 || n == N - 1) ? 0.0 : W2[(size_t)n * rst]; };
-        double xN = 0.0;
-        stream_forward<KL>(lu1, pv1, N, inD, [&](int cc, double v) { W1[(size_t)cc * rst] = v; });
-        stream_backward<KL>(lu1, N, [&](int n) { return W1[(size_t)n * rst]; }, [&](int cc, double v) {
-          W2[(size_t)cc * rst] = v;
-          if (cc == N - 1) xN = v;
-          if (cc == 0) x0 = v;
+        stream_forward<KL>(v.B2, N, inC, w1);
+        stream_backward<KL>(v.B2, N, r1, [&](int cc, double2 x) { v.W2[(size_t)cc * rst] = x; });
+        auto inD = [&](int n) { return (n == 0 || n == N - 1) ? z2 : v.W2[(size_t)n * rst]; };
+        double2 xN = z2;
+        stream_forward<KL>(v.B1, N, inD, w1);
+        stream_backward<KL>(v.B1, N, r1, [&](int cc, double2 x) {
+          v.W2[(size_t)cc * rst] = x;
+          if (cc == N - 1) xN = x;
+          if (cc == 0) x0 = x;
         });
-        const double* g = a.gre + (size_t)l * 2 * N;
-        const double* iG = a.invg + (size_t)l * 4;
-        const double ca = iG[0] * x0 + iG[2] * xN, cb = iG[1] * x0 + iG[3] * xN;
+        double2 ca, cb;
+        gre_coeffs(v.iG, x0, xN, ca, cb);
 #pragma unroll 8
-        for (int n = 0; n < N; ++n) addcorr(n, W2[(size_t)n * rst] - ca * g[n] - cb * g[N + n]);
+        for (int n = 0; n < N; ++n) {
+          const double g1 = __ldg(v.g + (size_t)(2 * n) * L), g2 = __ldg(v.g + (size_t)(2 * n + 1) * L);
+          const double2 x = v.W2[(size_t)n * rst];
+          addcorr(n, make_double2(x.x - ca.x * g1 - cb.x * g2, x.y - ca.y * g1 - cb.y * g2));
+        }
       }
     } else if (l != 0 || zero) {
-      stream_forward<KL>(lu1, pv1, N, inC, [&](int cc, double v) { W1[(size_t)cc * rst] = v; });
-      // the back substitution runs from n = N-1 down; tim_addcorr's sum runs up, so the
-      // corrections are kept and added in increasing n afterwards (same summation order)
-      stream_backward<KL>(lu1, N, [&](int n) { return W1[(size_t)n * rst]; },
-                          [&](int cc, double v) { W2[(size_t)cc * rst] = v; if (cc == 0) x0 = v; });
-#pragma unroll 8
-      for (int n = 0; n < N; ++n) addcorr(n, W2[(size_t)n * rst]);
+      stream_forward<KL>(v.B1, N, inC, w1);
+      stream_backward<KL>(v.B1, N, r1, [&](int cc, double2 x) { addcorr(cc, x); if (cc == 0) x0 = x; });
     } else {
       for (int n = 0; n < N; ++n) addcorr(n, inC(n));
     }
-    if ((job == J_MTOR || job == J_MPOL) && l != 0) ssic = x0 * x0;  // inner-core copy (Ni = 1)
+    if ((job == J_MTOR || job == J_MPOL) && l != 0) ssic = x0.x * x0.x + x0.y * x0.y;  // inner-core copy (Ni = 1)
   }
   int slot = job == J_VTOR ? 0 : job == J_VPOL ? 1 : job == J_COD ? 2 : job == J_COMP ? 3 : job == J_MTOR ? 4 : 6;
   warp_block_add(ss, a.red + slot);
@@ -559,11 +604,10 @@ SpecArgs spec_args(lsd_ctx* ctx) {
 
 StepArgs step_args(lsd_ctx* ctx) {
   StepArgs a;
-  a.N = ctx->N; a.H = ctx->H; a.KL = ctx->KL; a.L = ctx->L; a.nblk = ctx->nsblk;
+  a.N = ctx->N; a.H = ctx->H; a.KL = ctx->KL; a.L = ctx->L;
   a.hl = ctx->d_l; a.hm = ctx->d_m;
-  a.blk_l = ctx->d_sblk_l; a.blk_nh = ctx->d_sblk_nh;
-  a.lu = ctx->d_lu; a.ipiv = ctx->d_ipiv; a.y = ctx->d_y;
-  a.gre = ctx->d_gre; a.invg = ctx->d_invg;
+  a.lus = ctx->d_lus; a.ipivs = ctx->d_ipivs; a.yt = ctx->d_yt;
+  a.gret = ctx->d_gret; a.invg = ctx->d_invg;
   a.state = ctx->d_state; a.nl = ctx->d_nl; a.sv = ctx->d_sv;
   a.work = ctx->d_spec;
   a.implicit = ctx->cfg.implicit;
@@ -647,9 +691,9 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
 namespace {
 template <int KL>
 void launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
-  dim3 g(ceil_div(ctx->nsblk, SOLVE_WARPS), J_NJOB);
-  if (corr) k_corrector<KL><<<g, 32 * SOLVE_WARPS, 0, ctx->stream>>>(a);
-  else k_predictor<KL><<<g, 32 * SOLVE_WARPS, 0, ctx->stream>>>(a);
+  dim3 g(ceil_div(ctx->H, SOLVE_THREADS), J_NJOB);
+  if (corr) k_corrector<KL><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a);
+  else k_predictor<KL><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a);
 }
 
 int launch_step_kernel(lsd_ctx* ctx, const StepArgs& a, bool corr) {

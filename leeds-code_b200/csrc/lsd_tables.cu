@@ -317,16 +317,20 @@ __global__ void k_build_ops(int N, int KL, int L, const double* r, const double*
 #undef MB
 }
 
-// LAPACK layout [fam][L][N][3KL+1] -> solve layout [fam][N][3KL+1][L]
-__global__ void k_lu_transpose(int N, int KL, int L, const double* lu, const int* ipiv, double* lus, int* ipivs) {
+// LAPACK layouts [fam][L][N][band] -> solve layouts [fam][N][band][L] (degree fastest),
+// for the factors, the pivots and the Y bands
+__global__ void k_lu_transpose(int N, int KL, int L, const double* lu, const int* ipiv, const double* y,
+                               double* lus, int* ipivs, double* yt) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y;
   int fam = blockIdx.z;
   if (l >= L) return;
-  const int ld = 3 * KL + 1;
+  const int ld = 3 * KL + 1, ldm = 2 * KL + 1;
   const double* A = lu + (((size_t)fam * L + l) * N + j) * ld;
   for (int row = 0; row < ld; ++row) lus[(((size_t)fam * N + j) * ld + row) * L + l] = A[row];
   ipivs[((size_t)fam * N + j) * L + l] = ipiv[((size_t)fam * L + l) * N + j];
+  const double* Y = y + (((size_t)fam * L + l) * N + j) * ldm;
+  for (int row = 0; row < ldm; ++row) yt[(((size_t)fam * N + j) * ldm + row) * L + l] = Y[row];
 }
 
 // Green's functions and influence matrices (velocity.F90:148-168)
@@ -418,7 +422,7 @@ int lsd_build_operators(lsd_ctx* ctx) {
   dim3 g(ceil_div(L, 32), OP_NFAM);
   k_build_ops<<<g, 32, 0, s>>>(N, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap, P, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_info);
   dim3 gt(ceil_div(L, 64), N, OP_NFAM);
-  k_lu_transpose<<<gt, 64, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_lus, ctx->d_ipivs);
+  k_lu_transpose<<<gt, 64, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_lus, ctx->d_ipivs, ctx->d_yt);
   CUDA_TRY(cudaMemsetAsync(ctx->d_gret, 0, sizeof(double) * 2 * N * L, s));
   k_greens<<<ceil_div(L, 32), 32, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_gre, ctx->d_gret, ctx->d_invg, d_fail);
   ctx->launches += 3;
