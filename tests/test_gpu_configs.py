@@ -1,0 +1,157 @@
+"""Parity at the sizes of the other scope configurations.
+
+config[1]: the SHT round trip at lmax = mmax = 255 (L = M = 256, Th = 384, Ph = 768),
+64 shells x 8 scalar fields, coefficients N(0,1) l^-1 from the seed (l = 0: 1), through
+the device-resident batched entry points.  Per field: the synthesis against the oracle
+(field 0, all 64 shells), the analysis of the oracle's grid values against the oracle's
+analysis, and the round trip synthesis -> analysis of every field against the input.
+The round trip is exact only up to the reference's Gauss nodes (Newton stopped at
+1e-13, auxiliary/gauwts.f), about 3e-11 at this size for any arithmetic, so it is
+checked against the oracle's own round trip of field 0 and bounded by 5e-11 per field.
+Variants: the plain FP64 contraction and the tensor-core contraction at several slice
+counts (S int8 slices of 7 bits, about 7S bits of the FP64 mantissa).
+Tolerances, relative to the largest magnitude of the compared field:
+  FP64            synthesis, analysis, round trip vs the oracle's: 1e-12
+  tensor, S = 8   1e-13
+  tensor, S = 7   5e-12
+  tensor, S = 4   1e-6    (28-bit digits, about FP32)
+config[2]: batched banded solves at N = 257, KL = 4, one operator per degree l < 256 for
+4 fields, every (l, m) right-hand side (Re and Im columns, 4 x 32896 x 2), residual
+|A x - b| / |b| <= 1e-13 on a sample checked on the host.
+"""
+import importlib
+import time
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+pkg = importlib.import_module("leeds-code_b200")
+capi = pkg.capi
+
+
+def sht256_cfg(**kw):
+    return capi.template_config(L=256, M=256, Mp=1, N=64, timestep=1e-5, **kw)
+
+
+def seeded_spectra(nf, N, l, m, seed=1):
+    rng = np.random.default_rng(seed)
+    amp = np.where(l == 0, 1.0, 1.0 / np.maximum(l, 1))
+    re = rng.standard_normal((nf, N, l.size)) * amp
+    im = rng.standard_normal((nf, N, l.size)) * amp
+    im[:, :, m == 0] = 0.0
+    return re, im
+
+
+@pytest.fixture(scope="module")
+def sht256_reference():
+    o = ol.Oracle(sht256_cfg())
+    l, m, _ = o.harmonics()
+    re, im = seeded_spectra(8, o.N, l, m)
+    p0 = o.spec2phys(re[0], im[0])
+    a0 = o.phys2spec(p0)
+    return re, im, p0, a0
+
+
+def relerr(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,S,tol", [(capi.PREC_FP64, 0, 1e-12), (capi.PREC_OZAKI, 8, 1e-13),
+                                        (capi.PREC_OZAKI, 7, 5e-12), (capi.PREC_OZAKI, 4, 1e-6)])
+def test_sht_round_trip_lmax255(sht256_reference, prec, S, tol):
+    import torch
+    re, im, p0, a0 = sht256_reference
+    nf = re.shape[0]
+    g = pkg.Context(sht256_cfg(precision=prec, ozaki_slices=S))
+    N, H, Ph, Th = g.N, g.H, g.Ph, g.Th
+    spec = np.stack([re, im], axis=-1)  # [f][n][nh][2]
+    d_spec = torch.tensor(spec, device="cuda", dtype=torch.float64).contiguous()
+    d_phys = torch.empty((nf, N, Ph, Th), device="cuda", dtype=torch.float64)
+    d_back = torch.empty_like(d_spec)
+    g.sht_synth_device(nf, d_spec.data_ptr(), d_phys.data_ptr())
+    g.sht_analys_device(nf, d_phys.data_ptr(), d_back.data_ptr())
+    g.synchronize()
+    # wall time of round trips with the inputs resident in HBM (host-synchronised)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        g.sht_synth_device(nf, d_spec.data_ptr(), d_phys.data_ptr())
+        g.sht_analys_device(nf, d_phys.data_ptr(), d_back.data_ptr())
+    g.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / 3
+    phys = d_phys.cpu().numpy()
+    back = d_back.cpu().numpy()
+    # analysis of the oracle's grid values (field 0)
+    d_p0 = torch.tensor(p0, device="cuda", dtype=torch.float64).contiguous()
+    d_a0 = torch.empty((N, H, 2), device="cuda", dtype=torch.float64)
+    g.sht_analys_device(1, d_p0.data_ptr(), d_a0.data_ptr())
+    g.synchronize()
+    a0g = d_a0.cpu().numpy()
+    e_syn = relerr(phys[0], p0)
+    e_ana = max(relerr(a0g[..., 0], a0[0]), relerr(a0g[..., 1], a0[1]))
+    e_rt = [relerr(back[f], spec[f]) for f in range(nf)]
+    rt_oracle = np.stack([a0[0], a0[1]], axis=-1)
+    e_rt_vs = relerr(back[0], rt_oracle)
+    flops = 2 * 2 * 4 * H * (Th // 2) * N * nf  # complex x real MACs of synthesis + analysis
+    print("prec %d S %d: synthesis %.2e analysis %.2e, round trip vs oracle's %.2e (vs input max %.2e), "
+          "%.2f ms per round trip of %d fields (%.2f TF/s Legendre-equivalent, host-timed)"
+          % (prec, S, e_syn, e_ana, e_rt_vs, max(e_rt), ms, nf, flops / (ms * 1e-3) / 1e12))
+    assert e_syn <= tol, e_syn
+    assert e_ana <= tol, e_ana
+    assert e_rt_vs <= max(tol, 1e-12), e_rt_vs
+    assert max(e_rt) <= max(tol, 5e-11), e_rt
+    g.close()
+
+
+@pytest.mark.gpu
+def test_batched_banded_solves_n257():
+    import torch
+    import scipy.linalg.lapack as lapack
+    n, kl, L, nfield = 257, 4, 256, 4
+    H = L * L - (L - 1) * L // 2  # (l, m) pairs, m <= l < L
+    nmat = nfield * L
+    rng = np.random.default_rng(257)
+    ab = np.zeros((nmat, n, 3 * kl + 1))
+    ab[:, :, kl:] = rng.standard_normal((nmat, n, 2 * kl + 1))
+    ab[:, :, 2 * kl] += 6.0
+    # every (field, l, m) right-hand side, Re and Im columns; column r uses matrix map[r]
+    degs = np.concatenate([np.full(l + 1, l) for l in range(L)])
+    assert degs.size == H
+    rmap = np.concatenate([f * L + np.repeat(degs, 2) for f in range(nfield)]).astype(np.int32)
+    nrhs = rmap.size
+    g = pkg.Context(capi.template_config(L=16, M=16, Mp=1, N=9, timestep=1e-5))
+    d_ab = torch.tensor(ab, device="cuda", dtype=torch.float64)
+    d_ip = torch.zeros((nmat, n), device="cuda", dtype=torch.int32)
+    d_info = torch.zeros(nmat, device="cuda", dtype=torch.int32)
+    d_b = torch.randn((n, nrhs), device="cuda", dtype=torch.float64,
+                      generator=torch.Generator(device="cuda").manual_seed(5))
+    b = d_b.cpu().numpy()
+    d_map = torch.tensor(rmap, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.banded_factor_device(n, kl, nmat, d_ab.data_ptr(), d_ip.data_ptr(), d_info.data_ptr())
+    g.banded_solve_device(n, kl, nmat, d_ab.data_ptr(), d_ip.data_ptr(), nrhs, d_map.data_ptr(), d_b.data_ptr())
+    g.synchronize()
+    dt = time.perf_counter() - t0
+    assert (d_info.cpu().numpy() == 0).all()
+    x = d_b.cpu().numpy()
+    print("factor %d operators + %d right-hand sides (n=%d, kl=%d): %.2f ms" % (nmat, nrhs, n, kl, dt * 1e3))
+    sample = rng.choice(nrhs, 300, replace=False)
+    worst = 0.0
+    for r in sample:
+        k = rmap[r]
+        A = np.zeros((n, n))
+        for j in range(n):
+            for i in range(max(0, j - kl), min(n, j + kl + 1)):
+                A[i, j] = ab[k, j, 2 * kl + i - j]
+        res = np.abs(A @ x[:, r] - b[:, r]).max() / np.abs(b[:, r]).max()
+        worst = max(worst, res)
+    assert worst <= 1e-13, worst
+    # and the factors equal LAPACK's for a few operators
+    lu_g = d_ab.cpu().numpy()
+    for k in (0, 255, 511, 1023):
+        lu_l, ip_l, info = lapack.dgbtrf(ab[k].T.copy(), kl, kl)
+        assert np.abs(lu_g[k].T - lu_l).max() <= 1e-13 * np.abs(lu_l).max()
+    g.close()
