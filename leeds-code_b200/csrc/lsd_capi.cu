@@ -349,7 +349,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   CTRY(cudaMemset(ctx->d_sv, 0, sizeof(cplx) * LSD_NFIELD * F));
   ctx->nspec = 13;
   TRY(dalloc(ctx, &ctx->d_spec, (size_t)ctx->nspec * F));
-  ctx->nfour = 15;
+  ctx->nfour = 22;  // 15 synthesised fields (FFT layout) + 7 products (analysis layout)
   TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * ctx->HB * NM * 4));
   TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));

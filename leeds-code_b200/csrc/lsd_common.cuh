@@ -52,6 +52,12 @@ enum AnalKind {
 __host__ __device__ __forceinline__ size_t four_off(int n, int c, int p, int h, int NM, int HB) {
   return ((((size_t)n * HB + (h >> 1)) * NM + c) * 2 + p) * 2 + (h & 1);
 }
+// theta-Fourier rows on their way to the analysis (written by the products and r2c
+// kernels): [m-counter c][n][p = E/O][h] per field, so one (c, n) row is contiguous along h
+// (the analysis contraction runs over h).  Same field size as four_off's.
+__host__ __device__ __forceinline__ size_t four_off_a(int n, int c, int p, int h, int N, int Th2) {
+  return (((size_t)c * N + n) * 2 + p) * Th2 + h;
+}
 
 struct SynthGroup {
   int kind;

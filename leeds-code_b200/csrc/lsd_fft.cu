@@ -26,7 +26,8 @@
 //   -(Pr/Pm) u . grad C                     (nonlinear.F90:269-272)
 //   u x B                                   (nonlinear.F90:421-430)
 // at every grid point in shared memory, transforms the 7 results back and writes their
-// folded theta-Fourier rows.  Physical-space fields never touch HBM.
+// folded theta-Fourier rows in the analysis layout (four_off_a).  Physical-space fields
+// never touch HBM.
 #include <algorithm>
 #include <type_traits>
 
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
     const double2 xn = row_unpack<G>(rows + (size_t)(q * 2 + 1) * RS, b, pl);
     double2 val = p == 0 ? add2(xs, xn) : sub2(xs, xn);
     if (p == 0 && equator) { val.x *= 0.5; val.y *= 0.5; }
-    four_out[(size_t)q * fstride + boff + 2 * e] = val;
+    four_out[(size_t)q * fstride + four_off_a(n, c, p, h, N, Th2)] = val;
   }
 }
 
@@ -384,7 +385,7 @@ __global__ void __launch_bounds__(128) k_c2r(FFTPlanDev pl, int N, const cplx* f
   }
 }
 
-// ---- standalone r2c: phys [f][n][Ph][Th] -> folded theta-Fourier --------------------------
+// ---- standalone r2c: phys [f][n][Ph][Th] -> folded theta-Fourier, analysis layout ---------
 template <int E, int G>
 __global__ void __launch_bounds__(128) k_r2c(FFTPlanDev pl, int N, const double* phys, cplx* four) {
   constexpr int RS = E * (G + 1), P2 = E * G;
@@ -408,7 +409,7 @@ __global__ void __launch_bounds__(128) k_r2c(FFTPlanDev pl, int N, const double*
   __syncthreads();
   col_pass<E, G, -1>(rows, 4, tabs);
   __syncthreads();
-  cplx* blk = four + (((size_t)f * N + n) * pl.HB + hb) * NM * 4;
+  cplx* fld = four + (size_t)f * N * pl.HB * NM * 4;  // analysis layout (four_off_a)
   for (int i = threadIdx.x; i < NM * 2; i += blockDim.x) {
     const int c = i >> 1, q = i & 1, hh = 2 * hb + q, b = tabs.thm[c];
     if (hh >= Th2) continue;
@@ -416,8 +417,8 @@ __global__ void __launch_bounds__(128) k_r2c(FFTPlanDev pl, int N, const double*
     const double2 xn = row_unpack<G>(rows + (2 * q + 1) * RS, b, pl);
     double2 ev = add2(xs, xn);
     if ((Th & 1) && hh == Th2 - 1) { ev.x *= 0.5; ev.y *= 0.5; }
-    blk[(c * 2 + 0) * 2 + q] = ev;
-    blk[(c * 2 + 1) * 2 + q] = sub2(xs, xn);
+    fld[four_off_a(n, c, 0, hh, N, Th2)] = ev;
+    fld[four_off_a(n, c, 1, hh, N, Th2)] = sub2(xs, xn);
   }
 }
 

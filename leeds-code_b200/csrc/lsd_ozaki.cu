@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
           }
         } else {
           for (int i = lane; i < 2 * a.Th2; i += 32) {
-            const double2 y = src[four_off(n, c, i & 1, i >> 1, a.NM, a.HB)];
+            const double2 y = src[four_off_a(n, c, 0, 0, a.N, a.Th2) + i];  // E then O, contiguous
             mx = fmax(mx, fmax(fabs(y.x), fabs(y.y)));
           }
         }
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
               v = comp == 0 ? cv.x : comp == 1 ? cv.y : comp == 2 ? -cv.y : cv.x;
             }
           } else if (TYPE == OZ_Q) {
-            const double2 y = a.in0[g][four_off(n, c, p, k, a.NM, a.HB)];
+            const double2 y = a.in0[g][four_off_a(n, c, p, k, a.N, a.Th2)];
             v = comp ? y.y : y.x;
           } else {  // OZ_ST: segment 1 (gwllP_) on parity 1-p, segment 2 (gwllsin1mP) on parity p
             const int pp = seg1 ? 1 - p : p;
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
             // s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re) ...
             // (transform.fftw3.F90:866-909)
             const bool use_ph = seg1 ? comp >= 2 : comp < 2;
-            const double2 y = (use_ph ? a.in1[g] : a.in0[g])[four_off(n, c, pp, j, a.NM, a.HB)];
+            const double2 y = (use_ph ? a.in1[g] : a.in0[g])[four_off_a(n, c, pp, j, a.N, a.Th2)];
             if (seg1) v = (comp & 1) ? y.y : y.x;
             else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
           }

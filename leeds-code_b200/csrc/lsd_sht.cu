@@ -8,8 +8,9 @@
 // (transform.fftw3.F90:527-602, 825-949).
 //
 // Data layouts: spectral [n][H] complex (harmonic fastest, the reference's `spec`
-// order); theta-Fourier rows folded into even/odd half-grid sums in half-row pairs
-// (four_off: [n][h/2][m-counter][E/O][h%2]);
+// order); theta-Fourier rows folded into even/odd half-grid sums: synthesis writes them in
+// half-row pairs for the FFT (four_off: [n][h/2][m-counter][E/O][h%2]), analysis reads them
+// counter-major (four_off_a: [m-counter][n][E/O][h]);
 // tables [nh][Th2] (the reference's leg_*(Th2, 0:H-1)).
 //
 // Synthesis CTA = (m-counter, NT shells, group); thread = one theta row j of the half
@@ -229,8 +230,8 @@ __global__ void __launch_bounds__(288) k_anal(AnalArgs a) {
       double2 e = make_double2(0.0, 0.0), o = e;
       if (n < a.N) {  // folded E/O data (the FFT stage folded the two hemispheres)
         const int cn = cc ? c1 : c0, j = j0 + jj;
-        e = G.in[f][four_off(n, cn, 0, j, a.NM, a.HB)];
-        o = G.in[f][four_off(n, cn, 1, j, a.NM, a.HB)];
+        e = G.in[f][four_off_a(n, cn, 0, j, a.N, Th2)];
+        o = G.in[f][four_off_a(n, cn, 1, j, a.N, Th2)];
       }
       dat[((cc * NF + f) * 2 + 0) * DROW + jj * A_NT + q] = e;
       dat[((cc * NF + f) * 2 + 1) * DROW + jj * A_NT + q] = o;

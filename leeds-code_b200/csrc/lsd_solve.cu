@@ -653,17 +653,18 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   int rc;
   if ((rc = lsd_launch_synth(ctx, sg, 5))) return rc;
   if (marks) cudaEventRecord(marks[1], s);
-  if ((rc = lsd_launch_products(ctx, fo, fo))) return rc;
+  cplx* fa = fo + 15 * FF;  // the 7 product fields, in the analysis layout
+  if ((rc = lsd_launch_products(ctx, fo, fa))) return rc;
   if (marks) cudaEventRecord(marks[2], s);
   AnalGroup ag[3];
   ag[0].kind = AK_VECTOR;
   ag[1].kind = AK_VECTOR;
   ag[2].kind = AK_SCALAR;
   for (int k = 0; k < 3; ++k) {
-    ag[0].in[k] = fo + k * FF; ag[0].out[k] = sp + (S_VQ + k) * F;
-    ag[1].in[k] = fo + (3 + k) * FF; ag[1].out[k] = sp + (S_BQ + k) * F;
+    ag[0].in[k] = fa + k * FF; ag[0].out[k] = sp + (S_VQ + k) * F;
+    ag[1].in[k] = fa + (3 + k) * FF; ag[1].out[k] = sp + (S_BQ + k) * F;
   }
-  ag[2].in[0] = fo + 6 * FF; ag[2].out[0] = sp + S_DC * F;
+  ag[2].in[0] = fa + 6 * FF; ag[2].out[0] = sp + S_DC * F;
   ag[2].in[1] = ag[2].in[2] = nullptr; ag[2].out[1] = ag[2].out[2] = nullptr;
   if ((rc = lsd_launch_anal(ctx, ag, 3))) return rc;
   if (marks) cudaEventRecord(marks[3], s);
