@@ -107,11 +107,12 @@ def workload(name, precision):
     syn = pkg.synthetic
     capi = pkg.capi
     prec = capi.PREC_OZAKI if precision == "ozaki" else capi.PREC_FP64
+    slices = getattr(workload, "slices", 0)
     if name == "parity32":
-        cfg = syn.config_parity(precision=prec)
+        cfg = syn.config_parity(precision=prec, ozaki_slices=slices)
         desc = "Boussinesq MHD shell L=M=32 (lmax=31), Nr=33, Th=48, Ph=96, dt=1e-5"
     else:
-        cfg = syn.config_dynamo128(precision=prec)
+        cfg = syn.config_dynamo128(precision=prec, ozaki_slices=slices)
         desc = "Boussinesq MHD dynamo step lmax=mmax=127 (L=M=128), Nr=129, Th=192, Ph=384, dt=2e-6"
     return cfg, desc
 
@@ -362,9 +363,12 @@ def main():
     ap.add_argument("--precision", default="best", choices=["best", "fp64", "ozaki"])
     ap.add_argument("--workload", default="dynamo128", choices=["dynamo128", "parity32"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--slices", type=int, default=0,
+                    help="int8 slices per operand of the tensor-core contraction (0: library default 7)")
     ap.add_argument("--energy-steps", type=int, default=1000,
                     help="steps of the FP64 vs tensor-core energy comparison (0: skip)")
     args = ap.parse_args()
+    workload.slices = args.slices
     args.warmup = max(3, args.warmup) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

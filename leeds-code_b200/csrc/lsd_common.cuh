@@ -53,10 +53,11 @@ __host__ __device__ __forceinline__ size_t four_off(int n, int c, int p, int h, 
   return ((((size_t)n * HB + (h >> 1)) * NM + c) * 2 + p) * 2 + (h & 1);
 }
 // theta-Fourier rows on their way to the analysis (written by the products and r2c
-// kernels): [m-counter c][n][p = E/O][h] per field, so one (c, n) row is contiguous along h
-// (the analysis contraction runs over h).  Same field size as four_off's.
+// kernels): [m-counter c][n][h][p = E/O] per field, so one (c, n) row is contiguous along h
+// (the analysis contraction runs over h) and a writer of one half-row h fills whole
+// 32-byte (E, O) pairs.  Same field size as four_off's.
 __host__ __device__ __forceinline__ size_t four_off_a(int n, int c, int p, int h, int N, int Th2) {
-  return (((size_t)c * N + n) * 2 + p) * Th2 + h;
+  return (((size_t)c * N + n) * Th2 + h) * 2 + p;
 }
 
 struct SynthGroup {

@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
           }
         } else {
           for (int i = lane; i < 2 * a.Th2; i += 32) {
-            const double2 y = src[four_off_a(n, c, 0, 0, a.N, a.Th2) + i];  // E then O, contiguous
+            const double2 y = src[four_off_a(n, c, 0, 0, a.N, a.Th2) + i];  // (h, E/O) pairs, contiguous
             mx = fmax(mx, fmax(fabs(y.x), fabs(y.y)));
           }
         }

@@ -10,7 +10,7 @@
 // Data layouts: spectral [n][H] complex (harmonic fastest, the reference's `spec`
 // order); theta-Fourier rows folded into even/odd half-grid sums: synthesis writes them in
 // half-row pairs for the FFT (four_off: [n][h/2][m-counter][E/O][h%2]), analysis reads them
-// counter-major (four_off_a: [m-counter][n][E/O][h]);
+// counter-major (four_off_a: [m-counter][n][h][E/O]);
 // tables [nh][Th2] (the reference's leg_*(Th2, 0:H-1)).
 //
 // Synthesis CTA = (m-counter, NT shells, group); thread = one theta row j of the half
