@@ -170,25 +170,6 @@ __device__ __forceinline__ void oz_digits(double x, int e, int S, int8_t* d) {
     if (s < S) d[s] = (int8_t)(sgn * (int)((mag >> (7 * (S - 1 - s))) & 127));
 }
 
-// The same digits from 32-bit integers: y = x * sc (|y| < 1, exact power-of-two scaling),
-// the top S - L digits from trunc(|y| 2^(7(S-L))) and the low L = min(S, 4) digits from the
-// exact remainder scaled by 2^(7L); the sign is applied to every digit.
-__device__ __forceinline__ void oz_digits32(double x, double sc, int S, int (&d)[OZ_MAXS]) {
-  const double y = fabs(x) * sc;
-  const int L = S < 4 ? S : 4, SH = S - L;
-  const double yh = y * pow2i(7 * SH);
-  const int hi = (int)yh;                       // < 2^(7 SH) <= 2^28
-  const int lo = (int)((yh - (double)hi) * pow2i(7 * L));  // exact remainder, < 2^(7L)
-  const int m = x < 0.0 ? -1 : 0;               // conditional negation: (v ^ m) - m
-#pragma unroll
-  for (int s = 0; s < OZ_MAXS; ++s) {
-    int v = 0;
-    if (s < SH) v = (hi >> (7 * (SH - 1 - s))) & 127;
-    else if (s < S) v = (lo >> (7 * (S - 1 - s))) & 127;
-    d[s] = (v ^ m) - m;
-  }
-}
-
 __device__ __forceinline__ int oz_exponent(double maxabs) {
   if (!(maxabs > 0.0)) return -1000;
   int e;
@@ -284,11 +265,12 @@ template <int TYPE> struct OzT {
 };
 
 // One CTA = (counter c, z-block of 128 rows); both parities.
-template <int TYPE>
+template <int TYPE, int S>
 __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
   constexpr int PER = OzT<TYPE>::per, NIN = OzT<TYPE>::nin;
   constexpr int NPAIR = 128 / PER;  // shells of the z-block
   __shared__ int e_pair[NPAIR];
+  __shared__ int kx[2][512];  // harmonic lists of the two problems (synthesis)
   const int c = blockIdx.x, zb = blockIdx.y;
   const int R0 = zb * 128;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -323,7 +305,10 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
   __syncthreads();
   for (int r = tid; r < 128; r += 256)
     if (R0 + r < a.nrows) a.erow[(size_t)c * a.nrows + R0 + r] = e_pair[r / PER];
-  // ---- digits of both parities' A tiles: thread = (row r, K half kh), 16 values per K step
+  // ---- digits of both parities' A tiles: thread = (row r, K half kh), 16 values per K step.
+  // |x| 2^(7S - e) is an integer below 2^(7S) <= 2^56, split into two 28-bit halves whose
+  // 7-bit groups are the digits; four values make one 32-bit word per slice (byte permutes),
+  // the signs are applied per byte (two's complement).
   const int r = tid & 127, kh = tid >> 7;
   const int R = R0 + r;
   const bool live = R < a.nrows;
@@ -334,66 +319,81 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
     n = (R % a.rows_per_group) / PER;
     comp = R % PER;
     const int e = e_pair[r / PER];
-    sc = e > -1000 ? pow2i(-e) : 0.0;
+    sc = e > -1000 ? pow2i(7 * S - e) : 0.0;
   }
+  const double r1 = (TYPE == OZ_GRAD && live) ? a.rinv[n] : 1.0;
   const int toff = umma::tile_off(r, kh * 16);
   for (int p = 0; p < 2; ++p) {
     const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+    if (!OzT<TYPE>::anal)
+      for (int i = tid; i < pr.K && i < 512; i += 256) kx[p][i] = a.kidx[pr.kofs + i];
+  }
+  __syncthreads();
+  for (int p = 0; p < 2; ++p) {
+    const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
     if (pr.nchunk == 0) continue;
-    int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * a.S * 4096;
+    int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
     for (int ks = 0; ks < pr.nks; ++ks) {
-      uint32_t wd[OZ_MAXS][4];
+      uint32_t wd[S][4];
 #pragma unroll
-      for (int s2 = 0; s2 < OZ_MAXS; ++s2)
+      for (int q = 0; q < 4; ++q) {
+        uint32_t hi[4], lo[4];
+        uint32_t sg = 0u;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) wd[s2][q] = 0u;
-#pragma unroll
-      for (int u = 0; u < 16; ++u) {
-        const int k = ks * 32 + kh * 16 + u;
-        double v = 0.0;
-        if (live && k < pr.K) {
-          const bool seg1 = k < pr.len1;
-          if (TYPE == OZ_P) {
-            const double2 q = a.in0[g][(size_t)n * a.H + a.kidx[pr.kofs + k]];
-            v = comp ? q.y : q.x;
-          } else if (TYPE == OZ_VEC) {
-            // theta: s llP_ (segment 1) + (t.im, -t.re) llsin1mP (segment 2);
-            // phi:   t llP_ + (-s.im, s.re) llsin1mP        (transform.fftw3.F90:746-774)
-            const bool use_t = seg1 ? comp >= 2 : comp < 2;
-            const double2 x = (use_t ? a.in1[g] : a.in0[g])[(size_t)n * a.H + a.kidx[pr.kofs + k]];
-            if (seg1) v = (comp & 1) ? x.y : x.x;
-            else v = comp == 0 ? x.y : comp == 1 ? -x.x : comp == 2 ? -x.y : x.x;
-          } else if (TYPE == OZ_GRAD) {
-            // theta: (C/r) P_ ; phi: i (C/r) sin1mP              (transform.fftw3.F90:955-1000)
-            if (seg1 == (comp < 2)) {
-              double2 cv = a.in0[g][(size_t)n * a.H + a.kidx[pr.kofs + k]];
-              const double r1 = a.rinv[n];
-              cv.x *= r1; cv.y *= r1;
-              v = comp == 0 ? cv.x : comp == 1 ? cv.y : comp == 2 ? -cv.y : cv.x;
+        for (int u4 = 0; u4 < 4; ++u4) {
+          const int k = ks * 32 + kh * 16 + q * 4 + u4;
+          double v = 0.0;
+          if (live && k < pr.K) {
+            const bool seg1 = k < pr.len1;
+            if (TYPE == OZ_P) {
+              const double2 x = a.in0[g][(size_t)n * a.H + kx[p][k]];
+              v = comp ? x.y : x.x;
+            } else if (TYPE == OZ_VEC) {
+              // theta: s llP_ (segment 1) + (t.im, -t.re) llsin1mP (segment 2);
+              // phi:   t llP_ + (-s.im, s.re) llsin1mP        (transform.fftw3.F90:746-774)
+              const bool use_t = seg1 ? comp >= 2 : comp < 2;
+              const double2 x = (use_t ? a.in1[g] : a.in0[g])[(size_t)n * a.H + kx[p][k]];
+              if (seg1) v = (comp & 1) ? x.y : x.x;
+              else v = comp == 0 ? x.y : comp == 1 ? -x.x : comp == 2 ? -x.y : x.x;
+            } else if (TYPE == OZ_GRAD) {
+              // theta: (C/r) P_ ; phi: i (C/r) sin1mP              (transform.fftw3.F90:955-1000)
+              if (seg1 == (comp < 2)) {
+                const double2 x = a.in0[g][(size_t)n * a.H + kx[p][k]];
+                const double2 cv = make_double2(x.x * r1, x.y * r1);
+                v = comp == 0 ? cv.x : comp == 1 ? cv.y : comp == 2 ? -cv.y : cv.x;
+              }
+            } else if (TYPE == OZ_Q) {
+              const double2 y = a.in0[g][four_off_a(n, c, p, k, a.N, a.Th2)];
+              v = comp ? y.y : y.x;
+            } else {  // OZ_ST: segment 1 (gwllP_) on parity 1-p, segment 2 (gwllsin1mP) on parity p
+              const int pp = seg1 ? 1 - p : p;
+              const int j = seg1 ? k : k - pr.len1;
+              // s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re)
+              // (transform.fftw3.F90:866-909)
+              const bool use_ph = seg1 ? comp >= 2 : comp < 2;
+              const double2 y = (use_ph ? a.in1[g] : a.in0[g])[four_off_a(n, c, pp, j, a.N, a.Th2)];
+              if (seg1) v = (comp & 1) ? y.y : y.x;
+              else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
             }
-          } else if (TYPE == OZ_Q) {
-            const double2 y = a.in0[g][four_off_a(n, c, p, k, a.N, a.Th2)];
-            v = comp ? y.y : y.x;
-          } else {  // OZ_ST: segment 1 (gwllP_) on parity 1-p, segment 2 (gwllsin1mP) on parity p
-            const int pp = seg1 ? 1 - p : p;
-            const int j = seg1 ? k : k - pr.len1;
-            // s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re) ...
-            // (transform.fftw3.F90:866-909)
-            const bool use_ph = seg1 ? comp >= 2 : comp < 2;
-            const double2 y = (use_ph ? a.in1[g] : a.in0[g])[four_off_a(n, c, pp, j, a.N, a.Th2)];
-            if (seg1) v = (comp & 1) ? y.y : y.x;
-            else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
           }
+          const unsigned long long X = (unsigned long long)(fabs(v) * sc);  // exact scaling, truncation
+          hi[u4] = (uint32_t)(X >> 28);
+          lo[u4] = (uint32_t)X & 0x0FFFFFFFu;
+          if (v < 0.0) sg |= 0xFFu << (8 * u4);
         }
-        int d[OZ_MAXS];
-        oz_digits32(v, sc, a.S, d);
 #pragma unroll
-        for (int s2 = 0; s2 < OZ_MAXS; ++s2) wd[s2][u >> 2] |= ((uint32_t)d[s2] & 255u) << (8 * (u & 3));
+        for (int s2 = 0; s2 < S; ++s2) {
+          const int j = S - 1 - s2;  // digit s2 holds bits 7j .. 7j + 6
+          uint32_t m[4];
+#pragma unroll
+          for (int u4 = 0; u4 < 4; ++u4) m[u4] = j >= 4 ? (hi[u4] >> (7 * (j - 4))) & 127u : (lo[u4] >> (7 * j)) & 127u;
+          const uint32_t w = __byte_perm(__byte_perm(m[0], m[1], 0x0040), __byte_perm(m[2], m[3], 0x0040), 0x5410);
+          wd[s2][q] = __vsub4(w ^ sg, sg);
+        }
       }
 #pragma unroll
-      for (int s2 = 0; s2 < OZ_MAXS; ++s2)
-        if (s2 < a.S)
-          *(uint4*)(Ablk + ((size_t)ks * a.S + s2) * 4096 + toff) = make_uint4(wd[s2][0], wd[s2][1], wd[s2][2], wd[s2][3]);
+      for (int s2 = 0; s2 < S; ++s2)
+        *(uint4*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) = make_uint4(wd[s2][0], wd[s2][1], wd[s2][2], wd[s2][3]);
     }
   }
 }
@@ -606,6 +606,8 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
   if (S < 2 || S > OZ_MAXS) return lsd_fail(ctx, LSD_EARG, "ozaki_slices must be 2..8");
   o->S = S;
   const int NM = ctx->NM, Th2 = ctx->Th2, N = ctx->N;
+  for (int c = 0; c < NM; ++c)
+    if (ctx->mlen[c] > 512) return lsd_fail(ctx, LSD_EARG, "tensor-core path: more than 512 harmonics per m");
   std::vector<std::vector<int>> Kcp((size_t)NM * 2);  // harmonics per (counter, parity)
   for (int c = 0; c < NM; ++c)
     for (int k = 0; k < ctx->mlen[c]; ++k) {
@@ -719,7 +721,16 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
     ga.out0[i] = on ? gs[i].out0 : nullptr; ga.out1[i] = on ? gs[i].out1 : nullptr;
     ga.zero_m0_im[i] = on ? gs[i].zero_m0_im : 0;
   }
-  k_oz_prep<TYPE><<<dim3(ctx->NM, nzb), 256, 0, ctx->stream>>>(pa);
+  const dim3 pg(ctx->NM, nzb);
+  switch (o->S) {
+    case 2: k_oz_prep<TYPE, 2><<<pg, 256, 0, ctx->stream>>>(pa); break;
+    case 3: k_oz_prep<TYPE, 3><<<pg, 256, 0, ctx->stream>>>(pa); break;
+    case 4: k_oz_prep<TYPE, 4><<<pg, 256, 0, ctx->stream>>>(pa); break;
+    case 5: k_oz_prep<TYPE, 5><<<pg, 256, 0, ctx->stream>>>(pa); break;
+    case 6: k_oz_prep<TYPE, 6><<<pg, 256, 0, ctx->stream>>>(pa); break;
+    case 7: k_oz_prep<TYPE, 7><<<pg, 256, 0, ctx->stream>>>(pa); break;
+    default: k_oz_prep<TYPE, 8><<<pg, 256, 0, ctx->stream>>>(pa); break;
+  }
   k_oz_gemm<TYPE><<<dim3(ctx->NM, 2, nzb), OZ_THREADS, o->smem, ctx->stream>>>(ga);
   ctx->launches += 2;
   cudaError_t e = cudaGetLastError();
