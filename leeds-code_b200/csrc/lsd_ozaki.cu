@@ -413,9 +413,13 @@ __device__ __forceinline__ bool oz_wait(uint64_t* mbar, uint32_t parity, int* er
   return false;
 }
 
-// One CTA = (counter c, parity p, z-block of 128 rows); loops over the column chunks.
+// Persistent: CTA b walks the tiles t = b, b + gridDim.x, ... of the (counter c, parity p,
+// z-block of 128 rows) grid, each a loop over column chunks.  The bulk-copy ring, the MMA
+// issue and the tensor-memory handshakes run on counters over all of the CTA's tiles, so
+// the pipeline does not drain between tiles.  Two CTAs per SM (256 tensor-memory columns
+// each).
 template <int TYPE>
-__global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
+__global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb) {
   constexpr int PER = OzT<TYPE>::per;
   extern __shared__ __align__(1024) uint8_t oz_smem[];
   __shared__ __align__(8) uint64_t full[OZ_STAGES], empty[OZ_STAGES], accf, tfree, fin;
@@ -423,12 +427,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
   __shared__ cplx* pbase[64];  // output base of each (re, im) row pair of the z-block
   __shared__ int pzero[64];    // analysis: drop the imaginary part of m = 0 for this pair
   __shared__ double csc[OZ_NC];  // column scales 2^fexp of the current chunk
-  const int c = blockIdx.x, p = blockIdx.y, zb = blockIdx.z;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int S = a.S;
-  const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
-  if (pr.nchunk == 0) return;  // no harmonics of this parity: nothing to write
-  const int nks = pr.nks, nch = pr.nchunk, total = nks * nch;
+  const int ntile = a.NM * 2 * nzb;
   const uint32_t stage_bytes = (uint32_t)S * 5120;  // A: S x 4096, B: S x 1024
   double* stg = (double*)(oz_smem + (size_t)OZ_STAGES * stage_bytes);  // [128][OZ_STG]
   if (tid == 0) {
@@ -439,37 +440,37 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
     umma::fence_mbar_init();
   }
   if (warp == 0) umma::tmem_alloc(&tbase, 256);
-  if (tid < 64) {
-    const int Rr = zb * 128 + 2 * tid;
-    cplx* base = nullptr;
-    int zero = 0;
-    if (Rr < a.nrows) {
-      const int g = Rr / a.rows_per_group, n = (Rr % a.rows_per_group) / PER, comp = Rr % PER;
-      cplx* out = (comp < 2) ? a.out0[g] : a.out1[g];
-      base = OzT<TYPE>::anal ? out + (size_t)n * a.H : out + four_off(n, c, p, 0, a.NM, a.HB);
-      zero = TYPE == OZ_ST || a.zero_m0_im[g];
-    }
-    pbase[tid] = base;
-    pzero[tid] = zero;
-  }
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tmem = tbase;
+  // tile t -> (c, p, zb), z-block fastest
+  auto tile = [&](int t, int& c, int& p, int& zb) {
+    zb = t % nzb;
+    p = (t / nzb) & 1;
+    c = t / (2 * nzb);
+  };
 
   if (tid == 128) {
-    // ---- producer: A (this z-block, K step) and B (chunk, K step) tiles into the ring
-    const int8_t* Ablk = a.A + pr.aofs + (size_t)zb * nks * S * 4096;
-    const int8_t* Bblk = a.B + pr.bofs;
+    // ---- producer: A (z-block, K step) and B (chunk, K step) tiles into the ring
     int it = 0;
-    for (; it < total; ++it) {
-      const int st = it % OZ_STAGES, use = it / OZ_STAGES;
-      if (use > 0 && !oz_wait(&empty[st], (use - 1) & 1, a.err)) break;
-      const int ch = it / nks, ks = it % nks;
-      uint8_t* sA = oz_smem + (size_t)st * stage_bytes;
-      umma::mbar_expect_tx(&full[st], stage_bytes);
-      umma::bulk_g2s(sA, Ablk + (size_t)ks * S * 4096, (uint32_t)S * 4096, &full[st]);
-      umma::bulk_g2s(sA + (size_t)S * 4096, Bblk + ((size_t)ch * nks + ks) * S * 1024, (uint32_t)S * 1024, &full[st]);
+    bool ok = true;
+    for (int t = blockIdx.x; t < ntile && ok; t += gridDim.x) {
+      int c, p, zb;
+      tile(t, c, p, zb);
+      const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+      const int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
+      const int8_t* Bblk = a.B + pr.bofs;
+      for (int q = 0; q < pr.nchunk * pr.nks; ++q, ++it) {
+        const int st = it % OZ_STAGES, use = it / OZ_STAGES;
+        if (use > 0 && !oz_wait(&empty[st], (use - 1) & 1, a.err)) { ok = false; break; }
+        const int ch = q / pr.nks, ks = q % pr.nks;
+        uint8_t* sA = oz_smem + (size_t)st * stage_bytes;
+        umma::mbar_expect_tx(&full[st], stage_bytes);
+        umma::bulk_g2s(sA, Ablk + (size_t)ks * S * 4096, (uint32_t)S * 4096, &full[st]);
+        umma::bulk_g2s(sA + (size_t)S * 4096, Bblk + ((size_t)ch * pr.nks + ks) * S * 1024, (uint32_t)S * 1024,
+                       &full[st]);
+      }
     }
     // drain: the copies of the last stages have landed before the CTA can exit
     for (int j = (it > OZ_STAGES ? it - OZ_STAGES : 0); j < it; ++j)
@@ -477,83 +478,112 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a) {
   } else if (tid == 160) {
     // ---- MMA issuer: S(S+1)/2 digit pairs per K step into S diagonals of 32 columns
     const uint32_t idesc = umma::idesc_s8(128, OZ_NC);
+    int it = 0, cc = 0;
     bool ok = true;
-    for (int ch = 0; ch < nch && ok; ++ch) {
-      if (ch > 0 && !oz_wait(&tfree, (ch - 1) & 1, a.err)) { ok = false; break; }
-      umma::fence_after_sync();
-      for (int ks = 0; ks < nks; ++ks) {
-        const int it = ch * nks + ks, st = it % OZ_STAGES;
-        if (!oz_wait(&full[st], (it / OZ_STAGES) & 1, a.err)) { ok = false; break; }
+    for (int t = blockIdx.x; t < ntile && ok; t += gridDim.x) {
+      int c, p, zb;
+      tile(t, c, p, zb);
+      const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+      for (int ch = 0; ch < pr.nchunk && ok; ++ch, ++cc) {
+        if (cc > 0 && !oz_wait(&tfree, (cc - 1) & 1, a.err)) { ok = false; break; }
         umma::fence_after_sync();
-        const uint32_t sa0 = umma::smem_u32(oz_smem + (size_t)st * stage_bytes);
-        const uint32_t sb0 = sa0 + (uint32_t)S * 4096;
-        for (int d = 0; d < S; ++d)
-          for (int sa = 0; sa <= d; ++sa) {
-            const uint64_t ad = umma::desc_kmajor_noswz(sa0 + (uint32_t)sa * 4096, 128, 256);
-            const uint64_t bd = umma::desc_kmajor_noswz(sb0 + (uint32_t)(d - sa) * 1024, 128, 256);
-            umma::mma_s8(tmem + (uint32_t)(d * OZ_NC), ad, bd, idesc, (ks > 0 || sa > 0) ? 1 : 0);
-          }
-        umma::commit(&empty[st]);
+        for (int ks = 0; ks < pr.nks; ++ks, ++it) {
+          const int st = it % OZ_STAGES;
+          if (!oz_wait(&full[st], (it / OZ_STAGES) & 1, a.err)) { ok = false; break; }
+          umma::fence_after_sync();
+          const uint32_t sa0 = umma::smem_u32(oz_smem + (size_t)st * stage_bytes);
+          const uint32_t sb0 = sa0 + (uint32_t)S * 4096;
+          for (int d = 0; d < S; ++d)
+            for (int sa = 0; sa <= d; ++sa) {
+              const uint64_t ad = umma::desc_kmajor_noswz(sa0 + (uint32_t)sa * 4096, 128, 256);
+              const uint64_t bd = umma::desc_kmajor_noswz(sb0 + (uint32_t)(d - sa) * 1024, 128, 256);
+              umma::mma_s8(tmem + (uint32_t)(d * OZ_NC), ad, bd, idesc, (ks > 0 || sa > 0) ? 1 : 0);
+            }
+          umma::commit(&empty[st]);
+        }
+        if (ok) umma::commit(&accf);
       }
-      if (ok) umma::commit(&accf);
     }
     umma::commit(&fin);  // arrives when every MMA issued above has completed
     umma::mbar_wait(&fin, 0, WAIT_ITERS);
   } else if (tid < 128) {
-    // ---- epilogue: row tid of the z-block
-    const int R = zb * 128 + tid;
-    const bool live = R < a.nrows;
-    // sum_d D_d 2^(-7(d+2)) = 2^(-7(S+1)) H with H = Horner over d in 2^7; the power of two
-    // and the row scale 2^erow are one factor
-    const double rsc = live ? pow2i(a.erow[(size_t)c * a.nrows + R] - 7 * (S + 1)) : 0.0;
-    for (int ch = 0; ch < nch; ++ch) {
-      if (tid < OZ_NC) csc[tid] = pow2i(a.fexp[pr.fofs + ch * OZ_NC + tid]);
-      const bool got = umma::mbar_wait(&accf, ch & 1, WAIT_ITERS);
-      if (!umma::bar_and(1, 128, got)) {  // uniform over the 128 epilogue threads
-        if (tid == 0) atomicExch(a.err, 1);
-        break;
-      }
-      umma::fence_after_sync();
-#pragma unroll
-      for (int c0 = 0; c0 < OZ_NC; c0 += 8) {
-        int32_t v[OZ_MAXS][8];
-#pragma unroll
-        for (int d = 0; d < OZ_MAXS; ++d)
-          if (d < S) umma::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * OZ_NC + c0), v[d]);
-        umma::tmem_wait_ld();
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          double hsum = (double)v[0][q];
-#pragma unroll
-          for (int d = 1; d < OZ_MAXS; ++d)
-            if (d < S) hsum = fma(hsum, 128.0, (double)v[d][q]);
-          stg[tid * OZ_STG + c0 + q] = hsum * (rsc * csc[c0 + q]);
+    // ---- epilogue: row tid of each z-block
+    int cc = 0;
+    for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+      int c, p, zb;
+      tile(t, c, p, zb);
+      const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+      if (pr.nchunk == 0) continue;  // no harmonics of this parity: nothing to write
+      if (tid < 64) {
+        const int Rr = zb * 128 + 2 * tid;
+        cplx* base = nullptr;
+        int zero = 0;
+        if (Rr < a.nrows) {
+          const int g = Rr / a.rows_per_group, n = (Rr % a.rows_per_group) / PER, comp = Rr % PER;
+          cplx* out = (comp < 2) ? a.out0[g] : a.out1[g];
+          base = OzT<TYPE>::anal ? out + (size_t)n * a.H : out + four_off(n, c, p, 0, a.NM, a.HB);
+          zero = TYPE == OZ_ST || a.zero_m0_im[g];
         }
+        pbase[tid] = base;
+        pzero[tid] = zero;
       }
-      umma::fence_before_sync();
-      umma::mbar_arrive(&tfree);  // tensor memory may take the next chunk
-      umma::bar_sync(1, 128);
-      // coalesced stores: row pairs (re, im) x 32 columns
-      for (int idx = tid; idx < 64 * OZ_NC; idx += 128) {
-        const int pair = idx / OZ_NC, q = idx % OZ_NC;
-        cplx* base = pbase[pair];
-        if (!base) continue;
-        double2 val = make_double2(stg[(2 * pair) * OZ_STG + q], stg[(2 * pair + 1) * OZ_STG + q]);
-        if (!OzT<TYPE>::anal) {
-          const int j = ch * OZ_NC + q;
-          if (j < a.Th2) base[(size_t)(j >> 1) * a.NM * 4 + (j & 1)] = val;
-        } else {
-          const int k = ch * OZ_NC + q;
-          if (k < pr.nk) {
-            const int nh = a.nhlist[pr.nhofs + k];
-            // m = 0: s, t (and a scalar) keep no imaginary part; q keeps its own
-            // (transform.fftw3.F90:599, 869, 902, 908)
-            if (pzero[pair] && a.hm[nh] == 0) val.y = 0.0;
-            base[nh] = val;
+      const int R = zb * 128 + tid;
+      const bool live = R < a.nrows;
+      // sum_d D_d 2^(-7(d+2)) = 2^(-7(S+1)) H with H = Horner over d in 2^7; the power of
+      // two and the row scale 2^erow are one factor
+      const double rsc = live ? pow2i(a.erow[(size_t)c * a.nrows + R] - 7 * (S + 1)) : 0.0;
+      bool ok = true;
+      for (int ch = 0; ch < pr.nchunk; ++ch, ++cc) {
+        if (tid < OZ_NC) csc[tid] = pow2i(a.fexp[pr.fofs + ch * OZ_NC + tid]);
+        const bool got = umma::mbar_wait(&accf, cc & 1, WAIT_ITERS);
+        if (!umma::bar_and(1, 128, got)) {  // uniform over the 128 epilogue threads
+          if (tid == 0) atomicExch(a.err, 1);
+          ok = false;
+          break;
+        }
+        umma::fence_after_sync();
+#pragma unroll
+        for (int c0 = 0; c0 < OZ_NC; c0 += 8) {
+          int32_t v[OZ_MAXS][8];
+#pragma unroll
+          for (int d = 0; d < OZ_MAXS; ++d)
+            if (d < S) umma::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * OZ_NC + c0), v[d]);
+          umma::tmem_wait_ld();
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            double hsum = (double)v[0][q];
+#pragma unroll
+            for (int d = 1; d < OZ_MAXS; ++d)
+              if (d < S) hsum = fma(hsum, 128.0, (double)v[d][q]);
+            stg[tid * OZ_STG + c0 + q] = hsum * (rsc * csc[c0 + q]);
           }
         }
+        umma::fence_before_sync();
+        umma::mbar_arrive(&tfree);  // tensor memory may take the next chunk
+        umma::bar_sync(1, 128);
+        // coalesced stores: row pairs (re, im) x 32 columns
+        for (int idx = tid; idx < 64 * OZ_NC; idx += 128) {
+          const int pair = idx / OZ_NC, q = idx % OZ_NC;
+          cplx* base = pbase[pair];
+          if (!base) continue;
+          double2 val = make_double2(stg[(2 * pair) * OZ_STG + q], stg[(2 * pair + 1) * OZ_STG + q]);
+          if (!OzT<TYPE>::anal) {
+            const int j = ch * OZ_NC + q;
+            if (j < a.Th2) base[(size_t)(j >> 1) * a.NM * 4 + (j & 1)] = val;
+          } else {
+            const int k = ch * OZ_NC + q;
+            if (k < pr.nk) {
+              const int nh = a.nhlist[pr.nhofs + k];
+              // m = 0: s, t (and a scalar) keep no imaginary part; q keeps its own
+              // (transform.fftw3.F90:599, 869, 902, 908)
+              if (pzero[pair] && a.hm[nh] == 0) val.y = 0.0;
+              base[nh] = val;
+            }
+          }
+        }
+        umma::bar_sync(1, 128);
       }
-      umma::bar_sync(1, 128);
+      if (!ok) break;
     }
   }
   umma::fence_before_sync();
@@ -731,7 +761,10 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
     case 7: k_oz_prep<TYPE, 7><<<pg, 256, 0, ctx->stream>>>(pa); break;
     default: k_oz_prep<TYPE, 8><<<pg, 256, 0, ctx->stream>>>(pa); break;
   }
-  k_oz_gemm<TYPE><<<dim3(ctx->NM, 2, nzb), OZ_THREADS, o->smem, ctx->stream>>>(ga);
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->dev);
+  const int ntile = ctx->NM * 2 * nzb;
+  k_oz_gemm<TYPE><<<std::min(ntile, 2 * nsm), OZ_THREADS, o->smem, ctx->stream>>>(ga, nzb);
   ctx->launches += 2;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("tensor-core contraction: ") + cudaGetErrorString(e));
