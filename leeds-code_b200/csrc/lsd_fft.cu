@@ -58,10 +58,119 @@ __device__ __forceinline__ double2 sub2(double2 a, double2 b) { return make_doub
 template <int SIGN>
 __device__ __forceinline__ double2 twid(double2 a, double2 w) { return SIGN > 0 ? cmul(a, w) : cmulc(a, w); }
 
+// Short DFTs with their constants written out (no twiddle tables): 3- and 4-point
+// butterflies, 16 = 4 x 4 (radix 4 with the 16th roots of unity), and the prime-factor
+// (Good-Thomas) splits 6 = 2 x 3 and 12 = 3 x 4, which need no twiddles at all: input
+// index n = (N2 n1 + N1 n2) mod N, output index k = (N2 <N2^-1>_N1 k1 + N1 <N1^-1>_N2 k2) mod N.
+constexpr double kSqrt3_2 = 0.86602540378443864676;  // sin(pi/3)
+constexpr double kSqrt2_2 = 0.70710678118654752440;  // cos(pi/4)
+constexpr double kCos8 = 0.92387953251128675613;     // cos(pi/8)
+constexpr double kSin8 = 0.38268343236508977173;     // sin(pi/8)
+
+template <int SIGN>
+__device__ __forceinline__ double2 mul_i(double2 a) {  // a * (SIGN i)
+  return SIGN > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+template <int SIGN>
+__device__ __forceinline__ void dft3(double2& a, double2& b, double2& c) {
+  const double2 t1 = add2(b, c);
+  const double2 t2 = make_double2(a.x - 0.5 * t1.x, a.y - 0.5 * t1.y);
+  const double2 t3 = make_double2(SIGN * kSqrt3_2 * (b.x - c.x), SIGN * kSqrt3_2 * (b.y - c.y));
+  a = add2(a, t1);
+  b = make_double2(t2.x - t3.y, t2.y + t3.x);
+  c = make_double2(t2.x + t3.y, t2.y - t3.x);
+}
+template <int SIGN>
+__device__ __forceinline__ void dft4(double2& x0, double2& x1, double2& x2, double2& x3) {
+  const double2 a = add2(x0, x2), b = sub2(x0, x2), c = add2(x1, x3), d = mul_i<SIGN>(sub2(x1, x3));
+  x0 = add2(a, c);
+  x1 = add2(b, d);
+  x2 = sub2(a, c);
+  x3 = sub2(b, d);
+}
+// multiplication by w16^e, w16 = e^{SIGN 2 pi i / 16}, e in {1, 2, 3, 6, 9}
+template <int SIGN, int E16>
+__device__ __forceinline__ double2 tw16(double2 a) {
+  double c, s;
+  if (E16 == 1) { c = kCos8; s = kSin8; }
+  else if (E16 == 2) { c = kSqrt2_2; s = kSqrt2_2; }
+  else if (E16 == 3) { c = kSin8; s = kCos8; }
+  else if (E16 == 6) { c = -kSqrt2_2; s = kSqrt2_2; }
+  else { c = -kCos8; s = -kSin8; }  // 9
+  s = SIGN * s;
+  return make_double2(a.x * c - a.y * s, a.x * s + a.y * c);
+}
+template <int SIGN>
+__device__ __forceinline__ void dft16(double2 (&x)[16]) {
+  // columns n2: 4-point DFTs over n1 of x[4 n1 + n2], then the twiddles w16^(n2 k1)
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) dft4<SIGN>(x[n2], x[4 + n2], x[8 + n2], x[12 + n2]);
+  // x[4 k1 + n2] now holds Y[n2][k1]
+  x[4 * 1 + 1] = tw16<SIGN, 1>(x[4 * 1 + 1]);
+  x[4 * 2 + 1] = tw16<SIGN, 2>(x[4 * 2 + 1]);
+  x[4 * 3 + 1] = tw16<SIGN, 3>(x[4 * 3 + 1]);
+  x[4 * 1 + 2] = tw16<SIGN, 2>(x[4 * 1 + 2]);
+  x[4 * 2 + 2] = mul_i<SIGN>(x[4 * 2 + 2]);
+  x[4 * 3 + 2] = tw16<SIGN, 6>(x[4 * 3 + 2]);
+  x[4 * 1 + 3] = tw16<SIGN, 3>(x[4 * 1 + 3]);
+  x[4 * 2 + 3] = tw16<SIGN, 6>(x[4 * 2 + 3]);
+  x[4 * 3 + 3] = tw16<SIGN, 9>(x[4 * 3 + 3]);
+  // rows k1: 4-point DFTs over n2 give X[k1 + 4 k2]
+  double2 y[16];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    double2 a = x[4 * k1], b = x[4 * k1 + 1], c = x[4 * k1 + 2], d = x[4 * k1 + 3];
+    dft4<SIGN>(a, b, c, d);
+    y[k1] = a; y[k1 + 4] = b; y[k1 + 8] = c; y[k1 + 12] = d;
+  }
+#pragma unroll
+  for (int i = 0; i < 16; ++i) x[i] = y[i];
+}
+template <int SIGN>
+__device__ __forceinline__ void dft12(double2 (&x)[12]) {  // 3 x 4, n = (4 n1 + 3 n2) % 12
+  double2 y[3][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+    double2 a = x[(3 * n2) % 12], b = x[(4 + 3 * n2) % 12], c = x[(8 + 3 * n2) % 12];
+    dft3<SIGN>(a, b, c);
+    y[0][n2] = a; y[1][n2] = b; y[2][n2] = c;
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < 3; ++k1) {
+    dft4<SIGN>(y[k1][0], y[k1][1], y[k1][2], y[k1][3]);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) x[(4 * k1 + 9 * k2) % 12] = y[k1][k2];
+  }
+}
+template <int SIGN>
+__device__ __forceinline__ void dft6(double2 (&x)[6]) {  // 2 x 3, n = (3 n1 + 2 n2) % 6
+  double2 y[2][3];
+#pragma unroll
+  for (int n2 = 0; n2 < 3; ++n2) {
+    const double2 a = x[(2 * n2) % 6], b = x[(3 + 2 * n2) % 6];
+    y[0][n2] = add2(a, b);
+    y[1][n2] = sub2(a, b);
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < 2; ++k1) {
+    dft3<SIGN>(y[k1][0], y[k1][1], y[k1][2]);
+#pragma unroll
+    for (int k2 = 0; k2 < 3; ++k2) x[(3 * k1 + 4 * k2) % 6] = y[k1][k2];
+  }
+}
+
 template <int N, int EF, int SIGN>
 __device__ __forceinline__ void rdft(double2 (&x)[N], const double2* w) {
   if constexpr (N == 1) {
     return;
+  } else if constexpr (N == 16) {
+    dft16<SIGN>(x);
+  } else if constexpr (N == 12) {
+    dft12<SIGN>(x);
+  } else if constexpr (N == 6) {
+    dft6<SIGN>(x);
+  } else if constexpr (N == 4) {
+    dft4<SIGN>(x[0], x[1], x[2], x[3]);
   } else if constexpr (N == 2) {
     const double2 a = x[0], b = x[1];
     x[0] = add2(a, b);

@@ -65,7 +65,7 @@ def test_layout_tables_grid(pair):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("LMMp", [(32, 32, 1), (64, 16, 4), (24, 8, 2)])
+@pytest.mark.parametrize("LMMp", [(32, 32, 1), (64, 16, 4), (24, 8, 2), (64, 64, 1)])
 def test_transforms(LMMp):
     L, M, Mp = LMMp
     cfg = capi.template_config(L=L, M=M, Mp=Mp, N=9, timestep=1e-5)
