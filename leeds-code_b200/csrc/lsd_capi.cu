@@ -82,23 +82,6 @@ void build_layout(lsd_ctx* c) {
 
 // radix plan for the complex FFT of length P2 = 3^a 2^b
 
-// packing between Fortran split (re, im) arrays and device interleaved [n][nh]
-void pack_coll(const lsd_ctx* c, const double* re, const double* im, double* out) {  // coll (N,H)
-  for (int n = 0; n < c->N; ++n)
-    for (int nh = 0; nh < c->H; ++nh) {
-      size_t src = (size_t)n + (size_t)c->N * nh, dst = ((size_t)n * c->H + nh) * 2;
-      out[dst] = re[src];
-      out[dst + 1] = im[src];
-    }
-}
-void unpack_coll(const lsd_ctx* c, const double* in, double* re, double* im) {
-  for (int n = 0; n < c->N; ++n)
-    for (int nh = 0; nh < c->H; ++nh) {
-      size_t dst = (size_t)n + (size_t)c->N * nh, src = ((size_t)n * c->H + nh) * 2;
-      re[dst] = in[src];
-      im[dst] = in[src + 1];
-    }
-}
 void pack_spec(const lsd_ctx* c, const double* re, const double* im, double* out) {  // spec (H,N)
   size_t T = (size_t)c->N * c->H;
   for (size_t i = 0; i < T; ++i) { out[2 * i] = re[i]; out[2 * i + 1] = im[i]; }
@@ -416,31 +399,40 @@ int lsd_legendre_table(const lsd_ctx* c, int which, double* out) {
   return d2h(const_cast<lsd_ctx*>(c), out, c->d_leg + (size_t)which * T, sizeof(double) * T);
 }
 
+// coll fields cross the boundary in the reference's layout (Re, Im as (N, H) column-major
+// arrays); they are copied as they are and transposed into [n][nh] on the device
+// (lsd_coll_to_state / lsd_state_to_coll), with a scratch area of the spectral buffers.
 int lsd_set_coll(lsd_ctx* ctx, int field, const double* re, const double* im) {
   if (!ctx || !re || !im || field < 0 || field >= LSD_NFIELD) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
   const size_t F = (size_t)ctx->N * ctx->H;
-  pack_coll(ctx, re, im, ctx->h_pin);
-  CUDA_TRY(cudaMemcpyAsync(ctx->d_state + field * F, ctx->h_pin, sizeof(cplx) * F, cudaMemcpyHostToDevice, ctx->stream));
+  double* stage = (double*)ctx->d_spec;  // 2 F doubles: Re then Im
+  CUDA_TRY(cudaMemcpyAsync(stage, re, sizeof(double) * F, cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(stage + F, im, sizeof(double) * F, cudaMemcpyHostToDevice, ctx->stream));
+  int rc = lsd_coll_to_state(ctx, stage, stage + F, ctx->d_state + field * F);
+  if (rc) return rc;
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   ctx->have_eval = false;
   return LSD_OK;
 }
+static int coll_out(lsd_ctx* ctx, const cplx* src, double* re, double* im) {
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  const size_t F = (size_t)ctx->N * ctx->H;
+  double* stage = (double*)ctx->d_spec;
+  int rc = lsd_state_to_coll(ctx, src, stage, stage + F);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(re, stage, sizeof(double) * F, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(im, stage + F, sizeof(double) * F, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return LSD_OK;
+}
 int lsd_get_coll(lsd_ctx* ctx, int field, double* re, double* im) {
   if (!ctx || !re || !im || field < 0 || field >= LSD_NFIELD) return LSD_EARG;
-  const size_t F = (size_t)ctx->N * ctx->H;
-  int rc = d2h(ctx, ctx->h_pin, ctx->d_state + field * F, sizeof(cplx) * F);
-  if (rc) return rc;
-  unpack_coll(ctx, ctx->h_pin, re, im);
-  return LSD_OK;
+  return coll_out(ctx, ctx->d_state + field * (size_t)ctx->N * ctx->H, re, im);
 }
 int lsd_get_nonlinear(lsd_ctx* ctx, int which, double* re, double* im) {
   if (!ctx || !re || !im || which < 0 || which >= LSD_NFIELD) return LSD_EARG;
-  const size_t F = (size_t)ctx->N * ctx->H;
-  int rc = d2h(ctx, ctx->h_pin, ctx->d_nl + which * F, sizeof(cplx) * F);
-  if (rc) return rc;
-  unpack_coll(ctx, ctx->h_pin, re, im);
-  return LSD_OK;
+  return coll_out(ctx, ctx->d_nl + which * (size_t)ctx->N * ctx->H, re, im);
 }
 
 int lsd_set_time(lsd_ctx* ctx, double t, double dt) {

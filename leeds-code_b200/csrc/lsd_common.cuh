@@ -160,6 +160,8 @@ int lsd_pred(lsd_ctx* ctx);            // predictor solves (device)
 int lsd_corr(lsd_ctx* ctx);            // corrector solves + dterr (device)
 int lsd_energy_device(lsd_ctx* ctx, double* out);
 int lsd_energy_static(lsd_ctx* ctx, double* out);
+int lsd_coll_to_state(lsd_ctx* ctx, const double* re, const double* im, cplx* out);
+int lsd_state_to_coll(lsd_ctx* ctx, const cplx* in, double* re, double* im);
 int lsd_factor_batch(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info);
 int lsd_solve_batch(lsd_ctx* ctx, int n, int kl, int nmat, const double* d_ab, const int* d_ipiv,
                     int nrhs, const int* d_map, double* d_b);

@@ -899,6 +899,58 @@ int lsd_energy_static(lsd_ctx* ctx, double* out) {
   return energy_finish(ctx, Fh, wts, cod0, bpolN, r, dr1, out);
 }
 
+// ---- boundary layout: coll Re/Im (N, H) column-major <-> device [n][nh] complex ---------
+namespace {
+constexpr int TT = 32;  // transpose tile
+__global__ void k_coll_to_state(int N, int H, const double* __restrict__ re, const double* __restrict__ im,
+                                cplx* __restrict__ out) {
+  __shared__ double2 t[TT][TT + 1];
+  const int nh0 = blockIdx.x * TT, n0 = blockIdx.y * TT;
+  for (int i = threadIdx.y; i < TT; i += blockDim.y) {  // read along n (contiguous in coll)
+    const int nh = nh0 + i, n = n0 + threadIdx.x;
+    if (nh < H && n < N) t[i][threadIdx.x] = make_double2(re[(size_t)nh * N + n], im[(size_t)nh * N + n]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < TT; i += blockDim.y) {  // write along nh
+    const int n = n0 + i, nh = nh0 + threadIdx.x;
+    if (nh < H && n < N) out[(size_t)n * H + nh] = t[threadIdx.x][i];
+  }
+}
+__global__ void k_state_to_coll(int N, int H, const cplx* __restrict__ in, double* __restrict__ re,
+                                double* __restrict__ im) {
+  __shared__ double2 t[TT][TT + 1];
+  const int nh0 = blockIdx.x * TT, n0 = blockIdx.y * TT;
+  for (int i = threadIdx.y; i < TT; i += blockDim.y) {
+    const int n = n0 + i, nh = nh0 + threadIdx.x;
+    if (nh < H && n < N) t[threadIdx.x][i] = in[(size_t)n * H + nh];
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < TT; i += blockDim.y) {
+    const int nh = nh0 + i, n = n0 + threadIdx.x;
+    if (nh < H && n < N) {
+      const double2 v = t[i][threadIdx.x];
+      re[(size_t)nh * N + n] = v.x;
+      im[(size_t)nh * N + n] = v.y;
+    }
+  }
+}
+}  // namespace
+
+int lsd_coll_to_state(lsd_ctx* ctx, const double* re, const double* im, cplx* out) {
+  dim3 g(ceil_div(ctx->H, TT), ceil_div(ctx->N, TT)), b(TT, 8);
+  k_coll_to_state<<<g, b, 0, ctx->stream>>>(ctx->N, ctx->H, re, im, out);
+  ctx->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return LSD_OK;
+}
+int lsd_state_to_coll(lsd_ctx* ctx, const cplx* in, double* re, double* im) {
+  dim3 g(ceil_div(ctx->H, TT), ceil_div(ctx->N, TT)), b(TT, 8);
+  k_state_to_coll<<<g, b, 0, ctx->stream>>>(ctx->N, ctx->H, in, re, im);
+  ctx->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return LSD_OK;
+}
+
 int lsd_factor_batch(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info) {
   k_factor_batch<<<ceil_div(nmat, 64), 64, 0, ctx->stream>>>(n, kl, nmat, d_ab, d_ipiv, d_info);
   ctx->launches++;
