@@ -218,7 +218,6 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   else if (!c.boussinesq) why = "only the Boussinesq equations are supported";
   else if (c.timestep <= 0.0) why = "only a fixed timestep (d_timestep > 0) is supported";
   else if (!c.vel_tstep || !c.cod_tstep || !c.mag_tstep) why = "velocity, codensity and field must all be stepped";
-  else if (c.comp_tstep) why = "composition stepping is not supported on the device yet";
   else if (c.precision != LSD_PREC_FP64 && c.precision != LSD_PREC_OZAKI) why = "unknown precision";
   else if (c.precision == LSD_PREC_OZAKI && c.ozaki_slices != 0 && (c.ozaki_slices < 2 || c.ozaki_slices > 8))
     why = "ozaki_slices must be 0 (default) or 2..8";
@@ -330,9 +329,11 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   CTRY(cudaMemset(ctx->d_state, 0, sizeof(cplx) * LSD_NFIELD * F));
   CTRY(cudaMemset(ctx->d_nl, 0, sizeof(cplx) * LSD_NFIELD * F));
   CTRY(cudaMemset(ctx->d_sv, 0, sizeof(cplx) * LSD_NFIELD * F));
-  ctx->nspec = 13;
+  ctx->nspec = 14;  // 12 solve work columns / evaluation slots + dC + dComp
   TRY(dalloc(ctx, &ctx->d_spec, (size_t)ctx->nspec * F));
-  ctx->nfour = 22;  // 15 synthesised fields (FFT layout) + 7 products (analysis layout)
+  // 15 synthesised fields (FFT layout) + 7 products (analysis layout); composition adds
+  // grad Comp (3) and its product (1)
+  ctx->nfour = c.comp_tstep ? 26 : 22;
   TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * ctx->HB * NM * 4));
   TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));

@@ -338,14 +338,18 @@ __device__ __forceinline__ double2 row_unpack(const double2* row, int b, const F
   return r2c_unpack(b, row[ppos<G>(b)], row[ppos<G>(b == 0 ? 0 : pl.P2 - b)], pl);
 }
 
-// ---- fused: 15 theta-Fourier inputs -> products -> 7 theta-Fourier outputs -------------
+// ---- fused: 15 (18) theta-Fourier inputs -> products -> 7 (8) theta-Fourier outputs ----
 struct ProdConst {
-  double d_Cor, Cmag, d_qm1;
+  double d_Cor, Cmag, d_qm1, d_qm1c;
   const double* sn;  // sin(theta_j)
   const double* gp;  // cos(theta_j)
 };
 
-constexpr int NF_IN = 15, NF_OUT = 7;
+// inputs u, curl u, B, curl B, grad C (+ grad Comp); outputs u x curl u + Coriolis +
+// Lorentz (3), u x B (3), -Pr/Pm u.grad C (+ -Sc/Pm u.grad Comp)
+template <bool COMP> struct ProdFields {
+  static constexpr int in = COMP ? 18 : 15, out = COMP ? 8 : 7;
+};
 
 // grid (2 HB, N): one half-row h = blockIdx.x (its southern and northern theta row) per
 // CTA, 256 threads, two CTAs per SM so that one's memory waits overlap the other's work.
@@ -354,10 +358,11 @@ constexpr int NF_IN = 15, NF_OUT = 7;
 // stage into the padded rows [NF_IN][2][E (G+1)].
 constexpr int PROD_THREADS = 256;
 
-template <int E, int G>
+template <int E, int G, bool COMP>
 __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int N, ProdConst pc,
                                                               const cplx* four_in, cplx* four_out) {
   constexpr int RS = E * (G + 1), P2 = E * G;
+  constexpr int NF_IN = ProdFields<COMP>::in, NF_OUT = ProdFields<COMP>::out;
   extern __shared__ __align__(16) unsigned char psm[];
   const int n = blockIdx.y, h = blockIdx.x, hb = h >> 1, jj = h & 1;
   const int NM = pl.NM, M = pl.M, Th = pl.Th, Th2 = pl.Th2;
@@ -415,7 +420,6 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
       const double br = G_(6), bt = G_(7), bp = G_(8);
       const double jr = G_(9), jt = G_(10), jp = G_(11);
       const double cr = G_(12), ct = G_(13), cp = G_(14);
-#undef G_
       double a = vt * wp - vp * wt;
       double b = vp * wr - vr * wp;
       double c = vr * wt - vt * wr;
@@ -429,7 +433,13 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
       const double e1 = vp * br - vr * bp;
       const double e2 = vr * bt - vt * br;
       const double cod = -pc.d_qm1 * vr * cr - pc.d_qm1 * vt * ct - pc.d_qm1 * vp * cp;
-      const double o[NF_OUT] = {a, b, c, e0, e1, e2, cod};
+      double o[NF_OUT];
+      o[0] = a; o[1] = b; o[2] = c; o[3] = e0; o[4] = e1; o[5] = e2; o[6] = cod;
+      if constexpr (COMP) {  // non_composition (nonlinear.F90:294-341), Boussinesq
+        const double xr = G_(15), xt = G_(16), xp = G_(17);
+        o[NF_OUT - 1] = -pc.d_qm1c * vr * xr - pc.d_qm1c * vt * xt - pc.d_qm1c * vp * xp;
+      }
+#undef G_
 #pragma unroll
       for (int q = 0; q < NF_OUT; ++q) {
         if (part == 0) out[q].x = o[q] * scale; else out[q].y = o[q] * scale;
@@ -605,16 +615,24 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.d_Cor = 2.0 * c.Pm / c.E;
   pc.Cmag = 2 * c.Pm / c.E;
   pc.d_qm1 = c.Pr / c.Pm;
+  pc.d_qm1c = c.Sc / c.Pm;
   pc.sn = ctx->d_sn;
   pc.gp = ctx->d_gp;
-  const size_t smem = sizeof(double2) * ((size_t)NF_IN * 2 * ctx->fftE * (ctx->fftG + 1) + (size_t)4 * ctx->M) +
+  const bool comp = c.comp_tstep != 0;
+  const int nf_in = comp ? ProdFields<true>::in : ProdFields<false>::in;
+  const size_t smem = sizeof(double2) * ((size_t)nf_in * 2 * ctx->fftE * (ctx->fftG + 1) + (size_t)4 * ctx->M) +
                       fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
   if (smem > 224 * 1024) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
   dim3 grid(2 * ctx->HB, ctx->N);
   int rc = dispatch_EG(ctx->fftE, ctx->fftG, [&](auto e, auto g) {
     constexpr int E = decltype(e)::value, G = decltype(g)::value;
-    cudaFuncSetAttribute(k_products<E, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_products<E, G><<<grid, PROD_THREADS, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out);
+    if (comp) {
+      cudaFuncSetAttribute(k_products<E, G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_products<E, G, true><<<grid, PROD_THREADS, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out);
+    } else {
+      cudaFuncSetAttribute(k_products<E, G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_products<E, G, false><<<grid, PROD_THREADS, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out);
+    }
     return 0;
   });
   if (rc) return lsd_fail(ctx, LSD_EARG, "FFT length not supported");

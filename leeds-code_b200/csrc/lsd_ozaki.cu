@@ -136,6 +136,7 @@ constexpr int OZ_NC = 32;        // columns per chunk
 constexpr int OZ_STAGES = 2;     // bulk-copy ring
 constexpr int OZ_THREADS = 192;  // warps 0-3 epilogue (TMEM lane quarters), 4 copies, 5 MMA
 constexpr int OZ_STG = OZ_NC + 1;  // epilogue staging row (doubles)
+constexpr int OZ_MAXG = 6;       // groups (output fields) of one launch
 
 enum { OZ_VEC = 0, OZ_P = 1, OZ_GRAD = 2, OZ_ST = 3, OZ_Q = 4, OZ_NTYPE = 5 };
 
@@ -255,7 +256,7 @@ struct OzPrepArgs {
   const OzProb* probs; const int* kidx; const int* mstart; const int* mlen;
   const double* rinv;
   int8_t* A; int* erow;                  // erow [c][nrows]
-  const cplx* in0[5]; const cplx* in1[5];
+  const cplx* in0[OZ_MAXG]; const cplx* in1[OZ_MAXG];
 };
 
 template <int TYPE> struct OzT {
@@ -403,7 +404,7 @@ struct OzGemmArgs {
   int N, H, NM, Th2, HB, S, nrows, rows_per_group;
   const OzProb* probs; const int8_t* A; const int8_t* B; const int* fexp; const int* erow;
   const int* nhlist; const int* hm;
-  cplx* out0[5]; cplx* out1[5]; int zero_m0_im[5];
+  cplx* out0[OZ_MAXG]; cplx* out1[OZ_MAXG]; int zero_m0_im[OZ_MAXG];
   int* err;
 };
 
@@ -611,7 +612,7 @@ struct OzState {
 };
 
 namespace {
-constexpr int OZ_MAXG_SYNTH = 5, OZ_MAXG_ANAL = 3;  // groups per launch
+constexpr int OZ_MAXG_SYNTH = OZ_MAXG, OZ_MAXG_ANAL = 4;  // groups per launch
 
 template <int TYPE>
 void oz_set_smem(size_t smem) {
@@ -745,7 +746,7 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   ga.N = ctx->N; ga.H = ctx->H; ga.NM = ctx->NM; ga.Th2 = ctx->Th2; ga.HB = ctx->HB; ga.S = o->S; ga.nrows = nrows;
   ga.rows_per_group = rpg; ga.probs = o->d_probs; ga.A = o->d_A; ga.B = o->d_B; ga.fexp = o->d_fexp;
   ga.erow = o->d_erow; ga.nhlist = o->d_nh; ga.hm = ctx->d_m; ga.err = o->d_err;
-  for (int i = 0; i < 5; ++i) {
+  for (int i = 0; i < OZ_MAXG; ++i) {
     const bool on = i < ng;
     pa.in0[i] = on ? gs[i].in0 : nullptr; pa.in1[i] = on ? gs[i].in1 : nullptr;
     ga.out0[i] = on ? gs[i].out0 : nullptr; ga.out1[i] = on ? gs[i].out1 : nullptr;

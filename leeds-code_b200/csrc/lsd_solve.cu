@@ -19,7 +19,7 @@ namespace {
 enum SpecSlot {
   S_VQ = 0, S_VS, S_VT, S_VCQ, S_VCS, S_VCT,
   S_BQ, S_BS, S_BT, S_BCQ, S_BCS, S_BCT,
-  S_DC, S_NSPEC_EVAL
+  S_DC, S_DCOMP, S_NSPEC_EVAL
 };
 
 struct SpecArgs {
@@ -97,12 +97,13 @@ __global__ void k_drC(SpecArgs a, const cplx* c, cplx* dc) {
 //   vel: cq += Ra r Pm^2/Pr C (+ comp) ; NTor = qstllcurlr(t) ; NPol = qstllcurlcurlr(q,s)
 //   mag: NPol = qstllcurlr(t) ; NTor = qstllcurlcurlr(q,s)
 //   cod: NC = analysed scalar, NC(:, nh=0) += source ;  nh = 0 columns zeroed for vel/mag
+//   comp (when stepped): the same with source_comp (nonlinear.F90:341-356)
 struct TailArgs {
   SpecArgs s;
-  double Ra, Ra_comp, Pm2, Pr, Sc, source;
-  const cplx *vq, *vs, *vt, *bq, *bs, *bt, *cod;
+  double Ra, Ra_comp, Pm2, Pr, Sc, source, source_comp;
+  const cplx *vq, *vs, *vt, *bq, *bs, *bt, *cod, *comp;  // comp: nullptr when not stepped
   const cplx *C, *Comp;
-  cplx *vNTor, *vNPol, *bNTor, *bNPol, *codNC;
+  cplx *vNTor, *vNPol, *bNTor, *bNPol, *codNC, *compNC;
 };
 
 __global__ void k_tail(TailArgs a) {
@@ -148,6 +149,11 @@ __global__ void k_tail(TailArgs a) {
   double2 cv = a.cod[id];
   if (nh == 0) cv.x = cv.x + a.source;
   a.codNC[id] = cv;
+  if (a.comp) {
+    double2 xv = a.comp[id];
+    if (nh == 0) xv.x = xv.x + a.source_comp;
+    a.compNC[id] = xv;
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -639,9 +645,14 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   k_curl<<<g, 128, 0, s>>>(sa, sp + S_BQ * F, sp + S_BS * F, sp + S_BT * F, sp + S_BCQ * F, sp + S_BCS * F, sp + S_BCT * F);
   k_drC<<<g, 128, 0, s>>>(sa, st + LSD_COD_C * F, sp + S_DC * F);
   ctx->launches += 5;
+  const bool comp = ctx->cfg.comp_tstep != 0;
+  if (comp) {  // comp_transform (composition.F90:196-212)
+    k_drC<<<g, 128, 0, s>>>(sa, st + LSD_COMP_C * F, sp + S_DCOMP * F);
+    ctx->launches++;
+  }
   if (marks) cudaEventRecord(marks[0], s);
   cplx* fo = ctx->d_four;
-  SynthGroup sg[5];
+  SynthGroup sg[6];
   const int vin[4][3] = {{S_VQ, S_VS, S_VT}, {S_VCQ, S_VCS, S_VCT}, {S_BQ, S_BS, S_BT}, {S_BCQ, S_BCS, S_BCT}};
   for (int i = 0; i < 4; ++i) {
     sg[i].kind = SK_VECTOR;
@@ -650,13 +661,17 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   sg[4].kind = SK_GRAD3;
   sg[4].in[0] = sp + S_DC * F; sg[4].in[1] = st + LSD_COD_C * F; sg[4].in[2] = nullptr;
   for (int k = 0; k < 3; ++k) sg[4].out[k] = fo + (12 + k) * FF;
+  sg[5].kind = SK_GRAD3;
+  sg[5].in[0] = sp + S_DCOMP * F; sg[5].in[1] = st + LSD_COMP_C * F; sg[5].in[2] = nullptr;
+  for (int k = 0; k < 3; ++k) sg[5].out[k] = fo + (15 + k) * FF;
+  const int nsyn = comp ? 18 : 15;  // synthesised fields (FFT layout)
   int rc;
-  if ((rc = lsd_launch_synth(ctx, sg, 5))) return rc;
+  if ((rc = lsd_launch_synth(ctx, sg, comp ? 6 : 5))) return rc;
   if (marks) cudaEventRecord(marks[1], s);
-  cplx* fa = fo + 15 * FF;  // the 7 product fields, in the analysis layout
+  cplx* fa = fo + nsyn * FF;  // the 7 (8) product fields, in the analysis layout
   if ((rc = lsd_launch_products(ctx, fo, fa))) return rc;
   if (marks) cudaEventRecord(marks[2], s);
-  AnalGroup ag[3];
+  AnalGroup ag[4];
   ag[0].kind = AK_VECTOR;
   ag[1].kind = AK_VECTOR;
   ag[2].kind = AK_SCALAR;
@@ -666,21 +681,26 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   }
   ag[2].in[0] = fa + 6 * FF; ag[2].out[0] = sp + S_DC * F;
   ag[2].in[1] = ag[2].in[2] = nullptr; ag[2].out[1] = ag[2].out[2] = nullptr;
-  if ((rc = lsd_launch_anal(ctx, ag, 3))) return rc;
+  ag[3].kind = AK_SCALAR;
+  ag[3].in[0] = fa + 7 * FF; ag[3].out[0] = sp + S_DCOMP * F;
+  ag[3].in[1] = ag[3].in[2] = nullptr; ag[3].out[1] = ag[3].out[2] = nullptr;
+  if ((rc = lsd_launch_anal(ctx, ag, comp ? 4 : 3))) return rc;
   if (marks) cudaEventRecord(marks[3], s);
   TailArgs ta;
   ta.s = sa;
   const lsd_config& c = ctx->cfg;
   ta.Ra = c.Ra; ta.Ra_comp = c.Ra_comp; ta.Pm2 = c.Pm * c.Pm; ta.Pr = c.Pr; ta.Sc = c.Sc;
-  ta.source = c.source;
+  ta.source = c.source; ta.source_comp = c.source_comp;
   ta.vq = sp + S_VQ * F; ta.vs = sp + S_VS * F; ta.vt = sp + S_VT * F;
   ta.bq = sp + S_BQ * F; ta.bs = sp + S_BS * F; ta.bt = sp + S_BT * F;
   ta.cod = sp + S_DC * F;
+  ta.comp = comp ? sp + S_DCOMP * F : nullptr;
   ta.C = st + LSD_COD_C * F;
   ta.Comp = st + LSD_COMP_C * F;
   ta.vNTor = ctx->d_nl + LSD_N_VEL_TOR * F; ta.vNPol = ctx->d_nl + LSD_N_VEL_POL * F;
   ta.bNTor = ctx->d_nl + LSD_N_MAG_TOR * F; ta.bNPol = ctx->d_nl + LSD_N_MAG_POL * F;
   ta.codNC = ctx->d_nl + LSD_N_COD * F;
+  ta.compNC = ctx->d_nl + LSD_N_COMP * F;
   k_tail<<<g, 128, 0, s>>>(ta);
   ctx->launches++;
   if (marks) cudaEventRecord(marks[4], s);

@@ -27,11 +27,13 @@ def chebyshev_grid(N, rratio, alpha=-1.0):
 
 
 def boussinesq_state(cfg, seed=SEED, amplitude=1e-3, fields=(capi.VEL_TOR, capi.VEL_POL, capi.COD_C,
-                                                             capi.MAG_TOR, capi.MAG_POL)):
+                                                             capi.MAG_TOR, capi.MAG_POL),
+                     composition=False):
     """dict field -> (re, im), each (H, N) == Fortran coll (N, H).
 
-    Draw order: for each field in (uT, uP, C, BT, BP), one (H_file, 2) standard-normal
-    block in the state-file (m-major) harmonic order of io_state_nh."""
+    Draw order: for each field in (uT, uP, C, BT, BP) and then, with composition=True,
+    Comp, one (H_file, 2) standard-normal block in the state-file (m-major) harmonic order
+    of io_state_nh (so the first five fields do not depend on composition)."""
     L, M, Mp, N = cfg.L, cfg.M, cfg.Mp, cfg.N
     l, m_, _ = folded_harmonics(L, M, Mp)
     H = len(l)
@@ -43,7 +45,11 @@ def boussinesq_state(cfg, seed=SEED, amplitude=1e-3, fields=(capi.VEL_TOR, capi.
     amp = np.zeros(H)
     amp[l > 0] = amplitude / l[l > 0].astype(np.float64) ** 2
     out = {}
-    for f in (capi.VEL_TOR, capi.VEL_POL, capi.COD_C, capi.MAG_TOR, capi.MAG_POL):
+    order = [capi.VEL_TOR, capi.VEL_POL, capi.COD_C, capi.MAG_TOR, capi.MAG_POL]
+    if composition:
+        order.append(capi.COMP_C)
+        fields = tuple(fields) + (capi.COMP_C,)
+    for f in order:
         z = rng.standard_normal((H, 2))[idx]  # file order -> folded order
         re = (z[:, 0] * amp)[:, None] * prof[None, :]
         im = (z[:, 1] * amp)[:, None] * prof[None, :]
