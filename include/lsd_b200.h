@@ -135,6 +135,12 @@ int lsd_config_default(lsd_config* cfg);
  * all computed in FP64 on the device.  Replaces `initialise` (main.F90:220-380) up to
  * the state load.  Checks par_precompute (parameters.F90_template:274-288). */
 int lsd_create(const lsd_config* cfg, lsd_ctx** out);
+/* Anelastic reference state: the seven columns of planet_model.txt.in as read by
+ * io_load_radial_txtfiles (io.F90:559-608), prof[7][N] = rho, xi = rho'/rho, dxi/dr,
+ * T, dT/dr, eta, deta/dr.  Rebuilds the radial bands and weights (mes_rdom_init,
+ * meshs.F90:228-415) and the operators.  Only for cfg.boussinesq = 0 contexts; until it
+ * is called such a context uses rho = T = eta = 1 with zero gradients. */
+int lsd_set_reference_state(lsd_ctx* ctx, const double* prof);
 int lsd_destroy(lsd_ctx* ctx);
 const char* lsd_last_error(const lsd_ctx* ctx);
 int lsd_get_sizes(const lsd_ctx* ctx, lsd_sizes* out);
@@ -182,6 +188,19 @@ int lsd_tra_rtp2qst(lsd_ctx* ctx, const double* r, const double* th, const doubl
                     double* t_re, double* t_im);
 /* tra_grad (transform.fftw3.F90:955-1000) */
 int lsd_tra_grad(lsd_ctx* ctx, const double* s_re, const double* s_im, double* th, double* ph);
+/* tra_dth (transform.fftw3.F90:1006-1031) */
+int lsd_tra_dth(lsd_ctx* ctx, const double* s_re, const double* s_im, double* p);
+/* tra_qst2rtp_vel (transform.fftw3.F90:611-714), the anelastic velocity: from (q,s,t) and
+ * their radial derivatives (qr,sr,tr) the eight fields r, th, ph, dur, qv1, dutr, dupr, qv2 */
+int lsd_tra_qst2rtp_vel(lsd_ctx* ctx,
+                        const double* q_re, const double* q_im,
+                        const double* s_re, const double* s_im,
+                        const double* t_re, const double* t_im,
+                        const double* qr_re, const double* qr_im,
+                        const double* sr_re, const double* sr_im,
+                        const double* tr_re, const double* tr_im,
+                        double* r, double* th, double* ph, double* dur, double* qv1,
+                        double* dutr, double* dupr, double* qv2);
 
 /* ---- device-resident batched transforms (inputs already in HBM) ----------------------
  * d_spec: nbatch spectral fields, interleaved complex, [batch][N][H] (harmonic fastest).

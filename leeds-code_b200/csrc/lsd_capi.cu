@@ -32,7 +32,8 @@ void free_ctx(lsd_ctx* ctx) {
                   ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,
                   ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y, ctx->d_yt,
                   ctx->d_ipiv, ctx->d_ipivs, ctx->d_info, ctx->d_gre, ctx->d_gret, ctx->d_invg, ctx->d_state, ctx->d_nl,
-                  ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red};
+                  ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red, ctx->d_ref, ctx->d_laps,
+                  ctx->d_compr1dr, ctx->d_wts, ctx->d_ones};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -215,7 +216,6 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   else if (c.L <= (c.M - 1) * c.Mp) why = "set L > (M-1)*Mp";
   else if (c.M % 2 == 1) why = "if(M>1) set M even";
   else if (c.Nic != 1) why = "only an insulating inner core (Nic = 1) is supported";
-  else if (!c.boussinesq) why = "only the Boussinesq equations are supported";
   else if (c.timestep <= 0.0) why = "only a fixed timestep (d_timestep > 0) is supported";
   else if (!c.vel_tstep || !c.cod_tstep || !c.mag_tstep) why = "velocity, codensity and field must all be stepped";
   else if (c.precision != LSD_PREC_FP64 && c.precision != LSD_PREC_OZAKI) why = "unknown precision";
@@ -311,10 +311,30 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   TRY(dalloc(ctx, &ctx->d_gp, Th)); TRY(dalloc(ctx, &ctx->d_gw, Th));
   TRY(dalloc(ctx, &ctx->d_sn, Th)); TRY(dalloc(ctx, &ctx->d_sn1, Th));
   TRY(dalloc(ctx, &ctx->d_r, (size_t)7 * N));
+  ctx->d_rinv = ctx->d_r + (size_t)2 * N;
+  TRY(dalloc(ctx, &ctx->d_ones, N));
+  TRY(upload(ctx, ctx->d_ones, std::vector<double>(N, 1.0)));
   TRY(dalloc(ctx, &ctx->d_dr, (size_t)KL * (2 * KL + 1) * N));
   TRY(dalloc(ctx, &ctx->d_r1dr, (size_t)(2 * KL + 1) * N));
   TRY(dalloc(ctx, &ctx->d_radlap, (size_t)(2 * KL + 1) * N));
   TRY(dalloc(ctx, &ctx->d_intr2dr, N));
+  TRY(dalloc(ctx, &ctx->d_ref, (size_t)7 * N));
+  TRY(dalloc(ctx, &ctx->d_laps, (size_t)LAP_NBAND * (2 * KL + 1) * N));
+  TRY(dalloc(ctx, &ctx->d_compr1dr, (size_t)(2 * KL + 1) * N));
+  TRY(dalloc(ctx, &ctx->d_wts, (size_t)4 * N));
+  {  // reference state: Boussinesq rho = T = 0, eta = 1 (io.F90:545-556); anelastic until
+     // lsd_set_reference_state: rho = T = eta = 1, gradients 0
+    std::vector<double> ref((size_t)7 * N, 0.0);
+    for (int n = 0; n < N; ++n) {
+      ref[(size_t)REF_ETA * N + n] = 1.0;
+      if (!c.boussinesq) { ref[(size_t)REF_RHO * N + n] = 1.0; ref[(size_t)REF_T * N + n] = 1.0; }
+    }
+    TRY(upload(ctx, ctx->d_ref, ref));
+  }
+  for (int nh = 0; nh < H; ++nh) {
+    if (ctx->hl[nh] == 1 && ctx->hm[nh] == 0) ctx->nh_l1m0 = nh;
+    if (ctx->hl[nh] == 1 && ctx->hm[nh] == 1) ctx->nh_l1m1 = nh;
+  }
   const size_t lus = (size_t)OP_NFAM * L * N * (3 * KL + 1);
   TRY(dalloc(ctx, &ctx->d_lu, lus)); TRY(dalloc(ctx, &ctx->d_lus, lus));
   TRY(dalloc(ctx, &ctx->d_y, (size_t)OP_NFAM * N * (2 * KL + 1) * L));
@@ -329,11 +349,17 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   CTRY(cudaMemset(ctx->d_state, 0, sizeof(cplx) * LSD_NFIELD * F));
   CTRY(cudaMemset(ctx->d_nl, 0, sizeof(cplx) * LSD_NFIELD * F));
   CTRY(cudaMemset(ctx->d_sv, 0, sizeof(cplx) * LSD_NFIELD * F));
-  ctx->nspec = 14;  // 12 solve work columns / evaluation slots + dC + dComp
+  // 12 solve work columns / evaluation slots + dC + dComp (+ dr q, dr s, dr t, anelastic)
+  ctx->nspec = c.boussinesq ? 14 : 17;
   TRY(dalloc(ctx, &ctx->d_spec, (size_t)ctx->nspec * F));
   // 15 synthesised fields (FFT layout) + 7 products (analysis layout); composition adds
-  // grad Comp (3) and its product (1)
-  ctx->nfour = c.comp_tstep ? 26 : 22;
+  // grad Comp (3) and its product (1), the anelastic equations dr u (3)
+  ctx->nfour = 22 + (c.comp_tstep ? 4 : 0) + (c.boussinesq ? 0 : 3);
+  if (lsd_products_smem(ctx) > 224 * 1024) {
+    int rc2 = lsd_fail(ctx, LSD_EARG, "the products' FFT rows of this field set do not fit in shared memory at this M");
+    free_ctx(ctx);
+    return rc2;
+  }
   TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * ctx->HB * NM * 4));
   TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));
@@ -345,6 +371,24 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
 #undef TRY
 #undef CTRY
   *out = ctx;
+  return LSD_OK;
+}
+
+int lsd_set_reference_state(lsd_ctx* ctx, const double* prof) {
+  if (!ctx || !prof) return LSD_EARG;
+  if (ctx->cfg.boussinesq) return lsd_fail(ctx, LSD_EARG, "reference state: the context solves the Boussinesq equations");
+  const int N = ctx->N;
+  for (int n = 0; n < N; ++n)
+    if (!(prof[(size_t)REF_RHO * N + n] > 0.0) || !(prof[(size_t)REF_T * N + n] > 0.0))
+      return lsd_fail(ctx, LSD_EARG, "reference state: rho and T must be positive at every shell");
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_ref, prof, sizeof(double) * 7 * N, cudaMemcpyHostToDevice, ctx->stream));
+  int rc = lsd_build_radial(ctx);
+  if (rc) return rc;
+  rc = lsd_build_operators(ctx);
+  if (rc) return rc;
+  ctx->have_refstate = true;
+  ctx->have_eval = false;
   return LSD_OK;
 }
 
@@ -574,6 +618,68 @@ int lsd_tra_grad(lsd_ctx* ctx, const double* s_re, const double* s_im, double* t
   size_t P = phys_count(ctx);
   CUDA_TRY(cudaMemcpy(th, ctx->d_phys, sizeof(double) * P, cudaMemcpyDeviceToHost));
   CUDA_TRY(cudaMemcpy(ph, ctx->d_phys + P, sizeof(double) * P, cudaMemcpyDeviceToHost));
+  return LSD_OK;
+}
+
+// tra_dth (transform.fftw3.F90:1006-1031): the theta part of tra_grad without the 1/r
+int lsd_tra_dth(lsd_ctx* ctx, const double* s_re, const double* s_im, double* p) {
+  if (!ctx || !s_re || !s_im || !p) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc;
+  if ((rc = ensure_phys(ctx, 3))) return rc;
+  if ((rc = spec_in(ctx, 0, s_re, s_im))) return rc;
+  const size_t FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
+  SynthGroup g;
+  g.kind = SK_GRAD2;
+  g.in[0] = ctx->d_spec; g.in[1] = g.in[2] = nullptr;
+  g.out[0] = ctx->d_four; g.out[1] = ctx->d_four + FF; g.out[2] = nullptr;
+  if ((rc = time_begin(ctx))) return rc;
+  ctx->d_rinv = ctx->d_ones;  // c * 1.0 == c: the sums of tra_dth
+  rc = lsd_launch_synth(ctx, &g, 1);
+  ctx->d_rinv = ctx->d_r + (size_t)2 * ctx->N;
+  if (rc) return rc;
+  if ((rc = lsd_launch_c2r(ctx, ctx->d_four, ctx->d_phys, 1))) return rc;
+  if ((rc = time_end(ctx))) return rc;
+  CUDA_TRY(cudaMemcpy(p, ctx->d_phys, sizeof(double) * phys_count(ctx), cudaMemcpyDeviceToHost));
+  return LSD_OK;
+}
+
+// tra_qst2rtp_vel (transform.fftw3.F90:611-714): two vector syntheses, (q, s, t) and
+// (dq, ds, dt), and qv1 / qv2 formed from the u_th, u_ph theta-Fourier rows.
+int lsd_tra_qst2rtp_vel(lsd_ctx* ctx, const double* q_re, const double* q_im, const double* s_re,
+                        const double* s_im, const double* t_re, const double* t_im, const double* qr_re,
+                        const double* qr_im, const double* sr_re, const double* sr_im, const double* tr_re,
+                        const double* tr_im, double* r, double* th, double* ph, double* dur, double* qv1,
+                        double* dutr, double* dupr, double* qv2) {
+  const double* in[12] = {q_re, q_im, s_re, s_im, t_re, t_im, qr_re, qr_im, sr_re, sr_im, tr_re, tr_im};
+  double* out[8] = {r, th, ph, dur, qv1, dutr, dupr, qv2};
+  if (!ctx) return LSD_EARG;
+  for (const double* p : in) if (!p) return LSD_EARG;
+  for (double* p : out) if (!p) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc;
+  if ((rc = ensure_phys(ctx, 8))) return rc;
+  const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
+  for (int k = 0; k < 6; ++k) {  // one pinned slot, reused: upload field by field
+    if ((rc = spec_in(ctx, 0, in[2 * k], in[2 * k + 1]))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_spec + (size_t)(6 + k) * F, ctx->d_spec, sizeof(cplx) * F,
+                             cudaMemcpyDeviceToDevice, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  cplx* fo = ctx->d_four;
+  SynthGroup g[2];
+  const int slots[2][3] = {{0, 1, 2}, {3, 5, 6}};  // r th ph ; dur dutr dupr
+  for (int i = 0; i < 2; ++i) {
+    g[i].kind = SK_VECTOR;
+    for (int k = 0; k < 3; ++k) { g[i].in[k] = ctx->d_spec + (size_t)(6 + 3 * i + k) * F; g[i].out[k] = fo + slots[i][k] * FF; }
+  }
+  if ((rc = time_begin(ctx))) return rc;
+  if ((rc = lsd_launch_synth(ctx, g, 2))) return rc;
+  if ((rc = lsd_launch_qv(ctx, fo + 1 * FF, fo + 2 * FF, fo + 4 * FF, fo + 7 * FF))) return rc;
+  if ((rc = lsd_launch_c2r(ctx, fo, ctx->d_phys, 8))) return rc;
+  if ((rc = time_end(ctx))) return rc;
+  size_t P = phys_count(ctx);
+  for (int k = 0; k < 8; ++k) CUDA_TRY(cudaMemcpy(out[k], ctx->d_phys + k * P, sizeof(double) * P, cudaMemcpyDeviceToHost));
   return LSD_OK;
 }
 

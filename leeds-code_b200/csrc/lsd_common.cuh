@@ -35,6 +35,11 @@ enum OpFamily {
   OP_NFAM = 7
 };
 
+// reference-state bands (d_laps): meshs.F90:364-406
+enum LapBand { LAP_COMP = 0, LAP_GRE = 1, LAP_MAGTOR = 2, LAP_MAGPOL = 3, LAP_NBAND = 4 };
+// reference-state columns (d_ref, [7][N]): io.F90:559-608
+enum RefCol { REF_RHO = 0, REF_XI = 1, REF_DXI = 2, REF_T = 3, REF_DT = 4, REF_ETA = 5, REF_DETA = 6 };
+
 // synthesis group kinds (one CTA group = one output triple)
 enum SynthKind {
   SK_VECTOR = 0,  // (q,s,t) -> (r,th,ph)                 tra_qst2rtp  :719-818
@@ -91,6 +96,7 @@ struct lsd_ctx {
   int *d_aperm = nullptr;  // [Hc][Hr] analysis thread order
   int *d_sblk_l = nullptr, *d_sblk_nh = nullptr;  // solve blocks: degree, [16] harmonics
   int nsblk = 0;
+  int nh_l1m0 = -1, nh_l1m1 = -1;  // toroidal modes of vel_angmomclr
   // device Legendre tables, each [H][Th2] (== Fortran (Th2, H))
   double *d_leg = nullptr;  // 8 tables contiguous, LSD_LEG_* order
   double *d_gp = nullptr, *d_gw = nullptr, *d_sn = nullptr, *d_sn1 = nullptr;
@@ -100,10 +106,16 @@ struct lsd_ctx {
   int fftG = 1, fftE = 1;     // phi FFT: P2 = fftE * fftG (lanes x registers)
   // radial mesh
   double *d_r = nullptr;       // [7][N]: r^p, p = -3..3
+  const double* d_rinv = nullptr;  // 1/r used by the gradient syntheses (d_r + 2N; ones for tra_dth)
+  double *d_ones = nullptr;        // [N] ones
   double *d_dr = nullptr;      // [KL][N][2KL+1] bands (column-major per band, like Fortran)
   double *d_r1dr = nullptr;    // [N][2KL+1]
   double *d_radlap = nullptr;  // [N][2KL+1]
   double *d_intr2dr = nullptr; // [N]
+  // reference state [7][N] (RefCol order), its bands [LAP_NBAND][N][2KL+1], compr1dr
+  // [N][2KL+1] and the weighted integration weights [4][N] (comp, compS, magdiss, veldiss)
+  double *d_ref = nullptr, *d_laps = nullptr, *d_compr1dr = nullptr, *d_wts = nullptr;
+  bool have_refstate = false;
   // operators: LAPACK band LU [fam][L][N][3KL+1] + ipiv [fam][L][N]; Y bands
   // [fam][L][N][2KL+1]; (d_lus / d_ipivs: [fam][N][3KL+1][L] copies, l fastest)
   double *d_lu = nullptr, *d_lus = nullptr, *d_y = nullptr, *d_yt = nullptr;
@@ -145,6 +157,7 @@ int lsd_fail(lsd_ctx* ctx, int code, const std::string& msg);
 
 // ---- tables (lsd_tables.cu) ----
 int lsd_build_tables(lsd_ctx* ctx);
+int lsd_build_radial(lsd_ctx* ctx);
 int lsd_build_operators(lsd_ctx* ctx);
 // ---- transforms (lsd_sht.cu, lsd_fft.cu) ----
 int lsd_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups);
@@ -153,6 +166,8 @@ int lsd_launch_c2r(lsd_ctx* ctx, const cplx* four, double* phys, int nfields);
 int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields);
 bool lsd_fft_plan(lsd_ctx* c);
 int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out);
+size_t lsd_products_smem(const lsd_ctx* ctx);
+int lsd_launch_qv(lsd_ctx* ctx, const cplx* th, const cplx* ph, cplx* qv1, cplx* qv2);
 // ---- spectral algebra and solves (lsd_solve.cu) ----
 int lsd_eval(lsd_ctx* ctx);            // one nonlinear evaluation (device)
 int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks);

@@ -36,7 +36,7 @@
 namespace {
 
 struct FFTPlanDev {
-  int P2, Ph, M, NM, Th, Th2, HB;
+  int P2, Ph, M, NM, Th, Th2, HB, Mp;
   const double2* tw2;  // e^{+2 pi i k/P2}, k < P2
   const double2* twh;  // e^{+2 pi i k/Ph}, k < Ph
   const int* thm;      // m-counter -> bin
@@ -338,53 +338,159 @@ __device__ __forceinline__ double2 row_unpack(const double2* row, int b, const F
   return r2c_unpack(b, row[ppos<G>(b)], row[ppos<G>(b == 0 ? 0 : pl.P2 - b)], pl);
 }
 
-// ---- fused: 15 (18) theta-Fourier inputs -> products -> 7 (8) theta-Fourier outputs ----
+// ---- fused: theta-Fourier inputs -> products -> theta-Fourier outputs ---------------------
+// Product sets (the physical-space loops of nonlinear.F90):
+//   PS_BOUSS       u, w = curl u, B, J = curl B, grad C (15)      -> u x w + Coriolis +
+//                  Lorentz (3), u x B (3), -Pr/Pm u.grad C (1)      (:70-146, 269-272, 421-430)
+//   PS_BOUSS_COMP  + grad Comp (18)                                  -> + -Sc/Pm u.grad Comp (8)
+//   PS_ANEL_MOM    u, w, B, J (12) -> momentum with the compressible viscous force and
+//                  the Lorentz force / rho (3), u x B (3)            (:70-146)
+//   PS_ANEL_SCAL   u, w, J, grad C, dr u_r, dr u_th, dr u_ph (15) + qv1, qv2 (derived) ->
+//                  entropy with dissipation (1)                      (:239-266)
+//   PS_ANEL_SCAL_COMP  + grad Comp (18) -> + composition (2)         (:317-331)
+// qv1 and qv2 (tra_qst2rtp_vel, transform.fftw3.F90:678-700) are not synthesised: with
+// qva = m/sin llsin1mP - cot llP_ and qvb = cot llsin1mP - m/sin llP_ (legendre.F90:97-100)
+// the Legendre sums collapse, per theta row and order m, to
+//   qv1_m = (cot u_th,m + i m/sin u_ph,m) / r,   qv2_m = (i m/sin u_th,m - cot u_ph,m) / r,
+// which are formed from the staged u_th, u_ph bins of the same CTA.
+enum ProdSet { PS_BOUSS = 0, PS_BOUSS_COMP, PS_ANEL_MOM, PS_ANEL_SCAL, PS_ANEL_SCAL_COMP };
+template <int PS> struct PSet;
+template <> struct PSet<PS_BOUSS> { static constexpr int in = 15, deriv = 0, out = 7; };
+template <> struct PSet<PS_BOUSS_COMP> { static constexpr int in = 18, deriv = 0, out = 8; };
+template <> struct PSet<PS_ANEL_MOM> { static constexpr int in = 12, deriv = 0, out = 6; };
+template <> struct PSet<PS_ANEL_SCAL> { static constexpr int in = 15, deriv = 2, out = 1; };
+template <> struct PSet<PS_ANEL_SCAL_COMP> { static constexpr int in = 18, deriv = 2, out = 2; };
+constexpr int PROD_MAXIN = 18;
+
 struct ProdConst {
-  double d_Cor, Cmag, d_qm1, d_qm1c;
-  const double* sn;  // sin(theta_j)
-  const double* gp;  // cos(theta_j)
+  double d_Cor, Cmag, d_qm1, d_qm1c, Pm, E, Diss;
+  const double* sn;   // sin(theta_j)
+  const double* gp;   // cos(theta_j)
+  const double* sn1;  // 1/sin(theta_j)
+  const double* r;    // [7][N] powers of r
+  const double* ref;  // [7][N] reference state (anelastic)
+  int fin[PROD_MAXIN];  // input field slots of four_in
 };
 
-// inputs u, curl u, B, curl B, grad C (+ grad Comp); outputs u x curl u + Coriolis +
-// Lorentz (3), u x B (3), -Pr/Pm u.grad C (+ -Sc/Pm u.grad Comp)
-template <bool COMP> struct ProdFields {
-  static constexpr int in = COMP ? 18 : 15, out = COMP ? 8 : 7;
-};
+// per-shell constants of the anelastic sets
+struct ShellC { double xi0, xi1, rm1, rinv, rrr, rho, T0, dT0, eta, Cmag; };
+
+template <int PS>
+__device__ __forceinline__ void prod_point(const double* v, double* o, const ProdConst& pc, const ShellC& sh,
+                                           double sn, double cs) {
+  if constexpr (PS == PS_BOUSS || PS == PS_BOUSS_COMP || PS == PS_ANEL_MOM) {
+    const double vr = v[0], vt = v[1], vp = v[2];
+    const double wr = v[3], wt = v[4], wp = v[5];
+    const double br = v[6], bt = v[7], bp = v[8];
+    const double jr = v[9], jt = v[10], jp = v[11];
+    double a = vt * wp - vp * wt;
+    double b = vp * wr - vr * wp;
+    double c = vr * wt - vt * wr;
+    double Cmag = pc.Cmag;
+    if constexpr (PS == PS_ANEL_MOM) {  // compressible viscous force (nonlinear.F90:93-110)
+      double f = -(2.0 * sh.xi0 * sh.rm1) - sh.xi1;
+      f = f - (sh.xi0 * sh.xi0) / 3.0;
+      a = a + pc.Pm * vr * f;
+      double d1 = 2.0 * sh.xi0 * sh.rm1 + sh.xi1;
+      d1 = d1 + sh.xi0 * sh.xi0;
+      b = b - pc.Pm * (sh.xi0 * wp + d1 * vt);
+      c = c + pc.Pm * (sh.xi0 * wt - d1 * vp);
+      Cmag = sh.Cmag;
+    }
+    a = a + pc.d_Cor * sn * vp;
+    b = b + pc.d_Cor * cs * vp;
+    c = c - pc.d_Cor * (cs * vt + sn * vr);
+    a = a + Cmag * (jt * bp - jp * bt);
+    b = b + Cmag * (jp * br - jr * bp);
+    c = c + Cmag * (jr * bt - jt * br);
+    o[0] = a; o[1] = b; o[2] = c;
+    o[3] = vt * bp - vp * bt;
+    o[4] = vp * br - vr * bp;
+    o[5] = vr * bt - vt * br;
+    if constexpr (PS != PS_ANEL_MOM) {
+      const double cr = v[12], ct = v[13], cp = v[14];
+      o[6] = -pc.d_qm1 * vr * cr - pc.d_qm1 * vt * ct - pc.d_qm1 * vp * cp;
+    }
+    if constexpr (PS == PS_BOUSS_COMP) {  // non_composition (nonlinear.F90:294-341)
+      const double xr = v[15], xt = v[16], xp = v[17];
+      o[7] = -pc.d_qm1c * vr * xr - pc.d_qm1c * vt * xt - pc.d_qm1c * vp * xp;
+    }
+  } else {  // PS_ANEL_SCAL(_COMP): inputs u 0-2, w 3-5, J 6-8, grad C 9-11, du 12-14, grad Comp 15-17
+    constexpr int NI = PSet<PS>::in;
+    const double vr = v[0], vt = v[1], vp = v[2];
+    const double wr = v[3], wt = v[4], wp = v[5];
+    const double jr = v[6], jt = v[7], jp = v[8];
+    const double gr = v[9], gt = v[10], gq = v[11];
+    const double dur = v[12], dutr = v[13], dupr = v[14];
+    const double qv1 = v[NI], qv2 = v[NI + 1];
+    double x = 2.0 * (dur * dur);
+    double y = (sh.xi0 + 1.0 / sh.rrr) * vr + dur + qv1;
+    x = x + 2.0 * (y * y);
+    y = sh.xi0 * vr;
+    x = x - 2.0 * (y * y) / 3.0;
+    y = qv1 + vr / sh.rrr;
+    x = x + 2.0 * (y * y);
+    y = 2.0 * dutr - wp;
+    x = x + y * y;
+    y = 2.0 * dupr + wt;
+    x = x + y * y;
+    y = 2.0 * qv2 + wr;
+    x = x + y * y;
+    x = x + sh.eta * ((jr * jr + jp * jp + jt * jt) / (sh.rho * pc.E));
+    double e = -(pc.d_qm1 * vr * gr) + (sh.dT0 / sh.T0) * gr;
+    e = e - pc.d_qm1 * vt * gt;
+    e = e - pc.d_qm1 * vp * gq;
+    o[0] = e + (pc.Diss / sh.T0) * x;
+    if constexpr (PS == PS_ANEL_SCAL_COMP) {
+      const double xr = v[15], xt = v[16], xp = v[17];
+      o[1] = -pc.d_qm1c * vr * xr - pc.d_qm1c * vt * xt - pc.d_qm1c * vp * xp;
+    }
+  }
+}
 
 // grid (2 HB, N): one half-row h = blockIdx.x (its southern and northern theta row) per
-// CTA, 256 threads, two CTAs per SM so that one's memory waits overlap the other's work.
-// Every thread loads its share of all 15 input blocks into registers at the start (all
-// loads in flight at once); the blocks then pass through a double-buffered bin-order
-// stage into the padded rows [NF_IN][2][E (G+1)].
+// CTA, 256 threads, up to two CTAs per SM so that one's memory waits overlap the other's
+// work.  Every thread loads its share of all input blocks into registers at the start
+// (all loads in flight at once); the blocks then pass through a double-buffered bin-order
+// stage into the padded rows [NF][2][E (G+1)] (NF = inputs + derived rows).
 constexpr int PROD_THREADS = 256;
 
-template <int E, int G, bool COMP>
+template <int E, int G, int PS>
 __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int N, ProdConst pc,
                                                               const cplx* four_in, cplx* four_out) {
   constexpr int RS = E * (G + 1), P2 = E * G;
-  constexpr int NF_IN = ProdFields<COMP>::in, NF_OUT = ProdFields<COMP>::out;
+  constexpr int NF_IN = PSet<PS>::in, NDER = PSet<PS>::deriv, NF = NF_IN + NDER, NF_OUT = PSet<PS>::out;
   extern __shared__ __align__(16) unsigned char psm[];
   const int n = blockIdx.y, h = blockIdx.x, hb = h >> 1, jj = h & 1;
   const int NM = pl.NM, M = pl.M, Th = pl.Th, Th2 = pl.Th2;
   if (h >= Th2) return;  // padding half-row of an odd Th2
-  double2* rows = (double2*)psm;                 // [NF_IN][2][RS]
-  double2* stage = rows + (size_t)NF_IN * 2 * RS;  // [2 buffers][2 (E/O)][M]
+  double2* rows = (double2*)psm;                 // [NF][2][RS]
+  double2* stage = rows + (size_t)NF * 2 * RS;   // [2 buffers][2 (E/O)][M]
   const FFTTabs tabs = fft_tabs_init<E, G>((unsigned char*)(stage + (size_t)4 * M), pl);
   const int BLK = NM * 4;                        // one field's (n, h/2) block
   const size_t fstride = (size_t)N * pl.HB * BLK;
   const size_t boff = ((size_t)n * pl.HB + hb) * BLK + jj;  // element (c, p) at boff + 2 (2c + p)
   const int tid = threadIdx.x, NE = NM * 2;                 // (c, p) elements of this half-row
+  ShellC sh{};
+  if constexpr (PS >= PS_ANEL_MOM) {
+    const double* ref = pc.ref;
+    sh.xi0 = ref[REF_XI * N + n]; sh.xi1 = ref[REF_DXI * N + n];
+    sh.rho = ref[REF_RHO * N + n]; sh.T0 = ref[REF_T * N + n]; sh.dT0 = ref[REF_DT * N + n];
+    sh.eta = ref[REF_ETA * N + n];
+    sh.rm1 = pc.r[(size_t)2 * N + n]; sh.rinv = sh.rm1; sh.rrr = pc.r[(size_t)4 * N + n];
+    sh.Cmag = pc.Pm / (pc.E * sh.rho);
+  }
   // ---- all loads first: element tid of every field (the rest, for NM > 128, later)
   double2 pre[NF_IN];
 #pragma unroll
   for (int f = 0; f < NF_IN; ++f)
-    pre[f] = tid < NE ? four_in[(size_t)f * fstride + boff + 2 * tid] : make_double2(0.0, 0.0);
+    pre[f] = tid < NE ? four_in[(size_t)pc.fin[f] * fstride + boff + 2 * tid] : make_double2(0.0, 0.0);
   // ---- per field: bin-order stage (double buffer), then the packed half spectra
 #pragma unroll
   for (int f = 0; f < NF_IN; ++f) {
     double2* sp = stage + (size_t)(f & 1) * 2 * M;  // [p][M]
     for (int i = tid; i < NE; i += PROD_THREADS) {
-      const double2 val = i == tid ? pre[f] : four_in[(size_t)f * fstride + boff + 2 * i];
+      const double2 val = i == tid ? pre[f] : four_in[(size_t)pc.fin[f] * fstride + boff + 2 * i];
       sp[(i & 1) * M + tabs.thm[i >> 1]] = val;
     }
     __syncthreads();
@@ -395,51 +501,54 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
       const double2 ym = km < M ? (side ? sub2(sp[km], sp[M + km]) : add2(sp[km], sp[M + km])) : make_double2(0.0, 0.0);
       rows[(size_t)(f * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, yk, ym, pl);
     }
+    if constexpr (NDER > 0) {
+      if (f == 2) {  // u_th staged in buffer 1, u_ph in buffer 0: the qv1, qv2 rows
+        const double2* sth = stage + (size_t)2 * M;
+        const double2* sph = stage;
+        for (int i = tid; i < 2 * P2; i += PROD_THREADS) {
+          const int side = i / P2, k = i - side * P2;
+          const int j = row_theta(h, side, Th);
+          const double s1 = pc.sn1[j], cot = pc.gp[j] * s1;
+          auto bins = [&](int b, double2& q1, double2& q2) {
+            if (b >= M) { q1 = q2 = make_double2(0.0, 0.0); return; }
+            const double2 t = side ? sub2(sth[b], sth[M + b]) : add2(sth[b], sth[M + b]);
+            const double2 p = side ? sub2(sph[b], sph[M + b]) : add2(sph[b], sph[M + b]);
+            const double mk = (double)(b * pl.Mp) * s1;
+            q1 = make_double2(sh.rinv * (cot * t.x - mk * p.y), sh.rinv * (cot * t.y + mk * p.x));
+            q2 = make_double2(sh.rinv * (-mk * t.y - cot * p.x), sh.rinv * (mk * t.x - cot * p.y));
+          };
+          double2 q1k, q2k, q1m, q2m;
+          bins(k, q1k, q2k);
+          bins(k == 0 ? P2 : P2 - k, q1m, q2m);
+          rows[(size_t)(NF_IN * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, q1k, q1m, pl);
+          rows[(size_t)((NF_IN + 1) * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, q2k, q2m, pl);
+        }
+        __syncthreads();  // buffer 1 is restaged by field 3
+      }
+    }
   }
   __syncthreads();
-  // ---- inverse FFTs of the 30 rows
-  col_pass<E, G, +1>(rows, NF_IN * 2, tabs);
+  // ---- inverse FFTs of the 2 NF rows
+  col_pass<E, G, +1>(rows, NF * 2, tabs);
   __syncthreads();
-  row_pass<E, G, +1>(rows, NF_IN * 2, tabs);
+  row_pass<E, G, +1>(rows, NF * 2, tabs);
   __syncthreads();
-  // ---- products at every point (row side, sample position, part re/im), in place into 0..6
+  // ---- products at every point (row side, sample position, part re/im), in place into 0..NF_OUT-1
   const double scale = 1.0 / (double)pl.Ph;
   for (int i = tid; i < 2 * P2; i += PROD_THREADS) {
     const int r = i / P2, pos = ppos<G>(i - r * P2);
     const int j = row_theta(h, r, Th);
     const double sn = pc.sn[j], cs = pc.gp[j];
-    double2 v[NF_IN];
+    double2 v[NF];
 #pragma unroll
-    for (int f = 0; f < NF_IN; ++f) v[f] = rows[(size_t)(f * 2 + r) * RS + pos];
+    for (int f = 0; f < NF; ++f) v[f] = rows[(size_t)(f * 2 + r) * RS + pos];
     double2 out[NF_OUT];
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
-#define G_(f) (part == 0 ? v[f].x : v[f].y)
-      const double vr = G_(0), vt = G_(1), vp = G_(2);
-      const double wr = G_(3), wt = G_(4), wp = G_(5);
-      const double br = G_(6), bt = G_(7), bp = G_(8);
-      const double jr = G_(9), jt = G_(10), jp = G_(11);
-      const double cr = G_(12), ct = G_(13), cp = G_(14);
-      double a = vt * wp - vp * wt;
-      double b = vp * wr - vr * wp;
-      double c = vr * wt - vt * wr;
-      a = a + pc.d_Cor * sn * vp;
-      b = b + pc.d_Cor * cs * vp;
-      c = c - pc.d_Cor * (cs * vt + sn * vr);
-      a = a + pc.Cmag * (jt * bp - jp * bt);
-      b = b + pc.Cmag * (jp * br - jr * bp);
-      c = c + pc.Cmag * (jr * bt - jt * br);
-      const double e0 = vt * bp - vp * bt;
-      const double e1 = vp * br - vr * bp;
-      const double e2 = vr * bt - vt * br;
-      const double cod = -pc.d_qm1 * vr * cr - pc.d_qm1 * vt * ct - pc.d_qm1 * vp * cp;
-      double o[NF_OUT];
-      o[0] = a; o[1] = b; o[2] = c; o[3] = e0; o[4] = e1; o[5] = e2; o[6] = cod;
-      if constexpr (COMP) {  // non_composition (nonlinear.F90:294-341), Boussinesq
-        const double xr = G_(15), xt = G_(16), xp = G_(17);
-        o[NF_OUT - 1] = -pc.d_qm1c * vr * xr - pc.d_qm1c * vt * xt - pc.d_qm1c * vp * xp;
-      }
-#undef G_
+      double x[NF], o[NF_OUT];
+#pragma unroll
+      for (int f = 0; f < NF; ++f) x[f] = part == 0 ? v[f].x : v[f].y;
+      prod_point<PS>(x, o, pc, sh, sn, cs);
 #pragma unroll
       for (int q = 0; q < NF_OUT; ++q) {
         if (part == 0) out[q].x = o[q] * scale; else out[q].y = o[q] * scale;
@@ -449,7 +558,7 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
     for (int q = 0; q < NF_OUT; ++q) rows[(size_t)(q * 2 + r) * RS + pos] = out[q];
   }
   __syncthreads();
-  // ---- forward FFTs of the 14 product rows (spectrum back in natural order)
+  // ---- forward FFTs of the product rows (spectrum back in natural order)
   row_pass<E, G, -1>(rows, NF_OUT * 2, tabs);
   __syncthreads();
   col_pass<E, G, -1>(rows, NF_OUT * 2, tabs);
@@ -541,10 +650,36 @@ __global__ void __launch_bounds__(128) k_r2c(FFTPlanDev pl, int N, const double*
   }
 }
 
+// qv1, qv2 of tra_qst2rtp_vel (transform.fftw3.F90:678-700) from the u_th, u_ph
+// theta-Fourier rows, on the even/odd half-grid sums: cot theta is odd about the equator,
+// so it swaps E and O, while 1/sin theta keeps them (the identity is stated at PS_ANEL_SCAL).
+__global__ void k_qv_four(FFTPlanDev pl, int N, const double* rinv, const double* gp, const double* sn1,
+                          const cplx* th, const cplx* ph, cplx* q1, cplx* q2) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (n, hb, c, h & 1)
+  const size_t total = (size_t)N * pl.HB * pl.NM * 2;
+  if (i >= total) return;
+  const int hh = (int)(i & 1), c = (int)((i >> 1) % pl.NM);
+  const size_t nb = (i >> 1) / pl.NM;
+  const int hb = (int)(nb % pl.HB), n = (int)(nb / pl.HB), h = 2 * hb + hh;
+  const size_t oE = four_off(n, c, 0, h, pl.NM, pl.HB), oO = four_off(n, c, 1, h, pl.NM, pl.HB);
+  if (h >= pl.Th2) {
+    q1[oE] = q1[oO] = q2[oE] = q2[oO] = make_double2(0.0, 0.0);
+    return;
+  }
+  const double s1 = sn1[h], cot = gp[h] * s1, ri = rinv[n];
+  const double mk = (double)(pl.thm[c] * pl.Mp) * s1;
+  const double2 te = th[oE], to = th[oO], pe = ph[oE], po = ph[oO];
+  // i mk (x + i y) = (-mk y, mk x)
+  q1[oE] = make_double2(ri * (cot * to.x - mk * pe.y), ri * (cot * to.y + mk * pe.x));
+  q1[oO] = make_double2(ri * (cot * te.x - mk * po.y), ri * (cot * te.y + mk * po.x));
+  q2[oE] = make_double2(ri * (-mk * te.y - cot * po.x), ri * (mk * te.x - cot * po.y));
+  q2[oO] = make_double2(ri * (-mk * to.y - cot * pe.x), ri * (mk * to.x - cot * pe.y));
+}
+
 FFTPlanDev make_plan(lsd_ctx* ctx) {
   FFTPlanDev pl;
   pl.P2 = ctx->P2; pl.Ph = ctx->Ph; pl.M = ctx->M; pl.NM = ctx->NM; pl.Th = ctx->Th; pl.Th2 = ctx->Th2;
-  pl.HB = ctx->HB;
+  pl.HB = ctx->HB; pl.Mp = ctx->Mp;
   pl.tw2 = ctx->d_tw2; pl.twh = ctx->d_twh; pl.thm = ctx->d_thm;
   return pl;
 }
@@ -608,31 +743,19 @@ int lsd_launch_r2c(lsd_ctx* ctx, const double* phys, cplx* four, int nfields) {
   return LSD_OK;
 }
 
-int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
+namespace {
+template <int PS>
+int launch_products_set(lsd_ctx* ctx, const ProdConst& pc, const cplx* four_in, cplx* four_out) {
   FFTPlanDev pl = make_plan(ctx);
-  ProdConst pc;
-  const lsd_config& c = ctx->cfg;
-  pc.d_Cor = 2.0 * c.Pm / c.E;
-  pc.Cmag = 2 * c.Pm / c.E;
-  pc.d_qm1 = c.Pr / c.Pm;
-  pc.d_qm1c = c.Sc / c.Pm;
-  pc.sn = ctx->d_sn;
-  pc.gp = ctx->d_gp;
-  const bool comp = c.comp_tstep != 0;
-  const int nf_in = comp ? ProdFields<true>::in : ProdFields<false>::in;
-  const size_t smem = sizeof(double2) * ((size_t)nf_in * 2 * ctx->fftE * (ctx->fftG + 1) + (size_t)4 * ctx->M) +
+  constexpr int NF = PSet<PS>::in + PSet<PS>::deriv;
+  const size_t smem = sizeof(double2) * ((size_t)NF * 2 * ctx->fftE * (ctx->fftG + 1) + (size_t)4 * ctx->M) +
                       fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
   if (smem > 224 * 1024) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
   dim3 grid(2 * ctx->HB, ctx->N);
   int rc = dispatch_EG(ctx->fftE, ctx->fftG, [&](auto e, auto g) {
     constexpr int E = decltype(e)::value, G = decltype(g)::value;
-    if (comp) {
-      cudaFuncSetAttribute(k_products<E, G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_products<E, G, true><<<grid, PROD_THREADS, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out);
-    } else {
-      cudaFuncSetAttribute(k_products<E, G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_products<E, G, false><<<grid, PROD_THREADS, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out);
-    }
+    cudaFuncSetAttribute(k_products<E, G, PS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_products<E, G, PS><<<grid, PROD_THREADS, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out);
     return 0;
   });
   if (rc) return lsd_fail(ctx, LSD_EARG, "FFT length not supported");
@@ -640,4 +763,60 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_products: ") + cudaGetErrorString(e));
   return LSD_OK;
+}
+}  // namespace
+
+int lsd_launch_qv(lsd_ctx* ctx, const cplx* th, const cplx* ph, cplx* qv1, cplx* qv2) {
+  FFTPlanDev pl = make_plan(ctx);
+  const size_t total = (size_t)ctx->N * ctx->HB * ctx->NM * 2;
+  k_qv_four<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(pl, ctx->N, ctx->d_r + (size_t)2 * ctx->N,
+                                                                      ctx->d_gp, ctx->d_sn1, th, ph, qv1, qv2);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_qv_four: ") + cudaGetErrorString(e));
+  return LSD_OK;
+}
+
+size_t lsd_products_smem(const lsd_ctx* ctx) {
+  const bool comp = ctx->cfg.comp_tstep != 0;
+  int nf = comp ? 18 : 15;
+  if (!ctx->cfg.boussinesq) nf = (comp ? 18 : 15) + 2;
+  return sizeof(double2) * ((size_t)nf * 2 * ctx->fftE * (ctx->fftG + 1) + (size_t)4 * ctx->M) +
+         fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
+}
+
+// four_in: the synthesised fields in the FFT layout, slots u 0-2, curl u 3-5, B 6-8,
+// curl B 9-11, grad C 12-14, grad Comp 15-17 (composition), then (anelastic) dr u_r,
+// dr u_th, dr u_ph; four_out: the products in the analysis layout, slots 0-2 momentum,
+// 3-5 u x B, 6 codensity, 7 composition.
+int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
+  ProdConst pc;
+  const lsd_config& c = ctx->cfg;
+  pc.d_Cor = 2.0 * c.Pm / c.E;
+  pc.Cmag = 2 * c.Pm / c.E;
+  pc.d_qm1 = c.Pr / c.Pm;
+  pc.d_qm1c = c.Sc / c.Pm;
+  pc.Pm = c.Pm;
+  pc.E = c.E;
+  pc.Diss = pc.d_qm1 * pc.d_qm1 / c.Ra;
+  pc.sn = ctx->d_sn;
+  pc.gp = ctx->d_gp;
+  pc.sn1 = ctx->d_sn1;
+  pc.r = ctx->d_r;
+  pc.ref = ctx->d_ref;
+  const bool comp = c.comp_tstep != 0;
+  const size_t FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
+  if (c.boussinesq) {
+    for (int f = 0; f < PROD_MAXIN; ++f) pc.fin[f] = f;
+    return comp ? launch_products_set<PS_BOUSS_COMP>(ctx, pc, four_in, four_out)
+                : launch_products_set<PS_BOUSS>(ctx, pc, four_in, four_out);
+  }
+  for (int f = 0; f < PROD_MAXIN; ++f) pc.fin[f] = f < 12 ? f : 0;
+  int rc = launch_products_set<PS_ANEL_MOM>(ctx, pc, four_in, four_out);
+  if (rc) return rc;
+  const int du = comp ? 18 : 15;
+  const int sl[PROD_MAXIN] = {0, 1, 2, 3, 4, 5, 9, 10, 11, 12, 13, 14, du, du + 1, du + 2, 15, 16, 17};
+  for (int f = 0; f < PROD_MAXIN; ++f) pc.fin[f] = sl[f];
+  return comp ? launch_products_set<PS_ANEL_SCAL_COMP>(ctx, pc, four_in, four_out + 6 * FF)
+              : launch_products_set<PS_ANEL_SCAL>(ctx, pc, four_in, four_out + 6 * FF);
 }

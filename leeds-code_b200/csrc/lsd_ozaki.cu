@@ -136,7 +136,7 @@ constexpr int OZ_NC = 32;        // columns per chunk
 constexpr int OZ_STAGES = 2;     // bulk-copy ring
 constexpr int OZ_THREADS = 192;  // warps 0-3 epilogue (TMEM lane quarters), 4 copies, 5 MMA
 constexpr int OZ_STG = OZ_NC + 1;  // epilogue staging row (doubles)
-constexpr int OZ_MAXG = 6;       // groups (output fields) of one launch
+constexpr int OZ_MAXG = 8;       // groups (output fields) of one launch
 
 enum { OZ_VEC = 0, OZ_P = 1, OZ_GRAD = 2, OZ_ST = 3, OZ_Q = 4, OZ_NTYPE = 5 };
 
@@ -741,7 +741,7 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   OzPrepArgs pa;
   pa.N = ctx->N; pa.H = ctx->H; pa.NM = ctx->NM; pa.Th2 = ctx->Th2; pa.HB = ctx->HB; pa.S = o->S; pa.nrows = nrows;
   pa.rows_per_group = rpg; pa.probs = o->d_probs; pa.kidx = o->d_kidx; pa.mstart = ctx->d_mstart;
-  pa.mlen = ctx->d_mlen; pa.rinv = ctx->d_r + (size_t)2 * ctx->N; pa.A = o->d_A; pa.erow = o->d_erow;
+  pa.mlen = ctx->d_mlen; pa.rinv = ctx->d_rinv; pa.A = o->d_A; pa.erow = o->d_erow;
   OzGemmArgs ga;
   ga.N = ctx->N; ga.H = ctx->H; ga.NM = ctx->NM; ga.Th2 = ctx->Th2; ga.HB = ctx->HB; ga.S = o->S; ga.nrows = nrows;
   ga.rows_per_group = rpg; ga.probs = o->d_probs; ga.A = o->d_A; ga.B = o->d_B; ga.fexp = o->d_fexp;

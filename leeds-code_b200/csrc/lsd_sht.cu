@@ -293,7 +293,7 @@ int launch_synth_kind(lsd_ctx* ctx, const SynthGroup* groups, int ngroups) {
   SynthArgs a;
   a.N = ctx->N; a.H = ctx->H; a.Th = ctx->Th; a.Th2 = ctx->Th2; a.NM = ctx->NM; a.HB = ctx->HB;
   a.mstart = ctx->d_mstart; a.mlen = ctx->d_mlen; a.hs = ctx->d_s; a.leg = ctx->d_leg;
-  a.rinv = ctx->d_r + (size_t)2 * ctx->N;
+  a.rinv = ctx->d_rinv;
   int ng = 0;
   for (int i = 0; i < ngroups; ++i)
     if (groups[i].kind == KIND) a.g[ng++] = groups[i];

@@ -19,7 +19,9 @@ namespace {
 enum SpecSlot {
   S_VQ = 0, S_VS, S_VT, S_VCQ, S_VCS, S_VCT,
   S_BQ, S_BS, S_BT, S_BCQ, S_BCS, S_BCT,
-  S_DC, S_DCOMP, S_NSPEC_EVAL
+  S_DC, S_DCOMP,
+  S_VDQ, S_VDS, S_VDT,  // anelastic: dr q, dr s, dr t of the velocity (var_coll_TorPol2qstderiv)
+  S_NSPEC_EVAL
 };
 
 struct SpecArgs {
@@ -47,8 +49,9 @@ __device__ __forceinline__ double2 band_apply(const double* band, int KL, int N,
   return acc;
 }
 
-// q,s,t of a (Tor, Pol) pair: var_coll_TorPol2qst_mag (variables.F90:565-605)
-__global__ void k_qst(SpecArgs a, const cplx* tor, const cplx* pol, cplx* q, cplx* s, cplx* t) {
+// q,s,t of a (Tor, Pol) pair: var_coll_TorPol2qst_mag (variables.F90:565-605) with
+// s1dr = r1dr, the compressible var_coll_TorPol2qst (:511-556) with s1dr = compr1dr
+__global__ void k_qst(SpecArgs a, const double* s1dr, const cplx* tor, const cplx* pol, cplx* q, cplx* s, cplx* t) {
   int nh = blockIdx.x * blockDim.x + threadIdx.x;
   int n = blockIdx.y + 1;
   if (nh >= a.H) return;
@@ -58,7 +61,7 @@ __global__ void k_qst(SpecArgs a, const cplx* tor, const cplx* pol, cplx* q, cpl
   double f = ll1d(l) * rm1;
   double2 p = pol[id];
   q[id] = make_double2(p.x * f, p.y * f);
-  double2 sv = band_apply(a.r1dr, a.KL, a.N, pol + nh, a.H, n);
+  double2 sv = band_apply(s1dr, a.KL, a.N, pol + nh, a.H, n);
   double w = rtll1(l);
   s[id] = make_double2(sv.x * w, sv.y * w);
   double2 tv = tor[id];
@@ -93,6 +96,44 @@ __global__ void k_drC(SpecArgs a, const cplx* c, cplx* dc) {
   dc[(size_t)(n - 1) * a.H + nh] = band_apply(a.dr1, a.KL, a.N, c + nh, a.H, n);
 }
 
+// vel_angmomclr (velocity.F90:475-574), stress-free walls: remove the rigid rotations
+// carried by the toroidal (l, m) = (1, 0) and (1, 1) modes, the angular momentum being the
+// radial integral with the weights w (intr2dr; intr2dr_comp for the anelastic equations).
+// One CTA; thread 0 forms the three ratios in the reference's summation order.
+__global__ void k_angmom(int N, int H, int nh10, int nh11, const double* r, const double* w, int r2_as_product,
+                         cplx* tor) {
+  __shared__ double om[3];
+  const double* r1 = r + (size_t)4 * N;
+  const double* r2 = r + (size_t)5 * N;
+  if (threadIdx.x == 0) {
+    const double W = 8.0 / 3.0 * 3.1415926535897931;
+    double f2 = 0.0, a = 0.0, b = 0.0;
+    for (int n = 0; n < N; ++n) f2 = f2 + (r2_as_product ? r1[n] * r1[n] : r2[n]) * w[n];
+    om[0] = om[1] = om[2] = 0.0;
+    if (nh10 >= 0) {
+      for (int n = 0; n < N; ++n) a = a + tor[(size_t)n * H + nh10].x * r1[n] * w[n];
+      om[0] = (W * a) / (W * f2);
+    }
+    if (nh11 >= 0) {
+      a = 0.0; b = 0.0;
+      for (int n = 0; n < N; ++n) {
+        a = a + tor[(size_t)n * H + nh11].x * r1[n] * w[n];
+        b = b + tor[(size_t)n * H + nh11].y * r1[n] * w[n];
+      }
+      om[1] = (2.0 * W * a) / (2.0 * W * f2);
+      om[2] = (-2.0 * W * b) / (-2.0 * W * f2);
+    }
+  }
+  __syncthreads();
+  for (int n = threadIdx.x; n < N; n += blockDim.x) {
+    if (nh10 >= 0) tor[(size_t)n * H + nh10].x = tor[(size_t)n * H + nh10].x - om[0] * r1[n];
+    if (nh11 >= 0) {
+      tor[(size_t)n * H + nh11].x = tor[(size_t)n * H + nh11].x - om[1] * r1[n];
+      tor[(size_t)n * H + nh11].y = tor[(size_t)n * H + nh11].y - om[2] * r1[n];
+    }
+  }
+}
+
 // Tail of non_velocity / non_magnetic / non_codensity after the analysis:
 //   vel: cq += Ra r Pm^2/Pr C (+ comp) ; NTor = qstllcurlr(t) ; NPol = qstllcurlcurlr(q,s)
 //   mag: NPol = qstllcurlr(t) ; NTor = qstllcurlcurlr(q,s)
@@ -100,6 +141,7 @@ __global__ void k_drC(SpecArgs a, const cplx* c, cplx* dc) {
 //   comp (when stepped): the same with source_comp (nonlinear.F90:341-356)
 struct TailArgs {
   SpecArgs s;
+  const double* dT0;  // anelastic: dTemp0/dr per shell (buoyancy -Ra T0' Pm^2/Pr); null: Ra r
   double Ra, Ra_comp, Pm2, Pr, Sc, source, source_comp;
   const cplx *vq, *vs, *vt, *bq, *bs, *bt, *cod, *comp;  // comp: nullptr when not stepped
   const cplx *C, *Comp;
@@ -124,14 +166,17 @@ __global__ void k_tail(TailArgs a) {
   } else {
     double2 vt = a.vt[id];
     a.vNTor[id] = make_double2(-vt.x * w, -vt.y * w);
-    // buoyancy d2 = Ra*r*(Pm**2)/Pr (nonlinear.F90:158-185)
+    // buoyancy d2 = Ra*r*(Pm**2)/Pr, anelastic -Ra*Temp0'*(Pm**2)/Pr (nonlinear.F90:158-185)
     double2 q = a.vq[id];
     double2 c = a.C[id];
-    double d2 = a.Ra * r1 * a.Pm2 / a.Pr;
+    const double g = a.dT0 ? a.dT0[n - 1] : r1;
+    double d2 = a.Ra * g * a.Pm2 / a.Pr;
+    if (a.dT0) d2 = -d2;
     q.x = q.x + d2 * c.x;
     q.y = q.y + d2 * c.y;
     double2 cm = a.Comp[id];
-    double d2c = a.Ra_comp * r1 * a.Pm2 / a.Sc;
+    double d2c = a.Ra_comp * g * a.Pm2 / a.Sc;
+    if (a.dT0) d2c = -d2c;
     q.x = q.x + d2c * cm.x;
     q.y = q.y + d2c * cm.y;
     double2 rs = band_apply(s.r1dr, s.KL, s.N, a.vs + nh, s.H, n);
@@ -181,7 +226,7 @@ struct StepArgs {
   cplx* sv;
   cplx* work;   // scratch: two column sets per field, [2 field + k][N][H]
   double implicit;
-  int cod_bc, comp_bc;
+  int cod_bc, comp_bc, vel_bc;
   double qi, qo, qi_comp, qo_comp;
   int comp;
   double* red;  // corrector: [8] sums of squares
@@ -481,7 +526,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_corrector(StepArgs a) {
     const double2 z2 = make_double2(0.0, 0.0);
     const double c = a.implicit;
     // nc = c (N - N_saved) ; N_saved = N ; zerobc (tim_nlincorr, timestep.F90:696-715)
-    const bool tor10 = job == J_VTOR && l == 1 && a.hm[nh] == 0;  // vel_setbc_Tor (Re part)
+    // vel_setbc_Tor (Re part; velocity.F90:291-299): only no-slip walls (i_vel_bc <= 2)
+    const bool tor10 = job == J_VTOR && l == 1 && a.hm[nh] == 0 && a.vel_bc <= 2;
     auto inC = [&](int n) {
       const double2 x = __ldg(v.Nn + (size_t)n * rst), p = __ldg(v.S + (size_t)n * rst);
       v.S[(size_t)n * rst] = x;
@@ -617,7 +663,7 @@ StepArgs step_args(lsd_ctx* ctx) {
   a.state = ctx->d_state; a.nl = ctx->d_nl; a.sv = ctx->d_sv;
   a.work = ctx->d_spec;
   a.implicit = ctx->cfg.implicit;
-  a.cod_bc = ctx->cfg.cod_bc; a.comp_bc = ctx->cfg.comp_bc;
+  a.cod_bc = ctx->cfg.cod_bc; a.comp_bc = ctx->cfg.comp_bc; a.vel_bc = ctx->cfg.vel_bc;
   a.qi = ctx->cfg.qi; a.qo = ctx->cfg.qo; a.qi_comp = ctx->cfg.qi_comp; a.qo_comp = ctx->cfg.qo_comp;
   a.comp = ctx->cfg.comp_tstep;
   a.red = ctx->d_red;
@@ -639,8 +685,16 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   SpecArgs sa = spec_args(ctx);
   dim3 g(ceil_div(ctx->H, 128), ctx->N);
   cudaStream_t s = ctx->stream;
-  k_qst<<<g, 128, 0, s>>>(sa, st + LSD_VEL_TOR * F, st + LSD_VEL_POL * F, sp + S_VQ * F, sp + S_VS * F, sp + S_VT * F);
-  k_qst<<<g, 128, 0, s>>>(sa, st + LSD_MAG_TOR * F, st + LSD_MAG_POL * F, sp + S_BQ * F, sp + S_BS * F, sp + S_BT * F);
+  const bool anel = ctx->cfg.boussinesq == 0;
+  if (ctx->cfg.vel_bc == 4) {  // main.F90:101
+    k_angmom<<<1, 128, 0, s>>>(ctx->N, ctx->H, ctx->nh_l1m0, ctx->nh_l1m1, ctx->d_r,
+                               anel ? ctx->d_wts : ctx->d_intr2dr, anel ? 1 : 0, st + LSD_VEL_TOR * F);
+    ctx->launches++;
+  }
+  k_qst<<<g, 128, 0, s>>>(sa, anel ? ctx->d_compr1dr : ctx->d_r1dr, st + LSD_VEL_TOR * F, st + LSD_VEL_POL * F,
+                          sp + S_VQ * F, sp + S_VS * F, sp + S_VT * F);
+  k_qst<<<g, 128, 0, s>>>(sa, ctx->d_r1dr, st + LSD_MAG_TOR * F, st + LSD_MAG_POL * F, sp + S_BQ * F, sp + S_BS * F,
+                          sp + S_BT * F);
   k_curl<<<g, 128, 0, s>>>(sa, sp + S_VQ * F, sp + S_VS * F, sp + S_VT * F, sp + S_VCQ * F, sp + S_VCS * F, sp + S_VCT * F);
   k_curl<<<g, 128, 0, s>>>(sa, sp + S_BQ * F, sp + S_BS * F, sp + S_BT * F, sp + S_BCQ * F, sp + S_BCS * F, sp + S_BCT * F);
   k_drC<<<g, 128, 0, s>>>(sa, st + LSD_COD_C * F, sp + S_DC * F);
@@ -650,9 +704,13 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
     k_drC<<<g, 128, 0, s>>>(sa, st + LSD_COMP_C * F, sp + S_DCOMP * F);
     ctx->launches++;
   }
+  if (anel) {  // dr q, dr s, dr t (var_coll_TorPol2qstderiv, variables.F90:610-660)
+    for (int k = 0; k < 3; ++k) k_drC<<<g, 128, 0, s>>>(sa, sp + (S_VQ + k) * F, sp + (S_VDQ + k) * F);
+    ctx->launches += 3;
+  }
   if (marks) cudaEventRecord(marks[0], s);
   cplx* fo = ctx->d_four;
-  SynthGroup sg[6];
+  SynthGroup sg[7];
   const int vin[4][3] = {{S_VQ, S_VS, S_VT}, {S_VCQ, S_VCS, S_VCT}, {S_BQ, S_BS, S_BT}, {S_BCQ, S_BCS, S_BCT}};
   for (int i = 0; i < 4; ++i) {
     sg[i].kind = SK_VECTOR;
@@ -664,9 +722,16 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   sg[5].kind = SK_GRAD3;
   sg[5].in[0] = sp + S_DCOMP * F; sg[5].in[1] = st + LSD_COMP_C * F; sg[5].in[2] = nullptr;
   for (int k = 0; k < 3; ++k) sg[5].out[k] = fo + (15 + k) * FF;
-  const int nsyn = comp ? 18 : 15;  // synthesised fields (FFT layout)
+  int nsyn = comp ? 18 : 15;  // synthesised fields (FFT layout)
+  int ng = comp ? 6 : 5;
+  if (anel) {  // dr u_r, dr u_th, dr u_ph: tra_qst2rtp of (dr q, dr s, dr t) (transform.fftw3.F90:611-714)
+    SynthGroup& d = sg[ng++];
+    d.kind = SK_VECTOR;
+    for (int k = 0; k < 3; ++k) { d.in[k] = sp + (S_VDQ + k) * F; d.out[k] = fo + (nsyn + k) * FF; }
+    nsyn += 3;
+  }
   int rc;
-  if ((rc = lsd_launch_synth(ctx, sg, comp ? 6 : 5))) return rc;
+  if ((rc = lsd_launch_synth(ctx, sg, ng))) return rc;
   if (marks) cudaEventRecord(marks[1], s);
   cplx* fa = fo + nsyn * FF;  // the 7 (8) product fields, in the analysis layout
   if ((rc = lsd_launch_products(ctx, fo, fa))) return rc;
@@ -688,6 +753,7 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   if (marks) cudaEventRecord(marks[3], s);
   TailArgs ta;
   ta.s = sa;
+  ta.dT0 = anel ? ctx->d_ref + (size_t)REF_DT * ctx->N : nullptr;
   const lsd_config& c = ctx->cfg;
   ta.Ra = c.Ra; ta.Ra_comp = c.Ra_comp; ta.Pm2 = c.Pm * c.Pm; ta.Pr = c.Pr; ta.Sc = c.Sc;
   ta.source = c.source; ta.source_comp = c.source_comp;
@@ -756,8 +822,9 @@ namespace {
 // The derived fields (q, s, t and curl of velocity and field), their per-(field,
 // category, shell) norms summed into d_out (48 N doubles, zeroed here first), and host
 // copies of all that the radial sums need.  d_arrs: device room for 12 pointers.
+// wts: 5 N (intr2dr, intr2dr_comp, _compS, _magdiss, _veldiss), ref: 7 N.
 int energy_partials(lsd_ctx* ctx, const cplx** d_arrs, double* d_out, double* Fh, double* wts, double* cod0,
-                    double* bpolN, double* r, double* dr1) {
+                    double* bpolN, double* r, double* dr1, double* ref) {
   const int N = ctx->N, H = ctx->H, KL = ctx->KL;
   const size_t F = (size_t)N * H;
   cplx* sp = ctx->d_spec;
@@ -765,9 +832,12 @@ int energy_partials(lsd_ctx* ctx, const cplx** d_arrs, double* d_out, double* Fh
   SpecArgs sa = spec_args(ctx);
   dim3 g(ceil_div(H, 128), N);
   cudaStream_t s = ctx->stream;
-  k_qst<<<g, 128, 0, s>>>(sa, st + LSD_VEL_TOR * F, st + LSD_VEL_POL * F, sp + 0 * F, sp + 1 * F, sp + 2 * F);
+  // velocity: the compressible var_coll_TorPol2qst (io.F90:1799); compr1dr == r1dr when xi = 0
+  k_qst<<<g, 128, 0, s>>>(sa, ctx->cfg.boussinesq ? ctx->d_r1dr : ctx->d_compr1dr, st + LSD_VEL_TOR * F,
+                          st + LSD_VEL_POL * F, sp + 0 * F, sp + 1 * F, sp + 2 * F);
   k_curl<<<g, 128, 0, s>>>(sa, sp + 0 * F, sp + 1 * F, sp + 2 * F, sp + 3 * F, sp + 4 * F, sp + 5 * F);
-  k_qst<<<g, 128, 0, s>>>(sa, st + LSD_MAG_TOR * F, st + LSD_MAG_POL * F, sp + 6 * F, sp + 7 * F, sp + 8 * F);
+  k_qst<<<g, 128, 0, s>>>(sa, ctx->d_r1dr, st + LSD_MAG_TOR * F, st + LSD_MAG_POL * F, sp + 6 * F, sp + 7 * F,
+                          sp + 8 * F);
   k_curl<<<g, 128, 0, s>>>(sa, sp + 6 * F, sp + 7 * F, sp + 8 * F, sp + 9 * F, sp + 10 * F, sp + 11 * F);
   const cplx* arrs[12];
   for (int k = 0; k < 12; ++k) arrs[k] = sp + k * F;
@@ -778,6 +848,8 @@ int energy_partials(lsd_ctx* ctx, const cplx** d_arrs, double* d_out, double* Fh
   ctx->launches += 5;
   CUDA_TRY(cudaMemcpyAsync(Fh, d_out, sizeof(double) * 48 * N, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaMemcpyAsync(wts, ctx->d_intr2dr, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(wts + N, ctx->d_wts, sizeof(double) * 4 * N, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(ref, ctx->d_ref, sizeof(double) * 7 * N, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaMemcpyAsync(r, ctx->d_r, sizeof(double) * 7 * N, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaMemcpyAsync(dr1, ctx->d_dr, sizeof(double) * (2 * KL + 1) * N, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaMemcpy2DAsync(cod0, sizeof(double), st + LSD_COD_C * F, sizeof(cplx) * H, sizeof(double), N,
@@ -790,57 +862,74 @@ int energy_partials(lsd_ctx* ctx, const cplx** d_arrs, double* d_out, double* Fh
 
 // The radial dot products and the energy combinations, on the host in the reference's order.
 int energy_finish(lsd_ctx* ctx, const double* Fh, const double* wts, const double* cod0, const double* bpolN,
-                  const double* r, const double* dr1, double* out) {
+                  const double* r, const double* dr1, const double* ref, double* out) {
   const int N = ctx->N, KL = ctx->KL;
-  auto norm = [&](int k, double& Eo, double& Ee, double& E1, double& E0) {
+  const bool bq = ctx->cfg.boussinesq != 0;
+  // radial weights: intr2dr (Boussinesq velocity), intr2dr_comp (anelastic velocity,
+  // var_coll_norm_comp), intr2dr_magdiss (ohmic dissipation, var_coll_norm_magdiss)
+  const double* wv = bq ? wts : wts + N;
+  const double* wm = wts;
+  const double* wmd = wts + 3 * N;
+  const double* wvd = wts + 4 * N;
+  auto normw = [&](int k, const double* w, double& Eo, double& Ee, double& E1, double& E0) {
     double v[4];
     for (int q = 0; q < 4; ++q) {
       double acc = 0.0;
-      for (int n = 0; n < N; ++n) acc = acc + Fh[((size_t)k * 4 + q) * N + n] * wts[n];
+      for (int n = 0; n < N; ++n) acc = acc + Fh[((size_t)k * 4 + q) * N + n] * w[n];
       v[q] = acc;
     }
     Eo = v[0]; Ee = v[1]; E1 = v[2]; E0 = v[3];
   };
-  auto surf = [&](int k, int n) { return (Fh[((size_t)k * 4 + 0) * N + n] + Fh[((size_t)k * 4 + 1) * N + n]) * r[(size_t)4 * N + n]; };
+  // var_coll_norm_surf: rho r |a|^2 on the walls (r alone for the Boussinesq equations)
+  auto surf = [&](int k, int n) {
+    double f = Fh[((size_t)k * 4 + 0) * N + n] + Fh[((size_t)k * 4 + 1) * N + n];
+    return bq ? f * r[(size_t)4 * N + n] : f * ref[REF_RHO * N + n] * r[(size_t)4 * N + n];
+  };
   for (int i = 0; i < LSD_NENERGY; ++i) out[i] = 0.0;
   out[LSD_E_TIME] = ctx->t;
   const lsd_config& c = ctx->cfg;
-  const double KE = 0.5, VD = c.Pm, ME = c.Pm / c.E, OD = 2.0 * c.Pm / c.E;
+  // io_write2files prefactors (io.F90:234-247)
+  const double KE = 0.5, VD = c.Pm;
+  const double ME = bq ? c.Pm / c.E : 0.5 * c.Pm / c.E, OD = bq ? 2.0 * c.Pm / c.E : 1.0 * c.Pm / c.E;
   const int ldm = 2 * KL + 1;
   auto D1 = [&](int row, int col) { return dr1[(size_t)(row - 1) + (size_t)ldm * (col - 1)]; };
   double flx = 0.0;
   for (int j = N - KL; j <= N; ++j) flx = flx - cod0[(size_t)(j - 1)] * D1(KL + 1 + N - j, j);
   const double PI = 3.1415926535897931;
-  out[LSD_E_TOPFLX] = 4.0 * PI * r[(size_t)5 * N + N - 1] * flx;
+  if (bq) out[LSD_E_TOPFLX] = 4.0 * PI * r[(size_t)5 * N + N - 1] * flx;
+  else out[LSD_E_TOPFLX] = 4.0 * PI * r[(size_t)5 * N + N - 1] * ref[REF_RHO * N + N - 1] * ref[REF_T * N + N - 1] * flx;
   flx = 0.0;
   for (int j = 1; j <= 1 + KL; ++j) flx = flx - cod0[(size_t)(j - 1)] * D1(KL + 2 - j, j);
-  out[LSD_E_BOTFLX] = 4.0 * PI * r[(size_t)5 * N + 0] * flx;
+  if (bq) out[LSD_E_BOTFLX] = 4.0 * PI * r[(size_t)5 * N + 0] * flx;
+  else out[LSD_E_BOTFLX] = 4.0 * PI * r[(size_t)5 * N + 0] * ref[REF_RHO * N] * ref[REF_T * N] * flx;
   double Eo, Ee, E1, E0;
   {  // velocity: arrays 0..2 q,s,t ; 3..5 curl
-    double Ep, Epas, Esym, El1, Et, Etas, EDis, ESin = 0, ESout = 0;
-    norm(0, Eo, Ee, E1, E0); Ep = Eo + Ee; Epas = E0; Esym = Ee; El1 = E1;
-    norm(1, Eo, Ee, E1, E0); Ep = Ep + Eo + Ee; Epas = Epas + E0; Esym = Esym + Ee; El1 = El1 + E1;
-    norm(2, Eo, Ee, E1, E0); Et = Eo + Ee; Etas = E0; Esym = Esym + Eo; El1 = El1 + E1;
+    double Ep, Epas, Esym, El1, Et, Etas, EDis, ESin = 0, ESout = 0, Ecomp = 0;
+    normw(0, wv, Eo, Ee, E1, E0); Ep = Eo + Ee; Epas = E0; Esym = Ee; El1 = E1;
+    if (!bq)  // var_coll_norm_veldiss of q (variables.F90:1034-1061)
+      for (int n = 0; n < N; ++n) Ecomp = Ecomp + (Fh[(size_t)0 * N + n] + Fh[(size_t)1 * N + n]) * wvd[n];
+    normw(1, wv, Eo, Ee, E1, E0); Ep = Ep + Eo + Ee; Epas = Epas + E0; Esym = Esym + Ee; El1 = El1 + E1;
+    normw(2, wv, Eo, Ee, E1, E0); Et = Eo + Ee; Etas = E0; Esym = Esym + Eo; El1 = El1 + E1;
     for (int k = 0; k < 3; ++k) { ESin = ESin + surf(k, 0); ESout = ESout + surf(k, N - 1); }
-    norm(3, Eo, Ee, E1, E0); EDis = Eo + Ee;
-    norm(4, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
-    norm(5, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    normw(3, wv, Eo, Ee, E1, E0); EDis = Eo + Ee;
+    normw(4, wv, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    normw(5, wv, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
     out[LSD_E_KE] = KE * (Ep + Et);
     out[LSD_E_KE_TOR] = KE * Et;
     out[LSD_E_KE_SYM] = KE * Esym;
     out[LSD_E_KE_L1] = KE * El1;
     out[LSD_E_KE_TM0] = KE * E0;
-    out[LSD_E_KE_DIS] = VD * EDis + VD * 2.0 * (ESin - ESout);
+    out[LSD_E_KE_DIS] = VD * EDis + VD * 2.0 * (ESin - ESout) + Ecomp;
     out[LSD_E_KE_AX] = KE * Epas + KE * Etas;
   }
   {  // magnetic: arrays 6..8, curl 9..11
     double Ep, Epas, Esym, El1, Et, Etas, ETm0, EDis;
-    norm(6, Eo, Ee, E1, E0); Ep = Eo + Ee; Epas = E0; Esym = Ee; El1 = E1;
-    norm(7, Eo, Ee, E1, E0); Ep = Ep + Eo + Ee; Epas = Epas + E0; Esym = Esym + Ee; El1 = El1 + E1;
-    norm(8, Eo, Ee, E1, E0); Et = Eo + Ee; Etas = E0; ETm0 = E0; Esym = Esym + Eo; El1 = El1 + E1;
-    norm(9, Eo, Ee, E1, E0); EDis = Eo + Ee;
-    norm(10, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
-    norm(11, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    normw(6, wm, Eo, Ee, E1, E0); Ep = Eo + Ee; Epas = E0; Esym = Ee; El1 = E1;
+    normw(7, wm, Eo, Ee, E1, E0); Ep = Ep + Eo + Ee; Epas = Epas + E0; Esym = Esym + Ee; El1 = El1 + E1;
+    normw(8, wm, Eo, Ee, E1, E0); Et = Eo + Ee; Etas = E0; ETm0 = E0; Esym = Esym + Eo; El1 = El1 + E1;
+    normw(9, wmd, Eo, Ee, E1, E0); EDis = Eo + Ee;
+    normw(10, wmd, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    normw(11, wmd, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
     out[LSD_E_ME] = ME * (Ep + Et);
     out[LSD_E_ME_TOR] = ME * Et;
     out[LSD_E_ME_SYM] = ME * Esym;
@@ -860,11 +949,12 @@ int energy_finish(lsd_ctx* ctx, const double* Fh, const double* wts, const doubl
 // io.F90:1933-2024): device norms, host radial dot products in the reference's order.
 int lsd_energy_device(lsd_ctx* ctx, double* out) {
   const int N = ctx->N, KL = ctx->KL;
-  std::vector<double> Fh((size_t)48 * N), wts(N), cod0(N), bpolN(3 * 2), r(N * 7), dr1((size_t)(2 * KL + 1) * N);
+  std::vector<double> Fh((size_t)48 * N), wts(5 * N), cod0(N), bpolN(3 * 2), r(N * 7), dr1((size_t)(2 * KL + 1) * N),
+      ref(7 * N);
   int rc = energy_partials(ctx, (const cplx**)(ctx->d_red + 64), ctx->d_red + 128, Fh.data(), wts.data(),
-                           cod0.data(), bpolN.data(), r.data(), dr1.data());
+                           cod0.data(), bpolN.data(), r.data(), dr1.data(), ref.data());
   if (rc) return rc;
-  return energy_finish(ctx, Fh.data(), wts.data(), cod0.data(), bpolN.data(), r.data(), dr1.data(), out);
+  return energy_finish(ctx, Fh.data(), wts.data(), cod0.data(), bpolN.data(), r.data(), dr1.data(), ref.data(), out);
 }
 
 // ---- energies with no allocation -------------------------------------------------------
@@ -895,7 +985,7 @@ int lsd_energy_static(lsd_ctx* ctx, double* out) {
              ESTATIC_MAX_N);
     return lsd_fail(ctx, LSD_EARG, msg);
   }
-  const size_t stage = (size_t)(48 + 1 + 1 + 7 + 2 * KL + 1) * N + 6;
+  const size_t stage = (size_t)(48 + 5 + 1 + 7 + 2 * KL + 1 + 7) * N + 6;
   if (sizeof(double) * stage > ctx->h_pin_bytes)
     return lsd_fail(ctx, LSD_EARG, "lsd_energies_static: the context's pinned staging buffer is too small");
   if (ctx->dev < 0 || ctx->dev >= ESTATIC_MAX_DEV) return lsd_fail(ctx, LSD_EARG, "lsd_energies_static: device index");
@@ -910,13 +1000,14 @@ int lsd_energy_static(lsd_ctx* ctx, double* out) {
   }
   double* Fh = ctx->h_pin;
   double* wts = Fh + (size_t)48 * N;
-  double* cod0 = wts + N;
+  double* cod0 = wts + (size_t)5 * N;
   double* bpolN = cod0 + N;
   double* r = bpolN + 6;
   double* dr1 = r + (size_t)7 * N;
-  int rc = energy_partials(ctx, (const cplx**)dscr, dscr + ESTATIC_PTRS, Fh, wts, cod0, bpolN, r, dr1);
+  double* ref = dr1 + (size_t)(2 * KL + 1) * N;
+  int rc = energy_partials(ctx, (const cplx**)dscr, dscr + ESTATIC_PTRS, Fh, wts, cod0, bpolN, r, dr1, ref);
   if (rc) return rc;
-  return energy_finish(ctx, Fh, wts, cod0, bpolN, r, dr1, out);
+  return energy_finish(ctx, Fh, wts, cod0, bpolN, r, dr1, ref, out);
 }
 
 // ---- boundary layout: coll Re/Im (N, H) column-major <-> device [n][nh] complex ---------

@@ -122,7 +122,9 @@ __global__ void k_legendre(int L, int M, int Mp, int H, int Th2, const double* g
 }
 
 // ---------------------------------------------------------------------------------------
-// Radial mesh (meshs.F90:135-143, 228-419), Boussinesq profile (rho = 0, eta = 1)
+// Radial mesh (meshs.F90:135-143, 228-419).  The reference state ref[7][N] (rho, xi,
+// dxi/dr, T, dT/dr, eta, deta/dr) is zero with eta = 1 for the Boussinesq equations
+// (io.F90:545-556) and the planet model of the anelastic ones (io.F90:559-608).
 // ---------------------------------------------------------------------------------------
 __global__ void k_grid(int N, double rratio, double alpha, double* r) {
   int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -173,34 +175,68 @@ __global__ void k_fdweights(int N, int KL, const double* r, double* dr, double* 
 #undef Aa
 }
 
-// intr2dr(j) = sum over n ascending, i ascending of the contributions (meshs.F90:311-336)
-__global__ void k_intr2dr(int N, int KL, const double* wcontrib, double* intr2dr) {
+// intr2dr(j) = sum over n ascending, i ascending of the contributions (meshs.F90:311-336),
+// with the weighted variants wts[4][N]: intr2dr_comp (rho), intr2dr_compS (rho T),
+// intr2dr_magdiss (eta), intr2dr_veldiss (2 rho (dxi/dr - xi^2/3))
+__global__ void k_intr2dr(int N, int KL, const double* wcontrib, const double* ref, double* intr2dr, double* wts) {
   int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (j > N) return;
   const int lda = 2 * KL + 1;
-  double s = 0.0;
+  double s = 0.0, sc = 0.0, ss = 0.0, sm = 0.0, sv = 0.0;
   for (int n = max(1, j - KL); n <= min(j + KL, N); ++n) {
     int l = max(1, n - KL), rr = min(n + KL, N), nn = rr - l + 1;
-    for (int i = 1; i <= nn; ++i) s = s + wcontrib[((size_t)(n - 1) * lda + (i - 1)) * lda + (j - l)];
+    const double rho = ref[n - 1], xi = ref[N + n - 1], dxi = ref[2 * N + n - 1];
+    const double T = ref[3 * N + n - 1], eta = ref[5 * N + n - 1];
+    for (int i = 1; i <= nn; ++i) {
+      const double w = wcontrib[((size_t)(n - 1) * lda + (i - 1)) * lda + (j - l)];
+      s = s + w;
+      sc = sc + w * rho;
+      ss = ss + w * (rho * T);
+      sm = sm + w * eta;
+      sv = sv + w * 2.0 * rho * (dxi - xi * xi / 3.0);
+    }
   }
   intr2dr[j - 1] = s;
+  wts[j - 1] = sc;
+  wts[N + j - 1] = ss;
+  wts[2 * N + j - 1] = sm;
+  wts[3 * N + j - 1] = sv;
 }
 
-// radLap = dr2 + dr1*2/r ; r1dr = dr1 + diag(1/r)   (meshs.F90:339-415)
-__global__ void k_bands(int N, int KL, const double* r, const double* dr, double* radlap, double* r1dr) {
+// radLap = dr2 + dr1*2/r ; r1dr = dr1 + diag(1/r) ; the reference-state bands
+// laps[LAP_*] and compr1dr = dr1 + diag(1/r + xi)   (meshs.F90:339-415)
+__global__ void k_bands(int N, int KL, const double* r, const double* dr, const double* ref, double* radlap,
+                        double* r1dr, double* laps, double* compr1dr) {
   int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (j > N) return;
   const size_t band = (size_t)(2 * KL + 1) * N;
   const double* rm1 = r + (size_t)2 * N;
+  const double* xi = ref + N;
+  const double* eta = ref + (size_t)5 * N;
+  const double* deta = ref + (size_t)6 * N;
   for (int row = 1; row <= 2 * KL + 1; ++row) {
     size_t id = (size_t)(row - 1) + (size_t)(2 * KL + 1) * (j - 1);
     int n = row - KL - 1 + j;
-    double v = 0.0;
-    if (n >= 1 && n <= N) v = dr[band + id] + dr[id] * 2.0 * rm1[n - 1];
+    double v = 0.0, cl = 0.0, gl = 0.0, mt = 0.0, mp = 0.0;
+    if (n >= 1 && n <= N) {
+      const double d1 = dr[id], d2 = dr[band + id];
+      v = d2 + d1 * 2.0 * rm1[n - 1];
+      cl = d2 + 2.0 * (xi[n - 1] + rm1[n - 1]) * d1;                          // CompLap
+      mt = eta[n - 1] * (d2 + 2.0 * rm1[n - 1] * d1) + deta[n - 1] * d1;     // MagTorLap
+      mp = eta[n - 1] * (d2 + 2.0 * rm1[n - 1] * d1);                        // MagPolLap
+      gl = d2 + (xi[n - 1] + 2.0 * rm1[n - 1]) * d1;                          // GreLap
+    }
     radlap[id] = v;
+    laps[LAP_COMP * band + id] = cl;
+    laps[LAP_GRE * band + id] = gl;
+    laps[LAP_MAGTOR * band + id] = mt;
+    laps[LAP_MAGPOL * band + id] = mp;
     double w = dr[id];
     if (row == KL + 1) w = w + rm1[j - 1];
     r1dr[id] = w;
+    double wc = dr[id];
+    if (row == KL + 1) wc = wc + rm1[j - 1] + xi[j - 1];
+    compr1dr[id] = wc;
   }
 }
 
@@ -212,10 +248,43 @@ struct OpParams {
   double c1_[OP_NFAM], c2_[OP_NFAM], c2y[OP_NFAM];
   double Hyp;
   int vel_bc, cod_bc, comp_bc;
+  int anelastic;
 };
 
+// The diagonal term d of an anelastic operator family at shell n (1-based); X gets
+// c1_ + c2_ d and Y gets c1_ - c2y d on the diagonal (timestep.F90:47-128, 214-546).
+__device__ double anel_diag(int fam, int l, int n, int N, const double* r, const double* ref, double Hyp) {
+  const double ll1 = (double)(l * (l + 1));
+  const double rm1 = r[(size_t)2 * N + n - 1], rm2 = r[(size_t)1 * N + n - 1];
+  const double xi = ref[N + n - 1], dxi = ref[2 * N + n - 1];
+  const double eta = ref[5 * N + n - 1], deta = ref[6 * N + n - 1];
+  const double t = ll1 * rm2;
+  double d;
+  switch (fam) {
+    case OP_VTOR:
+    case OP_VPOL:  // tim_lumesh_vel_X / tim_mesh_vel_Y
+      d = t + Hyp * (t * t);
+      d = d - 2.0 * xi * rm1;
+      d = d - xi * xi;
+      return d - dxi;
+    case OP_VGRE:  // tim_lumesh_Gre_X
+      d = t - xi * rm1;
+      return d - dxi;
+    case OP_MTOR:  // tim_iclumesh_Tor_X / tim_mesh_mag_Tor_Y
+      d = ll1 * eta * rm2;
+      d = d - deta * rm1;
+      return d + Hyp * (t * t);
+    case OP_MPOL:  // tim_iclumesh_Pol_X / tim_mesh_mag_Pol_Y
+      d = ll1 * eta * rm2;
+      return d + Hyp * (t * t);
+    default:  // tim_lumesh_X / tim_mesh_Y (codensity, composition)
+      return t + Hyp * (t * t);
+  }
+}
+
 __global__ void k_build_ops(int N, int KL, int L, const double* r, const double* dr, const double* radlap,
-                            OpParams P, double* lu, int* ipiv, double* y, int* info) {
+                            const double* laps, const double* ref, OpParams P, double* lu, int* ipiv, double* y,
+                            int* info) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   int fam = blockIdx.y;
   if (l >= L) return;
@@ -236,16 +305,25 @@ __global__ void k_build_ops(int N, int KL, int L, const double* r, const double*
   }
   const double c1_ = P.c1_[fam], c2_ = P.c2_[fam], c2y = P.c2y[fam];
   const double ll1 = (double)(l * (l + 1));
-  // A(KL+1:, :) = -c2_ * Lap  (radLap == radLap_flayer == GreLap == MagTorLap == MagPolLap
-  // bit for bit in the Boussinesq case: f_factor = 1, xi = 0, eta = 1, deta = 0)
+  // A(KL+1:, :) = -c2_ * Lap.  Boussinesq: radLap == radLap_flayer == GreLap == MagTorLap
+  // == MagPolLap bit for bit (f_factor = 1, xi = 0, eta = 1, deta = 0); anelastic: CompLap
+  // (velocity), GreLap (Green's, codensity, composition), MagTorLap, MagPolLap.
+  const double* lap = radlap;
+  if (P.anelastic) {
+    const int which = (fam == OP_VTOR || fam == OP_VPOL) ? LAP_COMP
+                    : fam == OP_MTOR ? LAP_MAGTOR : fam == OP_MPOL ? LAP_MAGPOL : LAP_GRE;
+    lap = laps + which * band;
+  }
   for (int j = 1; j <= N; ++j)
     for (int row = 1; row <= ldm; ++row) {
-      double v = MB(radlap, row, j);
+      double v = MB(lap, row, j);
       AX(KL + row, j) = (fam == OP_MTOR || fam == OP_MPOL) ? 0.0 - c2_ * v : -c2_ * v;
     }
   for (int n = 1; n <= N; ++n) {
     double t = ll1 * rm2[n - 1];
-    if (fam == OP_MTOR || fam == OP_MPOL)
+    if (P.anelastic)
+      AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * anel_diag(fam, l, n, N, r, ref, P.Hyp);
+    else if (fam == OP_MTOR || fam == OP_MPOL)
       AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * ll1 * rm2[n - 1];
     else
       AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * (t + P.Hyp * t * t);
@@ -266,16 +344,24 @@ __global__ void k_build_ops(int N, int KL, int L, const double* r, const double*
         AX(2 * KL + 1, N) = AX(2 * KL + 1, N) - rm1[N - 1];
       }
       break;
-    case OP_VPOL:  // vel_bc_Pol (velocity.F90:207-254), Boussinesq
+    case OP_VPOL: {  // vel_bc_Pol (velocity.F90:207-254); anelastic stress-free adds xi dr
+      const double xi1 = P.anelastic ? ref[N] : 0.0, xiN = P.anelastic ? ref[2 * N - 1] : 0.0;
       if (P.vel_bc == 1 || P.vel_bc == 2)
         for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
-      else
+      else if (!P.anelastic)
         for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr + band, KL + 1 + 1 - j, j);
+      else
+        for (int j = 1; j <= 1 + KL; ++j)
+          AX(2 * KL + 1 + 1 - j, j) = MB(dr + band, KL + 1 + 1 - j, j) + xi1 * MB(dr, KL + 1 + 1 - j, j);
       if (P.vel_bc == 1 || P.vel_bc == 3)
         for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
-      else
+      else if (!P.anelastic)
         for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr + band, KL + 1 + N - j, j);
+      else
+        for (int j = N - KL; j <= N; ++j)
+          AX(2 * KL + 1 + N - j, j) = MB(dr + band, KL + 1 + N - j, j) + xiN * MB(dr, KL + 1 + N - j, j);
       break;
+    }
     case OP_VGRE:  // vel_bc_Gre (velocity.F90:260-267)
       AX(2 * KL + 1, 1) = 1.0;
       AX(2 * KL + 1, N) = 1.0;
@@ -301,14 +387,16 @@ __global__ void k_build_ops(int N, int KL, int L, const double* r, const double*
       break;
   }
   info[fam * L + l] = dev_dgbtf2(N, KL, A, ld, ip);
-  // Y = c2y*Lap ; diag += c1_ - c2y*(l(l+1)/r^2 + Hyp (.)^2)   (tim_mesh_Y / _flayer_Y)
+  // Y = c2y*Lap ; diag += c1_ - c2y*(l(l+1)/r^2 + Hyp (.)^2)   (tim_mesh_Y / _flayer_Y;
+  // anelastic: tim_mesh_vel_Y, tim_mesh_Y, tim_mesh_mag_Tor_Y / _Pol_Y)
   if (fam != OP_VGRE) {
     for (int j = 1; j <= N; ++j)
       for (int row = 1; row <= ldm; ++row) {
-        double v = c2y * MB(radlap, row, j);
+        double v = c2y * MB(lap, row, j);
         if (row == KL + 1) {
           double t = (double)(l * (l + 1)) * rm2[j - 1];
-          v = v + c1_ - c2y * (t + P.Hyp * t * t);
+          if (P.anelastic) v = v + c1_ - c2y * anel_diag(fam, l, j, N, r, ref, P.Hyp);
+          else v = v + c1_ - c2y * (t + P.Hyp * t * t);
         }
         y[(((size_t)fam * L + l) * N + (j - 1)) * ldm + (row - 1)] = v;
       }
@@ -374,23 +462,41 @@ int lsd_build_tables(lsd_ctx* ctx) {
   k_trig<<<ceil_div(Th, 128), 128, 0, s>>>(Th, ctx->d_gp, ctx->d_sn, ctx->d_sn1);
   dim3 gl(ceil_div(Th2, 64), M);
   k_legendre<<<gl, 64, 0, s>>>(L, M, ctx->Mp, H, Th2, ctx->d_gp, ctx->d_gw, ctx->d_sn1, ctx->d_lm2nh, ctx->d_leg, d_fail);
+  ctx->launches += 3;
+  CUDA_TRY(cudaGetLastError());
+  int fail = 0;
+  CUDA_TRY(cudaMemcpyAsync(&fail, d_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(d_fail);
+  if (fail == 2) return lsd_fail(ctx, LSD_EARG, "schnla: sin(theta) too small (legendre)");
+  if (fail) return lsd_fail(ctx, LSD_ESINGULAR, "table construction failed (code " + std::to_string(fail) + ")");
+  return lsd_build_radial(ctx);
+}
+
+// mes_precompute / mes_rdom_init (meshs.F90:116-419) on the current reference state
+int lsd_build_radial(lsd_ctx* ctx) {
+  const int N = ctx->N, KL = ctx->KL;
+  cudaStream_t s = ctx->stream;
+  int* d_fail = nullptr;
+  CUDA_TRY(cudaMalloc(&d_fail, sizeof(int)));
+  CUDA_TRY(cudaMemsetAsync(d_fail, 0, sizeof(int), s));
   k_grid<<<ceil_div(N, 128), 128, 0, s>>>(N, ctx->cfg.rratio, ctx->cfg.alpha, ctx->d_r);
   double* wc = nullptr;
   size_t lda = 2 * KL + 1;
   CUDA_TRY(cudaMalloc(&wc, sizeof(double) * N * lda * lda));
   CUDA_TRY(cudaMemsetAsync(ctx->d_dr, 0, sizeof(double) * KL * lda * N, s));
   k_fdweights<<<ceil_div(N, 64), 64, 0, s>>>(N, KL, ctx->d_r, ctx->d_dr, wc, d_fail);
-  k_intr2dr<<<ceil_div(N, 128), 128, 0, s>>>(N, KL, wc, ctx->d_intr2dr);
-  k_bands<<<ceil_div(N, 128), 128, 0, s>>>(N, KL, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_r1dr);
-  ctx->launches += 7;
+  k_intr2dr<<<ceil_div(N, 128), 128, 0, s>>>(N, KL, wc, ctx->d_ref, ctx->d_intr2dr, ctx->d_wts);
+  k_bands<<<ceil_div(N, 128), 128, 0, s>>>(N, KL, ctx->d_r, ctx->d_dr, ctx->d_ref, ctx->d_radlap, ctx->d_r1dr,
+                                           ctx->d_laps, ctx->d_compr1dr);
+  ctx->launches += 4;
   CUDA_TRY(cudaGetLastError());
   int fail = 0;
   CUDA_TRY(cudaMemcpyAsync(&fail, d_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   cudaFree(wc);
   cudaFree(d_fail);
-  if (fail == 2) return lsd_fail(ctx, LSD_EARG, "schnla: sin(theta) too small (legendre)");
-  if (fail) return lsd_fail(ctx, LSD_ESINGULAR, "table construction failed (code " + std::to_string(fail) + ")");
+  if (fail) return lsd_fail(ctx, LSD_ESINGULAR, "radial mesh construction failed (code " + std::to_string(fail) + ")");
   return LSD_OK;
 }
 
@@ -415,12 +521,14 @@ int lsd_build_operators(lsd_ctx* ctx) {
   setf(OP_MPOL, 1.0, 1.0);
   P.Hyp = c.Hyp;
   P.vel_bc = c.vel_bc; P.cod_bc = c.cod_bc; P.comp_bc = c.comp_bc;
+  P.anelastic = c.boussinesq ? 0 : 1;
   int* d_fail = nullptr;
   CUDA_TRY(cudaMalloc(&d_fail, sizeof(int)));
   CUDA_TRY(cudaMemsetAsync(d_fail, 0, sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(ctx->d_y, 0, sizeof(double) * OP_NFAM * N * (2 * KL + 1) * L, s));
   dim3 g(ceil_div(L, 32), OP_NFAM);
-  k_build_ops<<<g, 32, 0, s>>>(N, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap, P, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_info);
+  k_build_ops<<<g, 32, 0, s>>>(N, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_laps, ctx->d_ref, P, ctx->d_lu,
+                               ctx->d_ipiv, ctx->d_y, ctx->d_info);
   dim3 gt(ceil_div(L, 64), N, OP_NFAM);
   k_lu_transpose<<<gt, 64, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_lus, ctx->d_ipivs, ctx->d_yt);
   CUDA_TRY(cudaMemsetAsync(ctx->d_gret, 0, sizeof(double) * 2 * N * L, s));

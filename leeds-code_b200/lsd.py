@@ -61,6 +61,9 @@ def load_library(path=None):
         "lsd_tra_qst2rtp": [_V] + [_D] * 9,
         "lsd_tra_rtp2qst": [_V] + [_D] * 9,
         "lsd_tra_grad": [_V, _D, _D, _D, _D],
+        "lsd_tra_dth": [_V, _D, _D, _D],
+        "lsd_tra_qst2rtp_vel": [_V] + [_D] * 20,
+        "lsd_set_reference_state": [_V, _D],
         "lsd_sht_synth_device": [_V, ctypes.c_int, _V, _V],
         "lsd_sht_analys_device": [_V, ctypes.c_int, _V, _V],
         "lsd_matrices": [_V],
@@ -230,6 +233,26 @@ class Context:
         t, p = np.zeros((self.N, self.Ph, self.Th)), np.zeros((self.N, self.Ph, self.Th))
         self._ok(self.lib.lsd_tra_grad(self.h, _dp(_c(sre)), _dp(_c(sim)), _dp(t), _dp(p)))
         return t, p
+
+    def tra_dth(self, sre, sim):
+        p = np.zeros((self.N, self.Ph, self.Th))
+        self._ok(self.lib.lsd_tra_dth(self.h, _dp(_c(sre)), _dp(_c(sim)), _dp(p)))
+        return p
+
+    def tra_qst2rtp_vel(self, q, s, t, qr, sr, tr):
+        """tra_qst2rtp_vel: -> r, th, ph, dur, qv1, dutr, dupr, qv2."""
+        outs = [np.zeros((self.N, self.Ph, self.Th)) for _ in range(8)]
+        ins = [_c(x) for pair in (q, s, t, qr, sr, tr) for x in pair]
+        self._ok(self.lib.lsd_tra_qst2rtp_vel(self.h, *[_dp(a) for a in ins], *[_dp(o) for o in outs]))
+        return outs
+
+    # ---- anelastic reference state (io.F90:559-608)
+    def set_reference_state(self, prof):
+        """prof: (7, N) rho, xi, dxi/dr, T, dT/dr, eta, deta/dr (planet_model.txt.in)."""
+        prof = np.ascontiguousarray(prof, dtype=np.float64)
+        if prof.shape != (7, self.N):
+            raise ValueError("reference state must be (7, N)")
+        self._ok(self.lib.lsd_set_reference_state(self.h, _dp(prof)))
 
     # ---- time stepping (main.F90:100-164)
     def matrices(self):

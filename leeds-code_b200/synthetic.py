@@ -59,6 +59,28 @@ def boussinesq_state(cfg, seed=SEED, amplitude=1e-3, fields=(capi.VEL_TOR, capi.
     return out
 
 
+def polytrope_reference_state(N, rratio=0.35, alpha=-1.0, n=2.0, c0=-0.459754, c1=1.515898, file_precision=True):
+    """The seven columns of planet_model.txt.in (io.F90:559-608) for a polytrope of index n
+    (Jones et al. 2011, Icarus 216, 120-135): zeta = c0 + c1/r, rho = zeta^n,
+    xi = rho'/rho = -n c1 / (r^2 zeta), dxi/dr = 2 n c1/(r^3 zeta) - n c1^2/(r^4 zeta^2),
+    T = zeta/c1, dT/dr = -1/r^2, eta = 1, deta/dr = 0, on the Chebyshev grid.  The default
+    constants give rho_i/rho_o = e^3 at rratio 0.35 (N_rho = 3).  With file_precision the
+    values are rounded as the text file stores them (%12.8f for the first five columns,
+    %12.8e for the diffusivity).  Returns (7, N)."""
+    r = chebyshev_grid(N, rratio, alpha)
+    zeta = c0 + c1 / r
+    cols = [zeta ** n, -n * c1 / (r ** 2 * zeta),
+            2 * n * c1 / (r ** 3 * zeta) - n * c1 * c1 / (r ** 4 * zeta * zeta),
+            zeta / c1, -1.0 / (r * r), np.ones(N), np.zeros(N)]
+    prof = np.array(cols, dtype=np.float64)
+    if file_precision:
+        for k in range(5):
+            prof[k] = [float("%12.8f" % v) for v in prof[k]]
+        for k in (5, 6):
+            prof[k] = [float("%12.8e" % v) for v in prof[k]]
+    return prof
+
+
 def random_spectral(L, M, Mp, nshell, nfield, seed=SEED, power=1.0):
     """Random complex coefficients ~ N(0,1) * l^-power (l = 0 -> 1), m = 0 imaginary zero.
     Returns interleaved complex array [field][shell][H] (harmonic fastest)."""
@@ -78,6 +100,18 @@ def config_parity(**kw):
     N = 33, E = 3e-4, Ra = 200, Pr = 1, Pm = 3, dt = 1e-5, no-slip, fixed T, insulating."""
     base = dict(L=32, M=32, Mp=1, N=33, Nic=1, KL=3, rratio=0.35, E=3e-4, Ra=200.0, Pr=1.0,
                 Pm=3.0, vel_bc=1, cod_bc=1, timestep=1e-5, implicit=0.6, time_step_control=2)
+    base.update(kw)
+    return capi.template_config(**base)
+
+
+def config_anelastic(L=64, **kw):
+    """Anelastic dynamo shell (n = 2 polytrope, N_rho = 3, the reference's anelastic
+    benchmark parameters Ra = 8e4, Pr = 1, Pm = 50, E = 2e-3, rratio 0.35, stress-free
+    walls, fixed entropy) at L = M, N = L + 1, with composition (Sc = 3, Ra_comp = 4e4,
+    fixed composition), fixed dt = 1e-6, implicit 0.5."""
+    base = dict(L=L, M=L, Mp=1, N=L + 1, Nic=1, KL=3, rratio=0.35, E=2e-3, Ra=8.0e4, Pr=1.0,
+                Pm=50.0, vel_bc=4, cod_bc=1, comp_bc=1, comp_tstep=1, Sc=3.0, Ra_comp=4.0e4,
+                boussinesq=0, timestep=1e-6, implicit=0.5, time_step_control=2)
     base.update(kw)
     return capi.template_config(**base)
 

@@ -21,8 +21,10 @@
 //     partial pivoting and its solve), dgetrf/dgetf2 + dgetri/dtrtri (small inverses),
 //     restated from the reference LAPACK algorithms.  tests/ pin these against scipy's
 //     LAPACK (scipy.linalg.lapack.dgbtrf/dgbtrs).
-// Scope: Boussinesq MHD + codensity (+ composition) with an insulating inner core
-// (i_Nic = 1), fixed dt (d_timestep > 0), no SHTns, no inhomogeneous BC files.
+// Scope: Boussinesq or anelastic MHD + codensity (+ composition) with an insulating
+// inner core (i_Nic = 1), fixed dt (d_timestep > 0), no SHTns, no inhomogeneous BC
+// files.  The anelastic reference state (io.F90:559-608, the seven columns of
+// planet_model.txt.in) is handed over by orc_set_reference_state.
 //
 // Build: g++ -O3 -march=native -fopenmp -ffp-contract=off -shared -fPIC
 //        (oracle/build_oracle.sh).  -ffp-contract=off keeps a*b+c as two roundings, as
@@ -270,6 +272,7 @@ struct RDom {
   std::vector<double> rp[7];  // r(n, p), p = -3..3
   std::vector<double> rho0, rho1, rho2, temp0, temp1, eta0, eta1;
   std::vector<double> intr2dr, f_factor;
+  std::vector<double> intr2dr_comp, intr2dr_compS, intr2dr_magdiss, intr2dr_veldiss;
   std::vector<Band> dr;  // dr[1..KL]
   Band radLap, radLap_flayer, CompLap, GreLap, r1dr, compr1dr, MagTorLap, MagPolLap;
   double R(int n, int p) const { return rp[p + 3][n - 1]; }
@@ -299,6 +302,7 @@ struct Oracle {
   // physical fields
   Phys vel_r, vel_t, vel_p, vel_cr, vel_ct, vel_cp, mag_r, mag_t, mag_p, mag_cr, mag_ct, mag_cp;
   Phys cod_gr, cod_gt, cod_gp, comp_gr, comp_gt, comp_gp;
+  Phys vel_dur, vel_qv1, vel_dutr, vel_dupr, vel_qv2;  // anelastic (tra_qst2rtp_vel)
   // time
   double tim_t = 0, tim_dt = 0, tim_dterr = 0, tim_corr_dt = 0, lasterr = 1e99;
   int tim_it = 0, tim_step = 0, tim_pcn = -1;
@@ -518,6 +522,7 @@ int rdom_init(RDom& D, int KL) {
     b->init(KL, N);
   D.intr2dr.assign(N, 0.0);
   D.f_factor.assign(N, 0.0);
+  for (auto* v : {&D.intr2dr_comp, &D.intr2dr_compS, &D.intr2dr_magdiss, &D.intr2dr_veldiss}) v->assign(N, 0.0);
   if (N == 1) return 0;
   const int lda = 2 * KL + 1;
   std::vector<double> A((size_t)lda * lda);
@@ -538,6 +543,12 @@ int rdom_init(RDom& D, int KL) {
       for (int j = l; j <= r; ++j) {
         double w = 0.5 * (c - e) * Aa(i, j - l + 1) * D.R(n, 2);
         D.intr2dr[j - 1] = D.intr2dr[j - 1] + w;
+        // the density / temperature / diffusivity weighted weights (meshs.F90:318-333)
+        D.intr2dr_comp[j - 1] = D.intr2dr_comp[j - 1] + w * D.rho0[n - 1];
+        D.intr2dr_compS[j - 1] = D.intr2dr_compS[j - 1] + w * (D.rho0[n - 1] * D.temp0[n - 1]);
+        D.intr2dr_magdiss[j - 1] = D.intr2dr_magdiss[j - 1] + w * D.eta0[n - 1];
+        D.intr2dr_veldiss[j - 1] = D.intr2dr_veldiss[j - 1] +
+                                   w * 2.0 * D.rho0[n - 1] * (D.rho2[n - 1] - D.rho1[n - 1] * D.rho1[n - 1] / 3.0);
       }
     }
   }
@@ -596,6 +607,9 @@ int setup_mesh(Oracle& o) {
   for (int n = 0; n < o.N; ++n) D.rp[4][n] = D.rp[4][n] + ri;
   for (auto* v : {&D.rho0, &D.rho1, &D.rho2, &D.temp0, &D.temp1}) v->assign(o.N, 0.0);
   D.eta0.assign(o.N, 1.0); D.eta1.assign(o.N, 0.0);
+  if (!o.cfg.boussinesq) {  // until orc_set_reference_state: rho = T = 1, gradients 0
+    D.rho0.assign(o.N, 1.0); D.temp0.assign(o.N, 1.0);
+  }
   RDom& I = o.ic;
   I.N = o.Nic;
   I.rp[4].resize(o.Nic);
@@ -660,6 +674,83 @@ void tim_iclumesh_X(const Oracle& o, const RDom& D, double c1, double c2, int l,
   for (int n = 1; n <= D.N; ++n)
     A.at(2 * o.KL + 1, n) = A.at(2 * o.KL + 1, n) + c1_ + c2_ * ll1 * D.R(n, -2);
   lumesh_zero_bc_rows(A);
+}
+// tim_lumesh_vel_X (timestep.F90:47-86) -- the anelastic velocity operator
+void tim_lumesh_vel_X(const Oracle& o, const RDom& D, double c1, double c2, int l, LUBand& A) {
+  double c1_ = c1 / o.tim_dt, c2_ = c2 * o.cfg.implicit;
+  if (o.cfg.implicit == 0.0) c2_ = 1.0;
+  double ll1 = (double)(l * (l + 1));
+  A.init(o.KL, D.N);
+  lumesh_from_band(A, D.CompLap, -c2_);
+  for (int n = 1; n <= D.N; ++n) {
+    double t = ll1 * D.R(n, -2), x1 = D.rho1[n - 1];
+    double d = t + o.cfg.Hyp * (t * t);
+    d = d - 2.0 * x1 * D.R(n, -1);
+    d = d - x1 * x1;
+    d = d - D.rho2[n - 1];
+    A.at(2 * o.KL + 1, n) = A.at(2 * o.KL + 1, n) + c1_ + c2_ * d;
+  }
+  lumesh_zero_bc_rows(A);
+}
+// tim_lumesh_Gre_X (timestep.F90:92-128) -- the anelastic Green's function operator
+void tim_lumesh_Gre_X(const Oracle& o, const RDom& D, double c1, double c2, int l, LUBand& A) {
+  double c1_ = c1 / o.tim_dt, c2_ = c2 * o.cfg.implicit;
+  if (o.cfg.implicit == 0.0) c2_ = 1.0;
+  double ll1 = (double)(l * (l + 1));
+  A.init(o.KL, D.N);
+  lumesh_from_band(A, D.GreLap, -c2_);
+  for (int n = 1; n <= D.N; ++n) {
+    double d = ll1 * D.R(n, -2) - D.rho1[n - 1] * D.R(n, -1);
+    d = d - D.rho2[n - 1];
+    A.at(2 * o.KL + 1, n) = A.at(2 * o.KL + 1, n) + c1_ + c2_ * d;
+  }
+  lumesh_zero_bc_rows(A);
+}
+// tim_iclumesh_Tor_X / _Pol_X with Ni = 1, anelastic diagonal (timestep.F90:243-262, 311-322)
+void tim_iclumesh_X_anel(const Oracle& o, const RDom& D, double c1, double c2, int l, bool tor, LUBand& A) {
+  double c1_ = c1 / o.tim_dt, c2_ = c2 * o.cfg.implicit;
+  if (o.cfg.implicit == 0.0) c2_ = 1.0;
+  double ll1 = (double)(l * (l + 1));
+  A.init(o.KL, D.N);
+  const Band& lap = tor ? D.MagTorLap : D.MagPolLap;
+  for (int j = 1; j <= A.N; ++j)
+    for (int row = 1; row <= 2 * o.KL + 1; ++row) A.at(o.KL + row, j) = A.at(o.KL + row, j) - c2_ * lap.at(row, j);
+  for (int n = 1; n <= D.N; ++n) {
+    double t = ll1 * D.R(n, -2);
+    double d = ll1 * D.eta0[n - 1] * D.R(n, -2);
+    if (tor) d = d - D.eta1[n - 1] * D.R(n, -1);
+    d = d + o.cfg.Hyp * (t * t);
+    A.at(2 * o.KL + 1, n) = A.at(2 * o.KL + 1, n) + c1_ + c2_ * d;
+  }
+  lumesh_zero_bc_rows(A);
+}
+// tim_mesh_vel_Y (timestep.F90:350-380)
+void tim_mesh_vel_Y(const Oracle& o, const RDom& D, double c1, double c2, int l, Band& A) {
+  double c1_ = c1 / o.tim_dt, c2_ = c2 * (1.0 - o.cfg.implicit);
+  A.init(o.KL, D.N);
+  for (size_t i = 0; i < A.M.size(); ++i) A.M[i] = c2_ * D.CompLap.M[i];
+  for (int n = 1; n <= D.N; ++n) {
+    double t = (double)(l * (l + 1)) * D.R(n, -2), x1 = D.rho1[n - 1];
+    double d = t + o.cfg.Hyp * (t * t);
+    d = d - 2.0 * x1 * D.R(n, -1);
+    d = d - x1 * x1;
+    d = d - D.rho2[n - 1];
+    A.at(o.KL + 1, n) = A.at(o.KL + 1, n) + c1_ - c2_ * d;
+  }
+}
+// tim_mesh_mag_Tor_Y / _Pol_Y (timestep.F90:466-546)
+void tim_mesh_mag_Y(const Oracle& o, const RDom& D, double c1, double c2, int l, bool tor, Band& A) {
+  double c1_ = c1 / o.tim_dt, c2_ = c2 * (1.0 - o.cfg.implicit);
+  A.init(o.KL, D.N);
+  const Band& lap = tor ? D.MagTorLap : D.MagPolLap;
+  for (size_t i = 0; i < A.M.size(); ++i) A.M[i] = c2_ * lap.M[i];
+  for (int n = 1; n <= D.N; ++n) {
+    double t = (double)(l * (l + 1)) * D.R(n, -2);
+    double d = (double)(l * (l + 1)) * D.eta0[n - 1] * D.R(n, -2);
+    if (tor) d = d - D.eta1[n - 1] * D.R(n, -1);
+    d = d + o.cfg.Hyp * (t * t);
+    A.at(o.KL + 1, n) = A.at(o.KL + 1, n) + c1_ - c2_ * d;
+  }
 }
 // tim_mesh_flayer_Y (timestep.F90:442-458)
 void tim_mesh_flayer_Y(const Oracle& o, const RDom& D, double c1, double c2, int l, Band& A) {
@@ -756,10 +847,13 @@ int build_matrices(Oracle& o) {
   o.XC.assign(L, LUBand()); o.YC.assign(L, Band()); o.XComp.assign(L, LUBand()); o.YComp.assign(L, Band());
   o.mXTor.assign(L, LUBand()); o.mXPol.assign(L, LUBand()); o.mYTor.assign(L, Band()); o.mYPol.assign(L, Band());
   int bad = 0;
-  // vel_matrices (velocity.F90:56-168); Boussinesq uses the flayer operators
+  // vel_matrices (velocity.F90:56-168); Boussinesq uses the flayer operators, the
+  // anelastic equations tim_lumesh_vel_X / tim_mesh_vel_Y / tim_lumesh_Gre_X
+  const bool bq = o.cfg.boussinesq != 0;
   double c1 = 1.0, c2 = o.cfg.Pm;
   for (int l = 1; l < L; ++l) {
-    tim_lumesh_flayer_X(o, D, c1, c2, l, o.XTor[l]);
+    if (bq) tim_lumesh_flayer_X(o, D, c1, c2, l, o.XTor[l]);
+    else tim_lumesh_vel_X(o, D, c1, c2, l, o.XTor[l]);
     // vel_bc_Tor (velocity.F90:177-201)
     LUBand& A = o.XTor[l];
     if (o.cfg.vel_bc == 1 || o.cfg.vel_bc == 2) {
@@ -775,27 +869,37 @@ int build_matrices(Oracle& o) {
       A.at(2 * KL + 1, N) = A.at(2 * KL + 1, N) - D.R(N, -1);
     }
     bad |= lu_find(A);
-    tim_mesh_flayer_Y(o, D, c1, c2, l, o.YTor[l]);
+    if (bq) tim_mesh_flayer_Y(o, D, c1, c2, l, o.YTor[l]);
+    else tim_mesh_vel_Y(o, D, c1, c2, l, o.YTor[l]);
   }
   for (int l = 1; l < L; ++l) {
-    tim_lumesh_flayer_X(o, D, c1, c2, l, o.XPol[l]);
-    LUBand& A = o.XPol[l];  // vel_bc_Pol (velocity.F90:207-254), Boussinesq
+    if (bq) tim_lumesh_flayer_X(o, D, c1, c2, l, o.XPol[l]);
+    else tim_lumesh_vel_X(o, D, c1, c2, l, o.XPol[l]);
+    LUBand& A = o.XPol[l];  // vel_bc_Pol (velocity.F90:207-254)
     if (o.cfg.vel_bc == 1 || o.cfg.vel_bc == 2) {
       for (int j = 1; j <= 1 + KL; ++j) A.at(2 * KL + 1 + 1 - j, j) = D.dr[1].at(KL + 1 + 1 - j, j);
-    } else {
+    } else if (bq) {
       for (int j = 1; j <= 1 + KL; ++j) A.at(2 * KL + 1 + 1 - j, j) = D.dr[2].at(KL + 1 + 1 - j, j);
+    } else {  // compressible part of the stress-free condition
+      for (int j = 1; j <= 1 + KL; ++j)
+        A.at(2 * KL + 1 + 1 - j, j) = D.dr[2].at(KL + 1 + 1 - j, j) + D.rho1[0] * D.dr[1].at(KL + 1 + 1 - j, j);
     }
     if (o.cfg.vel_bc == 1 || o.cfg.vel_bc == 3) {
       for (int j = N - KL; j <= N; ++j) A.at(2 * KL + 1 + N - j, j) = D.dr[1].at(KL + 1 + N - j, j);
+    } else if (!bq) {
+      for (int j = N - KL; j <= N; ++j)
+        A.at(2 * KL + 1 + N - j, j) = D.dr[2].at(KL + 1 + N - j, j) + D.rho1[N - 1] * D.dr[1].at(KL + 1 + N - j, j);
     } else {
       for (int j = N - KL; j <= N; ++j) A.at(2 * KL + 1 + N - j, j) = D.dr[2].at(KL + 1 + N - j, j);
     }
     bad |= lu_find(A);
-    tim_mesh_flayer_Y(o, D, c1, c2, l, o.YPol[l]);
+    if (bq) tim_mesh_flayer_Y(o, D, c1, c2, l, o.YPol[l]);
+    else tim_mesh_vel_Y(o, D, c1, c2, l, o.YPol[l]);
   }
   c1 = 0.0; c2 = 1.0 / o.cfg.implicit;
   for (int l = 1; l < L; ++l) {
-    tim_lumesh_flayer_X(o, D, c1, c2, l, o.XGre[l]);
+    if (bq) tim_lumesh_flayer_X(o, D, c1, c2, l, o.XGre[l]);
+    else tim_lumesh_Gre_X(o, D, c1, c2, l, o.XGre[l]);
     o.XGre[l].at(2 * KL + 1, 1) = 1.0;  // vel_bc_Gre (velocity.F90:260-267)
     o.XGre[l].at(2 * KL + 1, N) = 1.0;
     bad |= lu_find(o.XGre[l]);
@@ -836,21 +940,25 @@ int build_matrices(Oracle& o) {
   }
   // mag_matrices (magnetic.F90:62-133), insulating inner core (Ni = 1)
   for (int l = 1; l < L; ++l) {
-    tim_iclumesh_X(o, D, 1.0, 1.0, l, true, o.mXTor[l]);
+    if (bq) tim_iclumesh_X(o, D, 1.0, 1.0, l, true, o.mXTor[l]);
+    else tim_iclumesh_X_anel(o, D, 1.0, 1.0, l, true, o.mXTor[l]);
     o.mXTor[l].at(2 * KL + 1, 1) = 1.0;  // mag_bc_Tor (magnetic.F90:137-192)
     o.mXTor[l].at(2 * KL + 1, N) = 1.0;
     bad |= lu_find(o.mXTor[l]);
-    tim_mesh_Y(o, D, 1.0, 1.0, l, o.mYTor[l]);
+    if (bq) tim_mesh_Y(o, D, 1.0, 1.0, l, o.mYTor[l]);
+    else tim_mesh_mag_Y(o, D, 1.0, 1.0, l, true, o.mYTor[l]);
   }
   for (int l = 1; l < L; ++l) {
-    tim_iclumesh_X(o, D, 1.0, 1.0, l, false, o.mXPol[l]);
+    if (bq) tim_iclumesh_X(o, D, 1.0, 1.0, l, false, o.mXPol[l]);
+    else tim_iclumesh_X_anel(o, D, 1.0, 1.0, l, false, o.mXPol[l]);
     LUBand& A = o.mXPol[l];  // mag_bc_Pol (magnetic.F90:198-282), Ni = 1, homogeneous
     for (int j = 1; j <= 1 + KL; ++j) A.at(2 * KL + 1 + 1 - j, j) = D.dr[1].at(KL + 1 + 1 - j, j);
     A.at(2 * KL + 1, 1) = A.at(2 * KL + 1, 1) - D.R(1, -1) * l;
     for (int j = N - KL; j <= N; ++j) A.at(2 * KL + 1 + N - j, j) = D.dr[1].at(KL + 1 + N - j, j);
     A.at(2 * KL + 1, N) = A.at(2 * KL + 1, N) + D.R(N, -1) * (l + 1);
     bad |= lu_find(A);
-    tim_mesh_Y(o, D, 1.0, 1.0, l, o.mYPol[l]);
+    if (bq) tim_mesh_Y(o, D, 1.0, 1.0, l, o.mYPol[l]);
+    else tim_mesh_mag_Y(o, D, 1.0, 1.0, l, false, o.mYPol[l]);
   }
   return bad ? 1 : 0;
 }
@@ -1033,6 +1141,97 @@ void tra_qst2rtp(const Oracle& o, const Spec& q, const Spec& s, const Spec& t, P
   }
 }
 
+// ---- tra_qst2rtp_vel (transform.fftw3.F90:611-714), anelastic -----------------------------
+// outs: r, th, ph, dur, qv1, dutr, dupr, qv2
+void tra_qst2rtp_vel(const Oracle& o, const Spec& q, const Spec& s, const Spec& t, const Spec& qr, const Spec& sr,
+                     const Spec& tr, Phys* outs[8]) {
+  std::vector<int> mc = mcount(o);
+  size_t psz = (size_t)o.Th * o.Ph * o.N;
+  for (int k = 0; k < 8; ++k) outs[k]->assign(psz, 0.0);
+#pragma omp parallel
+  {
+    Work w; w.init(o);
+    std::vector<cplx> Y3b((size_t)o.Th * 2 * o.Hc);
+    auto emit = [&](int k, const std::vector<cplx>& Y, int n) {
+      combine_ns(o, Y, Y3b);
+      s2p_shell(o, Y3b.data(), &(*outs[k])[(size_t)o.Th * o.Ph * n], w.a.data(), w.b.data(), w.scr.data());
+    };
+#pragma omp for schedule(static)
+    for (int n = 0; n < o.N; ++n) {
+      // Ar = q, dur = qr
+      for (int k = 0; k < 2; ++k) std::fill(w.Y[k].begin(), w.Y[k].end(), cplx(0, 0));
+      for (int nh = 0; nh < o.H; ++nh) {
+        size_t i = nh + (size_t)o.H * n;
+        int m = mc[nh], sp = o.hs[nh];
+        cplx c1(q.re[i], q.im[i]), c2(qr.re[i], qr.im[i]);
+        const double* P = &o.P[(size_t)o.Th2 * nh];
+        cplx* Y1 = &w.Y[0][yidx(o, 0, m, sp)];
+        cplx* Y2 = &w.Y[1][yidx(o, 0, m, sp)];
+        for (int j = 0; j < o.Th2; ++j) { Y1[j] = Y1[j] + c1 * P[j]; Y2[j] = Y2[j] + c2 * P[j]; }
+      }
+      emit(0, w.Y[0], n);
+      emit(3, w.Y[1], n);
+      // At = s dth - t/sin dph, and the same of (sr, tr)
+      for (int k = 0; k < 2; ++k) std::fill(w.Y[k].begin(), w.Y[k].end(), cplx(0, 0));
+      for (int nh = 0; nh < o.H; ++nh) {
+        size_t i = nh + (size_t)o.H * n;
+        int m = mc[nh], sp = o.hs[nh];
+        cplx c1(s.re[i], s.im[i]), c2(t.im[i], -t.re[i]), c3(sr.re[i], sr.im[i]), c4(tr.im[i], -tr.re[i]);
+        const double* A1 = &o.llP_[(size_t)o.Th2 * nh];
+        const double* A2 = &o.llsin1mP[(size_t)o.Th2 * nh];
+        cplx* Y1o = &w.Y[0][yidx(o, 0, m, 1 - sp)];
+        cplx* Y1s = &w.Y[0][yidx(o, 0, m, sp)];
+        cplx* Y2o = &w.Y[1][yidx(o, 0, m, 1 - sp)];
+        cplx* Y2s = &w.Y[1][yidx(o, 0, m, sp)];
+        for (int j = 0; j < o.Th2; ++j) {
+          Y1o[j] = Y1o[j] + c1 * A1[j];
+          Y1s[j] = Y1s[j] + c2 * A2[j];
+          Y2o[j] = Y2o[j] + c3 * A1[j];
+          Y2s[j] = Y2s[j] + c4 * A2[j];
+        }
+      }
+      emit(1, w.Y[0], n);
+      emit(5, w.Y[1], n);
+      // Aph = s/sin dph + t dth, the same of (sr, tr), and the qva / qvb sums
+      for (int k = 0; k < 4; ++k) std::fill(w.Y[k].begin(), w.Y[k].end(), cplx(0, 0));
+      double rinv = o.oc.R(n + 1, -1);
+      for (int nh = 0; nh < o.H; ++nh) {
+        size_t i = nh + (size_t)o.H * n;
+        int m = mc[nh], sp = o.hs[nh];
+        cplx c1(-s.im[i], s.re[i]), c2(t.re[i], t.im[i]), c3(-sr.im[i], sr.re[i]), c4(tr.re[i], tr.im[i]);
+        cplx c5(-s.re[i] * rinv, -s.im[i] * rinv), c6(t.im[i] * rinv, -t.re[i] * rinv);
+        cplx c7(t.re[i] * rinv, t.im[i] * rinv), c8(s.im[i] * rinv, -s.re[i] * rinv);
+        const double* A1 = &o.llP_[(size_t)o.Th2 * nh];
+        const double* A2 = &o.llsin1mP[(size_t)o.Th2 * nh];
+        const double* QA = &o.qva[(size_t)o.Th2 * nh];
+        const double* QB = &o.qvb[(size_t)o.Th2 * nh];
+        cplx* Y1s = &w.Y[0][yidx(o, 0, m, sp)];
+        cplx* Y1o = &w.Y[0][yidx(o, 0, m, 1 - sp)];
+        cplx* Y2s = &w.Y[1][yidx(o, 0, m, sp)];
+        cplx* Y2o = &w.Y[1][yidx(o, 0, m, 1 - sp)];
+        cplx* Y3s = &w.Y[2][yidx(o, 0, m, sp)];
+        cplx* Y3o = &w.Y[2][yidx(o, 0, m, 1 - sp)];
+        cplx* Y4s = &w.Y[3][yidx(o, 0, m, sp)];
+        cplx* Y4o = &w.Y[3][yidx(o, 0, m, 1 - sp)];
+        for (int j = 0; j < o.Th2; ++j) {
+          Y1s[j] = Y1s[j] + c1 * A2[j];
+          Y1o[j] = Y1o[j] + c2 * A1[j];
+          Y2s[j] = Y2s[j] + c3 * A2[j];
+          Y2o[j] = Y2o[j] + c4 * A1[j];
+          Y3s[j] = Y3s[j] + c5 * QA[j];
+          Y3o[j] = Y3o[j] + c6 * QB[j];
+          Y4s[j] = Y4s[j] + c7 * QA[j];
+          Y4o[j] = Y4o[j] + c8 * QB[j];
+        }
+      }
+      emit(2, w.Y[0], n);
+      emit(6, w.Y[1], n);
+      emit(4, w.Y[2], n);
+      emit(7, w.Y[3], n);
+    }
+  }
+}
+
 // ---- tra_rtp2qst (transform.fftw3.F90:825-949) -----------------------------------------
 void tra_rtp2qst(const Oracle& o, const Phys& r, const Phys& th, const Phys& ph, Spec& q, Spec& s, Spec& t) {
   std::vector<int> mc = mcount(o);
@@ -1120,6 +1319,29 @@ void tra_grad(const Oracle& o, const Spec& s, Phys& tp, Phys& pp) {
   }
 }
 
+// ---- tra_dth (transform.fftw3.F90:1006-1031) -------------------------------------------
+void tra_dth(const Oracle& o, const Spec& s, Phys& pp) {
+  std::vector<int> mc = mcount(o);
+  pp.assign((size_t)o.Th * o.Ph * o.N, 0.0);
+#pragma omp parallel
+  {
+    Work w; w.init(o);
+#pragma omp for schedule(static)
+    for (int n = 0; n < o.N; ++n) {
+      std::fill(w.Y[0].begin(), w.Y[0].end(), cplx(0, 0));
+      for (int nh = 0; nh < o.H; ++nh) {
+        size_t i = nh + (size_t)o.H * n;
+        cplx c(s.re[i], s.im[i]);
+        const double* A = &o.P_[(size_t)o.Th2 * nh];
+        cplx* Y = &w.Y[0][yidx(o, 0, mc[nh], 1 - o.hs[nh])];
+        for (int j = 0; j < o.Th2; ++j) Y[j] = Y[j] + c * A[j];
+      }
+      combine_ns(o, w.Y[0], w.Y3[0]);
+      s2p_shell(o, w.Y3[0].data(), &pp[(size_t)o.Th * o.Ph * n], w.a.data(), w.b.data(), w.scr.data());
+    }
+  }
+}
+
 // ========================================================================================
 // coll algebra (variables.F90:246-829)
 // ========================================================================================
@@ -1183,6 +1405,15 @@ void torpol2qst(const Oracle& o, const Coll& Tor, const Coll& Pol, Coll& q, Coll
       t.im[i] = -Tor.im[i] * o.ad_rtll1[l];
     }
   }
+}
+// var_coll_TorPol2qstderiv (variables.F90:610-660): q, s (compressible), t and their
+// radial derivatives dr(1) q, dr(1) s, dr(1) t
+void torpol2qstderiv(const Oracle& o, const Coll& Tor, const Coll& Pol, Coll& q, Coll& s, Coll& t, Coll& qr,
+                     Coll& sr, Coll& tr) {
+  torpol2qst(o, Tor, Pol, q, s, t, true);
+  meshmult(o, o.oc.dr[1], q, qr);
+  meshmult(o, o.oc.dr[1], s, sr);
+  meshmult(o, o.oc.dr[1], t, tr);
 }
 // var_coll_qstcurl (variables.F90:713-754)
 void qstcurl(const Oracle& o, const Coll& q, const Coll& s, const Coll& t, Coll& oq, Coll& os, Coll& ot) {
@@ -1248,6 +1479,59 @@ void vec_transform(Oracle& o, const Coll& Tor, const Coll& Pol, Phys& r, Phys& t
   coll2spec(o, q, sq); coll2spec(o, s, ss); coll2spec(o, tt, st);
   tra_qst2rtp(o, sq, ss, st, cr, ct, cp);
 }
+// vel_transform, anelastic branch (velocity.F90:333-347)
+void vel_transform_anel(Oracle& o) {
+  Coll q, s, tt, qr, sr, tr;
+  torpol2qstderiv(o, o.vTor, o.vPol, q, s, tt, qr, sr, tr);
+  Spec sq, ss, st, sqr, ssr, str;
+  coll2spec(o, q, sq); coll2spec(o, s, ss); coll2spec(o, tt, st);
+  coll2spec(o, qr, sqr); coll2spec(o, sr, ssr); coll2spec(o, tr, str);
+  Phys* outs[8] = {&o.vel_r, &o.vel_t, &o.vel_p, &o.vel_dur, &o.vel_qv1, &o.vel_dutr, &o.vel_dupr, &o.vel_qv2};
+  tra_qst2rtp_vel(o, sq, ss, st, sqr, ssr, str, outs);
+  qstcurl(o, q, s, tt, q, s, tt);
+  coll2spec(o, q, sq); coll2spec(o, s, ss); coll2spec(o, tt, st);
+  tra_qst2rtp(o, sq, ss, st, o.vel_cr, o.vel_ct, o.vel_cp);
+}
+// vel_angmomclr (velocity.F90:475-574): with stress-free walls (i_vel_bc = 4) remove the
+// rigid rotation carried by the l = 1, m <= 1 toroidal modes
+void vel_angmomclr(Oracle& o) {
+  if (o.cfg.vel_bc != 4) return;
+  const int N = o.N;
+  const bool bq = o.cfg.boussinesq != 0;
+  const std::vector<double>& wt = bq ? o.oc.intr2dr : o.oc.intr2dr_comp;
+  const double w = 8.0 / 3.0 * d_PI;
+  auto dot = [&](const std::vector<double>& f) { double a = 0; for (int n = 0; n < N; ++n) a = a + f[n] * wt[n]; return a; };
+  std::vector<double> f1(N), f2(N);
+  for (int n = 0; n < N; ++n) f2[n] = bq ? o.oc.R(n + 1, 2) : o.oc.R(n + 1, 1) * o.oc.R(n + 1, 1);
+  double omz = 0, omx = 0, omy = 0;
+  int nz = -1, nx = -1;
+  for (int nh = 0; nh < o.H; ++nh) {
+    if (o.hl[nh] != 1 || o.hm[nh] > 1) continue;
+    double* re = &o.vTor.re[(size_t)N * nh];
+    double* im = &o.vTor.im[(size_t)N * nh];
+    if (o.hm[nh] == 0) {
+      for (int n = 0; n < N; ++n) f1[n] = re[n] * o.oc.R(n + 1, 1);
+      double Lz = w * dot(f1), Lz2 = w * dot(f2);
+      omz = Lz / Lz2;
+      nz = nh;
+    } else {
+      for (int n = 0; n < N; ++n) f1[n] = re[n] * o.oc.R(n + 1, 1);
+      double Lx = 2.0 * w * dot(f1), Lx2 = 2.0 * w * dot(f2);
+      for (int n = 0; n < N; ++n) f1[n] = im[n] * o.oc.R(n + 1, 1);
+      double Ly = -2.0 * w * dot(f1), Ly2 = -2.0 * w * dot(f2);
+      omx = Lx / Lx2;
+      omy = Ly / Ly2;
+      nx = nh;
+    }
+  }
+  if (nz >= 0)
+    for (int n = 0; n < N; ++n) o.vTor.re[(size_t)N * nz + n] = o.vTor.re[(size_t)N * nz + n] - omz * o.oc.R(n + 1, 1);
+  if (nx >= 0)
+    for (int n = 0; n < N; ++n) {
+      o.vTor.re[(size_t)N * nx + n] = o.vTor.re[(size_t)N * nx + n] - omx * o.oc.R(n + 1, 1);
+      o.vTor.im[(size_t)N * nx + n] = o.vTor.im[(size_t)N * nx + n] - omy * o.oc.R(n + 1, 1);
+    }
+}
 void scal_transform(Oracle& o, const Coll& C, Phys& gr, Phys& gt, Phys& gp) {
   Coll cC; meshmult(o, o.oc.dr[1], C, cC);
   Spec sC, sC_;
@@ -1259,18 +1543,23 @@ void scal_transform(Oracle& o, const Coll& C, Phys& gr, Phys& gt, Phys& gp) {
 void evaluate(Oracle& o) {
   size_t psz = (size_t)o.Th * o.Ph * o.N;
   int Th = o.Th, Ph = o.Ph;
+  const bool bq = o.cfg.boussinesq != 0;
   // transforms (main.F90:101-107)
-  vec_transform(o, o.vTor, o.vPol, o.vel_r, o.vel_t, o.vel_p, o.vel_cr, o.vel_ct, o.vel_cp);
+  vel_angmomclr(o);
+  if (bq) vec_transform(o, o.vTor, o.vPol, o.vel_r, o.vel_t, o.vel_p, o.vel_cr, o.vel_ct, o.vel_cp);
+  else vel_transform_anel(o);
   scal_transform(o, o.codC, o.cod_gr, o.cod_gt, o.cod_gp);
   if (o.cfg.comp_tstep) scal_transform(o, o.compC, o.comp_gr, o.comp_gt, o.comp_gp);
   vec_transform(o, o.bTor, o.bPol, o.mag_r, o.mag_t, o.mag_p, o.mag_cr, o.mag_ct, o.mag_cp);
   Phys r(psz), th(psz), ph(psz);
-  // ---- non_velocity (nonlinear.F90:28-199), Boussinesq
+  // ---- non_velocity (nonlinear.F90:28-199)
   {
     double d_Cor = 2.0 * o.cfg.Pm / o.cfg.E;
-    double Cmag = 2 * o.cfg.Pm / o.cfg.E;
+    const double Pm = o.cfg.Pm;
 #pragma omp parallel for schedule(static)
-    for (int n = 0; n < o.N; ++n)
+    for (int n = 0; n < o.N; ++n) {
+      const double Cmag = bq ? 2 * o.cfg.Pm / o.cfg.E : o.cfg.Pm / (o.cfg.E * o.oc.rho0[n]);
+      const double xi0 = o.oc.rho1[n], xi1 = o.oc.rho2[n], rm1 = o.oc.R(n + 1, -1);
       for (int m = 0; m < Ph; ++m)
         for (int j = 0; j < Th; ++j) {
           size_t i = j + (size_t)Th * (m + (size_t)Ph * n);
@@ -1279,6 +1568,15 @@ void evaluate(Oracle& o) {
           double a = vt * wp - vp * wt;
           double b = vp * wr - vr * wp;
           double c = vr * wt - vt * wr;
+          if (!bq) {  // compressible part of the viscous force (nonlinear.F90:93-110)
+            double f = -(2.0 * xi0 * rm1) - xi1;
+            f = f - (xi0 * xi0) / 3.0;
+            a = a + Pm * vr * f;
+            double d1 = 2.0 * xi0 * rm1 + xi1;
+            d1 = d1 + xi0 * xi0;
+            b = b - Pm * (xi0 * wp + d1 * vt);
+            c = c + Pm * (xi0 * wt - d1 * vp);
+          }
           a = a + d_Cor * o.sn[j] * vp;
           b = b + d_Cor * o.gp[j] * vp;
           c = c - d_Cor * (o.gp[j] * vt + o.sn[j] * vr);
@@ -1287,20 +1585,23 @@ void evaluate(Oracle& o) {
           c = c + Cmag * (o.mag_cr[i] * o.mag_t[i] - o.mag_ct[i] * o.mag_r[i]);
           r[i] = a; th[i] = b; ph[i] = c;
         }
+    }
     Spec sq, ss, st;
     tra_rtp2qst(o, r, th, ph, sq, ss, st);
     Coll cq, cs, ct;
     spec2coll(o, sq, cq); spec2coll(o, ss, cs); spec2coll(o, st, ct);
     for (int nh = 0; nh < o.H; ++nh)
       for (int n = 1; n <= o.N; ++n) {
-        double d2 = o.cfg.Ra * o.oc.R(n, 1) * (o.cfg.Pm * o.cfg.Pm) / o.cfg.Pr;
+        double d2 = bq ? o.cfg.Ra * o.oc.R(n, 1) * (o.cfg.Pm * o.cfg.Pm) / o.cfg.Pr
+                       : -(o.cfg.Ra * o.oc.temp1[n - 1] * (o.cfg.Pm * o.cfg.Pm) / o.cfg.Pr);
         size_t i = (n - 1) + (size_t)o.N * nh;
         cq.re[i] = cq.re[i] + d2 * o.codC.re[i];
         cq.im[i] = cq.im[i] + d2 * o.codC.im[i];
       }
     for (int nh = 0; nh < o.H; ++nh)
       for (int n = 1; n <= o.N; ++n) {
-        double d2 = o.cfg.Ra_comp * o.oc.R(n, 1) * (o.cfg.Pm * o.cfg.Pm) / o.cfg.Sc;
+        double d2 = bq ? o.cfg.Ra_comp * o.oc.R(n, 1) * (o.cfg.Pm * o.cfg.Pm) / o.cfg.Sc
+                       : -(o.cfg.Ra_comp * o.oc.temp1[n - 1] * (o.cfg.Pm * o.cfg.Pm) / o.cfg.Sc);
         size_t i = (n - 1) + (size_t)o.N * nh;
         cq.re[i] = cq.re[i] + d2 * o.compC.re[i];
         cq.im[i] = cq.im[i] + d2 * o.compC.im[i];
@@ -1309,15 +1610,49 @@ void evaluate(Oracle& o) {
     qstllcurlcurlr(o, cq, cs, o.vNPol);
     for (int n = 0; n < o.N; ++n) { o.vNTor.re[n] = 0; o.vNTor.im[n] = 0; o.vNPol.re[n] = 0; o.vNPol.im[n] = 0; }
   }
-  // ---- non_codensity / non_composition (nonlinear.F90:205-357), Boussinesq
+  // ---- non_codensity / non_composition (nonlinear.F90:205-357); composition keeps the
+  // Boussinesq form in both cases, the anelastic codensity (entropy) adds the reference
+  // temperature gradient term and the viscous + ohmic dissipation (nonlinear.F90:239-266)
   for (int which = 0; which < (o.cfg.comp_tstep ? 2 : 1); ++which) {
     double d_qm1 = which == 0 ? o.cfg.Pr / o.cfg.Pm : o.cfg.Sc / o.cfg.Pm;
     const Phys& gr = which == 0 ? o.cod_gr : o.comp_gr;
     const Phys& gt = which == 0 ? o.cod_gt : o.comp_gt;
     const Phys& gq = which == 0 ? o.cod_gp : o.comp_gp;
+    if (bq || which == 1) {
 #pragma omp parallel for schedule(static)
-    for (size_t i = 0; i < psz; ++i)
-      r[i] = -d_qm1 * o.vel_r[i] * gr[i] - d_qm1 * o.vel_t[i] * gt[i] - d_qm1 * o.vel_p[i] * gq[i];
+      for (size_t i = 0; i < psz; ++i)
+        r[i] = -d_qm1 * o.vel_r[i] * gr[i] - d_qm1 * o.vel_t[i] * gt[i] - d_qm1 * o.vel_p[i] * gq[i];
+    } else {
+      const double Diss = d_qm1 * d_qm1 / o.cfg.Ra;
+#pragma omp parallel for schedule(static)
+      for (int n = 0; n < o.N; ++n) {
+        const double xi0 = o.oc.rho1[n], T0 = o.oc.temp0[n], dT0 = o.oc.temp1[n], rho = o.oc.rho0[n];
+        const double rrr = o.oc.R(n + 1, 1), eta = o.oc.eta0[n];
+        for (size_t k = 0; k < (size_t)Th * Ph; ++k) {
+          size_t i = k + (size_t)Th * Ph * n;
+          double vr = o.vel_r[i], dur = o.vel_dur[i], qv1 = o.vel_qv1[i], qv2 = o.vel_qv2[i];
+          double x = 2.0 * (dur * dur);
+          double y = (xi0 + 1.0 / rrr) * vr + dur + qv1;
+          x = x + 2.0 * (y * y);
+          y = xi0 * vr;
+          x = x - 2.0 * (y * y) / 3.0;
+          y = qv1 + vr / rrr;
+          x = x + 2.0 * (y * y);
+          y = 2.0 * o.vel_dutr[i] - o.vel_cp[i];
+          x = x + y * y;
+          y = 2.0 * o.vel_dupr[i] + o.vel_ct[i];
+          x = x + y * y;
+          y = 2.0 * qv2 + o.vel_cr[i];
+          x = x + y * y;
+          double jr = o.mag_cr[i], jt = o.mag_ct[i], jp = o.mag_cp[i];
+          x = x + eta * ((jr * jr + jp * jp + jt * jt) / (rho * o.cfg.E));
+          double v = -(d_qm1 * vr * gr[i]) + (dT0 / T0) * gr[i];
+          v = v - d_qm1 * o.vel_t[i] * gt[i];
+          v = v - d_qm1 * o.vel_p[i] * gq[i];
+          r[i] = v + (Diss / T0) * x;
+        }
+      }
+    }
     Spec ss;
     tra_phys2spec(o, r, ss);
     Coll& NC = which == 0 ? o.codNC : o.compNC;
@@ -1521,7 +1856,14 @@ int check_cgce(Oracle& o) {
 // ========================================================================================
 // Energies (io.F90:1739-2024, variables.F90:903-957, 1118-1170)
 // ========================================================================================
+// var_coll_norm / _norm_comp / _norm_magdiss differ only in the radial weights
+void coll_norm_w(const Oracle& o, const Coll& a, const std::vector<double>& wts, double& Eodd, double& Eeven,
+                 double& Em0le, double& Em0);
 void coll_norm(const Oracle& o, const Coll& a, double& Eodd, double& Eeven, double& Em0le, double& Em0) {
+  coll_norm_w(o, a, o.oc.intr2dr, Eodd, Eeven, Em0le, Em0);
+}
+void coll_norm_w(const Oracle& o, const Coll& a, const std::vector<double>& wts, double& Eodd, double& Eeven,
+                 double& Em0le, double& Em0) {
   int N = o.N;
   std::vector<double> Fod(N, 0), Fev(N, 0), Fm0le(N, 0), Fm0(N, 0), f(N);
   for (int nh = 0; nh < o.H; ++nh) {
@@ -1537,8 +1879,25 @@ void coll_norm(const Oracle& o, const Coll& a, double& Eodd, double& Eeven, doub
     if (((l - m_) % 2 + 2) % 2 == 1) for (int n = 0; n < N; ++n) Fod[n] = Fod[n] + f[n];
     else for (int n = 0; n < N; ++n) Fev[n] = Fev[n] + f[n];
   }
-  auto dot = [&](const std::vector<double>& v) { double s = 0; for (int n = 0; n < N; ++n) s = s + v[n] * o.oc.intr2dr[n]; return s; };
+  auto dot = [&](const std::vector<double>& v) { double s = 0; for (int n = 0; n < N; ++n) s = s + v[n] * wts[n]; return s; };
   Eodd = dot(Fod); Eeven = dot(Fev); Em0le = dot(Fm0le); Em0 = dot(Fm0);
+}
+// var_coll_norm_veldiss (variables.F90:1034-1061)
+double coll_norm_veldiss(const Oracle& o, const Coll& a) {
+  int N = o.N;
+  std::vector<double> F(N, 0.0);
+  for (int nh = 0; nh < o.H; ++nh) {
+    int l = o.hl[nh], m_ = o.hm[nh];
+    double w = 4.0 * d_PI / (double)(2 * l + 1);
+    if (m_ != 0) w = 4.0 * w;
+    for (int n = 0; n < N; ++n) {
+      size_t i = n + (size_t)N * nh;
+      F[n] = F[n] + w * (a.re[i] * a.re[i] + a.im[i] * a.im[i]);
+    }
+  }
+  double s = 0;
+  for (int n = 0; n < N; ++n) s = s + F[n] * o.oc.intr2dr_veldiss[n];
+  return s;
 }
 double coll_norm_surf_in(const Oracle& o, const Coll& a, bool outer) {
   int N = o.N;
@@ -1550,47 +1909,55 @@ double coll_norm_surf_in(const Oracle& o, const Coll& a, bool outer) {
     size_t i = (outer ? N - 1 : 0) + (size_t)N * nh;
     F = F + w * (a.re[i] * a.re[i] + a.im[i] * a.im[i]);
   }
+  if (!o.cfg.boussinesq) return F * o.oc.rho0[outer ? N - 1 : 0] * o.oc.R(outer ? N : 1, 1);
   return F * o.oc.R(outer ? N : 1, 1);
 }
 
 void energies(Oracle& o, double* out) {
   for (int i = 0; i < LSD_NENERGY; ++i) out[i] = 0.0;
   out[LSD_E_TIME] = o.tim_t;
-  double KE = 0.5, VD = o.cfg.Pm, ME = o.cfg.Pm / o.cfg.E, OD = 2.0 * o.cfg.Pm / o.cfg.E;
+  // io_write2files prefactors (io.F90:234-247)
+  const bool bq = o.cfg.boussinesq != 0;
+  double KE = 0.5, VD = o.cfg.Pm, ME = 0.5 * o.cfg.Pm / o.cfg.E, OD = 1.0 * o.cfg.Pm / o.cfg.E;
+  if (bq) { ME = o.cfg.Pm / o.cfg.E; OD = 2.0 * o.cfg.Pm / o.cfg.E; }
+  const std::vector<double>& wv = bq ? o.oc.intr2dr : o.oc.intr2dr_comp;
   int N = o.N, KL = o.KL;
-  // heat fluxes
+  // heat fluxes (io.F90:1773-1794)
   double flx = 0;
   for (int j = N - KL; j <= N; ++j) flx = flx - o.codC.re[j - 1] * o.oc.dr[1].at(KL + 1 + N - j, j);
-  out[LSD_E_TOPFLX] = 4.0 * d_PI * o.oc.R(N, 2) * flx;
+  if (bq) out[LSD_E_TOPFLX] = 4.0 * d_PI * o.oc.R(N, 2) * flx;
+  else out[LSD_E_TOPFLX] = 4.0 * d_PI * o.oc.R(N, 2) * o.oc.rho0[N - 1] * o.oc.temp0[N - 1] * flx;
   flx = 0;
   for (int j = 1; j <= 1 + KL; ++j) flx = flx - o.codC.re[j - 1] * o.oc.dr[1].at(KL + 2 - j, j);
-  out[LSD_E_BOTFLX] = 4.0 * d_PI * o.oc.R(1, 2) * flx;
+  if (bq) out[LSD_E_BOTFLX] = 4.0 * d_PI * o.oc.R(1, 2) * flx;
+  else out[LSD_E_BOTFLX] = 4.0 * d_PI * o.oc.R(1, 2) * o.oc.rho0[0] * o.oc.temp0[0] * flx;
   // velocity
   {
     Coll q, s, t;
     torpol2qst(o, o.vTor, o.vPol, q, s, t, true);
     double Eo, Ee, E1, E0, Ep, Epas, Esym, El1, Et, Etas;
-    coll_norm(o, q, Eo, Ee, E1, E0);
+    coll_norm_w(o, q, wv, Eo, Ee, E1, E0);
     double ESin = coll_norm_surf_in(o, q, false), ESout = coll_norm_surf_in(o, q, true);
+    const double Ecomp = bq ? 0.0 : coll_norm_veldiss(o, q);
     Ep = Eo + Ee; Epas = E0; Esym = Ee; El1 = E1;
-    coll_norm(o, s, Eo, Ee, E1, E0);
+    coll_norm_w(o, s, wv, Eo, Ee, E1, E0);
     ESin = ESin + coll_norm_surf_in(o, s, false); ESout = ESout + coll_norm_surf_in(o, s, true);
     Ep = Ep + Eo + Ee; Epas = Epas + E0; Esym = Esym + Ee; El1 = El1 + E1;
-    coll_norm(o, t, Eo, Ee, E1, E0);
+    coll_norm_w(o, t, wv, Eo, Ee, E1, E0);
     ESin = ESin + coll_norm_surf_in(o, t, false); ESout = ESout + coll_norm_surf_in(o, t, true);
     Et = Eo + Ee; Etas = E0; Esym = Esym + Eo; El1 = El1 + E1;
     qstcurl(o, q, s, t, q, s, t);
     double EDis;
-    coll_norm(o, q, Eo, Ee, E1, E0); EDis = Eo + Ee;
-    coll_norm(o, s, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
-    coll_norm(o, t, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    coll_norm_w(o, q, wv, Eo, Ee, E1, E0); EDis = Eo + Ee;
+    coll_norm_w(o, s, wv, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    coll_norm_w(o, t, wv, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
     double ETm0 = KE * E0;
     out[LSD_E_KE] = KE * (Ep + Et);
     out[LSD_E_KE_TOR] = KE * Et;
     out[LSD_E_KE_SYM] = KE * Esym;
     out[LSD_E_KE_L1] = KE * El1;
     out[LSD_E_KE_TM0] = ETm0;
-    out[LSD_E_KE_DIS] = VD * EDis + VD * 2.0 * (ESin - ESout);
+    out[LSD_E_KE_DIS] = VD * EDis + VD * 2.0 * (ESin - ESout) + Ecomp;
     out[LSD_E_KE_AX] = KE * Epas + KE * Etas;
   }
   // magnetic
@@ -1605,10 +1972,10 @@ void energies(Oracle& o, double* out) {
     coll_norm(o, t, Eo, Ee, E1, E0);
     Et = Eo + Ee; Etas = E0; ETm0 = E0; Esym = Esym + Eo; El1 = El1 + E1;
     qstcurl(o, q, s, t, q, s, t);
-    double EDis;
-    coll_norm(o, q, Eo, Ee, E1, E0); EDis = Eo + Ee;
-    coll_norm(o, s, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
-    coll_norm(o, t, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    double EDis;  // var_coll_norm_magdiss
+    coll_norm_w(o, q, o.oc.intr2dr_magdiss, Eo, Ee, E1, E0); EDis = Eo + Ee;
+    coll_norm_w(o, s, o.oc.intr2dr_magdiss, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    coll_norm_w(o, t, o.oc.intr2dr_magdiss, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
     out[LSD_E_ME] = ME * (Ep + Et);
     out[LSD_E_ME_TOR] = ME * Et;
     out[LSD_E_ME_SYM] = ME * Esym;
@@ -1667,7 +2034,7 @@ Oracle* orc_create(const lsd_config* cfg, int* status) {
   o->L = cfg->L; o->M = cfg->M; o->Mp = cfg->Mp; o->N = cfg->N; o->KL = cfg->KL; o->Nic = cfg->Nic;
   *status = 0;
   if (o->L <= (o->M - 1) * o->Mp || (o->M > 1 && o->M % 2 == 1) || o->N < 2 * o->KL + 1 || o->Nic != 1 ||
-      !cfg->boussinesq || cfg->timestep <= 0) {
+      cfg->timestep <= 0) {
     *status = LSD_EARG;
     delete o;
     return nullptr;
@@ -1691,6 +2058,19 @@ Oracle* orc_create(const lsd_config* cfg, int* status) {
   return o;
 }
 void orc_destroy(Oracle* o) { delete o; }
+// io_load_radial_txtfiles (io.F90:559-608): prof = the seven columns of
+// planet_model.txt.in, [7][N]: rho, xi = rho'/rho, dxi/dr, T, dT/dr, eta, deta/dr.
+// Rebuilds the radial mesh weights/bands and the operators (mes_precompute + *_matrices).
+int orc_set_reference_state(Oracle* o, const double* prof) {
+  if (o->cfg.boussinesq) return LSD_EARG;
+  RDom& D = o->oc;
+  const int N = o->N;
+  std::vector<double>* cols[7] = {&D.rho0, &D.rho1, &D.rho2, &D.temp0, &D.temp1, &D.eta0, &D.eta1};
+  for (int k = 0; k < 7; ++k) cols[k]->assign(prof + (size_t)k * N, prof + (size_t)(k + 1) * N);
+  if (rdom_init(D, o->KL)) return LSD_ESINGULAR;
+  if (build_matrices(*o)) return LSD_ESINGULAR;
+  return 0;
+}
 void orc_sizes(const Oracle* o, lsd_sizes* s) {
   s->H = o->H; s->Th = o->Th; s->Th2 = o->Th2; s->Ph = o->Ph; s->Ma = o->Ma; s->Hc = o->Hc; s->Hr = o->Hr;
   s->N = o->N; s->L = o->L; s->M = o->M; s->Mp = o->Mp; s->KL = o->KL;
@@ -1809,6 +2189,20 @@ int orc_qst2rtp(Oracle* o, const double* qr, const double* qi, const double* sr,
   std::memcpy(r, a.data(), pn); std::memcpy(th, b.data(), pn); std::memcpy(ph, c.data(), pn);
   return 0;
 }
+int orc_qst2rtp_vel(Oracle* o, const double* const* in /*12: q s t qr sr tr, re/im*/, double* const* out /*8*/) {
+  Spec sp[6];
+  size_t n = (size_t)o->N * o->H * 8;
+  for (int k = 0; k < 6; ++k) {
+    sp[k].init(o->N, o->H);
+    std::memcpy(sp[k].re.data(), in[2 * k], n); std::memcpy(sp[k].im.data(), in[2 * k + 1], n);
+  }
+  Phys ph[8];
+  Phys* outs[8];
+  for (int k = 0; k < 8; ++k) outs[k] = &ph[k];
+  tra_qst2rtp_vel(*o, sp[0], sp[1], sp[2], sp[3], sp[4], sp[5], outs);
+  for (int k = 0; k < 8; ++k) std::memcpy(out[k], ph[k].data(), ph[k].size() * 8);
+  return 0;
+}
 int orc_rtp2qst(Oracle* o, const double* r, const double* th, const double* ph, double* qr, double* qi,
                 double* sr, double* si, double* tr, double* ti) {
   size_t psz = (size_t)o->Th * o->Ph * o->N;
@@ -1829,6 +2223,13 @@ int orc_grad(Oracle* o, const double* sre, const double* sim, double* th, double
   return 0;
 }
 
+int orc_dth(Oracle* o, const double* sre, const double* sim, double* p) {
+  Spec s; s.init(o->N, o->H);
+  std::memcpy(s.re.data(), sre, s.re.size() * 8); std::memcpy(s.im.data(), sim, s.im.size() * 8);
+  Phys a; tra_dth(*o, s, a);
+  std::memcpy(p, a.data(), a.size() * 8);
+  return 0;
+}
 int orc_nonlinear(Oracle* o) { evaluate(*o); return 0; }
 int orc_predictor(Oracle* o) { predictor(*o); o->tim_it = 1; return 0; }
 int orc_corrector(Oracle* o, double* dterr) {

@@ -8,7 +8,10 @@ Outputs (committed):
                     and the radial grid r, dt, t), copied verbatim;
   golden_t0.json    the t=0 rows of the reference's own time series for that state:
                     Benchmark_files/Boussinesq/Christensen_case1_benchmark/
-                    vel_energy.dat and mag_energy.dat (columns as written there).
+                    vel_energy.dat and mag_energy.dat (columns as written there);
+  planet_model_anelastic_benchmark.txt  the reference state of the anelastic benchmark
+                    (Benchmark_files/Anelastic/Anelastic_benchmark/planet_model.txt.in,
+                    128 shells, written by Scripts/anelastic_benchmark.m), copied verbatim.
 """
 import json
 import os
@@ -49,4 +52,7 @@ golden = {
 }
 with open(os.path.join(here, "golden_t0.json"), "w") as fh:
     json.dump(golden, fh, indent=1)
+src = os.path.join(ref, "Benchmark_files", "Anelastic", "Anelastic_benchmark", "planet_model.txt.in")
+with open(src) as fh, open(os.path.join(here, "planet_model_anelastic_benchmark.txt"), "w") as out:
+    out.write(fh.read())
 print("wrote", os.listdir(here))

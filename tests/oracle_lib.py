@@ -71,6 +71,9 @@ def load():
         "orc_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(capi.LsdStats)]),
         "orc_energies": (ctypes.c_int, [vp, _D]),
         "orc_set_threads": (ctypes.c_int, [ctypes.c_int]),
+        "orc_set_reference_state": (ctypes.c_int, [vp, _D]),
+        "orc_dth": (ctypes.c_int, [vp, _D, _D, _D]),
+        "orc_qst2rtp_vel": (ctypes.c_int, [vp, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)
@@ -195,6 +198,28 @@ class Oracle:
         ins = [np.ascontiguousarray(x) for x in (r, th, ph)]
         self.lib.orc_rtp2qst(self.h, *[_dp(a) for a in ins], *[_dp(o) for o in outs])
         return (outs[0], outs[1]), (outs[2], outs[3]), (outs[4], outs[5])
+
+    def qst2rtp_vel(self, q, s, t, qr, sr, tr):
+        """tra_qst2rtp_vel: -> r, th, ph, dur, qv1, dutr, dupr, qv2."""
+        ins = [np.ascontiguousarray(x) for pair in (q, s, t, qr, sr, tr) for x in pair]
+        outs = [np.zeros((self.N, self.Ph, self.Th)) for _ in range(8)]
+        pin = (_D * 12)(*[_dp(a) for a in ins])
+        pout = (_D * 8)(*[_dp(a) for a in outs])
+        assert self.lib.orc_qst2rtp_vel(self.h, pin, pout) == 0
+        return outs
+
+    def dth(self, sre, sim):
+        p = np.zeros((self.N, self.Ph, self.Th))
+        self.lib.orc_dth(self.h, _dp(np.ascontiguousarray(sre)), _dp(np.ascontiguousarray(sim)), _dp(p))
+        return p
+
+    def set_reference_state(self, prof):
+        """prof: (7, N) rho, xi, dxi/dr, T, dT/dr, eta, deta/dr (planet_model.txt.in)."""
+        prof = np.ascontiguousarray(prof, dtype=np.float64)
+        assert prof.shape == (7, self.N)
+        rc = self.lib.orc_set_reference_state(self.h, _dp(prof))
+        if rc != 0:
+            raise RuntimeError("oracle reference state failed: %d" % rc)
 
     def grad(self, sre, sim):
         t, p = np.zeros((self.N, self.Ph, self.Th)), np.zeros((self.N, self.Ph, self.Th))
