@@ -234,6 +234,22 @@ int lsd_energies(lsd_ctx* ctx, double* out);
  * any stream capture. */
 int lsd_energies_static(lsd_ctx* ctx, double* out);
 
+/* ---- ensembles (independent runs at their own resolutions) ---------------------------
+ * The reference runs one configuration per job; an ensemble (e.g. a parameter or
+ * resolution sweep) is n of them.  lsd_ensemble_create creates one context per config on
+ * one device (all cfgs[i].device equal); members are set up, read and diagnosed through
+ * the context API (lsd_ensemble_member); lsd_ensemble_step advances every member by
+ * nsteps completed steps of main.F90:100-164, the members' graphs running concurrently
+ * on their own streams.  stats: n entries, or NULL.  On an error lsd_ensemble_last_error
+ * names the member and its message. */
+typedef struct lsd_ensemble lsd_ensemble;
+int lsd_ensemble_create(int n, const lsd_config* cfgs, lsd_ensemble** out);
+int lsd_ensemble_destroy(lsd_ensemble* ens);
+int lsd_ensemble_size(const lsd_ensemble* ens);
+int lsd_ensemble_member(lsd_ensemble* ens, int i, lsd_ctx** ctx);
+int lsd_ensemble_step(lsd_ensemble* ens, int nsteps, lsd_stats* stats);
+const char* lsd_ensemble_last_error(const lsd_ensemble* ens);
+
 /* ---- batched banded radial solves (timestep.F90:566-588 over every (l,m)) -----------
  * Factorise nmat banded operators A_k (LAPACK band storage with ldab = 3*kl+1, columns
  * of length n, k = 0..nmat-1, overwritten by their LU factors and pivots like dgbtrf,

@@ -5,4 +5,4 @@ files), synthetic (seeded workloads), build (nvcc build of liblsd_b200.so).
 Import with importlib.import_module("leeds-code_b200").
 """
 from . import capi, state, synthetic  # noqa: F401
-from .lsd import Context, LsdError, load_library  # noqa: F401
+from .lsd import Context, Ensemble, LsdError, load_library  # noqa: F401

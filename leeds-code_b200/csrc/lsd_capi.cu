@@ -142,13 +142,19 @@ int check_cgce(lsd_ctx* c) {
   return fail ? LSD_ENOTCONVERGED : LSD_OK;
 }
 
-// read the corrector's sums of squares and form tim_dterr (timestep.F90:715-737)
-int finish_corrector(lsd_ctx* ctx) {
+// queue the copy of the corrector's sums of squares (and the tensor-core error flag) to
+// the pinned mirror; finish_corrector_host reads them once the stream got there
+int enqueue_corrector_readback(lsd_ctx* ctx) {
   CUDA_TRY(cudaMemcpyAsync(ctx->h_red, ctx->d_red, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream));
   int* oz_err = (int*)(ctx->h_red + 16);
   *oz_err = 0;
   if (ctx->oz) CUDA_TRY(cudaMemcpyAsync(oz_err, lsd_ozaki_err_flag(ctx), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return LSD_OK;
+}
+
+// form tim_dterr (timestep.F90:715-737) from the mirrored sums of squares
+int finish_corrector_host(lsd_ctx* ctx) {
+  const int* oz_err = (const int*)(ctx->h_red + 16);
   if (*oz_err) return lsd_fail(ctx, LSD_ECUDA, "tensor-core Legendre contraction: an mbarrier wait timed out");
   const double* r = ctx->h_red;
   double d = ctx->dterr;
@@ -162,6 +168,23 @@ int finish_corrector(lsd_ctx* ctx) {
   d = d + std::sqrt(r[7]);  // inner-core Pol
   ctx->dterr = d;
   if (!std::isfinite(d)) return lsd_fail(ctx, LSD_ENONFINITE, "non-finite corrector norm (state diverged)");
+  return LSD_OK;
+}
+
+int finish_corrector(lsd_ctx* ctx) {
+  int rc = enqueue_corrector_readback(ctx);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return finish_corrector_host(ctx);
+}
+
+int capture(lsd_ctx* ctx, bool pred, cudaGraphExec_t* out, long long* nkernels);
+int ensure_graphs(lsd_ctx* ctx) {
+  int rc;
+  if (!ctx->g_pred) {
+    if ((rc = capture(ctx, true, &ctx->g_pred, &ctx->g_pred_kernels))) return rc;
+    if ((rc = capture(ctx, false, &ctx->g_corr, &ctx->g_corr_kernels))) return rc;
+  }
   return LSD_OK;
 }
 
@@ -780,10 +803,7 @@ int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats) {
   CUDA_TRY(cudaSetDevice(ctx->dev));
   int rc;
   long long l0 = ctx->launches;
-  if (!ctx->g_pred) {
-    if ((rc = capture(ctx, true, &ctx->g_pred, &ctx->g_pred_kernels))) return rc;
-    if ((rc = capture(ctx, false, &ctx->g_corr, &ctx->g_corr_kernels))) return rc;
-  }
+  if ((rc = ensure_graphs(ctx))) return rc;
   const long long per_pred = ctx->g_pred_kernels, per_corr = ctx->g_corr_kernels;
   int done = 0, corr = 0, evals = 0;
   double last = 0.0;
@@ -816,6 +836,129 @@ int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats) {
     stats->steps_done = done; stats->correctors = corr; stats->evaluations = evals;
     stats->kernel_launches = (int)(ctx->launches - l0); stats->last_dterr = last;
     stats->t = ctx->t; stats->dt = ctx->dt;
+  }
+  return LSD_OK;
+}
+
+// ---- ensembles: independent runs advanced in lock-step, one stream each ------------------
+// Each pass enqueues, for every member still short of its steps, the graphs up to its
+// next host decision (predictor + first corrector of a new step, or one more corrector)
+// and the copy of its corrector norms, on the member's own stream; only then does the
+// host wait, member by member, and apply tim_check_cgce.  The members' kernels therefore
+// share the device while any one of them waits for its host decision.
+struct lsd_ensemble {
+  std::vector<lsd_ctx*> m;
+  std::string err;
+};
+
+int lsd_ensemble_create(int n, const lsd_config* cfgs, lsd_ensemble** out) {
+  if (!cfgs || !out || n < 1) return LSD_EARG;
+  *out = nullptr;
+  lsd_ensemble* e = new (std::nothrow) lsd_ensemble();
+  if (!e) return LSD_ENOMEM;
+  for (int i = 0; i < n; ++i) {
+    lsd_ctx* c = nullptr;
+    int rc = lsd_create(&cfgs[i], &c);
+    if (rc) {
+      for (lsd_ctx* x : e->m) lsd_destroy(x);
+      delete e;
+      return rc;
+    }
+    if (i > 0 && c->dev != e->m[0]->dev) {
+      lsd_destroy(c);
+      for (lsd_ctx* x : e->m) lsd_destroy(x);
+      delete e;
+      return LSD_EARG;
+    }
+    e->m.push_back(c);
+  }
+  *out = e;
+  return LSD_OK;
+}
+
+int lsd_ensemble_destroy(lsd_ensemble* e) {
+  if (!e) return LSD_OK;
+  for (lsd_ctx* c : e->m) lsd_destroy(c);
+  delete e;
+  return LSD_OK;
+}
+
+int lsd_ensemble_size(const lsd_ensemble* e) { return e ? (int)e->m.size() : 0; }
+
+int lsd_ensemble_member(lsd_ensemble* e, int i, lsd_ctx** ctx) {
+  if (!e || !ctx || i < 0 || i >= (int)e->m.size()) return LSD_EARG;
+  *ctx = e->m[i];
+  return LSD_OK;
+}
+
+const char* lsd_ensemble_last_error(const lsd_ensemble* e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int lsd_ensemble_step(lsd_ensemble* e, int nsteps, lsd_stats* stats) {
+  if (!e || nsteps < 0) return LSD_EARG;
+  const int n = (int)e->m.size();
+  auto fail = [&](int i, int rc) {
+    e->err = "member " + std::to_string(i) + ": " + e->m[i]->err;
+    return rc;
+  };
+  if (cudaSetDevice(e->m[0]->dev) != cudaSuccess) return LSD_ECUDA;
+  std::vector<int> done(n, 0), corr(n, 0), evals(n, 0);
+  std::vector<long long> l0(n);
+  std::vector<double> last(n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    int rc = ensure_graphs(e->m[i]);
+    if (rc) return fail(i, rc);
+    l0[i] = e->m[i]->launches;
+    if ((rc = time_begin(e->m[i]))) return fail(i, rc);
+  }
+  std::vector<char> pending(n, 0);
+  for (;;) {
+    bool any = false;
+    for (int i = 0; i < n; ++i) {  // enqueue up to each member's next host decision
+      lsd_ctx* c = e->m[i];
+      pending[i] = 0;
+      if (done[i] >= nsteps) continue;
+      if (c->it == 0) {
+        if (cudaGraphLaunch(c->g_pred, c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "graph launch"));
+        c->launches += c->g_pred_kernels;
+        ++evals[i];
+        c->it = 1;
+      }
+      c->dterr = 0.0;
+      if (cudaGraphLaunch(c->g_corr, c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "graph launch"));
+      c->launches += c->g_corr_kernels;
+      ++evals[i];
+      ++corr[i];
+      int rc = enqueue_corrector_readback(c);
+      if (rc) return fail(i, rc);
+      pending[i] = 1;
+      any = true;
+    }
+    if (!any) break;
+    for (int i = 0; i < n; ++i) {  // host decisions (tim_check_cgce), member by member
+      if (!pending[i]) continue;
+      lsd_ctx* c = e->m[i];
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "stream"));
+      int rc = finish_corrector_host(c);
+      if (rc) return fail(i, rc);
+      last[i] = c->dterr;
+      if ((rc = check_cgce(c))) return fail(i, lsd_fail(c, rc, "tim_check_cgce: corrector iterations did not converge"));
+      if (c->it == 0) {
+        c->t = c->t + c->dt;
+        c->step = c->step + 1;
+        ++done[i];
+      }
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    lsd_ctx* c = e->m[i];
+    int rc = time_end(c);
+    if (rc) return fail(i, rc);
+    c->have_eval = false;
+    if (stats) {
+      stats[i].steps_done = done[i]; stats[i].correctors = corr[i]; stats[i].evaluations = evals[i];
+      stats[i].kernel_launches = (int)(c->launches - l0[i]); stats[i].last_dterr = last[i];
+      stats[i].t = c->t; stats[i].dt = c->dt;
+    }
   }
   return LSD_OK;
 }

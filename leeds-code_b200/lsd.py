@@ -64,6 +64,11 @@ def load_library(path=None):
         "lsd_tra_dth": [_V, _D, _D, _D],
         "lsd_tra_qst2rtp_vel": [_V] + [_D] * 20,
         "lsd_set_reference_state": [_V, _D],
+        "lsd_ensemble_create": [ctypes.c_int, ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(_V)],
+        "lsd_ensemble_destroy": [_V],
+        "lsd_ensemble_size": [_V],
+        "lsd_ensemble_member": [_V, ctypes.c_int, ctypes.POINTER(_V)],
+        "lsd_ensemble_step": [_V, ctypes.c_int, ctypes.POINTER(capi.LsdStats)],
         "lsd_sht_synth_device": [_V, ctypes.c_int, _V, _V],
         "lsd_sht_analys_device": [_V, ctypes.c_int, _V, _V],
         "lsd_matrices": [_V],
@@ -87,6 +92,8 @@ def load_library(path=None):
         f.argtypes = args
     lib.lsd_last_error.restype = ctypes.c_char_p
     lib.lsd_last_error.argtypes = [_V]
+    lib.lsd_ensemble_last_error.restype = ctypes.c_char_p
+    lib.lsd_ensemble_last_error.argtypes = [_V]
     _LIB = lib
     return lib
 
@@ -114,12 +121,16 @@ def _c(a):
 class Context:
     """One simulation context on one GPU (the reference's module state of one run)."""
 
-    def __init__(self, cfg):
+    def __init__(self, cfg, _handle=None):
         self.lib = load_library()
-        h = _V()
-        rc = self.lib.lsd_create(ctypes.byref(cfg), ctypes.byref(h))
-        if rc != 0:
-            raise LsdError(rc, "lsd_create failed (check the configuration and the device)")
+        self.owned = _handle is None
+        if _handle is None:
+            h = _V()
+            rc = self.lib.lsd_create(ctypes.byref(cfg), ctypes.byref(h))
+            if rc != 0:
+                raise LsdError(rc, "lsd_create failed (check the configuration and the device)")
+        else:
+            h = _handle
         self.h = h
         self.cfg = cfg
         s = capi.LsdSizes()
@@ -135,7 +146,8 @@ class Context:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.lsd_destroy(self.h)
+            if self.owned:
+                self.lib.lsd_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -330,3 +342,47 @@ class Context:
     def load_fields(self, fields):
         for f, (re, im) in fields.items():
             self.set_coll(f, re, im)
+
+
+class Ensemble:
+    """n independent runs (their own configurations and resolutions) on one GPU, stepped
+    in lock-step with their graphs on separate streams (lsd_ensemble_*).  members[i] is a
+    Context view of run i (set_coll, set_reference_state, energies, ...)."""
+
+    def __init__(self, cfgs):
+        self.lib = load_library()
+        arr = (capi.LsdConfig * len(cfgs))(*cfgs)
+        h = _V()
+        rc = self.lib.lsd_ensemble_create(len(cfgs), arr, ctypes.byref(h))
+        if rc != 0:
+            raise LsdError(rc, "lsd_ensemble_create failed")
+        self.h = h
+        self.members = []
+        for i, cfg in enumerate(cfgs):
+            m = _V()
+            self._ok(self.lib.lsd_ensemble_member(self.h, i, ctypes.byref(m)))
+            self.members.append(Context(cfg, _handle=m))
+
+    def _ok(self, rc):
+        if rc != 0:
+            msg = self.lib.lsd_ensemble_last_error(self.h)
+            raise LsdError(rc, msg.decode() if msg else "")
+        return rc
+
+    def step(self, nsteps=1):
+        st = (capi.LsdStats * len(self.members))()
+        self._ok(self.lib.lsd_ensemble_step(self.h, int(nsteps), st))
+        return list(st)
+
+    def close(self):
+        if getattr(self, "h", None):
+            for m in self.members:
+                m.h = None
+            self.lib.lsd_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
