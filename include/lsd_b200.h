@@ -169,6 +169,11 @@ int lsd_get_nonlinear(lsd_ctx* ctx, int which, double* re, double* im);
 /* tim_t, tim_dt; setting dt rebuilds the operators (vel/cod/mag_matrices). */
 int lsd_set_time(lsd_ctx* ctx, double t, double dt);
 int lsd_get_time(const lsd_ctx* ctx, double* t, double* dt, int* step);
+/* With cfg.timestep < 0 (d_timestep < 0) lsd_step sets dt itself each step:
+ * non_maxtstep (nonlinear.F90:546-615) + tim_new_tstep (timestep.F90:837-870), the
+ * operators rebuilt on a change (main.F90:126-134).  out[3] = tim_dt, tim_corr_dt,
+ * tim_cfl_dt (io_write_timestep, io.F90:2343-2346). */
+int lsd_get_dt_control(const lsd_ctx* ctx, double* out);
 
 /* ---- transforms on host buffers (unit parity with transform.fftw3.F90) --------------
  * Each works on all N shells of the context. */

@@ -27,13 +27,15 @@ void free_ctx(lsd_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->g_pred) cudaGraphExecDestroy(ctx->g_pred);
   if (ctx->g_corr) cudaGraphExecDestroy(ctx->g_corr);
+  if (ctx->g_eval) cudaGraphExecDestroy(ctx->g_eval);
+  if (ctx->g_psolve) cudaGraphExecDestroy(ctx->g_psolve);
   lsd_ozaki_free(ctx);
   void* ptrs[] = {ctx->d_sblk_l, ctx->d_sblk_nh, ctx->d_aperm, ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_bin2c, ctx->d_lm2nh,
                   ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,
                   ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y, ctx->d_yt,
                   ctx->d_ipiv, ctx->d_ipivs, ctx->d_info, ctx->d_gre, ctx->d_gret, ctx->d_invg, ctx->d_state, ctx->d_nl,
                   ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red, ctx->d_ref, ctx->d_laps,
-                  ctx->d_compr1dr, ctx->d_wts, ctx->d_ones};
+                  ctx->d_compr1dr, ctx->d_wts, ctx->d_ones, ctx->d_cfl};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -178,22 +180,61 @@ int finish_corrector(lsd_ctx* ctx) {
   return finish_corrector_host(ctx);
 }
 
-int capture(lsd_ctx* ctx, bool pred, cudaGraphExec_t* out, long long* nkernels);
+enum CaptureKind { CAP_EVAL_PRED = 0, CAP_EVAL_CORR, CAP_EVAL, CAP_PRED };
+int capture(lsd_ctx* ctx, int kind, cudaGraphExec_t* out, long long* nkernels);
 int ensure_graphs(lsd_ctx* ctx) {
   int rc;
-  if (!ctx->g_pred) {
-    if ((rc = capture(ctx, true, &ctx->g_pred, &ctx->g_pred_kernels))) return rc;
-    if ((rc = capture(ctx, false, &ctx->g_corr, &ctx->g_corr_kernels))) return rc;
+  if (!ctx->g_corr) {
+    if ((rc = capture(ctx, CAP_EVAL_CORR, &ctx->g_corr, &ctx->g_corr_kernels))) return rc;
+    if (ctx->cfg.timestep < 0) {
+      if ((rc = capture(ctx, CAP_EVAL, &ctx->g_eval, &ctx->g_eval_kernels))) return rc;
+      if ((rc = capture(ctx, CAP_PRED, &ctx->g_psolve, &ctx->g_psolve_kernels))) return rc;
+    } else {
+      if ((rc = capture(ctx, CAP_EVAL_PRED, &ctx->g_pred, &ctx->g_pred_kernels))) return rc;
+    }
   }
   return LSD_OK;
 }
 
-int capture(lsd_ctx* ctx, bool pred, cudaGraphExec_t* out, long long* nkernels) {
+// tim_new_tstep (timestep.F90:837-870) with the CFL limit of the last evaluation; on a new
+// dt the operators are rebuilt (main.F90:126-134)
+int new_tstep(lsd_ctx* c) {
+  double dt = c->dt;
+  const lsd_config& g = c->cfg;
+  if (g.time_step_control == 1) {
+    if (c->corr_dt > g.corr_upper) dt = 0.5 * dt;
+    if (c->corr_dt < g.corr_lower) dt = 1.273974 * dt;
+    if (c->step == 0) dt = std::min(dt / 1e3, 1e-8);
+  } else {
+    if (c->corr_dt > 0.0) dt = std::min(c->corr_dt, dt * 2.0 / g.courant);
+    if (c->cfl_dt > 0.0) dt = std::min(c->cfl_dt, dt);
+    if (c->step == 0) dt = std::min(dt / 1e3, 1e-10);
+    dt = dt * g.courant;
+  }
+  if (dt < c->dt * 0.97 || dt > c->dt * 1.03) {
+    c->dt = dt;
+    return lsd_build_operators(c);
+  }
+  return LSD_OK;
+}
+
+// the CFL limit of the evaluation queued last (d_cfl), read on the host
+int read_cfl(lsd_ctx* ctx) {
+  CUDA_TRY(cudaMemcpyAsync(ctx->h_red + 24, ctx->d_cfl + 2 * ctx->N, sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->cfl_dt = ctx->h_red[24];
+  return LSD_OK;
+}
+
+int capture(lsd_ctx* ctx, int kind, cudaGraphExec_t* out, long long* nkernels) {
   cudaGraph_t g = nullptr;
   CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
   long long before = ctx->launches;
-  int rc = lsd_eval(ctx);
-  if (!rc) rc = pred ? lsd_pred(ctx) : lsd_corr(ctx);
+  int rc = kind == CAP_PRED ? LSD_OK : lsd_eval(ctx);
+  if (!rc && kind == CAP_EVAL_PRED) rc = lsd_pred(ctx);
+  if (!rc && kind == CAP_EVAL_CORR) rc = lsd_corr(ctx);
+  if (!rc && kind == CAP_PRED) rc = lsd_pred(ctx);
   cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
   *nkernels = ctx->launches - before;
   ctx->launches = before;
@@ -239,7 +280,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   else if (c.L <= (c.M - 1) * c.Mp) why = "set L > (M-1)*Mp";
   else if (c.M % 2 == 1) why = "if(M>1) set M even";
   else if (c.Nic != 1) why = "only an insulating inner core (Nic = 1) is supported";
-  else if (c.timestep <= 0.0) why = "only a fixed timestep (d_timestep > 0) is supported";
+  else if (c.timestep == 0.0) why = "d_timestep must be > 0 (fixed) or < 0 (CFL / corrector controlled)";
   else if (!c.vel_tstep || !c.cod_tstep || !c.mag_tstep) why = "velocity, codensity and field must all be stepped";
   else if (c.precision != LSD_PREC_FP64 && c.precision != LSD_PREC_OZAKI) why = "unknown precision";
   else if (c.precision == LSD_PREC_OZAKI && c.ozaki_slices != 0 && (c.ozaki_slices < 2 || c.ozaki_slices > 8))
@@ -254,7 +295,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   ctx->Hr = ctx->H / ctx->Hc;
   ctx->NM = 2 * ctx->Hc;
   ctx->P2 = ctx->Ma;
-  ctx->dt = c.timestep;
+  ctx->dt = c.timestep < 0 ? -c.timestep : c.timestep;  // d_timestep < 0: |d_timestep| until lsd_set_time
   ctx->HB = (ctx->Th2 + 1) / 2;
   if (!lsd_fft_plan(ctx)) { int rc = lsd_fail(ctx, LSD_EARG, "phi FFT length 3M/2 not supported"); free_ctx(ctx); return rc; }
   int ndev = 0;
@@ -385,6 +426,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   }
   TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * ctx->HB * NM * 4));
   TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
+  TRY(dalloc(ctx, &ctx->d_cfl, (size_t)2 * N + 1));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));
   ctx->h_pin_bytes = std::max(sizeof(cplx) * F * 3, sizeof(double) * 16);
   CTRY(cudaMallocHost((void**)&ctx->h_pin, ctx->h_pin_bytes));
@@ -511,9 +553,13 @@ int lsd_set_time(lsd_ctx* ctx, double t, double dt) {
     ctx->dt = dt;
     int rc = lsd_build_operators(ctx);
     if (rc) return rc;
-    if (ctx->g_pred) { cudaGraphExecDestroy(ctx->g_pred); ctx->g_pred = nullptr; }
-    if (ctx->g_corr) { cudaGraphExecDestroy(ctx->g_corr); ctx->g_corr = nullptr; }
   }
+  return LSD_OK;
+}
+// tim_dt, tim_corr_dt, tim_cfl_dt (the columns of io_write_timestep, io.F90:2343-2346)
+int lsd_get_dt_control(const lsd_ctx* ctx, double* out) {
+  if (!ctx || !out) return LSD_EARG;
+  out[0] = ctx->dt; out[1] = ctx->corr_dt; out[2] = ctx->cfl_dt;
   return LSD_OK;
 }
 int lsd_get_time(const lsd_ctx* ctx, double* t, double* dt, int* step) {
@@ -808,8 +854,17 @@ int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats) {
   int done = 0, corr = 0, evals = 0;
   double last = 0.0;
   if ((rc = time_begin(ctx))) return rc;
+  const bool vardt = ctx->cfg.timestep < 0;
   while (done < nsteps) {
-    if (ctx->it == 0) {
+    if (ctx->it == 0 && vardt) {  // evaluation, then non_maxtstep + tim_new_tstep (main.F90:126-134)
+      CUDA_TRY(cudaGraphLaunch(ctx->g_eval, ctx->stream));
+      ctx->launches += ctx->g_eval_kernels;
+      ++evals;
+      if ((rc = read_cfl(ctx)) || (rc = new_tstep(ctx))) return rc;
+      CUDA_TRY(cudaGraphLaunch(ctx->g_psolve, ctx->stream));
+      ctx->launches += ctx->g_psolve_kernels;
+      ctx->it = 1;
+    } else if (ctx->it == 0) {
       CUDA_TRY(cudaGraphLaunch(ctx->g_pred, ctx->stream));
       ctx->launches += per_pred;
       ++evals;
@@ -912,6 +967,30 @@ int lsd_ensemble_step(lsd_ensemble* e, int nsteps, lsd_stats* stats) {
   }
   std::vector<char> pending(n, 0);
   for (;;) {
+    // members with d_timestep < 0 that start a step: evaluation, then the dt decision
+    for (int i = 0; i < n; ++i) {
+      lsd_ctx* c = e->m[i];
+      pending[i] = 0;
+      if (done[i] >= nsteps || c->it != 0 || c->cfg.timestep >= 0) continue;
+      if (cudaGraphLaunch(c->g_eval, c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "graph launch"));
+      c->launches += c->g_eval_kernels;
+      ++evals[i];
+      if (cudaMemcpyAsync(c->h_red + 24, c->d_cfl + 2 * c->N, sizeof(double), cudaMemcpyDeviceToHost, c->stream) !=
+          cudaSuccess)
+        return fail(i, lsd_fail(c, LSD_ECUDA, "cfl readback"));
+      pending[i] = 1;
+    }
+    for (int i = 0; i < n; ++i) {
+      if (!pending[i]) continue;
+      lsd_ctx* c = e->m[i];
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "stream"));
+      c->cfl_dt = c->h_red[24];
+      int rc = new_tstep(c);
+      if (rc) return fail(i, rc);
+      if (cudaGraphLaunch(c->g_psolve, c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "graph launch"));
+      c->launches += c->g_psolve_kernels;
+      c->it = 1;
+    }
     bool any = false;
     for (int i = 0; i < n; ++i) {  // enqueue up to each member's next host decision
       lsd_ctx* c = e->m[i];

@@ -143,13 +143,18 @@ struct lsd_ctx {
   double *d_red = nullptr;   // small reduction area
   double *h_red = nullptr;   // pinned mirror
   // time
-  double t = 0.0, dt = 0.0, dterr = 0.0, corr_dt = 0.0, lasterr = 1e99;
+  double t = 0.0, dt = 0.0, dterr = 0.0, corr_dt = 0.0, lasterr = 1e99, cfl_dt = 0.0;
+  double* d_cfl = nullptr;  // variable dt: [2N] per-shell CFL maxima + tim_cfl_dt
   int it = 0, step = 0;
   bool have_eval = false;
   int tim_pcn = -1;
   // CUDA graph of one (evaluation + predictor/corrector) pass
   cudaGraphExec_t g_pred = nullptr, g_corr = nullptr;
   long long g_pred_kernels = 0, g_corr_kernels = 0;
+  // variable dt: the evaluation and the predictor solve as separate graphs (a host
+  // decision on dt sits between them)
+  cudaGraphExec_t g_eval = nullptr, g_psolve = nullptr;
+  long long g_eval_kernels = 0, g_psolve_kernels = 0;
   void* oz = nullptr;  // tensor-core path state (lsd_ozaki.cu)
 };
 
@@ -168,6 +173,7 @@ bool lsd_fft_plan(lsd_ctx* c);
 int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out);
 size_t lsd_products_smem(const lsd_ctx* ctx);
 int lsd_launch_qv(lsd_ctx* ctx, const cplx* th, const cplx* ph, cplx* qv1, cplx* qv2);
+int lsd_launch_cfl_finish(lsd_ctx* ctx);
 // ---- spectral algebra and solves (lsd_solve.cu) ----
 int lsd_eval(lsd_ctx* ctx);            // one nonlinear evaluation (device)
 int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks);

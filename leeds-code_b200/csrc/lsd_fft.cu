@@ -369,8 +369,22 @@ struct ProdConst {
   const double* sn1;  // 1/sin(theta_j)
   const double* r;    // [7][N] powers of r
   const double* ref;  // [7][N] reference state (anelastic)
+  unsigned long long* cflmax;  // variable dt: per-shell CFL maxima [N][2] (bits of doubles >= 0), or null
+  int L;
   int fin[PROD_MAXIN];  // input field slots of four_in
 };
+
+// the two velocities of non_maxtstep (nonlinear.F90:577-603) at one point: radial
+// B_r^2 / sqrt(B_r^2 E/Pm + d_r) + |u_r| and horizontal
+// (B_th^2 + B_ph^2) / sqrt((B_th^2 + B_ph^2) E/Pm + d_h) + |u_h|
+__device__ __forceinline__ void cfl_point(const double* v, double EPm, double E, double Pm, double dr2,
+                                          double dh2, double& mr, double& mh) {
+  const double vr = v[0], vt = v[1], vp = v[2], br = v[6], bt = v[7], bp = v[8];
+  const double p = br * br;
+  mr = fmax(mr, p / sqrt(p * EPm + dr2) + fabs(vr));
+  const double q = bt * bt + bp * bp;
+  mh = fmax(mh, q / sqrt(q * E / Pm + dh2) + sqrt(vt * vt + vp * vp));
+}
 
 // per-shell constants of the anelastic sets
 struct ShellC { double xi0, xi1, rm1, rinv, rrr, rho, T0, dT0, eta, Cmag; };
@@ -535,6 +549,19 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
   __syncthreads();
   // ---- products at every point (row side, sample position, part re/im), in place into 0..NF_OUT-1
   const double scale = 1.0 / (double)pl.Ph;
+  constexpr bool HAS_UB = (PS == PS_BOUSS || PS == PS_BOUSS_COMP || PS == PS_ANEL_MOM);
+  double cmr = 0.0, cmh = 0.0, cdr2 = 0.0, cdh2 = 0.0, EPm = 0.0;
+  if (HAS_UB && pc.cflmax) {  // non_maxtstep's d per shell (nonlinear.F90:574-592)
+    const double* r1 = pc.r + (size_t)4 * N;
+    const double dr = n == 0 ? r1[1] - r1[0] : n == N - 1 ? r1[N - 1] - r1[N - 2]
+                                              : fmin(r1[n] - r1[n - 1], r1[n + 1] - r1[n]);
+    double d = (pc.E + pc.E / pc.Pm) / (2.0 * dr);
+    cdr2 = d * d;
+    const double drh = r1[n] / sqrt((double)(pc.L * (pc.L - 1)));
+    d = pc.E / (2.0 * drh);
+    cdh2 = d * d;
+    EPm = pc.E / pc.Pm;
+  }
   for (int i = tid; i < 2 * P2; i += PROD_THREADS) {
     const int r = i / P2, pos = ppos<G>(i - r * P2);
     const int j = row_theta(h, r, Th);
@@ -548,6 +575,8 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
       double x[NF], o[NF_OUT];
 #pragma unroll
       for (int f = 0; f < NF; ++f) x[f] = part == 0 ? v[f].x : v[f].y;
+      if constexpr (HAS_UB)
+        if (pc.cflmax) cfl_point(x, EPm, pc.E, pc.Pm, cdr2, cdh2, cmr, cmh);
       prod_point<PS>(x, o, pc, sh, sn, cs);
 #pragma unroll
       for (int q = 0; q < NF_OUT; ++q) {
@@ -556,6 +585,18 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
     }
 #pragma unroll
     for (int q = 0; q < NF_OUT; ++q) rows[(size_t)(q * 2 + r) * RS + pos] = out[q];
+  }
+  if constexpr (HAS_UB) {
+    if (pc.cflmax) {  // CTA maxima -> the shell's slots (doubles >= 0 order as their bits)
+      for (int o = 16; o > 0; o >>= 1) {
+        cmr = fmax(cmr, __shfl_down_sync(0xffffffffu, cmr, o));
+        cmh = fmax(cmh, __shfl_down_sync(0xffffffffu, cmh, o));
+      }
+      if ((tid & 31) == 0) {
+        atomicMax(pc.cflmax + 2 * n, (unsigned long long)__double_as_longlong(cmr));
+        atomicMax(pc.cflmax + 2 * n + 1, (unsigned long long)__double_as_longlong(cmh));
+      }
+    }
   }
   __syncthreads();
   // ---- forward FFTs of the product rows (spectrum back in natural order)
@@ -766,6 +807,35 @@ int launch_products_set(lsd_ctx* ctx, const ProdConst& pc, const cplx* four_in, 
 }
 }  // namespace
 
+// tim_cfl_dt from the per-shell maxima (nonlinear.F90:593-605); one thread, shells in order
+__global__ void k_cfl_finish(int N, int L, double E, double Pm, const double* r, const unsigned long long* cflmax,
+                             double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double* r1 = r + (size_t)4 * N;
+  double cfl = 1e99;
+  for (int n = 0; n < N; ++n) {
+    const double dr = n == 0 ? r1[1] - r1[0] : n == N - 1 ? r1[N - 1] - r1[N - 2]
+                                              : fmin(r1[n] - r1[n - 1], r1[n + 1] - r1[n]);
+    const double mr = __longlong_as_double((long long)cflmax[2 * n]);
+    if (mr != 0.0) cfl = fmin(cfl, dr / mr);
+    const double drh = r1[n] / sqrt((double)(L * (L - 1)));
+    const double mh = __longlong_as_double((long long)cflmax[2 * n + 1]);
+    if (mh != 0.0) cfl = fmin(cfl, drh / mh);
+  }
+  cfl = fmin(cfl, E / Pm);
+  cfl = fmin(cfl, sqrt(E));
+  *out = cfl;
+}
+
+int lsd_launch_cfl_finish(lsd_ctx* ctx) {
+  k_cfl_finish<<<1, 32, 0, ctx->stream>>>(ctx->N, ctx->L, ctx->cfg.E, ctx->cfg.Pm, ctx->d_r,
+                                          (const unsigned long long*)ctx->d_cfl, ctx->d_cfl + 2 * ctx->N);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_cfl_finish: ") + cudaGetErrorString(e));
+  return LSD_OK;
+}
+
 int lsd_launch_qv(lsd_ctx* ctx, const cplx* th, const cplx* ph, cplx* qv1, cplx* qv2) {
   FFTPlanDev pl = make_plan(ctx);
   const size_t total = (size_t)ctx->N * ctx->HB * ctx->NM * 2;
@@ -804,6 +874,8 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.sn1 = ctx->d_sn1;
   pc.r = ctx->d_r;
   pc.ref = ctx->d_ref;
+  pc.L = ctx->L;
+  pc.cflmax = c.timestep < 0 ? (unsigned long long*)ctx->d_cfl : nullptr;
   const bool comp = c.comp_tstep != 0;
   const size_t FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
   if (c.boussinesq) {

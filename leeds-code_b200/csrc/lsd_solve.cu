@@ -734,7 +734,10 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   if ((rc = lsd_launch_synth(ctx, sg, ng))) return rc;
   if (marks) cudaEventRecord(marks[1], s);
   cplx* fa = fo + nsyn * FF;  // the 7 (8) product fields, in the analysis layout
+  const bool vardt = ctx->cfg.timestep < 0;
+  if (vardt) CUDA_TRY(cudaMemsetAsync(ctx->d_cfl, 0, sizeof(double) * 2 * ctx->N, s));
   if ((rc = lsd_launch_products(ctx, fo, fa))) return rc;
+  if (vardt && (rc = lsd_launch_cfl_finish(ctx))) return rc;  // non_maxtstep
   if (marks) cudaEventRecord(marks[2], s);
   AnalGroup ag[4];
   ag[0].kind = AK_VECTOR;

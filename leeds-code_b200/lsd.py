@@ -64,6 +64,7 @@ def load_library(path=None):
         "lsd_tra_dth": [_V, _D, _D, _D],
         "lsd_tra_qst2rtp_vel": [_V] + [_D] * 20,
         "lsd_set_reference_state": [_V, _D],
+        "lsd_get_dt_control": [_V, _D],
         "lsd_ensemble_create": [ctypes.c_int, ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(_V)],
         "lsd_ensemble_destroy": [_V],
         "lsd_ensemble_size": [_V],
@@ -257,6 +258,12 @@ class Context:
         ins = [_c(x) for pair in (q, s, t, qr, sr, tr) for x in pair]
         self._ok(self.lib.lsd_tra_qst2rtp_vel(self.h, *[_dp(a) for a in ins], *[_dp(o) for o in outs]))
         return outs
+
+    def dt_control(self):
+        """tim_dt, tim_corr_dt, tim_cfl_dt (io.F90:2346)."""
+        out = np.zeros(3)
+        self._ok(self.lib.lsd_get_dt_control(self.h, _dp(out)))
+        return out
 
     # ---- anelastic reference state (io.F90:559-608)
     def set_reference_state(self, prof):

@@ -22,8 +22,8 @@
 //     restated from the reference LAPACK algorithms.  tests/ pin these against scipy's
 //     LAPACK (scipy.linalg.lapack.dgbtrf/dgbtrs).
 // Scope: Boussinesq or anelastic MHD + codensity (+ composition) with an insulating
-// inner core (i_Nic = 1), fixed dt (d_timestep > 0), no SHTns, no inhomogeneous BC
-// files.  The anelastic reference state (io.F90:559-608, the seven columns of
+// inner core (i_Nic = 1), fixed dt (d_timestep > 0) or the CFL / corrector-controlled
+// dt (d_timestep < 0), no SHTns, no inhomogeneous BC files.  The anelastic reference state (io.F90:559-608, the seven columns of
 // planet_model.txt.in) is handed over by orc_set_reference_state.
 //
 // Build: g++ -O3 -march=native -fopenmp -ffp-contract=off -shared -fPIC
@@ -304,7 +304,8 @@ struct Oracle {
   Phys cod_gr, cod_gt, cod_gp, comp_gr, comp_gt, comp_gp;
   Phys vel_dur, vel_qv1, vel_dutr, vel_dupr, vel_qv2;  // anelastic (tra_qst2rtp_vel)
   // time
-  double tim_t = 0, tim_dt = 0, tim_dterr = 0, tim_corr_dt = 0, lasterr = 1e99;
+  double tim_t = 0, tim_dt = 0, tim_dterr = 0, tim_corr_dt = 0, tim_cfl_dt = 0, lasterr = 1e99;
+  bool tim_new_dt = false;
   int tim_it = 0, tim_step = 0, tim_pcn = -1;
   int nthreads = 1;
   std::string err;
@@ -1825,6 +1826,58 @@ void corrector(Oracle& o) {
   }
 }
 
+// non_maxtstep (nonlinear.F90:546-615): the CFL limit from u and B on the grid
+void non_maxtstep(Oracle& o) {
+  const int N = o.N, Th = o.Th, Ph = o.Ph;
+  const double E = o.cfg.E, Pm = o.cfg.Pm;
+  o.tim_cfl_dt = 1e99;
+  for (int n = 1; n <= N; ++n) {
+    double dr;
+    if (n == 1) dr = o.oc.R(2, 1) - o.oc.R(1, 1);
+    else if (n == N) dr = o.oc.R(N, 1) - o.oc.R(N - 1, 1);
+    else dr = std::min(o.oc.R(n, 1) - o.oc.R(n - 1, 1), o.oc.R(n + 1, 1) - o.oc.R(n, 1));
+    double d = (E + E / Pm) / (2.0 * dr);
+    d = d * d;
+    double mx = -1e300;
+    const size_t base = (size_t)Th * Ph * (n - 1);
+    for (size_t k = 0; k < (size_t)Th * Ph; ++k) {
+      double p = o.mag_r[base + k] * o.mag_r[base + k];
+      double v = p / std::sqrt(p * (E / Pm) + d) + std::fabs(o.vel_r[base + k]);
+      mx = std::max(mx, v);
+    }
+    if (mx != 0.0) o.tim_cfl_dt = std::min(o.tim_cfl_dt, dr / mx);
+    dr = o.oc.R(n, 1) / std::sqrt((double)(o.L * (o.L - 1)));
+    d = E / (2.0 * dr);
+    d = d * d;
+    mx = -1e300;
+    for (size_t k = 0; k < (size_t)Th * Ph; ++k) {
+      double p = o.mag_t[base + k] * o.mag_t[base + k] + o.mag_p[base + k] * o.mag_p[base + k];
+      double vt = o.vel_t[base + k], vp = o.vel_p[base + k];
+      double v = p / std::sqrt(p * E / Pm + d) + std::sqrt(vt * vt + vp * vp);
+      mx = std::max(mx, v);
+    }
+    if (mx != 0.0) o.tim_cfl_dt = std::min(o.tim_cfl_dt, dr / mx);
+  }
+  o.tim_cfl_dt = std::min(o.tim_cfl_dt, E / Pm);
+  o.tim_cfl_dt = std::min(o.tim_cfl_dt, std::sqrt(E));
+}
+// tim_new_tstep (timestep.F90:837-870)
+void tim_new_tstep(Oracle& o) {
+  double dt = o.tim_dt;
+  if (o.cfg.time_step_control == 1) {
+    if (o.tim_corr_dt > o.cfg.corr_upper) dt = 0.5 * dt;
+    if (o.tim_corr_dt < o.cfg.corr_lower) dt = 1.273974 * dt;
+    if (o.tim_step == 0) dt = std::min(dt / 1e3, 1e-8);
+  } else {
+    if (o.tim_corr_dt > 0.0) dt = std::min(o.tim_corr_dt, dt * 2.0 / o.cfg.courant);
+    if (o.tim_cfl_dt > 0.0) dt = std::min(o.tim_cfl_dt, dt);
+    if (o.tim_step == 0) dt = std::min(dt / 1e3, 1e-10);
+    dt = dt * o.cfg.courant;
+  }
+  o.tim_new_dt = (dt < o.tim_dt * 0.97 || dt > o.tim_dt * 1.03);
+  if (o.tim_new_dt) o.tim_dt = dt;
+}
+
 // tim_check_cgce (timestep.F90:744-830); returns 1 when the loop gave up.
 int check_cgce(Oracle& o) {
   int fail = 0;
@@ -2034,7 +2087,7 @@ Oracle* orc_create(const lsd_config* cfg, int* status) {
   o->L = cfg->L; o->M = cfg->M; o->Mp = cfg->Mp; o->N = cfg->N; o->KL = cfg->KL; o->Nic = cfg->Nic;
   *status = 0;
   if (o->L <= (o->M - 1) * o->Mp || (o->M > 1 && o->M % 2 == 1) || o->N < 2 * o->KL + 1 || o->Nic != 1 ||
-      cfg->timestep <= 0) {
+      cfg->timestep == 0) {
     *status = LSD_EARG;
     delete o;
     return nullptr;
@@ -2046,7 +2099,7 @@ Oracle* orc_create(const lsd_config* cfg, int* status) {
   o->Ph = o->Ma * 2;
   o->Hc = (o->M + 1) / 2;
   o->Hr = o->H / o->Hc;
-  o->tim_dt = cfg->timestep;
+  o->tim_dt = cfg->timestep < 0 ? -cfg->timestep : cfg->timestep;
   setup_layout(*o);
   if (setup_legendre(*o) || setup_mesh(*o)) { *status = LSD_ESINGULAR; delete o; return nullptr; }
   o->fft.init(o->Ph);
@@ -2161,6 +2214,13 @@ int orc_get_nonlinear(Oracle* o, int f, double* re, double* im) {
   return 0;
 }
 void orc_set_time(Oracle* o, double t) { o->tim_t = t; }
+// io_load_state's tim_dt (io.F90:426-429) with the matrices at that dt
+int orc_set_dt(Oracle* o, double dt) {
+  if (!(dt > 0)) return LSD_EARG;
+  o->tim_dt = dt;
+  return build_matrices(*o) ? LSD_ESINGULAR : 0;
+}
+void orc_dt_control(const Oracle* o, double* out) { out[0] = o->tim_dt; out[1] = o->tim_corr_dt; out[2] = o->tim_cfl_dt; }
 
 int orc_spec2phys(Oracle* o, const double* sre, const double* sim, double* p) {
   Spec s; s.init(o->N, o->H);
@@ -2244,6 +2304,11 @@ int orc_step(Oracle* o, int nsteps, lsd_stats* st) {
   while (done < nsteps) {
     evaluate(*o); ++evals;
     if (o->tim_it == 0) {
+      if (o->cfg.timestep < 0) {  // main.F90:126-134
+        non_maxtstep(*o);
+        tim_new_tstep(*o);
+        if (o->tim_new_dt && build_matrices(*o)) return LSD_ESINGULAR;
+      }
       predictor(*o);
       o->tim_it = 1;
     } else {

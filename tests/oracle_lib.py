@@ -73,6 +73,8 @@ def load():
         "orc_set_threads": (ctypes.c_int, [ctypes.c_int]),
         "orc_set_reference_state": (ctypes.c_int, [vp, _D]),
         "orc_dth": (ctypes.c_int, [vp, _D, _D, _D]),
+        "orc_set_dt": (ctypes.c_int, [vp, ctypes.c_double]),
+        "orc_dt_control": (None, [vp, _D]),
         "orc_qst2rtp_vel": (ctypes.c_int, [vp, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     }
     for name, (res, args) in sigs.items():
@@ -173,8 +175,16 @@ class Oracle:
         assert self.lib.orc_get_nonlinear(self.h, f, _dp(re), _dp(im)) == 0
         return re, im
 
-    def set_time(self, t):
+    def set_time(self, t, dt=None):
         self.lib.orc_set_time(self.h, t)
+        if dt is not None:
+            assert self.lib.orc_set_dt(self.h, dt) == 0
+
+    def dt_control(self):
+        """tim_dt, tim_corr_dt, tim_cfl_dt (io.F90:2346)."""
+        out = np.zeros(3)
+        self.lib.orc_dt_control(self.h, _dp(out))
+        return out
 
     # ---- transforms: spec as (N, H) C-order == Fortran (H, N); phys (N, Ph, Th)
     def spec2phys(self, sre, sim):
