@@ -352,7 +352,7 @@ __device__ __forceinline__ double2 row_unpack(const double2* row, int b, const F
 // qva = m/sin llsin1mP - cot llP_ and qvb = cot llsin1mP - m/sin llP_ (legendre.F90:97-100)
 // the Legendre sums collapse, per theta row and order m, to
 //   qv1_m = (cot u_th,m + i m/sin u_ph,m) / r,   qv2_m = (i m/sin u_th,m - cot u_ph,m) / r,
-// which are formed from the staged u_th, u_ph bins of the same CTA.
+// which are formed from the u_th, u_ph bins that the same CTA gathers.
 enum ProdSet { PS_BOUSS = 0, PS_BOUSS_COMP, PS_ANEL_MOM, PS_ANEL_SCAL, PS_ANEL_SCAL_COMP };
 template <int PS> struct PSet;
 template <> struct PSet<PS_BOUSS> { static constexpr int in = 15, deriv = 0, out = 7; };
@@ -370,6 +370,7 @@ struct ProdConst {
   const double* r;    // [7][N] powers of r
   const double* ref;  // [7][N] reference state (anelastic)
   unsigned long long* cflmax;  // variable dt: per-shell CFL maxima [N][2] (bits of doubles >= 0), or null
+  const int* bin2c;   // FFT bin -> m-counter (M entries)
   int L;
   int fin[PROD_MAXIN];  // input field slots of four_in
 };
@@ -464,9 +465,9 @@ __device__ __forceinline__ void prod_point(const double* v, double* o, const Pro
 
 // grid (2 HB, N): one half-row h = blockIdx.x (its southern and northern theta row) per
 // CTA, 256 threads, up to two CTAs per SM so that one's memory waits overlap the other's
-// work.  Every thread loads its share of all input blocks into registers at the start
-// (all loads in flight at once); the blocks then pass through a double-buffered bin-order
-// stage into the padded rows [NF][2][E (G+1)] (NF = inputs + derived rows).
+// work.  The inputs are gathered bin by bin (bin -> m-counter map, L1-cached) straight into
+// the packed half spectra of the padded rows [NF][2][E (G+1)] (NF = inputs + derived rows),
+// so the load phase has no barrier; barriers separate only the FFT passes and products.
 constexpr int PROD_THREADS = 256;
 
 template <int E, int G, int PS>
@@ -479,8 +480,7 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
   const int NM = pl.NM, M = pl.M, Th = pl.Th, Th2 = pl.Th2;
   if (h >= Th2) return;  // padding half-row of an odd Th2
   double2* rows = (double2*)psm;                 // [NF][2][RS]
-  double2* stage = rows + (size_t)NF * 2 * RS;   // [2 buffers][2 (E/O)][M]
-  const FFTTabs tabs = fft_tabs_init<E, G>((unsigned char*)(stage + (size_t)4 * M), pl);
+  const FFTTabs tabs = fft_tabs_init<E, G>((unsigned char*)(rows + (size_t)NF * 2 * RS), pl);
   const int BLK = NM * 4;                        // one field's (n, h/2) block
   const size_t fstride = (size_t)N * pl.HB * BLK;
   const size_t boff = ((size_t)n * pl.HB + hb) * BLK + jj;  // element (c, p) at boff + 2 (2c + p)
@@ -494,51 +494,62 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
     sh.rm1 = pc.r[(size_t)2 * N + n]; sh.rinv = sh.rm1; sh.rrr = pc.r[(size_t)4 * N + n];
     sh.Cmag = pc.Pm / (pc.E * sh.rho);
   }
-  // ---- all loads first: element tid of every field (the rest, for NM > 128, later)
-  double2 pre[NF_IN];
+  // ---- gather + pack, no barrier: item (f, k) loads the (E, O) pairs of bins k and P2-k
+  // (counters bin2c[.]) straight from this half-row's block, forms the southern (E + O)
+  // and northern (E - O) half spectra and writes both packed rows at position k.  Bins
+  // >= M are zero (dealiasing).  Batches of U items per thread keep their loads in flight.
+  constexpr int U = 4, NITEM = NF_IN * P2;
+  for (int it0 = tid; it0 < NITEM; it0 += U * PROD_THREADS) {
+    double2 e0[U], o0[U], e1[U], o1[U];
 #pragma unroll
-  for (int f = 0; f < NF_IN; ++f)
-    pre[f] = tid < NE ? four_in[(size_t)pc.fin[f] * fstride + boff + 2 * tid] : make_double2(0.0, 0.0);
-  // ---- per field: bin-order stage (double buffer), then the packed half spectra
-#pragma unroll
-  for (int f = 0; f < NF_IN; ++f) {
-    double2* sp = stage + (size_t)(f & 1) * 2 * M;  // [p][M]
-    for (int i = tid; i < NE; i += PROD_THREADS) {
-      const double2 val = i == tid ? pre[f] : four_in[(size_t)pc.fin[f] * fstride + boff + 2 * i];
-      sp[(i & 1) * M + tabs.thm[i >> 1]] = val;
+    for (int u = 0; u < U; ++u) {
+      const int it = it0 + u * PROD_THREADS;
+      e0[u] = o0[u] = e1[u] = o1[u] = make_double2(0.0, 0.0);
+      if (it < NITEM) {
+        const int f = it / P2, k = it - f * P2, km = k == 0 ? P2 : P2 - k;
+        const cplx* src = four_in + (size_t)pc.fin[f] * fstride + boff;
+        if (k < M) {
+          const int c = __ldg(pc.bin2c + k);
+          e0[u] = src[4 * c]; o0[u] = src[4 * c + 2];
+        }
+        if (km < M) {
+          const int c = __ldg(pc.bin2c + km);
+          e1[u] = src[4 * c]; o1[u] = src[4 * c + 2];
+        }
+      }
     }
-    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int it = it0 + u * PROD_THREADS;
+      if (it < NITEM) {
+        const int f = it / P2, k = it - f * P2;
+        rows[(size_t)(f * 2) * RS + ppos<G>(k)] = c2r_pack(k, add2(e0[u], o0[u]), add2(e1[u], o1[u]), pl);
+        rows[(size_t)(f * 2 + 1) * RS + ppos<G>(k)] = c2r_pack(k, sub2(e0[u], o0[u]), sub2(e1[u], o1[u]), pl);
+      }
+    }
+  }
+  if constexpr (NDER > 0) {  // the qv1, qv2 rows from the u_th (input 1), u_ph (input 2) bins
+    const cplx* sth = four_in + (size_t)pc.fin[1] * fstride + boff;
+    const cplx* sph = four_in + (size_t)pc.fin[2] * fstride + boff;
     for (int i = tid; i < 2 * P2; i += PROD_THREADS) {
       const int side = i / P2, k = i - side * P2;
-      const double2 yk = k < M ? (side ? sub2(sp[k], sp[M + k]) : add2(sp[k], sp[M + k])) : make_double2(0.0, 0.0);
-      const int km = k == 0 ? P2 : P2 - k;
-      const double2 ym = km < M ? (side ? sub2(sp[km], sp[M + km]) : add2(sp[km], sp[M + km])) : make_double2(0.0, 0.0);
-      rows[(size_t)(f * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, yk, ym, pl);
-    }
-    if constexpr (NDER > 0) {
-      if (f == 2) {  // u_th staged in buffer 1, u_ph in buffer 0: the qv1, qv2 rows
-        const double2* sth = stage + (size_t)2 * M;
-        const double2* sph = stage;
-        for (int i = tid; i < 2 * P2; i += PROD_THREADS) {
-          const int side = i / P2, k = i - side * P2;
-          const int j = row_theta(h, side, Th);
-          const double s1 = pc.sn1[j], cot = pc.gp[j] * s1;
-          auto bins = [&](int b, double2& q1, double2& q2) {
-            if (b >= M) { q1 = q2 = make_double2(0.0, 0.0); return; }
-            const double2 t = side ? sub2(sth[b], sth[M + b]) : add2(sth[b], sth[M + b]);
-            const double2 p = side ? sub2(sph[b], sph[M + b]) : add2(sph[b], sph[M + b]);
-            const double mk = (double)(b * pl.Mp) * s1;
-            q1 = make_double2(sh.rinv * (cot * t.x - mk * p.y), sh.rinv * (cot * t.y + mk * p.x));
-            q2 = make_double2(sh.rinv * (-mk * t.y - cot * p.x), sh.rinv * (mk * t.x - cot * p.y));
-          };
-          double2 q1k, q2k, q1m, q2m;
-          bins(k, q1k, q2k);
-          bins(k == 0 ? P2 : P2 - k, q1m, q2m);
-          rows[(size_t)(NF_IN * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, q1k, q1m, pl);
-          rows[(size_t)((NF_IN + 1) * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, q2k, q2m, pl);
-        }
-        __syncthreads();  // buffer 1 is restaged by field 3
-      }
+      const int j = row_theta(h, side, Th);
+      const double s1 = pc.sn1[j], cot = pc.gp[j] * s1;
+      auto bins = [&](int b, double2& q1, double2& q2) {
+        if (b >= M) { q1 = q2 = make_double2(0.0, 0.0); return; }
+        const int c = __ldg(pc.bin2c + b);
+        const double2 te = sth[4 * c], to = sth[4 * c + 2], pe = sph[4 * c], po = sph[4 * c + 2];
+        const double2 t = side ? sub2(te, to) : add2(te, to);
+        const double2 p = side ? sub2(pe, po) : add2(pe, po);
+        const double mk = (double)(b * pl.Mp) * s1;
+        q1 = make_double2(sh.rinv * (cot * t.x - mk * p.y), sh.rinv * (cot * t.y + mk * p.x));
+        q2 = make_double2(sh.rinv * (-mk * t.y - cot * p.x), sh.rinv * (mk * t.x - cot * p.y));
+      };
+      double2 q1k, q2k, q1m, q2m;
+      bins(k, q1k, q2k);
+      bins(k == 0 ? P2 : P2 - k, q1m, q2m);
+      rows[(size_t)(NF_IN * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, q1k, q1m, pl);
+      rows[(size_t)((NF_IN + 1) * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, q2k, q2m, pl);
     }
   }
   __syncthreads();
@@ -789,7 +800,7 @@ template <int PS>
 int launch_products_set(lsd_ctx* ctx, const ProdConst& pc, const cplx* four_in, cplx* four_out) {
   FFTPlanDev pl = make_plan(ctx);
   constexpr int NF = PSet<PS>::in + PSet<PS>::deriv;
-  const size_t smem = sizeof(double2) * ((size_t)NF * 2 * ctx->fftE * (ctx->fftG + 1) + (size_t)4 * ctx->M) +
+  const size_t smem = sizeof(double2) * ((size_t)NF * 2 * ctx->fftE * (ctx->fftG + 1)) +
                       fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
   if (smem > 224 * 1024) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
   dim3 grid(2 * ctx->HB, ctx->N);
@@ -851,7 +862,7 @@ size_t lsd_products_smem(const lsd_ctx* ctx) {
   const bool comp = ctx->cfg.comp_tstep != 0;
   int nf = comp ? 18 : 15;
   if (!ctx->cfg.boussinesq) nf = (comp ? 18 : 15) + 2;
-  return sizeof(double2) * ((size_t)nf * 2 * ctx->fftE * (ctx->fftG + 1) + (size_t)4 * ctx->M) +
+  return sizeof(double2) * ((size_t)nf * 2 * ctx->fftE * (ctx->fftG + 1)) +
          fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
 }
 
@@ -875,6 +886,7 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.r = ctx->d_r;
   pc.ref = ctx->d_ref;
   pc.L = ctx->L;
+  pc.bin2c = ctx->d_bin2c;
   pc.cflmax = c.timestep < 0 ? (unsigned long long*)ctx->d_cfl : nullptr;
   const bool comp = c.comp_tstep != 0;
   const size_t FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;

@@ -256,6 +256,7 @@ struct OzPrepArgs {
   const OzProb* probs; const int* kidx; const int* mstart; const int* mlen;
   const double* rinv;
   int8_t* A; int* erow;                  // erow [c][nrows]
+  int* err;
   const cplx* in0[OZ_MAXG]; const cplx* in1[OZ_MAXG];
 };
 
@@ -265,106 +266,141 @@ template <int TYPE> struct OzT {
   static constexpr int nin = (TYPE == OZ_VEC || TYPE == OZ_ST) ? 2 : 1;
 };
 
-// One CTA = (counter c, z-block of 128 rows); both parities.
+// One CTA = (counter c, z-block of 128 rows), both parities, in four quarters of 32 rows.
+// The input rows of a quarter (the counter's harmonic segment of a shell for the
+// synthesis, the (h, E/O) row of (c, n) for the analysis: contiguous in HBM) arrive by
+// bulk copies (cp.async.bulk, no multicast) into one of two shared-memory stages, the
+// next quarter's while this one is converted; every input value is fetched from HBM once,
+// although the parity problems, K segments and row components read it up to eight times.
+// Stage rows are padded to an odd number of 16-byte units, so that the shells a warp
+// reads fall in distinct banks.  Every mbarrier wait is bounded; on a timeout the CTA sets
+// the error flag, waits (bounded) for its copies in flight and returns.
+template <int TYPE> struct OzStage {
+  static constexpr int NIN = OzT<TYPE>::nin, PER = OzT<TYPE>::per, NSQ = 32 / PER;  // shells per quarter
+};
+template <int TYPE>
+__host__ __device__ __forceinline__ size_t oz_prep_smem(int srow) {
+  return sizeof(double2) * (size_t)2 * OzStage<TYPE>::NSQ * OzStage<TYPE>::NIN * srow;
+}
+
 template <int TYPE, int S>
-__global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
-  constexpr int PER = OzT<TYPE>::per, NIN = OzT<TYPE>::nin;
-  constexpr int NPAIR = 128 / PER;  // shells of the z-block
-  __shared__ int e_pair[NPAIR];
-  __shared__ int kx[2][512];  // harmonic lists of the two problems (synthesis)
+__global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
+  constexpr int PER = OzT<TYPE>::per, NIN = OzT<TYPE>::nin, NSQ = OzStage<TYPE>::NSQ;
+  extern __shared__ __align__(16) double2 stg[];  // [2 stages][slot][field][srow]
+  __shared__ __align__(8) uint64_t full[2];
+  __shared__ int e_slot[NSQ];
+  __shared__ int kx[2][512];  // harmonic lists of the two problems (synthesis), local indices
   const int c = blockIdx.x, zb = blockIdx.y;
-  const int R0 = zb * 128;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int kbeg = a.mstart[c], klen = a.mlen[c];
-  // ---- exponents: one warp per shell of the block, max over the counter's data
-  for (int pi = warp; pi < NPAIR; pi += 8) {
-    const int R = R0 + pi * PER;
-    double mx = 0.0;
-    if (R < a.nrows) {
+  const int rowlen = OzT<TYPE>::anal ? 2 * a.Th2 : klen;  // values per (shell, field)
+  const size_t stage_elems = (size_t)NSQ * NIN * srow;
+  if (tid == 0) {
+    umma::mbar_init(&full[0], 1);
+    umma::mbar_init(&full[1], 1);
+    umma::fence_mbar_init();
+  }
+  if (!OzT<TYPE>::anal)
+    for (int p = 0; p < 2; ++p) {
+      const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+      for (int i = tid; i < pr.K && i < 512; i += 256) kx[p][i] = a.kidx[pr.kofs + i] - kbeg;
+    }
+  __syncthreads();
+  // quarter q -> stage q & 1 (issued by thread 0)
+  auto issue = [&](int q) {
+    uint64_t* bar = &full[q & 1];
+    double2* dst = stg + (size_t)(q & 1) * stage_elems;
+    const int R0 = zb * 128 + q * 32;
+    uint32_t bytes = 0;
+    for (int sl = 0; sl < NSQ; ++sl)
+      if (R0 + sl * PER < a.nrows) bytes += NIN * rowlen * 16;
+    umma::mbar_expect_tx(bar, bytes);
+    for (int sl = 0; sl < NSQ; ++sl) {
+      const int R = R0 + sl * PER;
+      if (R >= a.nrows) break;
       const int g = R / a.rows_per_group, n = (R % a.rows_per_group) / PER;
-#pragma unroll
       for (int f = 0; f < NIN; ++f) {
         const cplx* src = f == 0 ? a.in0[g] : a.in1[g];
-        if (!OzT<TYPE>::anal) {
-          const double r1 = (TYPE == OZ_GRAD) ? a.rinv[n] : 1.0;
-          for (int k = lane; k < klen; k += 32) {
-            double2 v = src[(size_t)n * a.H + kbeg + k];
-            if (TYPE == OZ_GRAD) { v.x *= r1; v.y *= r1; }
-            mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
-          }
-        } else {
-          for (int i = lane; i < 2 * a.Th2; i += 32) {
-            const double2 y = src[four_off_a(n, c, 0, 0, a.N, a.Th2) + i];  // (h, E/O) pairs, contiguous
-            mx = fmax(mx, fmax(fabs(y.x), fabs(y.y)));
-          }
-        }
+        src += OzT<TYPE>::anal ? four_off_a(n, c, 0, 0, a.N, a.Th2) : (size_t)n * a.H + kbeg;
+        umma::bulk_g2s(dst + (size_t)(sl * NIN + f) * srow, src, (uint32_t)rowlen * 16, bar);
       }
     }
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) e_pair[pi] = oz_exponent(mx);
-  }
-  __syncthreads();
-  for (int r = tid; r < 128; r += 256)
-    if (R0 + r < a.nrows) a.erow[(size_t)c * a.nrows + R0 + r] = e_pair[r / PER];
-  // ---- digits of both parities' A tiles: thread = (row r, K half kh), 16 values per K step.
-  // |x| 2^(7S - e) is an integer below 2^(7S) <= 2^56, split into two 28-bit halves whose
-  // 7-bit groups are the digits; four values make one 32-bit word per slice (byte permutes),
-  // the signs are applied per byte (two's complement).
-  const int r = tid & 127, kh = tid >> 7;
-  const int R = R0 + r;
-  const bool live = R < a.nrows;
-  int g = 0, n = 0, comp = 0;
-  double sc = 0.0;
-  if (live) {
-    g = R / a.rows_per_group;
-    n = (R % a.rows_per_group) / PER;
-    comp = R % PER;
-    const int e = e_pair[r / PER];
-    sc = e > -1000 ? pow2i(7 * S - e) : 0.0;
-  }
-  const double r1 = (TYPE == OZ_GRAD && live) ? a.rinv[n] : 1.0;
-  const int toff = umma::tile_off(r, kh * 16);
-  for (int p = 0; p < 2; ++p) {
-    const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
-    if (!OzT<TYPE>::anal)
-      for (int i = tid; i < pr.K && i < 512; i += 256) kx[p][i] = a.kidx[pr.kofs + i];
-  }
-  __syncthreads();
-  for (int p = 0; p < 2; ++p) {
-    const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
-    if (pr.nchunk == 0) continue;
-    int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
-    for (int ks = 0; ks < pr.nks; ++ks) {
-      uint32_t wd[S][4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
+  };
+  if (tid == 0) { issue(0); issue(1); }
+  // thread = (row r of the quarter, K eighth kq): 4 values per K step -> one word per slice
+  const int r = tid & 31, kq = tid >> 5;
+  for (int q = 0; q < 4; ++q) {
+    const int R0 = zb * 128 + q * 32;
+    const double2* st = stg + (size_t)(q & 1) * stage_elems;
+    const bool got = umma::mbar_wait(&full[q & 1], (q >> 1) & 1, WAIT_ITERS);
+    if (__syncthreads_or(!got)) {  // give up: flag, let the copies in flight land, leave
+      if (tid == 0) {
+        atomicExch(a.err, 1);
+        for (int qq = q; qq < 4 && qq < q + 2; ++qq) umma::mbar_wait(&full[qq & 1], (qq >> 1) & 1, WAIT_ITERS);
+      }
+      __syncthreads();
+      return;
+    }
+    // ---- exponents: one warp per shell, max over the staged values of its fields
+    for (int sl = warp; sl < NSQ; sl += 8) {
+      const int R = R0 + sl * PER;
+      const double r1 = (TYPE == OZ_GRAD && R < a.nrows) ? a.rinv[(R % a.rows_per_group) / PER] : 1.0;
+      double mx = 0.0;
+      if (R < a.nrows)
+        for (int i = lane; i < NIN * rowlen; i += 32) {
+          const int f = i / rowlen, k = i - f * rowlen;
+          double2 v = st[(size_t)(sl * NIN + f) * srow + k];
+          if (TYPE == OZ_GRAD) { v.x *= r1; v.y *= r1; }
+          mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+        }
+      for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if (lane == 0) e_slot[sl] = oz_exponent(mx);
+    }
+    __syncthreads();
+    if (tid < 32 && R0 + tid < a.nrows) a.erow[(size_t)c * a.nrows + R0 + tid] = e_slot[tid / PER];
+    // ---- digits of both parities' A tiles.  |x| 2^(7S - e) is an integer below
+    // 2^(7S) <= 2^56, split into two 28-bit halves whose 7-bit groups are the digits; four
+    // values make one 32-bit word per slice (byte permutes), the signs applied per byte.
+    const int R = R0 + r;
+    const bool live = R < a.nrows;
+    const int sl = r / PER, comp = R % PER;
+    const double sc = live && e_slot[sl] > -1000 ? pow2i(7 * S - e_slot[sl]) : 0.0;
+    const double r1 = (TYPE == OZ_GRAD && live) ? a.rinv[(R % a.rows_per_group) / PER] : 1.0;
+    const double2* row0 = st + (size_t)(sl * NIN) * srow;
+    const double2* row1 = row0 + srow;  // second field (VEC: t, ST: phi)
+    const int rt = q * 32 + r;          // row inside the 128-row tile
+    for (int p = 0; p < 2; ++p) {
+      const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+      if (pr.nchunk == 0) continue;
+      int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
+      for (int ks = 0; ks < pr.nks; ++ks) {
         uint32_t hi[4], lo[4];
         uint32_t sg = 0u;
 #pragma unroll
         for (int u4 = 0; u4 < 4; ++u4) {
-          const int k = ks * 32 + kh * 16 + q * 4 + u4;
+          const int k = ks * 32 + kq * 4 + u4;
           double v = 0.0;
           if (live && k < pr.K) {
             const bool seg1 = k < pr.len1;
             if (TYPE == OZ_P) {
-              const double2 x = a.in0[g][(size_t)n * a.H + kx[p][k]];
+              const double2 x = row0[kx[p][k]];
               v = comp ? x.y : x.x;
             } else if (TYPE == OZ_VEC) {
               // theta: s llP_ (segment 1) + (t.im, -t.re) llsin1mP (segment 2);
               // phi:   t llP_ + (-s.im, s.re) llsin1mP        (transform.fftw3.F90:746-774)
               const bool use_t = seg1 ? comp >= 2 : comp < 2;
-              const double2 x = (use_t ? a.in1[g] : a.in0[g])[(size_t)n * a.H + kx[p][k]];
+              const double2 x = (use_t ? row1 : row0)[kx[p][k]];
               if (seg1) v = (comp & 1) ? x.y : x.x;
               else v = comp == 0 ? x.y : comp == 1 ? -x.x : comp == 2 ? -x.y : x.x;
             } else if (TYPE == OZ_GRAD) {
               // theta: (C/r) P_ ; phi: i (C/r) sin1mP              (transform.fftw3.F90:955-1000)
               if (seg1 == (comp < 2)) {
-                const double2 x = a.in0[g][(size_t)n * a.H + kx[p][k]];
+                const double2 x = row0[kx[p][k]];
                 const double2 cv = make_double2(x.x * r1, x.y * r1);
                 v = comp == 0 ? cv.x : comp == 1 ? cv.y : comp == 2 ? -cv.y : cv.x;
               }
             } else if (TYPE == OZ_Q) {
-              const double2 y = a.in0[g][four_off_a(n, c, p, k, a.N, a.Th2)];
+              const double2 y = row0[2 * k + p];
               v = comp ? y.y : y.x;
             } else {  // OZ_ST: segment 1 (gwllP_) on parity 1-p, segment 2 (gwllsin1mP) on parity p
               const int pp = seg1 ? 1 - p : p;
@@ -372,7 +408,7 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
               // s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re)
               // (transform.fftw3.F90:866-909)
               const bool use_ph = seg1 ? comp >= 2 : comp < 2;
-              const double2 y = (use_ph ? a.in1[g] : a.in0[g])[four_off_a(n, c, pp, j, a.N, a.Th2)];
+              const double2 y = (use_ph ? row1 : row0)[2 * j + pp];
               if (seg1) v = (comp & 1) ? y.y : y.x;
               else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
             }
@@ -382,6 +418,7 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
           lo[u4] = (uint32_t)X & 0x0FFFFFFFu;
           if (v < 0.0) sg |= 0xFFu << (8 * u4);
         }
+        const int toff = umma::tile_off(rt, kq * 4);
 #pragma unroll
         for (int s2 = 0; s2 < S; ++s2) {
           const int j = S - 1 - s2;  // digit s2 holds bits 7j .. 7j + 6
@@ -389,13 +426,12 @@ __global__ void __launch_bounds__(256) k_oz_prep(OzPrepArgs a) {
 #pragma unroll
           for (int u4 = 0; u4 < 4; ++u4) m[u4] = j >= 4 ? (hi[u4] >> (7 * (j - 4))) & 127u : (lo[u4] >> (7 * j)) & 127u;
           const uint32_t w = __byte_perm(__byte_perm(m[0], m[1], 0x0040), __byte_perm(m[2], m[3], 0x0040), 0x5410);
-          wd[s2][q] = __vsub4(w ^ sg, sg);
+          *(uint32_t*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) = __vsub4(w ^ sg, sg);
         }
       }
-#pragma unroll
-      for (int s2 = 0; s2 < S; ++s2)
-        *(uint4*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) = make_uint4(wd[s2][0], wd[s2][1], wd[s2][2], wd[s2][3]);
     }
+    __syncthreads();  // stage q & 1 fully read
+    if (tid == 0 && q + 2 < 4) issue(q + 2);
   }
 }
 
@@ -451,15 +487,27 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
     p = (t / nzb) & 1;
     c = t / (2 * nzb);
   };
+  // the problem of tile t (loaded one tile ahead, so the load's latency is hidden)
+  auto prob = [&](int t) {
+    OzProb pr{};
+    if (t < ntile) {
+      int c, p, zb;
+      tile(t, c, p, zb);
+      pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+    }
+    return pr;
+  };
 
   if (tid == 128) {
     // ---- producer: A (z-block, K step) and B (chunk, K step) tiles into the ring
     int it = 0;
     bool ok = true;
+    OzProb nxt = prob(blockIdx.x);
     for (int t = blockIdx.x; t < ntile && ok; t += gridDim.x) {
       int c, p, zb;
       tile(t, c, p, zb);
-      const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+      const OzProb pr = nxt;
+      nxt = prob(t + gridDim.x);
       const int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
       const int8_t* Bblk = a.B + pr.bofs;
       for (int q = 0; q < pr.nchunk * pr.nks; ++q, ++it) {
@@ -477,14 +525,16 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
     for (int j = (it > OZ_STAGES ? it - OZ_STAGES : 0); j < it; ++j)
       umma::mbar_wait(&full[j % OZ_STAGES], (j / OZ_STAGES) & 1, WAIT_ITERS);
   } else if (tid == 160) {
-    // ---- MMA issuer: S(S+1)/2 digit pairs per K step into S diagonals of 32 columns
-    const uint32_t idesc = umma::idesc_s8(128, OZ_NC);
+    // ---- MMA issuer: the S(S+1)/2 digit pairs of a K step into S diagonals of 32 columns,
+    // as S MMAs: A slice sa against B slices 0 .. S-1-sa at once (stacked in the stage, they
+    // are one K-major operand of N = 32 (S - sa) rows), accumulating into the tensor-memory
+    // columns 32 sa .. 32 S - 1, i.e. diagonals d = sa + s
     int it = 0, cc = 0;
     bool ok = true;
+    OzProb nxt = prob(blockIdx.x);
     for (int t = blockIdx.x; t < ntile && ok; t += gridDim.x) {
-      int c, p, zb;
-      tile(t, c, p, zb);
-      const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+      const OzProb pr = nxt;
+      nxt = prob(t + gridDim.x);
       for (int ch = 0; ch < pr.nchunk && ok; ++ch, ++cc) {
         if (cc > 0 && !oz_wait(&tfree, (cc - 1) & 1, a.err)) { ok = false; break; }
         umma::fence_after_sync();
@@ -494,12 +544,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
           umma::fence_after_sync();
           const uint32_t sa0 = umma::smem_u32(oz_smem + (size_t)st * stage_bytes);
           const uint32_t sb0 = sa0 + (uint32_t)S * 4096;
-          for (int d = 0; d < S; ++d)
-            for (int sa = 0; sa <= d; ++sa) {
-              const uint64_t ad = umma::desc_kmajor_noswz(sa0 + (uint32_t)sa * 4096, 128, 256);
-              const uint64_t bd = umma::desc_kmajor_noswz(sb0 + (uint32_t)(d - sa) * 1024, 128, 256);
-              umma::mma_s8(tmem + (uint32_t)(d * OZ_NC), ad, bd, idesc, (ks > 0 || sa > 0) ? 1 : 0);
-            }
+          const uint64_t bd = umma::desc_kmajor_noswz(sb0, 128, 256);
+          for (int sa = 0; sa < S; ++sa) {
+            const uint64_t ad = umma::desc_kmajor_noswz(sa0 + (uint32_t)sa * 4096, 128, 256);
+            umma::mma_s8(tmem + (uint32_t)(sa * OZ_NC), ad, bd, umma::idesc_s8(128, OZ_NC * (S - sa)),
+                         (ks > 0 || sa > 0) ? 1 : 0);
+          }
           umma::commit(&empty[st]);
         }
         if (ok) umma::commit(&accf);
@@ -510,10 +560,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
   } else if (tid < 128) {
     // ---- epilogue: row tid of each z-block
     int cc = 0;
+    OzProb nxt = prob(blockIdx.x);
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
       int c, p, zb;
       tile(t, c, p, zb);
-      const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+      const OzProb pr = nxt;
+      nxt = prob(t + gridDim.x);
       if (pr.nchunk == 0) continue;  // no harmonics of this parity: nothing to write
       if (tid < 64) {
         const int Rr = zb * 128 + 2 * tid;
@@ -609,6 +661,7 @@ struct OzState {
   int* d_erow = nullptr;  // row exponents [c][rows]
   int* d_err = nullptr;
   size_t smem = 0;
+  int srow[2] = {1, 1};  // pre-pass stage row length (odd, in complex): synthesis, analysis
 };
 
 namespace {
@@ -694,6 +747,14 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
     abytes_max = std::max(abytes_max, abytes);
   }
   o->smem = (size_t)OZ_STAGES * S * 5120 + sizeof(double) * 128 * OZ_STG;
+  {
+    int mx = 1;
+    for (int c = 0; c < NM; ++c) mx = std::max(mx, ctx->mlen[c]);
+    o->srow[0] = mx | 1;
+    o->srow[1] = (2 * Th2) | 1;
+    if (oz_prep_smem<OZ_ST>(o->srow[1]) > 200 * 1024 || oz_prep_smem<OZ_VEC>(o->srow[0]) > 200 * 1024)
+      return lsd_fail(ctx, LSD_EARG, "tensor-core path: pre-pass rows do not fit in shared memory");
+  }
   if (kidx.empty()) kidx.push_back(0);
   if (nhl.empty()) nhl.push_back(0);
   CUDA_TRY(cudaMalloc(&o->d_probs, sizeof(OzProb) * probs.size()));
@@ -742,6 +803,7 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   pa.N = ctx->N; pa.H = ctx->H; pa.NM = ctx->NM; pa.Th2 = ctx->Th2; pa.HB = ctx->HB; pa.S = o->S; pa.nrows = nrows;
   pa.rows_per_group = rpg; pa.probs = o->d_probs; pa.kidx = o->d_kidx; pa.mstart = ctx->d_mstart;
   pa.mlen = ctx->d_mlen; pa.rinv = ctx->d_rinv; pa.A = o->d_A; pa.erow = o->d_erow;
+  pa.err = o->d_err;
   OzGemmArgs ga;
   ga.N = ctx->N; ga.H = ctx->H; ga.NM = ctx->NM; ga.Th2 = ctx->Th2; ga.HB = ctx->HB; ga.S = o->S; ga.nrows = nrows;
   ga.rows_per_group = rpg; ga.probs = o->d_probs; ga.A = o->d_A; ga.B = o->d_B; ga.fexp = o->d_fexp;
@@ -753,14 +815,20 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
     ga.zero_m0_im[i] = on ? gs[i].zero_m0_im : 0;
   }
   const dim3 pg(ctx->NM, nzb);
+  const int srow = o->srow[OzT<TYPE>::anal ? 1 : 0];
+  const size_t psm = oz_prep_smem<TYPE>(srow);
+  auto go = [&](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm);
+    kern<<<pg, 256, psm, ctx->stream>>>(pa, srow);
+  };
   switch (o->S) {
-    case 2: k_oz_prep<TYPE, 2><<<pg, 256, 0, ctx->stream>>>(pa); break;
-    case 3: k_oz_prep<TYPE, 3><<<pg, 256, 0, ctx->stream>>>(pa); break;
-    case 4: k_oz_prep<TYPE, 4><<<pg, 256, 0, ctx->stream>>>(pa); break;
-    case 5: k_oz_prep<TYPE, 5><<<pg, 256, 0, ctx->stream>>>(pa); break;
-    case 6: k_oz_prep<TYPE, 6><<<pg, 256, 0, ctx->stream>>>(pa); break;
-    case 7: k_oz_prep<TYPE, 7><<<pg, 256, 0, ctx->stream>>>(pa); break;
-    default: k_oz_prep<TYPE, 8><<<pg, 256, 0, ctx->stream>>>(pa); break;
+    case 2: go(k_oz_prep<TYPE, 2>); break;
+    case 3: go(k_oz_prep<TYPE, 3>); break;
+    case 4: go(k_oz_prep<TYPE, 4>); break;
+    case 5: go(k_oz_prep<TYPE, 5>); break;
+    case 6: go(k_oz_prep<TYPE, 6>); break;
+    case 7: go(k_oz_prep<TYPE, 7>); break;
+    default: go(k_oz_prep<TYPE, 8>); break;
   }
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->dev);
