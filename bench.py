@@ -191,7 +191,7 @@ def energy_check(args, local_rank, nsteps):
 # DRAM traffic per launch of the dominant kernel from an ncu capture of this benchmark
 # (dram__bytes_read.sum + dram__bytes_write.sum); see profiles/ for the command.
 NCU_TRAFFIC = {
-    "fft_products": {"kernel": "k_products<12,16>", "bytes": 761.12e6 + 313.09e6,
+    "fft_products": {"kernel": "k_products<12,16>", "bytes": 760.93e6 + 331.13e6,
                      "profile": "profiles/k_products_dynamo128.md"},
 }
 

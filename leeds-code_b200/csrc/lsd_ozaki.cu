@@ -250,6 +250,14 @@ __global__ void k_oz_tab_anal(OzTabArgs a, int type) {
   }
 }
 
+// Four 7-bit digits (one per byte, each 0..127) with per-byte signs: the bytes of w whose
+// byte of sg is 0xFF are negated (two's complement).  For 0 <= b <= 127,
+// -b mod 256 = (0x80 - b) ^ 0x80, and 0x80808080 - w borrows across no byte.
+__device__ __forceinline__ uint32_t signed_digits(uint32_t w, uint32_t sg) {
+  const uint32_t neg = (0x80808080u - w) ^ 0x80808080u;
+  return (neg & sg) | (w & ~sg);
+}
+
 // ---- the slicing pre-pass ---------------------------------------------------------------
 struct OzPrepArgs {
   int N, H, NM, Th2, HB, S, nrows, rows_per_group;
@@ -426,7 +434,7 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
 #pragma unroll
           for (int u4 = 0; u4 < 4; ++u4) m[u4] = j >= 4 ? (hi[u4] >> (7 * (j - 4))) & 127u : (lo[u4] >> (7 * j)) & 127u;
           const uint32_t w = __byte_perm(__byte_perm(m[0], m[1], 0x0040), __byte_perm(m[2], m[3], 0x0040), 0x5410);
-          *(uint32_t*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) = __vsub4(w ^ sg, sg);
+          *(uint32_t*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) = signed_digits(w, sg);
         }
       }
     }
