@@ -89,6 +89,30 @@ extern "C" {
 #define LSD_E_BOTFLX  18   /* bottom heat flux (io.F90:1785-1794)                        */
 #define LSD_NENERGY   19
 
+/* scalars written by lsd_diagnostics (the other time series of io_write2files) */
+#define LSD_D_TIME       0   /* tim_t                                                      */
+#define LSD_D_VPART      1   /* vel_partition.dat (io.F90:1906-1914): Et, Ep, Etas, Epas,  */
+                             /*   Etes, Epes, Etesas, Epesas, sum l E(l), lpol (10 values) */
+#define LSD_D_MPART     11   /* mag_partition.dat (io.F90:2018-2020): Et .. Epesas (8)     */
+#define LSD_D_CMB       19   /* mag_cmb.dat (io.F90:2036-2145): EPol, ESym, El1, theta,    */
+                             /*   phi of the north magnetic pole, Epas, El12 (7)           */
+#define LSD_D_NUSC      26   /* codensity Nusselt (io.F90:2158-2243): Nu, T_ro, T_ri,      */
+                             /*   dC/dr(ri), dC/dr(ro), Nu_top, Nu_bot, Nu_flux (8)        */
+#define LSD_D_NUSX      34   /* the same for composition (8)                               */
+#define LSD_D_DYN       42   /* dyn_outputs (io.F90:2355-2399): Rm, Re, Pe, Pe_comp,       */
+                             /*   Rossby, M_ratio, Elsasser, Lehnert, fdip, fohm,          */
+                             /*   theta_dip, Nusselt, Sherwood (13)                        */
+#define LSD_D_DT        55   /* timestep.dat (io.F90:2341-2347): tim_dt, tim_corr_dt,      */
+                             /*   tim_cfl_dt (3)                                           */
+#define LSD_NDIAG       58
+/* spectra (io_save_spectrum / _anelastic / io_save_spectrum1, io.F90:2405-2624), doubles:
+ *   velocity: [l = 0..L-1][E, Epol, Etor], then [m = 0..M-1][E, Epol, Etor]
+ *   field:    the same;  codensity: [l][E], [m][E];  composition: the same;
+ * i.e. 8 (L + M) doubles.  Anelastic velocity: the density-weighted norms
+ * (var_coll_normlm_comp) of the compressible q, s, t.
+ * profiles (io_rad_profile / io_save_profile, io.F90:2632-2738), [11][N]: r; velocity
+ * E, Epol, Etor; field E, Epol, Etor; C, dC/dr (l = 0); Comp, dComp/dr. */
+
 /* ---- configuration: the compile-time `parameters` module as a runtime struct --------- */
 typedef struct lsd_config {
   /* resolution (parameters.F90_template:19-23,250) */
@@ -238,6 +262,13 @@ int lsd_energies(lsd_ctx* ctx, double* out);
  * calls race.  The first call on a device does the set-up (symbol lookup): make it before
  * any stream capture. */
 int lsd_energies_static(lsd_ctx* ctx, double* out);
+/* The other time series, spectra and profiles of io_write2files (io.F90:290-340):
+ * io_write_vel_energy / io_write_mag_energy partitions, io_write_cmb, io_write_nussel,
+ * io_write_dyn_outputs, io_write_timestep (scalars, LSD_NDIAG doubles, LSD_D_* order);
+ * io_save_spectrum / io_save_spectrum_anelastic / io_save_spectrum1 (spectra,
+ * 8 (L + M) doubles, or NULL); io_rad_profile / io_save_profile (profiles, 11 N doubles,
+ * or NULL).  Layouts above the configuration struct.  Synchronises the context's stream. */
+int lsd_diagnostics(lsd_ctx* ctx, double* scalars, double* spectra, double* profiles);
 
 /* ---- ensembles (independent runs at their own resolutions) ---------------------------
  * The reference runs one configuration per job; an ensemble (e.g. a parameter or

@@ -38,6 +38,40 @@ ENERGY_NAMES = [
 ]
 NENERGY = len(ENERGY_NAMES)
 
+# lsd_diagnostics scalars (LSD_D_* order of the header)
+DIAG_NAMES = (
+    ["time"]
+    + ["vel_" + k for k in ("Et", "Ep", "Etas", "Epas", "Etes", "Epes", "Etesas", "Epesas", "l_Eofl", "lpol")]
+    + ["mag_" + k for k in ("Et", "Ep", "Etas", "Epas", "Etes", "Epes", "Etesas", "Epesas")]
+    + ["cmb_" + k for k in ("EPol", "ESym", "El1", "theta", "phi", "Epas", "El12")]
+    + ["nus_" + k for k in ("Nu", "T_ro", "T_ri", "dCdr_ri", "dCdr_ro", "Nu_top", "Nu_bot", "Nu_flux")]
+    + ["nuscomp_" + k for k in ("Nu", "T_ro", "T_ri", "dCdr_ri", "dCdr_ro", "Nu_top", "Nu_bot", "Nu_flux")]
+    + ["Rm", "Re", "Pe", "Pe_comp", "Rossby", "M_ratio", "Elsasser", "Lehnert", "fdip", "fohm", "theta_dip",
+       "Nusselt", "Sherwood"]
+    + ["tim_dt", "tim_corr_dt", "tim_cfl_dt"]
+)
+NDIAG = len(DIAG_NAMES)
+PROFILE_NAMES = ["r", "vel_E", "vel_Epol", "vel_Etor", "mag_E", "mag_Epol", "mag_Etor",
+                 "temp_C", "temp_dCdr", "comp_C", "comp_dCdr"]
+
+
+def spectra_size(L, M):
+    """doubles of the lsd_diagnostics spectra buffer"""
+    return 8 * (L + M)
+
+
+def split_spectra(buf, L, M):
+    """lsd_diagnostics spectra -> {name: array}: vel_l / vel_m / mag_l / mag_m are
+    (L or M, 3) arrays of E, Epol, Etor; cod_l / cod_m / comp_l / comp_m are E."""
+    out, o = {}, 0
+    for f in ("vel", "mag"):
+        out[f + "_l"] = buf[o:o + 3 * L].reshape(L, 3); o += 3 * L
+        out[f + "_m"] = buf[o:o + 3 * M].reshape(M, 3); o += 3 * M
+    for f in ("cod", "comp"):
+        out[f + "_l"] = buf[o:o + L]; o += L
+        out[f + "_m"] = buf[o:o + M]; o += M
+    return out
+
 
 class LsdConfig(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (

@@ -1048,6 +1048,12 @@ int lsd_energies(lsd_ctx* ctx, double* out) {
   return lsd_energy_device(ctx, out);
 }
 
+int lsd_diagnostics(lsd_ctx* ctx, double* scalars, double* spectra, double* profiles) {
+  if (!ctx || !scalars) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  return lsd_diagnostics_device(ctx, scalars, spectra, profiles);
+}
+
 int lsd_energies_static(lsd_ctx* ctx, double* out) {
   if (!ctx || !out) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));

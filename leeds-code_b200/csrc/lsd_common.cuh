@@ -181,6 +181,7 @@ int lsd_pred(lsd_ctx* ctx);            // predictor solves (device)
 int lsd_corr(lsd_ctx* ctx);            // corrector solves + dterr (device)
 int lsd_energy_device(lsd_ctx* ctx, double* out);
 int lsd_energy_static(lsd_ctx* ctx, double* out);
+int lsd_diagnostics_device(lsd_ctx* ctx, double* scalars, double* spectra, double* profiles);
 int lsd_coll_to_state(lsd_ctx* ctx, const double* re, const double* im, cplx* out);
 int lsd_state_to_coll(lsd_ctx* ctx, const cplx* in, double* re, double* im);
 int lsd_factor_batch(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info);

@@ -1013,6 +1013,333 @@ int lsd_energy_static(lsd_ctx* ctx, double* out) {
   return energy_finish(ctx, Fh, wts, cod0, bpolN, r, dr1, ref, out);
 }
 
+// ---- the other diagnostics of io_write2files ------------------------------------------
+namespace {
+constexpr int HN_MAX = 12;  // arrays per k_hnorm launch
+struct HNormArgs {
+  const cplx* a[HN_MAX];
+  const double* wt[HN_MAX];
+};
+
+// Radially integrated norm of every harmonic (the per-harmonic sums of var_coll_normlm,
+// variables.F90:1267-1364): out[k][nh] = sum_n w(l,m) |a_k(n,nh)|^2 wt_k(n), n ascending.
+// One thread per harmonic; a warp reads 32 consecutive harmonics of row n of the [n][nh]
+// layout, so every load is coalesced and the sum order is the reference's.
+__global__ void k_hnorm(int N, int H, const int* __restrict__ hl, const int* __restrict__ hm, HNormArgs p,
+                        double* __restrict__ out) {
+  const int nh = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (nh >= H) return;
+  const int l = hl[nh];
+  double w = 4.0 * 3.1415926535897931 / (double)(2 * l + 1);
+  if (hm[nh] != 0) w = 4.0 * w;
+  const cplx* __restrict__ a = p.a[k];
+  const double* __restrict__ wt = p.wt[k];
+  double e = 0.0;
+  for (int n = 0; n < N; ++n) {
+    const double2 v = a[(size_t)n * H + nh];
+    e = e + w * (v.x * v.x + v.y * v.y) * wt[n];
+  }
+  out[(size_t)k * H + nh] = e;
+}
+
+// Per-shell sums over the harmonics (io_rad_profile, io.F90:2679-2738) for group g of
+// three arrays q, s, t: out[g][0][n] = sum_nh w (|q|^2 + |s|^2), out[g][1][n] = sum_nh w |t|^2.
+// One block per (shell, group); strided partial sums, then a fixed-order reduction (the
+// result does not depend on scheduling).
+constexpr int SS_THREADS = 256;
+__global__ void __launch_bounds__(SS_THREADS) k_shell_sums(int N, int H, const int* __restrict__ hl,
+                                                           const int* __restrict__ hm, HNormArgs p,
+                                                           double* __restrict__ out) {
+  const int n = blockIdx.x, g = blockIdx.y;
+  const cplx* __restrict__ q = p.a[3 * g] + (size_t)n * H;
+  const cplx* __restrict__ s = p.a[3 * g + 1] + (size_t)n * H;
+  const cplx* __restrict__ t = p.a[3 * g + 2] + (size_t)n * H;
+  double ep = 0.0, et = 0.0;
+  for (int nh = threadIdx.x; nh < H; nh += SS_THREADS) {
+    double w = 4.0 * 3.1415926535897931 / (double)(2 * hl[nh] + 1);
+    if (hm[nh] != 0) w = 4.0 * w;
+    const double2 a = q[nh], b = s[nh], c = t[nh];
+    ep = ep + (w * (a.x * a.x + a.y * a.y) + w * (b.x * b.x + b.y * b.y));
+    et = et + w * (c.x * c.x + c.y * c.y);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ep += __shfl_xor_sync(0xffffffffu, ep, o);
+    et += __shfl_xor_sync(0xffffffffu, et, o);
+  }
+  __shared__ double red[2][SS_THREADS / 32];
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { red[0][warp] = ep; red[1][warp] = et; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < SS_THREADS / 32; ++i) { a = a + red[0][i]; b = b + red[1][i]; }
+    out[((size_t)g * 2 + 0) * N + n] = a;
+    out[((size_t)g * 2 + 1) * N + n] = b;
+  }
+}
+
+// row n (1-based) of dr(1) applied to a real column x (var_coll_meshmult of one column)
+double dr1_row(const double* dr1, int N, int KL, const double* x, int n) {
+  const int ldm = 2 * KL + 1;
+  double acc = 0.0;
+  for (int j = std::max(1, n - KL); j <= std::min(n + KL, N); ++j)
+    acc = acc + dr1[(size_t)(KL + n - j) + (size_t)ldm * (j - 1)] * x[j - 1];
+  return acc;
+}
+
+// io_write_nussel (io.F90:2158-2243) from the l = 0 column of a buoyancy field
+void nusselt(const lsd_config& c, const double* dr1, int N, int KL, const double* col0, double* out) {
+  const double T_ri = col0[0], T_ro = col0[N - 1];
+  const double dCdr_ri = dr1_row(dr1, N, KL, col0, 1), dCdr_ro = dr1_row(dr1, N, KL, col0, N);
+  const double ri = c.rratio / (1 - c.rratio), ro = 1 / (1 - c.rratio);
+  const double A = (ri * ro) / (ri - ro);
+  double nu_top = 0, nu_bot = 0, nu_flux = 0, nu = 0;
+  if (c.cod_bc == 1) {
+    nu_bot = dCdr_ri / (A / (ri * ri));
+    nu_top = dCdr_ro / (A / (ro * ro));
+    nu = nu_top;
+  } else if (c.cod_bc == 4) {
+    const double DT_cond = 1 / ri - 1 / ro, DT = T_ri - T_ro;
+    nu_flux = DT_cond / DT;
+    nu = nu_flux;
+  }
+  const double v[8] = {nu, T_ro, T_ri, dCdr_ri, dCdr_ro, nu_top, nu_bot, nu_flux};
+  for (int k = 0; k < 8; ++k) out[k] = v[k];
+}
+}  // namespace
+
+// The time series, spectra and profiles that io_write2files writes besides the energies
+// (io.F90:290-340).  Device: the q, s, t fields of velocity and field, their
+// per-harmonic radial integrals (k_hnorm) and per-shell harmonic sums (k_shell_sums);
+// host: the sums over l and m, the partitions and the scalars in the reference's order.
+int lsd_diagnostics_device(lsd_ctx* ctx, double* sc, double* spec, double* prof) {
+  const int N = ctx->N, H = ctx->H, KL = ctx->KL, L = ctx->L, M = ctx->M, Mp = ctx->Mp;
+  const size_t F = (size_t)N * H;
+  const lsd_config& c = ctx->cfg;
+  const bool bq = c.boussinesq != 0, comp = c.comp_tstep != 0;
+  cplx* sp = ctx->d_spec;
+  cplx* st = ctx->d_state;
+  cudaStream_t s = ctx->stream;
+  // energies and the category norms of q, s, t (slots 0..11 of the spectral scratch)
+  std::vector<double> Fh((size_t)48 * N), wts(5 * N), cod0(N), bpolN(3 * 2), r(N * 7),
+      dr1((size_t)(2 * KL + 1) * N), ref(7 * N), en(LSD_NENERGY);
+  int rc = energy_partials(ctx, (const cplx**)(ctx->d_red + 64), ctx->d_red + 128, Fh.data(), wts.data(),
+                           cod0.data(), bpolN.data(), r.data(), dr1.data(), ref.data());
+  if (rc) return rc;
+  if ((rc = energy_finish(ctx, Fh.data(), wts.data(), cod0.data(), bpolN.data(), r.data(), dr1.data(), ref.data(),
+                          en.data())))
+    return rc;
+  // the field through the compressible var_coll_TorPol2qst (io_write_cmb, io_rad_profile):
+  // slots 12..14 when anelastic; the same arrays as slots 6..8 when xi = 0
+  const cplx* mc = sp + 6 * F;
+  if (!bq) {
+    SpecArgs sa = spec_args(ctx);
+    dim3 g(ceil_div(H, 128), N);
+    k_qst<<<g, 128, 0, s>>>(sa, ctx->d_compr1dr, st + LSD_MAG_TOR * F, st + LSD_MAG_POL * F, sp + 12 * F,
+                            sp + 13 * F, sp + 14 * F);
+    ctx->launches++;
+    mc = sp + 12 * F;
+  }
+  // output room: the first free slot of the spectral scratch
+  const int slot = bq ? 12 : 15;
+  const int K = bq ? 8 : 11;
+  if (slot + 1 > ctx->nspec || (size_t)(K * H + 4 * N) > 2 * F)
+    return lsd_fail(ctx, LSD_EARG, "lsd_diagnostics: spectral scratch too small");
+  double* dout = (double*)(sp + (size_t)slot * F);
+  HNormArgs p{};
+  const double* w2 = ctx->d_intr2dr;
+  for (int k = 0; k < 3; ++k) {
+    p.a[k] = sp + k * F;            p.wt[k] = w2;   // velocity q, s, t (compressible)
+    p.a[3 + k] = sp + (6 + k) * F;  p.wt[3 + k] = w2;  // field q, s, t (var_coll_TorPol2qst_mag)
+    if (!bq) { p.a[8 + k] = sp + k * F; p.wt[8 + k] = ctx->d_wts; }  // velocity, intr2dr_comp
+  }
+  p.a[6] = st + LSD_COD_C * F;  p.wt[6] = w2;
+  p.a[7] = st + LSD_COMP_C * F; p.wt[7] = w2;
+  k_hnorm<<<dim3(ceil_div(H, 128), K), 128, 0, s>>>(N, H, ctx->d_l, ctx->d_m, p, dout);
+  HNormArgs ps{};
+  for (int k = 0; k < 3; ++k) { ps.a[k] = sp + k * F; ps.a[3 + k] = mc + k * F; }
+  k_shell_sums<<<dim3(N, 2), SS_THREADS, 0, s>>>(N, H, ctx->d_l, ctx->d_m, ps, dout + (size_t)K * H);
+  ctx->launches += 2;
+  std::vector<double> hn((size_t)K * H + 4 * N), comp0(N);
+  std::vector<cplx> cmb((size_t)2 * H), bpol1(2);
+  CUDA_TRY(cudaMemcpyAsync(hn.data(), dout, sizeof(double) * hn.size(), cudaMemcpyDeviceToHost, s));
+  for (int k = 0; k < 2; ++k)
+    CUDA_TRY(cudaMemcpyAsync(cmb.data() + (size_t)k * H, mc + k * F + (size_t)(N - 1) * H, sizeof(cplx) * H,
+                             cudaMemcpyDeviceToHost, s));
+  const cplx* polN = st + LSD_MAG_POL * F + (size_t)(N - 1) * H;
+  CUDA_TRY(cudaMemcpyAsync(&bpol1[0], polN + std::max(ctx->nh_l1m0, 0), sizeof(cplx), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(&bpol1[1], polN + std::max(ctx->nh_l1m1, 0), sizeof(cplx), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpy2DAsync(comp0.data(), sizeof(double), st + LSD_COMP_C * F, sizeof(cplx) * H, sizeof(double), N,
+                             cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("lsd_diagnostics: ") + cudaGetErrorString(e));
+
+  const double PI = 3.1415926535897931;
+  const double KE = 0.5, ME = bq ? c.Pm / c.E : 0.5 * c.Pm / c.E;
+  for (int i = 0; i < LSD_NDIAG; ++i) sc[i] = 0.0;
+  sc[LSD_D_TIME] = ctx->t;
+  // per-l / per-m sums of one k_hnorm array (var_coll_normlm), nh ascending
+  auto normlm = [&](int k, std::vector<double>& El, std::vector<double>& Em) {
+    El.assign(L, 0.0); Em.assign(M, 0.0);
+    for (int nh = 0; nh < H; ++nh) {
+      const double v = hn[(size_t)k * H + nh];
+      El[ctx->hl[nh]] = El[ctx->hl[nh]] + v;
+      Em[ctx->hm[nh] / Mp] = Em[ctx->hm[nh] / Mp] + v;
+    }
+  };
+  auto normw = [&](int k, const double* w, double& Eo, double& Ee, double& E1, double& E0) {
+    double v[4];
+    for (int q = 0; q < 4; ++q) {
+      double acc = 0.0;
+      for (int n = 0; n < N; ++n) acc = acc + Fh[((size_t)k * 4 + q) * N + n] * w[n];
+      v[q] = acc;
+    }
+    Eo = v[0]; Ee = v[1]; E1 = v[2]; E0 = v[3];
+  };
+  // ---- vel_partition (io.F90:1800-1921)
+  {
+    const double* wv = bq ? wts.data() : wts.data() + N;
+    double Eo, Ee, E1, E0, Ep, Epes, Epesas, Epas, Et, Etes, Etesas, Etas;
+    normw(0, wv, Eo, Ee, E1, E0); Ep = Eo + Ee; Epes = Ee; Epesas = E1; Epas = E0;
+    normw(1, wv, Eo, Ee, E1, E0); Ep = Ep + Eo + Ee; Epes = Epes + Ee; Epesas = Epesas + E1; Epas = Epas + E0;
+    normw(2, wv, Eo, Ee, E1, E0); Et = Eo + Ee; Etes = Eo; Etesas = E0 - E1; Etas = E0;
+    std::vector<double> ETl, ETm, EQl, EQm, ESl, ESm;
+    normlm(2, ETl, ETm); normlm(0, EQl, EQm); normlm(1, ESl, ESm);
+    double l_Eofl = 0.0;
+    for (int i = 1; i < L; ++i) l_Eofl = l_Eofl + i * KE * (ETl[i] + EQl[i] + ESl[i]);
+    int lpol = 0;
+    double best = -1.0;
+    for (int i = 0; i < L; ++i)
+      if (EQl[i] + ESl[i] > best) { best = EQl[i] + ESl[i]; lpol = i + 1; }  // maxloc, 1-based
+    const double v[10] = {KE * Et, KE * Ep, KE * Etas, KE * Epas, KE * Etes, KE * Epes, KE * Etesas, KE * Epesas,
+                          l_Eofl, (double)lpol};
+    for (int k = 0; k < 10; ++k) sc[LSD_D_VPART + k] = v[k];
+  }
+  // ---- mag_partition (io.F90:1959-2020)
+  {
+    const double* wm = wts.data();
+    double Eo, Ee, E1, E0, Ep, Epes, Epesas, Epas, Et, Etes, Etesas, Etas;
+    normw(6, wm, Eo, Ee, E1, E0); Ep = Eo + Ee; Epes = Ee; Epesas = E1; Epas = E0;
+    normw(7, wm, Eo, Ee, E1, E0); Ep = Ep + Eo + Ee; Epes = Epes + Ee; Epesas = Epesas + E1; Epas = Epas + E0;
+    normw(8, wm, Eo, Ee, E1, E0); Et = Eo + Ee; Etes = Eo; Etesas = E0 - E1; Etas = E0;
+    const double v[8] = {ME * Et, ME * Ep, ME * Etas, ME * Epas, ME * Etes, ME * Epes, ME * Etesas, ME * Epesas};
+    for (int k = 0; k < 8; ++k) sc[LSD_D_MPART + k] = v[k];
+  }
+  // ---- mag_cmb (io.F90:2036-2145): var_coll_norm_orig of q, s zeroed below the outer shell
+  double fdip, thdip;
+  {
+    double EPol = 0, ESym = 0, El1 = 0, Epas = 0, El12 = 0;
+    const double wN = wts[N - 1];
+    for (int k = 0; k < 2; ++k) {
+      double Fod = 0, Fev = 0, Fl1 = 0, Fm0 = 0, Fl12 = 0;
+      for (int nh = 0; nh < H; ++nh) {
+        const int l = ctx->hl[nh], m_ = ctx->hm[nh];
+        double w = 4.0 * PI / (double)(2 * l + 1);
+        if (m_ != 0) w = 4.0 * w;
+        const cplx a = cmb[(size_t)k * H + nh];
+        const double f = w * (a.x * a.x + a.y * a.y);
+        if (m_ == 0) Fm0 = Fm0 + f;
+        if (l > 0 && l <= 12) Fl12 = Fl12 + f;
+        if (l == 1) Fl1 = Fl1 + f;
+        if (((l - m_) % 2 + 2) % 2 == 1) Fod = Fod + f; else Fev = Fev + f;
+      }
+      EPol = EPol + Fod * wN + Fev * wN;
+      ESym = ESym + Fev * wN;
+      El1 = El1 + Fl1 * wN;
+      Epas = Epas + Fm0 * wN;
+      El12 = El12 + Fl12 * wN;
+    }
+    const double fac = r[(size_t)5 * N + N - 1] / wN;  // r(N,2) / intr2dr(N)
+    EPol = ME * EPol * fac; Epas = ME * Epas * fac; ESym = ME * ESym * fac; El1 = ME * El1 * fac;
+    El12 = ME * El12 * fac;
+    const double g10 = ctx->nh_l1m0 >= 0 ? bpol1[0].x : 0.0;
+    double th, ph;
+    if (Mp == 1 && M > 1 && ctx->nh_l1m1 >= 0) {
+      const double g11 = -2.0 * bpol1[1].x, h11 = 2.0 * bpol1[1].y;
+      th = std::sqrt(g10 * g10 + g11 * g11 + h11 * h11);
+      if (th != 0.0) th = std::acos(g10 / std::max(th, std::fabs(g10)));
+      if (std::fabs(g11) < 1e-99) {
+        ph = h11 >= 0.0 ? 0.5 * PI : 1.5 * PI;
+      } else {
+        ph = std::atan(h11 / g11);
+        if (g11 < 0.0) ph = ph + PI;
+        if (ph < 0.0) ph = ph + 2.0 * PI;
+      }
+    } else {
+      th = g10 >= 0.0 ? 0.0 : PI;
+      ph = 0.0;
+    }
+    fdip = std::sqrt(El1 / El12);
+    thdip = th;
+    const double v[7] = {EPol, ESym, El1, th, ph, Epas, El12};
+    for (int k = 0; k < 7; ++k) sc[LSD_D_CMB + k] = v[k];
+  }
+  // ---- Nusselt numbers
+  nusselt(c, dr1.data(), N, KL, cod0.data(), sc + LSD_D_NUSC);
+  if (comp) nusselt(c, dr1.data(), N, KL, comp0.data(), sc + LSD_D_NUSX);
+  // ---- dyn_outputs (io.F90:2355-2399; io_vol io.F90:76)
+  {
+    const double ri = c.rratio / (1 - c.rratio), ro = 1 / (1 - c.rratio);
+    const double vol = (4.0 / 3.0 * PI) * (ro * ro * ro - ri * ri * ri);
+    const double Kin = en[LSD_E_KE], Mag = en[LSD_E_ME], Visc = en[LSD_E_KE_DIS], Ohm = en[LSD_E_ME_DIS];
+    const double Rm = std::sqrt((2 * Kin) / vol), Re = Rm / c.Pm;
+    const double El = (c.E * Mag) / (c.Pm * vol);
+    const double Le = std::sqrt((2 * c.E * c.E * Mag) / (c.Pm * c.Pm * vol));
+    const double v[13] = {Rm, Re, Re * c.Pr, Re * c.Sc, Re * c.E, Mag / Kin, El, Le, fdip, Ohm / (Ohm + Visc),
+                          thdip, sc[LSD_D_NUSC], comp ? sc[LSD_D_NUSX] : 0.0};
+    for (int k = 0; k < 13; ++k) sc[LSD_D_DYN + k] = v[k];
+  }
+  sc[LSD_D_DT + 0] = ctx->dt;
+  sc[LSD_D_DT + 1] = ctx->corr_dt;
+  sc[LSD_D_DT + 2] = ctx->cfl_dt;
+  // ---- spectra (io_save_spectrum / _anelastic / io_save_spectrum1)
+  if (spec) {
+    double* q = spec;
+    auto vec_spec = [&](int k0, double Efac) {
+      std::vector<double> ETl, ETm, EQl, EQm, ESl, ESm;
+      normlm(k0 + 2, ETl, ETm); normlm(k0, EQl, EQm); normlm(k0 + 1, ESl, ESm);
+      for (int l = 0; l < L; ++l) {
+        *q++ = Efac * (ETl[l] + EQl[l] + ESl[l]); *q++ = Efac * (EQl[l] + ESl[l]); *q++ = Efac * ETl[l];
+      }
+      for (int m = 0; m < M; ++m) {
+        *q++ = Efac * (ETm[m] + EQm[m] + ESm[m]); *q++ = Efac * (EQm[m] + ESm[m]); *q++ = Efac * ETm[m];
+      }
+    };
+    vec_spec(bq ? 0 : 8, KE);
+    vec_spec(3, ME);
+    for (int k = 6; k < 8; ++k) {
+      std::vector<double> El, Em;
+      normlm(k, El, Em);
+      for (int l = 0; l < L; ++l) *q++ = El[l];
+      for (int m = 0; m < M; ++m) *q++ = Em[m];
+    }
+  }
+  // ---- profiles (io_rad_profile, io_save_profile)
+  if (prof) {
+    const double* ssum = hn.data() + (size_t)K * H;
+    for (int n = 0; n < N; ++n) prof[n] = r[(size_t)4 * N + n];
+    for (int g = 0; g < 2; ++g) {
+      const double Efac = g == 0 ? KE : ME;
+      double* out = prof + (size_t)(1 + 3 * g) * N;
+      for (int n = 0; n < N; ++n) {
+        out[N + n] = Efac * ssum[((size_t)g * 2 + 0) * N + n];
+        out[2 * N + n] = Efac * ssum[((size_t)g * 2 + 1) * N + n];
+        out[n] = out[2 * N + n] + out[N + n];
+      }
+    }
+    for (int k = 0; k < 2; ++k) {
+      const double* col = k == 0 ? cod0.data() : comp0.data();
+      for (int n = 0; n < N; ++n) {
+        prof[(size_t)(7 + 2 * k) * N + n] = col[n];
+        prof[(size_t)(8 + 2 * k) * N + n] = dr1_row(dr1.data(), N, KL, col, n + 1);
+      }
+    }
+  }
+  return LSD_OK;
+}
+
 // ---- boundary layout: coll Re/Im (N, H) column-major <-> device [n][nh] complex ---------
 namespace {
 constexpr int TT = 32;  // transpose tile

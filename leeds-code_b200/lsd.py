@@ -79,6 +79,7 @@ def load_library(path=None):
         "lsd_step": [_V, ctypes.c_int, ctypes.POINTER(capi.LsdStats)],
         "lsd_energies": [_V, _D],
         "lsd_energies_static": [_V, _D],
+        "lsd_diagnostics": [_V, _D, _D, _D],
         "lsd_banded_factor_device": [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V, _V, _V],
         "lsd_banded_solve_device": [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V, _V, ctypes.c_int, _V, _V],
         "lsd_profile_phases": [_V, _D, _I],
@@ -297,6 +298,16 @@ class Context:
         e = np.zeros(capi.NENERGY)
         self._ok(self.lib.lsd_energies(self.h, _dp(e)))
         return dict(zip(capi.ENERGY_NAMES, e))
+
+    def diagnostics(self):
+        """lsd_diagnostics: (scalars {name: value}, spectra {name: array}, profiles {name: array})."""
+        L, M, N = (self.sizes[k] for k in ("L", "M", "N"))
+        sc = np.zeros(capi.NDIAG)
+        sp = np.zeros(capi.spectra_size(L, M))
+        pr = np.zeros((len(capi.PROFILE_NAMES), N))
+        self._ok(self.lib.lsd_diagnostics(self.h, _dp(sc), _dp(sp), _dp(pr)))
+        return (dict(zip(capi.DIAG_NAMES, sc)), capi.split_spectra(sp, L, M),
+                dict(zip(capi.PROFILE_NAMES, pr)))
 
     def energies_static(self):
         """lsd_energies_static: the same diagnostics with a static device scratch (no allocation)."""

@@ -2041,6 +2041,230 @@ void energies(Oracle& o, double* out) {
   }
 }
 
+// ========================================================================================
+// The other diagnostics of io_write2files (io.F90:1739-2738)
+// ========================================================================================
+// var_coll_normlm / _normlm_comp (variables.F90:1267-1364): per-l and per-m energies
+void normlm(const Oracle& o, const Coll& a, const std::vector<double>& wts, std::vector<double>& El,
+            std::vector<double>& Em) {
+  const int N = o.N;
+  El.assign(o.L, 0.0); Em.assign(o.M, 0.0);
+  std::vector<double> f(N);
+  for (int nh = 0; nh < o.H; ++nh) {
+    int l = o.hl[nh], m = o.hm[nh] / o.Mp;
+    double w = 4.0 * d_PI / (double)(2 * l + 1);
+    if (m != 0) w = 4.0 * w;
+    double e = 0.0;
+    for (int n = 0; n < N; ++n) {
+      size_t i = n + (size_t)N * nh;
+      f[n] = w * (a.re[i] * a.re[i] + a.im[i] * a.im[i]);
+      e = e + f[n] * wts[n];
+    }
+    El[l] = El[l] + e;
+    Em[m] = Em[m] + e;
+  }
+}
+// meshmult of dr(1) at row n (1-based) of column nh (Re part)
+double dr1_row(const Oracle& o, const Coll& a, int nh, int n) {
+  const int N = o.N, KL = o.KL;
+  double acc = 0.0;
+  for (int j = std::max(1, n - KL); j <= std::min(n + KL, N); ++j)
+    acc = acc + o.oc.dr[1].at(KL + 1 + n - j, j) * a.re[(j - 1) + (size_t)N * nh];
+  return acc;
+}
+// io_write_nussel (io.F90:2158-2243)
+void nusselt(const Oracle& o, const Coll& C, double* out) {
+  const int N = o.N;
+  const double T_ri = C.re[0], T_ro = C.re[N - 1];
+  const double dCdr_ri = dr1_row(o, C, 0, 1), dCdr_ro = dr1_row(o, C, 0, N);
+  const double ri = o.cfg.rratio / (1 - o.cfg.rratio), ro = 1 / (1 - o.cfg.rratio);
+  const double A = (ri * ro) / (ri - ro);
+  double nu_top = 0, nu_bot = 0, nu_flux = 0, nu = 0;
+  if (o.cfg.cod_bc == 1) {
+    nu_bot = dCdr_ri / (A / (ri * ri));
+    nu_top = dCdr_ro / (A / (ro * ro));
+    nu = nu_top;
+  } else if (o.cfg.cod_bc == 4) {
+    const double DT_cond = 1 / ri - 1 / ro, DT = T_ri - T_ro;
+    nu_flux = DT_cond / DT;
+    nu = nu_flux;
+  }
+  const double v[8] = {nu, T_ro, T_ri, dCdr_ri, dCdr_ro, nu_top, nu_bot, nu_flux};
+  for (int k = 0; k < 8; ++k) out[k] = v[k];
+}
+
+void diagnostics(Oracle& o, double* sc, double* spec, double* prof) {
+  const bool bq = o.cfg.boussinesq != 0;
+  const int N = o.N, L = o.L, M = o.M;
+  const double KE = 0.5;
+  double ME = 0.5 * o.cfg.Pm / o.cfg.E;
+  if (bq) ME = o.cfg.Pm / o.cfg.E;
+  for (int i = 0; i < LSD_NDIAG; ++i) sc[i] = 0.0;
+  sc[LSD_D_TIME] = o.tim_t;
+  double en[LSD_NENERGY];
+  energies(o, en);
+  const std::vector<double>& w2 = o.oc.intr2dr;
+  const std::vector<double>& wv = bq ? o.oc.intr2dr : o.oc.intr2dr_comp;
+  // ---- velocity: compressible q, s, t (io_write_vel_energy, io_rad_profile)
+  Coll q, s, t, qm, sm, tm;
+  torpol2qst(o, o.vTor, o.vPol, q, s, t, true);
+  torpol2qst(o, o.vTor, o.vPol, qm, sm, tm, false);
+  {
+    double Eo, Ee, E1, E0, Ep, Epes, Epesas, Epas, Et, Etes, Etesas, Etas;
+    coll_norm_w(o, q, wv, Eo, Ee, E1, E0); Ep = Eo + Ee; Epes = Ee; Epesas = E1; Epas = E0;
+    coll_norm_w(o, s, wv, Eo, Ee, E1, E0); Ep = Ep + Eo + Ee; Epes = Epes + Ee; Epesas = Epesas + E1; Epas = Epas + E0;
+    coll_norm_w(o, t, wv, Eo, Ee, E1, E0); Et = Eo + Ee; Etes = Eo; Etesas = E0 - E1; Etas = E0;
+    std::vector<double> ETl, ETm, EQl, EQm, ESl, ESm;
+    normlm(o, t, w2, ETl, ETm); normlm(o, q, w2, EQl, EQm); normlm(o, s, w2, ESl, ESm);
+    double l_Eofl = 0.0;
+    for (int i = 1; i < L; ++i) l_Eofl = l_Eofl + i * KE * (ETl[i] + EQl[i] + ESl[i]);
+    int lpol = 0;
+    double best = -1.0;
+    for (int i = 0; i < L; ++i) if (EQl[i] + ESl[i] > best) { best = EQl[i] + ESl[i]; lpol = i + 1; }
+    const double v[10] = {KE * Et, KE * Ep, KE * Etas, KE * Epas, KE * Etes, KE * Epes, KE * Etesas, KE * Epesas,
+                          l_Eofl, (double)lpol};
+    for (int k = 0; k < 10; ++k) sc[LSD_D_VPART + k] = v[k];
+  }
+  // ---- field: q, s, t of var_coll_TorPol2qst_mag (io_write_mag_energy)
+  Coll bq_, bs_, bt_, bcq, bcs, bct;
+  torpol2qst(o, o.bTor, o.bPol, bq_, bs_, bt_, false);
+  torpol2qst(o, o.bTor, o.bPol, bcq, bcs, bct, true);  // io_rad_profile, io_write_cmb
+  {
+    double Eo, Ee, E1, E0, Ep, Epes, Epesas, Epas, Et, Etes, Etesas, Etas;
+    coll_norm(o, bq_, Eo, Ee, E1, E0); Ep = Eo + Ee; Epes = Ee; Epesas = E1; Epas = E0;
+    coll_norm(o, bs_, Eo, Ee, E1, E0); Ep = Ep + Eo + Ee; Epes = Epes + Ee; Epesas = Epesas + E1; Epas = Epas + E0;
+    coll_norm(o, bt_, Eo, Ee, E1, E0); Et = Eo + Ee; Etes = Eo; Etesas = E0 - E1; Etas = E0;
+    const double v[8] = {ME * Et, ME * Ep, ME * Etas, ME * Epas, ME * Etes, ME * Epes, ME * Etesas, ME * Epesas};
+    for (int k = 0; k < 8; ++k) sc[LSD_D_MPART + k] = v[k];
+  }
+  // ---- CMB (io_write_cmb): the norms of q, s on the outer shell only
+  double fdip = 0.0, thdip = 0.0;
+  {
+    double EPol = 0, ESym = 0, El1 = 0, Epas = 0, El12 = 0;
+    for (const Coll* a : {&bcq, &bcs}) {
+      double Fod = 0, Fev = 0, Fl1 = 0, Fm0 = 0, Fl12 = 0;
+      for (int nh = 0; nh < o.H; ++nh) {
+        int l = o.hl[nh], m_ = o.hm[nh];
+        double w = 4.0 * d_PI / (double)(2 * l + 1);
+        if (m_ != 0) w = 4.0 * w;
+        size_t i = (N - 1) + (size_t)N * nh;
+        double f = w * (a->re[i] * a->re[i] + a->im[i] * a->im[i]);
+        if (m_ == 0) Fm0 = Fm0 + f;
+        if (l > 0 && l <= 12) Fl12 = Fl12 + f;
+        if (l == 1) Fl1 = Fl1 + f;
+        if (((l - m_) % 2 + 2) % 2 == 1) Fod = Fod + f; else Fev = Fev + f;
+      }
+      const double wN = w2[N - 1];
+      EPol = EPol + Fod * wN + Fev * wN;
+      ESym = ESym + Fev * wN;
+      El1 = El1 + Fl1 * wN;
+      Epas = Epas + Fm0 * wN;
+      El12 = El12 + Fl12 * wN;
+    }
+    const double fac = o.oc.R(N, 2) / w2[N - 1];
+    EPol = ME * EPol * fac; Epas = ME * Epas * fac; ESym = ME * ESym * fac; El1 = ME * El1 * fac; El12 = ME * El12 * fac;
+    int nh10 = 0, nh11 = -1;
+    for (int nh = 0; nh < o.H; ++nh) {
+      if (o.hl[nh] == 1 && o.hm[nh] == 0) nh10 = nh;
+      if (o.hl[nh] == 1 && o.hm[nh] == 1) nh11 = nh;
+    }
+    const double g10 = o.bPol.re[(N - 1) + (size_t)N * nh10];
+    double th, ph;
+    if (o.Mp == 1 && o.M > 1 && nh11 >= 0) {
+      const double g11 = -2.0 * o.bPol.re[(N - 1) + (size_t)N * nh11];
+      const double h11 = 2.0 * o.bPol.im[(N - 1) + (size_t)N * nh11];
+      th = std::sqrt(g10 * g10 + g11 * g11 + h11 * h11);
+      if (th != 0.0) th = std::acos(g10 / std::max(th, std::fabs(g10)));
+      if (std::fabs(g11) < 1e-99) ph = h11 >= 0.0 ? 0.5 * d_PI : 1.5 * d_PI;
+      else {
+        ph = std::atan(h11 / g11);
+        if (g11 < 0.0) ph = ph + d_PI;
+        if (ph < 0.0) ph = ph + 2.0 * d_PI;
+      }
+    } else {
+      th = g10 >= 0.0 ? 0.0 : d_PI;
+      ph = 0.0;
+    }
+    fdip = std::sqrt(El1 / El12);
+    thdip = th;
+    const double v[7] = {EPol, ESym, El1, th, ph, Epas, El12};
+    for (int k = 0; k < 7; ++k) sc[LSD_D_CMB + k] = v[k];
+  }
+  // ---- Nusselt numbers (codensity, composition)
+  nusselt(o, o.codC, sc + LSD_D_NUSC);
+  if (o.cfg.comp_tstep) nusselt(o, o.compC, sc + LSD_D_NUSX);
+  // ---- io_write_dyn_outputs
+  {
+    const double ri = o.cfg.rratio / (1 - o.cfg.rratio), ro = 1 / (1 - o.cfg.rratio);
+    const double vol = (4.0 / 3.0 * d_PI) * (ro * ro * ro - ri * ri * ri);
+    const double Kin = en[LSD_E_KE], Mag = en[LSD_E_ME], Visc = en[LSD_E_KE_DIS], Ohm = en[LSD_E_ME_DIS];
+    const double Rm = std::sqrt((2 * Kin) / vol), Re = Rm / o.cfg.Pm;
+    const double El = (o.cfg.E * Mag) / (o.cfg.Pm * vol);
+    const double Le = std::sqrt((2 * o.cfg.E * o.cfg.E * Mag) / (o.cfg.Pm * o.cfg.Pm * vol));
+    const double v[13] = {Rm, Re, Re * o.cfg.Pr, Re * o.cfg.Sc, Re * o.cfg.E, Mag / Kin, El, Le, fdip,
+                          Ohm / (Ohm + Visc), thdip, sc[LSD_D_NUSC], o.cfg.comp_tstep ? sc[LSD_D_NUSX] : 0.0};
+    for (int k = 0; k < 13; ++k) sc[LSD_D_DYN + k] = v[k];
+  }
+  sc[LSD_D_DT + 0] = o.tim_dt; sc[LSD_D_DT + 1] = o.tim_corr_dt; sc[LSD_D_DT + 2] = o.tim_cfl_dt;
+  // ---- spectra
+  if (spec) {
+    double* p = spec;
+    auto vec_spec = [&](const Coll& a, const Coll& b, const Coll& c, const std::vector<double>& wt, double Efac) {
+      std::vector<double> ETl, ETm, EQl, EQm, ESl, ESm;
+      normlm(o, c, wt, ETl, ETm); normlm(o, a, wt, EQl, EQm); normlm(o, b, wt, ESl, ESm);
+      for (int l = 0; l < L; ++l) {
+        *p++ = Efac * (ETl[l] + EQl[l] + ESl[l]); *p++ = Efac * (EQl[l] + ESl[l]); *p++ = Efac * ETl[l];
+      }
+      for (int m = 0; m < M; ++m) {
+        *p++ = Efac * (ETm[m] + EQm[m] + ESm[m]); *p++ = Efac * (EQm[m] + ESm[m]); *p++ = Efac * ETm[m];
+      }
+    };
+    if (bq) vec_spec(qm, sm, tm, w2, KE);
+    else vec_spec(q, s, t, o.oc.intr2dr_comp, KE);  // io_save_spectrum_anelastic
+    vec_spec(bq_, bs_, bt_, w2, ME);
+    for (const Coll* a : {&o.codC, &o.compC}) {
+      std::vector<double> El, Em;
+      normlm(o, *a, w2, El, Em);
+      for (int l = 0; l < L; ++l) *p++ = El[l];
+      for (int m = 0; m < M; ++m) *p++ = Em[m];
+    }
+  }
+  // ---- profiles
+  if (prof) {
+    for (int n = 0; n < N; ++n) prof[n] = o.oc.R(n + 1, 1);
+    auto rad = [&](const Coll& a, const Coll& b, const Coll& c, double Efac, double* out) {
+      std::vector<double> Ep(N, 0.0), Et(N, 0.0);
+      for (int nh = 0; nh < o.H; ++nh) {
+        int l = o.hl[nh], m_ = o.hm[nh];
+        double w = 4.0 * d_PI / (double)(2 * l + 1);
+        if (m_ != 0) w = 4.0 * w;
+        for (int n = 0; n < N; ++n) {
+          size_t i = n + (size_t)N * nh;
+          double eq = w * (a.re[i] * a.re[i] + a.im[i] * a.im[i]);
+          double es = w * (b.re[i] * b.re[i] + b.im[i] * b.im[i]);
+          double et = w * (c.re[i] * c.re[i] + c.im[i] * c.im[i]);
+          Ep[n] = Ep[n] + eq + es;
+          Et[n] = Et[n] + et;
+        }
+      }
+      for (int n = 0; n < N; ++n) {
+        out[N + n] = Efac * Ep[n];
+        out[2 * N + n] = Efac * Et[n];
+        out[n] = out[2 * N + n] + out[N + n];
+      }
+    };
+    rad(q, s, t, KE, prof + N);
+    rad(bcq, bcs, bct, ME, prof + 4 * N);
+    for (int k = 0; k < 2; ++k) {
+      const Coll& C = k == 0 ? o.codC : o.compC;
+      for (int n = 0; n < N; ++n) {
+        prof[(7 + 2 * k) * N + n] = C.re[n];
+        prof[(8 + 2 * k) * N + n] = dr1_row(o, C, 0, n + 1);
+      }
+    }
+  }
+}
+
 Coll* field_ptr(Oracle& o, int f) {
   switch (f) {
     case LSD_VEL_TOR: return &o.vTor;
@@ -2329,5 +2553,9 @@ int orc_step(Oracle* o, int nsteps, lsd_stats* st) {
   return 0;
 }
 int orc_energies(Oracle* o, double* out) { energies(*o, out); return 0; }
+int orc_diagnostics(Oracle* o, double* scalars, double* spectra, double* profiles) {
+  diagnostics(*o, scalars, spectra, profiles);
+  return 0;
+}
 
 }  // extern "C"

@@ -70,6 +70,7 @@ def load():
         "orc_corrector": (ctypes.c_int, [vp, _D]),
         "orc_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(capi.LsdStats)]),
         "orc_energies": (ctypes.c_int, [vp, _D]),
+        "orc_diagnostics": (ctypes.c_int, [vp, _D, _D, _D]),
         "orc_set_threads": (ctypes.c_int, [ctypes.c_int]),
         "orc_set_reference_state": (ctypes.c_int, [vp, _D]),
         "orc_dth": (ctypes.c_int, [vp, _D, _D, _D]),
@@ -259,6 +260,16 @@ class Oracle:
         e = np.zeros(capi.NENERGY)
         self.lib.orc_energies(self.h, _dp(e))
         return dict(zip(capi.ENERGY_NAMES, e))
+
+    def diagnostics(self):
+        """orc_diagnostics, unpacked like Context.diagnostics."""
+        L, M, N = (self.sz[k] for k in ("L", "M", "N"))
+        sc = np.zeros(capi.NDIAG)
+        sp = np.zeros(capi.spectra_size(L, M))
+        pr = np.zeros((len(capi.PROFILE_NAMES), N))
+        self.lib.orc_diagnostics(self.h, _dp(sc), _dp(sp), _dp(pr))
+        return (dict(zip(capi.DIAG_NAMES, sc)), capi.split_spectra(sp, L, M),
+                dict(zip(capi.PROFILE_NAMES, pr)))
 
 
 def dgbtrf(ab, kl):
