@@ -44,6 +44,10 @@ extern "C" {
 #define LSD_MAG_POL   4   /* mag_Pol                    */
 #define LSD_COMP_C    5   /* comp_C   (composition.F90) */
 #define LSD_NFIELD    6
+/* the conducting inner core's field (Nic > 1), coll layout (Nic, H): lsd_set_coll /
+ * lsd_get_coll only (magnetic.F90:14-21, io.F90:436-447) */
+#define LSD_MAG_IC_TOR 6  /* mag_icTor */
+#define LSD_MAG_IC_POL 7  /* mag_icPol */
 
 /* nonlinear terms (outputs of nonlinear.F90), readable with lsd_get_nonlinear */
 #define LSD_N_VEL_TOR 0   /* vel_NTor  nonlinear.F90:188 */
@@ -104,7 +108,12 @@ extern "C" {
                              /*   theta_dip, Nusselt, Sherwood (13)                        */
 #define LSD_D_DT        55   /* timestep.dat (io.F90:2341-2347): tim_dt, tim_corr_dt,      */
                              /*   tim_cfl_dt (3)                                           */
-#define LSD_NDIAG       58
+#define LSD_D_ROT       58   /* rot_torque.dat (io.F90:2249-2266): rot_omega, viscous and   */
+                             /*   magnetic torque on the inner core (3)                    */
+#define LSD_D_MIC       61   /* mag_ic.dat (io.F90:1933-2024 on mag_icTor/icPol): E, Et,   */
+                             /*   Esym, El1, ETm0, EDis, Dip, Quad, Eaxtot (9; Nic > 1)    */
+#define LSD_D_MICPART   70   /* its mag_partition.dat line: Et .. Epesas (8; Nic > 1)      */
+#define LSD_NDIAG       78
 /* spectra (io_save_spectrum / _anelastic / io_save_spectrum1, io.F90:2405-2624), doubles:
  *   velocity: [l = 0..L-1][E, Epol, Etor], then [m = 0..M-1][E, Epol, Etor]
  *   field:    the same;  codensity: [l][E], [m][E];  composition: the same;
@@ -129,7 +138,10 @@ typedef struct lsd_config {
   double implicit, timestep, dterr, courant, corr_upper, corr_lower;
   /* sources and fluxes (parameters.F90_template:134-171) */
   double source, source_comp, qi, qo, qi_comp, qo_comp;
-  int reserved[8];
+  /* inner-core rotation (parameters.F90_template:100-102, rotation.F90) */
+  int rot_tstep;            /* b_rot_tstep: step rot_omega with the torques           */
+  int rot_force_0;          /* b_rot_force_0: hold rot_omega at zero                  */
+  int reserved[6];
 } lsd_config;
 
 /* derived sizes (parameters.F90_template:251-262; parallel.h_template:54-62) */
@@ -198,6 +210,11 @@ int lsd_get_time(const lsd_ctx* ctx, double* t, double* dt, int* step);
  * operators rebuilt on a change (main.F90:126-134).  out[3] = tim_dt, tim_corr_dt,
  * tim_cfl_dt (io_write_timestep, io.F90:2343-2346). */
 int lsd_get_dt_control(const lsd_ctx* ctx, double* out);
+/* Inner-core rotation rate rot_omega (the state file's 'omega', io.F90:432) and, read
+ * back, out[3] = rot_omega, rot_velTorq, rot_magTorq of the last evaluation
+ * (non_rotation, nonlinear.F90:479-538; rotation.F90). */
+int lsd_set_rotation(lsd_ctx* ctx, double omega);
+int lsd_get_rotation(const lsd_ctx* ctx, double* out);
 
 /* ---- transforms on host buffers (unit parity with transform.fftw3.F90) --------------
  * Each works on all N shells of the context. */

@@ -21,6 +21,7 @@ STATUS_NAMES = {
 }
 
 VEL_TOR, VEL_POL, COD_C, MAG_TOR, MAG_POL, COMP_C = range(6)
+MAG_IC_TOR, MAG_IC_POL = 6, 7  # the conducting inner core's field, (H, Nic) arrays
 FIELD_NAMES = ["vel_Tor", "vel_Pol", "cod_C", "mag_Tor", "mag_Pol", "comp_C"]
 N_VEL_TOR, N_VEL_POL, N_COD, N_MAG_TOR, N_MAG_POL, N_COMP = range(6)
 
@@ -49,6 +50,9 @@ DIAG_NAMES = (
     + ["Rm", "Re", "Pe", "Pe_comp", "Rossby", "M_ratio", "Elsasser", "Lehnert", "fdip", "fohm", "theta_dip",
        "Nusselt", "Sherwood"]
     + ["tim_dt", "tim_corr_dt", "tim_cfl_dt"]
+    + ["rot_omega", "rot_velTorq", "rot_magTorq"]
+    + ["ic_" + k for k in ("E", "Et", "Esym", "El1", "ETm0", "EDis", "Dip", "Quad", "Eaxtot")]
+    + ["icpart_" + k for k in ("Et", "Ep", "Etas", "Epas", "Etes", "Epes", "Etesas", "Epesas")]
 )
 NDIAG = len(DIAG_NAMES)
 PROFILE_NAMES = ["r", "vel_E", "vel_Epol", "vel_Etor", "mag_E", "mag_Epol", "mag_Etor",
@@ -83,7 +87,7 @@ class LsdConfig(ctypes.Structure):
             "rratio", "alpha", "Ra", "Ra_comp", "Pr", "Sc", "Pm", "E", "Hyp",
             "implicit", "timestep", "dterr", "courant", "corr_upper", "corr_lower",
             "source", "source_comp", "qi", "qo", "qi_comp", "qo_comp")] + \
-        [("reserved", ctypes.c_int * 8)]
+        [("rot_tstep", ctypes.c_int), ("rot_force_0", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
 class LsdSizes(ctypes.Structure):

@@ -116,6 +116,42 @@ def config_anelastic(L=64, **kw):
     return capi.template_config(**base)
 
 
+def config_inner_core(L=32, **kw):
+    """Christensen case 2 parameters (conducting, rotating inner core; E = 1e-3,
+    Ra = 7.15e4, Pr = 1, Pm = 5, rratio 0.35, no-slip walls, fixed T; the reference's
+    tests/parameters-case2.F90) at L = M, N = L + 1, Nic = L / 2 + 1, KL = 3, fixed
+    dt = 1e-5, implicit 0.5."""
+    base = dict(L=L, M=L, Mp=1, N=L + 1, Nic=L // 2 + 1, KL=3, rratio=0.35, E=1e-3, Ra=7.15e4, Pr=1.0,
+                Pm=5.0, vel_bc=1, cod_bc=1, timestep=1e-5, implicit=0.5, time_step_control=2, rot_tstep=1)
+    base.update(kw)
+    return capi.template_config(**base)
+
+
+def inner_core_grid(Nic, rratio):
+    """mes_ic%r(:,1) (meshs.F90:165-169): ri cos(pi (Nic - n) / (2 Nic - 1)), n = 1..Nic."""
+    ri = rratio / (1.0 - rratio)
+    N_ = 2 * Nic
+    n = np.arange(Nic + 1, N_ + 1)
+    return ri * np.cos(np.pi * (N_ - n) / float(N_ - 1))
+
+
+def ic_extend(re, im, r_oc, dr1_first, r_ic):
+    """io_ic_extend (io.F90:1438-1477): continue an outer-core field (H, N) into the inner
+    core as a r^3 + b r^2, matching its value and dr(1) derivative at r_i.  dr1_first: the
+    weights of dr(1) at the first point on points 1..KL+1."""
+    ri = r_oc[0]
+    out = []
+    for x in (re, im):
+        f = x[:, 0]
+        f1 = np.zeros_like(f)
+        for j, w in enumerate(dr1_first):
+            f1 = f1 + w * x[:, j]
+        a = (f1 * ri - 2.0 * f) / ri ** 3
+        b = (f - a * ri ** 3) / ri ** 2
+        out.append(a[:, None] * r_ic[None, :] ** 3 + b[:, None] * r_ic[None, :] ** 2)
+    return out[0], out[1]
+
+
 def config_dynamo128(**kw):
     """Full Boussinesq dynamo step at lmax = mmax = 127 (L = M = 128; Th = 192, Ph = 384),
     N = 129, parameters of config_parity, dt = 2e-6."""

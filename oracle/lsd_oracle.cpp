@@ -22,8 +22,9 @@
 //     restated from the reference LAPACK algorithms.  tests/ pin these against scipy's
 //     LAPACK (scipy.linalg.lapack.dgbtrf/dgbtrs).
 // Scope: Boussinesq or anelastic MHD + codensity (+ composition) with an insulating
-// inner core (i_Nic = 1), fixed dt (d_timestep > 0) or the CFL / corrector-controlled
-// dt (d_timestep < 0), no SHTns, no inhomogeneous BC files.  The anelastic reference state (io.F90:559-608, the seven columns of
+// inner core (i_Nic = 1), or Boussinesq with a conducting inner core (i_Nic > 1, no-slip
+// inner wall) and its rotation (b_rot_tstep), fixed dt (d_timestep > 0) or the CFL /
+// corrector-controlled dt (d_timestep < 0), no SHTns, no inhomogeneous BC files.  The anelastic reference state (io.F90:559-608, the seven columns of
 // planet_model.txt.in) is handed over by orc_set_reference_state.
 //
 // Build: g++ -O3 -march=native -fopenmp -ffp-contract=off -shared -fPIC
@@ -293,6 +294,13 @@ struct Oracle {
   std::vector<LUBand> XTor, XPol, XGre, XC, XComp, mXTor, mXPol;
   std::vector<Band> YTor, YPol, YC, YComp, mYTor, mYPol;
   std::vector<double> Gre, invG;  // Gre(N,2,L) ; invG(2,2,L)
+  // conducting inner core (Nic > 1): coupled field operators of size Nic + N - 1
+  // (iclumesh), the inner core's Y bands, its field [Nic][H], nonlinear and saved terms
+  std::vector<Band> icYTor, icYPol;
+  Coll icTor, icPol, icNTor, icNPol, sv_icNTor, sv_icNPol;
+  // inner-core rotation (rotation.F90; main.F90:92-94): rate, moment of inertia, the
+  // torques of the last evaluation and the ones saved by rot_predictor / rot_corrector
+  double rot_omega = 0, rot_inertia = 0, rot_velTorq = 0, rot_magTorq = 0, sv_velTorq = 0, sv_magTorq = 0;
   // state
   Coll vTor, vPol, codC, compC, bTor, bPol, bicTor, bicPol;
   // last nonlinear terms
@@ -676,6 +684,50 @@ void tim_iclumesh_X(const Oracle& o, const RDom& D, double c1, double c2, int l,
     A.at(2 * o.KL + 1, n) = A.at(2 * o.KL + 1, n) + c1_ + c2_ * ll1 * D.R(n, -2);
   lumesh_zero_bc_rows(A);
 }
+// tim_iclumesh_Tor_X / _Pol_X with a conducting inner core (Ni > 1), Boussinesq
+// (timestep.F90:218-344), and the rows of mag_bc_Tor / mag_bc_Pol (magnetic.F90:137-282):
+// unknowns 1..Ni on the inner-core mesh, Ni..Ni+No-1 on the outer-core mesh (point Ni,
+// the inner-core boundary, shared); row 1 regularity at the innermost point, row Ni the
+// continuity of dr across the boundary, row Ni+No-1 the insulating exterior.
+void tim_iclumesh_X_cic(const Oracle& o, double c1, double c2, int l, bool tor, LUBand& A) {
+  const RDom& I = o.ic;
+  const RDom& D = o.oc;
+  const int KL = o.KL, Ni = I.N, No = D.N, N_ = Ni + No - 1;
+  double c1_ = c1 / o.tim_dt, c2_ = c2 * o.cfg.implicit;
+  if (o.cfg.implicit == 0.0) c2_ = 1.0;
+  const double ll1 = (double)(l * (l + 1));
+  A.init(KL, N_);
+  for (int j = 1; j <= Ni; ++j)
+    for (int row = 1; row <= 2 * KL + 1; ++row) A.at(KL + row, j) = -c2_ * I.radLap.at(row, j);
+  for (int n = 1; n <= Ni; ++n) A.at(2 * KL + 1, n) = A.at(2 * KL + 1, n) + c1_ + c2_ * ll1 * I.R(n, -2);
+  const Band& lap = tor ? D.MagTorLap : D.MagPolLap;
+  for (int j = 1; j <= No; ++j)
+    for (int row = 1; row <= 2 * KL + 1; ++row)
+      A.at(KL + row, j + Ni - 1) = A.at(KL + row, j + Ni - 1) - c2_ * lap.at(row, j);
+  for (int n = 1; n <= No; ++n)
+    A.at(2 * KL + 1, n + Ni - 1) = A.at(2 * KL + 1, n + Ni - 1) + c1_ + c2_ * ll1 * D.R(n, -2);
+  for (int j = 1; j <= 1 + KL; ++j) A.at(2 * KL + 1 + 1 - j, j) = 0.0;
+  for (int j = N_ - KL; j <= N_; ++j) A.at(2 * KL + 1 + N_ - j, j) = 0.0;
+  for (int j = Ni - KL; j <= Ni + KL; ++j) A.at(2 * KL + 1 + Ni - j, j) = 0.0;
+  if (tor) {  // BTor = 0 at the innermost point and outside
+    A.at(2 * KL + 1, 1) = 1.0;
+    A.at(2 * KL + 1, N_) = 1.0;
+  } else {  // (dr - l/r) BPol = 0 innermost, (dr + (l+1)/r) BPol = 0 at the outer wall
+    for (int j = 1; j <= 1 + KL; ++j) A.at(2 * KL + 1 + 1 - j, j) = I.dr[1].at(KL + 1 + 1 - j, j);
+    A.at(2 * KL + 1, 1) = A.at(2 * KL + 1, 1) - I.R(1, -1) * l;
+    for (int j = No - KL; j <= No; ++j) {
+      const int j_ = j + Ni - 1;
+      A.at(2 * KL + 1 + N_ - j_, j_) = D.dr[1].at(KL + 1 + No - j, j);
+    }
+    A.at(2 * KL + 1, N_) = A.at(2 * KL + 1, N_) + D.R(No, -1) * (l + 1);
+  }
+  for (int j = 2; j <= 1 + KL; ++j) {  // dr continuous across the inner-core boundary
+    const int j_ = j + Ni - 1;
+    A.at(2 * KL + 1 + Ni - j_, j_) = D.dr[1].at(KL + 1 + 1 - j, j);
+  }
+  for (int j = Ni - KL; j <= Ni - 1; ++j) A.at(2 * KL + 1 + Ni - j, j) = -I.dr[1].at(KL + 1 + Ni - j, j);
+  A.at(2 * KL + 1, Ni) = D.dr[1].at(KL + 1, 1) - I.dr[1].at(KL + 1, Ni);
+}
 // tim_lumesh_vel_X (timestep.F90:47-86) -- the anelastic velocity operator
 void tim_lumesh_vel_X(const Oracle& o, const RDom& D, double c1, double c2, int l, LUBand& A) {
   double c1_ = c1 / o.tim_dt, c2_ = c2 * o.cfg.implicit;
@@ -789,9 +841,33 @@ void tim_invX(const Oracle& o, bool zero, const std::vector<LUBand>& A, Coll& b)
     dgbtrs1(N, o.KL, o.KL, A[l].M.data(), 3 * o.KL + 1, A[l].ipiv.data(), &b.im[(size_t)N * nh]);
   }
 }
-// tim_multY (timestep.F90:640-670): d = A b + c
+// tim_icinvX (timestep.F90:594-634): the coupled solve, b = (ic rows 1..Ni-1, oc rows)
+void tim_icinvX(const Oracle& o, const std::vector<LUBand>& A, Coll& oc, Coll& ic) {
+  const int Ni = o.Nic, No = o.N, N_ = Ni + No - 1;
+#pragma omp parallel for schedule(static)
+  for (int nh = 0; nh < o.H; ++nh) {
+    if (o.hl[nh] == 0) continue;
+    std::vector<double> b(N_);
+    for (int part = 0; part < 2; ++part) {
+      double* icv = part == 0 ? &ic.re[(size_t)Ni * nh] : &ic.im[(size_t)Ni * nh];
+      double* ocv = part == 0 ? &oc.re[(size_t)No * nh] : &oc.im[(size_t)No * nh];
+      for (int n = 0; n < Ni - 1; ++n) b[n] = icv[n];
+      for (int n = 0; n < No; ++n) b[Ni - 1 + n] = ocv[n];
+      dgbtrs1(N_, o.KL, o.KL, A[o.hl[nh]].M.data(), 3 * o.KL + 1, A[o.hl[nh]].ipiv.data(), b.data());
+      for (int n = 0; n < Ni; ++n) icv[n] = b[n];
+      for (int n = 0; n < No; ++n) ocv[n] = b[Ni - 1 + n];
+    }
+  }
+}
+// tim_multY (timestep.F90:640-670): d = A b + c, columns of N rows
+void tim_multY_n(const Oracle& o, int N, bool zero, const std::vector<Band>& A, const Coll& b, const Coll& c,
+                 Coll& d);
 void tim_multY(const Oracle& o, bool zero, const std::vector<Band>& A, const Coll& b, const Coll& c, Coll& d) {
-  int N = o.N, KL = o.KL;
+  tim_multY_n(o, o.N, zero, A, b, c, d);
+}
+void tim_multY_n(const Oracle& o, int N, bool zero, const std::vector<Band>& A, const Coll& b, const Coll& c,
+                 Coll& d) {
+  int KL = o.KL;
   if (&d != &c) d = c;
 #pragma omp parallel for schedule(static)
   for (int nh = 0; nh < o.H; ++nh) {
@@ -810,13 +886,13 @@ void tim_multY(const Oracle& o, bool zero, const std::vector<Band>& A, const Col
     }
   }
 }
-void tim_zerobc(const Oracle& o, Coll& a) {
-  int N = o.N;
+void tim_zerobc_n(const Oracle& o, int N, Coll& a) {
   for (int nh = 0; nh < o.H; ++nh) {
     a.re[(size_t)N * nh] = 0.0; a.re[(size_t)N * nh + N - 1] = 0.0;
     a.im[(size_t)N * nh] = 0.0; a.im[(size_t)N * nh + N - 1] = 0.0;
   }
 }
+void tim_zerobc(const Oracle& o, Coll& a) { tim_zerobc_n(o, o.N, a); }
 void tim_nlincorr(const Oracle& o, const Coll& n, const Coll& np, Coll& nc) {
   double c = o.cfg.implicit;
   nc.re.resize(n.re.size()); nc.im.resize(n.im.size());
@@ -825,10 +901,9 @@ void tim_nlincorr(const Oracle& o, const Coll& n, const Coll& np, Coll& nc) {
     nc.im[i] = c * (n.im[i] - np.im[i]);
   }
 }
-void tim_addcorr(Oracle& o, const Coll& ac, Coll& a, int nrows) {
-  // nrows = a%D%N ; for the ic fields with Ni = 1 only row 1 of each column
+void tim_addcorr(Oracle& o, const Coll& ac, Coll& a, int nrows, int N) {
+  // nrows = a%D%N (columns of stride N); for the ic fields with Ni = 1 only row 1
   double dterr = 0.0;
-  int N = o.N;
   for (int nh = 0; nh < o.H; ++nh)
     for (int n = 0; n < nrows; ++n) {
       size_t i = (size_t)N * nh + n;
@@ -939,7 +1014,25 @@ int build_matrices(Oracle& o) {
       tim_mesh_Y(o, D, cc1, 1.0, l, Y[l]);
     }
   }
-  // mag_matrices (magnetic.F90:62-133), insulating inner core (Ni = 1)
+  // mag_matrices (magnetic.F90:62-133); conducting inner core: the coupled operators
+  // and tim_mesh_Y on the inner-core mesh (the Boussinesq equations)
+  if (o.Nic > 1) {
+    o.icYTor.assign(L, Band()); o.icYPol.assign(L, Band());
+    for (int l = 1; l < L; ++l) {
+      tim_iclumesh_X_cic(o, 1.0, 1.0, l, true, o.mXTor[l]);
+      bad |= lu_find(o.mXTor[l]);
+      tim_mesh_Y(o, D, 1.0, 1.0, l, o.mYTor[l]);
+      tim_mesh_Y(o, o.ic, 1.0, 1.0, l, o.icYTor[l]);
+    }
+    for (int l = 1; l < L; ++l) {
+      tim_iclumesh_X_cic(o, 1.0, 1.0, l, false, o.mXPol[l]);
+      bad |= lu_find(o.mXPol[l]);
+      tim_mesh_Y(o, D, 1.0, 1.0, l, o.mYPol[l]);
+      tim_mesh_Y(o, o.ic, 1.0, 1.0, l, o.icYPol[l]);
+    }
+    return bad ? 1 : 0;
+  }
+  // insulating inner core (Ni = 1)
   for (int l = 1; l < L; ++l) {
     if (bq) tim_iclumesh_X(o, D, 1.0, 1.0, l, true, o.mXTor[l]);
     else tim_iclumesh_X_anel(o, D, 1.0, 1.0, l, true, o.mXTor[l]);
@@ -1363,8 +1456,10 @@ void spec2coll(const Oracle& o, const Spec& s, Coll& c) {
     }
 }
 // var_coll_meshmult (variables.F90:476-505)
-void meshmult(const Oracle& o, const Band& A, const Coll& in, Coll& out) {
-  int N = o.N, KL = o.KL;
+void meshmult_n(const Oracle& o, int N, const Band& A, const Coll& in, Coll& out);
+void meshmult(const Oracle& o, const Band& A, const Coll& in, Coll& out) { meshmult_n(o, o.N, A, in, out); }
+void meshmult_n(const Oracle& o, int N, const Band& A, const Coll& in, Coll& out) {
+  int KL = o.KL;
   Coll tmp; tmp.init(N, o.H);
   for (int nh = 0; nh < o.H; ++nh) {
     double* re = &tmp.re[(size_t)N * nh];
@@ -1383,19 +1478,26 @@ void meshmult(const Oracle& o, const Band& A, const Coll& in, Coll& out) {
 }
 // var_coll_TorPol2qst_mag (variables.F90:565-605); with the Boussinesq zero rho the
 // compressible var_coll_TorPol2qst (:511-556) is the same arithmetic up to the +0 of xi.
+void torpol2qst_d(const Oracle& o, const RDom& D, const Coll& Tor, const Coll& Pol, Coll& q, Coll& s, Coll& t,
+                  bool comp);
 void torpol2qst(const Oracle& o, const Coll& Tor, const Coll& Pol, Coll& q, Coll& s, Coll& t, bool comp) {
-  int N = o.N;
+  torpol2qst_d(o, o.oc, Tor, Pol, q, s, t, comp);
+}
+// the same on a radial domain D (the inner core's mesh for its energies)
+void torpol2qst_d(const Oracle& o, const RDom& D, const Coll& Tor, const Coll& Pol, Coll& q, Coll& s, Coll& t,
+                  bool comp) {
+  int N = D.N;
   q.init(N, o.H); t.init(N, o.H);
   for (int nh = 0; nh < o.H; ++nh) {
     int l = o.hl[nh];
     for (int n = 1; n <= N; ++n) {
       size_t i = (n - 1) + (size_t)N * nh;
-      double a = o.ad_ll1[l] * o.oc.R(n, -1);
+      double a = o.ad_ll1[l] * D.R(n, -1);
       q.re[i] = Pol.re[i] * a;
       q.im[i] = Pol.im[i] * a;
     }
   }
-  meshmult(o, comp ? o.oc.compr1dr : o.oc.r1dr, Pol, s);
+  meshmult_n(o, N, comp ? D.compr1dr : D.r1dr, Pol, s);
   for (int nh = 0; nh < o.H; ++nh) {
     int l = o.hl[nh];
     for (int n = 0; n < N; ++n) {
@@ -1417,27 +1519,33 @@ void torpol2qstderiv(const Oracle& o, const Coll& Tor, const Coll& Pol, Coll& q,
   meshmult(o, o.oc.dr[1], t, tr);
 }
 // var_coll_qstcurl (variables.F90:713-754)
+void qstcurl_d(const Oracle& o, const RDom& D, const Coll& q, const Coll& s, const Coll& t, Coll& oq, Coll& os,
+               Coll& ot);
 void qstcurl(const Oracle& o, const Coll& q, const Coll& s, const Coll& t, Coll& oq, Coll& os, Coll& ot) {
-  int N = o.N;
+  qstcurl_d(o, o.oc, q, s, t, oq, os, ot);
+}
+void qstcurl_d(const Oracle& o, const RDom& D, const Coll& q, const Coll& s, const Coll& t, Coll& oq, Coll& os,
+               Coll& ot) {
+  int N = D.N;
   Coll tt = t;
-  Coll nt; meshmult(o, o.oc.r1dr, s, nt);
+  Coll nt; meshmult_n(o, N, D.r1dr, s, nt);
   for (int nh = 0; nh < o.H; ++nh) {
     int l = o.hl[nh];
     for (int n = 1; n <= N; ++n) {
       size_t i = (n - 1) + (size_t)N * nh;
-      double a = o.ad_rtll1[l] * o.oc.R(n, -1);
+      double a = o.ad_rtll1[l] * D.R(n, -1);
       nt.re[i] = nt.re[i] - a * q.re[i];
       nt.im[i] = nt.im[i] - a * q.im[i];
     }
   }
-  Coll ns; meshmult(o, o.oc.r1dr, tt, ns);
+  Coll ns; meshmult_n(o, N, D.r1dr, tt, ns);
   for (size_t i = 0; i < ns.re.size(); ++i) { ns.re[i] = -ns.re[i]; ns.im[i] = -ns.im[i]; }
   Coll nq; nq.init(N, o.H);
   for (int nh = 0; nh < o.H; ++nh) {
     int l = o.hl[nh];
     for (int n = 1; n <= N; ++n) {
       size_t i = (n - 1) + (size_t)N * nh;
-      double a = -o.ad_rtll1[l] * o.oc.R(n, -1);
+      double a = -o.ad_rtll1[l] * D.R(n, -1);
       nq.re[i] = tt.re[i] * a;
       nq.im[i] = tt.im[i] * a;
     }
@@ -1541,6 +1649,7 @@ void scal_transform(Oracle& o, const Coll& C, Phys& gr, Phys& gt, Phys& gp) {
   tra_grad(o, sC, gt, gp);
 }
 
+void non_rotation(Oracle& o);
 void evaluate(Oracle& o) {
   size_t psz = (size_t)o.Th * o.Ph * o.N;
   int Th = o.Th, Ph = o.Ph;
@@ -1552,6 +1661,7 @@ void evaluate(Oracle& o) {
   scal_transform(o, o.codC, o.cod_gr, o.cod_gt, o.cod_gp);
   if (o.cfg.comp_tstep) scal_transform(o, o.compC, o.comp_gr, o.comp_gt, o.comp_gp);
   vec_transform(o, o.bTor, o.bPol, o.mag_r, o.mag_t, o.mag_p, o.mag_cr, o.mag_ct, o.mag_cp);
+  if (o.cfg.rot_tstep) non_rotation(o);
   Phys r(psz), th(psz), ph(psz);
   // ---- non_velocity (nonlinear.F90:28-199)
   {
@@ -1677,6 +1787,61 @@ void evaluate(Oracle& o) {
     qstllcurlcurlr(o, cq, cs, o.bNTor);
     for (int n = 0; n < o.N; ++n) { o.bNTor.re[n] = 0; o.bNTor.im[n] = 0; o.bNPol.re[n] = 0; o.bNPol.im[n] = 0; }
   }
+  // the inner core (nonlinear.F90:451-472): N = -rot_omega d/dphi of its field
+  if (o.Nic > 1) {
+    const int Ni = o.Nic;
+    for (int part = 0; part < 2; ++part) {
+      const Coll& a = part == 0 ? o.icTor : o.icPol;
+      Coll& Nn = part == 0 ? o.icNTor : o.icNPol;
+      for (int nh = 0; nh < o.H; ++nh) {
+        const double m_ = (double)o.hm[nh];
+        for (int n = 0; n < Ni; ++n) {
+          const size_t i = (size_t)n + (size_t)Ni * nh;
+          const double dre = -(a.im[i] * m_), dim = a.re[i] * m_;  // var_coll_dph
+          Nn.re[i] = -o.rot_omega * dre;
+          Nn.im[i] = -o.rot_omega * dim;
+        }
+      }
+      for (int n = 0; n < Ni; ++n) { Nn.re[n] = 0.0; Nn.im[n] = 0.0; }
+    }
+  }
+}
+
+// non_rotation (nonlinear.F90:479-538): the viscous and magnetic torques on the inner core,
+// surface integrals over r = r_i (tra_surfintegral, transform.fftw3.F90:1039-1062)
+void non_rotation(Oracle& o) {
+  const int Th = o.Th, Ph = o.Ph;
+  const double vfac = o.oc.R(1, 3) * o.cfg.Pm, mfac = o.oc.R(1, 3) * 2 * o.cfg.Pm / o.cfg.E;
+  auto surf = [&](auto f) {
+    std::vector<double> Y(Th, 0.0);
+    for (int m = 0; m < Ph; ++m)
+      for (int j = 0; j < Th; ++j) Y[j] = Y[j] + f(j, (size_t)j + (size_t)Th * m);
+    double S = 0.0;
+    for (int j = 0; j < Th; ++j) S = S + Y[j] * o.gwP0[j];
+    return S * 4.0 * d_PI / (double)Ph;
+  };
+  if (o.cfg.vel_bc > 2) {
+    o.rot_velTorq = 0.0;
+  } else {
+    const double S = -2.0 / o.oc.R(1, 1);
+    o.rot_velTorq = surf([&](int j, size_t i) { return (S * o.vel_p[i] - o.vel_ct[i]) * o.sn[j]; }) * vfac;
+  }
+  if (o.Nic == 1) o.rot_magTorq = 0.0;
+  else o.rot_magTorq = surf([&](int j, size_t i) { return o.mag_r[i] * o.mag_p[i] * o.sn[j]; }) * mfac;
+}
+// rot_predictor / rot_corrector (rotation.F90:40-87)
+void rot_predictor(Oracle& o) {
+  if (o.cfg.rot_force_0) { o.rot_omega = 0.0; return; }
+  o.rot_omega = o.rot_omega + (o.tim_dt / o.rot_inertia) * (o.rot_velTorq + o.rot_magTorq);
+  o.sv_velTorq = o.rot_velTorq;
+  o.sv_magTorq = o.rot_magTorq;
+}
+void rot_corrector(Oracle& o) {
+  if (o.cfg.rot_force_0) return;
+  o.rot_omega = o.rot_omega + (o.tim_dt * o.cfg.implicit / o.rot_inertia) *
+                                  ((o.rot_velTorq + o.rot_magTorq) - (o.sv_velTorq + o.sv_magTorq));
+  o.sv_velTorq = o.rot_velTorq;
+  o.sv_magTorq = o.rot_magTorq;
 }
 
 // ---- predictor / corrector (velocity.F90:369-465, codensity.F90:224-259,
@@ -1700,7 +1865,7 @@ void vel_gre_adjust(const Oracle& o, Coll& Pol) {
 }
 void vel_setbc_Tor(const Oracle& o, Coll& a) {
   int N = o.N;
-  const double rot_omega = 0.0;
+  const double rot_omega = o.rot_omega;
   for (int nh = 0; nh < o.H; ++nh) {
     a.re[(size_t)N * nh] = 0; a.re[(size_t)N * nh + N - 1] = 0;
     a.im[(size_t)N * nh] = 0; a.im[(size_t)N * nh + N - 1] = 0;
@@ -1724,6 +1889,7 @@ void scal_setbc(const Oracle& o, Coll& a, int bc, double qi, double qo) {
 
 void predictor(Oracle& o) {
   Coll T, Pq;
+  if (o.cfg.rot_tstep) rot_predictor(o);  // main.F90:136, before vel_predictor's boundary value
   // vel_predictor
   o.sv_vNTor = o.vNTor;
   tim_multY(o, false, o.YTor, o.vTor, o.vNTor, T);
@@ -1751,6 +1917,26 @@ void predictor(Oracle& o) {
     scal_setbc(o, T, o.cfg.comp_bc, o.cfg.qi_comp, o.cfg.qo_comp);
     tim_invX(o, true, o.XComp, T);
     o.compC = T;
+  }
+  if (o.Nic > 1) {  // mag_predictor with the conducting inner core (magnetic.F90:370-408)
+    Coll icT;
+    for (int part = 0; part < 2; ++part) {
+      const bool tor = part == 0;
+      Coll& X = tor ? o.bTor : o.bPol;
+      Coll& Nn = tor ? o.bNTor : o.bNPol;
+      Coll& icX = tor ? o.icTor : o.icPol;
+      Coll& icN = tor ? o.icNTor : o.icNPol;
+      (tor ? o.sv_bNTor : o.sv_bNPol) = Nn;
+      tim_multY(o, false, tor ? o.mYTor : o.mYPol, X, Nn, T);
+      (tor ? o.sv_icNTor : o.sv_icNPol) = icN;
+      tim_multY_n(o, o.Nic, false, tor ? o.icYTor : o.icYPol, icX, icN, icT);
+      tim_zerobc_n(o, o.Nic, icT);
+      tim_zerobc(o, T);  // mag_setbc_Tor / mag_setbc_Pol with zero boundary data
+      tim_icinvX(o, tor ? o.mXTor : o.mXPol, T, icT);
+      X = T;
+      icX = icT;
+    }
+    return;
   }
   // mag_predictor (Ni = 1; zero toroidal/poloidal boundary data)
   o.sv_bNTor = o.bNTor;
@@ -1781,12 +1967,13 @@ void predictor(Oracle& o) {
 
 void corrector(Oracle& o) {
   Coll T, Pq, ic;
+  if (o.cfg.rot_tstep) rot_corrector(o);  // main.F90:148
   // vel_corrector
   tim_nlincorr(o, o.vNTor, o.sv_vNTor, T);
   o.sv_vNTor = o.vNTor;
   vel_setbc_Tor(o, T);
   tim_invX(o, false, o.XTor, T);
-  tim_addcorr(o, T, o.vTor, o.N);
+  tim_addcorr(o, T, o.vTor, o.N, o.N);
   tim_nlincorr(o, o.vNPol, o.sv_vNPol, Pq);
   o.sv_vNPol = o.vNPol;
   tim_zerobc(o, Pq);
@@ -1794,19 +1981,38 @@ void corrector(Oracle& o) {
   tim_zerobc(o, Pq);
   tim_invX(o, false, o.XPol, Pq);
   vel_gre_adjust(o, Pq);
-  tim_addcorr(o, Pq, o.vPol, o.N);
+  tim_addcorr(o, Pq, o.vPol, o.N, o.N);
   // cod_corrector
   tim_nlincorr(o, o.codNC, o.sv_codNC, T);
   o.sv_codNC = o.codNC;
   tim_zerobc(o, T);
   tim_invX(o, true, o.XC, T);
-  tim_addcorr(o, T, o.codC, o.N);
+  tim_addcorr(o, T, o.codC, o.N, o.N);
   if (o.cfg.comp_tstep) {
     tim_nlincorr(o, o.compNC, o.sv_compNC, T);
     o.sv_compNC = o.compNC;
     tim_zerobc(o, T);
     tim_invX(o, true, o.XComp, T);
-    tim_addcorr(o, T, o.compC, o.N);
+    tim_addcorr(o, T, o.compC, o.N, o.N);
+  }
+  if (o.Nic > 1) {  // mag_corrector with the conducting inner core (magnetic.F90:414-461)
+    for (int part = 0; part < 2; ++part) {
+      const bool tor = part == 0;
+      const Coll& Nn = tor ? o.bNTor : o.bNPol;
+      const Coll& icN = tor ? o.icNTor : o.icNPol;
+      Coll& sv = tor ? o.sv_bNTor : o.sv_bNPol;
+      Coll& icsv = tor ? o.sv_icNTor : o.sv_icNPol;
+      tim_nlincorr(o, Nn, sv, T);
+      sv = Nn;
+      tim_nlincorr(o, icN, icsv, ic);
+      icsv = icN;
+      tim_zerobc_n(o, o.Nic, ic);
+      tim_zerobc(o, T);
+      tim_icinvX(o, tor ? o.mXTor : o.mXPol, T, ic);
+      tim_addcorr(o, T, tor ? o.bTor : o.bPol, o.N, o.N);
+      tim_addcorr(o, ic, tor ? o.icTor : o.icPol, o.Nic, o.Nic);
+    }
+    return;
   }
   // mag_corrector; with Ni = 1 the inner-core correction is row 1 of the outer-core one
   for (int part = 0; part < 2; ++part) {
@@ -1821,8 +2027,8 @@ void corrector(Oracle& o) {
       if (o.hl[nh] == 0) continue;
       ic.re[(size_t)o.N * nh] = T.re[(size_t)o.N * nh]; ic.im[(size_t)o.N * nh] = T.im[(size_t)o.N * nh];
     }
-    tim_addcorr(o, T, part == 0 ? o.bTor : o.bPol, o.N);
-    tim_addcorr(o, ic, part == 0 ? o.bicTor : o.bicPol, 1);
+    tim_addcorr(o, T, part == 0 ? o.bTor : o.bPol, o.N, o.N);
+    tim_addcorr(o, ic, part == 0 ? o.bicTor : o.bicPol, 1, o.N);
   }
 }
 
@@ -1915,9 +2121,14 @@ void coll_norm_w(const Oracle& o, const Coll& a, const std::vector<double>& wts,
 void coll_norm(const Oracle& o, const Coll& a, double& Eodd, double& Eeven, double& Em0le, double& Em0) {
   coll_norm_w(o, a, o.oc.intr2dr, Eodd, Eeven, Em0le, Em0);
 }
+void coll_norm_n(const Oracle& o, int N, const Coll& a, const std::vector<double>& wts, double& Eodd,
+                 double& Eeven, double& Em0le, double& Em0);
 void coll_norm_w(const Oracle& o, const Coll& a, const std::vector<double>& wts, double& Eodd, double& Eeven,
                  double& Em0le, double& Em0) {
-  int N = o.N;
+  coll_norm_n(o, o.N, a, wts, Eodd, Eeven, Em0le, Em0);
+}
+void coll_norm_n(const Oracle& o, int N, const Coll& a, const std::vector<double>& wts, double& Eodd,
+                 double& Eeven, double& Em0le, double& Em0) {
   std::vector<double> Fod(N, 0), Fev(N, 0), Fm0le(N, 0), Fm0(N, 0), f(N);
   for (int nh = 0; nh < o.H; ++nh) {
     int l = o.hl[nh], m_ = o.hm[nh];
@@ -2137,6 +2348,36 @@ void diagnostics(Oracle& o, double* sc, double* spec, double* prof) {
     const double v[8] = {ME * Et, ME * Ep, ME * Etas, ME * Epas, ME * Etes, ME * Epes, ME * Etesas, ME * Epesas};
     for (int k = 0; k < 8; ++k) sc[LSD_D_MPART + k] = v[k];
   }
+  // ---- the inner core's field (io_write_mag_energy on mag_icTor / icPol, io.F90:315):
+  // its own mesh, the outer core's Dip / Quad; the call leaves io_MagEn / io_OhmDiss at
+  // the inner core's values for io_write_dyn_outputs
+  double icE = 0.0, icEDis = 0.0;
+  if (o.Nic > 1) {
+    const RDom& I = o.ic;
+    const int Ni = o.Nic;
+    const double OD = bq ? 2.0 * o.cfg.Pm / o.cfg.E : 1.0 * o.cfg.Pm / o.cfg.E;
+    Coll q, s, t, cq, cs, ct;
+    torpol2qst_d(o, I, o.icTor, o.icPol, q, s, t, false);
+    double Eo, Ee, E1, E0, Ep, Epes, Epesas, Epas, Et, Etes, Etesas, Etas, Esym, El1, ETm0, EDis;
+    coll_norm_n(o, Ni, q, I.intr2dr, Eo, Ee, E1, E0);
+    Ep = Eo + Ee; Epes = Ee; Epesas = E1; Epas = E0; Esym = Ee; El1 = E1;
+    coll_norm_n(o, Ni, s, I.intr2dr, Eo, Ee, E1, E0);
+    Ep = Ep + Eo + Ee; Epes = Epes + Ee; Epesas = Epesas + E1; Epas = Epas + E0; Esym = Esym + Ee; El1 = El1 + E1;
+    coll_norm_n(o, Ni, t, I.intr2dr, Eo, Ee, E1, E0);
+    Et = Eo + Ee; Etes = Eo; Etesas = E0 - E1; Etas = E0; ETm0 = E0; Esym = Esym + Eo; El1 = El1 + E1;
+    qstcurl_d(o, I, q, s, t, cq, cs, ct);
+    coll_norm_n(o, Ni, cq, I.intr2dr_magdiss, Eo, Ee, E1, E0); EDis = Eo + Ee;
+    coll_norm_n(o, Ni, cs, I.intr2dr_magdiss, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    coll_norm_n(o, Ni, ct, I.intr2dr_magdiss, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    icE = ME * (Ep + Et);
+    icEDis = OD * EDis;
+    const double v[9] = {icE, ME * Et, ME * Esym, ME * El1, ME * ETm0, icEDis, en[LSD_E_DIP], en[LSD_E_QUAD],
+                         ME * Etas + ME * Epas};
+    for (int k = 0; k < 9; ++k) sc[LSD_D_MIC + k] = v[k];
+    const double w[8] = {ME * Et, ME * Ep, ME * Etas, ME * Epas, ME * Etes, ME * Epes, ME * Etesas, ME * Epesas};
+    for (int k = 0; k < 8; ++k) sc[LSD_D_MICPART + k] = w[k];
+  }
+  sc[LSD_D_ROT + 0] = o.rot_omega; sc[LSD_D_ROT + 1] = o.rot_velTorq; sc[LSD_D_ROT + 2] = o.rot_magTorq;
   // ---- CMB (io_write_cmb): the norms of q, s on the outer shell only
   double fdip = 0.0, thdip = 0.0;
   {
@@ -2197,7 +2438,8 @@ void diagnostics(Oracle& o, double* sc, double* spec, double* prof) {
   {
     const double ri = o.cfg.rratio / (1 - o.cfg.rratio), ro = 1 / (1 - o.cfg.rratio);
     const double vol = (4.0 / 3.0 * d_PI) * (ro * ro * ro - ri * ri * ri);
-    const double Kin = en[LSD_E_KE], Mag = en[LSD_E_ME], Visc = en[LSD_E_KE_DIS], Ohm = en[LSD_E_ME_DIS];
+    const double Kin = en[LSD_E_KE], Visc = en[LSD_E_KE_DIS];
+    const double Mag = o.Nic > 1 ? icE : en[LSD_E_ME], Ohm = o.Nic > 1 ? icEDis : en[LSD_E_ME_DIS];
     const double Rm = std::sqrt((2 * Kin) / vol), Re = Rm / o.cfg.Pm;
     const double El = (o.cfg.E * Mag) / (o.cfg.Pm * vol);
     const double Le = std::sqrt((2 * o.cfg.E * o.cfg.E * Mag) / (o.cfg.Pm * o.cfg.Pm * vol));
@@ -2273,6 +2515,8 @@ Coll* field_ptr(Oracle& o, int f) {
     case LSD_MAG_TOR: return &o.bTor;
     case LSD_MAG_POL: return &o.bPol;
     case LSD_COMP_C: return &o.compC;
+    case LSD_MAG_IC_TOR: return o.Nic > 1 ? &o.icTor : nullptr;
+    case LSD_MAG_IC_POL: return o.Nic > 1 ? &o.icPol : nullptr;
   }
   return nullptr;
 }
@@ -2310,8 +2554,10 @@ Oracle* orc_create(const lsd_config* cfg, int* status) {
   o->cfg = *cfg;
   o->L = cfg->L; o->M = cfg->M; o->Mp = cfg->Mp; o->N = cfg->N; o->KL = cfg->KL; o->Nic = cfg->Nic;
   *status = 0;
-  if (o->L <= (o->M - 1) * o->Mp || (o->M > 1 && o->M % 2 == 1) || o->N < 2 * o->KL + 1 || o->Nic != 1 ||
-      cfg->timestep == 0) {
+  const bool cic_ok = o->Nic == 1 || (o->Nic >= 2 * o->KL + 1 && o->Nic <= o->N && cfg->boussinesq &&
+                                       cfg->vel_bc <= 2);
+  if (o->L <= (o->M - 1) * o->Mp || (o->M > 1 && o->M % 2 == 1) || o->N < 2 * o->KL + 1 || !cic_ok ||
+      (cfg->rot_tstep && !cfg->boussinesq) || cfg->timestep == 0) {
     *status = LSD_EARG;
     delete o;
     return nullptr;
@@ -2331,6 +2577,12 @@ Oracle* orc_create(const lsd_config* cfg, int* status) {
                   &o->vNTor, &o->vNPol, &o->codNC, &o->compNC, &o->bNTor, &o->bNPol,
                   &o->sv_vNTor, &o->sv_vNPol, &o->sv_codNC, &o->sv_compNC, &o->sv_bNTor, &o->sv_bNPol})
     c->init(o->N, o->H);
+  if (o->Nic > 1)
+    for (Coll* c : {&o->icTor, &o->icPol, &o->icNTor, &o->icNPol, &o->sv_icNTor, &o->sv_icNPol}) c->init(o->Nic, o->H);
+  {  // rot_precompute (rotation.F90:20-33): 8 pi / 15 r_i^5
+    const double ri = o->oc.R(1, 1), r2 = ri * ri, r4 = r2 * r2;
+    o->rot_inertia = (8.0 * d_PI / 15.0) * (r4 * ri);
+  }
   if (build_matrices(*o)) { *status = LSD_ESINGULAR; delete o; return nullptr; }
   return o;
 }
@@ -2412,6 +2664,10 @@ void orc_fft_r2c(int n, const double* x, double* yre, double* yim) {
   for (int k = 0; k <= n / 2; ++k) { yre[k] = b[k].real(); yim[k] = (k == 0 || 2 * k == n) ? 0.0 : b[k].imag(); }
 }
 
+int orc_set_rotation(Oracle* o, double omega) { o->rot_omega = omega; return 0; }
+void orc_get_rotation(const Oracle* o, double* out) {
+  out[0] = o->rot_omega; out[1] = o->rot_velTorq; out[2] = o->rot_magTorq;
+}
 int orc_set_coll(Oracle* o, int f, const double* re, const double* im) {
   Coll* c = field_ptr(*o, f);
   if (!c) return LSD_EARG;

@@ -71,6 +71,8 @@ def load():
         "orc_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(capi.LsdStats)]),
         "orc_energies": (ctypes.c_int, [vp, _D]),
         "orc_diagnostics": (ctypes.c_int, [vp, _D, _D, _D]),
+        "orc_set_rotation": (ctypes.c_int, [vp, ctypes.c_double]),
+        "orc_get_rotation": (None, [vp, _D]),
         "orc_set_threads": (ctypes.c_int, [ctypes.c_int]),
         "orc_set_reference_state": (ctypes.c_int, [vp, _D]),
         "orc_dth": (ctypes.c_int, [vp, _D, _D, _D]),
@@ -103,6 +105,7 @@ class Oracle:
         self.lib.orc_sizes(self.h, ctypes.byref(s))
         self.sz = {k: getattr(s, k) for k, _ in capi.LsdSizes._fields_}
         self.H, self.N, self.Th, self.Th2, self.Ph = (self.sz[k] for k in ("H", "N", "Th", "Th2", "Ph"))
+        self.cfg_Nic = cfg.Nic
 
     def close(self):
         if self.h:
@@ -160,14 +163,19 @@ class Oracle:
         return ab.T.copy(), ipiv
 
     # ---- state (coll arrays returned as (H, N) C-order == Fortran (N, H))
+    def rows(self, f):
+        """radial points of a field: Nic for the inner core's, N otherwise"""
+        return self.cfg_Nic if f in (capi.MAG_IC_TOR, capi.MAG_IC_POL) else self.N
+
     def set_coll(self, f, re, im):
         re = np.ascontiguousarray(re, dtype=np.float64)
         im = np.ascontiguousarray(im, dtype=np.float64)
-        assert re.size == self.N * self.H
+        assert re.size == self.rows(f) * self.H
         assert self.lib.orc_set_coll(self.h, f, _dp(re), _dp(im)) == 0
 
     def get_coll(self, f):
-        re, im = np.zeros((self.H, self.N)), np.zeros((self.H, self.N))
+        n = self.rows(f)
+        re, im = np.zeros((self.H, n)), np.zeros((self.H, n))
         assert self.lib.orc_get_coll(self.h, f, _dp(re), _dp(im)) == 0
         return re, im
 
@@ -260,6 +268,15 @@ class Oracle:
         e = np.zeros(capi.NENERGY)
         self.lib.orc_energies(self.h, _dp(e))
         return dict(zip(capi.ENERGY_NAMES, e))
+
+    def set_rotation(self, omega):
+        assert self.lib.orc_set_rotation(self.h, float(omega)) == 0
+
+    def rotation(self):
+        """rot_omega, rot_velTorq, rot_magTorq"""
+        out = np.zeros(3)
+        self.lib.orc_get_rotation(self.h, _dp(out))
+        return out
 
     def diagnostics(self):
         """orc_diagnostics, unpacked like Context.diagnostics."""
