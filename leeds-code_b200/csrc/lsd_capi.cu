@@ -35,7 +35,9 @@ void free_ctx(lsd_ctx* ctx) {
                   ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y, ctx->d_yt,
                   ctx->d_ipiv, ctx->d_ipivs, ctx->d_info, ctx->d_gre, ctx->d_gret, ctx->d_invg, ctx->d_state, ctx->d_nl,
                   ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red, ctx->d_ref, ctx->d_laps,
-                  ctx->d_compr1dr, ctx->d_wts, ctx->d_ones, ctx->d_cfl};
+                  ctx->d_compr1dr, ctx->d_wts, ctx->d_ones, ctx->d_cfl, ctx->d_icr, ctx->d_icdr, ctx->d_icradlap,
+                  ctx->d_icr1dr, ctx->d_icintr2dr, ctx->d_icwts, ctx->d_icref, ctx->d_iclaps, ctx->d_iccompr1dr,
+                  ctx->d_icyt, ctx->d_icstate, ctx->d_icsv, ctx->d_rot, ctx->d_gwP0};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -274,12 +276,20 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   ctx->dev = -1;
   const lsd_config& c = *cfg;
   ctx->L = c.L; ctx->M = c.M; ctx->Mp = c.Mp; ctx->N = c.N; ctx->KL = c.KL;
+  ctx->Nic = c.Nic; ctx->NL = c.N + c.Nic - 1;
   // par_precompute (parameters.F90_template:274-288) and this library's scope
   std::string why;
   if (c.L < 2 || c.M < 2 || c.Mp < 1 || c.N < 2 * c.KL + 2 || c.KL < 2 || c.KL > LSD_MAX_KL) why = "bad resolution";
   else if (c.L <= (c.M - 1) * c.Mp) why = "set L > (M-1)*Mp";
   else if (c.M % 2 == 1) why = "if(M>1) set M even";
-  else if (c.Nic != 1) why = "only an insulating inner core (Nic = 1) is supported";
+  else if (c.Nic < 1) why = "Nic must be >= 1";
+  else if (c.Nic > 1 && (c.Nic < 2 * c.KL + 1 || c.Nic > c.N))
+    why = "a conducting inner core needs 2 KL + 1 <= Nic <= N radial points";
+  else if (c.Nic > 1 && !c.boussinesq)
+    why = "a conducting inner core is supported for the Boussinesq equations";
+  else if (c.Nic > 1 && c.vel_bc > 2)
+    why = "a conducting inner core needs a no-slip inner wall (i_vel_bc 1 or 2)";
+  else if (c.rot_tstep && !c.boussinesq) why = "inner-core rotation is supported for the Boussinesq equations";
   else if (c.timestep == 0.0) why = "d_timestep must be > 0 (fixed) or < 0 (CFL / corrector controlled)";
   else if (!c.vel_tstep || !c.cod_tstep || !c.mag_tstep) why = "velocity, codensity and field must all be stepped";
   else if (c.precision != LSD_PREC_FP64 && c.precision != LSD_PREC_OZAKI) why = "unknown precision";
@@ -399,11 +409,38 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
     if (ctx->hl[nh] == 1 && ctx->hm[nh] == 0) ctx->nh_l1m0 = nh;
     if (ctx->hl[nh] == 1 && ctx->hm[nh] == 1) ctx->nh_l1m1 = nh;
   }
-  const size_t lus = (size_t)OP_NFAM * L * N * (3 * KL + 1);
+  const int NL = ctx->NL;
+  const size_t lus = (size_t)OP_NFAM * L * NL * (3 * KL + 1);
   TRY(dalloc(ctx, &ctx->d_lu, lus)); TRY(dalloc(ctx, &ctx->d_lus, lus));
   TRY(dalloc(ctx, &ctx->d_y, (size_t)OP_NFAM * N * (2 * KL + 1) * L));
   TRY(dalloc(ctx, &ctx->d_yt, (size_t)OP_NFAM * N * (2 * KL + 1) * L));
-  TRY(dalloc(ctx, &ctx->d_ipiv, (size_t)OP_NFAM * L * N)); TRY(dalloc(ctx, &ctx->d_ipivs, (size_t)OP_NFAM * L * N));
+  TRY(dalloc(ctx, &ctx->d_ipiv, (size_t)OP_NFAM * L * NL)); TRY(dalloc(ctx, &ctx->d_ipivs, (size_t)OP_NFAM * L * NL));
+  if (ctx->Nic > 1) {  // the inner core's mesh, field, saved terms and Y bands
+    const int Ni = ctx->Nic;
+    TRY(dalloc(ctx, &ctx->d_icr, (size_t)7 * Ni));
+    TRY(dalloc(ctx, &ctx->d_icdr, (size_t)KL * (2 * KL + 1) * Ni));
+    TRY(dalloc(ctx, &ctx->d_icradlap, (size_t)(2 * KL + 1) * Ni));
+    TRY(dalloc(ctx, &ctx->d_icr1dr, (size_t)(2 * KL + 1) * Ni));
+    TRY(dalloc(ctx, &ctx->d_icintr2dr, Ni));
+    TRY(dalloc(ctx, &ctx->d_icwts, (size_t)4 * Ni));
+    TRY(dalloc(ctx, &ctx->d_iclaps, (size_t)LAP_NBAND * (2 * KL + 1) * Ni));
+    TRY(dalloc(ctx, &ctx->d_iccompr1dr, (size_t)(2 * KL + 1) * Ni));
+    TRY(dalloc(ctx, &ctx->d_icref, (size_t)7 * Ni));
+    std::vector<double> ref((size_t)7 * Ni, 0.0);
+    for (int n = 0; n < Ni; ++n) ref[(size_t)REF_ETA * Ni + n] = 1.0;
+    TRY(upload(ctx, ctx->d_icref, ref));
+    TRY(dalloc(ctx, &ctx->d_icyt, (size_t)2 * Ni * (2 * KL + 1) * L));
+    TRY(dalloc(ctx, &ctx->d_icstate, (size_t)2 * Ni * H)); TRY(dalloc(ctx, &ctx->d_icsv, (size_t)2 * Ni * H));
+    CTRY(cudaMemset(ctx->d_icstate, 0, sizeof(cplx) * 2 * Ni * H));
+    CTRY(cudaMemset(ctx->d_icsv, 0, sizeof(cplx) * 2 * Ni * H));
+  }
+  TRY(dalloc(ctx, &ctx->d_rot, (size_t)ROT_NSLOT));
+  CTRY(cudaMemset(ctx->d_rot, 0, sizeof(double) * ROT_NSLOT));
+  TRY(dalloc(ctx, &ctx->d_gwP0, Th));
+  {  // rot_precompute (rotation.F90:20-33): 8 pi / 15 r_i^5, r_i = rratio / (1 - rratio)
+    const double ri = c.rratio / (1.0 - c.rratio), r2 = ri * ri, r4 = r2 * r2;
+    ctx->rot_inertia = (8.0 * 3.1415926535897931 / 15.0) * (r4 * ri);
+  }
   TRY(dalloc(ctx, &ctx->d_info, (size_t)OP_NFAM * L));
   TRY(dalloc(ctx, &ctx->d_gre, (size_t)L * 2 * N)); TRY(dalloc(ctx, &ctx->d_invg, (size_t)L * 4));
   TRY(dalloc(ctx, &ctx->d_gret, (size_t)L * 2 * N));
@@ -512,8 +549,26 @@ int lsd_legendre_table(const lsd_ctx* c, int which, double* out) {
 // coll fields cross the boundary in the reference's layout (Re, Im as (N, H) column-major
 // arrays); they are copied as they are and transposed into [n][nh] on the device
 // (lsd_coll_to_state / lsd_state_to_coll), with a scratch area of the spectral buffers.
+// the inner core's field (Nic > 1): [Nic][H] on the device
+static cplx* ic_field(lsd_ctx* ctx, int field) {
+  if (ctx->Nic <= 1 || (field != LSD_MAG_IC_TOR && field != LSD_MAG_IC_POL)) return nullptr;
+  return ctx->d_icstate + (size_t)(field - LSD_MAG_IC_TOR) * ctx->Nic * ctx->H;
+}
 int lsd_set_coll(lsd_ctx* ctx, int field, const double* re, const double* im) {
-  if (!ctx || !re || !im || field < 0 || field >= LSD_NFIELD) return LSD_EARG;
+  if (!ctx || !re || !im) return LSD_EARG;
+  if (cplx* ic = ic_field(ctx, field)) {
+    CUDA_TRY(cudaSetDevice(ctx->dev));
+    const size_t Fi = (size_t)ctx->Nic * ctx->H;
+    double* stage = (double*)ctx->d_spec;
+    CUDA_TRY(cudaMemcpyAsync(stage, re, sizeof(double) * Fi, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(stage + Fi, im, sizeof(double) * Fi, cudaMemcpyHostToDevice, ctx->stream));
+    int rc = lsd_coll_to_state_n(ctx, ctx->Nic, stage, stage + Fi, ic);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    ctx->have_eval = false;
+    return LSD_OK;
+  }
+  if (field < 0 || field >= LSD_NFIELD) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
   const size_t F = (size_t)ctx->N * ctx->H;
   double* stage = (double*)ctx->d_spec;  // 2 F doubles: Re then Im
@@ -537,7 +592,19 @@ static int coll_out(lsd_ctx* ctx, const cplx* src, double* re, double* im) {
   return LSD_OK;
 }
 int lsd_get_coll(lsd_ctx* ctx, int field, double* re, double* im) {
-  if (!ctx || !re || !im || field < 0 || field >= LSD_NFIELD) return LSD_EARG;
+  if (!ctx || !re || !im) return LSD_EARG;
+  if (cplx* ic = ic_field(ctx, field)) {
+    CUDA_TRY(cudaSetDevice(ctx->dev));
+    const size_t Fi = (size_t)ctx->Nic * ctx->H;
+    double* stage = (double*)ctx->d_spec;
+    int rc = lsd_state_to_coll_n(ctx, ctx->Nic, ic, stage, stage + Fi);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(re, stage, sizeof(double) * Fi, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(im, stage + Fi, sizeof(double) * Fi, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return LSD_OK;
+  }
+  if (field < 0 || field >= LSD_NFIELD) return LSD_EARG;
   return coll_out(ctx, ctx->d_state + field * (size_t)ctx->N * ctx->H, re, im);
 }
 int lsd_get_nonlinear(lsd_ctx* ctx, int which, double* re, double* im) {
@@ -554,6 +621,25 @@ int lsd_set_time(lsd_ctx* ctx, double t, double dt) {
     int rc = lsd_build_operators(ctx);
     if (rc) return rc;
   }
+  return LSD_OK;
+}
+// rot_omega (the state file's 'omega'); the rate at the last evaluation follows it
+int lsd_set_rotation(lsd_ctx* ctx, double omega) {
+  if (!ctx) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  const double w[2] = {omega, omega};
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_rot + ROT_OMEGA, w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return LSD_OK;
+}
+int lsd_get_rotation(const lsd_ctx* cctx, double* out) {
+  if (!cctx || !out) return LSD_EARG;
+  lsd_ctx* ctx = const_cast<lsd_ctx*>(cctx);
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  double r[ROT_NSLOT];
+  CUDA_TRY(cudaMemcpyAsync(r, ctx->d_rot, sizeof(r), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  out[0] = r[ROT_OMEGA]; out[1] = r[ROT_VEL]; out[2] = r[ROT_MAG];
   return LSD_OK;
 }
 // tim_dt, tim_corr_dt, tim_cfl_dt (the columns of io_write_timestep, io.F90:2343-2346)

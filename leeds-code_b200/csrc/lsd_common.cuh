@@ -35,6 +35,12 @@ enum OpFamily {
   OP_NFAM = 7
 };
 
+// rotation state on the device (d_rot): the rate, the rate at the last evaluation (the
+// inner core's -omega d/dphi), the torques saved by rot_predictor / rot_corrector, the
+// torques of the last evaluation, their surface sums (k_products), and dt
+enum RotSlot { ROT_OMEGA = 0, ROT_OMEGA_EVAL, ROT_SV_VEL, ROT_SV_MAG, ROT_VEL, ROT_MAG, ROT_SUM_VEL, ROT_SUM_MAG,
+               ROT_DT, ROT_NSLOT };
+
 // reference-state bands (d_laps): meshs.F90:364-406
 enum LapBand { LAP_COMP = 0, LAP_GRE = 1, LAP_MAGTOR = 2, LAP_MAGPOL = 3, LAP_NBAND = 4 };
 // reference-state columns (d_ref, [7][N]): io.F90:559-608
@@ -116,6 +122,19 @@ struct lsd_ctx {
   // [N][2KL+1] and the weighted integration weights [4][N] (comp, compS, magdiss, veldiss)
   double *d_ref = nullptr, *d_laps = nullptr, *d_compr1dr = nullptr, *d_wts = nullptr;
   bool have_refstate = false;
+  // conducting inner core (Nic > 1): its mesh (the same tables as the outer core's on
+  // Nic points: r powers [7][Nic], dr bands, radLap, r1dr, intr2dr, weighted weights,
+  // reference columns [7][Nic] with eta = 1, reference bands, compr1dr); its field
+  // [2][Nic][H] (mag_icTor, mag_icPol) and saved nonlinear terms; the Y bands of its two
+  // families [2][Nic][2KL+1][L].  NL = N + Nic - 1 rows per operator (the field families'
+  // coupled systems; N rows used by the others).
+  int Nic = 1, NL = 0;
+  double *d_icr = nullptr, *d_icdr = nullptr, *d_icradlap = nullptr, *d_icr1dr = nullptr, *d_icintr2dr = nullptr;
+  double *d_icwts = nullptr, *d_icref = nullptr, *d_iclaps = nullptr, *d_iccompr1dr = nullptr, *d_icyt = nullptr;
+  cplx *d_icstate = nullptr, *d_icsv = nullptr;
+  // inner-core rotation (rotation.F90), ROT_* slots; Gauss weight x P_0^0 / 2 per theta
+  double *d_rot = nullptr, *d_gwP0 = nullptr;
+  double rot_inertia = 0.0;
   // operators: LAPACK band LU [fam][L][N][3KL+1] + ipiv [fam][L][N]; Y bands
   // [fam][L][N][2KL+1]; (d_lus / d_ipivs: [fam][N][3KL+1][L] copies, l fastest)
   double *d_lu = nullptr, *d_lus = nullptr, *d_y = nullptr, *d_yt = nullptr;
@@ -181,6 +200,8 @@ int lsd_pred(lsd_ctx* ctx);            // predictor solves (device)
 int lsd_corr(lsd_ctx* ctx);            // corrector solves + dterr (device)
 int lsd_energy_device(lsd_ctx* ctx, double* out);
 int lsd_energy_static(lsd_ctx* ctx, double* out);
+int lsd_coll_to_state_n(lsd_ctx* ctx, int rows, const double* re, const double* im, cplx* out);
+int lsd_state_to_coll_n(lsd_ctx* ctx, int rows, const cplx* in, double* re, double* im);
 int lsd_diagnostics_device(lsd_ctx* ctx, double* scalars, double* spectra, double* profiles);
 int lsd_coll_to_state(lsd_ctx* ctx, const double* re, const double* im, cplx* out);
 int lsd_state_to_coll(lsd_ctx* ctx, const cplx* in, double* re, double* im);

@@ -371,6 +371,9 @@ struct ProdConst {
   const double* ref;  // [7][N] reference state (anelastic)
   unsigned long long* cflmax;  // variable dt: per-shell CFL maxima [N][2] (bits of doubles >= 0), or null
   const int* bin2c;   // FFT bin -> m-counter (M entries)
+  double* rotsum;     // inner-core rotation: the two torque surface sums (shell 0), or null
+  const double* gwP0; // Gauss weight x P_0^0 / 2 per theta row
+  double rotS;        // -2 / r_i
   int L;
   int fin[PROD_MAXIN];  // input field slots of four_in
 };
@@ -573,10 +576,16 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
     cdh2 = d * d;
     EPm = pc.E / pc.Pm;
   }
+  // non_rotation (nonlinear.F90:479-538) on the inner shell: sums of gwP0 (S u_ph - curl_th u)
+  // sin and gwP0 B_r B_ph sin over this CTA's two theta rows (the equator row of an odd Th
+  // once)
+  double tv = 0.0, tm = 0.0;
+  const bool torque = (PS == PS_BOUSS || PS == PS_BOUSS_COMP) && pc.rotsum && n == 0;
   for (int i = tid; i < 2 * P2; i += PROD_THREADS) {
     const int r = i / P2, pos = ppos<G>(i - r * P2);
     const int j = row_theta(h, r, Th);
     const double sn = pc.sn[j], cs = pc.gp[j];
+    const bool tq = torque && !(r == 1 && (Th & 1) && h == Th2 - 1);
     double2 v[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) v[f] = rows[(size_t)(f * 2 + r) * RS + pos];
@@ -588,6 +597,11 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
       for (int f = 0; f < NF; ++f) x[f] = part == 0 ? v[f].x : v[f].y;
       if constexpr (HAS_UB)
         if (pc.cflmax) cfl_point(x, EPm, pc.E, pc.Pm, cdr2, cdh2, cmr, cmh);
+      if (tq) {
+        const double gw = pc.gwP0[j];
+        tv = tv + gw * ((pc.rotS * x[2] - x[4]) * sn);
+        tm = tm + gw * ((x[6] * x[8]) * sn);
+      }
       prod_point<PS>(x, o, pc, sh, sn, cs);
 #pragma unroll
       for (int q = 0; q < NF_OUT; ++q) {
@@ -596,6 +610,16 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
     }
 #pragma unroll
     for (int q = 0; q < NF_OUT; ++q) rows[(size_t)(q * 2 + r) * RS + pos] = out[q];
+  }
+  if (torque) {
+    for (int o = 16; o > 0; o >>= 1) {
+      tv += __shfl_down_sync(0xffffffffu, tv, o);
+      tm += __shfl_down_sync(0xffffffffu, tm, o);
+    }
+    if ((tid & 31) == 0) {
+      atomicAdd(pc.rotsum, tv);
+      atomicAdd(pc.rotsum + 1, tm);
+    }
   }
   if constexpr (HAS_UB) {
     if (pc.cflmax) {  // CTA maxima -> the shell's slots (doubles >= 0 order as their bits)
@@ -888,6 +912,9 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.L = ctx->L;
   pc.bin2c = ctx->d_bin2c;
   pc.cflmax = c.timestep < 0 ? (unsigned long long*)ctx->d_cfl : nullptr;
+  pc.rotsum = c.rot_tstep ? ctx->d_rot + ROT_SUM_VEL : nullptr;
+  pc.gwP0 = ctx->d_gwP0;
+  pc.rotS = -2.0 / (c.rratio / (1.0 - c.rratio));  // r(1,1) = r_i
   const bool comp = c.comp_tstep != 0;
   const size_t FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
   if (c.boussinesq) {

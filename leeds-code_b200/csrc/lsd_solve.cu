@@ -230,6 +230,13 @@ struct StepArgs {
   double qi, qo, qi_comp, qo_comp;
   int comp;
   double* red;  // corrector: [8] sums of squares
+  int NL;       // rows per operator in lus / ipivs (N + Nic - 1)
+  int Nic;      // inner-core points (> 1: conducting, the field families are coupled)
+  cplx* icstate;       // [2][Nic][H] mag_icTor, mag_icPol
+  cplx* icsv;          // [2][Nic][H] their saved nonlinear terms
+  const double* icyt;  // [2][Nic][2KL+1][L] the inner core's Y bands
+  const double* rot;   // ROT_* slots: rot_omega and the rate of the last evaluation
+  const double* rtor10;  // vel_setbc_Tor's mes_oc%r(1, nh) at nh of (l, m) = (1, 0)
 };
 
 // which solve a grid row performs
@@ -344,10 +351,10 @@ __device__ __forceinline__ void stream_backward(const Band& B, int N, IN&& in, O
 }
 
 // (Y b)(n) + w(n) with the Y band (2KL+1, N) (tim_multY, timestep.F90:640-660), b streamed
-// through a window of 2KL+1 rows; rows are requested in increasing n.  Right-hand-side
-// inputs that a thread reads before it writes them (state, nonlinear terms, the saved
-// terms) go through the read-only path: no thread re-reads an element after writing it,
-// so the loads may be hoisted above the saves.
+// through a window of 2KL+1 rows; rows are requested in increasing n.  Only arrays that no
+// thread of the kernel writes (the bands, the nonlinear terms) go through the read-only
+// path (__ldg): that path lets the compiler move a load past a store to the same address,
+// so the state and the saved terms, which the solves overwrite, use ordinary loads.
 template <int KL>
 struct MultY {
   const double* y;  // this degree's band: element (r, j) at y[(j LDM + r) L]
@@ -362,7 +369,7 @@ struct MultY {
 #pragma unroll
     for (int t = 0; t <= 2 * KL; ++t) {
       const int j = t - KL;
-      win[t] = (j >= 0 && j < N) ? __ldg(b + (size_t)j * rst) : make_double2(0.0, 0.0);
+      win[t] = (j >= 0 && j < N) ? b[(size_t)j * rst] : make_double2(0.0, 0.0);
     }
     next = KL + 1;
   }
@@ -375,7 +382,7 @@ struct MultY {
     }
 #pragma unroll
     for (int t = 0; t < 2 * KL; ++t) win[t] = win[t + 1];
-    win[2 * KL] = next < N ? __ldg(b + (size_t)next * rst) : make_double2(0.0, 0.0);
+    win[2 * KL] = next < N ? b[(size_t)next * rst] : make_double2(0.0, 0.0);
     ++next;
     return acc;
   }
@@ -406,9 +413,10 @@ __device__ ColView col_view(const StepArgs& a, int job, int nh, int l) {
   v.S = a.sv + fld * F + nh;
   v.W1 = a.work + (size_t)(2 * fld) * F + nh;
   v.W2 = a.work + (size_t)(2 * fld + 1) * F + nh;
-  v.B1.f = a.lus + (size_t)fam * N * LD * L + l; v.B1.piv = a.ipivs + (size_t)fam * N * L + l;
+  const int NL = a.NL;
+  v.B1.f = a.lus + (size_t)fam * NL * LD * L + l; v.B1.piv = a.ipivs + (size_t)fam * NL * L + l;
   v.B1.L = L; v.B1.LD = LD;
-  v.B2.f = a.lus + (size_t)OP_VGRE * N * LD * L + l; v.B2.piv = a.ipivs + (size_t)OP_VGRE * N * L + l;
+  v.B2.f = a.lus + (size_t)OP_VGRE * NL * LD * L + l; v.B2.piv = a.ipivs + (size_t)OP_VGRE * NL * L + l;
   v.B2.L = L; v.B2.LD = LD;
   v.y1 = a.yt + (size_t)fam * N * LDM * L + l;
   v.g = a.gret + l;
@@ -428,6 +436,7 @@ template <int KL>
 __global__ void __launch_bounds__(SOLVE_THREADS) k_predictor(StepArgs a) {
   const int job = blockIdx.y;
   if (job == J_COMP && !a.comp) return;
+  if ((job == J_MTOR || job == J_MPOL) && a.Nic > 1) return;  // k_mag_ic
   const int nh = blockIdx.x * blockDim.x + threadIdx.x;
   if (nh >= a.H) return;
   const int l = a.hl[nh], N = a.N, L = a.L;
@@ -444,6 +453,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_predictor(StepArgs a) {
     else if (bc == 3 || bc == 4) bc0 = qi;
     bcN = (bc == 2 || bc == 4) ? qo : 0.0;
   }
+  // vel_setbc_Tor (velocity.F90:291-300): the no-slip inner wall turns with the inner core
+  if (job == J_VTOR && l == 1 && a.hm[nh] == 0 && a.vel_bc <= 2) bc0 = a.rot[ROT_OMEGA] * a.rtor10[0];
   auto w1 = [&](int c, double2 x) { v.W1[(size_t)c * rst] = x; };
   auto r1 = [&](int n) { return v.W1[(size_t)n * rst]; };
   if (job == J_VPOL) {
@@ -495,7 +506,6 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_predictor(StepArgs a) {
     if (n == N - 1) return make_double2(bcN, 0.0);
     return x;
   };
-  // vel_setbc_Tor: the l = 1, m = 0 inner value rot_omega r_i is 0 (no inner-core rotation)
   if (!solve) {
     for (int n = 0; n < N; ++n) v.X[(size_t)n * rst] = inC(n);
     return;
@@ -517,6 +527,7 @@ template <int KL>
 __global__ void __launch_bounds__(SOLVE_THREADS) k_corrector(StepArgs a) {
   const int job = blockIdx.y;
   if (job == J_COMP && !a.comp) return;
+  if ((job == J_MTOR || job == J_MPOL) && a.Nic > 1) return;  // k_mag_ic
   const int nh = blockIdx.x * blockDim.x + threadIdx.x;
   double ss = 0.0, ssic = 0.0;
   if (nh < a.H) {
@@ -528,10 +539,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_corrector(StepArgs a) {
     // nc = c (N - N_saved) ; N_saved = N ; zerobc (tim_nlincorr, timestep.F90:696-715)
     // vel_setbc_Tor (Re part; velocity.F90:291-299): only no-slip walls (i_vel_bc <= 2)
     const bool tor10 = job == J_VTOR && l == 1 && a.hm[nh] == 0 && a.vel_bc <= 2;
+    const double wr = tor10 ? a.rot[ROT_OMEGA] * a.rtor10[0] : 0.0;
     auto inC = [&](int n) {
-      const double2 x = __ldg(v.Nn + (size_t)n * rst), p = __ldg(v.S + (size_t)n * rst);
+      const double2 x = __ldg(v.Nn + (size_t)n * rst), p = v.S[(size_t)n * rst];
       v.S[(size_t)n * rst] = x;
-      if (n == 0) return tor10 ? make_double2(-v.X[0].x, 0.0) : z2;
+      if (n == 0) return tor10 ? make_double2(wr - v.X[0].x, 0.0) : z2;
       if (n == N - 1) return z2;
       return make_double2(c * (x.x - p.x), c * (x.y - p.y));
     };
@@ -579,6 +591,132 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_corrector(StepArgs a) {
   int slot = job == J_VTOR ? 0 : job == J_VPOL ? 1 : job == J_COD ? 2 : job == J_COMP ? 3 : job == J_MTOR ? 4 : 6;
   warp_block_add(ss, a.red + slot);
   if (job == J_MTOR || job == J_MPOL) warp_block_add(ssic, a.red + slot + 1);
+}
+
+// The field with a conducting inner core (mag_predictor / mag_corrector, magnetic.F90:370-461;
+// tim_icinvX, timestep.F90:594-634).  Each column is one system of NL = Nic + N - 1 unknowns:
+// index c < Nic - 1 is the inner core's row c, c >= Nic - 1 the outer core's row c - (Nic - 1)
+// (c = Nic - 1, the inner-core boundary, belongs to both).  The inner core's nonlinear term
+// -rot_omega d/dphi of its field (nonlinear.F90:451-472) is formed here from the field and
+// the rate of the evaluation.  The forward pass keeps its rows in the field's two work
+// column sets (2 N >= NL rows).  grid (ceil(H / SOLVE_THREADS), 2): job row 0 toroidal,
+// 1 poloidal.  CORR: the corrector (nc = c (N - N_saved), x += correction, dterr sums).
+template <int KL, bool CORR>
+__global__ void __launch_bounds__(SOLVE_THREADS) k_mag_ic(StepArgs a) {
+  const int k = blockIdx.y, job = k == 0 ? J_MTOR : J_MPOL;
+  const int nh = blockIdx.x * blockDim.x + threadIdx.x;
+  double ss = 0.0, ssic = 0.0;
+  if (nh < a.H) {
+    const int l = a.hl[nh], N = a.N, L = a.L, Ni = a.Nic, NL = N + Ni - 1;
+    const ColView v = col_view<KL>(a, job, nh, l);
+    const size_t rst = v.rst;
+    const double2 z2 = make_double2(0.0, 0.0);
+    const size_t Fi = (size_t)Ni * a.H;
+    cplx* icX = a.icstate + (size_t)k * Fi + nh;
+    cplx* icS = a.icsv + (size_t)k * Fi + nh;
+    const double om = a.rot[ROT_OMEGA_EVAL], m_ = (double)a.hm[nh], c = a.implicit;
+    auto icN = [&](int n) {  // -omega (var_coll_dph of the field)
+      const double2 x = icX[(size_t)n * rst];
+      const double dre = -(x.y * m_), dim = x.x * m_;
+      return make_double2(-om * dre, -om * dim);
+    };
+    auto wk = [&](int cc) { return cc < N ? v.W1 + (size_t)cc * rst : v.W2 + (size_t)(cc - N) * rst; };
+    if (!CORR) {
+      if (l == 0) {  // not solved: the right-hand sides with their boundary rows
+        for (int n = 0; n < Ni; ++n) {
+          const double2 x = icN(n);
+          icS[(size_t)n * rst] = x;
+          icX[(size_t)n * rst] = (n == 0 || n == Ni - 1) ? z2 : x;
+        }
+        for (int n = 0; n < N; ++n) {
+          const double2 x = __ldg(v.Nn + (size_t)n * rst);
+          v.S[(size_t)n * rst] = x;
+          v.X[(size_t)n * rst] = (n == 0 || n == N - 1) ? z2 : x;
+        }
+      } else {
+        // B := Y B + N (both meshes) ; zerobc ; invX
+        icS[(size_t)(Ni - 1) * rst] = icN(Ni - 1);
+        MultY<KL> myo, myi;
+        myo.init(v.y1, L, v.X, rst, N);
+        myi.init(a.icyt + (size_t)k * Ni * (2 * KL + 1) * L + l, L, icX, rst, Ni);
+        auto in = [&](int cc) {
+          if (cc < Ni - 1) {
+            const double2 nn = icN(cc);
+            icS[(size_t)cc * rst] = nn;
+            const double2 x = myi.apply(cc, nn);
+            return cc == 0 ? z2 : x;
+          }
+          const int n = cc - (Ni - 1);
+          double2 x = __ldg(v.Nn + (size_t)n * rst);
+          v.S[(size_t)n * rst] = x;
+          x = myo.apply(n, x);
+          return (n == 0 || n == N - 1) ? z2 : x;
+        };
+        stream_forward<KL>(v.B1, NL, in, [&](int cc, double2 x) { *wk(cc) = x; });
+        stream_backward<KL>(v.B1, NL, [&](int cc) { return *wk(cc); }, [&](int cc, double2 x) {
+          if (cc <= Ni - 1) icX[(size_t)cc * rst] = x;
+          if (cc >= Ni - 1) v.X[(size_t)(cc - (Ni - 1)) * rst] = x;
+        });
+      }
+    } else {
+      icS[(size_t)(Ni - 1) * rst] = icN(Ni - 1);  // saved whole (tim_nlincorr + copy)
+      auto in = [&](int cc) {
+        if (cc < Ni - 1) {
+          const double2 nn = icN(cc), p = icS[(size_t)cc * rst];
+          icS[(size_t)cc * rst] = nn;
+          return cc == 0 ? z2 : make_double2(c * (nn.x - p.x), c * (nn.y - p.y));
+        }
+        const int n = cc - (Ni - 1);
+        const double2 x = __ldg(v.Nn + (size_t)n * rst), p = v.S[(size_t)n * rst];
+        v.S[(size_t)n * rst] = x;
+        return (n == 0 || n == N - 1) ? z2 : make_double2(c * (x.x - p.x), c * (x.y - p.y));
+      };
+      auto add = [&](cplx* X, double2 d) {
+        const double2 x = *X;
+        *X = make_double2(x.x + d.x, x.y + d.y);
+      };
+      if (l == 0) {
+        for (int cc = 0; cc < NL; ++cc) {
+          const double2 d = in(cc);
+          if (cc <= Ni - 1) { add(icX + (size_t)cc * rst, d); ssic = ssic + d.x * d.x + d.y * d.y; }
+          if (cc >= Ni - 1) { add(v.X + (size_t)(cc - (Ni - 1)) * rst, d); ss = ss + d.x * d.x + d.y * d.y; }
+        }
+      } else {
+        stream_forward<KL>(v.B1, NL, in, [&](int cc, double2 x) { *wk(cc) = x; });
+        stream_backward<KL>(v.B1, NL, [&](int cc) { return *wk(cc); }, [&](int cc, double2 d) {
+          if (cc <= Ni - 1) { add(icX + (size_t)cc * rst, d); ssic = ssic + d.x * d.x + d.y * d.y; }
+          if (cc >= Ni - 1) { add(v.X + (size_t)(cc - (Ni - 1)) * rst, d); ss = ss + d.x * d.x + d.y * d.y; }
+        });
+      }
+    }
+  }
+  if (CORR) {  // red slots 4 bTor, 5 bicTor, 6 bPol, 7 bicPol
+    warp_block_add(ss, a.red + (k == 0 ? 4 : 6));
+    warp_block_add(ssic, a.red + (k == 0 ? 5 : 7));
+  }
+}
+
+// rot_predictor / rot_corrector (rotation.F90:40-87) with the torques of non_rotation
+// (nonlinear.F90:479-538) from k_products' surface sums; one thread.  The rate of the
+// evaluation is kept for the inner core's nonlinear term of the solves that follow.
+__global__ void k_rot(double* rot, int corr, double inertia, double implicit, double Ph, double vfac, double mfac,
+                      int vel_on, int mag_on, int force0) {
+  if (threadIdx.x != 0) return;
+  const double PI = 3.1415926535897931;
+  rot[ROT_OMEGA_EVAL] = rot[ROT_OMEGA];
+  const double tv = vel_on ? (rot[ROT_SUM_VEL] * 4.0 * PI / Ph) * vfac : 0.0;  // tra_surfintegral's 4 pi / Ph
+  const double tm = mag_on ? (rot[ROT_SUM_MAG] * 4.0 * PI / Ph) * mfac : 0.0;
+  rot[ROT_VEL] = tv;
+  rot[ROT_MAG] = tm;
+  if (force0) {
+    if (!corr) rot[ROT_OMEGA] = 0.0;
+    return;
+  }
+  const double dt = rot[ROT_DT];
+  if (!corr) rot[ROT_OMEGA] = rot[ROT_OMEGA] + (dt / inertia) * (tv + tm);
+  else rot[ROT_OMEGA] = rot[ROT_OMEGA] + (dt * implicit / inertia) * ((tv + tm) - (rot[ROT_SV_VEL] + rot[ROT_SV_MAG]));
+  rot[ROT_SV_VEL] = tv;
+  rot[ROT_SV_MAG] = tm;
 }
 
 // ---- energies: per-(field, category, n) partial sums of w_lm |a|^2 ------------------
@@ -667,6 +805,10 @@ StepArgs step_args(lsd_ctx* ctx) {
   a.qi = ctx->cfg.qi; a.qo = ctx->cfg.qo; a.qi_comp = ctx->cfg.qi_comp; a.qo_comp = ctx->cfg.qo_comp;
   a.comp = ctx->cfg.comp_tstep;
   a.red = ctx->d_red;
+  a.NL = ctx->NL; a.Nic = ctx->Nic;
+  a.icstate = ctx->d_icstate; a.icsv = ctx->d_icsv; a.icyt = ctx->d_icyt;
+  a.rot = ctx->d_rot;
+  a.rtor10 = ctx->d_r + (size_t)(3 + (ctx->nh_l1m0 >= 0 && ctx->nh_l1m0 <= 3 ? ctx->nh_l1m0 : 1)) * ctx->N;
   return a;
 }
 
@@ -736,6 +878,7 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   cplx* fa = fo + nsyn * FF;  // the 7 (8) product fields, in the analysis layout
   const bool vardt = ctx->cfg.timestep < 0;
   if (vardt) CUDA_TRY(cudaMemsetAsync(ctx->d_cfl, 0, sizeof(double) * 2 * ctx->N, s));
+  if (ctx->cfg.rot_tstep) CUDA_TRY(cudaMemsetAsync(ctx->d_rot + ROT_SUM_VEL, 0, sizeof(double) * 2, s));
   if ((rc = lsd_launch_products(ctx, fo, fa))) return rc;
   if (vardt && (rc = lsd_launch_cfl_finish(ctx))) return rc;  // non_maxtstep
   if (marks) cudaEventRecord(marks[2], s);
@@ -784,6 +927,23 @@ void launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
   dim3 g(ceil_div(ctx->H, SOLVE_THREADS), J_NJOB);
   if (corr) k_corrector<KL><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a);
   else k_predictor<KL><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a);
+  if (ctx->Nic > 1) {  // the field coupled to the inner core
+    dim3 gi(ceil_div(ctx->H, SOLVE_THREADS), 2);
+    if (corr) k_mag_ic<KL, true><<<gi, SOLVE_THREADS, 0, ctx->stream>>>(a);
+    else k_mag_ic<KL, false><<<gi, SOLVE_THREADS, 0, ctx->stream>>>(a);
+    ctx->launches++;
+  }
+}
+
+// rot_predictor / rot_corrector before the solves (main.F90:136, 148)
+void launch_rot(lsd_ctx* ctx, bool corr) {
+  const lsd_config& c = ctx->cfg;
+  if (!c.rot_tstep) return;
+  const double ri = c.rratio / (1.0 - c.rratio), r3 = ri * ri * ri;  // mes_oc%r(1,3)
+  k_rot<<<1, 32, 0, ctx->stream>>>(ctx->d_rot, corr ? 1 : 0, ctx->rot_inertia, c.implicit, (double)ctx->Ph,
+                                   r3 * c.Pm, r3 * 2 * c.Pm / c.E, c.vel_bc <= 2 ? 1 : 0, ctx->Nic > 1 ? 1 : 0,
+                                   c.rot_force_0);
+  ctx->launches++;
 }
 
 int launch_step_kernel(lsd_ctx* ctx, const StepArgs& a, bool corr) {
@@ -801,6 +961,7 @@ int launch_step_kernel(lsd_ctx* ctx, const StepArgs& a, bool corr) {
 
 int lsd_pred(lsd_ctx* ctx) {
   StepArgs a = step_args(ctx);
+  launch_rot(ctx, false);
   int rc = launch_step_kernel(ctx, a, false);
   if (rc) return rc;
   ctx->launches++;
@@ -812,6 +973,7 @@ int lsd_pred(lsd_ctx* ctx) {
 int lsd_corr(lsd_ctx* ctx) {
   StepArgs a = step_args(ctx);
   cudaMemsetAsync(ctx->d_red, 0, sizeof(double) * 8, ctx->stream);
+  launch_rot(ctx, true);
   int rc = launch_step_kernel(ctx, a, true);
   if (rc) return rc;
   ctx->launches++;
@@ -1227,6 +1389,67 @@ int lsd_diagnostics_device(lsd_ctx* ctx, double* sc, double* spec, double* prof)
     const double v[8] = {ME * Et, ME * Ep, ME * Etas, ME * Epas, ME * Etes, ME * Epes, ME * Etesas, ME * Epesas};
     for (int k = 0; k < 8; ++k) sc[LSD_D_MPART + k] = v[k];
   }
+  // ---- the inner core's field (io_write_mag_energy on mag_icTor / icPol, io.F90:315): q, s,
+  // t and curl on its own mesh (spectral slots 0..5, free once the outer core's sums are on
+  // the host), category norms per shell, radial sums here; the outer core's Dip / Quad.
+  // The call leaves io_MagEn / io_OhmDiss at the inner core's values for dyn_outputs.
+  double icE = 0.0, icEDis = 0.0;
+  if (ctx->Nic > 1) {
+    const int Ni = ctx->Nic;
+    const size_t Fi = (size_t)Ni * H;
+    SpecArgs si;
+    si.N = Ni; si.H = H; si.KL = KL; si.L = L; si.hl = ctx->d_l;
+    si.r = ctx->d_icr; si.r1dr = ctx->d_icr1dr; si.dr1 = ctx->d_icdr;
+    dim3 gi(ceil_div(H, 128), Ni);
+    k_qst<<<gi, 128, 0, s>>>(si, ctx->d_icr1dr, ctx->d_icstate, ctx->d_icstate + Fi, sp, sp + F, sp + 2 * F);
+    k_curl<<<gi, 128, 0, s>>>(si, sp, sp + F, sp + 2 * F, sp + 3 * F, sp + 4 * F, sp + 5 * F);
+    const cplx* arrs[6];
+    for (int k = 0; k < 6; ++k) arrs[k] = sp + k * F;
+    const cplx** d_arrs = (const cplx**)(ctx->d_red + 64);
+    double* d_out = ctx->d_red + 128;
+    CUDA_TRY(cudaMemcpyAsync(d_arrs, arrs, sizeof(arrs), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(double) * 24 * Ni, s));
+    k_norms<<<dim3(ceil_div(H, 128), Ni, 6), 128, 0, s>>>(Ni, H, ctx->d_l, ctx->d_m, d_arrs, 6, d_out);
+    ctx->launches += 3;
+    std::vector<double> Fi_h((size_t)24 * Ni), wic((size_t)5 * Ni);
+    CUDA_TRY(cudaMemcpyAsync(Fi_h.data(), d_out, sizeof(double) * Fi_h.size(), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(wic.data(), ctx->d_icintr2dr, sizeof(double) * Ni, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(wic.data() + Ni, ctx->d_icwts, sizeof(double) * 4 * Ni, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    auto nw = [&](int k, const double* w, double& Eo, double& Ee, double& E1, double& E0) {
+      double v4[4];
+      for (int q = 0; q < 4; ++q) {
+        double acc = 0.0;
+        for (int n = 0; n < Ni; ++n) acc = acc + Fi_h[((size_t)k * 4 + q) * Ni + n] * w[n];
+        v4[q] = acc;
+      }
+      Eo = v4[0]; Ee = v4[1]; E1 = v4[2]; E0 = v4[3];
+    };
+    const double* w2i = wic.data();
+    const double* wmd = wic.data() + 3 * Ni;  // intr2dr_magdiss of the inner core's mesh
+    const double OD = bq ? 2.0 * c.Pm / c.E : 1.0 * c.Pm / c.E;
+    double Eo, Ee, E1, E0, Ep, Epes, Epesas, Epas, Et, Etes, Etesas, Etas, Esym, El1, ETm0, EDis;
+    nw(0, w2i, Eo, Ee, E1, E0); Ep = Eo + Ee; Epes = Ee; Epesas = E1; Epas = E0; Esym = Ee; El1 = E1;
+    nw(1, w2i, Eo, Ee, E1, E0);
+    Ep = Ep + Eo + Ee; Epes = Epes + Ee; Epesas = Epesas + E1; Epas = Epas + E0; Esym = Esym + Ee; El1 = El1 + E1;
+    nw(2, w2i, Eo, Ee, E1, E0);
+    Et = Eo + Ee; Etes = Eo; Etesas = E0 - E1; Etas = E0; ETm0 = E0; Esym = Esym + Eo; El1 = El1 + E1;
+    nw(3, wmd, Eo, Ee, E1, E0); EDis = Eo + Ee;
+    nw(4, wmd, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    nw(5, wmd, Eo, Ee, E1, E0); EDis = EDis + Eo + Ee;
+    icE = ME * (Ep + Et);
+    icEDis = OD * EDis;
+    const double v9[9] = {icE, ME * Et, ME * Esym, ME * El1, ME * ETm0, icEDis, en[LSD_E_DIP], en[LSD_E_QUAD],
+                          ME * Etas + ME * Epas};
+    for (int k = 0; k < 9; ++k) sc[LSD_D_MIC + k] = v9[k];
+    const double v8[8] = {ME * Et, ME * Ep, ME * Etas, ME * Epas, ME * Etes, ME * Epes, ME * Etesas, ME * Epesas};
+    for (int k = 0; k < 8; ++k) sc[LSD_D_MICPART + k] = v8[k];
+  }
+  {  // rot_torque.dat
+    double rot[ROT_NSLOT];
+    CUDA_TRY(cudaMemcpy(rot, ctx->d_rot, sizeof(rot), cudaMemcpyDeviceToHost));
+    sc[LSD_D_ROT + 0] = rot[ROT_OMEGA]; sc[LSD_D_ROT + 1] = rot[ROT_VEL]; sc[LSD_D_ROT + 2] = rot[ROT_MAG];
+  }
   // ---- mag_cmb (io.F90:2036-2145): var_coll_norm_orig of q, s zeroed below the outer shell
   double fdip, thdip;
   {
@@ -1283,7 +1506,8 @@ int lsd_diagnostics_device(lsd_ctx* ctx, double* sc, double* spec, double* prof)
   {
     const double ri = c.rratio / (1 - c.rratio), ro = 1 / (1 - c.rratio);
     const double vol = (4.0 / 3.0 * PI) * (ro * ro * ro - ri * ri * ri);
-    const double Kin = en[LSD_E_KE], Mag = en[LSD_E_ME], Visc = en[LSD_E_KE_DIS], Ohm = en[LSD_E_ME_DIS];
+    const double Kin = en[LSD_E_KE], Visc = en[LSD_E_KE_DIS];
+    const double Mag = ctx->Nic > 1 ? icE : en[LSD_E_ME], Ohm = ctx->Nic > 1 ? icEDis : en[LSD_E_ME_DIS];
     const double Rm = std::sqrt((2 * Kin) / vol), Re = Rm / c.Pm;
     const double El = (c.E * Mag) / (c.Pm * vol);
     const double Le = std::sqrt((2 * c.E * c.E * Mag) / (c.Pm * c.Pm * vol));
@@ -1378,15 +1602,22 @@ __global__ void k_state_to_coll(int N, int H, const cplx* __restrict__ in, doubl
 }  // namespace
 
 int lsd_coll_to_state(lsd_ctx* ctx, const double* re, const double* im, cplx* out) {
-  dim3 g(ceil_div(ctx->H, TT), ceil_div(ctx->N, TT)), b(TT, 8);
-  k_coll_to_state<<<g, b, 0, ctx->stream>>>(ctx->N, ctx->H, re, im, out);
+  return lsd_coll_to_state_n(ctx, ctx->N, re, im, out);
+}
+int lsd_state_to_coll(lsd_ctx* ctx, const cplx* in, double* re, double* im) {
+  return lsd_state_to_coll_n(ctx, ctx->N, in, re, im);
+}
+// the same for columns of `rows` radial points (the inner core's Nic)
+int lsd_coll_to_state_n(lsd_ctx* ctx, int rows, const double* re, const double* im, cplx* out) {
+  dim3 g(ceil_div(ctx->H, TT), ceil_div(rows, TT)), b(TT, 8);
+  k_coll_to_state<<<g, b, 0, ctx->stream>>>(rows, ctx->H, re, im, out);
   ctx->launches++;
   CUDA_TRY(cudaGetLastError());
   return LSD_OK;
 }
-int lsd_state_to_coll(lsd_ctx* ctx, const cplx* in, double* re, double* im) {
-  dim3 g(ceil_div(ctx->H, TT), ceil_div(ctx->N, TT)), b(TT, 8);
-  k_state_to_coll<<<g, b, 0, ctx->stream>>>(ctx->N, ctx->H, in, re, im);
+int lsd_state_to_coll_n(lsd_ctx* ctx, int rows, const cplx* in, double* re, double* im) {
+  dim3 g(ceil_div(ctx->H, TT), ceil_div(rows, TT)), b(TT, 8);
+  k_state_to_coll<<<g, b, 0, ctx->stream>>>(rows, ctx->H, in, re, im);
   ctx->launches++;
   CUDA_TRY(cudaGetLastError());
   return LSD_OK;

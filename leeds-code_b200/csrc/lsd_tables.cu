@@ -145,6 +145,32 @@ __global__ void k_grid(int N, double rratio, double alpha, double* r) {
   }
 }
 
+// The inner core's mesh (meshs.F90:165-169): r(n) = ri cos(pi (2 Nic - n') / (2 Nic - 1)),
+// n' = Nic + n, so that r(Nic) = ri; powers as in k_grid.
+__global__ void k_grid_ic(int Ni, double rratio, double* r) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (n > Ni) return;
+  const double PI = 3.1415926535897931;
+  const int N_ = 2 * Ni, np = n + Ni;
+  const double ri = rratio / (1.0 - rratio);
+  const double x = ri * cos(PI * (N_ - np) / (double)(N_ - 1));
+  for (int p = -3; p <= 3; ++p) {
+    double y = 1.0;
+    int ap = p < 0 ? -p : p;
+    for (int k = 0; k < ap; ++k) y = (k == 0) ? x : y * x;
+    r[(size_t)(p + 3) * Ni + (n - 1)] = p < 0 ? 1.0 / y : (p == 1 ? x : y);
+  }
+}
+
+// leg_gwP0 (legendre.F90:103-104): P_0^0 * gw / 2 on both hemispheres
+__global__ void k_gwP0(int Th, int Th2, const double* leg_P, const double* gw, double* gwP0) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Th2) return;
+  const double v = leg_P[j] * gw[j] * 0.5;  // table P, harmonic nh = 0 (l = m = 0)
+  gwP0[j] = v;
+  gwP0[Th - 1 - j] = v;
+}
+
 // FD weights at point n by inverting the local Taylor matrix; integration-weight
 // contributions w(n, i, j) kept for an ordered sum.
 __global__ void k_fdweights(int N, int KL, const double* r, double* dr, double* wcontrib, int* fail) {
@@ -282,15 +308,15 @@ __device__ double anel_diag(int fam, int l, int n, int N, const double* r, const
   }
 }
 
-__global__ void k_build_ops(int N, int KL, int L, const double* r, const double* dr, const double* radlap,
+__global__ void k_build_ops(int N, int NL, int KL, int L, const double* r, const double* dr, const double* radlap,
                             const double* laps, const double* ref, OpParams P, double* lu, int* ipiv, double* y,
                             int* info) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   int fam = blockIdx.y;
   if (l >= L) return;
   const int ld = 3 * KL + 1, ldm = 2 * KL + 1;
-  double* A = lu + ((size_t)fam * L + l) * (size_t)ld * N;
-  int* ip = ipiv + ((size_t)fam * L + l) * N;
+  double* A = lu + ((size_t)fam * L + l) * (size_t)ld * NL;  // NL: the families' row stride
+  int* ip = ipiv + ((size_t)fam * L + l) * NL;
   const double* rm1 = r + (size_t)2 * N;
   const double* rm2 = r + (size_t)1 * N;
   const size_t band = (size_t)ldm * N;
@@ -407,29 +433,35 @@ __global__ void k_build_ops(int N, int KL, int L, const double* r, const double*
 
 // LAPACK layouts [fam][L][N][band] -> solve layouts [fam][N][band][L] (degree fastest),
 // for the factors, the pivots and the Y bands
-__global__ void k_lu_transpose(int N, int KL, int L, const double* lu, const int* ipiv, const double* y,
-                               double* lus, int* ipivs, double* yt) {
+// (factors and pivots with the row stride NL; the field families of a conducting inner
+// core have NL rows, the others N)
+__global__ void k_lu_transpose(int N, int NL, int icfam, int KL, int L, const double* lu, const int* ipiv,
+                               const double* y, double* lus, int* ipivs, double* yt) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y;
   int fam = blockIdx.z;
   if (l >= L) return;
+  const bool coupled = icfam && (fam == OP_MTOR || fam == OP_MPOL);
+  if (j >= (coupled ? NL : N)) return;
   const int ld = 3 * KL + 1, ldm = 2 * KL + 1;
-  const double* A = lu + (((size_t)fam * L + l) * N + j) * ld;
-  for (int row = 0; row < ld; ++row) lus[(((size_t)fam * N + j) * ld + row) * L + l] = A[row];
-  ipivs[((size_t)fam * N + j) * L + l] = ipiv[((size_t)fam * L + l) * N + j];
+  const double* A = lu + (((size_t)fam * L + l) * NL + j) * ld;
+  for (int row = 0; row < ld; ++row) lus[(((size_t)fam * NL + j) * ld + row) * L + l] = A[row];
+  ipivs[((size_t)fam * NL + j) * L + l] = ipiv[((size_t)fam * L + l) * NL + j];
+  if (j >= N) return;
   const double* Y = y + (((size_t)fam * L + l) * N + j) * ldm;
   for (int row = 0; row < ldm; ++row) yt[(((size_t)fam * N + j) * ldm + row) * L + l] = Y[row];
 }
 
 // Green's functions and influence matrices (velocity.F90:148-168)
-__global__ void k_greens(int N, int KL, int L, const double* lu, const int* ipiv, double* gre, double* gret, double* invg, int* fail) {
+__global__ void k_greens(int N, int NL, int KL, int L, const double* lu, const int* ipiv, double* gre, double* gret,
+                         double* invg, int* fail) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l < 1 || l >= L) return;
   const int ld = 3 * KL + 1;
-  const double* Agre = lu + ((size_t)OP_VGRE * L + l) * (size_t)ld * N;
-  const int* pgre = ipiv + ((size_t)OP_VGRE * L + l) * N;
-  const double* Apol = lu + ((size_t)OP_VPOL * L + l) * (size_t)ld * N;
-  const int* ppol = ipiv + ((size_t)OP_VPOL * L + l) * N;
+  const double* Agre = lu + ((size_t)OP_VGRE * L + l) * (size_t)ld * NL;
+  const int* pgre = ipiv + ((size_t)OP_VGRE * L + l) * NL;
+  const double* Apol = lu + ((size_t)OP_VPOL * L + l) * (size_t)ld * NL;
+  const int* ppol = ipiv + ((size_t)OP_VPOL * L + l) * NL;
   double* g1 = gre + (size_t)l * 2 * N;
   double* g2 = g1 + N;
   for (int n = 0; n < N; ++n) { g1[n] = 0.0; g2[n] = 0.0; }
@@ -449,6 +481,79 @@ __global__ void k_greens(int N, int KL, int L, const double* lu, const int* ipiv
   }
 }
 
+// The field's operators with a conducting inner core, Boussinesq (tim_iclumesh_Tor_X /
+// _Pol_X, timestep.F90:218-344; mag_bc_Tor / mag_bc_Pol, magnetic.F90:137-282): NL = Ni +
+// N - 1 unknowns, 1..Ni on the inner core's mesh and Ni..NL on the outer core's (Ni the
+// inner-core boundary, shared); row 1 the innermost point's condition, row Ni the
+// continuity of dr across the boundary, row NL the insulating exterior.  Also the inner
+// core's Y bands (tim_mesh_Y on its mesh) in the solve layout [k][Ni][2KL+1][L].
+// One thread per (l, k), k = 0 toroidal, 1 poloidal.
+__global__ void k_build_icops(int N, int Ni, int KL, int L, const double* r, const double* dr, const double* radlap,
+                              const double* icr, const double* icdr, const double* icradlap, OpParams P,
+                              double* lu, int* ipiv, double* icyt, int* info) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (l >= L) return;
+  const int fam = k == 0 ? OP_MTOR : OP_MPOL;
+  const int NL = N + Ni - 1, ld = 3 * KL + 1, ldm = 2 * KL + 1;
+  double* A = lu + ((size_t)fam * L + l) * (size_t)ld * NL;
+  int* ip = ipiv + ((size_t)fam * L + l) * NL;
+#define AX(i, j) A[(size_t)((i) - 1) + (size_t)ld * ((j) - 1)]
+#define MB(B, i, j) (B)[(size_t)((i) - 1) + (size_t)ldm * ((j) - 1)]
+  for (size_t i = 0; i < (size_t)ld * NL; ++i) A[i] = 0.0;
+  if (l == 0) {  // never solved
+    for (int j = 1; j <= NL; ++j) AX(2 * KL + 1, j) = 1.0;
+    info[fam * L + l] = dev_dgbtf2(NL, KL, A, ld, ip);
+    return;
+  }
+  const double c1_ = P.c1_[fam], c2_ = P.c2_[fam], c2y = P.c2y[fam];
+  const double ll1 = (double)(l * (l + 1));
+  const double* rm2 = r + (size_t)1 * N;
+  const double* rm1 = r + (size_t)2 * N;
+  const double* icrm2 = icr + (size_t)1 * Ni;
+  const double* icrm1 = icr + (size_t)2 * Ni;
+  const size_t icband = (size_t)ldm * Ni;
+  for (int j = 1; j <= Ni; ++j)
+    for (int row = 1; row <= ldm; ++row) AX(KL + row, j) = -c2_ * MB(icradlap, row, j);
+  for (int n = 1; n <= Ni; ++n) AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * ll1 * icrm2[n - 1];
+  for (int j = 1; j <= N; ++j)
+    for (int row = 1; row <= ldm; ++row) AX(KL + row, j + Ni - 1) = AX(KL + row, j + Ni - 1) - c2_ * MB(radlap, row, j);
+  for (int n = 1; n <= N; ++n) AX(2 * KL + 1, n + Ni - 1) = AX(2 * KL + 1, n + Ni - 1) + c1_ + c2_ * ll1 * rm2[n - 1];
+  for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = 0.0;
+  for (int j = NL - KL; j <= NL; ++j) AX(2 * KL + 1 + NL - j, j) = 0.0;
+  for (int j = Ni - KL; j <= Ni + KL; ++j) AX(2 * KL + 1 + Ni - j, j) = 0.0;
+  if (k == 0) {  // BTor = 0 at the innermost point and outside
+    AX(2 * KL + 1, 1) = 1.0;
+    AX(2 * KL + 1, NL) = 1.0;
+  } else {  // (dr - l/r) BPol = 0 innermost, (dr + (l+1)/r) BPol = 0 at the outer wall
+    for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(icdr, KL + 1 + 1 - j, j);
+    AX(2 * KL + 1, 1) = AX(2 * KL + 1, 1) - icrm1[0] * l;
+    for (int j = N - KL; j <= N; ++j) {
+      const int j_ = j + Ni - 1;
+      AX(2 * KL + 1 + NL - j_, j_) = MB(dr, KL + 1 + N - j, j);
+    }
+    AX(2 * KL + 1, NL) = AX(2 * KL + 1, NL) + rm1[N - 1] * (l + 1);
+  }
+  for (int j = 2; j <= 1 + KL; ++j) {  // dr continuous across the inner-core boundary
+    const int j_ = j + Ni - 1;
+    AX(2 * KL + 1 + Ni - j_, j_) = MB(dr, KL + 1 + 1 - j, j);
+  }
+  for (int j = Ni - KL; j <= Ni - 1; ++j) AX(2 * KL + 1 + Ni - j, j) = -MB(icdr, KL + 1 + Ni - j, j);
+  AX(2 * KL + 1, Ni) = MB(dr, KL + 1, 1) - MB(icdr, KL + 1, Ni);
+  info[fam * L + l] = dev_dgbtf2(NL, KL, A, ld, ip);
+  for (int j = 1; j <= Ni; ++j)  // tim_mesh_Y on the inner core's mesh
+    for (int row = 1; row <= ldm; ++row) {
+      double v = c2y * MB(icradlap, row, j);
+      if (row == KL + 1) {
+        const double t = ll1 * icrm2[j - 1];
+        v = v + c1_ - c2y * (t + P.Hyp * t * t);
+      }
+      icyt[(((size_t)k * Ni + (j - 1)) * ldm + (row - 1)) * L + l] = v;
+    }
+  (void)icband;
+#undef AX
+#undef MB
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------------------
@@ -462,7 +567,8 @@ int lsd_build_tables(lsd_ctx* ctx) {
   k_trig<<<ceil_div(Th, 128), 128, 0, s>>>(Th, ctx->d_gp, ctx->d_sn, ctx->d_sn1);
   dim3 gl(ceil_div(Th2, 64), M);
   k_legendre<<<gl, 64, 0, s>>>(L, M, ctx->Mp, H, Th2, ctx->d_gp, ctx->d_gw, ctx->d_sn1, ctx->d_lm2nh, ctx->d_leg, d_fail);
-  ctx->launches += 3;
+  k_gwP0<<<ceil_div(Th2, 128), 128, 0, s>>>(Th, Th2, ctx->d_leg, ctx->d_gw, ctx->d_gwP0);
+  ctx->launches += 4;
   CUDA_TRY(cudaGetLastError());
   int fail = 0;
   CUDA_TRY(cudaMemcpyAsync(&fail, d_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -490,11 +596,24 @@ int lsd_build_radial(lsd_ctx* ctx) {
   k_bands<<<ceil_div(N, 128), 128, 0, s>>>(N, KL, ctx->d_r, ctx->d_dr, ctx->d_ref, ctx->d_radlap, ctx->d_r1dr,
                                            ctx->d_laps, ctx->d_compr1dr);
   ctx->launches += 4;
+  double* wci = nullptr;
+  if (ctx->Nic > 1) {  // the inner core's mesh: the same construction on its Nic points
+    const int Ni = ctx->Nic;
+    CUDA_TRY(cudaMalloc(&wci, sizeof(double) * Ni * lda * lda));
+    CUDA_TRY(cudaMemsetAsync(ctx->d_icdr, 0, sizeof(double) * KL * lda * Ni, s));
+    k_grid_ic<<<ceil_div(Ni, 128), 128, 0, s>>>(Ni, ctx->cfg.rratio, ctx->d_icr);
+    k_fdweights<<<ceil_div(Ni, 64), 64, 0, s>>>(Ni, KL, ctx->d_icr, ctx->d_icdr, wci, d_fail);
+    k_intr2dr<<<ceil_div(Ni, 128), 128, 0, s>>>(Ni, KL, wci, ctx->d_icref, ctx->d_icintr2dr, ctx->d_icwts);
+    k_bands<<<ceil_div(Ni, 128), 128, 0, s>>>(Ni, KL, ctx->d_icr, ctx->d_icdr, ctx->d_icref, ctx->d_icradlap,
+                                              ctx->d_icr1dr, ctx->d_iclaps, ctx->d_iccompr1dr);
+    ctx->launches += 4;
+  }
   CUDA_TRY(cudaGetLastError());
   int fail = 0;
   CUDA_TRY(cudaMemcpyAsync(&fail, d_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   cudaFree(wc);
+  if (wci) cudaFree(wci);
   cudaFree(d_fail);
   if (fail) return lsd_fail(ctx, LSD_ESINGULAR, "radial mesh construction failed (code " + std::to_string(fail) + ")");
   return LSD_OK;
@@ -527,12 +646,23 @@ int lsd_build_operators(lsd_ctx* ctx) {
   CUDA_TRY(cudaMemsetAsync(d_fail, 0, sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(ctx->d_y, 0, sizeof(double) * OP_NFAM * N * (2 * KL + 1) * L, s));
   dim3 g(ceil_div(L, 32), OP_NFAM);
-  k_build_ops<<<g, 32, 0, s>>>(N, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_laps, ctx->d_ref, P, ctx->d_lu,
-                               ctx->d_ipiv, ctx->d_y, ctx->d_info);
-  dim3 gt(ceil_div(L, 64), N, OP_NFAM);
-  k_lu_transpose<<<gt, 64, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_lus, ctx->d_ipivs, ctx->d_yt);
+  const int NL = ctx->NL, Ni = ctx->Nic;
+  k_build_ops<<<g, 32, 0, s>>>(N, NL, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_laps, ctx->d_ref, P,
+                               ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_info);
+  if (Ni > 1) {  // the field families coupled to the inner core
+    k_build_icops<<<dim3(ceil_div(L, 32), 2), 32, 0, s>>>(N, Ni, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap,
+                                                          ctx->d_icr, ctx->d_icdr, ctx->d_icradlap, P, ctx->d_lu,
+                                                          ctx->d_ipiv, ctx->d_icyt, ctx->d_info);
+    ctx->launches++;
+  }
+  dim3 gt(ceil_div(L, 64), NL, OP_NFAM);
+  k_lu_transpose<<<gt, 64, 0, s>>>(N, NL, Ni > 1 ? 1 : 0, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_lus,
+                                   ctx->d_ipivs, ctx->d_yt);
   CUDA_TRY(cudaMemsetAsync(ctx->d_gret, 0, sizeof(double) * 2 * N * L, s));
-  k_greens<<<ceil_div(L, 32), 32, 0, s>>>(N, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_gre, ctx->d_gret, ctx->d_invg, d_fail);
+  k_greens<<<ceil_div(L, 32), 32, 0, s>>>(N, NL, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_gre, ctx->d_gret, ctx->d_invg,
+                                          d_fail);
+  // the step's dt for rot_predictor / rot_corrector, read on the device
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_rot + ROT_DT, &ctx->dt, sizeof(double), cudaMemcpyHostToDevice, s));
   ctx->launches += 3;
   CUDA_TRY(cudaGetLastError());
   std::vector<int> info((size_t)OP_NFAM * L);

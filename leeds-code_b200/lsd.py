@@ -80,6 +80,8 @@ def load_library(path=None):
         "lsd_energies": [_V, _D],
         "lsd_energies_static": [_V, _D],
         "lsd_diagnostics": [_V, _D, _D, _D],
+        "lsd_set_rotation": [_V, ctypes.c_double],
+        "lsd_get_rotation": [_V, _D],
         "lsd_banded_factor_device": [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V, _V, _V],
         "lsd_banded_solve_device": [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V, _V, ctypes.c_int, _V, _V],
         "lsd_profile_phases": [_V, _D, _I],
@@ -197,13 +199,19 @@ class Context:
         return t.T.copy()
 
     # ---- state (coll (H, N))
+    def rows(self, field):
+        """radial points of a field: Nic for the inner core's (MAG_IC_*), N otherwise"""
+        return self.cfg.Nic if field in (capi.MAG_IC_TOR, capi.MAG_IC_POL) else self.N
+
     def set_coll(self, field, re, im):
         re, im = _c(re), _c(im)
-        assert re.size == self.H * self.N and im.size == self.H * self.N
+        n = self.rows(field)
+        assert re.size == self.H * n and im.size == self.H * n
         self._ok(self.lib.lsd_set_coll(self.h, field, _dp(re), _dp(im)))
 
     def get_coll(self, field):
-        re, im = np.zeros((self.H, self.N)), np.zeros((self.H, self.N))
+        n = self.rows(field)
+        re, im = np.zeros((self.H, n)), np.zeros((self.H, n))
         self._ok(self.lib.lsd_get_coll(self.h, field, _dp(re), _dp(im)))
         return re, im
 
@@ -259,6 +267,16 @@ class Context:
         ins = [_c(x) for pair in (q, s, t, qr, sr, tr) for x in pair]
         self._ok(self.lib.lsd_tra_qst2rtp_vel(self.h, *[_dp(a) for a in ins], *[_dp(o) for o in outs]))
         return outs
+
+    def set_rotation(self, omega):
+        """lsd_set_rotation: the inner core's rotation rate rot_omega."""
+        self._ok(self.lib.lsd_set_rotation(self.h, float(omega)))
+
+    def rotation(self):
+        """lsd_get_rotation: rot_omega, rot_velTorq, rot_magTorq."""
+        out = np.zeros(3)
+        self._ok(self.lib.lsd_get_rotation(self.h, _dp(out)))
+        return out
 
     def dt_control(self):
         """tim_dt, tim_corr_dt, tim_cfl_dt (io.F90:2346)."""
