@@ -14,6 +14,9 @@ from . import capi
 STATE_VARS = ("uT", "uP", "C", "BT", "BP")
 FIELD_OF_VAR = {"uT": capi.VEL_TOR, "uP": capi.VEL_POL, "C": capi.COD_C,
                 "BT": capi.MAG_TOR, "BP": capi.MAG_POL, "Comp": capi.COMP_C}
+# the inner core's field: declared on the outer core's r dimension, its first Nic radial
+# entries written (io.F90:1594-1595, 1613-1614; read back with Nic rows, io.F90:445-446)
+IC_FIELD_OF_VAR = {"icBT": capi.MAG_IC_TOR, "icBP": capi.MAG_IC_POL}
 
 
 def folded_harmonics(L, M, Mp):
@@ -45,12 +48,14 @@ def state_nh(l, m_, L, M, Mp):
     return np.where(ok, nh, -1)
 
 
-def load_state(path, L, M, Mp, N, r_expected=None):
+def load_state(path, L, M, Mp, N, r_expected=None, Nic=1):
     """Return dict(field -> (re, im) arrays of shape (H, N)), t, dt, r.
 
     Modes of the run that are not in the file are zero (the reference fills them with
     uniform noise of amplitude d_init_pert from an unseeded generator, io.F90:1316-1324,
-    which no run can reproduce)."""
+    which no run can reproduce).  With Nic > 1 the inner core's field (icBT, icBP) is
+    returned too, arrays (H, Nic), when the file holds it on Nic points; otherwise the run
+    continues the outer core's field inward (synthetic.ic_extend, io.F90:440-443)."""
     from scipy.io import netcdf_file
     f = netcdf_file(path, "r", mmap=False)
     r = np.array(f.variables["r"].data, dtype=np.float64)
@@ -60,27 +65,42 @@ def load_state(path, L, M, Mp, N, r_expected=None):
         raise ValueError("state radial grid differs from the run's grid")
     l, m_, _ = folded_harmonics(L, M, Mp)
     out = {}
+    nic_file = len(f.variables["icr"].data) if "icr" in f.variables else 1
     for name, var in f.variables.items():
-        if name not in FIELD_OF_VAR:
+        if name in FIELD_OF_VAR:
+            field, rows = FIELD_OF_VAR[name], N
+        elif name in IC_FIELD_OF_VAR and Nic > 1 and nic_file == Nic:
+            field, rows = IC_FIELD_OF_VAR[name], Nic
+        else:
             continue
         a = var._attributes
         Lf, Mf, Mpf = int(a["L"]), int(a["M"]), int(a["Mp"])
         data = np.array(var.data, dtype=np.float64)  # (2, Hfile, N)
         idx = state_nh(l, m_, Lf, Mf, Mpf)
-        re = np.zeros((len(l), N))
-        im = np.zeros((len(l), N))
+        re = np.zeros((len(l), rows))
+        im = np.zeros((len(l), rows))
         ok = idx >= 0
-        re[ok] = data[0, idx[ok], :]
-        im[ok] = data[1, idx[ok], :]
-        out[FIELD_OF_VAR[name]] = (re, im)
+        re[ok] = data[0, idx[ok], :rows]
+        im[ok] = data[1, idx[ok], :rows]
+        out[field] = (re, im)
     t = float(f._attributes.get("t", 0.0))
     dt = float(f.variables["dt"].data) if "dt" in f.variables else 0.0
     f.close()
     return out, t, dt, r
 
 
-def save_state(path, fields, L, M, Mp, r, ric, t, dt, attrs):
-    """Write a state file in the current layout of io_save_state (dims r, icr, H, ReIm)."""
+def load_rotation(path):
+    """The inner core's rotation rate rot_omega of a state file ('icOmega', io.F90:431-432)."""
+    from scipy.io import netcdf_file
+    f = netcdf_file(path, "r", mmap=False)
+    w = float(f.variables["icOmega"].data) if "icOmega" in f.variables else 0.0
+    f.close()
+    return w
+
+
+def save_state(path, fields, L, M, Mp, r, ric, t, dt, attrs, omega=0.0):
+    """Write a state file in the current layout of io_save_state (dims r, icr, H, ReIm).
+    fields may hold the inner core's (MAG_IC_TOR / MAG_IC_POL, (H, Nic)); omega: rot_omega."""
     from scipy.io import netcdf_file
     l, m_, _ = folded_harmonics(L, M, Mp)
     H = len(l)
@@ -99,15 +119,17 @@ def save_state(path, fields, L, M, Mp, r, ric, t, dt, attrs):
     vic = f.createVariable("icr", "d", ("icr",))
     vic[:] = ric
     vdt = f.createVariable("dt", "d", ())
-    vdt.assignValue(dt)
+    vdt[...] = dt  # a 0-d variable (assignValue fails on numpy 2 for these)
     vom = f.createVariable("icOmega", "d", ())
-    vom.assignValue(0.0)
+    vom[...] = omega
     inv = {v: k for k, v in FIELD_OF_VAR.items()}
+    inv.update({v: k for k, v in IC_FIELD_OF_VAR.items()})
     for fld, (re, im) in fields.items():
         v = f.createVariable(inv[fld], "d", ("ReIm", "H", "r"))
         data = np.zeros((2, H, N))
-        data[0, idx, :] = re
-        data[1, idx, :] = im
+        rows = re.shape[1]
+        data[0, idx, :rows] = re
+        data[1, idx, :rows] = im
         v[:] = data
         v.L, v.M, v.Mp = np.int32(L), np.int32(M), np.int32(Mp)
     f.close()

@@ -123,3 +123,25 @@ def test_viscous_torque_rigid_rotation_and_braking():
     assert abs(rigid[1]) < 1e-9 * abs(tv), (rigid, tv)
     assert tv < 0 and tm == 0.0
     assert abs(w1 - (w0 + cfg.timestep / inertia * tv)) <= 1e-12 * abs(w1)
+
+
+def test_state_file_round_trip_inner_core(tmp_path):
+    """save_state / load_state / load_rotation with the inner core's field (icBT, icBP on
+    the r dimension, Nic entries written) and icOmega."""
+    cfg = syn.config_inner_core(L=12, N=17, Nic=9)
+    st = syn.boussinesq_state(cfg, seed=3)
+    rng = np.random.default_rng(4)
+    l, m_, _ = syn.folded_harmonics(cfg.L, cfg.M, cfg.Mp)
+    for f in (capi.MAG_IC_TOR, capi.MAG_IC_POL):
+        re = rng.standard_normal((len(l), cfg.Nic))
+        im = rng.standard_normal((len(l), cfg.Nic))
+        im[m_ == 0] = 0.0
+        st[f] = (re, im)
+    r = syn.chebyshev_grid(cfg.N, cfg.rratio, cfg.alpha)
+    ric = syn.inner_core_grid(cfg.Nic, cfg.rratio)
+    p = str(tmp_path / "state.cdf")
+    pkg.state.save_state(p, st, cfg.L, cfg.M, cfg.Mp, r, ric, 0.25, 1e-5, {}, omega=-13.3)
+    out, t, dt, r2 = pkg.state.load_state(p, cfg.L, cfg.M, cfg.Mp, cfg.N, r_expected=r, Nic=cfg.Nic)
+    assert t == 0.25 and dt == 1e-5 and pkg.state.load_rotation(p) == -13.3
+    for f, (re, im) in st.items():
+        assert np.array_equal(out[f][0], re) and np.array_equal(out[f][1], im), f
