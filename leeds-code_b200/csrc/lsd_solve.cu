@@ -350,43 +350,50 @@ __device__ __forceinline__ void stream_backward(const Band& B, int N, IN&& in, O
   }
 }
 
-// (Y b)(n) + w(n) with the Y band (2KL+1, N) (tim_multY, timestep.F90:640-660), b streamed
-// through a window of 2KL+1 rows; rows are requested in increasing n.  Only arrays that no
-// thread of the kernel writes (the bands, the nonlinear terms) go through the read-only
-// path (__ldg): that path lets the compiler move a load past a store to the same address,
-// so the state and the saved terms, which the solves overwrite, use ordinary loads.
+// W(n) := (Y X)(n) + R(n) with the Y band (2KL+1, N) for every row of a column (tim_multY,
+// timestep.F90:640-670) as a pass of its own, eight rows per batch: the batch's X rows,
+// band values and R rows are all loaded before any of its rows is stored, so their loads
+// overlap (a window advanced one row per streamed row would wait for each X row in turn).
+// R may be W (in place) or the nonlinear terms.  Only arrays that no thread of the kernel
+// writes (the bands, the nonlinear terms) go through the read-only path (__ldg): that path
+// lets the compiler move a load past a store to the same address.
+constexpr int MY_BATCH = 8;
 template <int KL>
-struct MultY {
-  const double* y;  // this degree's band: element (r, j) at y[(j LDM + r) L]
-  int L;
-  const double2* b;
-  size_t rst;
-  int N;
-  double2 win[2 * KL + 1];  // b(n - KL .. n + KL)
-  int next;
-  __device__ void init(const double* y_, int L_, const double2* b_, size_t rst_, int N_) {
-    y = y_; L = L_; b = b_; rst = rst_; N = N_;
+__device__ __forceinline__ void multy_rows(const double* y, int L, const double2* X, const double2* R, double2* W,
+                                           size_t rst, int N) {
+  constexpr int LDM = 2 * KL + 1, WIN = 2 * KL + MY_BATCH;
+  double2 win[WIN];  // X rows n0 - KL .. n0 + MY_BATCH - 1 + KL
 #pragma unroll
-    for (int t = 0; t <= 2 * KL; ++t) {
-      const int j = t - KL;
-      win[t] = (j >= 0 && j < N) ? b[(size_t)j * rst] : make_double2(0.0, 0.0);
-    }
-    next = KL + 1;
+  for (int t = 0; t < 2 * KL; ++t) {
+    const int j = t - KL;
+    win[t] = (j >= 0 && j < N) ? X[(size_t)j * rst] : make_double2(0.0, 0.0);
   }
-  __device__ double2 apply(int n, double2 acc) {
-    constexpr int LDM = 2 * KL + 1;
+  for (int n0 = 0; n0 < N; n0 += MY_BATCH) {
+    double2 r[MY_BATCH];
+    double yb[MY_BATCH][LDM];
 #pragma unroll
-    for (int t = 0; t < LDM; ++t) {
-      const int j = n - KL + t;
-      if (j >= 0 && j < N) acc = axpy2(acc, __ldg(y + ((size_t)j * LDM + (LDM - 1 - t)) * L), win[t]);
+    for (int u = 0; u < MY_BATCH; ++u) {
+      const int j = n0 + KL + u;
+      win[2 * KL + u] = j < N ? X[(size_t)j * rst] : make_double2(0.0, 0.0);
+      const int n = n0 + u;
+      r[u] = n < N ? R[(size_t)n * rst] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int t = 0; t < LDM; ++t) {
+        const int jj = n - KL + t;
+        yb[u][t] = (n < N && jj >= 0 && jj < N) ? __ldg(y + ((size_t)jj * LDM + (LDM - 1 - t)) * L) : 0.0;
+      }
     }
 #pragma unroll
-    for (int t = 0; t < 2 * KL; ++t) win[t] = win[t + 1];
-    win[2 * KL] = next < N ? b[(size_t)next * rst] : make_double2(0.0, 0.0);
-    ++next;
-    return acc;
+    for (int u = 0; u < MY_BATCH; ++u) {
+      double2 acc = r[u];
+#pragma unroll
+      for (int t = 0; t < LDM; ++t) acc = axpy2(acc, yb[u][t], win[u + t]);
+      if (n0 + u < N) W[(size_t)(n0 + u) * rst] = acc;
+    }
+#pragma unroll
+    for (int t = 0; t < 2 * KL; ++t) win[t] = win[t + MY_BATCH];
   }
-};
+}
 
 __device__ __forceinline__ void warp_block_add(double v, double* target);
 
@@ -430,6 +437,38 @@ __device__ __forceinline__ void gre_coeffs(const double* iG, double2 x0, double2
   cb = make_double2(iG[1] * x0.x + iG[3] * xN.x, iG[1] * x0.y + iG[3] * xN.y);
 }
 
+// The saves of the nonlinear terms, apart from the streamed solves: every load of a batch of
+// eight rows is issued before its stores, so that a column's loads overlap.  (Inside the
+// streamed passes the right-hand-side callbacks only load: a store there would keep the
+// compiler from hoisting the next rows' loads above it, one memory round trip per row.)
+// save_terms: S := N.  diff_terms: W := c (N - S), S := N (tim_nlincorr).
+constexpr int SAVE_BATCH = 8;
+__device__ __forceinline__ void save_terms(const double2* Nn, double2* S, size_t rst, int N) {
+  for (int n0 = 0; n0 < N; n0 += SAVE_BATCH) {
+    double2 x[SAVE_BATCH];
+#pragma unroll
+    for (int u = 0; u < SAVE_BATCH; ++u)
+      if (n0 + u < N) x[u] = __ldg(Nn + (size_t)(n0 + u) * rst);
+#pragma unroll
+    for (int u = 0; u < SAVE_BATCH; ++u)
+      if (n0 + u < N) S[(size_t)(n0 + u) * rst] = x[u];
+  }
+}
+__device__ __forceinline__ void diff_terms(const double2* Nn, double2* S, double2* W, size_t rst, int N, double c) {
+  for (int n0 = 0; n0 < N; n0 += SAVE_BATCH) {
+    double2 x[SAVE_BATCH], p[SAVE_BATCH];
+#pragma unroll
+    for (int u = 0; u < SAVE_BATCH; ++u)
+      if (n0 + u < N) { x[u] = __ldg(Nn + (size_t)(n0 + u) * rst); p[u] = S[(size_t)(n0 + u) * rst]; }
+#pragma unroll
+    for (int u = 0; u < SAVE_BATCH; ++u)
+      if (n0 + u < N) {
+        S[(size_t)(n0 + u) * rst] = x[u];
+        W[(size_t)(n0 + u) * rst] = make_double2(c * (x[u].x - p[u].x), c * (x[u].y - p[u].y));
+      }
+  }
+}
+
 // Predictor (velocity.F90:369-395, codensity.F90:224-234, magnetic.F90:370-408).
 // grid (ceil(H / SOLVE_THREADS), J_NJOB).
 template <int KL>
@@ -460,9 +499,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_predictor(StepArgs a) {
   if (job == J_VPOL) {
     // Pol := NPol ; zerobc ; invX(XGre) ; Pol := YPol vel_Pol + Pol ; zerobc ; invX(XPol) ;
     // vel_gre_adjust (velocity.F90:369-395, 445-465)
+    save_terms(v.Nn, v.S, rst, N);
     auto inA = [&](int n) {
       const double2 x = __ldg(v.Nn + (size_t)n * rst);
-      v.S[(size_t)n * rst] = x;
       return (n == 0 || n == N - 1) ? z2 : x;
     };
     if (l == 0) {
@@ -471,12 +510,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_predictor(StepArgs a) {
     }
     stream_forward<KL>(v.B2, N, inA, w1);
     stream_backward<KL>(v.B2, N, r1, [&](int c, double2 x) { v.W2[(size_t)c * rst] = x; });
-    MultY<KL> my;
-    my.init(v.y1, L, v.X, rst, N);
-    auto inB = [&](int n) {
-      const double2 x = my.apply(n, v.W2[(size_t)n * rst]);
-      return (n == 0 || n == N - 1) ? z2 : x;
-    };
+    multy_rows<KL>(v.y1, L, v.X, v.W2, v.W2, rst, N);  // YPol vel_Pol + Pol, in place
+    auto inB = [&](int n) { return (n == 0 || n == N - 1) ? z2 : v.W2[(size_t)n * rst]; };
     double2 x0 = z2, xN = z2;
     stream_forward<KL>(v.B1, N, inB, w1);
     stream_backward<KL>(v.B1, N, r1, [&](int c, double2 x) {
@@ -495,21 +530,20 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_predictor(StepArgs a) {
     return;
   }
   // other fields: X := Y X + N ; zerobc (+ setbc) ; invX
-  MultY<KL> my;
   const bool solve = (l != 0 || zero);
-  if (solve) my.init(v.y1, L, v.X, rst, N);
-  auto inC = [&](int n) {
-    double2 x = __ldg(v.Nn + (size_t)n * rst);
-    v.S[(size_t)n * rst] = x;
-    if (solve) x = my.apply(n, x);
-    if (n == 0) return make_double2(bc0, 0.0);
-    if (n == N - 1) return make_double2(bcN, 0.0);
-    return x;
-  };
+  save_terms(v.Nn, v.S, rst, N);
   if (!solve) {
-    for (int n = 0; n < N; ++n) v.X[(size_t)n * rst] = inC(n);
+    for (int n = 0; n < N; ++n)
+      v.X[(size_t)n * rst] = n == 0 ? make_double2(bc0, 0.0) : n == N - 1 ? make_double2(bcN, 0.0)
+                                                                         : __ldg(v.Nn + (size_t)n * rst);
     return;
   }
+  multy_rows<KL>(v.y1, L, v.X, v.Nn, v.W1, rst, N);  // Y X + N into W1 (solved in place)
+  auto inC = [&](int n) {
+    if (n == 0) return make_double2(bc0, 0.0);
+    if (n == N - 1) return make_double2(bcN, 0.0);
+    return v.W1[(size_t)n * rst];
+  };
   stream_forward<KL>(v.B1, N, inC, w1);
   stream_backward<KL>(v.B1, N, r1, [&](int c, double2 x) { v.X[(size_t)c * rst] = x; });
 }
@@ -540,12 +574,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_corrector(StepArgs a) {
     // vel_setbc_Tor (Re part; velocity.F90:291-299): only no-slip walls (i_vel_bc <= 2)
     const bool tor10 = job == J_VTOR && l == 1 && a.hm[nh] == 0 && a.vel_bc <= 2;
     const double wr = tor10 ? a.rot[ROT_OMEGA] * a.rtor10[0] : 0.0;
+    // the right-hand side in W1 (the forward pass then overwrites it row by row, in place)
+    diff_terms(v.Nn, v.S, v.W1, rst, N, c);
     auto inC = [&](int n) {
-      const double2 x = __ldg(v.Nn + (size_t)n * rst), p = v.S[(size_t)n * rst];
-      v.S[(size_t)n * rst] = x;
       if (n == 0) return tor10 ? make_double2(wr - v.X[0].x, 0.0) : z2;
       if (n == N - 1) return z2;
-      return make_double2(c * (x.x - p.x), c * (x.y - p.y));
+      return v.W1[(size_t)n * rst];
     };
     // x += d ; dterr sum of d^2 (tim_addcorr, timestep.F90:717-737)
     auto addcorr = [&](int n, double2 d) {
@@ -620,7 +654,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_mag_ic(StepArgs a) {
       const double dre = -(x.y * m_), dim = x.x * m_;
       return make_double2(-om * dre, -om * dim);
     };
-    auto wk = [&](int cc) { return cc < N ? v.W1 + (size_t)cc * rst : v.W2 + (size_t)(cc - N) * rst; };
+    // work rows: the outer core's in W1 (row n at cc = n + Nic - 1), the inner core's in W2
+    auto wk = [&](int cc) { return cc >= Ni - 1 ? v.W1 + (size_t)(cc - (Ni - 1)) * rst : v.W2 + (size_t)cc * rst; };
     if (!CORR) {
       if (l == 0) {  // not solved: the right-hand sides with their boundary rows
         for (int n = 0; n < Ni; ++n) {
@@ -635,22 +670,14 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_mag_ic(StepArgs a) {
         }
       } else {
         // B := Y B + N (both meshes) ; zerobc ; invX
-        icS[(size_t)(Ni - 1) * rst] = icN(Ni - 1);
-        MultY<KL> myo, myi;
-        myo.init(v.y1, L, v.X, rst, N);
-        myi.init(a.icyt + (size_t)k * Ni * (2 * KL + 1) * L + l, L, icX, rst, Ni);
+        for (int n = 0; n < Ni; ++n) icS[(size_t)n * rst] = icN(n);
+        save_terms(v.Nn, v.S, rst, N);
+        multy_rows<KL>(v.y1, L, v.X, v.Nn, v.W1, rst, N);           // outer core: Y B + N
+        multy_rows<KL>(a.icyt + (size_t)k * Ni * (2 * KL + 1) * L + l, L, icX, icS, v.W2, rst, Ni);  // inner
         auto in = [&](int cc) {
-          if (cc < Ni - 1) {
-            const double2 nn = icN(cc);
-            icS[(size_t)cc * rst] = nn;
-            const double2 x = myi.apply(cc, nn);
-            return cc == 0 ? z2 : x;
-          }
+          if (cc < Ni - 1) return cc == 0 ? z2 : *wk(cc);
           const int n = cc - (Ni - 1);
-          double2 x = __ldg(v.Nn + (size_t)n * rst);
-          v.S[(size_t)n * rst] = x;
-          x = myo.apply(n, x);
-          return (n == 0 || n == N - 1) ? z2 : x;
+          return (n == 0 || n == N - 1) ? z2 : *wk(cc);
         };
         stream_forward<KL>(v.B1, NL, in, [&](int cc, double2 x) { *wk(cc) = x; });
         stream_backward<KL>(v.B1, NL, [&](int cc) { return *wk(cc); }, [&](int cc, double2 x) {
@@ -659,17 +686,18 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_mag_ic(StepArgs a) {
         });
       }
     } else {
-      icS[(size_t)(Ni - 1) * rst] = icN(Ni - 1);  // saved whole (tim_nlincorr + copy)
+      // the right-hand side c (N - N_saved) of all NL rows in the work rows (the forward
+      // pass overwrites it in place); the saves N_saved := N of both cores
+      for (int n = 0; n < Ni; ++n) {
+        const double2 nn = icN(n), p = icS[(size_t)n * rst];
+        icS[(size_t)n * rst] = nn;
+        if (n < Ni - 1) *wk(n) = make_double2(c * (nn.x - p.x), c * (nn.y - p.y));
+      }
+      diff_terms(v.Nn, v.S, v.W1, rst, N, c);
       auto in = [&](int cc) {
-        if (cc < Ni - 1) {
-          const double2 nn = icN(cc), p = icS[(size_t)cc * rst];
-          icS[(size_t)cc * rst] = nn;
-          return cc == 0 ? z2 : make_double2(c * (nn.x - p.x), c * (nn.y - p.y));
-        }
+        if (cc < Ni - 1) return cc == 0 ? z2 : *wk(cc);
         const int n = cc - (Ni - 1);
-        const double2 x = __ldg(v.Nn + (size_t)n * rst), p = v.S[(size_t)n * rst];
-        v.S[(size_t)n * rst] = x;
-        return (n == 0 || n == N - 1) ? z2 : make_double2(c * (x.x - p.x), c * (x.y - p.y));
+        return (n == 0 || n == N - 1) ? z2 : *wk(cc);
       };
       auto add = [&](cplx* X, double2 d) {
         const double2 x = *X;
