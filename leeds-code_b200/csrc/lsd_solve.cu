@@ -315,7 +315,7 @@ __device__ __forceinline__ void stream_forward(const Band& B, int N, IN&& in, OU
 // dtbsv (upper, non-unit, bandwidth 2KL; LAPACK column order) on the forward result:
 // for c = N-1..0: x(c) = y(c) / U(c, c); x(c-t) -= x(c) U(c-t, c), t <= 2KL.
 // in(n) supplies y rows in decreasing n; out(c, x) receives x(c) in decreasing c.
-constexpr int SPB = 4;  // rows per batch of the back substitution
+constexpr int SPB = 8;  // rows per batch of the back substitution
 template <int KL, class IN, class OUT>
 __device__ __forceinline__ void stream_backward(const Band& B, int N, IN&& in, OUT&& out) {
   constexpr int K2 = 2 * KL;
