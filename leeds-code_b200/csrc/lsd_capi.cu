@@ -37,7 +37,7 @@ void free_ctx(lsd_ctx* ctx) {
                   ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red, ctx->d_ref, ctx->d_laps,
                   ctx->d_compr1dr, ctx->d_wts, ctx->d_ones, ctx->d_cfl, ctx->d_icr, ctx->d_icdr, ctx->d_icradlap,
                   ctx->d_icr1dr, ctx->d_icintr2dr, ctx->d_icwts, ctx->d_icref, ctx->d_iclaps, ctx->d_iccompr1dr,
-                  ctx->d_icyt, ctx->d_icstate, ctx->d_icsv, ctx->d_rot, ctx->d_gwP0};
+                  ctx->d_icyt, ctx->d_icstate, ctx->d_icsv, ctx->d_rot, ctx->d_gwP0, ctx->d_grescr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -444,6 +444,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   TRY(dalloc(ctx, &ctx->d_info, (size_t)OP_NFAM * L));
   TRY(dalloc(ctx, &ctx->d_gre, (size_t)L * 2 * N)); TRY(dalloc(ctx, &ctx->d_invg, (size_t)L * 4));
   TRY(dalloc(ctx, &ctx->d_gret, (size_t)L * 2 * N));
+  TRY(dalloc(ctx, &ctx->d_grescr, (size_t)L * N));
   const size_t F = (size_t)N * H;
   TRY(dalloc(ctx, &ctx->d_state, LSD_NFIELD * F)); TRY(dalloc(ctx, &ctx->d_nl, LSD_NFIELD * F));
   TRY(dalloc(ctx, &ctx->d_sv, LSD_NFIELD * F));

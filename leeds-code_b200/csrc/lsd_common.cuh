@@ -142,6 +142,7 @@ struct lsd_ctx {
   double *d_gre = nullptr;   // [L][2][N]
   double *d_gret = nullptr;  // [N][2][L]
   double *d_invg = nullptr;  // [L][4]
+  double2 *d_grescr = nullptr;  // [N][L] scratch of k_greens
   bool have_ops = false;
   double op_dt = 0.0;
   // state, nonlinear terms, saved nonlinear terms: [field][N][H] complex
@@ -201,6 +202,7 @@ int lsd_corr(lsd_ctx* ctx);            // corrector solves + dterr (device)
 int lsd_energy_device(lsd_ctx* ctx, double* out);
 int lsd_energy_static(lsd_ctx* ctx, double* out);
 int lsd_coll_to_state_n(lsd_ctx* ctx, int rows, const double* re, const double* im, cplx* out);
+int lsd_launch_greens(lsd_ctx* ctx, int* d_fail);
 int lsd_state_to_coll_n(lsd_ctx* ctx, int rows, const cplx* in, double* re, double* im);
 int lsd_diagnostics_device(lsd_ctx* ctx, double* scalars, double* spectra, double* profiles);
 int lsd_coll_to_state(lsd_ctx* ctx, const double* re, const double* im, cplx* out);

@@ -747,6 +747,46 @@ __global__ void k_rot(double* rot, int corr, double inertia, double implicit, do
   rot[ROT_SV_MAG] = tm;
 }
 
+// Green's functions and influence matrices of the poloidal velocity (velocity.F90:148-168)
+// with the streamed solves on the solve-layout factors: thread l carries both unit
+// right-hand sides (g1 in .x: 1 at r_i; g2 in .y: 1 at r_o) through XGre, zeroes the
+// boundary rows (tim_zerobc) and solves with XPol; the passes work in place on scr [N][L].
+template <int KL>
+__global__ void k_greens(int N, int NL, int L, const double* lus, const int* ipivs, double2* scr, double* gre,
+                         double* gret, double* invg, int* fail) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l < 1 || l >= L) return;
+  constexpr int LD = 3 * KL + 1;
+  Band bg, bp;
+  bg.f = lus + (size_t)OP_VGRE * NL * LD * L + l; bg.piv = ipivs + (size_t)OP_VGRE * NL * L + l;
+  bp.f = lus + (size_t)OP_VPOL * NL * LD * L + l; bp.piv = ipivs + (size_t)OP_VPOL * NL * L + l;
+  bg.L = bp.L = L; bg.LD = bp.LD = LD;
+  double2* w = scr + l;
+  const size_t rst = L;
+  auto unit = [&](int n) { return make_double2(n == 0 ? 1.0 : 0.0, n == N - 1 ? 1.0 : 0.0); };
+  auto rd = [&](int n) { return w[(size_t)n * rst]; };
+  auto wr = [&](int n, double2 x) { w[(size_t)n * rst] = x; };
+  stream_forward<KL>(bg, N, unit, wr);
+  stream_backward<KL>(bg, N, rd, wr);
+  w[0] = make_double2(0.0, 0.0);
+  w[(size_t)(N - 1) * rst] = make_double2(0.0, 0.0);
+  stream_forward<KL>(bp, N, rd, wr);
+  stream_backward<KL>(bp, N, rd, wr);
+  const double2 x0 = w[0], xN = w[(size_t)(N - 1) * rst];
+  double a4[4] = {x0.x, xN.x, x0.y, xN.y};  // invG(i,j) at a4[(i-1)+2(j-1)]
+  if (dev_mat_invert(2, a4, 2) != 0) atomicExch(fail, 4);
+  for (int k = 0; k < 4; ++k) invg[(size_t)l * 4 + k] = a4[k];
+  double* g1 = gre + (size_t)l * 2 * N;
+  double* g2 = g1 + N;
+  for (int n = 0; n < N; ++n) {
+    const double2 g = w[(size_t)n * rst];
+    g1[n] = g.x;
+    g2[n] = g.y;
+    gret[((size_t)n * 2 + 0) * L + l] = g.x;  // [n][2][L] copy for coalesced use in the solves
+    gret[((size_t)n * 2 + 1) * L + l] = g.y;
+  }
+}
+
 // ---- energies: per-(field, category, n) partial sums of w_lm |a|^2 ------------------
 // categories: 0 odd (l-m odd), 1 even, 2 m=0 & l even, 3 m=0   (variables.F90:903-957)
 __global__ void k_norms(int N, int H, const int* hl, const int* hm, const cplx* const* arrs, int narr, double* out) {
@@ -1628,6 +1668,24 @@ __global__ void k_state_to_coll(int N, int H, const cplx* __restrict__ in, doubl
   }
 }
 }  // namespace
+
+int lsd_launch_greens(lsd_ctx* ctx, int* d_fail) {
+  const int N = ctx->N, NL = ctx->NL, L = ctx->L;
+  const int g = ceil_div(L, 32);
+  double2* scr = ctx->d_grescr;
+  cudaStream_t s = ctx->stream;
+  switch (ctx->KL) {
+    case 2: k_greens<2><<<g, 32, 0, s>>>(N, NL, L, ctx->d_lus, ctx->d_ipivs, scr, ctx->d_gre, ctx->d_gret, ctx->d_invg, d_fail); break;
+    case 3: k_greens<3><<<g, 32, 0, s>>>(N, NL, L, ctx->d_lus, ctx->d_ipivs, scr, ctx->d_gre, ctx->d_gret, ctx->d_invg, d_fail); break;
+    case 4: k_greens<4><<<g, 32, 0, s>>>(N, NL, L, ctx->d_lus, ctx->d_ipivs, scr, ctx->d_gre, ctx->d_gret, ctx->d_invg, d_fail); break;
+    case 5: k_greens<5><<<g, 32, 0, s>>>(N, NL, L, ctx->d_lus, ctx->d_ipivs, scr, ctx->d_gre, ctx->d_gret, ctx->d_invg, d_fail); break;
+    case 6: k_greens<6><<<g, 32, 0, s>>>(N, NL, L, ctx->d_lus, ctx->d_ipivs, scr, ctx->d_gre, ctx->d_gret, ctx->d_invg, d_fail); break;
+    default: return lsd_fail(ctx, LSD_EARG, "stencil half-width KL must be 2..6 for the step kernels");
+  }
+  ctx->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return LSD_OK;
+}
 
 int lsd_coll_to_state(lsd_ctx* ctx, const double* re, const double* im, cplx* out) {
   return lsd_coll_to_state_n(ctx, ctx->N, re, im, out);

@@ -4,6 +4,7 @@
 // the radial Chebyshev grid with finite-difference weights and integration weights
 // (meshs.F90:116-419), and the banded time-stepping operators with their LU factors
 // (timestep.F90:47-546, velocity.F90:56-273, codensity.F90:37-119, magnetic.F90:62-282).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 
@@ -308,25 +309,35 @@ __device__ double anel_diag(int fam, int l, int n, int N, const double* r, const
   }
 }
 
-__global__ void k_build_ops(int N, int NL, int KL, int L, const double* r, const double* dr, const double* radlap,
-                            const double* laps, const double* ref, OpParams P, double* lu, int* ipiv, double* y,
-                            int* info) {
-  int l = blockIdx.x * blockDim.x + threadIdx.x;
-  int fam = blockIdx.y;
+// One warp per (family, l): the lanes build the band in shared memory, lane 0 factorises
+// it there (dgbtf2 at shared-memory latency: one matrix per thread on global memory took
+// 1.3 ms per rebuild at L = 128, N = 129), and the lanes write it out.  wpb warps per CTA.
+__global__ void k_build_ops(int N, int NL, int KL, int L, int wpb, const double* r, const double* dr,
+                            const double* radlap, const double* laps, const double* ref, OpParams P, double* lu,
+                            int* ipiv, double* y, int* info) {
+  extern __shared__ double osm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int l = blockIdx.x * wpb + warp;
+  const int fam = blockIdx.y;
   if (l >= L) return;
   const int ld = 3 * KL + 1, ldm = 2 * KL + 1;
-  double* A = lu + ((size_t)fam * L + l) * (size_t)ld * NL;  // NL: the families' row stride
+  double* A = osm + (size_t)warp * ld * N;
+  double* Ag = lu + ((size_t)fam * L + l) * (size_t)ld * NL;  // NL: the families' row stride
   int* ip = ipiv + ((size_t)fam * L + l) * NL;
   const double* rm1 = r + (size_t)2 * N;
   const double* rm2 = r + (size_t)1 * N;
   const size_t band = (size_t)ldm * N;
 #define AX(i, j) A[(size_t)((i) - 1) + (size_t)ld * ((j) - 1)]
 #define MB(B, i, j) (B)[(size_t)((i) - 1) + (size_t)ldm * ((j) - 1)]
-  for (size_t i = 0; i < (size_t)ld * N; ++i) A[i] = 0.0;
+  for (int i = lane; i < ld * N; i += 32) A[i] = 0.0;
+  __syncwarp();
   bool skip_l0 = (fam != OP_COD && fam != OP_COMP);
   if (l == 0 && skip_l0) {  // never solved: keep an identity so the factors are defined
-    for (int j = 1; j <= N; ++j) AX(2 * KL + 1, j) = 1.0;
-    info[fam * L + l] = dev_dgbtf2(N, KL, A, ld, ip);
+    for (int j = 1 + lane; j <= N; j += 32) AX(2 * KL + 1, j) = 1.0;
+    __syncwarp();
+    if (lane == 0) info[fam * L + l] = dev_dgbtf2(N, KL, A, ld, ip);
+    __syncwarp();
+    for (int i = lane; i < ld * N; i += 32) Ag[i] = A[i];
     return;
   }
   const double c1_ = P.c1_[fam], c2_ = P.c2_[fam], c2y = P.c2y[fam];
@@ -340,12 +351,13 @@ __global__ void k_build_ops(int N, int NL, int KL, int L, const double* r, const
                     : fam == OP_MTOR ? LAP_MAGTOR : fam == OP_MPOL ? LAP_MAGPOL : LAP_GRE;
     lap = laps + which * band;
   }
-  for (int j = 1; j <= N; ++j)
+  for (int j = 1 + lane; j <= N; j += 32)
     for (int row = 1; row <= ldm; ++row) {
       double v = MB(lap, row, j);
       AX(KL + row, j) = (fam == OP_MTOR || fam == OP_MPOL) ? 0.0 - c2_ * v : -c2_ * v;
     }
-  for (int n = 1; n <= N; ++n) {
+  __syncwarp();
+  for (int n = 1 + lane; n <= N; n += 32) {
     double t = ll1 * rm2[n - 1];
     if (P.anelastic)
       AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * anel_diag(fam, l, n, N, r, ref, P.Hyp);
@@ -354,69 +366,73 @@ __global__ void k_build_ops(int N, int NL, int KL, int L, const double* r, const
     else
       AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * (t + P.Hyp * t * t);
   }
-  for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = 0.0;
-  for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = 0.0;
-  // boundary rows
-  switch (fam) {
-    case OP_VTOR:  // vel_bc_Tor (velocity.F90:177-201)
-      if (P.vel_bc == 1 || P.vel_bc == 2) AX(2 * KL + 1, 1) = 1.0;
-      else {
-        for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
-        AX(2 * KL + 1, 1) = AX(2 * KL + 1, 1) - rm1[0];
+  __syncwarp();
+  if (lane == 0) {  // boundary rows, then the factorisation
+    for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = 0.0;
+    for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = 0.0;
+    switch (fam) {
+      case OP_VTOR:  // vel_bc_Tor (velocity.F90:177-201)
+        if (P.vel_bc == 1 || P.vel_bc == 2) AX(2 * KL + 1, 1) = 1.0;
+        else {
+          for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
+          AX(2 * KL + 1, 1) = AX(2 * KL + 1, 1) - rm1[0];
+        }
+        if (P.vel_bc == 1 || P.vel_bc == 3) AX(2 * KL + 1, N) = 1.0;
+        else {
+          for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
+          AX(2 * KL + 1, N) = AX(2 * KL + 1, N) - rm1[N - 1];
+        }
+        break;
+      case OP_VPOL: {  // vel_bc_Pol (velocity.F90:207-254); anelastic stress-free adds xi dr
+        const double xi1 = P.anelastic ? ref[N] : 0.0, xiN = P.anelastic ? ref[2 * N - 1] : 0.0;
+        if (P.vel_bc == 1 || P.vel_bc == 2)
+          for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
+        else if (!P.anelastic)
+          for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr + band, KL + 1 + 1 - j, j);
+        else
+          for (int j = 1; j <= 1 + KL; ++j)
+            AX(2 * KL + 1 + 1 - j, j) = MB(dr + band, KL + 1 + 1 - j, j) + xi1 * MB(dr, KL + 1 + 1 - j, j);
+        if (P.vel_bc == 1 || P.vel_bc == 3)
+          for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
+        else if (!P.anelastic)
+          for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr + band, KL + 1 + N - j, j);
+        else
+          for (int j = N - KL; j <= N; ++j)
+            AX(2 * KL + 1 + N - j, j) = MB(dr + band, KL + 1 + N - j, j) + xiN * MB(dr, KL + 1 + N - j, j);
+        break;
       }
-      if (P.vel_bc == 1 || P.vel_bc == 3) AX(2 * KL + 1, N) = 1.0;
-      else {
-        for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
-        AX(2 * KL + 1, N) = AX(2 * KL + 1, N) - rm1[N - 1];
+      case OP_VGRE:  // vel_bc_Gre (velocity.F90:260-267)
+        AX(2 * KL + 1, 1) = 1.0;
+        AX(2 * KL + 1, N) = 1.0;
+        break;
+      case OP_COD:
+      case OP_COMP: {  // cod_bc_C (codensity.F90:85-112)
+        int bc = fam == OP_COD ? P.cod_bc : P.comp_bc;
+        if (bc == 1 || bc == 2) AX(2 * KL + 1, 1) = 1.0;
+        else for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
+        if (bc == 1 || bc == 3) AX(2 * KL + 1, N) = 1.0;
+        else for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
+        break;
       }
-      break;
-    case OP_VPOL: {  // vel_bc_Pol (velocity.F90:207-254); anelastic stress-free adds xi dr
-      const double xi1 = P.anelastic ? ref[N] : 0.0, xiN = P.anelastic ? ref[2 * N - 1] : 0.0;
-      if (P.vel_bc == 1 || P.vel_bc == 2)
+      case OP_MTOR:  // mag_bc_Tor (magnetic.F90:137-192), Ni = 1
+        AX(2 * KL + 1, 1) = 1.0;
+        AX(2 * KL + 1, N) = 1.0;
+        break;
+      case OP_MPOL:  // mag_bc_Pol (magnetic.F90:198-282), insulating, Ni = 1
         for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
-      else if (!P.anelastic)
-        for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr + band, KL + 1 + 1 - j, j);
-      else
-        for (int j = 1; j <= 1 + KL; ++j)
-          AX(2 * KL + 1 + 1 - j, j) = MB(dr + band, KL + 1 + 1 - j, j) + xi1 * MB(dr, KL + 1 + 1 - j, j);
-      if (P.vel_bc == 1 || P.vel_bc == 3)
+        AX(2 * KL + 1, 1) = AX(2 * KL + 1, 1) - rm1[0] * l;
         for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
-      else if (!P.anelastic)
-        for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr + band, KL + 1 + N - j, j);
-      else
-        for (int j = N - KL; j <= N; ++j)
-          AX(2 * KL + 1 + N - j, j) = MB(dr + band, KL + 1 + N - j, j) + xiN * MB(dr, KL + 1 + N - j, j);
-      break;
+        AX(2 * KL + 1, N) = AX(2 * KL + 1, N) + rm1[N - 1] * (l + 1);
+        break;
     }
-    case OP_VGRE:  // vel_bc_Gre (velocity.F90:260-267)
-      AX(2 * KL + 1, 1) = 1.0;
-      AX(2 * KL + 1, N) = 1.0;
-      break;
-    case OP_COD:
-    case OP_COMP: {  // cod_bc_C (codensity.F90:85-112)
-      int bc = fam == OP_COD ? P.cod_bc : P.comp_bc;
-      if (bc == 1 || bc == 2) AX(2 * KL + 1, 1) = 1.0;
-      else for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
-      if (bc == 1 || bc == 3) AX(2 * KL + 1, N) = 1.0;
-      else for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
-      break;
-    }
-    case OP_MTOR:  // mag_bc_Tor (magnetic.F90:137-192), Ni = 1
-      AX(2 * KL + 1, 1) = 1.0;
-      AX(2 * KL + 1, N) = 1.0;
-      break;
-    case OP_MPOL:  // mag_bc_Pol (magnetic.F90:198-282), insulating, Ni = 1
-      for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(dr, KL + 1 + 1 - j, j);
-      AX(2 * KL + 1, 1) = AX(2 * KL + 1, 1) - rm1[0] * l;
-      for (int j = N - KL; j <= N; ++j) AX(2 * KL + 1 + N - j, j) = MB(dr, KL + 1 + N - j, j);
-      AX(2 * KL + 1, N) = AX(2 * KL + 1, N) + rm1[N - 1] * (l + 1);
-      break;
+    info[fam * L + l] = dev_dgbtf2(N, KL, A, ld, ip);
   }
-  info[fam * L + l] = dev_dgbtf2(N, KL, A, ld, ip);
+  __syncwarp();
+  for (int i = lane; i < ld * N; i += 32) Ag[i] = A[i];
   // Y = c2y*Lap ; diag += c1_ - c2y*(l(l+1)/r^2 + Hyp (.)^2)   (tim_mesh_Y / _flayer_Y;
   // anelastic: tim_mesh_vel_Y, tim_mesh_Y, tim_mesh_mag_Tor_Y / _Pol_Y)
   if (fam != OP_VGRE) {
-    for (int j = 1; j <= N; ++j)
+    for (int j = 1 + lane; j <= N; j += 32)
       for (int row = 1; row <= ldm; ++row) {
         double v = c2y * MB(lap, row, j);
         if (row == KL + 1) {
@@ -452,57 +468,35 @@ __global__ void k_lu_transpose(int N, int NL, int icfam, int KL, int L, const do
   for (int row = 0; row < ldm; ++row) yt[(((size_t)fam * N + j) * ldm + row) * L + l] = Y[row];
 }
 
-// Green's functions and influence matrices (velocity.F90:148-168)
-__global__ void k_greens(int N, int NL, int KL, int L, const double* lu, const int* ipiv, double* gre, double* gret,
-                         double* invg, int* fail) {
-  int l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l < 1 || l >= L) return;
-  const int ld = 3 * KL + 1;
-  const double* Agre = lu + ((size_t)OP_VGRE * L + l) * (size_t)ld * NL;
-  const int* pgre = ipiv + ((size_t)OP_VGRE * L + l) * NL;
-  const double* Apol = lu + ((size_t)OP_VPOL * L + l) * (size_t)ld * NL;
-  const int* ppol = ipiv + ((size_t)OP_VPOL * L + l) * NL;
-  double* g1 = gre + (size_t)l * 2 * N;
-  double* g2 = g1 + N;
-  for (int n = 0; n < N; ++n) { g1[n] = 0.0; g2[n] = 0.0; }
-  g1[0] = 1.0;
-  g2[N - 1] = 1.0;
-  dev_dgbtrs1(N, KL, Agre, ld, pgre, g1);
-  dev_dgbtrs1(N, KL, Agre, ld, pgre, g2);
-  g1[0] = 0.0; g1[N - 1] = 0.0; g2[0] = 0.0; g2[N - 1] = 0.0;
-  dev_dgbtrs1(N, KL, Apol, ld, ppol, g1);
-  dev_dgbtrs1(N, KL, Apol, ld, ppol, g2);
-  double a[4] = {g1[0], g1[N - 1], g2[0], g2[N - 1]};  // invG(i,j) at a[(i-1)+2(j-1)]
-  if (dev_mat_invert(2, a, 2) != 0) atomicExch(fail, 4);
-  for (int k = 0; k < 4; ++k) invg[(size_t)l * 4 + k] = a[k];
-  for (int n = 0; n < N; ++n) {  // [n][2][L] copy for coalesced use in the solves
-    gret[((size_t)n * 2 + 0) * L + l] = g1[n];
-    gret[((size_t)n * 2 + 1) * L + l] = g2[n];
-  }
-}
-
 // The field's operators with a conducting inner core, Boussinesq (tim_iclumesh_Tor_X /
 // _Pol_X, timestep.F90:218-344; mag_bc_Tor / mag_bc_Pol, magnetic.F90:137-282): NL = Ni +
 // N - 1 unknowns, 1..Ni on the inner core's mesh and Ni..NL on the outer core's (Ni the
 // inner-core boundary, shared); row 1 the innermost point's condition, row Ni the
 // continuity of dr across the boundary, row NL the insulating exterior.  Also the inner
 // core's Y bands (tim_mesh_Y on its mesh) in the solve layout [k][Ni][2KL+1][L].
-// One thread per (l, k), k = 0 toroidal, 1 poloidal.
-__global__ void k_build_icops(int N, int Ni, int KL, int L, const double* r, const double* dr, const double* radlap,
-                              const double* icr, const double* icdr, const double* icradlap, OpParams P,
-                              double* lu, int* ipiv, double* icyt, int* info) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+// One warp per (l, k), k = 0 toroidal, 1 poloidal, in shared memory as k_build_ops.
+__global__ void k_build_icops(int N, int Ni, int KL, int L, int wpb, const double* r, const double* dr,
+                              const double* radlap, const double* icr, const double* icdr, const double* icradlap,
+                              OpParams P, double* lu, int* ipiv, double* icyt, int* info) {
+  extern __shared__ double osm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int l = blockIdx.x * wpb + warp, k = blockIdx.y;
   if (l >= L) return;
   const int fam = k == 0 ? OP_MTOR : OP_MPOL;
   const int NL = N + Ni - 1, ld = 3 * KL + 1, ldm = 2 * KL + 1;
-  double* A = lu + ((size_t)fam * L + l) * (size_t)ld * NL;
+  double* A = osm + (size_t)warp * ld * NL;
+  double* Ag = lu + ((size_t)fam * L + l) * (size_t)ld * NL;
   int* ip = ipiv + ((size_t)fam * L + l) * NL;
 #define AX(i, j) A[(size_t)((i) - 1) + (size_t)ld * ((j) - 1)]
 #define MB(B, i, j) (B)[(size_t)((i) - 1) + (size_t)ldm * ((j) - 1)]
-  for (size_t i = 0; i < (size_t)ld * NL; ++i) A[i] = 0.0;
+  for (int i = lane; i < ld * NL; i += 32) A[i] = 0.0;
+  __syncwarp();
   if (l == 0) {  // never solved
-    for (int j = 1; j <= NL; ++j) AX(2 * KL + 1, j) = 1.0;
-    info[fam * L + l] = dev_dgbtf2(NL, KL, A, ld, ip);
+    for (int j = 1 + lane; j <= NL; j += 32) AX(2 * KL + 1, j) = 1.0;
+    __syncwarp();
+    if (lane == 0) info[fam * L + l] = dev_dgbtf2(NL, KL, A, ld, ip);
+    __syncwarp();
+    for (int i = lane; i < ld * NL; i += 32) Ag[i] = A[i];
     return;
   }
   const double c1_ = P.c1_[fam], c2_ = P.c2_[fam], c2y = P.c2y[fam];
@@ -512,35 +506,45 @@ __global__ void k_build_icops(int N, int Ni, int KL, int L, const double* r, con
   const double* icrm2 = icr + (size_t)1 * Ni;
   const double* icrm1 = icr + (size_t)2 * Ni;
   const size_t icband = (size_t)ldm * Ni;
-  for (int j = 1; j <= Ni; ++j)
+  // the phases keep the reference's order of additions on the shared column Ni; lanes
+  // split the columns within a phase
+  for (int j = 1 + lane; j <= Ni; j += 32)
     for (int row = 1; row <= ldm; ++row) AX(KL + row, j) = -c2_ * MB(icradlap, row, j);
-  for (int n = 1; n <= Ni; ++n) AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * ll1 * icrm2[n - 1];
-  for (int j = 1; j <= N; ++j)
+  __syncwarp();
+  for (int n = 1 + lane; n <= Ni; n += 32) AX(2 * KL + 1, n) = AX(2 * KL + 1, n) + c1_ + c2_ * ll1 * icrm2[n - 1];
+  __syncwarp();
+  for (int j = 1 + lane; j <= N; j += 32)
     for (int row = 1; row <= ldm; ++row) AX(KL + row, j + Ni - 1) = AX(KL + row, j + Ni - 1) - c2_ * MB(radlap, row, j);
-  for (int n = 1; n <= N; ++n) AX(2 * KL + 1, n + Ni - 1) = AX(2 * KL + 1, n + Ni - 1) + c1_ + c2_ * ll1 * rm2[n - 1];
-  for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = 0.0;
-  for (int j = NL - KL; j <= NL; ++j) AX(2 * KL + 1 + NL - j, j) = 0.0;
-  for (int j = Ni - KL; j <= Ni + KL; ++j) AX(2 * KL + 1 + Ni - j, j) = 0.0;
-  if (k == 0) {  // BTor = 0 at the innermost point and outside
-    AX(2 * KL + 1, 1) = 1.0;
-    AX(2 * KL + 1, NL) = 1.0;
-  } else {  // (dr - l/r) BPol = 0 innermost, (dr + (l+1)/r) BPol = 0 at the outer wall
-    for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(icdr, KL + 1 + 1 - j, j);
-    AX(2 * KL + 1, 1) = AX(2 * KL + 1, 1) - icrm1[0] * l;
-    for (int j = N - KL; j <= N; ++j) {
-      const int j_ = j + Ni - 1;
-      AX(2 * KL + 1 + NL - j_, j_) = MB(dr, KL + 1 + N - j, j);
+  __syncwarp();
+  for (int n = 1 + lane; n <= N; n += 32) AX(2 * KL + 1, n + Ni - 1) = AX(2 * KL + 1, n + Ni - 1) + c1_ + c2_ * ll1 * rm2[n - 1];
+  __syncwarp();
+  if (lane == 0) {  // boundary rows, then the factorisation
+    for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = 0.0;
+    for (int j = NL - KL; j <= NL; ++j) AX(2 * KL + 1 + NL - j, j) = 0.0;
+    for (int j = Ni - KL; j <= Ni + KL; ++j) AX(2 * KL + 1 + Ni - j, j) = 0.0;
+    if (k == 0) {  // BTor = 0 at the innermost point and outside
+      AX(2 * KL + 1, 1) = 1.0;
+      AX(2 * KL + 1, NL) = 1.0;
+    } else {  // (dr - l/r) BPol = 0 innermost, (dr + (l+1)/r) BPol = 0 at the outer wall
+      for (int j = 1; j <= 1 + KL; ++j) AX(2 * KL + 1 + 1 - j, j) = MB(icdr, KL + 1 + 1 - j, j);
+      AX(2 * KL + 1, 1) = AX(2 * KL + 1, 1) - icrm1[0] * l;
+      for (int j = N - KL; j <= N; ++j) {
+        const int j_ = j + Ni - 1;
+        AX(2 * KL + 1 + NL - j_, j_) = MB(dr, KL + 1 + N - j, j);
+      }
+      AX(2 * KL + 1, NL) = AX(2 * KL + 1, NL) + rm1[N - 1] * (l + 1);
     }
-    AX(2 * KL + 1, NL) = AX(2 * KL + 1, NL) + rm1[N - 1] * (l + 1);
+    for (int j = 2; j <= 1 + KL; ++j) {  // dr continuous across the inner-core boundary
+      const int j_ = j + Ni - 1;
+      AX(2 * KL + 1 + Ni - j_, j_) = MB(dr, KL + 1 + 1 - j, j);
+    }
+    for (int j = Ni - KL; j <= Ni - 1; ++j) AX(2 * KL + 1 + Ni - j, j) = -MB(icdr, KL + 1 + Ni - j, j);
+    AX(2 * KL + 1, Ni) = MB(dr, KL + 1, 1) - MB(icdr, KL + 1, Ni);
+    info[fam * L + l] = dev_dgbtf2(NL, KL, A, ld, ip);
   }
-  for (int j = 2; j <= 1 + KL; ++j) {  // dr continuous across the inner-core boundary
-    const int j_ = j + Ni - 1;
-    AX(2 * KL + 1 + Ni - j_, j_) = MB(dr, KL + 1 + 1 - j, j);
-  }
-  for (int j = Ni - KL; j <= Ni - 1; ++j) AX(2 * KL + 1 + Ni - j, j) = -MB(icdr, KL + 1 + Ni - j, j);
-  AX(2 * KL + 1, Ni) = MB(dr, KL + 1, 1) - MB(icdr, KL + 1, Ni);
-  info[fam * L + l] = dev_dgbtf2(NL, KL, A, ld, ip);
-  for (int j = 1; j <= Ni; ++j)  // tim_mesh_Y on the inner core's mesh
+  __syncwarp();
+  for (int i = lane; i < ld * NL; i += 32) Ag[i] = A[i];
+  for (int j = 1 + lane; j <= Ni; j += 32)  // tim_mesh_Y on the inner core's mesh
     for (int row = 1; row <= ldm; ++row) {
       double v = c2y * MB(icradlap, row, j);
       if (row == KL + 1) {
@@ -645,22 +649,36 @@ int lsd_build_operators(lsd_ctx* ctx) {
   CUDA_TRY(cudaMalloc(&d_fail, sizeof(int)));
   CUDA_TRY(cudaMemsetAsync(d_fail, 0, sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(ctx->d_y, 0, sizeof(double) * OP_NFAM * N * (2 * KL + 1) * L, s));
-  dim3 g(ceil_div(L, 32), OP_NFAM);
   const int NL = ctx->NL, Ni = ctx->Nic;
-  k_build_ops<<<g, 32, 0, s>>>(N, NL, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_laps, ctx->d_ref, P,
-                               ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_info);
+  // one warp per operator, its band in shared memory: up to four per CTA within 200 KB
+  auto warps_for = [&](int cols) {
+    const size_t per = sizeof(double) * (size_t)(3 * KL + 1) * cols;
+    return (int)std::min<size_t>(4, (size_t)(200 * 1024) / per);
+  };
+  const int wpb = warps_for(N), wpbi = warps_for(NL);
+  if (wpb < 1 || wpbi < 1)
+    return lsd_fail(ctx, LSD_EARG, "operator build: the band of one operator exceeds 200 KB of shared memory");
+  const size_t smem = sizeof(double) * (size_t)(3 * KL + 1) * N * wpb;
+  const size_t smemi = sizeof(double) * (size_t)(3 * KL + 1) * NL * wpbi;
+  CUDA_TRY(cudaFuncSetAttribute(k_build_ops, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 g(ceil_div(L, wpb), OP_NFAM);
+  k_build_ops<<<g, 32 * wpb, smem, s>>>(N, NL, KL, L, wpb, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_laps,
+                                        ctx->d_ref, P, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_info);
   if (Ni > 1) {  // the field families coupled to the inner core
-    k_build_icops<<<dim3(ceil_div(L, 32), 2), 32, 0, s>>>(N, Ni, KL, L, ctx->d_r, ctx->d_dr, ctx->d_radlap,
-                                                          ctx->d_icr, ctx->d_icdr, ctx->d_icradlap, P, ctx->d_lu,
-                                                          ctx->d_ipiv, ctx->d_icyt, ctx->d_info);
+    CUDA_TRY(cudaFuncSetAttribute(k_build_icops, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemi));
+    k_build_icops<<<dim3(ceil_div(L, wpbi), 2), 32 * wpbi, smemi, s>>>(
+        N, Ni, KL, L, wpbi, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_icr, ctx->d_icdr, ctx->d_icradlap, P,
+        ctx->d_lu, ctx->d_ipiv, ctx->d_icyt, ctx->d_info);
     ctx->launches++;
   }
   dim3 gt(ceil_div(L, 64), NL, OP_NFAM);
   k_lu_transpose<<<gt, 64, 0, s>>>(N, NL, Ni > 1 ? 1 : 0, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_lus,
                                    ctx->d_ipivs, ctx->d_yt);
   CUDA_TRY(cudaMemsetAsync(ctx->d_gret, 0, sizeof(double) * 2 * N * L, s));
-  k_greens<<<ceil_div(L, 32), 32, 0, s>>>(N, NL, KL, L, ctx->d_lu, ctx->d_ipiv, ctx->d_gre, ctx->d_gret, ctx->d_invg,
-                                          d_fail);
+  {
+    int rc = lsd_launch_greens(ctx, d_fail);  // on the solve-layout factors
+    if (rc) { cudaFree(d_fail); return rc; }
+  }
   // the step's dt for rot_predictor / rot_corrector, read on the device
   CUDA_TRY(cudaMemcpyAsync(ctx->d_rot + ROT_DT, &ctx->dt, sizeof(double), cudaMemcpyHostToDevice, s));
   ctx->launches += 3;
