@@ -145,3 +145,32 @@ def test_state_file_round_trip_inner_core(tmp_path):
     assert t == 0.25 and dt == 1e-5 and pkg.state.load_rotation(p) == -13.3
     for f, (re, im) in st.items():
         assert np.array_equal(out[f][0], re) and np.array_equal(out[f][1], im), f
+
+
+def test_state_file_radial_interpolation(tmp_path):
+    """load_state onto a run with other N and Nic (io_interp_wts / io_interp): smooth radial
+    profiles come back to 1e-6 at the points of the [0, 1] mapping, a file on the run's own
+    grid exactly."""
+    cfg = syn.config_inner_core(L=8, N=33, Nic=17)
+    l, m_, _ = syn.folded_harmonics(cfg.L, cfg.M, cfg.Mp)
+    r = syn.chebyshev_grid(cfg.N, cfg.rratio, cfg.alpha)
+    ric = syn.inner_core_grid(cfg.Nic, cfg.rratio)
+    amp = np.arange(1, len(l) + 1, dtype=np.float64)[:, None]
+    f_oc = lambda x: np.sin(2.0 * x) * np.exp(-x)
+    f_ic = lambda x: x ** 2 * np.cos(x)
+    st = {capi.VEL_TOR: (amp * f_oc(r)[None, :], -amp * f_oc(r)[None, :]),
+          capi.MAG_IC_TOR: (amp * f_ic(ric)[None, :], amp * f_ic(ric)[None, :])}
+    p = str(tmp_path / "state.cdf")
+    pkg.state.save_state(p, st, cfg.L, cfg.M, cfg.Mp, r, ric, 0.0, 1e-5, {})
+    r2 = syn.chebyshev_grid(25, cfg.rratio, cfg.alpha)
+    ric2 = syn.inner_core_grid(11, cfg.rratio)
+    out, _, _, _ = pkg.state.load_state(p, cfg.L, cfg.M, cfg.Mp, 25, r_expected=r2, Nic=11, ric_expected=ric2)
+    err_oc = np.abs(out[capi.VEL_TOR][0] - amp * f_oc(r2)[None, :]).max() / amp.max()
+    # both grids are mapped onto [0, 1] (io.F90:1377-1378): the inner core's first point
+    # depends on Nic, so the run's point t lands on the file's radius ric[0] + t (ric[-1] - ric[0])
+    t = (ric2 - ric2[0]) / (ric2[-1] - ric2[0])
+    err_ic = np.abs(out[capi.MAG_IC_TOR][0] - amp * f_ic(ric[0] + t * (ric[-1] - ric[0]))[None, :]).max() / amp.max()
+    assert err_oc < 1e-6 and err_ic < 1e-6, (err_oc, err_ic)
+    same, _, _, _ = pkg.state.load_state(p, cfg.L, cfg.M, cfg.Mp, cfg.N, r_expected=r, Nic=cfg.Nic,
+                                         ric_expected=ric)
+    assert np.array_equal(same[capi.VEL_TOR][0], st[capi.VEL_TOR][0])
