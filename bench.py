@@ -14,7 +14,10 @@ value  = timesteps/s over all ranks (independent replicas, one per GPU, no colle
          over ranks.  The per-step working set (theta-Fourier buffers ~0.8 GB) is far
          larger than the 126 MB L2, so no flush is needed between steps.
 e2e    = the same metric through the public API with host buffers: every step uploads
-         the five state fields from host memory, steps, and reads the energies back.
+         the five state fields from pinned host memory, steps, and reads the energies back;
+         the uploads are streamed (lsd_stage_coll on the copy stream while the step before
+         runs, lsd_commit_staged before the step); serial_value: upload, step and read back
+         one after another (lsd_set_coll).
 roofline: the dominant phase of the step (CUDA-event phase timings), algorithmic
          bytes or flops per launch over its measured duration.
 cpu_baseline: the CPU oracle (C++ restatement of the reference path, OpenMP over shells
@@ -293,9 +296,26 @@ def run_ours(args, rank, world, local_rank, dist):
         ctx.step(1)
         ctx.energies()
         ctx.synchronize()
+        # (a) one call after another: upload (lsd_set_coll), step, energies
         t0 = time.perf_counter()
         for _ in range(ne):
             ctx.load_fields(pinned)
+            ctx.step(1)
+            ctx.energies()
+        ctx.synchronize()
+        res["e2e_serial_s"] = (time.perf_counter() - t0) / ne
+        # (b) streamed inputs: each step's fields are staged (lsd_stage_coll, copy stream)
+        # while the step before runs, committed (lsd_commit_staged), stepped, energies read;
+        # every timed iteration uploads one state, as in (a)
+        ctx.stage_fields(pinned)
+        ctx.commit_staged()
+        ctx.step(1)
+        ctx.stage_fields(pinned)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            ctx.commit_staged()
+            ctx.stage_fields(pinned)
             ctx.step(1)
             ctx.energies()
         ctx.synchronize()
@@ -332,6 +352,7 @@ def run_ours(args, rank, world, local_rank, dist):
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "per-step working set ~1.9 GB >> 126 MB L2 (no flush)"},
         "e2e": {"value": world / r["e2e_s"], "unit": "timesteps/s", "h2d_bytes_per_step": r["h2d"],
+                "serial_value": world / r["e2e_serial_s"],
                 "d2h_bytes_per_step": r["d2h"]},
         "gpu_launches": r["launches"],
         "roofline": {k: r["roofline"][k] for k in ("bound", "achieved", "peak", "unit", "frac")},

@@ -200,6 +200,17 @@ int lsd_legendre_table(const lsd_ctx* ctx, int which, double* out);
  * (io_load_state, io.F90:349-483) and the refresh before output (io_write2files). */
 int lsd_set_coll(lsd_ctx* ctx, int field, const double* re, const double* im);
 int lsd_get_coll(lsd_ctx* ctx, int field, double* re, double* im);
+/* Streamed inputs (no counterpart in the reference, whose state is host memory): the next
+ * state can cross PCIe while the device steps.  lsd_stage_coll enqueues the host-to-device
+ * copy of one field (coll layout, as lsd_set_coll) into a staging buffer on the context's
+ * copy stream and returns without waiting (pinned host memory makes the copy asynchronous;
+ * the host buffer must stay unchanged until a call that waits for the context's work --
+ * lsd_step, lsd_energies, lsd_get_coll -- has returned after the commit);
+ * lsd_commit_staged makes every field staged since the previous commit the state, on the
+ * compute stream after their copies.  Two staging sets alternate, so fields for the next
+ * commit can be staged while the step after a commit runs. */
+int lsd_stage_coll(lsd_ctx* ctx, int field, const double* re, const double* im);
+int lsd_commit_staged(lsd_ctx* ctx);
 /* Nonlinear term of the last evaluation (LSD_N_*), coll layout. */
 int lsd_get_nonlinear(lsd_ctx* ctx, int which, double* re, double* im);
 /* tim_t, tim_dt; setting dt rebuilds the operators (vel/cod/mag_matrices). */

@@ -34,7 +34,7 @@ void free_ctx(lsd_ctx* ctx) {
                   ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,
                   ctx->d_dr, ctx->d_r1dr, ctx->d_radlap, ctx->d_intr2dr, ctx->d_lu, ctx->d_lus, ctx->d_y, ctx->d_yt,
                   ctx->d_ipiv, ctx->d_ipivs, ctx->d_info, ctx->d_gre, ctx->d_gret, ctx->d_invg, ctx->d_state, ctx->d_nl,
-                  ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red, ctx->d_ref, ctx->d_laps,
+                  ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red, ctx->d_cpart, ctx->d_ref, ctx->d_laps,
                   ctx->d_compr1dr, ctx->d_wts, ctx->d_ones, ctx->d_cfl, ctx->d_icr, ctx->d_icdr, ctx->d_icradlap,
                   ctx->d_icr1dr, ctx->d_icintr2dr, ctx->d_icwts, ctx->d_icref, ctx->d_iclaps, ctx->d_iccompr1dr,
                   ctx->d_icyt, ctx->d_icstate, ctx->d_icsv, ctx->d_rot, ctx->d_gwP0, ctx->d_grescr};
@@ -44,6 +44,13 @@ void free_ctx(lsd_ctx* ctx) {
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  if (ctx->d_stage) cudaFree(ctx->d_stage);
+  for (int k = 0; k < 2; ++k) {
+    if (ctx->ev_staged[k]) cudaEventDestroy(ctx->ev_staged[k]);
+    if (ctx->ev_committed[k]) cudaEventDestroy(ctx->ev_committed[k]);
+  }
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->stream && ctx->owns_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -434,8 +441,8 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
     CTRY(cudaMemset(ctx->d_icstate, 0, sizeof(cplx) * 2 * Ni * H));
     CTRY(cudaMemset(ctx->d_icsv, 0, sizeof(cplx) * 2 * Ni * H));
   }
-  TRY(dalloc(ctx, &ctx->d_rot, (size_t)ROT_NSLOT));
-  CTRY(cudaMemset(ctx->d_rot, 0, sizeof(double) * ROT_NSLOT));
+  TRY(dalloc(ctx, &ctx->d_rot, (size_t)ROT_NSLOT + 4 * ctx->HB));  // + the torque sums per half-row
+  CTRY(cudaMemset(ctx->d_rot, 0, sizeof(double) * (ROT_NSLOT + 4 * ctx->HB)));
   TRY(dalloc(ctx, &ctx->d_gwP0, Th));
   {  // rot_precompute (rotation.F90:20-33): 8 pi / 15 r_i^5, r_i = rratio / (1 - rratio)
     const double ri = c.rratio / (1.0 - c.rratio), r2 = ri * ri, r4 = r2 * r2;
@@ -464,6 +471,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   }
   TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * ctx->HB * NM * 4));
   TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
+  TRY(dalloc(ctx, &ctx->d_cpart, (size_t)8 * ((H + 31) / 32)));
   TRY(dalloc(ctx, &ctx->d_cfl, (size_t)2 * N + 1));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));
   ctx->h_pin_bytes = std::max(sizeof(cplx) * F * 3, sizeof(double) * 16);
@@ -555,6 +563,69 @@ static cplx* ic_field(lsd_ctx* ctx, int field) {
   if (ctx->Nic <= 1 || (field != LSD_MAG_IC_TOR && field != LSD_MAG_IC_POL)) return nullptr;
   return ctx->d_icstate + (size_t)(field - LSD_MAG_IC_TOR) * ctx->Nic * ctx->H;
 }
+// ---- staged uploads ---------------------------------------------------------------------
+// Staging slots: the six outer-core fields, then the inner core's two (Nic rows each).
+static const int STAGE_SLOTS = LSD_NFIELD + 2;
+static int stage_setup(lsd_ctx* ctx) {
+  if (ctx->d_stage) return LSD_OK;
+  CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k) {
+    CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_staged[k], cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_committed[k], cudaEventDisableTiming));
+  }
+  const size_t F = (size_t)ctx->N * ctx->H;
+  CUDA_TRY(cudaMalloc(&ctx->d_stage, sizeof(double) * 2 * STAGE_SLOTS * 2 * F));
+  return LSD_OK;
+}
+static double* stage_ptr(lsd_ctx* ctx, int set, int slot) {
+  const size_t F = (size_t)ctx->N * ctx->H;
+  return ctx->d_stage + ((size_t)set * STAGE_SLOTS + slot) * 2 * F;
+}
+
+int lsd_stage_coll(lsd_ctx* ctx, int field, const double* re, const double* im) {
+  if (!ctx || !re || !im) return LSD_EARG;
+  const bool ic = field == LSD_MAG_IC_TOR || field == LSD_MAG_IC_POL;
+  if ((ic && ctx->Nic <= 1) || (!ic && (field < 0 || field >= LSD_NFIELD))) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  int rc = stage_setup(ctx);
+  if (rc) return rc;
+  const int set = ctx->stage_set;
+  if (ctx->stage_mask[set] == 0u)  // the set's buffers are free once its last commit has run
+    CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_committed[set], 0));
+  const size_t n = (size_t)(ic ? ctx->Nic : ctx->N) * ctx->H;
+  double* dst = stage_ptr(ctx, set, field);
+  CUDA_TRY(cudaMemcpyAsync(dst, re, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->copy_stream));
+  CUDA_TRY(cudaMemcpyAsync(dst + n, im, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->copy_stream));
+  ctx->stage_mask[set] |= 1u << field;
+  return LSD_OK;
+}
+
+int lsd_commit_staged(lsd_ctx* ctx) {
+  if (!ctx) return LSD_EARG;
+  const int set = ctx->stage_set;
+  if (!ctx->d_stage || ctx->stage_mask[set] == 0u)
+    return lsd_fail(ctx, LSD_ESTATE, "lsd_commit_staged: no field staged since the last commit");
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  CUDA_TRY(cudaEventRecord(ctx->ev_staged[set], ctx->copy_stream));
+  CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_staged[set], 0));
+  const size_t F = (size_t)ctx->N * ctx->H;
+  for (int f = 0; f < STAGE_SLOTS; ++f) {
+    if (!(ctx->stage_mask[set] & (1u << f))) continue;
+    const bool ic = f >= LSD_NFIELD;
+    const int rows = ic ? ctx->Nic : ctx->N;
+    const size_t n = (size_t)rows * ctx->H;
+    const double* src = stage_ptr(ctx, set, f);
+    cplx* out = ic ? ctx->d_icstate + (size_t)(f - LSD_MAG_IC_TOR) * ctx->Nic * ctx->H : ctx->d_state + f * F;
+    int rc = lsd_coll_to_state_n(ctx, rows, src, src + n, out);
+    if (rc) return rc;
+  }
+  CUDA_TRY(cudaEventRecord(ctx->ev_committed[set], ctx->stream));
+  ctx->stage_mask[set] = 0u;
+  ctx->stage_set = 1 - set;
+  ctx->have_eval = false;
+  return LSD_OK;
+}
+
 int lsd_set_coll(lsd_ctx* ctx, int field, const double* re, const double* im) {
   if (!ctx || !re || !im) return LSD_EARG;
   if (cplx* ic = ic_field(ctx, field)) {
@@ -1196,6 +1267,7 @@ int lsd_synchronize(lsd_ctx* ctx) {
   if (!ctx) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (ctx->copy_stream) CUDA_TRY(cudaStreamSynchronize(ctx->copy_stream));
   if (ctx->oz) return lsd_ozaki_check(ctx);
   return LSD_OK;
 }

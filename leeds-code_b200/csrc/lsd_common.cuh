@@ -93,6 +93,14 @@ struct lsd_ctx {
   long long launches = 0;
   std::string err;
   bool owns_stream = false;
+  // staged uploads (lsd_stage_coll / lsd_commit_staged): a copy stream, two sets of staging
+  // buffers [set][field slot][2 (re, im)][N H] doubles, the fields staged in each set, and
+  // events ordering copies, commits and re-use
+  cudaStream_t copy_stream = nullptr;
+  double* d_stage = nullptr;
+  unsigned stage_mask[2] = {0u, 0u};
+  int stage_set = 0;
+  cudaEvent_t ev_staged[2] = {nullptr, nullptr}, ev_committed[2] = {nullptr, nullptr};
 
   // host layout
   std::vector<int> hl, hm, hs, thm, mcount, mstart, mlen;
@@ -161,6 +169,7 @@ struct lsd_ctx {
   size_t h_pin_bytes = 0;
   // reductions
   double *d_red = nullptr;   // small reduction area
+  double *d_cpart = nullptr; // corrector: per-warp sums of squares [8][ceil(H / 32)]
   double *h_red = nullptr;   // pinned mirror
   // time
   double t = 0.0, dt = 0.0, dterr = 0.0, corr_dt = 0.0, lasterr = 1e99, cfl_dt = 0.0;

@@ -371,7 +371,8 @@ struct ProdConst {
   const double* ref;  // [7][N] reference state (anelastic)
   unsigned long long* cflmax;  // variable dt: per-shell CFL maxima [N][2] (bits of doubles >= 0), or null
   const int* bin2c;   // FFT bin -> m-counter (M entries)
-  double* rotsum;     // inner-core rotation: the two torque surface sums (shell 0), or null
+  double* rotsum;     // inner-core rotation: per half-row h the two torque surface sums of
+                      // shell 0 at [2 h], [2 h + 1] (k_rot adds them up), or null
   const double* gwP0; // Gauss weight x P_0^0 / 2 per theta row
   double rotS;        // -2 / r_i
   int L;
@@ -611,14 +612,18 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
 #pragma unroll
     for (int q = 0; q < NF_OUT; ++q) rows[(size_t)(q * 2 + r) * RS + pos] = out[q];
   }
-  if (torque) {
+  if (torque) {  // this CTA's two sums, in a fixed order, into its slots of rotsum
+    __shared__ double tq[2][PROD_THREADS / 32];
     for (int o = 16; o > 0; o >>= 1) {
       tv += __shfl_down_sync(0xffffffffu, tv, o);
       tm += __shfl_down_sync(0xffffffffu, tm, o);
     }
-    if ((tid & 31) == 0) {
-      atomicAdd(pc.rotsum, tv);
-      atomicAdd(pc.rotsum + 1, tm);
+    if ((tid & 31) == 0) { tq[0][tid >> 5] = tv; tq[1][tid >> 5] = tm; }
+    __syncthreads();
+    if (tid < 2) {
+      double t = 0.0;
+      for (int w = 0; w < PROD_THREADS / 32; ++w) t = t + tq[tid][w];
+      pc.rotsum[2 * h + tid] = t;
     }
   }
   if constexpr (HAS_UB) {
@@ -912,7 +917,7 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.L = ctx->L;
   pc.bin2c = ctx->d_bin2c;
   pc.cflmax = c.timestep < 0 ? (unsigned long long*)ctx->d_cfl : nullptr;
-  pc.rotsum = c.rot_tstep ? ctx->d_rot + ROT_SUM_VEL : nullptr;
+  pc.rotsum = c.rot_tstep ? ctx->d_rot + ROT_NSLOT : nullptr;
   pc.gwP0 = ctx->d_gwP0;
   pc.rotS = -2.0 / (c.rratio / (1.0 - c.rratio));  // r(1,1) = r_i
   const bool comp = c.comp_tstep != 0;

@@ -230,6 +230,8 @@ struct StepArgs {
   double qi, qo, qi_comp, qo_comp;
   int comp;
   double* red;  // corrector: [8] sums of squares
+  double* cpart;  // corrector: the per-warp sums [8][nwarp] that k_cgce_sums adds up
+  int nwarp;      // ceil(H / 32)
   int NL;       // rows per operator in lus / ipivs (N + Nic - 1)
   int Nic;      // inner-core points (> 1: conducting, the field families are coupled)
   cplx* icstate;       // [2][Nic][H] mag_icTor, mag_icPol
@@ -395,7 +397,7 @@ __device__ __forceinline__ void multy_rows(const double* y, int L, const double2
   }
 }
 
-__device__ __forceinline__ void warp_block_add(double v, double* target);
+__device__ __forceinline__ void warp_partial(double v, const StepArgs& a, int slot);
 
 // per-thread view of one field's columns and this degree's operators
 struct ColView {
@@ -548,9 +550,23 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_predictor(StepArgs a) {
   stream_backward<KL>(v.B1, N, r1, [&](int c, double2 x) { v.X[(size_t)c * rst] = x; });
 }
 
-__device__ __forceinline__ void warp_block_add(double v, double* target) {
+// the warp's sum of v (harmonics 32 w .. 32 w + 31) into its own slot of the corrector's
+// partials: the sums reach k_cgce_sums in a fixed order, so the corrector norm -- and the
+// timestep the norm controls -- are the same bits on every run
+__device__ __forceinline__ void warp_partial(double v, const StepArgs& a, int slot) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(target, v);
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if ((threadIdx.x & 31) == 0 && w < a.nwarp) a.cpart[(size_t)slot * a.nwarp + w] = v;  // w >= nwarp: no harmonic
+}
+
+// red[s] = the sum of the per-warp partials of slot s; one warp per slot, lanes over the
+// warps in a fixed stride, then a fixed shuffle tree
+__global__ void k_cgce_sums(const double* part, int nwarp, double* red) {
+  const int s = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double v = 0.0;
+  for (int w = lane; w < nwarp; w += 32) v = v + part[(size_t)s * nwarp + w];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) red[s] = v;
 }
 
 // Corrector (velocity.F90:413-439, codensity.F90:240-259, magnetic.F90:414-461)
@@ -623,8 +639,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_corrector(StepArgs a) {
     if ((job == J_MTOR || job == J_MPOL) && l != 0) ssic = x0.x * x0.x + x0.y * x0.y;  // inner-core copy (Ni = 1)
   }
   int slot = job == J_VTOR ? 0 : job == J_VPOL ? 1 : job == J_COD ? 2 : job == J_COMP ? 3 : job == J_MTOR ? 4 : 6;
-  warp_block_add(ss, a.red + slot);
-  if (job == J_MTOR || job == J_MPOL) warp_block_add(ssic, a.red + slot + 1);
+  warp_partial(ss, a, slot);
+  if (job == J_MTOR || job == J_MPOL) warp_partial(ssic, a, slot + 1);
 }
 
 // The field with a conducting inner core (mag_predictor / mag_corrector, magnetic.F90:370-461;
@@ -719,18 +735,26 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_mag_ic(StepArgs a) {
     }
   }
   if (CORR) {  // red slots 4 bTor, 5 bicTor, 6 bPol, 7 bicPol
-    warp_block_add(ss, a.red + (k == 0 ? 4 : 6));
-    warp_block_add(ssic, a.red + (k == 0 ? 5 : 7));
+    warp_partial(ss, a, k == 0 ? 4 : 6);
+    warp_partial(ssic, a, k == 0 ? 5 : 7);
   }
 }
 
 // rot_predictor / rot_corrector (rotation.F90:40-87) with the torques of non_rotation
-// (nonlinear.F90:479-538) from k_products' surface sums; one thread.  The rate of the
-// evaluation is kept for the inner core's nonlinear term of the solves that follow.
-__global__ void k_rot(double* rot, int corr, double inertia, double implicit, double Ph, double vfac, double mfac,
-                      int vel_on, int mag_on, int force0) {
+// (nonlinear.F90:479-538) from k_products' surface sums (np half-rows' pairs after the
+// ROT_NSLOT slots, added here in order); one thread.  The rate of the evaluation is kept
+// for the inner core's nonlinear term of the solves that follow.
+__global__ void k_rot(double* rot, int np, int corr, double inertia, double implicit, double Ph, double vfac,
+                      double mfac, int vel_on, int mag_on, int force0) {
   if (threadIdx.x != 0) return;
   const double PI = 3.1415926535897931;
+  double sv = 0.0, sm = 0.0;
+  for (int h = 0; h < np; ++h) {
+    sv = sv + rot[ROT_NSLOT + 2 * h];
+    sm = sm + rot[ROT_NSLOT + 2 * h + 1];
+  }
+  rot[ROT_SUM_VEL] = sv;
+  rot[ROT_SUM_MAG] = sm;
   rot[ROT_OMEGA_EVAL] = rot[ROT_OMEGA];
   const double tv = vel_on ? (rot[ROT_SUM_VEL] * 4.0 * PI / Ph) * vfac : 0.0;  // tra_surfintegral's 4 pi / Ph
   const double tm = mag_on ? (rot[ROT_SUM_MAG] * 4.0 * PI / Ph) * mfac : 0.0;
@@ -787,27 +811,38 @@ __global__ void k_greens(int N, int NL, int L, const double* lus, const int* ipi
   }
 }
 
-// ---- energies: per-(field, category, n) partial sums of w_lm |a|^2 ------------------
+// ---- energies: per-(field, category, n) sums of w_lm |a|^2 ----------------------------
 // categories: 0 odd (l-m odd), 1 even, 2 m=0 & l even, 3 m=0   (variables.F90:903-957)
-__global__ void k_norms(int N, int H, const int* hl, const int* hm, const cplx* const* arrs, int narr, double* out) {
-  int nh = blockIdx.x * blockDim.x + threadIdx.x;
-  int n = blockIdx.y;
-  int k = blockIdx.z;
-  double f = 0.0;
-  int l = 0, m_ = 0;
-  if (nh < H) {
-    l = hl[nh]; m_ = hm[nh];
+// One CTA per (n, field): each thread strides over the harmonics and the CTA reduces in a
+// fixed tree, so the sums (and every diagnostic built on them) are the same bits on every
+// call for the same state.
+constexpr int NORM_THREADS = 256;
+__global__ void __launch_bounds__(NORM_THREADS) k_norms(int N, int H, const int* hl, const int* hm,
+                                                        const cplx* const* arrs, double* out) {
+  const int n = blockIdx.x, k = blockIdx.y;
+  const double2* a = arrs[k] + (size_t)n * H;
+  double c[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int nh = threadIdx.x; nh < H; nh += NORM_THREADS) {
+    const int l = hl[nh], m_ = hm[nh];
     double w = 4.0 * 3.1415926535897931 / (double)(2 * l + 1);
     if (m_ != 0) w = 4.0 * w;
-    double2 v = arrs[k][(size_t)n * H + nh];
-    f = w * (v.x * v.x + v.y * v.y);
+    const double2 v = a[nh];
+    const double f = w * (v.x * v.x + v.y * v.y);
+    c[((l - m_) & 1) ? 0 : 1] += f;
+    if (m_ == 0) {
+      if ((l & 1) == 0) c[2] += f;
+      c[3] += f;
+    }
   }
-  double c[4];
-  c[0] = (nh < H && ((l - m_) % 2 + 2) % 2 == 1) ? f : 0.0;
-  c[1] = (nh < H && ((l - m_) % 2 + 2) % 2 == 0) ? f : 0.0;
-  c[2] = (nh < H && m_ == 0 && l % 2 == 0) ? f : 0.0;
-  c[3] = (nh < H && m_ == 0) ? f : 0.0;
-  for (int q = 0; q < 4; ++q) warp_block_add(c[q], out + ((size_t)k * 4 + q) * N + n);
+  __shared__ double red[4][NORM_THREADS];
+  for (int q = 0; q < 4; ++q) red[q][threadIdx.x] = c[q];
+  __syncthreads();
+  for (int h = NORM_THREADS / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h)
+      for (int q = 0; q < 4; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[((size_t)k * 4 + threadIdx.x) * N + n] = red[threadIdx.x][0];
 }
 
 // ---- batched banded factorisation / solve (LAPACK band storage per matrix) ------------
@@ -873,6 +908,7 @@ StepArgs step_args(lsd_ctx* ctx) {
   a.qi = ctx->cfg.qi; a.qo = ctx->cfg.qo; a.qi_comp = ctx->cfg.qi_comp; a.qo_comp = ctx->cfg.qo_comp;
   a.comp = ctx->cfg.comp_tstep;
   a.red = ctx->d_red;
+  a.cpart = ctx->d_cpart; a.nwarp = (ctx->H + 31) / 32;
   a.NL = ctx->NL; a.Nic = ctx->Nic;
   a.icstate = ctx->d_icstate; a.icsv = ctx->d_icsv; a.icyt = ctx->d_icyt;
   a.rot = ctx->d_rot;
@@ -946,7 +982,7 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
   cplx* fa = fo + nsyn * FF;  // the 7 (8) product fields, in the analysis layout
   const bool vardt = ctx->cfg.timestep < 0;
   if (vardt) CUDA_TRY(cudaMemsetAsync(ctx->d_cfl, 0, sizeof(double) * 2 * ctx->N, s));
-  if (ctx->cfg.rot_tstep) CUDA_TRY(cudaMemsetAsync(ctx->d_rot + ROT_SUM_VEL, 0, sizeof(double) * 2, s));
+  if (ctx->cfg.rot_tstep) CUDA_TRY(cudaMemsetAsync(ctx->d_rot + ROT_NSLOT, 0, sizeof(double) * 4 * ctx->HB, s));
   if ((rc = lsd_launch_products(ctx, fo, fa))) return rc;
   if (vardt && (rc = lsd_launch_cfl_finish(ctx))) return rc;  // non_maxtstep
   if (marks) cudaEventRecord(marks[2], s);
@@ -1008,7 +1044,7 @@ void launch_rot(lsd_ctx* ctx, bool corr) {
   const lsd_config& c = ctx->cfg;
   if (!c.rot_tstep) return;
   const double ri = c.rratio / (1.0 - c.rratio), r3 = ri * ri * ri;  // mes_oc%r(1,3)
-  k_rot<<<1, 32, 0, ctx->stream>>>(ctx->d_rot, corr ? 1 : 0, ctx->rot_inertia, c.implicit, (double)ctx->Ph,
+  k_rot<<<1, 32, 0, ctx->stream>>>(ctx->d_rot, 2 * ctx->HB, corr ? 1 : 0, ctx->rot_inertia, c.implicit, (double)ctx->Ph,
                                    r3 * c.Pm, r3 * 2 * c.Pm / c.E, c.vel_bc <= 2 ? 1 : 0, ctx->Nic > 1 ? 1 : 0,
                                    c.rot_force_0);
   ctx->launches++;
@@ -1040,11 +1076,12 @@ int lsd_pred(lsd_ctx* ctx) {
 
 int lsd_corr(lsd_ctx* ctx) {
   StepArgs a = step_args(ctx);
-  cudaMemsetAsync(ctx->d_red, 0, sizeof(double) * 8, ctx->stream);
+  cudaMemsetAsync(ctx->d_cpart, 0, sizeof(double) * 8 * a.nwarp, ctx->stream);  // slots no job writes
   launch_rot(ctx, true);
   int rc = launch_step_kernel(ctx, a, true);
   if (rc) return rc;
-  ctx->launches++;
+  k_cgce_sums<<<1, 256, 0, ctx->stream>>>(ctx->d_cpart, a.nwarp, ctx->d_red);
+  ctx->launches += 2;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("k_corrector: ") + cudaGetErrorString(e));
   return LSD_OK;
@@ -1075,9 +1112,7 @@ int energy_partials(lsd_ctx* ctx, const cplx** d_arrs, double* d_out, double* Fh
   const cplx* arrs[12];
   for (int k = 0; k < 12; ++k) arrs[k] = sp + k * F;
   CUDA_TRY(cudaMemcpyAsync(d_arrs, arrs, sizeof(arrs), cudaMemcpyHostToDevice, s));
-  CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(double) * 48 * N, s));
-  dim3 gn(ceil_div(H, 128), N, 12);
-  k_norms<<<gn, 128, 0, s>>>(N, H, ctx->d_l, ctx->d_m, d_arrs, 12, d_out);
+  k_norms<<<dim3(N, 12), NORM_THREADS, 0, s>>>(N, H, ctx->d_l, ctx->d_m, d_arrs, d_out);
   ctx->launches += 5;
   CUDA_TRY(cudaMemcpyAsync(Fh, d_out, sizeof(double) * 48 * N, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaMemcpyAsync(wts, ctx->d_intr2dr, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
@@ -1476,8 +1511,7 @@ int lsd_diagnostics_device(lsd_ctx* ctx, double* sc, double* spec, double* prof)
     const cplx** d_arrs = (const cplx**)(ctx->d_red + 64);
     double* d_out = ctx->d_red + 128;
     CUDA_TRY(cudaMemcpyAsync(d_arrs, arrs, sizeof(arrs), cudaMemcpyHostToDevice, s));
-    CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(double) * 24 * Ni, s));
-    k_norms<<<dim3(ceil_div(H, 128), Ni, 6), 128, 0, s>>>(Ni, H, ctx->d_l, ctx->d_m, d_arrs, 6, d_out);
+    k_norms<<<dim3(Ni, 6), NORM_THREADS, 0, s>>>(Ni, H, ctx->d_l, ctx->d_m, d_arrs, d_out);
     ctx->launches += 3;
     std::vector<double> Fi_h((size_t)24 * Ni), wic((size_t)5 * Ni);
     CUDA_TRY(cudaMemcpyAsync(Fi_h.data(), d_out, sizeof(double) * Fi_h.size(), cudaMemcpyDeviceToHost, s));

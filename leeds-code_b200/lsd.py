@@ -80,6 +80,8 @@ def load_library(path=None):
         "lsd_energies": [_V, _D],
         "lsd_energies_static": [_V, _D],
         "lsd_diagnostics": [_V, _D, _D, _D],
+        "lsd_stage_coll": [_V, ctypes.c_int, _D, _D],
+        "lsd_commit_staged": [_V],
         "lsd_set_rotation": [_V, ctypes.c_double],
         "lsd_get_rotation": [_V, _D],
         "lsd_banded_factor_device": [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _V, _V, _V],
@@ -208,6 +210,22 @@ class Context:
         n = self.rows(field)
         assert re.size == self.H * n and im.size == self.H * n
         self._ok(self.lib.lsd_set_coll(self.h, field, _dp(re), _dp(im)))
+
+    def stage_coll(self, field, re, im):
+        """lsd_stage_coll: enqueue the upload of one field (keep re, im alive and unchanged
+        until a later waiting call -- step, energies, get_coll -- has returned after the commit)."""
+        n = self.rows(field)
+        assert re.size == self.H * n and im.size == self.H * n
+        assert re.flags["C_CONTIGUOUS"] and im.flags["C_CONTIGUOUS"]
+        self._ok(self.lib.lsd_stage_coll(self.h, field, _dp(re), _dp(im)))
+
+    def stage_fields(self, fields):
+        for f, (re, im) in fields.items():
+            self.stage_coll(f, re, im)
+
+    def commit_staged(self):
+        """lsd_commit_staged: the staged fields become the state."""
+        self._ok(self.lib.lsd_commit_staged(self.h))
 
     def get_coll(self, field):
         n = self.rows(field)
