@@ -498,11 +498,17 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
     sh.rm1 = pc.r[(size_t)2 * N + n]; sh.rinv = sh.rm1; sh.rrr = pc.r[(size_t)4 * N + n];
     sh.Cmag = pc.Pm / (pc.E * sh.rho);
   }
-  // ---- gather + pack, no barrier: item (f, k) loads the (E, O) pairs of bins k and P2-k
-  // (counters bin2c[.]) straight from this half-row's block, forms the southern (E + O)
-  // and northern (E - O) half spectra and writes both packed rows at position k.  Bins
-  // >= M are zero (dealiasing).  Batches of U items per thread keep their loads in flight.
-  constexpr int U = 4, NITEM = NF_IN * P2;
+  // ---- gather + pack, no barrier: item (f, k), k = 0 .. P2/2, loads the (E, O) pairs of
+  // bins k and P2-k (counters bin2c[.]) once, straight from this half-row's block, forms the
+  // southern (E + O) and northern (E - O) half spectra and writes the packed rows at
+  // positions k and P2-k (k = 0: position 0, whose partner is the Nyquist bin P2 >= M;
+  // k = P2/2: its own partner).  Bins >= M are zero (dealiasing).  Batches of U items per
+  // thread keep their loads in flight.
+  constexpr int KH = P2 / 2 + 1, U = 3, NITEM = NF_IN * KH;
+  auto put = [&](int row, int k, double2 yk, double2 ym) {
+    rows[(size_t)row * RS + ppos<G>(k)] = c2r_pack(k, yk, ym, pl);
+    if (k != 0 && 2 * k != P2) rows[(size_t)row * RS + ppos<G>(P2 - k)] = c2r_pack(P2 - k, ym, yk, pl);
+  };
   for (int it0 = tid; it0 < NITEM; it0 += U * PROD_THREADS) {
     double2 e0[U], o0[U], e1[U], o1[U];
 #pragma unroll
@@ -510,7 +516,7 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
       const int it = it0 + u * PROD_THREADS;
       e0[u] = o0[u] = e1[u] = o1[u] = make_double2(0.0, 0.0);
       if (it < NITEM) {
-        const int f = it / P2, k = it - f * P2, km = k == 0 ? P2 : P2 - k;
+        const int f = it / KH, k = it - f * KH, km = k == 0 ? P2 : P2 - k;
         const cplx* src = four_in + (size_t)pc.fin[f] * fstride + boff;
         if (k < M) {
           const int c = __ldg(pc.bin2c + k);
@@ -526,34 +532,43 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
     for (int u = 0; u < U; ++u) {
       const int it = it0 + u * PROD_THREADS;
       if (it < NITEM) {
-        const int f = it / P2, k = it - f * P2;
-        rows[(size_t)(f * 2) * RS + ppos<G>(k)] = c2r_pack(k, add2(e0[u], o0[u]), add2(e1[u], o1[u]), pl);
-        rows[(size_t)(f * 2 + 1) * RS + ppos<G>(k)] = c2r_pack(k, sub2(e0[u], o0[u]), sub2(e1[u], o1[u]), pl);
+        const int f = it / KH, k = it - f * KH;
+        put(f * 2, k, add2(e0[u], o0[u]), add2(e1[u], o1[u]));
+        put(f * 2 + 1, k, sub2(e0[u], o0[u]), sub2(e1[u], o1[u]));
       }
     }
   }
   if constexpr (NDER > 0) {  // the qv1, qv2 rows from the u_th (input 1), u_ph (input 2) bins
     const cplx* sth = four_in + (size_t)pc.fin[1] * fstride + boff;
     const cplx* sph = four_in + (size_t)pc.fin[2] * fstride + boff;
-    for (int i = tid; i < 2 * P2; i += PROD_THREADS) {
-      const int side = i / P2, k = i - side * P2;
-      const int j = row_theta(h, side, Th);
-      const double s1 = pc.sn1[j], cot = pc.gp[j] * s1;
-      auto bins = [&](int b, double2& q1, double2& q2) {
-        if (b >= M) { q1 = q2 = make_double2(0.0, 0.0); return; }
-        const int c = __ldg(pc.bin2c + b);
-        const double2 te = sth[4 * c], to = sth[4 * c + 2], pe = sph[4 * c], po = sph[4 * c + 2];
-        const double2 t = side ? sub2(te, to) : add2(te, to);
-        const double2 p = side ? sub2(pe, po) : add2(pe, po);
-        const double mk = (double)(b * pl.Mp) * s1;
-        q1 = make_double2(sh.rinv * (cot * t.x - mk * p.y), sh.rinv * (cot * t.y + mk * p.x));
-        q2 = make_double2(sh.rinv * (-mk * t.y - cot * p.x), sh.rinv * (mk * t.x - cot * p.y));
-      };
-      double2 q1k, q2k, q1m, q2m;
-      bins(k, q1k, q2k);
-      bins(k == 0 ? P2 : P2 - k, q1m, q2m);
-      rows[(size_t)(NF_IN * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, q1k, q1m, pl);
-      rows[(size_t)((NF_IN + 1) * 2 + side) * RS + ppos<G>(k)] = c2r_pack(k, q2k, q2m, pl);
+    for (int k = tid; k < KH; k += PROD_THREADS) {  // bins k and P2-k, both sides
+      const int km = k == 0 ? P2 : P2 - k;
+      double2 te[2], to[2], pe[2], po[2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int b = q ? km : k;
+        te[q] = to[q] = pe[q] = po[q] = make_double2(0.0, 0.0);
+        if (b < M) {
+          const int c = __ldg(pc.bin2c + b);
+          te[q] = sth[4 * c]; to[q] = sth[4 * c + 2]; pe[q] = sph[4 * c]; po[q] = sph[4 * c + 2];
+        }
+      }
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const int j = row_theta(h, side, Th);
+        const double s1 = pc.sn1[j], cot = pc.gp[j] * s1;
+        double2 q1[2], q2[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const double2 t = side ? sub2(te[q], to[q]) : add2(te[q], to[q]);
+          const double2 p = side ? sub2(pe[q], po[q]) : add2(pe[q], po[q]);
+          const double mk = (double)((q ? km : k) * pl.Mp) * s1;
+          q1[q] = make_double2(sh.rinv * (cot * t.x - mk * p.y), sh.rinv * (cot * t.y + mk * p.x));
+          q2[q] = make_double2(sh.rinv * (-mk * t.y - cot * p.x), sh.rinv * (mk * t.x - cot * p.y));
+        }
+        put(NF_IN * 2 + side, k, q1[0], q1[1]);
+        put((NF_IN + 1) * 2 + side, k, q2[0], q2[1]);
+      }
     }
   }
   __syncthreads();
