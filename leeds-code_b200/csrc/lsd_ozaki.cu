@@ -1,12 +1,17 @@
 // lsd_ozaki.cu -- FP64-accurate Legendre contractions on the tcgen05 tensor cores.
 //
-// Ozaki-style error-free splitting: an FP64 operand row (or column) is scaled by a power
-// of two so that all its entries are below 1 in magnitude, then written as a sum of S
-// signed 7-bit digits (int8, |digit| <= 127):  x = 2^e * sum_s d_s 2^(-7(s+1)).
-// Products of digit matrices are exact in int32 (|d_a d_b| K <= 127^2 * 256 < 2^31) and
-// are accumulated in tensor memory per diagonal s + t; the diagonals s + t < S are
-// recombined in FP64 in the epilogue.  The dropped terms bound the relative error by
-// about S * K * 2^(-7S) of (row max x column max).
+// Ozaki-style splitting: an FP64 operand row (or column) with entries below 2^e in
+// magnitude is rounded to the nearest integer X of x 2^(8S - 2 - e) (|X| < 2^(8S-2)) and
+// X is written as S balanced base-256 digits, int8 in [-128, 127]:
+//   x ~= 2^(e+2) * sum_s d_s 2^(-8(s+1)),  s = 0 most significant.
+// The digits are the bytes of X + C, C = 0x80 in every byte below the top one, with bit 7
+// of those lower bytes flipped (b - 128); the top byte of X + C is the top digit as it is
+// (|d_0| <= 65).  Rounding to nearest keeps the error unbiased, and the digits come out of
+// the integer by byte permutes alone.  Products of digit matrices are exact in int32
+// (S K 128^2 < 2^31 for K <= 16384) and are accumulated in tensor memory per diagonal
+// s + t; the diagonals s + t < S are recombined in FP64 in the epilogue.  Per product the
+// rounding costs 2^(1-8S) and the dropped diagonals about (S + 1) 2^(2-8S) of
+// (row max x column max).
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -160,15 +165,27 @@ __device__ __forceinline__ double pow2i(int e) {
   return ldexp(1.0, e);
 }
 
-// digits of x * 2^-e (|x| < 2^e): S signed 7-bit digits, most significant first
+// C of the digit split: 0x80 in each of the S - 1 lower bytes
+__host__ __device__ __forceinline__ unsigned long long oz_bias(int S) {
+  return 0x0080808080808080ull >> (8 * (8 - S));
+}
+
+// X + C for x 2^(8S - 2 - e), |x| < 2^e (exact scaling, round to nearest)
+__device__ __forceinline__ unsigned long long oz_biased(double x, double sc, unsigned long long bias) {
+  return (unsigned long long)__double2ll_rn(x * sc) + bias;
+}
+
+// digits of x (|x| < 2^e): S balanced base-256 digits, most significant first
 __device__ __forceinline__ void oz_digits(double x, int e, int S, int8_t* d) {
-  long long X = 0;
-  if (e > -1000) X = (long long)((x * pow2i(-e)) * pow2i(7 * S));  // exact scaling; truncation
-  const long long mag = X < 0 ? -X : X;
-  const int sgn = X < 0 ? -1 : 1;
+  const double sc = e > -1000 ? pow2i(8 * S - 2 - e) : 0.0;
+  const unsigned long long Y = oz_biased(x, sc, oz_bias(S));
 #pragma unroll
   for (int s = 0; s < OZ_MAXS; ++s)
-    if (s < S) d[s] = (int8_t)(sgn * (int)((mag >> (7 * (S - 1 - s))) & 127));
+    if (s < S) {
+      const int j = S - 1 - s;  // byte of Y
+      const uint32_t b = (uint32_t)(Y >> (8 * j)) & 0xFFu;
+      d[s] = (int8_t)(j == S - 1 ? b : b ^ 0x80u);
+    }
 }
 
 __device__ __forceinline__ int oz_exponent(double maxabs) {
@@ -250,12 +267,14 @@ __global__ void k_oz_tab_anal(OzTabArgs a, int type) {
   }
 }
 
-// Four 7-bit digits (one per byte, each 0..127) with per-byte signs: the bytes of w whose
-// byte of sg is 0xFF are negated (two's complement).  For 0 <= b <= 127,
-// -b mod 256 = (0x80 - b) ^ 0x80, and 0x80808080 - w borrows across no byte.
-__device__ __forceinline__ uint32_t signed_digits(uint32_t w, uint32_t sg) {
-  const uint32_t neg = (0x80808080u - w) ^ 0x80808080u;
-  return (neg & sg) | (w & ~sg);
+// 4 x 4 byte transpose: w[j] = byte j of x[0], x[1], x[2], x[3] (in that byte order)
+__device__ __forceinline__ void byte_transpose4(const uint32_t* x, uint32_t* w) {
+  const uint32_t a = __byte_perm(x[0], x[1], 0x5140), b = __byte_perm(x[0], x[1], 0x7362);
+  const uint32_t c = __byte_perm(x[2], x[3], 0x5140), d = __byte_perm(x[2], x[3], 0x7362);
+  w[0] = __byte_perm(a, c, 0x5410);
+  w[1] = __byte_perm(a, c, 0x7632);
+  w[2] = __byte_perm(b, d, 0x5410);
+  w[3] = __byte_perm(b, d, 0x7632);
 }
 
 // ---- the slicing pre-pass ---------------------------------------------------------------
@@ -366,13 +385,14 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
     }
     __syncthreads();
     if (tid < 32 && R0 + tid < a.nrows) a.erow[(size_t)c * a.nrows + R0 + tid] = e_slot[tid / PER];
-    // ---- digits of both parities' A tiles.  |x| 2^(7S - e) is an integer below
-    // 2^(7S) <= 2^56, split into two 28-bit halves whose 7-bit groups are the digits; four
-    // values make one 32-bit word per slice (byte permutes), the signs applied per byte.
+    // ---- digits of both parities' A tiles: the bytes of X + C (oz_digits) of four values
+    // make one 32-bit word per slice (a byte transpose of their low and high words), bit 7
+    // flipped in all but the top slice.
     const int R = R0 + r;
     const bool live = R < a.nrows;
     const int sl = r / PER, comp = R % PER;
-    const double sc = live && e_slot[sl] > -1000 ? pow2i(7 * S - e_slot[sl]) : 0.0;
+    const double sc = live && e_slot[sl] > -1000 ? pow2i(8 * S - 2 - e_slot[sl]) : 0.0;
+    const unsigned long long bias = oz_bias(S);
     const double r1 = (TYPE == OZ_GRAD && live) ? a.rinv[(R % a.rows_per_group) / PER] : 1.0;
     const double2* row0 = st + (size_t)(sl * NIN) * srow;
     const double2* row1 = row0 + srow;  // second field (VEC: t, ST: phi)
@@ -383,7 +403,6 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
       int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
       for (int ks = 0; ks < pr.nks; ++ks) {
         uint32_t hi[4], lo[4];
-        uint32_t sg = 0u;
 #pragma unroll
         for (int u4 = 0; u4 < 4; ++u4) {
           const int k = ks * 32 + kq * 4 + u4;
@@ -421,20 +440,19 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
               else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
             }
           }
-          const unsigned long long X = (unsigned long long)(fabs(v) * sc);  // exact scaling, truncation
-          hi[u4] = (uint32_t)(X >> 28);
-          lo[u4] = (uint32_t)X & 0x0FFFFFFFu;
-          if (v < 0.0) sg |= 0xFFu << (8 * u4);
+          const unsigned long long Y = oz_biased(v, sc, bias);
+          lo[u4] = (uint32_t)Y;
+          hi[u4] = (uint32_t)(Y >> 32);
         }
+        uint32_t wl[4], wh[4];
+        byte_transpose4(lo, wl);
+        if (S > 4) byte_transpose4(hi, wh);
         const int toff = umma::tile_off(rt, kq * 4);
 #pragma unroll
         for (int s2 = 0; s2 < S; ++s2) {
-          const int j = S - 1 - s2;  // digit s2 holds bits 7j .. 7j + 6
-          uint32_t m[4];
-#pragma unroll
-          for (int u4 = 0; u4 < 4; ++u4) m[u4] = j >= 4 ? (hi[u4] >> (7 * (j - 4))) & 127u : (lo[u4] >> (7 * j)) & 127u;
-          const uint32_t w = __byte_perm(__byte_perm(m[0], m[1], 0x0040), __byte_perm(m[2], m[3], 0x0040), 0x5410);
-          *(uint32_t*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) = signed_digits(w, sg);
+          const int j = S - 1 - s2;  // slice s2 = byte j of X + C
+          const uint32_t w = j >= 4 ? wh[j - 4] : wl[j];
+          *(uint32_t*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) = j == S - 1 ? w : w ^ 0x80808080u;
         }
       }
     }
@@ -590,9 +608,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
       }
       const int R = zb * 128 + tid;
       const bool live = R < a.nrows;
-      // sum_d D_d 2^(-7(d+2)) = 2^(-7(S+1)) H with H = Horner over d in 2^7; the power of
-      // two and the row scale 2^erow are one factor
-      const double rsc = live ? pow2i(a.erow[(size_t)c * a.nrows + R] - 7 * (S + 1)) : 0.0;
+      // x y = 2^(ea + eb + 4) sum_d D_d 2^(-8(d+2)) = 2^(ea + eb + 4 - 8(S+1)) H with
+      // H = Horner over d in 2^8; the power of two and the row scale 2^erow are one factor
+      const double rsc = live ? pow2i(a.erow[(size_t)c * a.nrows + R] + 4 - 8 * (S + 1)) : 0.0;
       bool ok = true;
       for (int ch = 0; ch < pr.nchunk; ++ch, ++cc) {
         if (tid < OZ_NC) csc[tid] = pow2i(a.fexp[pr.fofs + ch * OZ_NC + tid]);
@@ -615,7 +633,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
             double hsum = (double)v[0][q];
 #pragma unroll
             for (int d = 1; d < OZ_MAXS; ++d)
-              if (d < S) hsum = fma(hsum, 128.0, (double)v[d][q]);
+              if (d < S) hsum = fma(hsum, 256.0, (double)v[d][q]);
             stg[tid * OZ_STG + c0 + q] = hsum * (rsc * csc[c0 + q]);
           }
         }

@@ -1,15 +1,17 @@
 """The tensor-core (Ozaki int8-slice) Legendre path against the CPU oracle.
 
-Each operand is split into S signed 7-bit slices under a power-of-two scale per row
-(spectral coefficients of one shell and order m) and per column (one theta row, or one
-harmonic); the products of slice pairs whose index sum is below S are accumulated exactly
-in int32 on the tcgen05 tensor cores and recombined in FP64.  The dropped tail is about
-(S + 2) 2^(-7S) of (row max) x (column max) per product, so with the default S = 7 a
-single transform agrees with the FP64 oracle to about 1e-13 of the largest output, and the
-tolerances below (relative to the largest magnitude of the compared array) are:
-  single transforms, S = 7       5e-12
-  single transforms, S = 8       5e-14
-  one nonlinear evaluation       2e-12
+Each operand is scaled by a power of two per row (spectral coefficients of one shell and
+order m) or per column (one theta row, or one harmonic), rounded to an integer of 8S - 2
+bits and split into S balanced base-256 int8 digits; the products of digit pairs whose
+index sum is below S are accumulated exactly in int32 on the tcgen05 tensor cores and
+recombined in FP64.  Rounding costs 2^(1-8S) and the dropped tail about (S + 1) 2^(2-8S)
+of (row max) x (column max) per product, so a single transform agrees with the FP64
+oracle to about 1e-14 of the largest output for S >= 7 (FP64 rounding), 1e-11 for S = 6
+and 3e-9 for S = 5.  Tolerances (relative to the largest magnitude of the compared array):
+  single transforms, S = 5       2e-8
+  single transforms, S = 6       1e-10
+  single transforms, S = 7, 8    5e-13
+  one nonlinear evaluation       2e-12 (default S = 7)
   energies after 100 steps       1e-9 (the mixed-precision acceptance bar)
 """
 import importlib
@@ -40,8 +42,9 @@ def test_ozaki_slices_are_validated():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("LMMp,S,tol", [((32, 32, 1), 7, 5e-12), ((64, 16, 4), 7, 5e-12),
-                                         ((24, 8, 2), 7, 5e-12), ((32, 32, 1), 8, 5e-14)])
+@pytest.mark.parametrize("LMMp,S,tol", [((32, 32, 1), 7, 5e-13), ((64, 16, 4), 7, 5e-13),
+                                         ((24, 8, 2), 7, 5e-13), ((32, 32, 1), 8, 5e-13),
+                                         ((64, 16, 4), 6, 1e-10), ((64, 16, 4), 5, 2e-8)])
 def test_ozaki_transforms(LMMp, S, tol):
     L, M, Mp = LMMp
     cfg = capi.template_config(L=L, M=M, Mp=Mp, N=9, timestep=1e-5, precision=capi.PREC_OZAKI,
