@@ -130,7 +130,7 @@ int lsd_umma_selftest(lsd_ctx* ctx, double* maxerr) {
 //
 // Two kernels per contraction: a slicing pre-pass reads the FP64 data once, takes each
 // row's exponent and writes the int8 digits in the tcgen05 shared-memory tile layout; the
-// GEMM streams A and B tiles with bulk copies (a two-stage ring), issues the int8 MMAs of
+// GEMM streams A and B tiles with bulk copies (a ring of 2-4 stages), issues the int8 MMAs of
 // the S(S+1)/2 digit pairs into S tensor-memory diagonals, and its epilogue warps recombine
 // the diagonals in FP64 and store through shared memory (coalesced).
 // =========================================================================================
@@ -138,7 +138,7 @@ namespace {
 
 constexpr int OZ_MAXS = 8;       // slices per operand
 constexpr int OZ_NC = 32;        // columns per chunk
-constexpr int OZ_STAGES = 2;     // bulk-copy ring
+constexpr int OZ_MAXSTAGES = 4;  // bulk-copy ring: up to 4 stages, as many as leave two CTAs per SM
 constexpr int OZ_THREADS = 192;  // warps 0-3 epilogue (TMEM lane quarters), 4 copies, 5 MMA
 constexpr int OZ_STG = OZ_NC + 1;  // epilogue staging row (doubles)
 constexpr int OZ_MAXG = 8;       // groups (output fields) of one launch
@@ -397,62 +397,106 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
     const double2* row0 = st + (size_t)(sl * NIN) * srow;
     const double2* row1 = row0 + srow;  // second field (VEC: t, ST: phi)
     const int rt = q * 32 + r;          // row inside the 128-row tile
-    for (int p = 0; p < 2; ++p) {
-      const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
-      if (pr.nchunk == 0) continue;
-      int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
-      for (int ks = 0; ks < pr.nks; ++ks) {
-        uint32_t hi[4], lo[4];
-#pragma unroll
-        for (int u4 = 0; u4 < 4; ++u4) {
-          const int k = ks * 32 + kq * 4 + u4;
-          double v = 0.0;
-          if (live && k < pr.K) {
-            const bool seg1 = k < pr.len1;
-            if (TYPE == OZ_P) {
-              const double2 x = row0[kx[p][k]];
-              v = comp ? x.y : x.x;
-            } else if (TYPE == OZ_VEC) {
-              // theta: s llP_ (segment 1) + (t.im, -t.re) llsin1mP (segment 2);
-              // phi:   t llP_ + (-s.im, s.re) llsin1mP        (transform.fftw3.F90:746-774)
-              const bool use_t = seg1 ? comp >= 2 : comp < 2;
-              const double2 x = (use_t ? row1 : row0)[kx[p][k]];
-              if (seg1) v = (comp & 1) ? x.y : x.x;
-              else v = comp == 0 ? x.y : comp == 1 ? -x.x : comp == 2 ? -x.y : x.x;
-            } else if (TYPE == OZ_GRAD) {
-              // theta: (C/r) P_ ; phi: i (C/r) sin1mP              (transform.fftw3.F90:955-1000)
-              if (seg1 == (comp < 2)) {
-                const double2 x = row0[kx[p][k]];
-                const double2 cv = make_double2(x.x * r1, x.y * r1);
-                v = comp == 0 ? cv.x : comp == 1 ? cv.y : comp == 2 ? -cv.y : cv.x;
-              }
-            } else if (TYPE == OZ_Q) {
-              const double2 y = row0[2 * k + p];
-              v = comp ? y.y : y.x;
-            } else {  // OZ_ST: segment 1 (gwllP_) on parity 1-p, segment 2 (gwllsin1mP) on parity p
-              const int pp = seg1 ? 1 - p : p;
-              const int j = seg1 ? k : k - pr.len1;
-              // s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re)
-              // (transform.fftw3.F90:866-909)
-              const bool use_ph = seg1 ? comp >= 2 : comp < 2;
-              const double2 y = (use_ph ? row1 : row0)[2 * j + pp];
-              if (seg1) v = (comp & 1) ? y.y : y.x;
-              else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
-            }
+    // the A value of row R, harmonic / theta-row slot k of parity p (0 beyond K)
+    auto value = [&](int p, const OzProb& pr, int k) {
+      double v = 0.0;
+      if (live && k < pr.K) {
+        const bool seg1 = k < pr.len1;
+        if (TYPE == OZ_P) {
+          const double2 x = row0[kx[p][k]];
+          v = comp ? x.y : x.x;
+        } else if (TYPE == OZ_VEC) {
+          // theta: s llP_ (segment 1) + (t.im, -t.re) llsin1mP (segment 2);
+          // phi:   t llP_ + (-s.im, s.re) llsin1mP        (transform.fftw3.F90:746-774)
+          const bool use_t = seg1 ? comp >= 2 : comp < 2;
+          const double2 x = (use_t ? row1 : row0)[kx[p][k]];
+          if (seg1) v = (comp & 1) ? x.y : x.x;
+          else v = comp == 0 ? x.y : comp == 1 ? -x.x : comp == 2 ? -x.y : x.x;
+        } else if (TYPE == OZ_GRAD) {
+          // theta: (C/r) P_ ; phi: i (C/r) sin1mP              (transform.fftw3.F90:955-1000)
+          if (seg1 == (comp < 2)) {
+            const double2 x = row0[kx[p][k]];
+            const double2 cv = make_double2(x.x * r1, x.y * r1);
+            v = comp == 0 ? cv.x : comp == 1 ? cv.y : comp == 2 ? -cv.y : cv.x;
           }
-          const unsigned long long Y = oz_biased(v, sc, bias);
-          lo[u4] = (uint32_t)Y;
-          hi[u4] = (uint32_t)(Y >> 32);
+        } else if (TYPE == OZ_Q) {
+          const double2 y = row0[2 * k + p];
+          v = comp ? y.y : y.x;
+        } else {  // OZ_ST: segment 1 (gwllP_) on parity 1-p, segment 2 (gwllsin1mP) on parity p
+          const int pp = seg1 ? 1 - p : p;
+          const int j = seg1 ? k : k - pr.len1;
+          // s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re)
+          // (transform.fftw3.F90:866-909)
+          const bool use_ph = seg1 ? comp >= 2 : comp < 2;
+          const double2 y = (use_ph ? row1 : row0)[2 * j + pp];
+          if (seg1) v = (comp & 1) ? y.y : y.x;
+          else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
         }
-        uint32_t wl[4], wh[4];
-        byte_transpose4(lo, wl);
-        if (S > 4) byte_transpose4(hi, wh);
-        const int toff = umma::tile_off(rt, kq * 4);
+      }
+      return v;
+    };
+    if constexpr (OzT<TYPE>::anal) {
+      // items (parity, K step, 16-byte half of the step) over the warps; a thread writes one
+      // full 16-byte core-matrix row per slice, a warp four whole 128-byte lines (the
+      // analysis has K steps enough for all warps)
+      const OzProb pr0 = a.probs[(TYPE * a.NM + c) * 2], pr1 = a.probs[(TYPE * a.NM + c) * 2 + 1];
+      const int n0 = pr0.nchunk ? 2 * pr0.nks : 0, n1 = pr1.nchunk ? 2 * pr1.nks : 0;
+      for (int i = kq; i < n0 + n1; i += 8) {
+        const int p = i < n0 ? 0 : 1;
+        const OzProb& pr = p ? pr1 : pr0;
+        const int li = i - (p ? n0 : 0), ks = li >> 1, hh = li & 1;
+        int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
+        uint32_t ow[S][4];
 #pragma unroll
-        for (int s2 = 0; s2 < S; ++s2) {
-          const int j = S - 1 - s2;  // slice s2 = byte j of X + C
-          const uint32_t w = j >= 4 ? wh[j - 4] : wl[j];
-          *(uint32_t*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) = j == S - 1 ? w : w ^ 0x80808080u;
+        for (int b4 = 0; b4 < 4; ++b4) {
+          uint32_t hi[4], lo[4];
+#pragma unroll
+          for (int u4 = 0; u4 < 4; ++u4) {
+            const unsigned long long Y = oz_biased(value(p, pr, ks * 32 + hh * 16 + b4 * 4 + u4), sc, bias);
+            lo[u4] = (uint32_t)Y;
+            hi[u4] = (uint32_t)(Y >> 32);
+          }
+          uint32_t wl[4], wh[4];
+          byte_transpose4(lo, wl);
+          if (S > 4) byte_transpose4(hi, wh);
+#pragma unroll
+          for (int s2 = 0; s2 < S; ++s2) {
+            const int j = S - 1 - s2;  // slice s2 = byte j of X + C
+            const uint32_t w = j >= 4 ? wh[j - 4] : wl[j];
+            ow[s2][b4] = j == S - 1 ? w : w ^ 0x80808080u;
+          }
+        }
+        const int toff = umma::tile_off(rt, hh * 16);
+#pragma unroll
+        for (int s2 = 0; s2 < S; ++s2)
+          *(uint4*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) =
+              make_uint4(ow[s2][0], ow[s2][1], ow[s2][2], ow[s2][3]);
+      }
+    } else {
+      // thread (row, K eighth kq): four values of every K step, one 32-bit word per slice
+      // (the synthesis has few K steps per counter)
+      for (int p = 0; p < 2; ++p) {
+        const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
+        if (pr.nchunk == 0) continue;
+        int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
+        for (int ks = 0; ks < pr.nks; ++ks) {
+          uint32_t hi[4], lo[4];
+#pragma unroll
+          for (int u4 = 0; u4 < 4; ++u4) {
+            const unsigned long long Y = oz_biased(value(p, pr, ks * 32 + kq * 4 + u4), sc, bias);
+            lo[u4] = (uint32_t)Y;
+            hi[u4] = (uint32_t)(Y >> 32);
+          }
+          uint32_t wl[4], wh[4];
+          byte_transpose4(lo, wl);
+          if (S > 4) byte_transpose4(hi, wh);
+          const int toff = umma::tile_off(rt, kq * 4);
+#pragma unroll
+          for (int s2 = 0; s2 < S; ++s2) {
+            const int j = S - 1 - s2;  // slice s2 = byte j of X + C
+            const uint32_t w = j >= 4 ? wh[j - 4] : wl[j];
+            *(uint32_t*)(Ablk + ((size_t)ks * S + s2) * 4096 + toff) = j == S - 1 ? w : w ^ 0x80808080u;
+          }
         }
       }
     }
@@ -468,6 +512,7 @@ struct OzGemmArgs {
   const int* nhlist; const int* hm;
   cplx* out0[OZ_MAXG]; cplx* out1[OZ_MAXG]; int zero_m0_im[OZ_MAXG];
   int* err;
+  int nst;  // stages of the bulk-copy ring
 };
 
 __device__ __forceinline__ bool oz_wait(uint64_t* mbar, uint32_t parity, int* err) {
@@ -485,7 +530,7 @@ template <int TYPE>
 __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb) {
   constexpr int PER = OzT<TYPE>::per;
   extern __shared__ __align__(1024) uint8_t oz_smem[];
-  __shared__ __align__(8) uint64_t full[OZ_STAGES], empty[OZ_STAGES], accf, tfree, fin;
+  __shared__ __align__(8) uint64_t full[OZ_MAXSTAGES], empty[OZ_MAXSTAGES], accf, tfree, fin;
   __shared__ uint32_t tbase;
   __shared__ cplx* pbase[64];  // output base of each (re, im) row pair of the z-block
   __shared__ int pzero[64];    // analysis: drop the imaginary part of m = 0 for this pair
@@ -494,9 +539,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
   const int S = a.S;
   const int ntile = a.NM * 2 * nzb;
   const uint32_t stage_bytes = (uint32_t)S * 5120;  // A: S x 4096, B: S x 1024
-  double* stg = (double*)(oz_smem + (size_t)OZ_STAGES * stage_bytes);  // [128][OZ_STG]
+  const int nst = a.nst;
+  double* stg = (double*)(oz_smem + (size_t)nst * stage_bytes);  // [128][OZ_STG]
   if (tid == 0) {
-    for (int i = 0; i < OZ_STAGES; ++i) { umma::mbar_init(&full[i], 1); umma::mbar_init(&empty[i], 1); }
+    for (int i = 0; i < nst; ++i) { umma::mbar_init(&full[i], 1); umma::mbar_init(&empty[i], 1); }
     umma::mbar_init(&accf, 1);
     umma::mbar_init(&tfree, 128);
     umma::mbar_init(&fin, 1);
@@ -537,7 +583,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
       const int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
       const int8_t* Bblk = a.B + pr.bofs;
       for (int q = 0; q < pr.nchunk * pr.nks; ++q, ++it) {
-        const int st = it % OZ_STAGES, use = it / OZ_STAGES;
+        const int st = it % nst, use = it / nst;
         if (use > 0 && !oz_wait(&empty[st], (use - 1) & 1, a.err)) { ok = false; break; }
         const int ch = q / pr.nks, ks = q % pr.nks;
         uint8_t* sA = oz_smem + (size_t)st * stage_bytes;
@@ -548,8 +594,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
       }
     }
     // drain: the copies of the last stages have landed before the CTA can exit
-    for (int j = (it > OZ_STAGES ? it - OZ_STAGES : 0); j < it; ++j)
-      umma::mbar_wait(&full[j % OZ_STAGES], (j / OZ_STAGES) & 1, WAIT_ITERS);
+    for (int j = (it > nst ? it - nst : 0); j < it; ++j)
+      umma::mbar_wait(&full[j % nst], (j / nst) & 1, WAIT_ITERS);
   } else if (tid == 160) {
     // ---- MMA issuer: the S(S+1)/2 digit pairs of a K step into S diagonals of 32 columns,
     // as S MMAs: A slice sa against B slices 0 .. S-1-sa at once (stacked in the stage, they
@@ -565,8 +611,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
         if (cc > 0 && !oz_wait(&tfree, (cc - 1) & 1, a.err)) { ok = false; break; }
         umma::fence_after_sync();
         for (int ks = 0; ks < pr.nks; ++ks, ++it) {
-          const int st = it % OZ_STAGES;
-          if (!oz_wait(&full[st], (it / OZ_STAGES) & 1, a.err)) { ok = false; break; }
+          const int st = it % nst;
+          if (!oz_wait(&full[st], (it / nst) & 1, a.err)) { ok = false; break; }
           umma::fence_after_sync();
           const uint32_t sa0 = umma::smem_u32(oz_smem + (size_t)st * stage_bytes);
           const uint32_t sb0 = sa0 + (uint32_t)S * 4096;
@@ -687,6 +733,7 @@ struct OzState {
   int* d_erow = nullptr;  // row exponents [c][rows]
   int* d_err = nullptr;
   size_t smem = 0;
+  int nst = 2;           // GEMM ring stages
   int srow[2] = {1, 1};  // pre-pass stage row length (odd, in complex): synthesis, analysis
 };
 
@@ -772,7 +819,9 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
       }
     abytes_max = std::max(abytes_max, abytes);
   }
-  o->smem = (size_t)OZ_STAGES * S * 5120 + sizeof(double) * 128 * OZ_STG;
+  // ring stages: as many (2..4) as keep two CTAs per SM (<= 78 KiB of stages each)
+  o->nst = std::max(2, std::min(OZ_MAXSTAGES, 79872 / (S * 5120)));
+  o->smem = (size_t)o->nst * S * 5120 + sizeof(double) * 128 * OZ_STG;
   {
     int mx = 1;
     for (int c = 0; c < NM; ++c) mx = std::max(mx, ctx->mlen[c]);
@@ -833,7 +882,7 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   OzGemmArgs ga;
   ga.N = ctx->N; ga.H = ctx->H; ga.NM = ctx->NM; ga.Th2 = ctx->Th2; ga.HB = ctx->HB; ga.S = o->S; ga.nrows = nrows;
   ga.rows_per_group = rpg; ga.probs = o->d_probs; ga.A = o->d_A; ga.B = o->d_B; ga.fexp = o->d_fexp;
-  ga.erow = o->d_erow; ga.nhlist = o->d_nh; ga.hm = ctx->d_m; ga.err = o->d_err;
+  ga.erow = o->d_erow; ga.nhlist = o->d_nh; ga.hm = ctx->d_m; ga.err = o->d_err; ga.nst = o->nst;
   for (int i = 0; i < OZ_MAXG; ++i) {
     const bool on = i < ng;
     pa.in0[i] = on ? gs[i].in0 : nullptr; pa.in1[i] = on ? gs[i].in1 : nullptr;
