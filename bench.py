@@ -42,6 +42,18 @@ sys.path.insert(0, ROOT)
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 
 
+def max_over_ranks(dist, x, device):
+    """The largest x over all ranks (every rank passes its own x and gets the maximum back);
+    x itself when there is no process group.  device: where the reduction tensor lives
+    ("cuda:<local rank>" under NCCL, "cpu" under gloo)."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -274,9 +286,7 @@ def run_ours(args, rank, world, local_rank, dist):
         launches = ctx.kernel_launches() - l0
         clocks = sampler.stop() if sampler else None
         if dist:
-            t = torch.tensor([ms], device="cuda:%d" % local_rank, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(dist, ms, "cuda:%d" % local_rank)
             dist.barrier()
         e = ctx.energies()
         res = {"ms": ms, "steps": st.steps_done, "correctors": st.correctors, "launches": launches,
@@ -297,13 +307,15 @@ def run_ours(args, rank, world, local_rank, dist):
         ctx.energies()
         ctx.synchronize()
         # (a) one call after another: upload (lsd_set_coll), step, energies
+        if dist:
+            dist.barrier()
         t0 = time.perf_counter()
         for _ in range(ne):
             ctx.load_fields(pinned)
             ctx.step(1)
             ctx.energies()
         ctx.synchronize()
-        res["e2e_serial_s"] = (time.perf_counter() - t0) / ne
+        res["e2e_serial_s"] = max_over_ranks(dist, (time.perf_counter() - t0) / ne, "cuda:%d" % local_rank)
         # (b) streamed inputs: each step's fields are staged (lsd_stage_coll, copy stream)
         # while the step before runs, committed (lsd_commit_staged), stepped, energies read;
         # every timed iteration uploads one state, as in (a)
@@ -312,6 +324,8 @@ def run_ours(args, rank, world, local_rank, dist):
         ctx.step(1)
         ctx.stage_fields(pinned)
         ctx.synchronize()
+        if dist:
+            dist.barrier()
         t0 = time.perf_counter()
         for _ in range(ne):
             ctx.commit_staged()
@@ -319,7 +333,7 @@ def run_ours(args, rank, world, local_rank, dist):
             ctx.step(1)
             ctx.energies()
         ctx.synchronize()
-        res["e2e_s"] = (time.perf_counter() - t0) / ne
+        res["e2e_s"] = max_over_ranks(dist, (time.perf_counter() - t0) / ne, "cuda:%d" % local_rank)
         res["h2d"] = 5 * ctx.N * ctx.H * 16
         res["d2h"] = (48 + 2) * ctx.N * 8 + 3 * 16
         ph, rf = phase_roofline(ctx, peaks, src)
