@@ -178,6 +178,8 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out);
  * is called such a context uses rho = T = eta = 1 with zero gradients. */
 int lsd_set_reference_state(lsd_ctx* ctx, const double* prof);
 int lsd_destroy(lsd_ctx* ctx);
+/* The text of the context's last error; with ctx = NULL, why the calling thread's last
+ * lsd_create failed (the configuration rule it broke, or the device it did not find). */
 const char* lsd_last_error(const lsd_ctx* ctx);
 int lsd_get_sizes(const lsd_ctx* ctx, lsd_sizes* out);
 

@@ -274,8 +274,12 @@ int lsd_config_default(lsd_config* c) {
   return LSD_OK;
 }
 
+// why the last lsd_create of this thread failed (lsd_last_error(NULL) returns it)
+static thread_local std::string t_create_err;
+
 int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
-  if (!cfg || !out) return LSD_EARG;
+  t_create_err.clear();
+  if (!cfg || !out) { t_create_err = "lsd_create: null argument"; return LSD_EARG; }
   *out = nullptr;
   lsd_ctx* ctx = new (std::nothrow) lsd_ctx();
   if (!ctx) return LSD_ENOMEM;
@@ -289,6 +293,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   if (c.L < 2 || c.M < 2 || c.Mp < 1 || c.N < 2 * c.KL + 2 || c.KL < 2 || c.KL > LSD_MAX_KL) why = "bad resolution";
   else if (c.L <= (c.M - 1) * c.Mp) why = "set L > (M-1)*Mp";
   else if (c.M % 2 == 1) why = "if(M>1) set M even";
+  else if (c.KL > 6) why = "the timestep kernels are built for stencil half-widths KL = 2..6";
   else if (c.Nic < 1) why = "Nic must be >= 1";
   else if (c.Nic > 1 && (c.Nic < 2 * c.KL + 1 || c.Nic > c.N))
     why = "a conducting inner core needs 2 KL + 1 <= Nic <= N radial points";
@@ -302,7 +307,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   else if (c.precision != LSD_PREC_FP64 && c.precision != LSD_PREC_OZAKI) why = "unknown precision";
   else if (c.precision == LSD_PREC_OZAKI && c.ozaki_slices != 0 && (c.ozaki_slices < 2 || c.ozaki_slices > 8))
     why = "ozaki_slices must be 0 (default) or 2..8";
-  if (!why.empty()) { int rc = lsd_fail(ctx, LSD_EARG, why); free_ctx(ctx); return rc; }
+  if (!why.empty()) { t_create_err = why; int rc = lsd_fail(ctx, LSD_EARG, why); free_ctx(ctx); return rc; }
   ctx->Ma = c.M * 3 / 2;
   ctx->H = c.L * c.M - c.Mp * (c.M - 1) * c.M / 2;
   ctx->Th = c.L * 3 / 2;
@@ -314,9 +319,15 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   ctx->P2 = ctx->Ma;
   ctx->dt = c.timestep < 0 ? -c.timestep : c.timestep;  // d_timestep < 0: |d_timestep| until lsd_set_time
   ctx->HB = (ctx->Th2 + 1) / 2;
-  if (!lsd_fft_plan(ctx)) { int rc = lsd_fail(ctx, LSD_EARG, "phi FFT length 3M/2 not supported"); free_ctx(ctx); return rc; }
+  if (!lsd_fft_plan(ctx)) {
+    t_create_err = "phi FFT length 3M/2 not supported";
+    int rc = lsd_fail(ctx, LSD_EARG, t_create_err);
+    free_ctx(ctx);
+    return rc;
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || c.device < 0 || c.device >= ndev) {
+    t_create_err = ndev == 0 ? "no CUDA device" : "device index out of range";
     free_ctx(ctx);
     return LSD_ECUDA;
   }
@@ -508,7 +519,7 @@ int lsd_destroy(lsd_ctx* ctx) {
   return LSD_OK;
 }
 
-const char* lsd_last_error(const lsd_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+const char* lsd_last_error(const lsd_ctx* ctx) { return ctx ? ctx->err.c_str() : t_create_err.c_str(); }
 
 int lsd_get_sizes(const lsd_ctx* c, lsd_sizes* s) {
   if (!c || !s) return LSD_EARG;

@@ -134,7 +134,8 @@ class Context:
             h = _V()
             rc = self.lib.lsd_create(ctypes.byref(cfg), ctypes.byref(h))
             if rc != 0:
-                raise LsdError(rc, "lsd_create failed (check the configuration and the device)")
+                msg = self.lib.lsd_last_error(None)
+                raise LsdError(rc, "lsd_create: " + (msg.decode() if msg else ""))
         else:
             h = _handle
         self.h = h
