@@ -131,7 +131,9 @@ typedef struct lsd_config {
   int boussinesq, vel_tstep, cod_tstep, comp_tstep, mag_tstep;
   int precision;            /* LSD_PREC_* for the Legendre contraction                */
   int device;               /* CUDA device ordinal                                    */
-  int ozaki_slices;         /* int8 slices per operand for LSD_PREC_OZAKI (0 = default)*/
+  int ozaki_slices;         /* int8 slices per operand for LSD_PREC_OZAKI, 2..8 (0 = 7):
+                               S balanced base-256 digits carry 8S - 2 bits (rounded); 5
+                               keep 1000-step energies within ~1e-11 of FP64, 7 match FP64 */
   /* physics (parameters.F90_template:29-44) */
   double rratio, alpha, Ra, Ra_comp, Pr, Sc, Pm, E, Hyp;
   /* time integration (parameters.F90_template:229-243) */
