@@ -354,7 +354,8 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
     }
   };
   if (tid == 0) { issue(0); issue(1); }
-  // thread = (row r of the quarter, K eighth kq): 4 values per K step -> one word per slice
+  // thread = (row r of the quarter, warp kq): the synthesis gives warp kq the K eighth kq of
+  // every K step, the analysis whole (K step, 16-byte half) items in turn (below)
   const int r = tid & 31, kq = tid >> 5;
   for (int q = 0; q < 4; ++q) {
     const int R0 = zb * 128 + q * 32;
