@@ -139,7 +139,9 @@ namespace {
 constexpr int OZ_MAXS = 8;       // slices per operand
 constexpr int OZ_NC = 32;        // columns per chunk
 constexpr int OZ_MAXSTAGES = 4;  // bulk-copy ring: up to 4 stages, as many as leave two CTAs per SM
-constexpr int OZ_THREADS = 192;  // warps 0-3 epilogue (TMEM lane quarters), 4 copies, 5 MMA
+constexpr int OZ_EPI = 256;      // epilogue threads: warps 0-7 (warp w: TMEM lane quarter w % 4,
+                                 // column half w / 4 of a chunk)
+constexpr int OZ_THREADS = OZ_EPI + 64;  // + warp 8 (bulk copies) and warp 9 (MMA issue)
 constexpr int OZ_STG = OZ_NC + 1;  // epilogue staging row (doubles)
 constexpr int OZ_MAXG = 8;       // groups (output fields) of one launch
 
@@ -545,7 +547,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
   if (tid == 0) {
     for (int i = 0; i < nst; ++i) { umma::mbar_init(&full[i], 1); umma::mbar_init(&empty[i], 1); }
     umma::mbar_init(&accf, 1);
-    umma::mbar_init(&tfree, 128);
+    umma::mbar_init(&tfree, OZ_EPI);
     umma::mbar_init(&fin, 1);
     umma::fence_mbar_init();
   }
@@ -571,7 +573,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
     return pr;
   };
 
-  if (tid == 128) {
+  if (tid == OZ_EPI) {
     // ---- producer: A (z-block, K step) and B (chunk, K step) tiles into the ring
     int it = 0;
     bool ok = true;
@@ -597,7 +599,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
     // drain: the copies of the last stages have landed before the CTA can exit
     for (int j = (it > nst ? it - nst : 0); j < it; ++j)
       umma::mbar_wait(&full[j % nst], (j / nst) & 1, WAIT_ITERS);
-  } else if (tid == 160) {
+  } else if (tid == OZ_EPI + 32) {
     // ---- MMA issuer: the S(S+1)/2 digit pairs of a K step into S diagonals of 32 columns,
     // as S MMAs: A slice sa against B slices 0 .. S-1-sa at once (stacked in the stage, they
     // are one K-major operand of N = 32 (S - sa) rows), accumulating into the tensor-memory
@@ -630,8 +632,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
     }
     umma::commit(&fin);  // arrives when every MMA issued above has completed
     umma::mbar_wait(&fin, 0, WAIT_ITERS);
-  } else if (tid < 128) {
-    // ---- epilogue: row tid of each z-block
+  } else if (tid < OZ_EPI) {
+    // ---- epilogue: row (tid mod 128) of each z-block, columns 16 (tid / 128) .. + 15 of a
+    // chunk
+    const int row = tid & 127, half = tid >> 7;
     int cc = 0;
     OzProb nxt = prob(blockIdx.x);
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
@@ -653,7 +657,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
         pbase[tid] = base;
         pzero[tid] = zero;
       }
-      const int R = zb * 128 + tid;
+      const int R = zb * 128 + row;
       const bool live = R < a.nrows;
       // x y = 2^(ea + eb + 4) sum_d D_d 2^(-8(d+2)) = 2^(ea + eb + 4 - 8(S+1)) H with
       // H = Horner over d in 2^8; the power of two and the row scale 2^erow are one factor
@@ -662,33 +666,33 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
       for (int ch = 0; ch < pr.nchunk; ++ch, ++cc) {
         if (tid < OZ_NC) csc[tid] = pow2i(a.fexp[pr.fofs + ch * OZ_NC + tid]);
         const bool got = umma::mbar_wait(&accf, cc & 1, WAIT_ITERS);
-        if (!umma::bar_and(1, 128, got)) {  // uniform over the 128 epilogue threads
+        if (!umma::bar_and(1, OZ_EPI, got)) {  // uniform over the epilogue threads
           if (tid == 0) atomicExch(a.err, 1);
           ok = false;
           break;
         }
         umma::fence_after_sync();
 #pragma unroll
-        for (int c0 = 0; c0 < OZ_NC; c0 += 8) {
-          int32_t v[OZ_MAXS][8];
+        for (int c0 = 16 * half; c0 < 16 * half + 16; c0 += 4) {
+          int32_t v[OZ_MAXS][4];
 #pragma unroll
           for (int d = 0; d < OZ_MAXS; ++d)
-            if (d < S) umma::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * OZ_NC + c0), v[d]);
+            if (d < S) umma::tmem_ld4(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * OZ_NC + c0), v[d]);
           umma::tmem_wait_ld();
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
+          for (int q = 0; q < 4; ++q) {
             double hsum = (double)v[0][q];
 #pragma unroll
             for (int d = 1; d < OZ_MAXS; ++d)
               if (d < S) hsum = fma(hsum, 256.0, (double)v[d][q]);
-            stg[tid * OZ_STG + c0 + q] = hsum * (rsc * csc[c0 + q]);
+            stg[row * OZ_STG + c0 + q] = hsum * (rsc * csc[c0 + q]);
           }
         }
         umma::fence_before_sync();
         umma::mbar_arrive(&tfree);  // tensor memory may take the next chunk
-        umma::bar_sync(1, 128);
+        umma::bar_sync(1, OZ_EPI);
         // coalesced stores: row pairs (re, im) x 32 columns
-        for (int idx = tid; idx < 64 * OZ_NC; idx += 128) {
+        for (int idx = tid; idx < 64 * OZ_NC; idx += OZ_EPI) {
           const int pair = idx / OZ_NC, q = idx % OZ_NC;
           cplx* base = pbase[pair];
           if (!base) continue;
@@ -707,7 +711,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
             }
           }
         }
-        umma::bar_sync(1, 128);
+        umma::bar_sync(1, OZ_EPI);
       }
       if (!ok) break;
     }
