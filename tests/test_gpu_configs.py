@@ -9,12 +9,12 @@ The round trip is exact only up to the reference's Gauss nodes (Newton stopped a
 1e-13, auxiliary/gauwts.f), about 3e-11 at this size for any arithmetic, so it is
 checked against the oracle's own round trip of field 0 and bounded by 5e-11 per field.
 Variants: the plain FP64 contraction and the tensor-core contraction at several slice
-counts (S int8 slices of 7 bits, about 7S bits of the FP64 mantissa).
+counts (S balanced base-256 int8 digits, 8S - 2 bits of the FP64 mantissa, rounded).
 Tolerances, relative to the largest magnitude of the compared field:
   FP64            synthesis, analysis, round trip vs the oracle's: 1e-12
   tensor, S = 8   1e-13
   tensor, S = 7   5e-12
-  tensor, S = 4   1e-6    (28-bit digits, about FP32)
+  tensor, S = 4   1e-6    (30 bits, about FP32)
 config[2]: batched banded solves at N = 257, KL = 4, one operator per degree l < 256 for
 4 fields, every (l, m) right-hand side (Re and Im columns, 4 x 32896 x 2), residual
 |A x - b| / |b| <= 1e-13 on a sample checked on the host.
