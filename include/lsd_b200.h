@@ -290,9 +290,11 @@ int lsd_energies(lsd_ctx* ctx, double* out);
  * that cannot allocate when they write diagnostics (device memory fully committed to the
  * state, or work still queued on the stream that a cudaMalloc/cudaFree would stall).  The
  * norm scratch is a static device array sized for N <= 1024 shells (larger N returns
- * LSD_EARG); it is cleared by each call, shared by all contexts of a device, so overlapping
- * calls race.  The first call on a device does the set-up (symbol lookup): make it before
- * any stream capture. */
+ * LSD_EARG); every call overwrites all of it (nothing carries over between calls).  It is
+ * shared by all contexts of a device, so calls that overlap on the GPU (from two host
+ * threads or two streams) race on it.  Each call looks the array up (cudaGetSymbolAddress,
+ * no allocation); the first lookup in a process may load the module: make the first call
+ * before any stream capture. */
 int lsd_energies_static(lsd_ctx* ctx, double* out);
 /* The other time series, spectra and profiles of io_write2files (io.F90:290-340):
  * io_write_vel_energy / io_write_mag_energy partitions, io_write_cmb, io_write_nussel,

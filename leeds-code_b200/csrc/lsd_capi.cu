@@ -485,7 +485,9 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   TRY(dalloc(ctx, &ctx->d_cpart, (size_t)8 * ((H + 31) / 32)));
   TRY(dalloc(ctx, &ctx->d_cfl, (size_t)2 * N + 1));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));
-  ctx->h_pin_bytes = std::max(sizeof(cplx) * F * 3, sizeof(double) * 16);
+  // pinned staging: three spectral fields, and at least the host staging of the energy
+  // diagnostics ((75 + 2 KL) N + 6 doubles, lsd_energy_device / lsd_energy_static)
+  ctx->h_pin_bytes = std::max(sizeof(cplx) * F * 3, sizeof(double) * ((size_t)(75 + 2 * c.KL) * N + 16));
   CTRY(cudaMallocHost((void**)&ctx->h_pin, ctx->h_pin_bytes));
   TRY(lsd_build_tables(ctx));
   TRY(lsd_build_operators(ctx));

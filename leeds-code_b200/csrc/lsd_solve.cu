@@ -1090,8 +1090,9 @@ int lsd_corr(lsd_ctx* ctx) {
 namespace {
 
 // The derived fields (q, s, t and curl of velocity and field), their per-(field,
-// category, shell) norms summed into d_out (48 N doubles, zeroed here first), and host
-// copies of all that the radial sums need.  d_arrs: device room for 12 pointers.
+// category, shell) norms written to d_out (48 N doubles; k_norms writes every slot once,
+// each a fixed-order tree sum, so nothing needs clearing), and host copies of all that
+// the radial sums need.  d_arrs: device room for 12 pointers.
 // wts: 5 N (intr2dr, intr2dr_comp, _compS, _magdiss, _veldiss), ref: 7 N.
 int energy_partials(lsd_ctx* ctx, const cplx** d_arrs, double* d_out, double* Fh, double* wts, double* cod0,
                     double* bpolN, double* r, double* dr1, double* ref) {
@@ -1231,19 +1232,19 @@ int lsd_energy_device(lsd_ctx* ctx, double* out) {
 // its state arrays (cudaMalloc would fail), or one that keeps work queued on its stream
 // while it writes output (cudaMalloc / cudaFree synchronise the device and would stall that
 // pipeline).  The norm partial sums and the 12 field pointers live in a file-scope device
-// array instead of context memory; host staging uses the context's pinned buffer.  The
-// partial sums are accumulated with atomics, so they must start at zero: every call clears
-// them on the context's stream before the norm kernel.  Nothing else needs clearing.  The
-// array is shared by every context on a device, so overlapping calls (two threads, or two
-// streams) race on it.  The first call on a device looks the array up (set-up, which may
-// load this module): make that first call before any stream capture.
+// array instead of context memory; host staging uses the context's pinned buffer, which
+// lsd_create sizes for it.  The norm kernel writes every slot of the array once per call
+// (a fixed-order tree sum per slot, no atomics), so the previous call's contents are
+// simply overwritten and nothing is cleared.  The array is shared by every context on a
+// device, so calls that overlap on the GPU (two threads, or two streams) race on it.
+// Set-up: each call looks up the array's device address with cudaGetSymbolAddress, with
+// the context's device current (the lookup allocates nothing; the first lookup in a
+// process may load this module, so make the first call before any stream capture).
 namespace {
 constexpr int ESTATIC_MAX_N = 1024;  // shells
 constexpr int ESTATIC_PTRS = 16;     // 12 field pointers, padded to 128 bytes
-constexpr int ESTATIC_MAX_DEV = 64;
 }  // namespace
 static __device__ __align__(256) double g_energy_scratch[ESTATIC_PTRS + 48 * ESTATIC_MAX_N];  // 384 KiB + 128 B
-static double* g_energy_scratch_ptr[ESTATIC_MAX_DEV] = {};  // per device, filled by the first call
 
 int lsd_energy_static(lsd_ctx* ctx, double* out) {
   const int N = ctx->N, KL = ctx->KL;
@@ -1256,12 +1257,10 @@ int lsd_energy_static(lsd_ctx* ctx, double* out) {
   const size_t stage = (size_t)(48 + 5 + 1 + 7 + 2 * KL + 1 + 7) * N + 6;
   if (sizeof(double) * stage > ctx->h_pin_bytes)
     return lsd_fail(ctx, LSD_EARG, "lsd_energies_static: the context's pinned staging buffer is too small");
-  if (ctx->dev < 0 || ctx->dev >= ESTATIC_MAX_DEV) return lsd_fail(ctx, LSD_EARG, "lsd_energies_static: device index");
-  double*& dscr = g_energy_scratch_ptr[ctx->dev];
-  if (!dscr) {  // set-up, once per device, with that device current
+  double* dscr = nullptr;  // the array's address on the context's device (current here)
+  {
     cudaError_t e = cudaGetSymbolAddress((void**)&dscr, g_energy_scratch);
     if (e != cudaSuccess) {
-      dscr = nullptr;
       snprintf(msg, sizeof(msg), "lsd_energies_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
       return lsd_fail(ctx, LSD_ECUDA, msg);
     }

@@ -7,8 +7,8 @@
   codensity + composition, l^-2 seeded perturbations (a different seed per member).
   Checked by (a) the L = 64 member against the oracle after 5 steps (energies 1e-9) and
   (b) lock-step ensemble stepping against stand-alone stepping of the same member
-  (identical coefficients; the kernels are deterministic apart from the order of the
-  atomic norm sums, which enter only through dterr), then 200 ensemble steps.
+  (identical coefficients: every sum that feeds the state, dterr included, is formed in
+  a fixed order), then 200 ensemble steps.
 """
 import importlib
 import time

@@ -8,12 +8,12 @@ Tolerances (relative to the largest magnitude of the compared array):
   energies after 100 steps         1e-9
 """
 import importlib
-import json
 import os
 
 import numpy as np
 import pytest
 
+import case1_fixture as case1
 import oracle_lib as ol
 
 pkg = importlib.import_module("leeds-code_b200")
@@ -154,28 +154,23 @@ def test_hundred_steps_energies():
 
 
 @pytest.mark.gpu
-def test_golden_t0_energies_on_device():
-    """Device energies of the reference's tests/state.cdf.in equal its own t=0 output."""
-    z = np.load(os.path.join(GOLDEN, "state_case1.npz"))
-    cfg = capi.template_config(L=int(z["L"]), M=int(z["M"]), Mp=int(z["Mp"]), N=len(z["r"]),
-                               timestep=float(z["dt"]), Ra=float(z["Ra"]), Pr=float(z["Pr"]),
-                               Pm=float(z["Pm"]), E=float(z["E"]), rratio=float(z["riro"]), implicit=0.5)
+def test_golden_t0_energies_on_device(parity_report):
+    """Device energies of the reference's tests/state.cdf.in (read by state.load_state)
+    equal its own t=0 output row."""
+    cfg = case1.config()
     g = pkg.Context(cfg)
-    assert np.abs(g.radial_grid() - z["r"]).max() < 1e-14
-    l, m_, _ = state.folded_harmonics(cfg.L, cfg.M, cfg.Mp)
-    idx = state.state_nh(l, m_, cfg.L, cfg.M, cfg.Mp)
-    for name, f in (("uT", 0), ("uP", 1), ("C", 2), ("BT", 3), ("BP", 4)):
-        d = z[name]
-        g.set_coll(f, d[0, idx, :], d[1, idx, :])
-    e = g.energies()
-    gold = json.load(open(os.path.join(GOLDEN, "golden_t0.json")))
-    v, mg = gold["vel_energy_t0"], gold["mag_energy_t0"]
-    Pm = float(z["Pm"])
-    for got, want in ((e["KE"], v["KE"]), (e["KE_ax"], v["KE_ax"]), (e["topflx"], v["topflx"]),
-                      (e["botflx"], v["botflx"]), (e["KE_dis"] * 0.5 / Pm, v["Edis"]),
-                      (e["ME"] / 2, mg["ME"]), (e["ME_ax"] / 2, mg["ME_ax"]),
-                      (e["ME_dis"] / 2, mg["Mdis"]), (e["dipole"], mg["dipole"])):
-        assert abs(got - want) <= 1e-11 * abs(want), (got, want)
+    fields, r = case1.load(cfg)
+    assert np.abs(g.radial_grid() - r).max() < 1e-14
+    for f, (re, im) in fields.items():
+        g.set_coll(f, re, im)
+    e = case1.dat_columns(g.energies(), cfg.Pm)
+    want = case1.golden_rows()[0]
+    worst = 0.0
+    for k in ("KE", "KE_ax", "topflx", "botflx", "Edis", "ME", "ME_ax", "Mdis", "dipole"):
+        err = abs(e[k] - want[k]) / abs(want[k])
+        worst = max(worst, err)
+        assert err <= 1e-11, (k, e[k], want[k])
+    parity_report("t=0 energies vs reference row, max rel", worst, 1e-11)
     g.close()
 
 

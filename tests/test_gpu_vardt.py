@@ -1,6 +1,13 @@
 """CFL / corrector-controlled timestep (d_timestep < 0): non_maxtstep + tim_new_tstep
 before each predictor, operators rebuilt on a change (main.F90:126-134).
 
+i_time_step_control = 2 (below) and i_time_step_control = 1, the controller of every
+reference test case and of the Christensen benchmarks (tests/parameters-case1_symmetry.F90:
+237-243: d_timestep = -5e-5, d_corr_upper = 0.02, d_corr_lower = 0.002): tim_corr_dt is
+the corrector norm itself, dt halves above d_corr_upper, grows by 1.273974 below
+d_corr_lower (kept within 3 %), the first step takes min(dt/1e3, 1e-8), and the corrector
+repeats while its norm exceeds 1 (timestep.F90:744-777, 843-853).
+
 CPU: the oracle's first step uses dt = min(dt/1e3, 1e-10) * courant (tim_step == 0,
 timestep.F90:862) and later steps grow dt by at most 2/courant * courant = 2.
 GPU: the device against the oracle step by step over 40 steps (Boussinesq) and 20 steps
@@ -82,3 +89,62 @@ def test_variable_dt_boussinesq():
 def test_variable_dt_anelastic():
     cfg = syn.config_anelastic(L=16, N=17, timestep=-5e-5)
     run_pair(cfg, 20, prof=syn.polytrope_reference_state(cfg.N, cfg.rratio), composition=True)
+
+
+def control1_cfg(**kw):
+    base = dict(N=17, timestep=-5e-5, time_step_control=1, corr_upper=0.02, corr_lower=0.002)
+    base.update(kw)
+    return syn.config_parity(**base)
+
+
+def test_oracle_control1_dt_rules():
+    """The oracle's tim_new_tstep under i_time_step_control = 1: the first dt is
+    min(dt/1e3, 1e-8); afterwards each dt is the previous one, halved, or grown by
+    1.273974, as tim_corr_dt (the last corrector norm) lies above d_corr_upper, below
+    d_corr_lower or between (timestep.F90:843-853)."""
+    cfg = control1_cfg(L=16, M=16, N=13)
+    o = ol.Oracle(cfg)
+    for f, (re, im) in syn.boussinesq_state(cfg, seed=3).items():
+        o.set_coll(f, re, im)
+    o.set_time(0.0, 5e-5)
+    o.step(1)
+    dt = o.dt_control()[0]
+    assert dt == min(5e-5 / 1e3, 1e-8)
+    grew = False
+    for _ in range(12):
+        corr = o.dt_control()[1]
+        o.step(1)
+        new = o.dt_control()[0]
+        want = dt * (0.5 if corr > cfg.corr_upper else 1.273974 if corr < cfg.corr_lower else 1.0)
+        if not (want < dt * 0.97 or want > dt * 1.03):
+            want = dt
+        assert new == want, (dt, corr, new)
+        grew |= new > dt
+        dt = new
+    assert grew
+    o.close()
+
+
+@pytest.mark.gpu
+def test_variable_dt_control1():
+    """Device against the oracle step by step under i_time_step_control = 1: dt,
+    tim_corr_dt and the corrector count at every step, the state at the end."""
+    cfg = control1_cfg()
+    g, o = pkg.Context(cfg), ol.Oracle(cfg)
+    for f, (re, im) in syn.boussinesq_state(cfg, seed=23).items():
+        g.set_coll(f, re, im)
+        o.set_coll(f, re, im)
+    g.set_time(0.0, 5e-5)
+    o.set_time(0.0, 5e-5)
+    for k in range(30):
+        sg, so = g.step(1), o.step(1)
+        assert sg.correctors == so.correctors, k
+        a, b = g.dt_control(), o.dt_control()
+        assert a[0] == b[0] or abs(a[0] - b[0]) <= 1e-12 * b[0], (k, a, b)
+        assert abs(a[1] - b[1]) <= 1e-9 * abs(b[1]), (k, a, b)
+    for f in range(5):
+        a, b = g.get_coll(f), o.get_coll(f)
+        assert relerr(a[0], b[0]) < 1e-10, f
+        assert relerr(a[1], b[1]) < 1e-10, f
+    g.close()
+    o.close()

@@ -11,6 +11,7 @@ import pytest
 import scipy.linalg.lapack as lapack
 import scipy.special as sps
 
+import case1_fixture as case1
 import oracle_lib as ol
 
 capi = importlib.import_module("leeds-code_b200.capi")
@@ -18,41 +19,66 @@ state = importlib.import_module("leeds-code_b200.state")
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
-def case1_oracle():
-    z = np.load(os.path.join(GOLDEN, "state_case1.npz"))
-    cfg = capi.template_config(L=int(z["L"]), M=int(z["M"]), Mp=int(z["Mp"]), N=len(z["r"]),
-                               timestep=float(z["dt"]), Ra=float(z["Ra"]), Pr=float(z["Pr"]),
-                               Pm=float(z["Pm"]), E=float(z["E"]), rratio=float(z["riro"]),
-                               implicit=0.5)
+def case1_oracle(**over):
+    cfg = case1.config(**over)
     o = ol.Oracle(cfg)
-    l, m_, _ = state.folded_harmonics(cfg.L, cfg.M, cfg.Mp)
-    idx = state.state_nh(l, m_, cfg.L, cfg.M, cfg.Mp)
-    for name, f in (("uT", 0), ("uP", 1), ("C", 2), ("BT", 3), ("BP", 4)):
-        d = z[name]
-        o.set_coll(f, d[0, idx, :], d[1, idx, :])
-    return o, z
+    fields, r = case1.load(cfg)
+    for f, (re, im) in fields.items():
+        o.set_coll(f, re, im)
+    return o, cfg, r
 
 
 def test_golden_t0_energies():
-    """Energies of tests/state.cdf.in equal the reference's own t=0 output row (12 digits).
-    The shipped .dat files predate two prefactor changes in io_write2files
-    (io.F90:238-247): magnetic energy and ohmic dissipation were half of today's
-    Pm/E and 2Pm/E, viscous dissipation used 1/2 instead of Pm."""
-    o, z = case1_oracle()
-    np.testing.assert_allclose(o.radial_grid(), z["r"], rtol=0, atol=1e-15)
-    e = o.energies()
-    g = json.load(open(os.path.join(GOLDEN, "golden_t0.json")))
-    v, m = g["vel_energy_t0"], g["mag_energy_t0"]
-    Pm = float(z["Pm"])
-    checks = [
-        (e["KE"], v["KE"]), (e["KE_ax"], v["KE_ax"]), (e["topflx"], v["topflx"]),
-        (e["botflx"], v["botflx"]), (e["KE_dis"] * 0.5 / Pm, v["Edis"]),
-        (e["ME"] / 2, m["ME"]), (e["ME_ax"] / 2, m["ME_ax"]), (e["ME_dis"] / 2, m["Mdis"]),
-        (e["dipole"], m["dipole"]),
-    ]
-    for got, want in checks:
-        assert abs(got - want) <= 1e-11 * abs(want), (got, want)
-    assert abs(e["quadrupole"] - m["quadrupole"]) <= 1e-11 * abs(m["dipole"])
+    """Energies of the reference's tests/state.cdf.in, read by state.load_state, equal the
+    reference's own t=0 output row (12 digits).  The field is loaded in the current
+    normalisation (B / sqrt 2, tests/case1_fixture.py); the shipped .dat files predate
+    that and the viscous-dissipation prefactor change in io_write2files (io.F90:238-247)."""
+    o, cfg, r = case1_oracle()
+    np.testing.assert_allclose(o.radial_grid(), r, rtol=0, atol=1e-15)
+    e = case1.dat_columns(o.energies(), cfg.Pm)
+    want = case1.golden_rows()[0]
+    for k in ("KE", "KE_ax", "topflx", "botflx", "Edis", "ME", "ME_ax", "Mdis", "dipole"):
+        assert abs(e[k] - want[k]) <= 1e-11 * abs(want[k]), (k, e[k], want[k])
+    assert abs(e["quadrupole"] - want["quadrupole"]) <= 1e-11 * abs(want["dipole"])
+
+
+def test_golden_first_step():
+    """One timestep of the oracle from the reference's state (dt = 4.59265755232e-6, the
+    reference's first step; one predictor and one corrector, implicit 0.5) against the
+    reference's second output row: every energy increment within the band measured for
+    the restated equations (tests/case1_fixture.py, main.F90:100-164)."""
+    r0, r1 = case1.golden_rows()
+    o, cfg, _ = case1_oracle(timestep=r1["time"], time_step_control=1)
+    before = case1.dat_columns(o.energies(), cfg.Pm)
+    st = o.step(1)
+    assert st.steps_done == 1 and st.correctors == 1 and abs(st.t - r1["time"]) < 1e-20
+    after = case1.dat_columns(o.energies(), cfg.Pm)
+    case1.check_first_step(before, after)
+
+
+@pytest.mark.parametrize("L,M,Mp", [(48, 12, 4), (80, 20, 4), (64, 32, 2)])
+def test_load_state_truncation(L, M, Mp):
+    """io_load_state re-truncation (io.F90:1299-1354): a run with other L, M, Mp takes the
+    file's (l, m) where both have it; modes the file lacks start at zero (the reference
+    fills them with unseeded noise of amplitude d_init_pert)."""
+    from scipy.io import netcdf_file
+    f = netcdf_file(case1.state_file(), "r", mmap=False)
+    raw = np.array(f.variables["uP"].data, dtype=np.float64)
+    f.close()
+    fields, _, _, _ = state.load_state(case1.state_file(), L, M, Mp, 64)
+    re, im = fields[capi.VEL_POL]
+    l, m_, _ = state.folded_harmonics(L, M, Mp)
+    idx = state.state_nh(l, m_, 64, 16, 4)
+    assert re.shape == (len(l), 64)
+    for nh in range(len(l)):
+        if idx[nh] >= 0:
+            assert np.array_equal(re[nh], raw[0, idx[nh]]) and np.array_equal(im[nh], raw[1, idx[nh]])
+        else:
+            assert not re[nh].any() and not im[nh].any()
+    if L <= 64 and M * Mp <= 64 and Mp % 4 == 0:
+        assert (idx >= 0).all() and len(l) < raw.shape[1]  # truncated: every run mode from the file
+    else:
+        assert (idx >= 0).any() and (idx < 0).any()  # padded: some modes start at zero
 
 
 def test_layout_folded_order():
