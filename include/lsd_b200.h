@@ -161,6 +161,13 @@ typedef struct lsd_stats {
   double t, dt;             /* tim_t, tim_dt after the call                             */
 } lsd_stats;
 
+/* The loop-control variables of timestep.F90 (tim_t, tim_dt, tim_dterr, tim_corr_dt, the
+ * saved lasterr of tim_check_cgce, tim_cfl_dt, tim_it, tim_step, tim_pcn). */
+typedef struct lsd_pc_state {
+  double t, dt, dterr, corr_dt, lasterr, cfl_dt;
+  int it, step, pcn, reserved;
+} lsd_pc_state;
+
 typedef struct lsd_ctx lsd_ctx;
 
 /* Fill cfg with the template parameter values of Scripts/parameters.F90_template. */
@@ -282,8 +289,24 @@ int lsd_predictor(lsd_ctx* ctx);
 /* vel/cod/comp/mag _corrector (main.F90:148-154); *dterr gets tim_dterr. */
 int lsd_corrector(lsd_ctx* ctx, double* dterr);
 /* nsteps full timesteps (main loop main.F90:100-164: evaluation, predictor, evaluations
- * and correctors until tim_check_cgce converges), captured as one CUDA graph. */
+ * and correctors until tim_check_cgce converges).  All nsteps run as one launch of one
+ * CUDA graph with no host synchronisation inside: a device-side WHILE loop over the
+ * steps holds, per step, the evaluation, (d_timestep < 0: non_maxtstep + tim_new_tstep
+ * and, when dt changed, the operator rebuild in an IF node), the predictor, and a
+ * device-side WHILE loop of corrector evaluations + solves whose condition
+ * tim_check_cgce sets on the device.  A step begun by lsd_predictor / lsd_corrector
+ * calls is finished first, on the host. */
 int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats);
+/* tim_check_cgce (timestep.F90:744-830) on a caller-held loop state, after a corrector
+ * whose norm is s->dterr (i_time_step_control 1 or 2 from cfg): s->it becomes 0 when the
+ * step is complete or k + 1 when another corrector follows, s->dterr is reset.  Returns
+ * LSD_ENOTCONVERGED where the reference gives up (dt -> 0, more than 10 iterations, or a
+ * growing error above the limit).  Host only, no device work: lsd_step runs the same
+ * function on the device; this entry serves drivers that keep their own loop. */
+int lsd_tim_check_cgce(const lsd_config* cfg, lsd_pc_state* s);
+/* tim_new_tstep (timestep.F90:837-870) with the CFL limit s->cfl_dt: s->dt takes the next
+ * step's dt and *new_dt (tim_new_dt) is 1 when it changed by more than 3 %. */
+int lsd_tim_new_tstep(const lsd_config* cfg, lsd_pc_state* s, int* new_dt);
 /* Energy diagnostics (io_write_vel_energy / io_write_mag_energy), LSD_NENERGY doubles. */
 int lsd_energies(lsd_ctx* ctx, double* out);
 /* lsd_energies without any allocation: no counterpart in the reference.  For host codes

@@ -102,6 +102,13 @@ class LsdStats(ctypes.Structure):
                 ("dt", ctypes.c_double)]
 
 
+class LsdPcState(ctypes.Structure):
+    """lsd_pc_state: tim_t, tim_dt, tim_dterr, tim_corr_dt, lasterr, tim_cfl_dt, tim_it,
+    tim_step, tim_pcn of timestep.F90."""
+    _fields_ = [(n, ctypes.c_double) for n in ("t", "dt", "dterr", "corr_dt", "lasterr", "cfl_dt")] + \
+        [(n, ctypes.c_int) for n in ("it", "step", "pcn", "reserved")]
+
+
 def template_config(**overrides):
     """The parameter values of Scripts/parameters.F90_template, then `overrides`."""
     c = LsdConfig()

@@ -13,6 +13,8 @@
 
 #include "lsd_common.cuh"
 
+static_assert(sizeof(PcState) == sizeof(lsd_pc_state), "lsd_pc_state mirrors PcState");
+
 int lsd_fail(lsd_ctx* ctx, int code, const std::string& msg) {
   if (ctx) ctx->err = msg;
   return code;
@@ -25,10 +27,9 @@ void free_ctx(lsd_ctx* ctx) {
   if (!ctx) return;
   if (ctx->dev >= 0) cudaSetDevice(ctx->dev);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  if (ctx->g_pred) cudaGraphExecDestroy(ctx->g_pred);
-  if (ctx->g_corr) cudaGraphExecDestroy(ctx->g_corr);
-  if (ctx->g_eval) cudaGraphExecDestroy(ctx->g_eval);
-  if (ctx->g_psolve) cudaGraphExecDestroy(ctx->g_psolve);
+  if (ctx->g_step) cudaGraphExecDestroy(ctx->g_step);
+  for (cudaStream_t cs : ctx->cap_stream)
+    if (cs) cudaStreamDestroy(cs);
   lsd_ozaki_free(ctx);
   void* ptrs[] = {ctx->d_sblk_l, ctx->d_sblk_nh, ctx->d_aperm, ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_bin2c, ctx->d_lm2nh,
                   ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,
@@ -37,11 +38,13 @@ void free_ctx(lsd_ctx* ctx) {
                   ctx->d_sv, ctx->d_spec, ctx->d_four, ctx->d_phys, ctx->d_red, ctx->d_cpart, ctx->d_ref, ctx->d_laps,
                   ctx->d_compr1dr, ctx->d_wts, ctx->d_ones, ctx->d_cfl, ctx->d_icr, ctx->d_icdr, ctx->d_icradlap,
                   ctx->d_icr1dr, ctx->d_icintr2dr, ctx->d_icwts, ctx->d_icref, ctx->d_iclaps, ctx->d_iccompr1dr,
-                  ctx->d_icyt, ctx->d_icstate, ctx->d_icsv, ctx->d_rot, ctx->d_gwP0, ctx->d_grescr};
+                  ctx->d_icyt, ctx->d_icstate, ctx->d_icsv, ctx->d_rot, ctx->d_gwP0, ctx->d_grescr,
+                  ctx->d_pc, ctx->d_opfail};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
+  if (ctx->h_pc) cudaFreeHost(ctx->h_pc);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
@@ -126,57 +129,61 @@ int time_end(lsd_ctx* ctx) {
   return LSD_OK;
 }
 
-// tim_check_cgce (timestep.F90:744-830); returns LSD_ENOTCONVERGED when it gives up.
+// the host copy of the loop control (lsd_ctx fields) as the shared PcState and back
+PcState pc_get(const lsd_ctx* c) {
+  PcState s;
+  s.t = c->t; s.dt = c->dt; s.dterr = c->dterr; s.corr_dt = c->corr_dt; s.lasterr = c->lasterr;
+  s.cfl_dt = c->cfl_dt; s.it = c->it; s.step = c->step; s.pcn = c->tim_pcn; s.pad_ = 0;
+  return s;
+}
+void pc_put(lsd_ctx* c, const PcState& s) {
+  c->t = s.t; c->dt = s.dt; c->dterr = s.dterr; c->corr_dt = s.corr_dt; c->lasterr = s.lasterr;
+  c->cfl_dt = s.cfl_dt; c->it = s.it; c->step = s.step; c->tim_pcn = s.pcn;
+}
+PcParams pc_params(const lsd_config& g) {
+  PcParams p;
+  p.timestep = g.timestep; p.dterr = g.dterr; p.courant = g.courant; p.corr_upper = g.corr_upper;
+  p.corr_lower = g.corr_lower; p.control = g.time_step_control; p.pad_ = 0;
+  return p;
+}
+
+// tim_check_cgce (timestep.F90:744-830) on the host copy; LSD_ENOTCONVERGED when it gives up
 int check_cgce(lsd_ctx* c) {
-  int fail = 0;
-  const double dterr = c->dterr;
-  if (c->cfg.time_step_control == 1) {
-    if (c->it == 1) { c->corr_dt = dterr; c->lasterr = 1e99; }
-    if (c->dt < 1e-12 && c->step > 30) { c->it = 0; fail = 1; }
-    else if (c->it > 10) { c->it = 0; fail = 1; }
-    else if (dterr > c->lasterr) { if (dterr > 1.0) fail = 1; c->it = 0; }
-    else if (dterr > 1.0) { c->lasterr = dterr; c->it = c->it + 1; }
-    else c->it = 0;
-  } else {
-    if (c->it == 1) { c->corr_dt = c->dt * std::sqrt(c->cfg.dterr / dterr); c->lasterr = 1e99; }
-    if (c->dt < 1e-12 && c->step > 30) { c->it = 0; fail = 1; }
-    else if (c->it == c->tim_pcn) c->it = 0;
-    else if (c->it > 10) { c->it = 0; fail = 1; }
-    else if (dterr > c->lasterr) {
-      if (dterr > 2.0 * c->cfg.dterr) fail = 1;
-      if (dterr < 2.0 * c->cfg.dterr) c->corr_dt = c->dt / (1e1 * c->cfg.courant);
-      c->it = 0;
-    } else if (dterr > c->cfg.dterr) { c->lasterr = dterr; c->it = c->it + 1; }
-    else c->it = 0;
-  }
-  c->dterr = 0.0;
-  return fail ? LSD_ENOTCONVERGED : LSD_OK;
+  PcState s = pc_get(c);
+  const bool ok = pc_check_cgce(s, pc_params(c->cfg));
+  pc_put(c, s);
+  return ok ? LSD_OK : LSD_ENOTCONVERGED;
 }
 
 // queue the copy of the corrector's sums of squares (and the tensor-core error flag) to
 // the pinned mirror; finish_corrector_host reads them once the stream got there
 int enqueue_corrector_readback(lsd_ctx* ctx) {
   CUDA_TRY(cudaMemcpyAsync(ctx->h_red, ctx->d_red, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  int* oz_err = (int*)(ctx->h_red + 16);
+  int* oz_err = (int*)(ctx->h_red + LSD_HRED_OZERR);
   *oz_err = 0;
   if (ctx->oz) CUDA_TRY(cudaMemcpyAsync(oz_err, lsd_ozaki_err_flag(ctx), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   return LSD_OK;
 }
 
-// form tim_dterr (timestep.F90:715-737) from the mirrored sums of squares
+// tim_dterr (timestep.F90:715-737) from the corrector's sums of squares r[0..7], added to
+// d in the reference's field order
+__host__ __device__ inline double dterr_sum(double d, const double* r, bool comp) {
+  d = d + sqrt(r[0]);  // vel Tor
+  d = d + sqrt(r[1]);  // vel Pol
+  d = d + sqrt(r[2]);  // codensity
+  if (comp) d = d + sqrt(r[3]);
+  d = d + sqrt(r[4]);  // mag Tor
+  d = d + sqrt(r[5]);  // inner-core Tor
+  d = d + sqrt(r[6]);  // mag Pol
+  d = d + sqrt(r[7]);  // inner-core Pol
+  return d;
+}
+
+// form tim_dterr from the mirrored sums of squares
 int finish_corrector_host(lsd_ctx* ctx) {
-  const int* oz_err = (const int*)(ctx->h_red + 16);
+  const int* oz_err = (const int*)(ctx->h_red + LSD_HRED_OZERR);
   if (*oz_err) return lsd_fail(ctx, LSD_ECUDA, "tensor-core Legendre contraction: an mbarrier wait timed out");
-  const double* r = ctx->h_red;
-  double d = ctx->dterr;
-  d = d + std::sqrt(r[0]);  // vel Tor
-  d = d + std::sqrt(r[1]);  // vel Pol
-  d = d + std::sqrt(r[2]);  // codensity
-  if (ctx->cfg.comp_tstep) d = d + std::sqrt(r[3]);
-  d = d + std::sqrt(r[4]);  // mag Tor
-  d = d + std::sqrt(r[5]);  // inner-core Tor
-  d = d + std::sqrt(r[6]);  // mag Pol
-  d = d + std::sqrt(r[7]);  // inner-core Pol
+  const double d = dterr_sum(ctx->dterr, ctx->h_red, ctx->cfg.comp_tstep != 0);
   ctx->dterr = d;
   if (!std::isfinite(d)) return lsd_fail(ctx, LSD_ENONFINITE, "non-finite corrector norm (state diverged)");
   return LSD_OK;
@@ -189,70 +196,260 @@ int finish_corrector(lsd_ctx* ctx) {
   return finish_corrector_host(ctx);
 }
 
-enum CaptureKind { CAP_EVAL_PRED = 0, CAP_EVAL_CORR, CAP_EVAL, CAP_PRED };
-int capture(lsd_ctx* ctx, int kind, cudaGraphExec_t* out, long long* nkernels);
-int ensure_graphs(lsd_ctx* ctx) {
-  int rc;
-  if (!ctx->g_corr) {
-    if ((rc = capture(ctx, CAP_EVAL_CORR, &ctx->g_corr, &ctx->g_corr_kernels))) return rc;
-    if (ctx->cfg.timestep < 0) {
-      if ((rc = capture(ctx, CAP_EVAL, &ctx->g_eval, &ctx->g_eval_kernels))) return rc;
-      if ((rc = capture(ctx, CAP_PRED, &ctx->g_psolve, &ctx->g_psolve_kernels))) return rc;
-    } else {
-      if ((rc = capture(ctx, CAP_EVAL_PRED, &ctx->g_pred, &ctx->g_pred_kernels))) return rc;
-    }
-  }
-  return LSD_OK;
+// ---- the one-graph step -------------------------------------------------------------
+// Control kernels (one thread each) of the graph lsd_step launches.  The loop state lives
+// in the context's PcDev; the WHILE / IF conditions are set with cudaGraphSetConditional.
+// Every loop has a hard iteration cap besides the reference's own limits, so the graph
+// always ends: the step loop stops after the call's nsteps iterations, the corrector loop
+// after 64 correctors of one step (tim_check_cgce gives up after 11).
+constexpr int PC_MAX_CORR = 64;
+
+// start of the call: the host has uploaded the state, steps_left = nsteps, counters zero
+__global__ void k_pc_begin(PcDev* pc, cudaGraphConditionalHandle h_steps) {
+  cudaGraphSetConditional(h_steps, pc->steps_left > 0 && pc->status == LSD_OK ? 1u : 0u);
 }
 
-// tim_new_tstep (timestep.F90:837-870) with the CFL limit of the last evaluation; on a new
-// dt the operators are rebuilt (main.F90:126-134)
-int new_tstep(lsd_ctx* c) {
-  double dt = c->dt;
-  const lsd_config& g = c->cfg;
-  if (g.time_step_control == 1) {
-    if (c->corr_dt > g.corr_upper) dt = 0.5 * dt;
-    if (c->corr_dt < g.corr_lower) dt = 1.273974 * dt;
-    if (c->step == 0) dt = std::min(dt / 1e3, 1e-8);
-  } else {
-    if (c->corr_dt > 0.0) dt = std::min(c->corr_dt, dt * 2.0 / g.courant);
-    if (c->cfl_dt > 0.0) dt = std::min(c->cfl_dt, dt);
-    if (c->step == 0) dt = std::min(dt / 1e3, 1e-10);
-    dt = dt * g.courant;
-  }
-  if (dt < c->dt * 0.97 || dt > c->dt * 1.03) {
-    c->dt = dt;
-    return lsd_build_operators(c);
-  }
-  return LSD_OK;
+// d_timestep < 0, after the step's first evaluation: non_maxtstep's tim_cfl_dt and
+// tim_new_tstep (main.F90:126-134); the IF node that follows rebuilds the operators when
+// dt changed
+__global__ void k_pc_newdt(PcDev* pc, const double* cfl, PcParams p, cudaGraphConditionalHandle h_rebuild) {
+  pc->s.cfl_dt = *cfl;
+  const bool nd = pc_new_tstep(pc->s, p);
+  if (nd) pc->rebuilds++;
+  cudaGraphSetConditional(h_rebuild, nd ? 1u : 0u);
 }
 
-// the CFL limit of the evaluation queued last (d_cfl), read on the host
-int read_cfl(lsd_ctx* ctx) {
-  CUDA_TRY(cudaMemcpyAsync(ctx->h_red + 24, ctx->d_cfl + 2 * ctx->N, sizeof(double), cudaMemcpyDeviceToHost,
-                           ctx->stream));
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  ctx->cfl_dt = ctx->h_red[24];
-  return LSD_OK;
+// after the predictor (main.F90:136-147): tim_it = 1, and the corrector loop starts
+__global__ void k_pc_pred(PcDev* pc, cudaGraphConditionalHandle h_corr) {
+  pc->s.it = 1;
+  pc->evaluations++;
+  pc->iters = 0;
+  cudaGraphSetConditional(h_corr, pc->status == LSD_OK ? 1u : 0u);
 }
 
-int capture(lsd_ctx* ctx, int kind, cudaGraphExec_t* out, long long* nkernels) {
+// after a corrector (main.F90:148-155): tim_dterr, tim_check_cgce, and at the end of the
+// step tim_t += tim_dt, tim_step += 1 (main.F90:158-161)
+__global__ void k_pc_corr(PcDev* pc, const double* red, int comp, const int* oz_err, PcParams p,
+                          cudaGraphConditionalHandle h_corr) {
+  pc->evaluations++;
+  pc->correctors++;
+  pc->iters++;
+  const double d = dterr_sum(0.0, red, comp != 0);
+  pc->s.dterr = d;
+  pc->last_dterr = d;
+  int st = pc->status;
+  if (st == LSD_OK) {
+    if (oz_err && *oz_err) st = LSD_ECUDA;
+    else if (!isfinite(d)) st = LSD_ENONFINITE;
+    else if (!pc_check_cgce(pc->s, p)) st = LSD_ENOTCONVERGED;
+    else if (pc->s.it == 0) {
+      pc->s.t = pc->s.t + pc->s.dt;
+      pc->s.step = pc->s.step + 1;
+      pc->steps_done++;
+      pc->steps_left--;
+    } else if (pc->iters >= PC_MAX_CORR) st = LSD_ENOTCONVERGED;
+  }
+  pc->status = st;
+  cudaGraphSetConditional(h_corr, st == LSD_OK && pc->s.it != 0 ? 1u : 0u);
+}
+
+// end of a step-loop iteration
+__global__ void k_pc_end(PcDev* pc, cudaGraphConditionalHandle h_steps) {
+  pc->loops++;
+  const bool more = pc->status == LSD_OK && pc->steps_left > 0 && pc->loops < pc->nsteps;
+  cudaGraphSetConditional(h_steps, more ? 1u : 0u);
+}
+
+// Adds a conditional node of `type` on handle h at the current point of the capture on
+// `s` and returns its body graph; the capture on s continues after the node.
+int cap_conditional(lsd_ctx* ctx, cudaStream_t s, cudaGraphConditionalNodeType type,
+                    cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs;
   cudaGraph_t g = nullptr;
-  CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
-  long long before = ctx->launches;
-  int rc = kind == CAP_PRED ? LSD_OK : lsd_eval(ctx);
-  if (!rc && kind == CAP_EVAL_PRED) rc = lsd_pred(ctx);
-  if (!rc && kind == CAP_EVAL_CORR) rc = lsd_corr(ctx);
-  if (!rc && kind == CAP_PRED) rc = lsd_pred(ctx);
-  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-  *nkernels = ctx->launches - before;
-  ctx->launches = before;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  CUDA_TRY(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) return lsd_fail(ctx, LSD_ECUDA, "graph capture: stream not capturing");
+  cudaGraphNodeParams prm = {};
+  prm.type = cudaGraphNodeTypeConditional;
+  prm.conditional.handle = h;
+  prm.conditional.type = type;
+  prm.conditional.size = 1;
+  cudaGraphNode_t node;
+  CUDA_TRY(cudaGraphAddNode(&node, g, deps, nd, &prm));
+  *body = prm.conditional.phGraph_out[0];
+  CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  return LSD_OK;
+}
+
+// a conditional handle of the graph being captured on s (reset to 0 at every launch)
+int cap_handle(lsd_ctx* ctx, cudaStream_t s, cudaGraphConditionalHandle* h) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr));
+  CUDA_TRY(cudaGraphConditionalHandleCreate(h, g, 0, cudaGraphCondAssignDefault));
+  return LSD_OK;
+}
+
+// Captures into `body` on capture stream k whatever fn launches on ctx->stream.
+template <class F>
+int cap_body(lsd_ctx* ctx, int k, cudaGraph_t body, F fn) {
+  cudaStream_t cs = ctx->cap_stream[k], saved = ctx->stream;
+  CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  ctx->stream = cs;
+  int rc = fn();
+  ctx->stream = saved;
+  cudaGraph_t out = nullptr;
+  cudaError_t e = cudaStreamEndCapture(cs, &out);
+  if (rc) return rc;
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("graph body capture: ") + cudaGetErrorString(e));
+  return LSD_OK;
+}
+
+// The whole of lsd_step as one graph (structure in include/lsd_b200.h at lsd_step).
+int capture_step(lsd_ctx* ctx) {
+  for (cudaStream_t& cs : ctx->cap_stream)
+    if (!cs) CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  const PcParams prm = pc_params(ctx->cfg);
+  const bool vardt = ctx->cfg.timestep < 0;
+  PcDev* pc = ctx->d_pc;
+  const int* ozerr = ctx->oz ? lsd_ozaki_err_flag(ctx) : nullptr;
+  cudaStream_t s0 = ctx->stream;
+  const long long l0 = ctx->launches;
+  long long loop = 0, rebuild = 0, corr = 0;
+  CUDA_TRY(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed));
+  int rc = LSD_OK;
+  cudaGraphConditionalHandle h_steps = 0;
+  cudaGraph_t b_steps = nullptr;
+  if (!rc) rc = cap_handle(ctx, s0, &h_steps);
+  if (!rc) {
+    k_pc_begin<<<1, 1, 0, s0>>>(pc, h_steps);
+    rc = cap_conditional(ctx, s0, cudaGraphCondTypeWhile, h_steps, &b_steps);
+  }
+  if (!rc) rc = cap_body(ctx, 0, b_steps, [&]() {
+    cudaStream_t s1 = ctx->stream;
+    const long long a = ctx->launches;
+    int r = lsd_eval(ctx);
+    if (!r && vardt) {
+      cudaGraphConditionalHandle h_rb = 0;
+      cudaGraph_t b_rb = nullptr;
+      if (!r) r = cap_handle(ctx, s1, &h_rb);
+      if (!r) {
+        k_pc_newdt<<<1, 1, 0, s1>>>(pc, ctx->d_cfl + 2 * ctx->N, prm, h_rb);
+        ++ctx->launches;
+        r = cap_conditional(ctx, s1, cudaGraphCondTypeIf, h_rb, &b_rb);
+      }
+      if (!r) r = cap_body(ctx, 1, b_rb, [&]() {
+        const long long b = ctx->launches;
+        int q = lsd_launch_operator_build(ctx, &pc->s.dt, &pc->status);
+        rebuild = ctx->launches - b;
+        return q;
+      });
+    }
+    if (!r) r = lsd_pred(ctx);
+    cudaGraphConditionalHandle h_corr = 0;
+    cudaGraph_t b_corr = nullptr;
+    if (!r) r = cap_handle(ctx, s1, &h_corr);
+    if (!r) {
+      k_pc_pred<<<1, 1, 0, s1>>>(pc, h_corr);
+      ++ctx->launches;
+      r = cap_conditional(ctx, s1, cudaGraphCondTypeWhile, h_corr, &b_corr);
+    }
+    if (!r) r = cap_body(ctx, 1, b_corr, [&]() {
+      const long long b = ctx->launches;
+      int q = lsd_eval(ctx);
+      if (!q) q = lsd_corr(ctx);
+      if (!q) {
+        k_pc_corr<<<1, 1, 0, ctx->stream>>>(pc, ctx->d_red, ctx->cfg.comp_tstep, ozerr, prm, h_corr);
+        ++ctx->launches;
+      }
+      corr = ctx->launches - b;
+      return q;
+    });
+    if (!r) {
+      k_pc_end<<<1, 1, 0, s1>>>(pc, h_steps);
+      ++ctx->launches;
+    }
+    loop = ctx->launches - a - corr - rebuild;
+    return r;
+  });
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s0, &g);
+  ctx->launches = l0;
   if (rc) { if (g) cudaGraphDestroy(g); return rc; }
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-  e = cudaGraphInstantiate(out, g, 0);
+  e = cudaGraphInstantiate(&ctx->g_step, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("step graph: ") + cudaGetErrorString(e));
+  ctx->k_begin = 1;
+  ctx->k_loop = loop;
+  ctx->k_rebuild = rebuild;
+  ctx->k_corr = corr;
   return LSD_OK;
+}
+
+// A step begun by lsd_predictor / lsd_corrector calls (tim_it != 0): its remaining
+// correctors on the host, with tim_check_cgce after each (main.F90:148-161).
+int finish_open_step(lsd_ctx* ctx, int* corr, int* evals, double* last) {
+  while (ctx->it != 0) {
+    ctx->dterr = 0.0;
+    int rc = lsd_eval(ctx);
+    if (!rc) rc = lsd_corr(ctx);
+    if (!rc) rc = finish_corrector(ctx);
+    if (rc) return rc;
+    ++*corr;
+    *evals += 1;
+    *last = ctx->dterr;
+    if ((rc = check_cgce(ctx))) return lsd_fail(ctx, rc, "tim_check_cgce: corrector iterations did not converge");
+  }
+  ctx->t = ctx->t + ctx->dt;
+  ctx->step = ctx->step + 1;
+  return LSD_OK;
+}
+
+// Queue one launch of the step graph for nsteps steps: the loop state goes up with it and
+// comes back into the pinned mirror (read by step_graph_finish after the stream is done).
+int step_graph_enqueue(lsd_ctx* ctx, int nsteps) {
+  if (!ctx->g_step) {
+    int rc = capture_step(ctx);
+    if (rc) return rc;
+  }
+  PcDev* h = ctx->h_pc;
+  std::memset(h, 0, sizeof(PcDev));
+  h->s = pc_get(ctx);
+  h->s.dterr = 0.0;
+  h->steps_left = nsteps;
+  h->nsteps = nsteps;
+  h->status = LSD_OK;
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_pc, h, sizeof(PcDev), cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(cudaGraphLaunch(ctx->g_step, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(h, ctx->d_pc, sizeof(PcDev), cudaMemcpyDeviceToHost, ctx->stream));
+  return LSD_OK;
+}
+
+// after the stream passed the graph: the loop state back into the context, the counts of
+// the call, and its outcome
+int step_graph_finish(lsd_ctx* ctx, int* done, int* corr, int* evals, double* last, long long* kernels) {
+  const PcDev& h = *ctx->h_pc;
+  const bool dt_changed = h.rebuilds > 0;
+  pc_put(ctx, h.s);
+  ctx->dterr = 0.0;
+  *done += h.steps_done;
+  *corr += h.correctors;
+  *evals += h.evaluations;
+  if (h.correctors > 0) *last = h.last_dterr;
+  *kernels += ctx->k_begin + (long long)h.loops * ctx->k_loop + (long long)h.correctors * ctx->k_corr +
+              (long long)h.rebuilds * ctx->k_rebuild;
+  if (dt_changed) ctx->op_dt = ctx->dt;
+  switch (h.status) {
+    case LSD_OK: return LSD_OK;
+    case LSD_ENOTCONVERGED: return lsd_fail(ctx, LSD_ENOTCONVERGED, "tim_check_cgce: corrector iterations did not converge");
+    case LSD_ENONFINITE: return lsd_fail(ctx, LSD_ENONFINITE, "non-finite corrector norm (state diverged)");
+    case LSD_ESINGULAR: return lsd_fail(ctx, LSD_ESINGULAR, "operator rebuild after a dt change: zero pivot or singular influence matrix");
+    default: return lsd_fail(ctx, LSD_ECUDA, "tensor-core Legendre contraction: an mbarrier wait timed out");
+  }
 }
 
 }  // namespace
@@ -489,6 +686,10 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   // diagnostics ((75 + 2 KL) N + 6 doubles, lsd_energy_device / lsd_energy_static)
   ctx->h_pin_bytes = std::max(sizeof(cplx) * F * 3, sizeof(double) * ((size_t)(75 + 2 * c.KL) * N + 16));
   CTRY(cudaMallocHost((void**)&ctx->h_pin, ctx->h_pin_bytes));
+  TRY(dalloc(ctx, &ctx->d_pc, 1));
+  TRY(dalloc(ctx, &ctx->d_opfail, 1));
+  CTRY(cudaMallocHost((void**)&ctx->h_pc, sizeof(PcDev)));
+  CTRY(cudaMemset(ctx->d_pc, 0, sizeof(PcDev)));
   TRY(lsd_build_tables(ctx));
   TRY(lsd_build_operators(ctx));
   if (c.precision == LSD_PREC_OZAKI) TRY(lsd_ozaki_setup(ctx));
@@ -1019,42 +1220,22 @@ int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats) {
   if (!ctx || nsteps < 0) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
   int rc;
-  long long l0 = ctx->launches;
-  if ((rc = ensure_graphs(ctx))) return rc;
-  const long long per_pred = ctx->g_pred_kernels, per_corr = ctx->g_corr_kernels;
   int done = 0, corr = 0, evals = 0;
+  long long kernels = 0;
   double last = 0.0;
+  const long long l0 = ctx->launches;
   if ((rc = time_begin(ctx))) return rc;
-  const bool vardt = ctx->cfg.timestep < 0;
-  while (done < nsteps) {
-    if (ctx->it == 0 && vardt) {  // evaluation, then non_maxtstep + tim_new_tstep (main.F90:126-134)
-      CUDA_TRY(cudaGraphLaunch(ctx->g_eval, ctx->stream));
-      ctx->launches += ctx->g_eval_kernels;
-      ++evals;
-      if ((rc = read_cfl(ctx)) || (rc = new_tstep(ctx))) return rc;
-      CUDA_TRY(cudaGraphLaunch(ctx->g_psolve, ctx->stream));
-      ctx->launches += ctx->g_psolve_kernels;
-      ctx->it = 1;
-    } else if (ctx->it == 0) {
-      CUDA_TRY(cudaGraphLaunch(ctx->g_pred, ctx->stream));
-      ctx->launches += per_pred;
-      ++evals;
-      ctx->it = 1;
-    } else {
-      ctx->dterr = 0.0;
-      CUDA_TRY(cudaGraphLaunch(ctx->g_corr, ctx->stream));
-      ctx->launches += per_corr;
-      ++evals;
-      ++corr;
-      if ((rc = finish_corrector(ctx))) return rc;
-      last = ctx->dterr;
-      if ((rc = check_cgce(ctx))) return lsd_fail(ctx, rc, "tim_check_cgce: corrector iterations did not converge");
-    }
-    if (ctx->it == 0) {
-      ctx->t = ctx->t + ctx->dt;
-      ctx->step = ctx->step + 1;
-      ++done;
-    }
+  if (ctx->it != 0 && nsteps > 0) {
+    if ((rc = finish_open_step(ctx, &corr, &evals, &last))) return rc;
+    ++done;
+    kernels += ctx->launches - l0;
+  }
+  if (done < nsteps) {
+    if ((rc = step_graph_enqueue(ctx, nsteps - done))) return rc;
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    rc = step_graph_finish(ctx, &done, &corr, &evals, &last, &kernels);
+    ctx->launches = l0 + kernels;
+    if (rc) return rc;
   }
   if ((rc = time_end(ctx))) return rc;
   ctx->have_eval = false;
@@ -1066,12 +1247,10 @@ int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats) {
   return LSD_OK;
 }
 
-// ---- ensembles: independent runs advanced in lock-step, one stream each ------------------
-// Each pass enqueues, for every member still short of its steps, the graphs up to its
-// next host decision (predictor + first corrector of a new step, or one more corrector)
-// and the copy of its corrector norms, on the member's own stream; only then does the
-// host wait, member by member, and apply tim_check_cgce.  The members' kernels therefore
-// share the device while any one of them waits for its host decision.
+// ---- ensembles: independent runs stepped together ---------------------------------------
+// Every member's step graph (all nsteps of its loop, no host decision inside) is launched
+// on the member's own stream before the host waits for any of them, so the members'
+// kernels share the device for the whole call.
 struct lsd_ensemble {
   std::vector<lsd_ctx*> m;
   std::string err;
@@ -1128,79 +1307,27 @@ int lsd_ensemble_step(lsd_ensemble* e, int nsteps, lsd_stats* stats) {
   };
   if (cudaSetDevice(e->m[0]->dev) != cudaSuccess) return LSD_ECUDA;
   std::vector<int> done(n, 0), corr(n, 0), evals(n, 0);
-  std::vector<long long> l0(n);
+  std::vector<long long> l0(n), kernels(n, 0);
   std::vector<double> last(n, 0.0);
   for (int i = 0; i < n; ++i) {
-    int rc = ensure_graphs(e->m[i]);
+    lsd_ctx* c = e->m[i];
+    l0[i] = c->launches;
+    int rc = time_begin(c);
+    if (!rc && c->it != 0 && nsteps > 0) {  // a step begun by single predictor / corrector calls
+      rc = finish_open_step(c, &corr[i], &evals[i], &last[i]);
+      if (!rc) { ++done[i]; kernels[i] += c->launches - l0[i]; }
+    }
+    if (!rc && done[i] < nsteps) rc = step_graph_enqueue(c, nsteps - done[i]);
     if (rc) return fail(i, rc);
-    l0[i] = e->m[i]->launches;
-    if ((rc = time_begin(e->m[i]))) return fail(i, rc);
-  }
-  std::vector<char> pending(n, 0);
-  for (;;) {
-    // members with d_timestep < 0 that start a step: evaluation, then the dt decision
-    for (int i = 0; i < n; ++i) {
-      lsd_ctx* c = e->m[i];
-      pending[i] = 0;
-      if (done[i] >= nsteps || c->it != 0 || c->cfg.timestep >= 0) continue;
-      if (cudaGraphLaunch(c->g_eval, c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "graph launch"));
-      c->launches += c->g_eval_kernels;
-      ++evals[i];
-      if (cudaMemcpyAsync(c->h_red + 24, c->d_cfl + 2 * c->N, sizeof(double), cudaMemcpyDeviceToHost, c->stream) !=
-          cudaSuccess)
-        return fail(i, lsd_fail(c, LSD_ECUDA, "cfl readback"));
-      pending[i] = 1;
-    }
-    for (int i = 0; i < n; ++i) {
-      if (!pending[i]) continue;
-      lsd_ctx* c = e->m[i];
-      if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "stream"));
-      c->cfl_dt = c->h_red[24];
-      int rc = new_tstep(c);
-      if (rc) return fail(i, rc);
-      if (cudaGraphLaunch(c->g_psolve, c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "graph launch"));
-      c->launches += c->g_psolve_kernels;
-      c->it = 1;
-    }
-    bool any = false;
-    for (int i = 0; i < n; ++i) {  // enqueue up to each member's next host decision
-      lsd_ctx* c = e->m[i];
-      pending[i] = 0;
-      if (done[i] >= nsteps) continue;
-      if (c->it == 0) {
-        if (cudaGraphLaunch(c->g_pred, c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "graph launch"));
-        c->launches += c->g_pred_kernels;
-        ++evals[i];
-        c->it = 1;
-      }
-      c->dterr = 0.0;
-      if (cudaGraphLaunch(c->g_corr, c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "graph launch"));
-      c->launches += c->g_corr_kernels;
-      ++evals[i];
-      ++corr[i];
-      int rc = enqueue_corrector_readback(c);
-      if (rc) return fail(i, rc);
-      pending[i] = 1;
-      any = true;
-    }
-    if (!any) break;
-    for (int i = 0; i < n; ++i) {  // host decisions (tim_check_cgce), member by member
-      if (!pending[i]) continue;
-      lsd_ctx* c = e->m[i];
-      if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "stream"));
-      int rc = finish_corrector_host(c);
-      if (rc) return fail(i, rc);
-      last[i] = c->dterr;
-      if ((rc = check_cgce(c))) return fail(i, lsd_fail(c, rc, "tim_check_cgce: corrector iterations did not converge"));
-      if (c->it == 0) {
-        c->t = c->t + c->dt;
-        c->step = c->step + 1;
-        ++done[i];
-      }
-    }
   }
   for (int i = 0; i < n; ++i) {
     lsd_ctx* c = e->m[i];
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "stream"));
+    if (done[i] < nsteps) {
+      int rc = step_graph_finish(c, &done[i], &corr[i], &evals[i], &last[i], &kernels[i]);
+      c->launches = l0[i] + kernels[i];
+      if (rc) return fail(i, rc);
+    }
     int rc = time_end(c);
     if (rc) return fail(i, rc);
     c->have_eval = false;
@@ -1210,6 +1337,25 @@ int lsd_ensemble_step(lsd_ensemble* e, int nsteps, lsd_stats* stats) {
       stats[i].t = c->t; stats[i].dt = c->dt;
     }
   }
+  return LSD_OK;
+}
+
+int lsd_tim_check_cgce(const lsd_config* cfg, lsd_pc_state* s) {
+  if (!cfg || !s) return LSD_EARG;
+  PcState st;
+  std::memcpy(&st, s, sizeof(st));
+  const bool ok = pc_check_cgce(st, pc_params(*cfg));
+  std::memcpy(s, &st, sizeof(st));
+  return ok ? LSD_OK : LSD_ENOTCONVERGED;
+}
+
+int lsd_tim_new_tstep(const lsd_config* cfg, lsd_pc_state* s, int* new_dt) {
+  if (!cfg || !s) return LSD_EARG;
+  PcState st;
+  std::memcpy(&st, s, sizeof(st));
+  const bool nd = pc_new_tstep(st, pc_params(*cfg));
+  std::memcpy(s, &st, sizeof(st));
+  if (new_dt) *new_dt = nd ? 1 : 0;
   return LSD_OK;
 }
 

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "../../include/lsd_b200.h"
+#include "lsd_control.cuh"
 
 #define LSD_MAX_KL 8
 
@@ -19,6 +20,10 @@ typedef double2 cplx;
       return lsd_fail(ctx, LSD_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e__)); \
     }                                                                                \
   } while (0)
+
+// slots of the pinned mirror h_red: corrector sums of squares [0, 8), the tensor-core error
+// flag (as int) at 16, tim_cfl_dt at 24, dt staged for the operator build at 32
+enum { LSD_HRED_OZERR = 16, LSD_HRED_CFL = 24, LSD_HRED_DT = 32 };
 
 // Kernel families counted for lsd_kernel_launches
 #define LSD_LAUNCH(ctx) ((ctx)->launches++)
@@ -170,20 +175,22 @@ struct lsd_ctx {
   // reductions
   double *d_red = nullptr;   // small reduction area
   double *d_cpart = nullptr; // corrector: per-warp sums of squares [8][ceil(H / 32)]
-  double *h_red = nullptr;   // pinned mirror
+  double *h_red = nullptr;   // pinned mirror (64 doubles; slots below)
   // time
   double t = 0.0, dt = 0.0, dterr = 0.0, corr_dt = 0.0, lasterr = 1e99, cfl_dt = 0.0;
   double* d_cfl = nullptr;  // variable dt: [2N] per-shell CFL maxima + tim_cfl_dt
   int it = 0, step = 0;
   bool have_eval = false;
   int tim_pcn = -1;
-  // CUDA graph of one (evaluation + predictor/corrector) pass
-  cudaGraphExec_t g_pred = nullptr, g_corr = nullptr;
-  long long g_pred_kernels = 0, g_corr_kernels = 0;
-  // variable dt: the evaluation and the predictor solve as separate graphs (a host
-  // decision on dt sits between them)
-  cudaGraphExec_t g_eval = nullptr, g_psolve = nullptr;
-  long long g_eval_kernels = 0, g_psolve_kernels = 0;
+  // the one-graph step (lsd_step): the device control block and its pinned mirror, the
+  // operator build's failure flag, the graph, the streams its conditional bodies are
+  // captured on, and the kernels of each section (for lsd_stats.kernel_launches)
+  PcDev* d_pc = nullptr;
+  PcDev* h_pc = nullptr;
+  int* d_opfail = nullptr;
+  cudaGraphExec_t g_step = nullptr;
+  cudaStream_t cap_stream[2] = {nullptr, nullptr};
+  long long k_begin = 0, k_loop = 0, k_rebuild = 0, k_corr = 0;
   void* oz = nullptr;  // tensor-core path state (lsd_ozaki.cu)
 };
 
@@ -193,6 +200,7 @@ int lsd_fail(lsd_ctx* ctx, int code, const std::string& msg);
 int lsd_build_tables(lsd_ctx* ctx);
 int lsd_build_radial(lsd_ctx* ctx);
 int lsd_build_operators(lsd_ctx* ctx);
+int lsd_launch_operator_build(lsd_ctx* ctx, const double* dtp, int* status);
 // ---- transforms (lsd_sht.cu, lsd_fft.cu) ----
 int lsd_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups);
 int lsd_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups);

@@ -272,7 +272,7 @@ __global__ void k_bands(int N, int KL, const double* r, const double* dr, const 
 // boundary rows, factorise; build Y in the solve layout [fam][N][2KL+1][L].
 // ---------------------------------------------------------------------------------------
 struct OpParams {
-  double c1_[OP_NFAM], c2_[OP_NFAM], c2y[OP_NFAM];
+  double c1[OP_NFAM], c2_[OP_NFAM], c2y[OP_NFAM];  // X = c1 / dt + c2_ (.), Y = c1 / dt - c2y (.)
   double Hyp;
   int vel_bc, cod_bc, comp_bc;
   int anelastic;
@@ -313,8 +313,8 @@ __device__ double anel_diag(int fam, int l, int n, int N, const double* r, const
 // it there (dgbtf2 at shared-memory latency: one matrix per thread on global memory took
 // 1.3 ms per rebuild at L = 128, N = 129), and the lanes write it out.  wpb warps per CTA.
 __global__ void k_build_ops(int N, int NL, int KL, int L, int wpb, const double* r, const double* dr,
-                            const double* radlap, const double* laps, const double* ref, OpParams P, double* lu,
-                            int* ipiv, double* y, int* info) {
+                            const double* radlap, const double* laps, const double* ref, OpParams P,
+                            const double* dtp, double* lu, int* ipiv, double* y, int* info) {
   extern __shared__ double osm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int l = blockIdx.x * wpb + warp;
@@ -340,7 +340,7 @@ __global__ void k_build_ops(int N, int NL, int KL, int L, int wpb, const double*
     for (int i = lane; i < ld * N; i += 32) Ag[i] = A[i];
     return;
   }
-  const double c1_ = P.c1_[fam], c2_ = P.c2_[fam], c2y = P.c2y[fam];
+  const double c1_ = P.c1[fam] / *dtp, c2_ = P.c2_[fam], c2y = P.c2y[fam];  // c1 / dt
   const double ll1 = (double)(l * (l + 1));
   // A(KL+1:, :) = -c2_ * Lap.  Boussinesq: radLap == radLap_flayer == GreLap == MagTorLap
   // == MagPolLap bit for bit (f_factor = 1, xi = 0, eta = 1, deta = 0); anelastic: CompLap
@@ -477,7 +477,7 @@ __global__ void k_lu_transpose(int N, int NL, int icfam, int KL, int L, const do
 // One warp per (l, k), k = 0 toroidal, 1 poloidal, in shared memory as k_build_ops.
 __global__ void k_build_icops(int N, int Ni, int KL, int L, int wpb, const double* r, const double* dr,
                               const double* radlap, const double* icr, const double* icdr, const double* icradlap,
-                              OpParams P, double* lu, int* ipiv, double* icyt, int* info) {
+                              OpParams P, const double* dtp, double* lu, int* ipiv, double* icyt, int* info) {
   extern __shared__ double osm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int l = blockIdx.x * wpb + warp, k = blockIdx.y;
@@ -499,7 +499,7 @@ __global__ void k_build_icops(int N, int Ni, int KL, int L, int wpb, const doubl
     for (int i = lane; i < ld * NL; i += 32) Ag[i] = A[i];
     return;
   }
-  const double c1_ = P.c1_[fam], c2_ = P.c2_[fam], c2y = P.c2y[fam];
+  const double c1_ = P.c1[fam] / *dtp, c2_ = P.c2_[fam], c2y = P.c2y[fam];  // c1 / dt
   const double ll1 = (double)(l * (l + 1));
   const double* rm2 = r + (size_t)1 * N;
   const double* rm1 = r + (size_t)2 * N;
@@ -623,15 +623,34 @@ int lsd_build_radial(lsd_ctx* ctx) {
   return LSD_OK;
 }
 
-int lsd_build_operators(lsd_ctx* ctx) {
+namespace {
+// After an operator build: the step's dt into rot's slot (rot_predictor / rot_corrector
+// read it there), and LSD_ESINGULAR into *status (when given) if a factorisation met a
+// zero pivot (mes_lu_find, meshs.F90:447-473) or an influence matrix was singular.
+__global__ void k_ops_finish(const double* dtp, double* rot_dt, const int* info, int ninfo, const int* fail,
+                             int* status) {
+  __shared__ int bad;
+  if (threadIdx.x == 0) { bad = *fail; *rot_dt = *dtp; }
+  __syncthreads();
+  for (int i = threadIdx.x; i < ninfo; i += blockDim.x)
+    if (info[i] != 0) bad = 1;
+  __syncthreads();
+  if (threadIdx.x == 0 && bad && status && *status == LSD_OK) *status = LSD_ESINGULAR;
+}
+}  // namespace
+
+// vel_matrices + cod_matrices + comp_matrices + mag_matrices (velocity.F90:56-168,
+// codensity.F90:37-79, magnetic.F90:62-133) at the dt held in device memory (*dtp): only
+// launches and memsets on the context's stream, no allocation and no host
+// synchronisation, so the one-graph step captures it (run when tim_new_tstep changes dt).
+int lsd_launch_operator_build(lsd_ctx* ctx, const double* dtp, int* status) {
   const int N = ctx->N, KL = ctx->KL, L = ctx->L;
   const lsd_config& c = ctx->cfg;
   cudaStream_t s = ctx->stream;
   OpParams P;
-  const double dt = ctx->dt;
   const double impl = c.implicit;
   auto setf = [&](int fam, double c1, double c2) {
-    P.c1_[fam] = c1 / dt;
+    P.c1[fam] = c1;
     P.c2_[fam] = (impl == 0.0) ? 1.0 : c2 * impl;
     P.c2y[fam] = c2 * (1.0 - impl);
   };
@@ -645,9 +664,7 @@ int lsd_build_operators(lsd_ctx* ctx) {
   P.Hyp = c.Hyp;
   P.vel_bc = c.vel_bc; P.cod_bc = c.cod_bc; P.comp_bc = c.comp_bc;
   P.anelastic = c.boussinesq ? 0 : 1;
-  int* d_fail = nullptr;
-  CUDA_TRY(cudaMalloc(&d_fail, sizeof(int)));
-  CUDA_TRY(cudaMemsetAsync(d_fail, 0, sizeof(int), s));
+  CUDA_TRY(cudaMemsetAsync(ctx->d_opfail, 0, sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(ctx->d_y, 0, sizeof(double) * OP_NFAM * N * (2 * KL + 1) * L, s));
   const int NL = ctx->NL, Ni = ctx->Nic;
   // one warp per operator, its band in shared memory: up to four per CTA within 200 KB
@@ -663,11 +680,11 @@ int lsd_build_operators(lsd_ctx* ctx) {
   CUDA_TRY(cudaFuncSetAttribute(k_build_ops, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 g(ceil_div(L, wpb), OP_NFAM);
   k_build_ops<<<g, 32 * wpb, smem, s>>>(N, NL, KL, L, wpb, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_laps,
-                                        ctx->d_ref, P, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_info);
+                                        ctx->d_ref, P, dtp, ctx->d_lu, ctx->d_ipiv, ctx->d_y, ctx->d_info);
   if (Ni > 1) {  // the field families coupled to the inner core
     CUDA_TRY(cudaFuncSetAttribute(k_build_icops, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemi));
     k_build_icops<<<dim3(ceil_div(L, wpbi), 2), 32 * wpbi, smemi, s>>>(
-        N, Ni, KL, L, wpbi, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_icr, ctx->d_icdr, ctx->d_icradlap, P,
+        N, Ni, KL, L, wpbi, ctx->d_r, ctx->d_dr, ctx->d_radlap, ctx->d_icr, ctx->d_icdr, ctx->d_icradlap, P, dtp,
         ctx->d_lu, ctx->d_ipiv, ctx->d_icyt, ctx->d_info);
     ctx->launches++;
   }
@@ -676,19 +693,30 @@ int lsd_build_operators(lsd_ctx* ctx) {
                                    ctx->d_ipivs, ctx->d_yt);
   CUDA_TRY(cudaMemsetAsync(ctx->d_gret, 0, sizeof(double) * 2 * N * L, s));
   {
-    int rc = lsd_launch_greens(ctx, d_fail);  // on the solve-layout factors
-    if (rc) { cudaFree(d_fail); return rc; }
+    int rc = lsd_launch_greens(ctx, ctx->d_opfail);  // on the solve-layout factors
+    if (rc) return rc;
   }
-  // the step's dt for rot_predictor / rot_corrector, read on the device
-  CUDA_TRY(cudaMemcpyAsync(ctx->d_rot + ROT_DT, &ctx->dt, sizeof(double), cudaMemcpyHostToDevice, s));
+  k_ops_finish<<<1, 256, 0, s>>>(dtp, ctx->d_rot + ROT_DT, ctx->d_info, OP_NFAM * L, ctx->d_opfail, status);
   ctx->launches += 3;
   CUDA_TRY(cudaGetLastError());
+  return LSD_OK;
+}
+
+// The operators at the host's dt (lsd_create, lsd_set_time, the host-controlled step):
+// dt to the device control block, the build, then the checks with their messages.
+int lsd_build_operators(lsd_ctx* ctx) {
+  const int L = ctx->L;
+  cudaStream_t s = ctx->stream;
+  const double dt = ctx->dt;
+  ctx->h_red[LSD_HRED_DT] = dt;
+  CUDA_TRY(cudaMemcpyAsync(&ctx->d_pc->s.dt, ctx->h_red + LSD_HRED_DT, sizeof(double), cudaMemcpyHostToDevice, s));
+  int rc = lsd_launch_operator_build(ctx, &ctx->d_pc->s.dt, nullptr);
+  if (rc) return rc;
   std::vector<int> info((size_t)OP_NFAM * L);
   int fail = 0;
   CUDA_TRY(cudaMemcpyAsync(info.data(), ctx->d_info, sizeof(int) * info.size(), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(&fail, d_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(&fail, ctx->d_opfail, sizeof(int), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
-  cudaFree(d_fail);
   for (int fam = 0; fam < OP_NFAM; ++fam)
     for (int l = 0; l < L; ++l)
       if (info[(size_t)fam * L + l] != 0)

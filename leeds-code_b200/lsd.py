@@ -91,6 +91,8 @@ def load_library(path=None):
         "lsd_synchronize": [_V],
         "lsd_last_elapsed_ms": [_V, _D],
         "lsd_kernel_launches": [_V, ctypes.POINTER(ctypes.c_longlong)],
+        "lsd_tim_check_cgce": [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState)],
+        "lsd_tim_new_tstep": [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState), _I],
     }
     for name, args in sigs.items():
         f = getattr(lib, name)
@@ -102,6 +104,21 @@ def load_library(path=None):
     lib.lsd_ensemble_last_error.argtypes = [_V]
     _LIB = lib
     return lib
+
+
+def tim_check_cgce(cfg, state):
+    """tim_check_cgce (timestep.F90:744-830) through the C ABI on a capi.LsdPcState (updated
+    in place); returns the status (LSD_OK or LSD_ENOTCONVERGED).  Host only."""
+    return load_library().lsd_tim_check_cgce(ctypes.byref(cfg), ctypes.byref(state))
+
+
+def tim_new_tstep(cfg, state):
+    """tim_new_tstep (timestep.F90:837-870) through the C ABI; returns tim_new_dt."""
+    nd = ctypes.c_int(0)
+    rc = load_library().lsd_tim_new_tstep(ctypes.byref(cfg), ctypes.byref(state), ctypes.byref(nd))
+    if rc:
+        raise LsdError(rc, "lsd_tim_new_tstep")
+    return bool(nd.value)
 
 
 def exported_symbols():

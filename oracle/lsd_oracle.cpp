@@ -2067,8 +2067,9 @@ void non_maxtstep(Oracle& o) {
   o.tim_cfl_dt = std::min(o.tim_cfl_dt, E / Pm);
   o.tim_cfl_dt = std::min(o.tim_cfl_dt, std::sqrt(E));
 }
-// tim_new_tstep (timestep.F90:837-870)
-void tim_new_tstep(Oracle& o) {
+// tim_new_tstep (timestep.F90:837-870); O: anything with the tim_* members and cfg
+template <class O>
+void tim_new_tstep(O& o) {
   double dt = o.tim_dt;
   if (o.cfg.time_step_control == 1) {
     if (o.tim_corr_dt > o.cfg.corr_upper) dt = 0.5 * dt;
@@ -2085,7 +2086,8 @@ void tim_new_tstep(Oracle& o) {
 }
 
 // tim_check_cgce (timestep.F90:744-830); returns 1 when the loop gave up.
-int check_cgce(Oracle& o) {
+template <class O>
+int check_cgce(O& o) {
   int fail = 0;
   const int i_maxtstep = 1500000;
   if (o.cfg.time_step_control == 1) {
@@ -2806,6 +2808,38 @@ int orc_step(Oracle* o, int nsteps, lsd_stats* st) {
     st->steps_done = done; st->correctors = corr; st->evaluations = evals; st->kernel_launches = 0;
     st->last_dterr = last; st->t = o->tim_t; st->dt = o->tim_dt;
   }
+  return 0;
+}
+// tim_check_cgce / tim_new_tstep on a bare loop state (lsd_pc_state), for the
+// comparison with the library's C-ABI mirrors
+struct TimOnly {
+  lsd_config cfg;
+  double tim_t, tim_dt, tim_dterr, tim_corr_dt, tim_cfl_dt, lasterr;
+  int tim_it, tim_step, tim_pcn;
+  bool tim_new_dt;
+};
+static TimOnly tim_in(const lsd_config* cfg, const lsd_pc_state* s) {
+  TimOnly o;
+  o.cfg = *cfg;
+  o.tim_t = s->t; o.tim_dt = s->dt; o.tim_dterr = s->dterr; o.tim_corr_dt = s->corr_dt; o.lasterr = s->lasterr;
+  o.tim_cfl_dt = s->cfl_dt; o.tim_it = s->it; o.tim_step = s->step; o.tim_pcn = s->pcn; o.tim_new_dt = false;
+  return o;
+}
+static void tim_out(const TimOnly& o, lsd_pc_state* s) {
+  s->t = o.tim_t; s->dt = o.tim_dt; s->dterr = o.tim_dterr; s->corr_dt = o.tim_corr_dt; s->lasterr = o.lasterr;
+  s->cfl_dt = o.tim_cfl_dt; s->it = o.tim_it; s->step = o.tim_step; s->pcn = o.tim_pcn;
+}
+int orc_tim_check_cgce(const lsd_config* cfg, lsd_pc_state* s) {
+  TimOnly o = tim_in(cfg, s);
+  const int fail = check_cgce(o);
+  tim_out(o, s);
+  return fail ? LSD_ENOTCONVERGED : 0;
+}
+int orc_tim_new_tstep(const lsd_config* cfg, lsd_pc_state* s, int* new_dt) {
+  TimOnly o = tim_in(cfg, s);
+  tim_new_tstep(o);
+  tim_out(o, s);
+  *new_dt = o.tim_new_dt ? 1 : 0;
   return 0;
 }
 int orc_energies(Oracle* o, double* out) { energies(*o, out); return 0; }

@@ -79,6 +79,8 @@ def load():
         "orc_set_dt": (ctypes.c_int, [vp, ctypes.c_double]),
         "orc_dt_control": (None, [vp, _D]),
         "orc_qst2rtp_vel": (ctypes.c_int, [vp, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+        "orc_tim_check_cgce": (ctypes.c_int, [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState)]),
+        "orc_tim_new_tstep": (ctypes.c_int, [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState), _I]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)
@@ -86,6 +88,17 @@ def load():
         f.argtypes = args
     _LIB = lib
     return lib
+
+
+def tim_check_cgce(cfg, state):
+    """The oracle's tim_check_cgce on a capi.LsdPcState (in place); returns the status."""
+    return load().orc_tim_check_cgce(ctypes.byref(cfg), ctypes.byref(state))
+
+
+def tim_new_tstep(cfg, state):
+    nd = ctypes.c_int(0)
+    load().orc_tim_new_tstep(ctypes.byref(cfg), ctypes.byref(state), ctypes.byref(nd))
+    return bool(nd.value)
 
 
 def set_threads(n):

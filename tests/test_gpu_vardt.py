@@ -127,8 +127,11 @@ def test_oracle_control1_dt_rules():
 
 @pytest.mark.gpu
 def test_variable_dt_control1():
-    """Device against the oracle step by step under i_time_step_control = 1: dt,
-    tim_corr_dt and the corrector count at every step, the state at the end."""
+    """Device against the oracle step by step under i_time_step_control = 1: the dt
+    sequence and the corrector count at every step, tim_corr_dt (the corrector norm) to
+    1e-6 (while dt is tiny the norm is close to the rounding level of the state: 2e-10 at
+    dt = 1.6e-8, where the two differ by 3e-9 of it; the decisions it drives compare it
+    with d_corr_lower = 0.002), the state at the end."""
     cfg = control1_cfg()
     g, o = pkg.Context(cfg), ol.Oracle(cfg)
     for f, (re, im) in syn.boussinesq_state(cfg, seed=23).items():
@@ -141,7 +144,7 @@ def test_variable_dt_control1():
         assert sg.correctors == so.correctors, k
         a, b = g.dt_control(), o.dt_control()
         assert a[0] == b[0] or abs(a[0] - b[0]) <= 1e-12 * b[0], (k, a, b)
-        assert abs(a[1] - b[1]) <= 1e-9 * abs(b[1]), (k, a, b)
+        assert abs(a[1] - b[1]) <= 1e-6 * abs(b[1]), (k, a, b)
     for f in range(5):
         a, b = g.get_coll(f), o.get_coll(f)
         assert relerr(a[0], b[0]) < 1e-10, f
