@@ -1,7 +1,8 @@
 """Benchmark of the B200 dynamo timestep (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision best|fp64|ozaki] [--workload dynamo128|parity32]
+                    [--precision best|fp64|ozaki]
+                    [--workload dynamo128|parity32|sht256|solve257|ensemble]
 
 Workload (default dynamo128): the full Boussinesq MHD + codensity step at lmax = mmax =
 127 (L = M = 128, Th = 192, Ph = 384), Nr = 129, E = 3e-4, Ra = 200, Pr = 1, Pm = 3,
@@ -17,11 +18,31 @@ e2e    = the same metric through the public API with host buffers: every step up
          the five state fields from pinned host memory, steps, and reads the energies back;
          the uploads are streamed (lsd_stage_coll on the copy stream while the step before
          runs, lsd_commit_staged before the step); serial_value: upload, step and read back
-         one after another (lsd_set_coll).
+         one after another (lsd_set_coll).  The advanced state stays on the device (the
+         library owns it between steps, as the reference's module storage does); the
+         read-back is the energy diagnostics' staging (d2h_bytes_per_step).
 roofline: the dominant phase of the step (CUDA-event phase timings), algorithmic
          bytes or flops per launch over its measured duration.
 cpu_baseline: the CPU oracle (C++ restatement of the reference path, OpenMP over shells
-         and harmonics) timed on this host for one timestep of the same workload.
+         and harmonics) timed on this host for one timestep of the same workload on all
+         host threads, and (single_thread) one evaluation + predictor on one thread, scaled
+         to a step by its two evaluations.
+
+Other scope configurations (one JSON line each, same keys):
+  --workload sht256    the SHT round trip at lmax = mmax = 255 (L = M = 256, Th = 384,
+         Ph = 768), 64 shells x 8 fields, device-resident synthesis + analysis
+         (lsd_sht_*_device); value = SHT TF/s (Legendre + FFT algorithmic flops) of the
+         tensor-core contraction at 7 slices, every variant (FP64, 8/7/5/4 slices) listed
+         with its time and its error against the FP64 variant per field.
+  --workload solve257  the batched banded solves at N = 257, KL = 4, L = M = 256: every
+         (l, m) right-hand side of five fields (codensity, toroidal velocity, the field's
+         toroidal / poloidal scalars, the poloidal velocity's fourth-order composite) on the
+         context's Crank-Nicolson operators in one launch (lsd_operator_solve_device);
+         value = GB/s of right-hand-side and factor bytes.
+  --workload ensemble  eight anelastic runs (L = 64, 64, 96, 96, 128, 128, 192, 192,
+         N = L + 1, N_rho = 3, composition) with the tensor-core contraction, all stepped
+         by one graph launch per call (lsd_ensemble_step); value = aggregate timesteps/s,
+         per_instance lists each member's own rate stepped alone.
 --impl reference: the same metric for the CPU oracle (the Fortran reference needs a
          Fortran compiler, FFTW, LAPACK and netCDF, none of which exists on this image).
 """
@@ -224,9 +245,11 @@ def cpu_oracle_step(cfg, threads):
 
 def run_reference(args, rank, world):
     """--impl reference: the CPU oracle on this host, rank 0 only."""
-    cfg, desc = workload(args.workload, "fp64")
     if rank != 0:
         return
+    if args.workload in ("sht256", "solve257", "ensemble"):
+        return run_reference_other(args, world)
+    cfg, desc = workload(args.workload, "fp64")
     threads = os.cpu_count() or 1
     o = cpu_oracle_step(cfg, threads)
     t0 = time.perf_counter()
@@ -250,6 +273,430 @@ def run_reference(args, rank, world):
                          "sample": "%d full timesteps of the workload after %d warm-up (timed steps capped at ~150 s)" % (k, warm)},
         "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    print(json.dumps(line), flush=True)
+
+
+def ctx_timer(handle):
+    """(stream, start(), stop() -> ms): CUDA events on a library stream (an int handle)"""
+    import torch
+    st = torch.cuda.ExternalStream(handle)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def start():
+        a.record(st)
+
+    def stop():
+        b.record(st)
+        b.synchronize()
+        return a.elapsed_time(b)
+    return st, start, stop
+
+
+def pinned_like(a):
+    import torch
+    t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    t.numpy()[...] = a
+    return t
+
+
+def sht256_cfg(capi, prec, slices, device):
+    return capi.template_config(L=256, M=256, Mp=1, N=64, timestep=1e-5, precision=prec,
+                                ozaki_slices=slices, device=device)
+
+
+SHT256_VARIANTS = [("fp64", 0), ("ozaki", 8), ("ozaki", 7), ("ozaki", 5), ("ozaki", 4)]
+SHT256_HEADLINE = ("ozaki", 7)
+
+
+def run_sht256(args, rank, world, local_rank, dist):
+    """config[1]: SHT round trips of 64 shells x 8 fields at L = M = 256"""
+    import torch
+    pkg = importlib.import_module("leeds-code_b200")
+    capi = pkg.capi
+    peaks, src = load_peaks()
+    nf = 8
+    out = {}
+    ref_phys = ref_back = None
+    for prec, S in SHT256_VARIANTS:
+        cp = capi.PREC_OZAKI if prec == "ozaki" else capi.PREC_FP64
+        ctx = pkg.Context(sht256_cfg(capi, cp, S, local_rank))
+        N, H, Ph, Th = ctx.N, ctx.H, ctx.Ph, ctx.Th
+        l, m, _ = ctx.harmonics()
+        rng = np.random.default_rng(pkg.synthetic.SEED + rank)
+        amp = np.where(l == 0, 1.0, 1.0 / np.maximum(l, 1))
+        spec = np.stack([rng.standard_normal((nf, N, H)) * amp, rng.standard_normal((nf, N, H)) * amp], axis=-1)
+        spec[:, :, m == 0, 1] = 0.0
+        st, start, stop = ctx_timer(ctx.stream())
+        with torch.cuda.stream(st):
+            d_spec = torch.tensor(spec, device="cuda:%d" % local_rank)
+            d_phys = torch.empty((nf, N, Ph, Th), device="cuda:%d" % local_rank, dtype=torch.float64)
+            d_back = torch.empty_like(d_spec)
+        st.synchronize()
+
+        def round_trip():
+            ctx.sht_synth_device(nf, d_spec.data_ptr(), d_phys.data_ptr())
+            ctx.sht_analys_device(nf, d_phys.data_ptr(), d_back.data_ptr())
+        for _ in range(args.warmup):
+            round_trip()
+        ctx.synchronize()
+        if dist:
+            dist.barrier()
+        l0 = ctx.kernel_launches()
+        start()
+        for _ in range(args.steps):
+            round_trip()
+        ms = stop() / args.steps
+        launches = (ctx.kernel_launches() - l0) // args.steps
+        if dist:
+            ms = max_over_ranks(dist, ms, "cuda:%d" % local_rank)
+        # errors: per field against the FP64 variant's synthesis and round trip, and the
+        # round trip against the input
+        with torch.cuda.stream(st):
+            if prec == "fp64":
+                ref_phys, ref_back = d_phys.clone(), d_back.clone()
+                e_syn = e_rt = [0.0] * nf
+            else:
+                e_syn = [float((d_phys[f] - ref_phys[f]).abs().max() / ref_phys[f].abs().max()) for f in range(nf)]
+                e_rt = [float((d_back[f] - ref_back[f]).abs().max() / ref_back[f].abs().max()) for f in range(nf)]
+            e_in = [float((d_back[f] - d_spec[f]).abs().max() / d_spec[f].abs().max()) for f in range(nf)]
+        # end to end with host buffers: pinned spectra up, round trip, spectra back
+        h_spec, h_back = pinned_like(spec), pinned_like(np.zeros_like(spec))
+        ne = max(1, min(args.steps, 5))
+        start()
+        with torch.cuda.stream(st):
+            for _ in range(ne):
+                d_spec.copy_(h_spec, non_blocking=True)
+                round_trip()
+                h_back.copy_(d_back, non_blocking=True)
+        e2e_ms = stop() / ne
+        if dist:
+            e2e_ms = max_over_ranks(dist, e2e_ms, "cuda:%d" % local_rank)
+        out[(prec, S)] = {"ms": ms, "e2e_ms": e2e_ms, "launches": launches, "err_synth_vs_fp64": max(e_syn),
+                          "err_round_trip_vs_fp64": max(e_rt), "err_round_trip_vs_input": max(e_in),
+                          "sizes": ctx.sizes}
+        del d_spec, d_phys, d_back
+        ctx.close()
+    if rank != 0:
+        return
+    sz = out[SHT256_HEADLINE]["sizes"]
+    H, Th2, Th, Ph, N = sz["H"], sz["Th2"], sz["Th"], sz["Ph"], 64
+    leg = 8 * H * Th2 * N * nf  # synthesis + analysis, 4 flops per complex x real MAC each
+    fft = 2 * Th * N * nf * 2.5 * Ph * np.log2(Ph)
+    bytes_rt = 2 * nf * N * H * 16 + 2 * nf * N * Th * Ph * 8
+    h = out[SHT256_HEADLINE]
+    tflops = world * (leg + fft) / (h["ms"] * 1e-3) / 1e12
+    ach = bytes_rt / (h["ms"] * 1e-3) / 1e9
+    line = {
+        "metric": "SHT TF/s lmax255 round trip, 64 shells x 8 fields", "value": tflops, "unit": "TF/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": h["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded N(0,1) l^-1 coefficients)",
+        "config": {"workload": "SHT round trip lmax=mmax=255 (L=M=256), Th=384, Ph=768, 64 shells x 8 fields",
+                   "precision": "ozaki", "ozaki_slices": SHT256_HEADLINE[1],
+                   "l2": "per-trip working set ~3 GB >> 126 MB L2 (no flush)"},
+        "e2e": {"value": world * (leg + fft) / (h["e2e_ms"] * 1e-3) / 1e12, "unit": "TF/s",
+                "h2d_bytes_per_step": nf * N * H * 16, "d2h_bytes_per_step": nf * N * H * 16},
+        "gpu_launches": h["launches"],
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": ach / peaks["hbm_gbs"], "traffic": None},
+        "roofline_note": "whole round trip: algorithmic bytes (spectra in/out, the physical grid written "
+                         "and read) over its device time; peak %s" % src,
+        "variants": {("%s_S%d" % k if k[0] == "ozaki" else "fp64"): {
+            "ms": v["ms"], "tflops": world * (leg + fft) / (v["ms"] * 1e-3) / 1e12,
+            "err_synth_vs_fp64": v["err_synth_vs_fp64"], "err_round_trip_vs_fp64": v["err_round_trip_vs_fp64"],
+            "err_round_trip_vs_input": v["err_round_trip_vs_input"]} for k, v in out.items()},
+    }
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_sht256(sz, leg + fft, nf)
+    print(json.dumps(line), flush=True)
+
+
+def cpu_sht256(sz, flops_all, nf):
+    """the oracle's synthesis + analysis of one of the nf fields (64 shells), all threads"""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    pkg = importlib.import_module("leeds-code_b200")
+    threads = os.cpu_count() or 1
+    ol.set_threads(threads)
+    o = ol.Oracle(pkg.capi.template_config(L=256, M=256, Mp=1, N=64, timestep=1e-5))
+    l, m, _ = o.harmonics()
+    rng = np.random.default_rng(1)
+    re = rng.standard_normal((o.N, o.H)) / np.maximum(l, 1)
+    im = rng.standard_normal((o.N, o.H)) / np.maximum(l, 1)
+    t0 = time.perf_counter()
+    p = o.spec2phys(re, im)
+    o.phys2spec(p)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": flops_all / nf / dt / 1e12, "unit": "TF/s", "cores": threads, "kind": "port",
+            "sample": "oracle synthesis + analysis of 1 of the 8 fields (64 shells), %.1f s" % dt}
+
+
+def solve257_bytes(sz, nf):
+    N, H, L, KL = sz["N"], sz["H"], sz["L"], sz["KL"]
+    rhs = 2 * nf * N * H * 16
+    factors = (nf + 1) * L * N * ((3 * KL + 1) * 8 + 4)  # + the Green's operator of the composite
+    return rhs + factors
+
+
+def run_solve257(args, rank, world, local_rank, dist):
+    """config[2]: every (l, m) right-hand side of five fields on the CN operators, one launch"""
+    import torch
+    pkg = importlib.import_module("leeds-code_b200")
+    capi, syn = pkg.capi, pkg.synthetic
+    peaks, src = load_peaks()
+    fields = (capi.COD_C, capi.VEL_TOR, capi.MAG_TOR, capi.MAG_POL, capi.VEL_POL)
+    cfg = syn.config_solve257(device=local_rank)
+    ctx = pkg.Context(cfg)
+    N, H = ctx.N, ctx.H
+    l, m, _ = ctx.harmonics()
+    re, im = syn.seeded_rhs(len(fields), N, H, m, seed=syn.SEED + rank)
+    rhs = np.stack([re, im], axis=-1)
+    st, start, stop = ctx_timer(ctx.stream())
+    dev = "cuda:%d" % local_rank
+    with torch.cuda.stream(st):
+        d_save = torch.tensor(rhs, device=dev)
+        d = d_save.clone()
+    st.synchronize()
+
+    def solve():
+        ctx.operator_solve_device(fields, d.data_ptr())
+    for _ in range(args.warmup):
+        with torch.cuda.stream(st):
+            d.copy_(d_save)
+        solve()
+    ctx.synchronize()
+    if dist:
+        dist.barrier()
+    tot = 0.0
+    l0 = ctx.kernel_launches()
+    for _ in range(args.steps):
+        with torch.cuda.stream(st):
+            d.copy_(d_save)  # fresh right-hand sides, outside the timed launch
+        start()
+        solve()
+        tot += stop()
+    ms = tot / args.steps
+    launches = (ctx.kernel_launches() - l0) // args.steps
+    if dist:
+        ms = max_over_ranks(dist, ms, dev)
+    h_rhs, h_out = pinned_like(rhs), pinned_like(np.zeros_like(rhs))
+    ne = max(1, min(args.steps, 5))
+    start()
+    with torch.cuda.stream(st):
+        for _ in range(ne):
+            d.copy_(h_rhs, non_blocking=True)
+            solve()
+            h_out.copy_(d, non_blocking=True)
+    e2e_ms = stop() / ne
+    if dist:
+        e2e_ms = max_over_ranks(dist, e2e_ms, dev)
+    sz = ctx.sizes
+    ctx.close()
+    if rank != 0:
+        return
+    nb = solve257_bytes(sz, len(fields))
+    gbs = world * nb / (ms * 1e-3) / 1e9
+    line = {
+        "metric": "batched banded solve GB/s Nr257 KL4, all (l,m) of 5 fields", "value": gbs, "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded complex N(0,1) right-hand sides)",
+        "config": {"workload": "CN operator solves N=257, KL=4, L=M=256 (H=32896), dt=2e-6, E=3e-4, Pm=3: "
+                               "codensity, toroidal velocity, field tor/pol, poloidal velocity composite",
+                   "l2": "right-hand sides 0.68 GB >> 126 MB L2 (no flush)"},
+        "e2e": {"value": world * nb / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
+                "h2d_bytes_per_step": rhs.nbytes, "d2h_bytes_per_step": rhs.nbytes},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": gbs / world, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": gbs / world / peaks["hbm_gbs"], "traffic": None},
+        "rhs_columns_per_s": world * 2 * len(fields) * H / (ms * 1e-3),
+    }
+    if world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as ol
+        threads = os.cpu_count() or 1
+        ol.set_threads(threads)
+        o = ol.Oracle(pkg.synthetic.config_solve257())
+        t0 = time.perf_counter()
+        for k, f in enumerate(fields):
+            o.operator_solve(f, re[k].T, im[k].T)
+        dt = time.perf_counter() - t0
+        o.close()
+        line["cpu_baseline"] = {"value": nb / dt / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+                                "sample": "the oracle's tim_invX / composite of the same five fields, %.1f s" % dt}
+    print(json.dumps(line), flush=True)
+
+
+def run_ensemble(args, rank, world, local_rank, dist):
+    """config[4]: eight anelastic runs stepped by one graph launch per call"""
+    import torch
+    pkg = importlib.import_module("leeds-code_b200")
+    capi, syn = pkg.capi, pkg.synthetic
+    peaks, src = load_peaks()
+    prec = capi.PREC_FP64 if args.precision == "fp64" else capi.PREC_OZAKI
+    cfgs = syn.config_ensemble(precision=prec, ozaki_slices=args.slices if prec == capi.PREC_OZAKI else 0)
+    for c in cfgs:
+        c.device = local_rank
+    ens = pkg.Ensemble(cfgs)
+    states = [syn.setup_ensemble_member(mb, c, seed=syn.SEED + 97 * rank + i)
+              for i, (mb, c) in enumerate(zip(ens.members, cfgs))]
+    ens.step(args.warmup)
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    l0 = sum(mb.kernel_launches() for mb in ens.members)
+    stats = ens.step(args.steps)
+    ms = ens.last_elapsed_ms()
+    launches = sum(mb.kernel_launches() for mb in ens.members) - l0
+    clocks = sampler.stop() if sampler else None
+    if dist:
+        ms = max_over_ranks(dist, ms, "cuda:%d" % local_rank)
+    agg = world * len(cfgs) * args.steps / (ms * 1e-3)
+    # end to end: every step uploads every member's state from pinned memory, steps the
+    # ensemble, and reads every member's energies back
+    pinned = [{f: (pinned_like(re).numpy(), pinned_like(im).numpy()) for f, (re, im) in stt.items()} for stt in states]
+    ne = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        for mb, pst in zip(ens.members, pinned):
+            mb.load_fields(pst)
+        ens.step(1)
+        for mb in ens.members:
+            mb.energies()
+    e2e_s = (time.perf_counter() - t0) / ne
+    if dist:
+        e2e_s = max_over_ranks(dist, e2e_s, "cuda:%d" % local_rank)
+    h2d = sum(sum(re.nbytes + im.nbytes for re, im in stt.values()) for stt in states)
+    ens.close()
+    # each member alone (its own lsd_step graph), for the per-instance rates
+    per = []
+    for i, c in enumerate(cfgs):
+        if i % 2:
+            per.append(per[-1])  # the twin member of the same resolution
+            continue
+        ctx = pkg.Context(c)
+        syn.setup_ensemble_member(ctx, c, seed=syn.SEED + i)
+        ctx.step(args.warmup)
+        s1 = ctx.step(args.steps)
+        per.append({"L": c.L, "N": c.N, "timesteps_per_s_alone": s1.steps_done / (ctx.last_elapsed_ms() * 1e-3)})
+        if c.L == max(syn.ENSEMBLE_L):
+            ph, rf = phase_roofline_anelastic(ctx, peaks, src)
+        ctx.close()
+    if rank != 0:
+        return
+    alone_ms = sum(1e3 * args.steps / p["timesteps_per_s_alone"] for p in per)
+    line = {
+        "metric": "aggregate timesteps/s, 8-member anelastic ensemble (lmax 63..191)", "value": agg,
+        "unit": "timesteps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (n=2 polytrope N_rho=3, seeded l^-2 perturbations)",
+        "config": {"workload": "8 anelastic runs L=M in {64,64,96,96,128,128,192,192}, N=L+1, "
+                               "codensity + composition, dt=1e-6, one graph launch per call",
+                   "precision": "ozaki" if prec == capi.PREC_OZAKI else "fp64",
+                   "ozaki_slices": args.slices if prec == capi.PREC_OZAKI else None,
+                   "l2": "per-step working set several GB >> 126 MB L2 (no flush)"},
+        "e2e": {"value": world * len(cfgs) / e2e_s, "unit": "timesteps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": len(cfgs) * 8 * 64},
+        "gpu_launches": launches,
+        "per_instance": per,
+        "ensemble_vs_members_alone": alone_ms / ms,
+        "roofline": {k: rf[k] for k in ("bound", "achieved", "peak", "unit", "frac")},
+        "roofline_detail": rf,
+        "correctors": [s.correctors for s in stats],
+    }
+    line["roofline"]["traffic"] = None
+    if clocks:
+        line["clocks"] = clocks
+    if world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as ol
+        threads = os.cpu_count() or 1
+        ol.set_threads(threads)
+        c = syn.config_anelastic(L=64)
+        o = ol.Oracle(c)
+        o.set_reference_state(syn.polytrope_reference_state(c.N, c.rratio))
+        for f, (re, im) in syn.boussinesq_state(c, seed=syn.SEED, composition=True).items():
+            o.set_coll(f, re, im)
+        t0 = time.perf_counter()
+        o.step(1)
+        dt = time.perf_counter() - t0
+        o.close()
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "timesteps/s", "cores": threads, "kind": "port",
+                                "sample": "1 timestep of the L=64 member (the smallest), %.1f s" % dt}
+    print(json.dumps(line), flush=True)
+
+
+def phase_roofline_anelastic(ctx, peaks, src):
+    """the dominant phase of one step of an anelastic member (products: two launches of the
+    momentum and scalar sets, 12 + 6 and 17 + 2 fields)"""
+    ph = ctx.profile_phases()
+    sz = ctx.sizes
+    FF = sz["N"] * 2 * sz["Hc"] * sz["Th"] * 16
+    b = (12 + 6 + 17 + 2) * FF
+    ms = ph["fft_products"]
+    ach = b / (ms * 1e-3) / 1e9
+    return ph, {"kernel": "fft_products (L=%d member)" % sz["L"], "bound": "hbm", "unit": "GB/s",
+                "peak": peaks["hbm_gbs"], "achieved": ach, "frac": ach / peaks["hbm_gbs"], "ms_per_launch": ms,
+                "bytes_per_launch": b, "peak_source": src, "phases_ms": ph}
+
+
+def run_reference_other(args, world):
+    """--impl reference for the other scope configurations: the oracle on the same
+    workload (bounded samples, all host threads), on the lines' own metrics."""
+    pkg = importlib.import_module("leeds-code_b200")
+    syn = pkg.synthetic
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    ol.set_threads(threads)
+    if args.workload == "sht256":
+        o = ol.Oracle(pkg.capi.template_config(L=256, M=256, Mp=1, N=64, timestep=1e-5))
+        sz = o.sz
+        leg = 8 * sz["H"] * sz["Th2"] * 64
+        fft = 2 * sz["Th"] * 64 * 2.5 * sz["Ph"] * np.log2(sz["Ph"])
+        o.close()
+        cb = cpu_sht256(sz, 8 * (leg + fft), 8)
+        metric, unit, desc = "SHT TF/s lmax255 round trip, 64 shells x 8 fields", "TF/s", \
+            "SHT round trip lmax=mmax=255 (L=M=256), Th=384, Ph=768, 64 shells x 8 fields"
+        v, sample = cb["value"], cb["sample"]
+    elif args.workload == "solve257":
+        cfg = syn.config_solve257()
+        o = ol.Oracle(cfg)
+        l, m, _ = o.harmonics()
+        fields = (pkg.capi.COD_C, pkg.capi.VEL_TOR, pkg.capi.MAG_TOR, pkg.capi.MAG_POL, pkg.capi.VEL_POL)
+        re, im = syn.seeded_rhs(len(fields), o.N, o.H, m)
+        sz = dict(o.sz)
+        t0 = time.perf_counter()
+        for k, f in enumerate(fields):
+            o.operator_solve(f, re[k].T, im[k].T)
+        dt = time.perf_counter() - t0
+        o.close()
+        v = solve257_bytes(sz, len(fields)) / dt / 1e9
+        metric, unit = "batched banded solve GB/s Nr257 KL4, all (l,m) of 5 fields", "GB/s"
+        desc = "CN operator solves N=257, KL=4, L=M=256 (H=32896): 5 fields, every (l,m)"
+        sample = "the oracle's tim_invX / composite of the five fields, %.1f s" % dt
+    else:
+        c = syn.config_anelastic(L=64)
+        o = ol.Oracle(c)
+        o.set_reference_state(syn.polytrope_reference_state(c.N, c.rratio))
+        for f, (re, im) in syn.boussinesq_state(c, seed=syn.SEED, composition=True).items():
+            o.set_coll(f, re, im)
+        t0 = time.perf_counter()
+        o.step(1)
+        dt = time.perf_counter() - t0
+        o.close()
+        v = 1.0 / dt
+        metric, unit = "aggregate timesteps/s, 8-member anelastic ensemble (lmax 63..191)", "timesteps/s"
+        desc = "8 anelastic runs L=M in {64,64,96,96,128,128,192,192}, N=L+1 (oracle: the L=64 member)"
+        sample = "1 timestep of the L=64 member (the smallest; the others are larger), %.1f s" % dt
+    line = {"impl": "reference", "metric": metric, "value": v, "unit": unit, "n_gpus": world, "steps": 1,
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": desc, "parallelism": "cpu-openmp"},
+            "cpu_baseline": {"value": v, "unit": unit, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -398,8 +845,23 @@ def run_ours(args, rank, world, local_rank, dist):
         t0 = time.perf_counter()
         o.step(1)
         dt = time.perf_counter() - t0
+        o.close()
         line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "timesteps/s", "cores": threads, "kind": "port",
                                 "sample": "1 full timestep of the same workload (cold buffers)"}
+        if args.workload == "dynamo128":
+            # one thread: one evaluation + the predictor (half of a step's two evaluations)
+            o = cpu_oracle_step(cfg, 1)
+            t0 = time.perf_counter()
+            o.nonlinear()
+            o.predictor()
+            dt1 = time.perf_counter() - t0
+            o.close()
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            import oracle_lib as ol
+            ol.set_threads(threads)
+            line["cpu_baseline"]["single_thread"] = {
+                "value": 1.0 / (2.0 * dt1), "unit": "timesteps/s", "cores": 1,
+                "sample": "1 evaluation + predictor on 1 thread (%.1f s), x2 for the step's two evaluations" % dt1}
     print(json.dumps(line), flush=True)
 
 
@@ -410,7 +872,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="best", choices=["best", "fp64", "ozaki"])
-    ap.add_argument("--workload", default="dynamo128", choices=["dynamo128", "parity32"])
+    ap.add_argument("--workload", default="dynamo128",
+                    choices=["dynamo128", "parity32", "sht256", "solve257", "ensemble"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     # 5 slices: the fewest whose 1000-step energy error (energy_check, reported on every run)
     # stays well inside the metric's 1e-9 (measured 6.0e-12; 6 slices: 6.1e-13, 4: above)
@@ -435,7 +898,8 @@ def main():
         torch.cuda.set_device(local_rank)
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
-    run_ours(args, rank, world, local_rank, dist)
+    legs = {"sht256": run_sht256, "solve257": run_solve257, "ensemble": run_ensemble}
+    legs.get(args.workload, run_ours)(args, rank, world, local_rank, dist)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

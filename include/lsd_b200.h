@@ -332,9 +332,12 @@ int lsd_diagnostics(lsd_ctx* ctx, double* scalars, double* spectra, double* prof
  * resolution sweep) is n of them.  lsd_ensemble_create creates one context per config on
  * one device (all cfgs[i].device equal); members are set up, read and diagnosed through
  * the context API (lsd_ensemble_member); lsd_ensemble_step advances every member by
- * nsteps completed steps of main.F90:100-164, the members' graphs running concurrently
- * on their own streams.  stats: n entries, or NULL.  On an error lsd_ensemble_last_error
- * names the member and its message. */
+ * nsteps completed steps of main.F90:100-164 as ONE launch of one CUDA graph, in which
+ * every member's device-side step loop (lsd_step's graph) is an independent branch, so
+ * the members' kernels run concurrently.  stats: n entries, or NULL.  On an error
+ * lsd_ensemble_last_error names the member and its message.
+ * lsd_ensemble_last_elapsed_ms: device time (CUDA events on the ensemble's stream) of the
+ * last lsd_ensemble_step's graph launch. */
 typedef struct lsd_ensemble lsd_ensemble;
 int lsd_ensemble_create(int n, const lsd_config* cfgs, lsd_ensemble** out);
 int lsd_ensemble_destroy(lsd_ensemble* ens);
@@ -342,6 +345,7 @@ int lsd_ensemble_size(const lsd_ensemble* ens);
 int lsd_ensemble_member(lsd_ensemble* ens, int i, lsd_ctx** ctx);
 int lsd_ensemble_step(lsd_ensemble* ens, int nsteps, lsd_stats* stats);
 const char* lsd_ensemble_last_error(const lsd_ensemble* ens);
+int lsd_ensemble_last_elapsed_ms(const lsd_ensemble* ens, double* ms);
 
 /* ---- batched banded radial solves (timestep.F90:566-588 over every (l,m)) -----------
  * Factorise nmat banded operators A_k (LAPACK band storage with ldab = 3*kl+1, columns
@@ -354,8 +358,23 @@ int lsd_banded_factor_device(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab
                              int* d_ipiv, int* d_info);
 int lsd_banded_solve_device(lsd_ctx* ctx, int n, int kl, int nmat, const double* d_ab,
                             const int* d_ipiv, int nrhs, const int* d_map, double* d_b);
+/* The context's own factorised Crank-Nicolson operators (built by lsd_create /
+ * lsd_set_time at the current dt) applied to caller right-hand sides: for each of the
+ * nfield (1..8) fields, X_l x = b for every (l, m) column with tim_zerobc first
+ * (tim_invX, timestep.F90:566-588): LSD_COD_C / LSD_COMP_C with tim_lumesh_X (every l),
+ * LSD_VEL_TOR with tim_lumesh_flayer_X / _vel_X, LSD_MAG_TOR / LSD_MAG_POL with
+ * tim_iclumesh_*_X (Nic = 1; l = 0 not solved, as tim_invX skips it), and LSD_VEL_POL
+ * with the reference's fourth-order composite (velocity.F90:369-395, 445-465 without
+ * the Y multiply: XGre, XPol, then vel_gre_adjust).  d_data: nfield consecutive device
+ * fields in the context's layout, [N][H] complex (re, im interleaved), solved in place;
+ * one launch for all fields, on the context's stream (not synchronised). */
+int lsd_operator_solve_device(lsd_ctx* ctx, int nfield, const int* fields, double* d_data);
 
 /* ---- synchronisation and timing ------------------------------------------------------ */
+/* The context's CUDA stream (a cudaStream_t), on which every asynchronous entry point
+ * queues its work: for callers that order their own device work (or CUDA events) with
+ * the library's.  No counterpart in the reference (single-threaded CPU code). */
+int lsd_get_stream(const lsd_ctx* ctx, void** stream);
 /* Phase timings (CUDA events on the context stream) of one predictor pass and one
  * corrector solve from the current state; the state advances by that step.  ms[]:
  * 0 spectral q,s,t and curls, 1 Legendre synthesis, 2 phi-FFT + products + FFT,

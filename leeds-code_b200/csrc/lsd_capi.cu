@@ -306,8 +306,10 @@ int cap_body(lsd_ctx* ctx, int k, cudaGraph_t body, F fn) {
   return LSD_OK;
 }
 
-// The whole of lsd_step as one graph (structure in include/lsd_b200.h at lsd_step).
-int capture_step(lsd_ctx* ctx) {
+// The whole of lsd_step (structure in include/lsd_b200.h at lsd_step), captured on
+// ctx->stream, which must be capturing already (into this context's graph, or into the
+// graph of an ensemble); sets the kernel counts of the sections.
+int capture_step_into(lsd_ctx* ctx) {
   for (cudaStream_t& cs : ctx->cap_stream)
     if (!cs) CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   const PcParams prm = pc_params(ctx->cfg);
@@ -317,7 +319,6 @@ int capture_step(lsd_ctx* ctx) {
   cudaStream_t s0 = ctx->stream;
   const long long l0 = ctx->launches;
   long long loop = 0, rebuild = 0, corr = 0;
-  CUDA_TRY(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed));
   int rc = LSD_OK;
   cudaGraphConditionalHandle h_steps = 0;
   cudaGraph_t b_steps = nullptr;
@@ -373,21 +374,33 @@ int capture_step(lsd_ctx* ctx) {
     loop = ctx->launches - a - corr - rebuild;
     return r;
   });
-  cudaGraph_t g = nullptr;
-  cudaError_t e = cudaStreamEndCapture(s0, &g);
   ctx->launches = l0;
-  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&ctx->g_step, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("step graph: ") + cudaGetErrorString(e));
+  if (rc) return rc;
   ctx->k_begin = 1;
   ctx->k_loop = loop;
   ctx->k_rebuild = rebuild;
   ctx->k_corr = corr;
   return LSD_OK;
+}
+
+int instantiate(lsd_ctx* ctx, cudaGraph_t g, cudaGraphExec_t* out) {
+  cudaError_t e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("step graph: ") + cudaGetErrorString(e));
+  return LSD_OK;
+}
+
+// lsd_step's graph of one context
+int capture_step(lsd_ctx* ctx) {
+  CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+  int rc = capture_step_into(ctx);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  return instantiate(ctx, g, &ctx->g_step);
 }
 
 // A step begun by lsd_predictor / lsd_corrector calls (tim_it != 0): its remaining
@@ -409,13 +422,8 @@ int finish_open_step(lsd_ctx* ctx, int* corr, int* evals, double* last) {
   return LSD_OK;
 }
 
-// Queue one launch of the step graph for nsteps steps: the loop state goes up with it and
-// comes back into the pinned mirror (read by step_graph_finish after the stream is done).
-int step_graph_enqueue(lsd_ctx* ctx, int nsteps) {
-  if (!ctx->g_step) {
-    int rc = capture_step(ctx);
-    if (rc) return rc;
-  }
+// The loop state of a call of nsteps steps into the control block (on stream s)
+int pc_upload(lsd_ctx* ctx, int nsteps, cudaStream_t s) {
   PcDev* h = ctx->h_pc;
   std::memset(h, 0, sizeof(PcDev));
   h->s = pc_get(ctx);
@@ -423,10 +431,25 @@ int step_graph_enqueue(lsd_ctx* ctx, int nsteps) {
   h->steps_left = nsteps;
   h->nsteps = nsteps;
   h->status = LSD_OK;
-  CUDA_TRY(cudaMemcpyAsync(ctx->d_pc, h, sizeof(PcDev), cudaMemcpyHostToDevice, ctx->stream));
-  CUDA_TRY(cudaGraphLaunch(ctx->g_step, ctx->stream));
-  CUDA_TRY(cudaMemcpyAsync(h, ctx->d_pc, sizeof(PcDev), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_pc, h, sizeof(PcDev), cudaMemcpyHostToDevice, s));
   return LSD_OK;
+}
+int pc_download(lsd_ctx* ctx, cudaStream_t s) {
+  CUDA_TRY(cudaMemcpyAsync(ctx->h_pc, ctx->d_pc, sizeof(PcDev), cudaMemcpyDeviceToHost, s));
+  return LSD_OK;
+}
+
+// Queue one launch of the step graph for nsteps steps: the loop state goes up with it and
+// comes back into the pinned mirror (read by step_graph_finish after the stream is done).
+int step_graph_enqueue(lsd_ctx* ctx, int nsteps) {
+  if (!ctx->g_step) {
+    int rc = capture_step(ctx);
+    if (rc) return rc;
+  }
+  int rc = pc_upload(ctx, nsteps, ctx->stream);
+  if (rc) return rc;
+  CUDA_TRY(cudaGraphLaunch(ctx->g_step, ctx->stream));
+  return pc_download(ctx, ctx->stream);
 }
 
 // after the stream passed the graph: the loop state back into the context, the counts of
@@ -1248,13 +1271,69 @@ int lsd_step(lsd_ctx* ctx, int nsteps, lsd_stats* stats) {
 }
 
 // ---- ensembles: independent runs stepped together ---------------------------------------
-// Every member's step graph (all nsteps of its loop, no host decision inside) is launched
-// on the member's own stream before the host waits for any of them, so the members'
-// kernels share the device for the whole call.
+// One graph holds every member's step loop (the one-graph step of lsd_step, all nsteps,
+// no host decision inside) as a branch of its own, forked from and joined to the
+// ensemble's stream: lsd_ensemble_step is one graph launch for all members, whose kernels
+// run concurrently as the graph's independent branches.
 struct lsd_ensemble {
   std::vector<lsd_ctx*> m;
   std::string err;
+  cudaStream_t stream = nullptr;          // the stream the ensemble's graph runs on
+  cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> join;          // one per member
+  cudaGraphExec_t g = nullptr;
+  float last_ms = 0.f;
 };
+
+namespace {
+void ensemble_free(lsd_ensemble* e) {
+  if (!e) return;
+  if (!e->m.empty()) cudaSetDevice(e->m[0]->dev);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->g) cudaGraphExecDestroy(e->g);
+  for (cudaEvent_t ev : e->join)
+    if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : {e->fork, e->ev0, e->ev1})
+    if (ev) cudaEventDestroy(ev);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  for (lsd_ctx* c : e->m) lsd_destroy(c);
+  delete e;
+}
+
+// the ensemble's graph: fork to every member's stream, each member's step loop, join
+int ensemble_capture(lsd_ensemble* e) {
+  const int n = (int)e->m.size();
+  if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    e->err = "ensemble graph: begin capture";
+    return LSD_ECUDA;
+  }
+  int rc = LSD_OK;
+  cudaError_t ce = cudaEventRecord(e->fork, e->stream);
+  for (int i = 0; i < n && !rc && ce == cudaSuccess; ++i) {
+    lsd_ctx* c = e->m[i];
+    ce = cudaStreamWaitEvent(c->stream, e->fork, 0);
+    if (ce == cudaSuccess) rc = capture_step_into(c);
+    if (rc) { e->err = "member " + std::to_string(i) + ": " + c->err; break; }
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->join[i], c->stream);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, e->join[i], 0);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t ee = cudaStreamEndCapture(e->stream, &g);
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (ce != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    e->err = std::string("ensemble graph capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee);
+    return LSD_ECUDA;
+  }
+  cudaError_t ie = cudaGraphInstantiate(&e->g, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    e->err = std::string("ensemble graph instantiate: ") + cudaGetErrorString(ie);
+    return LSD_ECUDA;
+  }
+  return LSD_OK;
+}
+}  // namespace
 
 int lsd_ensemble_create(int n, const lsd_config* cfgs, lsd_ensemble** out) {
   if (!cfgs || !out || n < 1) return LSD_EARG;
@@ -1277,14 +1356,22 @@ int lsd_ensemble_create(int n, const lsd_config* cfgs, lsd_ensemble** out) {
     }
     e->m.push_back(c);
   }
+  cudaSetDevice(e->m[0]->dev);
+  bool ok = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaEventCreate(&e->ev0) == cudaSuccess && cudaEventCreate(&e->ev1) == cudaSuccess;
+  e->join.assign(n, nullptr);
+  for (int i = 0; i < n && ok; ++i) ok = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    ensemble_free(e);
+    return LSD_ECUDA;
+  }
   *out = e;
   return LSD_OK;
 }
 
 int lsd_ensemble_destroy(lsd_ensemble* e) {
-  if (!e) return LSD_OK;
-  for (lsd_ctx* c : e->m) lsd_destroy(c);
-  delete e;
+  ensemble_free(e);
   return LSD_OK;
 }
 
@@ -1309,27 +1396,59 @@ int lsd_ensemble_step(lsd_ensemble* e, int nsteps, lsd_stats* stats) {
   std::vector<int> done(n, 0), corr(n, 0), evals(n, 0);
   std::vector<long long> l0(n), kernels(n, 0);
   std::vector<double> last(n, 0.0);
-  for (int i = 0; i < n; ++i) {
+  bool any = false;
+  for (int i = 0; i < n; ++i) {  // steps begun by single predictor / corrector calls
     lsd_ctx* c = e->m[i];
     l0[i] = c->launches;
-    int rc = time_begin(c);
-    if (!rc && c->it != 0 && nsteps > 0) {  // a step begun by single predictor / corrector calls
-      rc = finish_open_step(c, &corr[i], &evals[i], &last[i]);
-      if (!rc) { ++done[i]; kernels[i] += c->launches - l0[i]; }
+    if (c->it != 0 && nsteps > 0) {
+      int rc = finish_open_step(c, &corr[i], &evals[i], &last[i]);
+      if (rc) return fail(i, rc);
+      ++done[i];
+      kernels[i] += c->launches - l0[i];
     }
-    if (!rc && done[i] < nsteps) rc = step_graph_enqueue(c, nsteps - done[i]);
-    if (rc) return fail(i, rc);
+    any = any || done[i] < nsteps;
+  }
+  if (any) {
+    if (!e->g) {
+      int rc = ensemble_capture(e);
+      if (rc) return rc;
+    }
+    // the members' queued work first (their own streams), then the graph on the ensemble's
+    cudaError_t ce = cudaSuccess;
+    for (int i = 0; i < n && ce == cudaSuccess; ++i) {
+      ce = cudaEventRecord(e->join[i], e->m[i]->stream);
+      if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, e->join[i], 0);
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev0, e->stream);
+    for (int i = 0; i < n; ++i) {
+      int rc = pc_upload(e->m[i], nsteps - done[i], e->stream);
+      if (rc) return fail(i, rc);
+    }
+    if (ce == cudaSuccess) ce = cudaGraphLaunch(e->g, e->stream);
+    for (int i = 0; i < n; ++i) {
+      int rc = pc_download(e->m[i], e->stream);
+      if (rc) return fail(i, rc);
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev1, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1);
+    if (ce != cudaSuccess) {
+      e->err = std::string("ensemble graph launch: ") + cudaGetErrorString(ce);
+      return LSD_ECUDA;
+    }
   }
   for (int i = 0; i < n; ++i) {
     lsd_ctx* c = e->m[i];
-    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(i, lsd_fail(c, LSD_ECUDA, "stream"));
     if (done[i] < nsteps) {
       int rc = step_graph_finish(c, &done[i], &corr[i], &evals[i], &last[i], &kernels[i]);
       c->launches = l0[i] + kernels[i];
       if (rc) return fail(i, rc);
     }
-    int rc = time_end(c);
-    if (rc) return fail(i, rc);
+    if (c->oz) {
+      int rc = lsd_ozaki_check(c);
+      if (rc) return fail(i, rc);
+    }
+    c->last_ms = e->last_ms;
     c->have_eval = false;
     if (stats) {
       stats[i].steps_done = done[i]; stats[i].correctors = corr[i]; stats[i].evaluations = evals[i];
@@ -1337,6 +1456,18 @@ int lsd_ensemble_step(lsd_ensemble* e, int nsteps, lsd_stats* stats) {
       stats[i].t = c->t; stats[i].dt = c->dt;
     }
   }
+  return LSD_OK;
+}
+
+int lsd_ensemble_last_elapsed_ms(const lsd_ensemble* e, double* ms) {
+  if (!e || !ms) return LSD_EARG;
+  *ms = e->last_ms;
+  return LSD_OK;
+}
+
+int lsd_get_stream(const lsd_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return LSD_EARG;
+  *stream = (void*)ctx->stream;
   return LSD_OK;
 }
 
@@ -1387,6 +1518,12 @@ int lsd_banded_solve_device(lsd_ctx* ctx, int n, int kl, int nmat, const double*
   if (!ctx || n < 1 || kl < 1 || kl > LSD_MAX_KL || nmat < 1 || nrhs < 1 || !d_ab || !d_ipiv || !d_map || !d_b) return LSD_EARG;
   CUDA_TRY(cudaSetDevice(ctx->dev));
   return lsd_solve_batch(ctx, n, kl, nmat, d_ab, d_ipiv, nrhs, d_map, d_b);
+}
+
+int lsd_operator_solve_device(lsd_ctx* ctx, int nfield, const int* fields, double* d_data) {
+  if (!ctx || !fields || !d_data) return LSD_EARG;
+  CUDA_TRY(cudaSetDevice(ctx->dev));
+  return lsd_operator_solve(ctx, nfield, fields, d_data);
 }
 
 int lsd_profile_phases(lsd_ctx* ctx, double* ms, int* nphase) {

@@ -225,6 +225,7 @@ int lsd_diagnostics_device(lsd_ctx* ctx, double* scalars, double* spectra, doubl
 int lsd_coll_to_state(lsd_ctx* ctx, const double* re, const double* im, cplx* out);
 int lsd_state_to_coll(lsd_ctx* ctx, const cplx* in, double* re, double* im);
 int lsd_factor_batch(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info);
+int lsd_operator_solve(lsd_ctx* ctx, int nfield, const int* fields, double* d_data);
 int lsd_solve_batch(lsd_ctx* ctx, int n, int kl, int nmat, const double* d_ab, const int* d_ipiv,
                     int nrhs, const int* d_map, double* d_b);
 

@@ -1742,6 +1742,115 @@ int lsd_state_to_coll_n(lsd_ctx* ctx, int rows, const cplx* in, double* re, doub
   return LSD_OK;
 }
 
+// ---- the context's operators applied to caller right-hand sides ------------------------
+// X_l x = b for every (l, m) column of up to OPS_MAXF fields in one launch (tim_zerobc +
+// tim_invX, timestep.F90:566-588, 684-690): codensity / composition (every l), the
+// toroidal velocity and the field's toroidal / poloidal scalars (l >= 1; the l = 0 column
+// keeps b with zero boundary rows, as tim_invX skips it).  The poloidal velocity is the
+// reference's fourth-order composite (velocity.F90:369-395, 445-465 without the Y
+// multiply): x = XPol^-1 zerobc(XGre^-1 zerobc(b)), then vel_gre_adjust with the two
+// Green's functions so that dx/dr vanishes at both walls.  In place on [N][H] complex
+// fields; one thread per harmonic and field, the rows streamed through registers.
+constexpr int OPS_MAXF = 8;
+struct OpSolveArgs {
+  int N, H, L, NL;
+  const int* hl;
+  const double* lus;
+  const int* ipivs;
+  const double* gret;
+  const double* invg;
+  cplx* data;  // nfield consecutive [N][H] fields
+  int field[OPS_MAXF];
+};
+
+template <int KL>
+__global__ void __launch_bounds__(SOLVE_THREADS) k_opsolve(OpSolveArgs a) {
+  const int j = blockIdx.y, fld = a.field[j];
+  const int nh = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nh >= a.H) return;
+  const int N = a.N, L = a.L, l = a.hl[nh];
+  constexpr int LD = 3 * KL + 1;
+  const size_t rst = a.H;
+  double2* X = a.data + (size_t)j * N * a.H + nh;
+  const double2 z2 = make_double2(0.0, 0.0);
+  const bool zero = fld == LSD_COD_C || fld == LSD_COMP_C;
+  const int fam = fld == LSD_VEL_TOR ? OP_VTOR : fld == LSD_VEL_POL ? OP_VPOL : fld == LSD_COD_C ? OP_COD
+                : fld == LSD_COMP_C ? OP_COMP : fld == LSD_MAG_TOR ? OP_MTOR : OP_MPOL;
+  auto band = [&](int f) {
+    Band B;
+    B.f = a.lus + (size_t)f * a.NL * LD * L + l;
+    B.piv = a.ipivs + (size_t)f * a.NL * L + l;
+    B.L = L;
+    B.LD = LD;
+    return B;
+  };
+  auto in = [&](int n) { return (n == 0 || n == N - 1) ? z2 : X[(size_t)n * rst]; };  // tim_zerobc
+  auto rd = [&](int n) { return X[(size_t)n * rst]; };
+  auto wr = [&](int c, double2 x) { X[(size_t)c * rst] = x; };
+  if (l == 0 && !zero) {
+    X[0] = z2;
+    X[(size_t)(N - 1) * rst] = z2;
+    return;
+  }
+  const Band B1 = band(fam);
+  if (fld == LSD_VEL_POL) {
+    const Band B2 = band(OP_VGRE);
+    stream_forward<KL>(B2, N, in, wr);
+    stream_backward<KL>(B2, N, rd, wr);
+    double2 x0 = z2, xN = z2;
+    stream_forward<KL>(B1, N, in, wr);
+    stream_backward<KL>(B1, N, rd, [&](int c, double2 x) {
+      X[(size_t)c * rst] = x;
+      if (c == N - 1) xN = x;
+      if (c == 0) x0 = x;
+    });
+    double iG[4];
+    for (int i = 0; i < 4; ++i) iG[i] = __ldg(a.invg + (size_t)l * 4 + i);
+    double2 ca, cb;
+    gre_coeffs(iG, x0, xN, ca, cb);
+    const double* g = a.gret + l;
+#pragma unroll 8
+    for (int n = 0; n < N; ++n) {
+      const double g1 = __ldg(g + (size_t)(2 * n) * L), g2 = __ldg(g + (size_t)(2 * n + 1) * L);
+      const double2 x = X[(size_t)n * rst];
+      X[(size_t)n * rst] = make_double2(x.x - ca.x * g1 - cb.x * g2, x.y - ca.y * g1 - cb.y * g2);
+    }
+    return;
+  }
+  stream_forward<KL>(B1, N, in, wr);
+  stream_backward<KL>(B1, N, rd, wr);
+}
+
+int lsd_operator_solve(lsd_ctx* ctx, int nfield, const int* fields, double* d_data) {
+  if (nfield < 1 || nfield > OPS_MAXF) return lsd_fail(ctx, LSD_EARG, "lsd_operator_solve_device: 1..8 fields");
+  if (!ctx->have_ops) return lsd_fail(ctx, LSD_ESTATE, "lsd_operator_solve_device: no operators built");
+  OpSolveArgs a;
+  a.N = ctx->N; a.H = ctx->H; a.L = ctx->L; a.NL = ctx->NL;
+  a.hl = ctx->d_l; a.lus = ctx->d_lus; a.ipivs = ctx->d_ipivs; a.gret = ctx->d_gret; a.invg = ctx->d_invg;
+  a.data = (cplx*)d_data;
+  for (int i = 0; i < OPS_MAXF; ++i) a.field[i] = LSD_COD_C;
+  for (int i = 0; i < nfield; ++i) {
+    const int f = fields[i];
+    if (f < LSD_VEL_TOR || f > LSD_COMP_C)
+      return lsd_fail(ctx, LSD_EARG, "lsd_operator_solve_device: field must be one of the five state scalars or composition");
+    if ((f == LSD_MAG_TOR || f == LSD_MAG_POL) && ctx->Nic > 1)
+      return lsd_fail(ctx, LSD_EARG, "lsd_operator_solve_device: the field's operators are coupled to the inner core (Nic > 1)");
+    a.field[i] = f;
+  }
+  const dim3 g(ceil_div(ctx->H, SOLVE_THREADS), nfield);
+  switch (ctx->KL) {
+    case 2: k_opsolve<2><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
+    case 3: k_opsolve<3><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
+    case 4: k_opsolve<4><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
+    case 5: k_opsolve<5><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
+    case 6: k_opsolve<6><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
+    default: return lsd_fail(ctx, LSD_EARG, "stencil half-width KL must be 2..6");
+  }
+  ctx->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return LSD_OK;
+}
+
 int lsd_factor_batch(lsd_ctx* ctx, int n, int kl, int nmat, double* d_ab, int* d_ipiv, int* d_info) {
   k_factor_batch<<<ceil_div(nmat, 64), 64, 0, ctx->stream>>>(n, kl, nmat, d_ab, d_ipiv, d_info);
   ctx->launches++;

@@ -91,6 +91,9 @@ def load_library(path=None):
         "lsd_synchronize": [_V],
         "lsd_last_elapsed_ms": [_V, _D],
         "lsd_kernel_launches": [_V, ctypes.POINTER(ctypes.c_longlong)],
+        "lsd_operator_solve_device": [_V, ctypes.c_int, _I, _V],
+        "lsd_get_stream": [_V, ctypes.POINTER(_V)],
+        "lsd_ensemble_last_elapsed_ms": [_V, _D],
         "lsd_tim_check_cgce": [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState)],
         "lsd_tim_new_tstep": [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState), _I],
     }
@@ -382,6 +385,18 @@ class Context:
     def banded_solve_device(self, n, kl, nmat, d_ab, d_ipiv, nrhs, d_map, d_b):
         self._ok(self.lib.lsd_banded_solve_device(self.h, n, kl, nmat, _V(d_ab), _V(d_ipiv), nrhs, _V(d_map), _V(d_b)))
 
+    def stream(self):
+        """the context's CUDA stream handle (int), e.g. for torch.cuda.ExternalStream"""
+        v = _V()
+        self._ok(self.lib.lsd_get_stream(self.h, ctypes.byref(v)))
+        return v.value or 0
+
+    def operator_solve_device(self, fields, d_data):
+        """lsd_operator_solve_device: the context's operators applied in place to
+        len(fields) consecutive device fields [N][H] complex at d_data (one launch)."""
+        f = (ctypes.c_int * len(fields))(*fields)
+        self._ok(self.lib.lsd_operator_solve_device(self.h, len(fields), f, _V(d_data)))
+
     PHASES = ["spectral_prep", "synthesis", "fft_products", "analysis", "spectral_tail",
               "predictor_solve", "corrector_solve"]
 
@@ -418,8 +433,9 @@ class Context:
 
 class Ensemble:
     """n independent runs (their own configurations and resolutions) on one GPU, stepped
-    in lock-step with their graphs on separate streams (lsd_ensemble_*).  members[i] is a
-    Context view of run i (set_coll, set_reference_state, energies, ...)."""
+    together by one graph launch whose branches are the members' step loops
+    (lsd_ensemble_*).  members[i] is a Context view of run i (set_coll,
+    set_reference_state, energies, ...)."""
 
     def __init__(self, cfgs):
         self.lib = load_library()
@@ -440,6 +456,12 @@ class Ensemble:
             msg = self.lib.lsd_ensemble_last_error(self.h)
             raise LsdError(rc, msg.decode() if msg else "")
         return rc
+
+    def last_elapsed_ms(self):
+        """device time of the last step() call's graph launch"""
+        d = ctypes.c_double()
+        self._ok(self.lib.lsd_ensemble_last_elapsed_ms(self.h, ctypes.byref(d)))
+        return d.value
 
     def step(self, nsteps=1):
         st = (capi.LsdStats * len(self.members))()

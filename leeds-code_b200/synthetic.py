@@ -159,3 +159,42 @@ def config_dynamo128(**kw):
                 Pm=3.0, vel_bc=1, cod_bc=1, timestep=2e-6, implicit=0.6, time_step_control=2)
     base.update(kw)
     return capi.template_config(**base)
+
+
+def config_solve257(**kw):
+    """Batched banded solves: L = M = 256, Mp = 1, N = 257, KL = 4 (the 9-point stencil),
+    with the operator parameters of config_dynamo128 (E = 3e-4, Ra = 200, Pr = 1, Pm = 3,
+    dt = 2e-6, implicit 0.6)."""
+    base = dict(L=256, M=256, Mp=1, N=257, KL=4, E=3e-4, Ra=200.0, Pr=1.0, Pm=3.0, vel_bc=1, cod_bc=1,
+                timestep=2e-6, implicit=0.6, time_step_control=2)
+    base.update(kw)
+    return capi.template_config(**base)
+
+
+def seeded_rhs(nfield, N, H, hm, seed=SEED):
+    """complex N(0, 1) right-hand sides [field][N][H] (re, im), Im = 0 where m = 0"""
+    rng = np.random.default_rng(seed)
+    re = rng.standard_normal((nfield, N, H))
+    im = rng.standard_normal((nfield, N, H))
+    im[:, :, np.asarray(hm) == 0] = 0.0
+    return re, im
+
+
+ENSEMBLE_L = (64, 64, 96, 96, 128, 128, 192, 192)
+
+
+def config_ensemble(**kw):
+    """The anelastic ensemble: eight runs of config_anelastic, two each at L = M = 64, 96,
+    128, 192 with N = L + 1 (Th = 3L/2, Ph = 2 Th), N_rho = 3 polytrope, codensity +
+    composition; kw apply to every member (e.g. precision, ozaki_slices)."""
+    return [config_anelastic(L=L, **kw) for L in ENSEMBLE_L]
+
+
+def setup_ensemble_member(ctx, cfg, seed):
+    """reference state (polytrope on the member's grid) and the seeded l^-2 state"""
+    if not cfg.boussinesq:
+        ctx.set_reference_state(polytrope_reference_state(cfg.N, cfg.rratio))
+    st = boussinesq_state(cfg, seed=seed, composition=bool(cfg.comp_tstep))
+    for f, (re, im) in st.items():
+        ctx.set_coll(f, re, im)
+    return st

@@ -2633,6 +2633,34 @@ int orc_legendre_table(const Oracle* o, int which, double* out) {
   std::memcpy(out, t->data(), t->size() * sizeof(double));
   return 0;
 }
+// The operators applied to right-hand sides the way lsd_operator_solve_device does:
+// tim_zerobc + tim_invX (timestep.F90:566-588) with the field's operator, the poloidal
+// velocity as XGre, XPol and vel_gre_adjust (velocity.F90:369-395, 445-465, no Y multiply).
+// re, im: (H, N) C order, in place.
+int orc_operator_solve(Oracle* o, int field, double* re, double* im) {
+  Coll b;
+  b.init(o->N, o->H);
+  std::memcpy(b.re.data(), re, b.re.size() * 8);
+  std::memcpy(b.im.data(), im, b.im.size() * 8);
+  tim_zerobc(*o, b);
+  switch (field) {
+    case LSD_VEL_TOR: tim_invX(*o, false, o->XTor, b); break;
+    case LSD_VEL_POL:
+      tim_invX(*o, false, o->XGre, b);
+      tim_zerobc(*o, b);
+      tim_invX(*o, false, o->XPol, b);
+      vel_gre_adjust(*o, b);
+      break;
+    case LSD_COD_C: tim_invX(*o, true, o->XC, b); break;
+    case LSD_COMP_C: tim_invX(*o, true, o->XComp, b); break;
+    case LSD_MAG_TOR: if (o->Nic > 1) return LSD_EARG; tim_invX(*o, false, o->mXTor, b); break;
+    case LSD_MAG_POL: if (o->Nic > 1) return LSD_EARG; tim_invX(*o, false, o->mXPol, b); break;
+    default: return LSD_EARG;
+  }
+  std::memcpy(re, b.re.data(), b.re.size() * 8);
+  std::memcpy(im, b.im.data(), b.im.size() * 8);
+  return 0;
+}
 // LU factors of one operator: which 0 XTor 1 XPol 2 XGre 3 XC 4 mXTor 5 mXPol
 int orc_operator_lu(const Oracle* o, int which, int l, double* ab, int* ipiv) {
   const std::vector<LUBand>* v[] = {&o->XTor, &o->XPol, &o->XGre, &o->XC, &o->mXTor, &o->mXPol};

@@ -79,6 +79,7 @@ def load():
         "orc_set_dt": (ctypes.c_int, [vp, ctypes.c_double]),
         "orc_dt_control": (None, [vp, _D]),
         "orc_qst2rtp_vel": (ctypes.c_int, [vp, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+        "orc_operator_solve": (ctypes.c_int, [vp, ctypes.c_int, _D, _D]),
         "orc_tim_check_cgce": (ctypes.c_int, [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState)]),
         "orc_tim_new_tstep": (ctypes.c_int, [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState), _I]),
     }
@@ -167,6 +168,14 @@ class Oracle:
         t = np.zeros((self.H, self.Th2))
         assert self.lib.orc_legendre_table(self.h, which, _dp(t)) == 0
         return t.T.copy()  # (Th2, H)
+
+    def operator_solve(self, f, re, im):
+        """tim_zerobc + tim_invX of field f's operator (the poloidal velocity's composite)
+        on (H, N) arrays; returns the solution"""
+        re = np.array(re, dtype=np.float64, order="C")
+        im = np.array(im, dtype=np.float64, order="C")
+        assert self.lib.orc_operator_solve(self.h, f, _dp(re), _dp(im)) == 0
+        return re, im
 
     def operator_lu(self, which, l):
         kl = self.sz["KL"]

@@ -15,9 +15,17 @@ Tolerances, relative to the largest magnitude of the compared field:
   tensor, S = 8   1e-13
   tensor, S = 7   5e-12
   tensor, S = 4   1e-6    (30 bits, about FP32)
-config[2]: batched banded solves at N = 257, KL = 4, one operator per degree l < 256 for
-4 fields, every (l, m) right-hand side (Re and Im columns, 4 x 32896 x 2), residual
-|A x - b| / |b| <= 1e-13 on a sample checked on the host.
+config[2]: batched banded solves at N = 257, KL = 4.
+  * On the context's own Crank-Nicolson operators at L = M = 256 (dt = 2e-6, E = 3e-4,
+    Pm = 3, implicit 0.6; lsd_operator_solve_device): every (l, m) right-hand side of the
+    codensity, the toroidal velocity, the field's toroidal and poloidal scalars and the
+    poloidal velocity's fourth-order composite (5 x 32896 complex columns) in one launch,
+    against the oracle's tim_invX / composite on the same right-hand sides (1e-13 of each
+    field's largest solution value), and the residual |A x - b| / |b| of the second-order
+    families from the LAPACK factors (<= 1e-13, a sample of degrees).
+  * On random band matrices (lsd_banded_*_device): one operator per degree l < 256 for
+    4 fields, every (l, m) right-hand side (Re and Im columns, 4 x 32896 x 2), residual
+    |A x - b| / |b| <= 1e-13 on a sample checked on the host.
 """
 import importlib
 import time
@@ -155,3 +163,70 @@ def test_batched_banded_solves_n257():
         lu_l, ip_l, info = lapack.dgbtrf(ab[k].T.copy(), kl, kl)
         assert np.abs(lu_g[k].T - lu_l).max() <= 1e-13 * np.abs(lu_l).max()
     g.close()
+
+
+def lu_apply(ab, ipiv, kl, x):
+    """A x from LAPACK band LU factors: ab (3 kl + 1, n) band storage (0-based rows, U in
+    rows 0..2 kl, the multipliers below), ipiv 1-based; x (n, ncols).  Undoes dgbtrs's
+    forward elimination (b[j+1..] -= l_j b[j] after swapping j and ipiv[j]) on U x."""
+    n = ab.shape[1]
+    y = np.zeros_like(x)
+    for j in range(n):
+        i0 = max(0, j - 2 * kl)
+        y[i0:j + 1] += ab[2 * kl + np.arange(i0, j + 1) - j, j][:, None] * x[j]
+    for j in range(n - 2, -1, -1):
+        km = min(kl, n - 1 - j)
+        y[j + 1:j + 1 + km] += ab[2 * kl + 1:2 * kl + 1 + km, j][:, None] * y[j]
+        p = ipiv[j] - 1
+        if p != j:
+            y[[j, p]] = y[[p, j]]
+    return y
+
+
+SOLVE257_FIELDS = (capi.COD_C, capi.VEL_TOR, capi.MAG_TOR, capi.MAG_POL, capi.VEL_POL)
+# oracle operator_lu index of each second-order family
+LU_INDEX = {capi.VEL_TOR: 0, capi.COD_C: 3, capi.MAG_TOR: 4, capi.MAG_POL: 5}
+
+
+@pytest.mark.gpu
+def test_operator_solves_n257(parity_report):
+    import torch
+    syn = pkg.synthetic
+    cfg = syn.config_solve257()
+    g, o = pkg.Context(cfg), ol.Oracle(cfg)
+    l, m, _ = o.harmonics()
+    nf, N, H = len(SOLVE257_FIELDS), o.N, o.H
+    re, im = syn.seeded_rhs(nf, N, H, m)
+    d = torch.tensor(np.stack([re, im], axis=-1), device="cuda", dtype=torch.float64)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.operator_solve_device(SOLVE257_FIELDS, d.data_ptr())
+    g.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    x = d.cpu().numpy()
+    print("operator solves: %d fields x %d (l, m) columns, N = %d, KL = 4: %.2f ms (host-timed)" % (nf, H, N, ms))
+    for k, f in enumerate(SOLVE257_FIELDS):
+        xr, xi = o.operator_solve(f, re[k].T, im[k].T)  # (H, N)
+        gr, gi = x[k, :, :, 0].T, x[k, :, :, 1].T
+        err = np.hypot(gr - xr, gi - xi).max() / np.hypot(xr, xi).max()
+        parity_report("solve257 field %d: device vs oracle solve" % f, err, 1e-13)
+        assert err <= 1e-13, (f, err)
+        if f not in LU_INDEX:
+            continue
+        worst = 0.0
+        for deg in (1, 2, 17, 128, 255) + ((0,) if f == capi.COD_C else ()):
+            cols = np.nonzero(l == deg)[0]
+            ab, ipiv = o.operator_lu(LU_INDEX[f], deg)
+            for part in (0, 1):
+                xs = x[k, :, cols, part].T  # (N, ncols)
+                bs = (re if part == 0 else im)[k][:, cols].copy()
+                bs[0], bs[-1] = 0.0, 0.0  # tim_zerobc
+                res = lu_apply(ab, ipiv, 4, xs) - bs
+                nb = np.abs(bs).max(axis=0)
+                ok = nb > 0
+                if ok.any():
+                    worst = max(worst, float((np.abs(res).max(axis=0)[ok] / nb[ok]).max()))
+        parity_report("solve257 field %d: residual |A x - b| / |b|" % f, worst, 1e-13)
+        assert worst <= 1e-13, (f, worst)
+    g.close()
+    o.close()

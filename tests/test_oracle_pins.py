@@ -210,3 +210,40 @@ def test_sht_round_trip_exact():
     for a, b in ((q, q2), (sv, s2), (tv, t2)):
         np.testing.assert_allclose(b[0], a[0], rtol=0, atol=1e-10)
         np.testing.assert_allclose(b[1], a[1], rtol=0, atol=1e-10)
+
+
+def test_operator_solve_residual_small():
+    """The oracle's operator solves (tim_zerobc + tim_invX; the poloidal velocity's
+    composite) at L = M = 16, N = 33, KL = 4: the second-order families' residuals from
+    their LAPACK factors (as the device test forms them), and the composite's x = 0,
+    dx/dr = 0 at both walls (vel_gre_adjust)."""
+    from test_gpu_configs import lu_apply, LU_INDEX
+    cfg = capi.template_config(L=16, M=16, Mp=1, N=33, KL=4, timestep=2e-6, E=3e-4, Pm=3.0, Ra=200.0)
+    o = ol.Oracle(cfg)
+    l, m, _ = o.harmonics()
+    rng = np.random.default_rng(4)
+    N, H = o.N, o.H
+    for f, idx in LU_INDEX.items():
+        re, im = rng.standard_normal((H, N)), rng.standard_normal((H, N))
+        xr, xi = o.operator_solve(f, re, im)
+        for deg in range(0 if f == capi.COD_C else 1, 16):
+            cols = np.nonzero(l == deg)[0]
+            ab, ipiv = o.operator_lu(idx, deg)
+            b = re[cols].T.copy()
+            b[0], b[-1] = 0.0, 0.0
+            res = lu_apply(ab, ipiv, 4, xr[cols].T) - b
+            assert np.abs(res).max() <= 1e-13 * np.abs(b).max(), (f, deg)
+    re, im = rng.standard_normal((H, N)), rng.standard_normal((H, N))
+    xr, xi = o.operator_solve(capi.VEL_POL, re, im)
+    band = o.dr(1)  # first radial derivative, Fortran band: D(i, j) at [KL + i - j, j]
+    kl = 4
+    D = np.zeros((N, N))
+    for j in range(N):
+        for i in range(max(0, j - kl), min(N, j + kl + 1)):
+            D[i, j] = band[kl + i - j, j]
+    ok = l > 0
+    for x in (xr, xi):
+        assert np.abs(x[ok][:, [0, -1]]).max() <= 1e-13 * np.abs(x).max()
+        dx = x[ok] @ D.T
+        assert np.abs(dx[:, [0, -1]]).max() <= 1e-10 * np.abs(dx).max()
+    o.close()
