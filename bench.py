@@ -277,19 +277,30 @@ def run_reference(args, rank, world):
 
 
 def ctx_timer(handle):
-    """(stream, start(), stop() -> ms): CUDA events on a library stream (an int handle)"""
+    """(stream, start(), stop() -> ms): CUDA events on a library stream (an int handle).
+    Nothing is allocated on that stream (torch's allocator would tie blocks to it, and the
+    library destroys it with its context): tensors live on torch's stream, and the two
+    streams are ordered with events (after())."""
     import torch
     st = torch.cuda.ExternalStream(handle)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def start():
-        a.record(st)
+    def start(on=None):
+        a.record(on or st)
 
-    def stop():
-        b.record(st)
+    def stop(on=None):
+        b.record(on or st)
         b.synchronize()
         return a.elapsed_time(b)
     return st, start, stop
+
+
+def after(first, then):
+    """make stream `then` wait for the work queued so far on stream `first`"""
+    import torch
+    ev = torch.cuda.Event()
+    ev.record(first)
+    then.wait_event(ev)
 
 
 def pinned_like(a):
@@ -327,11 +338,11 @@ def run_sht256(args, rank, world, local_rank, dist):
         spec = np.stack([rng.standard_normal((nf, N, H)) * amp, rng.standard_normal((nf, N, H)) * amp], axis=-1)
         spec[:, :, m == 0, 1] = 0.0
         st, start, stop = ctx_timer(ctx.stream())
-        with torch.cuda.stream(st):
-            d_spec = torch.tensor(spec, device="cuda:%d" % local_rank)
-            d_phys = torch.empty((nf, N, Ph, Th), device="cuda:%d" % local_rank, dtype=torch.float64)
-            d_back = torch.empty_like(d_spec)
-        st.synchronize()
+        cur = torch.cuda.current_stream()
+        d_spec = torch.tensor(spec, device="cuda:%d" % local_rank)
+        d_phys = torch.empty((nf, N, Ph, Th), device="cuda:%d" % local_rank, dtype=torch.float64)
+        d_back = torch.empty_like(d_spec)
+        torch.cuda.synchronize()
 
         def round_trip():
             ctx.sht_synth_device(nf, d_spec.data_ptr(), d_phys.data_ptr())
@@ -351,29 +362,32 @@ def run_sht256(args, rank, world, local_rank, dist):
             ms = max_over_ranks(dist, ms, "cuda:%d" % local_rank)
         # errors: per field against the FP64 variant's synthesis and round trip, and the
         # round trip against the input
-        with torch.cuda.stream(st):
-            if prec == "fp64":
-                ref_phys, ref_back = d_phys.clone(), d_back.clone()
-                e_syn = e_rt = [0.0] * nf
-            else:
-                e_syn = [float((d_phys[f] - ref_phys[f]).abs().max() / ref_phys[f].abs().max()) for f in range(nf)]
-                e_rt = [float((d_back[f] - ref_back[f]).abs().max() / ref_back[f].abs().max()) for f in range(nf)]
-            e_in = [float((d_back[f] - d_spec[f]).abs().max() / d_spec[f].abs().max()) for f in range(nf)]
+        ctx.synchronize()
+        if prec == "fp64":
+            ref_phys, ref_back = d_phys.clone(), d_back.clone()
+            e_syn = e_rt = [0.0] * nf
+        else:
+            e_syn = [float((d_phys[f] - ref_phys[f]).abs().max() / ref_phys[f].abs().max()) for f in range(nf)]
+            e_rt = [float((d_back[f] - ref_back[f]).abs().max() / ref_back[f].abs().max()) for f in range(nf)]
+        e_in = [float((d_back[f] - d_spec[f]).abs().max() / d_spec[f].abs().max()) for f in range(nf)]
+        torch.cuda.synchronize()
         # end to end with host buffers: pinned spectra up, round trip, spectra back
         h_spec, h_back = pinned_like(spec), pinned_like(np.zeros_like(spec))
         ne = max(1, min(args.steps, 5))
-        start()
-        with torch.cuda.stream(st):
-            for _ in range(ne):
-                d_spec.copy_(h_spec, non_blocking=True)
-                round_trip()
-                h_back.copy_(d_back, non_blocking=True)
-        e2e_ms = stop() / ne
+        start(cur)
+        for _ in range(ne):
+            d_spec.copy_(h_spec, non_blocking=True)
+            after(cur, st)
+            round_trip()
+            after(st, cur)
+            h_back.copy_(d_back, non_blocking=True)
+        e2e_ms = stop(cur) / ne
         if dist:
             e2e_ms = max_over_ranks(dist, e2e_ms, "cuda:%d" % local_rank)
         out[(prec, S)] = {"ms": ms, "e2e_ms": e2e_ms, "launches": launches, "err_synth_vs_fp64": max(e_syn),
                           "err_round_trip_vs_fp64": max(e_rt), "err_round_trip_vs_input": max(e_in),
                           "sizes": ctx.sizes}
+        torch.cuda.synchronize()
         del d_spec, d_phys, d_back
         ctx.close()
     if rank != 0:
@@ -453,26 +467,28 @@ def run_solve257(args, rank, world, local_rank, dist):
     re, im = syn.seeded_rhs(len(fields), N, H, m, seed=syn.SEED + rank)
     rhs = np.stack([re, im], axis=-1)
     st, start, stop = ctx_timer(ctx.stream())
+    cur = torch.cuda.current_stream()
     dev = "cuda:%d" % local_rank
-    with torch.cuda.stream(st):
-        d_save = torch.tensor(rhs, device=dev)
-        d = d_save.clone()
-    st.synchronize()
+    d_save = torch.tensor(rhs, device=dev)
+    d = d_save.clone()
+    torch.cuda.synchronize()
 
     def solve():
         ctx.operator_solve_device(fields, d.data_ptr())
     for _ in range(args.warmup):
-        with torch.cuda.stream(st):
-            d.copy_(d_save)
+        d.copy_(d_save)
+        after(cur, st)
         solve()
+        after(st, cur)
     ctx.synchronize()
+    torch.cuda.synchronize()
     if dist:
         dist.barrier()
     tot = 0.0
     l0 = ctx.kernel_launches()
     for _ in range(args.steps):
-        with torch.cuda.stream(st):
-            d.copy_(d_save)  # fresh right-hand sides, outside the timed launch
+        d.copy_(d_save)  # fresh right-hand sides, outside the timed launch
+        after(cur, st)
         start()
         solve()
         tot += stop()
@@ -482,16 +498,19 @@ def run_solve257(args, rank, world, local_rank, dist):
         ms = max_over_ranks(dist, ms, dev)
     h_rhs, h_out = pinned_like(rhs), pinned_like(np.zeros_like(rhs))
     ne = max(1, min(args.steps, 5))
-    start()
-    with torch.cuda.stream(st):
-        for _ in range(ne):
-            d.copy_(h_rhs, non_blocking=True)
-            solve()
-            h_out.copy_(d, non_blocking=True)
-    e2e_ms = stop() / ne
+    start(cur)
+    for _ in range(ne):
+        d.copy_(h_rhs, non_blocking=True)
+        after(cur, st)
+        solve()
+        after(st, cur)
+        h_out.copy_(d, non_blocking=True)
+    e2e_ms = stop(cur) / ne
     if dist:
         e2e_ms = max_over_ranks(dist, e2e_ms, dev)
     sz = ctx.sizes
+    torch.cuda.synchronize()
+    del d, d_save
     ctx.close()
     if rank != 0:
         return

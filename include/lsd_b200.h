@@ -143,7 +143,12 @@ typedef struct lsd_config {
   /* inner-core rotation (parameters.F90_template:100-102, rotation.F90) */
   int rot_tstep;            /* b_rot_tstep: step rot_omega with the torques           */
   int rot_force_0;          /* b_rot_force_0: hold rot_omega at zero                  */
-  int reserved[6];
+  /* no counterpart in the reference (its analogue is FFTW's plan search,
+   * transform.fftw3.F90:76-93): 1 = lsd_create times the candidate phi-FFT radices, the
+   * tensor-core GEMM's ring depth and CTAs per SM, and the banded solves' threads per CTA
+   * on this configuration and keeps the fastest (lsd_get_tuning); 0 = the defaults */
+  int autotune;
+  int reserved[5];
 } lsd_config;
 
 /* derived sizes (parameters.F90_template:251-262; parallel.h_template:54-62) */
@@ -169,6 +174,28 @@ typedef struct lsd_pc_state {
 } lsd_pc_state;
 
 typedef struct lsd_ctx lsd_ctx;
+
+/* The tunable launch parameters of a context (lsd_get_tuning / lsd_set_tuning).  No
+ * counterpart in the reference (FFTW chooses its own plans there). */
+typedef struct lsd_tuning {
+  int tuned;             /* 1 when lsd_create timed the candidates (cfg.autotune)          */
+  int fft_E, fft_G;      /* phi FFT of P2 = 3M/2 complex points: E-point column DFTs, then
+                            G-point row DFTs (both in registers, shared memory between)     */
+  int gemm_stages;       /* tensor-core contraction: bulk-copy ring stages (2..4)           */
+  int gemm_ctas_per_sm;  /* tensor-core contraction: persistent CTAs per SM (1 or 2)        */
+  int solve_threads;     /* banded-solve kernels: threads per CTA (32, 64 or 128)            */
+  int reserved[2];
+  double ms_fft, ms_gemm, ms_solve;  /* timed ms of the chosen candidates (0: not tuned):
+                            one evaluation, one evaluation, one predictor solve             */
+} lsd_tuning;
+
+/* The candidates the autotuner times for a configuration (no device work). */
+#define LSD_TUNE_MAX 8
+typedef struct lsd_tune_space {
+  int nfft, fft_E[LSD_TUNE_MAX], fft_G[LSD_TUNE_MAX];
+  int ngemm, gemm_stages[LSD_TUNE_MAX], gemm_ctas[LSD_TUNE_MAX];
+  int nsolve, solve_threads[LSD_TUNE_MAX];
+} lsd_tune_space;
 
 /* Fill cfg with the template parameter values of Scripts/parameters.F90_template. */
 int lsd_config_default(lsd_config* cfg);
@@ -369,6 +396,18 @@ int lsd_banded_solve_device(lsd_ctx* ctx, int n, int kl, int nmat, const double*
  * fields in the context's layout, [N][H] complex (re, im interleaved), solved in place;
  * one launch for all fields, on the context's stream (not synchronised). */
 int lsd_operator_solve_device(lsd_ctx* ctx, int nfield, const int* fields, double* d_data);
+
+/* ---- autotuning (no counterpart in the reference) ------------------------------------
+ * lsd_tune_candidates: the candidates for cfg (the default first in each list), filtered by
+ * the compiled radices and the shared-memory limits.  lsd_tune_choose: the selection
+ * rule -- the fastest of n timed candidates (ms[]), unless it beats candidate dflt by
+ * less than 2 % (timing noise), in which case dflt.  lsd_get_tuning / lsd_set_tuning:
+ * the context's parameters (set: validated against its tune space; results may change in
+ * the last bits with the FFT radices, not with the other parameters). */
+int lsd_tune_candidates(const lsd_config* cfg, lsd_tune_space* out);
+int lsd_tune_choose(int n, const double* ms, int dflt);
+int lsd_get_tuning(const lsd_ctx* ctx, lsd_tuning* out);
+int lsd_set_tuning(lsd_ctx* ctx, const lsd_tuning* in);
 
 /* ---- synchronisation and timing ------------------------------------------------------ */
 /* The context's CUDA stream (a cudaStream_t), on which every asynchronous entry point

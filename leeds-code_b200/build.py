@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(ROOT, "_build", "lsd_b200")
 LIB = os.path.join(HERE, "liblsd_b200.so")
-SOURCES = ["lsd_tables.cu", "lsd_sht.cu", "lsd_fft.cu", "lsd_solve.cu", "lsd_capi.cu", "lsd_ozaki.cu"]
+SOURCES = ["lsd_tables.cu", "lsd_sht.cu", "lsd_fft.cu", "lsd_solve.cu", "lsd_capi.cu", "lsd_ozaki.cu", "lsd_tune.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]

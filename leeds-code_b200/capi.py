@@ -87,7 +87,8 @@ class LsdConfig(ctypes.Structure):
             "rratio", "alpha", "Ra", "Ra_comp", "Pr", "Sc", "Pm", "E", "Hyp",
             "implicit", "timestep", "dterr", "courant", "corr_upper", "corr_lower",
             "source", "source_comp", "qi", "qo", "qi_comp", "qo_comp")] + \
-        [("rot_tstep", ctypes.c_int), ("rot_force_0", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+        [("rot_tstep", ctypes.c_int), ("rot_force_0", ctypes.c_int), ("autotune", ctypes.c_int),
+         ("reserved", ctypes.c_int * 5)]
 
 
 class LsdSizes(ctypes.Structure):
@@ -100,6 +101,23 @@ class LsdStats(ctypes.Structure):
                 ("evaluations", ctypes.c_int), ("kernel_launches", ctypes.c_int),
                 ("last_dterr", ctypes.c_double), ("t", ctypes.c_double),
                 ("dt", ctypes.c_double)]
+
+
+class LsdTuning(ctypes.Structure):
+    """lsd_tuning: the tunable launch parameters of a context"""
+    _fields_ = [(n, ctypes.c_int) for n in ("tuned", "fft_E", "fft_G", "gemm_stages", "gemm_ctas_per_sm",
+                                            "solve_threads")] + [("reserved", ctypes.c_int * 2)] + \
+        [(n, ctypes.c_double) for n in ("ms_fft", "ms_gemm", "ms_solve")]
+
+
+TUNE_MAX = 8
+
+
+class LsdTuneSpace(ctypes.Structure):
+    _fields_ = [("nfft", ctypes.c_int), ("fft_E", ctypes.c_int * TUNE_MAX), ("fft_G", ctypes.c_int * TUNE_MAX),
+                ("ngemm", ctypes.c_int), ("gemm_stages", ctypes.c_int * TUNE_MAX),
+                ("gemm_ctas", ctypes.c_int * TUNE_MAX), ("nsolve", ctypes.c_int),
+                ("solve_threads", ctypes.c_int * TUNE_MAX)]
 
 
 class LsdPcState(ctypes.Structure):

@@ -716,6 +716,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   TRY(lsd_build_tables(ctx));
   TRY(lsd_build_operators(ctx));
   if (c.precision == LSD_PREC_OZAKI) TRY(lsd_ozaki_setup(ctx));
+  if (c.autotune) TRY(lsd_autotune(ctx));
 #undef TRY
 #undef CTRY
   *out = ctx;

@@ -192,6 +192,9 @@ struct lsd_ctx {
   cudaStream_t cap_stream[2] = {nullptr, nullptr};
   long long k_begin = 0, k_loop = 0, k_rebuild = 0, k_corr = 0;
   void* oz = nullptr;  // tensor-core path state (lsd_ozaki.cu)
+  // tunables besides fftE / fftG and the GEMM tiles (lsd_tune.cu)
+  int solve_threads = 128;
+  lsd_tuning tuning{};
 };
 
 int lsd_fail(lsd_ctx* ctx, int code, const std::string& msg);
@@ -237,6 +240,15 @@ int lsd_ozaki_check(lsd_ctx* ctx);
 int* lsd_ozaki_err_flag(lsd_ctx* ctx);
 int lsd_ozaki_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups);
 int lsd_ozaki_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups);
+bool lsd_ozaki_tiles_ok(int S, int nst, int ctas);
+int lsd_ozaki_default_stages(int S);
+void lsd_ozaki_default_tiles(int S, int* nst, int* ctas);
+void lsd_ozaki_get_tiles(const lsd_ctx* ctx, int* nst, int* ctas);
+int lsd_ozaki_set_tiles(lsd_ctx* ctx, int nst, int ctas);
+// ---- autotuner (lsd_tune.cu) ----
+bool lsd_fft_compiled(int E, int G);
+size_t lsd_products_smem_for(int nfields, int P2, int E, int G, int NM);
+int lsd_autotune(lsd_ctx* ctx);
 
 // small helpers
 static inline int ceil_div(int a, int b) { return (a + b - 1) / b; }

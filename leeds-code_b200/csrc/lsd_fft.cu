@@ -780,18 +780,34 @@ FFTPlanDev make_plan(lsd_ctx* ctx) {
   return pl;
 }
 
-// (E, G) pairs: P2 = 3 * 2^a or 9 * 2^a with the power of two split off up to 16
+// (E, G) pairs: P2 = 3 * 2^a or 9 * 2^a with the power of two split off up to 16 (the
+// default plan), and with one factor 2 moved to the column DFT (G = 8, the autotuner's
+// alternative for P2 = 48 .. 288)
 template <class F>
 int dispatch_EG(int E, int G, F&& f) {
 #define LSD_EG(e, g) if (E == e && G == g) return f(std::integral_constant<int, e>(), std::integral_constant<int, g>());
   LSD_EG(3, 1) LSD_EG(3, 2) LSD_EG(3, 4) LSD_EG(3, 8) LSD_EG(3, 16)
   LSD_EG(9, 1) LSD_EG(9, 2) LSD_EG(9, 4) LSD_EG(9, 8) LSD_EG(9, 16)
   LSD_EG(6, 16) LSD_EG(12, 16) LSD_EG(18, 16) LSD_EG(24, 16)
+  LSD_EG(6, 8) LSD_EG(12, 8) LSD_EG(18, 8) LSD_EG(24, 8) LSD_EG(36, 8)
 #undef LSD_EG
   return -1;
 }
 
 }  // namespace
+
+bool lsd_fft_compiled(int E, int G) { return dispatch_EG(E, G, [](auto, auto) { return 0; }) == 0; }
+
+// shared memory of the products kernel with the plan (E, G) for nfields staged rows
+size_t lsd_products_smem_for(int nfields, int P2, int E, int G, int NM) {
+  return sizeof(double2) * ((size_t)nfields * 2 * E * (G + 1)) + fft_tab_bytes(P2, E, G, NM);
+}
+size_t lsd_products_smem_eg(const lsd_ctx* ctx, int E, int G) {
+  const bool comp = ctx->cfg.comp_tstep != 0;
+  int nf = comp ? 18 : 15;
+  if (!ctx->cfg.boussinesq) nf = (comp ? 18 : 15) + 2;
+  return lsd_products_smem_for(nf, ctx->P2, E, G, ctx->NM);
+}
 
 // P2 = E G with G the power-of-two part of P2 capped at 16; (E, G) must be instantiated.
 bool lsd_fft_plan(lsd_ctx* c) {
@@ -902,13 +918,7 @@ int lsd_launch_qv(lsd_ctx* ctx, const cplx* th, const cplx* ph, cplx* qv1, cplx*
   return LSD_OK;
 }
 
-size_t lsd_products_smem(const lsd_ctx* ctx) {
-  const bool comp = ctx->cfg.comp_tstep != 0;
-  int nf = comp ? 18 : 15;
-  if (!ctx->cfg.boussinesq) nf = (comp ? 18 : 15) + 2;
-  return sizeof(double2) * ((size_t)nf * 2 * ctx->fftE * (ctx->fftG + 1)) +
-         fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
-}
+size_t lsd_products_smem(const lsd_ctx* ctx) { return lsd_products_smem_eg(ctx, ctx->fftE, ctx->fftG); }
 
 // four_in: the synthesised fields in the FFT layout, slots u 0-2, curl u 3-5, B 6-8,
 // curl B 9-11, grad C 12-14, grad Comp 15-17 (composition), then (anelastic) dr u_r,

@@ -739,6 +739,7 @@ struct OzState {
   int* d_err = nullptr;
   size_t smem = 0;
   int nst = 2;           // GEMM ring stages
+  int ctas = 2;          // persistent GEMM CTAs per SM
   int srow[2] = {1, 1};  // pre-pass stage row length (odd, in complex): synthesis, analysis
 };
 
@@ -825,7 +826,7 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
     abytes_max = std::max(abytes_max, abytes);
   }
   // ring stages: as many (2..4) as keep two CTAs per SM (<= 78 KiB of stages each)
-  o->nst = std::max(2, std::min(OZ_MAXSTAGES, 79872 / (S * 5120)));
+  lsd_ozaki_default_tiles(S, &o->nst, &o->ctas);
   o->smem = (size_t)o->nst * S * 5120 + sizeof(double) * 128 * OZ_STG;
   {
     int mx = 1;
@@ -913,7 +914,7 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->dev);
   const int ntile = ctx->NM * 2 * nzb;
-  k_oz_gemm<TYPE><<<std::min(ntile, 2 * nsm), OZ_THREADS, o->smem, ctx->stream>>>(ga, nzb);
+  k_oz_gemm<TYPE><<<std::min(ntile, o->ctas * nsm), OZ_THREADS, o->smem, ctx->stream>>>(ga, nzb);
   ctx->launches += 2;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("tensor-core contraction: ") + cudaGetErrorString(e));
@@ -980,6 +981,40 @@ int lsd_ozaki_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
 }
 
 int* lsd_ozaki_err_flag(lsd_ctx* ctx) { return ((OzState*)ctx->oz)->d_err; }
+
+// The GEMM's tunable tiles: ring stages and CTAs per SM.  A pair is valid when the
+// stages and the epilogue's staging fit the shared memory of that many CTAs per SM
+// (228 KB per SM, 1 KB reserved per CTA) and leave room for the 256 (ctas = 2) or 512
+// tensor-memory columns.
+bool lsd_ozaki_tiles_ok(int S, int nst, int ctas) {
+  if (nst < 2 || nst > OZ_MAXSTAGES || (ctas != 1 && ctas != 2) || S < 2 || S > OZ_MAXS) return false;
+  const size_t smem = (size_t)nst * S * 5120 + sizeof(double) * 128 * OZ_STG + 4096;  // + static
+  return smem * ctas <= (size_t)228 * 1024 - 1024 * ctas;
+}
+int lsd_ozaki_default_stages(int S) { return std::max(2, std::min(OZ_MAXSTAGES, 79872 / (S * 5120))); }
+// the default tiles: as many stages (2..4) as leave two CTAs per SM, one CTA per SM when
+// even two stages do not (S = 8), so that the persistent grid is all resident
+void lsd_ozaki_default_tiles(int S, int* nst, int* ctas) {
+  *nst = lsd_ozaki_default_stages(S);
+  *ctas = lsd_ozaki_tiles_ok(S, *nst, 2) ? 2 : 1;
+}
+void lsd_ozaki_get_tiles(const lsd_ctx* ctx, int* nst, int* ctas) {
+  const OzState* o = (const OzState*)ctx->oz;
+  *nst = o ? o->nst : 0;
+  *ctas = o ? o->ctas : 0;
+}
+int lsd_ozaki_set_tiles(lsd_ctx* ctx, int nst, int ctas) {
+  OzState* o = (OzState*)ctx->oz;
+  if (!o) return LSD_OK;
+  if (!lsd_ozaki_tiles_ok(o->S, nst, ctas)) return lsd_fail(ctx, LSD_EARG, "tensor-core GEMM tiles: invalid stages / CTAs");
+  o->nst = nst;
+  o->ctas = ctas;
+  o->smem = (size_t)o->nst * o->S * 5120 + sizeof(double) * 128 * OZ_STG;
+  oz_set_smem<OZ_VEC>(o->smem); oz_set_smem<OZ_P>(o->smem); oz_set_smem<OZ_GRAD>(o->smem);
+  oz_set_smem<OZ_ST>(o->smem); oz_set_smem<OZ_Q>(o->smem);
+  CUDA_TRY(cudaGetLastError());
+  return LSD_OK;
+}
 
 int lsd_ozaki_check(lsd_ctx* ctx) {
   OzState* o = (OzState*)ctx->oz;

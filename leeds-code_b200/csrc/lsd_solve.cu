@@ -1026,15 +1026,19 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
 }
 
 namespace {
+// threads per CTA: ctx->solve_threads (a multiple of 32, at most SOLVE_THREADS; the
+// autotuner's choice); one thread per harmonic whatever the CTA size, so the results and
+// the per-warp corrector partials do not depend on it
 template <int KL>
 void launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
-  dim3 g(ceil_div(ctx->H, SOLVE_THREADS), J_NJOB);
-  if (corr) k_corrector<KL><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a);
-  else k_predictor<KL><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a);
+  const int T = ctx->solve_threads;
+  dim3 g(ceil_div(ctx->H, T), J_NJOB);
+  if (corr) k_corrector<KL><<<g, T, 0, ctx->stream>>>(a);
+  else k_predictor<KL><<<g, T, 0, ctx->stream>>>(a);
   if (ctx->Nic > 1) {  // the field coupled to the inner core
-    dim3 gi(ceil_div(ctx->H, SOLVE_THREADS), 2);
-    if (corr) k_mag_ic<KL, true><<<gi, SOLVE_THREADS, 0, ctx->stream>>>(a);
-    else k_mag_ic<KL, false><<<gi, SOLVE_THREADS, 0, ctx->stream>>>(a);
+    dim3 gi(ceil_div(ctx->H, T), 2);
+    if (corr) k_mag_ic<KL, true><<<gi, T, 0, ctx->stream>>>(a);
+    else k_mag_ic<KL, false><<<gi, T, 0, ctx->stream>>>(a);
     ctx->launches++;
   }
 }
@@ -1837,13 +1841,14 @@ int lsd_operator_solve(lsd_ctx* ctx, int nfield, const int* fields, double* d_da
       return lsd_fail(ctx, LSD_EARG, "lsd_operator_solve_device: the field's operators are coupled to the inner core (Nic > 1)");
     a.field[i] = f;
   }
-  const dim3 g(ceil_div(ctx->H, SOLVE_THREADS), nfield);
+  const int T = ctx->solve_threads;
+  const dim3 g(ceil_div(ctx->H, T), nfield);
   switch (ctx->KL) {
-    case 2: k_opsolve<2><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
-    case 3: k_opsolve<3><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
-    case 4: k_opsolve<4><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
-    case 5: k_opsolve<5><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
-    case 6: k_opsolve<6><<<g, SOLVE_THREADS, 0, ctx->stream>>>(a); break;
+    case 2: k_opsolve<2><<<g, T, 0, ctx->stream>>>(a); break;
+    case 3: k_opsolve<3><<<g, T, 0, ctx->stream>>>(a); break;
+    case 4: k_opsolve<4><<<g, T, 0, ctx->stream>>>(a); break;
+    case 5: k_opsolve<5><<<g, T, 0, ctx->stream>>>(a); break;
+    case 6: k_opsolve<6><<<g, T, 0, ctx->stream>>>(a); break;
     default: return lsd_fail(ctx, LSD_EARG, "stencil half-width KL must be 2..6");
   }
   ctx->launches++;

@@ -94,6 +94,10 @@ def load_library(path=None):
         "lsd_operator_solve_device": [_V, ctypes.c_int, _I, _V],
         "lsd_get_stream": [_V, ctypes.POINTER(_V)],
         "lsd_ensemble_last_elapsed_ms": [_V, _D],
+        "lsd_tune_candidates": [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdTuneSpace)],
+        "lsd_tune_choose": [ctypes.c_int, _D, ctypes.c_int],
+        "lsd_get_tuning": [_V, ctypes.POINTER(capi.LsdTuning)],
+        "lsd_set_tuning": [_V, ctypes.POINTER(capi.LsdTuning)],
         "lsd_tim_check_cgce": [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState)],
         "lsd_tim_new_tstep": [ctypes.POINTER(capi.LsdConfig), ctypes.POINTER(capi.LsdPcState), _I],
     }
@@ -107,6 +111,23 @@ def load_library(path=None):
     lib.lsd_ensemble_last_error.argtypes = [_V]
     _LIB = lib
     return lib
+
+
+def tune_candidates(cfg):
+    """lsd_tune_candidates: the autotuner's candidate lists for cfg (no device work)"""
+    sp = capi.LsdTuneSpace()
+    rc = load_library().lsd_tune_candidates(ctypes.byref(cfg), ctypes.byref(sp))
+    if rc:
+        raise LsdError(rc, "lsd_tune_candidates")
+    return {"fft": [(sp.fft_E[i], sp.fft_G[i]) for i in range(sp.nfft)],
+            "gemm": [(sp.gemm_stages[i], sp.gemm_ctas[i]) for i in range(sp.ngemm)],
+            "solve_threads": [sp.solve_threads[i] for i in range(sp.nsolve)]}
+
+
+def tune_choose(ms, dflt=0):
+    """lsd_tune_choose: the selection rule on candidate timings ms"""
+    a = (ctypes.c_double * len(ms))(*ms)
+    return load_library().lsd_tune_choose(len(ms), a, int(dflt))
 
 
 def tim_check_cgce(cfg, state):
@@ -384,6 +405,20 @@ class Context:
 
     def banded_solve_device(self, n, kl, nmat, d_ab, d_ipiv, nrhs, d_map, d_b):
         self._ok(self.lib.lsd_banded_solve_device(self.h, n, kl, nmat, _V(d_ab), _V(d_ipiv), nrhs, _V(d_map), _V(d_b)))
+
+    def tuning(self):
+        """the context's launch parameters (lsd_get_tuning) as a dict"""
+        t = capi.LsdTuning()
+        self._ok(self.lib.lsd_get_tuning(self.h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in capi.LsdTuning._fields_ if k != "reserved"}
+
+    def set_tuning(self, **kw):
+        """change launch parameters (lsd_set_tuning); unspecified ones keep their values"""
+        t = capi.LsdTuning()
+        self._ok(self.lib.lsd_get_tuning(self.h, ctypes.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, v)
+        self._ok(self.lib.lsd_set_tuning(self.h, ctypes.byref(t)))
 
     def stream(self):
         """the context's CUDA stream handle (int), e.g. for torch.cuda.ExternalStream"""

@@ -14,15 +14,16 @@ Tolerances, relative to the largest magnitude of the compared field:
   FP64            synthesis, analysis, round trip vs the oracle's: 1e-12
   tensor, S = 8   1e-13
   tensor, S = 7   5e-12
+  tensor, S = 5   2e-8    (38 bits)
   tensor, S = 4   1e-6    (30 bits, about FP32)
 config[2]: batched banded solves at N = 257, KL = 4.
   * On the context's own Crank-Nicolson operators at L = M = 256 (dt = 2e-6, E = 3e-4,
     Pm = 3, implicit 0.6; lsd_operator_solve_device): every (l, m) right-hand side of the
     codensity, the toroidal velocity, the field's toroidal and poloidal scalars and the
     poloidal velocity's fourth-order composite (5 x 32896 complex columns) in one launch,
-    against the oracle's tim_invX / composite on the same right-hand sides (1e-13 of each
-    field's largest solution value), and the residual |A x - b| / |b| of the second-order
-    families from the LAPACK factors (<= 1e-13, a sample of degrees).
+    against the oracle's tim_invX / composite on the same right-hand sides, and the
+    backward error of the second-order families from the LAPACK factors (tolerances in
+    test_operator_solves_n257).
   * On random band matrices (lsd_banded_*_device): one operator per degree l < 256 for
     4 fields, every (l, m) right-hand side (Re and Im columns, 4 x 32896 x 2), residual
     |A x - b| / |b| <= 1e-13 on a sample checked on the host.
@@ -68,7 +69,8 @@ def relerr(a, b):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec,S,tol", [(capi.PREC_FP64, 0, 1e-12), (capi.PREC_OZAKI, 8, 1e-13),
-                                        (capi.PREC_OZAKI, 7, 5e-12), (capi.PREC_OZAKI, 4, 1e-6)])
+                                        (capi.PREC_OZAKI, 7, 5e-12), (capi.PREC_OZAKI, 5, 2e-8),
+                                        (capi.PREC_OZAKI, 4, 1e-6)])
 def test_sht_round_trip_lmax255(sht256_reference, prec, S, tol):
     import torch
     re, im, p0, a0 = sht256_reference
@@ -188,8 +190,25 @@ SOLVE257_FIELDS = (capi.COD_C, capi.VEL_TOR, capi.MAG_TOR, capi.MAG_POL, capi.VE
 LU_INDEX = {capi.VEL_TOR: 0, capi.COD_C: 3, capi.MAG_TOR: 4, capi.MAG_POL: 5}
 
 
+def masked_err(a, b, keep):
+    """max |a - b| over the complex coefficients of the harmonics `keep` ((H, N) arrays),
+    relative to the largest |b| there"""
+    d = np.hypot(a[0] - b[0], a[1] - b[1])[keep]
+    return float(d.max() / max(np.hypot(b[0], b[1])[keep].max(), 1e-300))
+
+
 @pytest.mark.gpu
 def test_operator_solves_n257(parity_report):
+    """The five operator families at N = 257, KL = 4 on every (l, m) column.
+    Forward error against the oracle's tim_invX / composite over the solved columns
+    (l = 0 only for the codensity), bounded by max(1e-13, 4 x the oracle's own change when
+    the right-hand sides are perturbed in the last bit): the Chebyshev grid's wall rows
+    (1/dr^2 ~ 7e8 against the O(1) boundary rows) make the operators badly scaled for
+    right-hand sides that are random in every row, and the codensity's wall values move by
+    6e-11 of its largest solution value under such a perturbation.  Backward error of the
+    second-order families from the oracle's LAPACK factors, |A x - b| / (|A| |x| + |b|)
+    (infinity norms, per column, a sample of degrees): <= 1e-15.  The unsolved l = 0
+    columns (tim_invX skips them) equal the right-hand side with zeroed boundary rows."""
     import torch
     syn = pkg.synthetic
     cfg = syn.config_solve257()
@@ -204,29 +223,47 @@ def test_operator_solves_n257(parity_report):
     g.synchronize()
     ms = (time.perf_counter() - t0) * 1e3
     x = d.cpu().numpy()
+    del d
     print("operator solves: %d fields x %d (l, m) columns, N = %d, KL = 4: %.2f ms (host-timed)" % (nf, H, N, ms))
+    rng = np.random.default_rng(3)
     for k, f in enumerate(SOLVE257_FIELDS):
-        xr, xi = o.operator_solve(f, re[k].T, im[k].T)  # (H, N)
-        gr, gi = x[k, :, :, 0].T, x[k, :, :, 1].T
-        err = np.hypot(gr - xr, gi - xi).max() / np.hypot(xr, xi).max()
-        parity_report("solve257 field %d: device vs oracle solve" % f, err, 1e-13)
-        assert err <= 1e-13, (f, err)
+        zero = f in (capi.COD_C, capi.COMP_C)
+        keep = np.ones(H, bool) if zero else l > 0
+        xo = o.operator_solve(f, re[k].T, im[k].T)  # (H, N)
+        xg = (x[k, :, :, 0].T, x[k, :, :, 1].T)
+        sens = 0.0
+        for _ in range(2):
+            pr = re[k] * (1.0 + 1e-16 * rng.standard_normal(re[k].shape))
+            pi = im[k] * (1.0 + 1e-16 * rng.standard_normal(im[k].shape))
+            sens = max(sens, masked_err(o.operator_solve(f, pr.T, pi.T), xo, keep))
+        err = masked_err(xg, xo, keep)
+        tol = max(1e-13, 4.0 * sens)
+        parity_report("solve257 field %d: device vs oracle (solved columns)" % f, err, tol)
+        parity_report("solve257 field %d: oracle vs last-bit perturbed right-hand sides" % f, sens)
+        assert err <= tol, (f, err, sens)
+        if not zero:  # l = 0: not solved, the right-hand side with zero boundary rows
+            c0 = np.nonzero(l == 0)[0]
+            for part, b in ((0, re[k]), (1, im[k])):
+                want = b[:, c0].T.copy()
+                want[:, [0, -1]] = 0.0
+                assert np.array_equal(xg[part][c0], want), f
         if f not in LU_INDEX:
             continue
         worst = 0.0
-        for deg in (1, 2, 17, 128, 255) + ((0,) if f == capi.COD_C else ()):
+        for deg in (1, 2, 17, 128, 255) + ((0,) if zero else ()):
             cols = np.nonzero(l == deg)[0]
             ab, ipiv = o.operator_lu(LU_INDEX[f], deg)
+            Anorm = np.abs(lu_apply(ab, ipiv, 4, np.eye(N))).sum(axis=1).max()
             for part in (0, 1):
-                xs = x[k, :, cols, part].T  # (N, ncols)
+                xs = xg[part][cols].T  # (N, ncols)
                 bs = (re if part == 0 else im)[k][:, cols].copy()
                 bs[0], bs[-1] = 0.0, 0.0  # tim_zerobc
-                res = lu_apply(ab, ipiv, 4, xs) - bs
-                nb = np.abs(bs).max(axis=0)
-                ok = nb > 0
+                res = np.abs(lu_apply(ab, ipiv, 4, xs) - bs).max(axis=0)
+                den = Anorm * np.abs(xs).max(axis=0) + np.abs(bs).max(axis=0)
+                ok = den > 0
                 if ok.any():
-                    worst = max(worst, float((np.abs(res).max(axis=0)[ok] / nb[ok]).max()))
-        parity_report("solve257 field %d: residual |A x - b| / |b|" % f, worst, 1e-13)
-        assert worst <= 1e-13, (f, worst)
+                    worst = max(worst, float((res[ok] / den[ok]).max()))
+        parity_report("solve257 field %d: backward error |A x - b| / (|A| |x| + |b|)" % f, worst, 1e-15)
+        assert worst <= 1e-15, (f, worst)
     g.close()
     o.close()
