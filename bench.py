@@ -144,11 +144,12 @@ def workload(name, precision):
     capi = pkg.capi
     prec = capi.PREC_OZAKI if precision == "ozaki" else capi.PREC_FP64
     slices = getattr(workload, "slices", 0)
+    tune = getattr(workload, "autotune", 1)
     if name == "parity32":
-        cfg = syn.config_parity(precision=prec, ozaki_slices=slices)
+        cfg = syn.config_parity(precision=prec, ozaki_slices=slices, autotune=tune)
         desc = "Boussinesq MHD shell L=M=32 (lmax=31), Nr=33, Th=48, Ph=96, dt=1e-5"
     else:
-        cfg = syn.config_dynamo128(precision=prec, ozaki_slices=slices)
+        cfg = syn.config_dynamo128(precision=prec, ozaki_slices=slices, autotune=tune)
         desc = "Boussinesq MHD dynamo step lmax=mmax=127 (L=M=128), Nr=129, Th=192, Ph=384, dt=2e-6"
     return cfg, desc
 
@@ -806,6 +807,7 @@ def run_ours(args, rank, world, local_rank, dist):
         res["phases_ms"] = ph
         res["roofline"] = rf
         res["sizes"] = ctx.sizes
+        res["tune"] = ctx.tuning()
         results[prec] = res
         ctx.close()
     if rank != 0:
@@ -841,6 +843,7 @@ def run_ours(args, rank, world, local_rank, dist):
         "evaluations_per_step": evals_per_step,
         "phases_ms": ph,
         "energies_after": {k: r["energies"][k] for k in ("KE", "ME")},
+        "tune": r["tune"],
     }
     tr = NCU_TRAFFIC.get(r["roofline"]["kernel"]) if args.workload == "dynamo128" else None
     line["roofline"]["traffic"] = tr["bytes"] if tr else None
@@ -894,6 +897,8 @@ def main():
     ap.add_argument("--workload", default="dynamo128",
                     choices=["dynamo128", "parity32", "sht256", "solve257", "ensemble"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default launch parameters instead of the ones lsd_create times (cfg.autotune)")
     # 5 slices: the fewest whose 1000-step energy error (energy_check, reported on every run)
     # stays well inside the metric's 1e-9 (measured 6.0e-12; 6 slices: 6.1e-13, 4: above)
     ap.add_argument("--slices", type=int, default=5,
@@ -902,6 +907,7 @@ def main():
                     help="steps of the FP64 vs tensor-core energy comparison (0: skip)")
     args = ap.parse_args()
     workload.slices = args.slices
+    workload.autotune = 0 if args.no_autotune else 1
     args.warmup = max(3, args.warmup) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
