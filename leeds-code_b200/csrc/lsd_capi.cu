@@ -702,7 +702,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   }
   TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * ctx->HB * NM * 4));
   TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
-  TRY(dalloc(ctx, &ctx->d_cpart, (size_t)8 * ((H + 31) / 32)));
+  TRY(dalloc(ctx, &ctx->d_cpart, (size_t)8 * ((2 * H + 31) / 32)));
   TRY(dalloc(ctx, &ctx->d_cfl, (size_t)2 * N + 1));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));
   // pinned staging: three spectral fields, and at least the host staging of the energy
