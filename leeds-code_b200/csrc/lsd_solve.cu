@@ -331,9 +331,10 @@ __device__ __forceinline__ void stream_forward(const Band& B, int N, IN&& in, OU
 // dtbsv (upper, non-unit, bandwidth 2KL; LAPACK column order) on the forward result:
 // for c = N-1..0: x(c) = y(c) / U(c, c); x(c-t) -= x(c) U(c-t, c), t <= 2KL.
 // in(n) supplies y rows in decreasing n; out(c, x) receives x(c) in decreasing c.
-constexpr int SPB = 4;  // rows per batch of the back substitution
-template <int KL, class IN, class OUT>
+constexpr int SPB = 4;  // rows per batch of the back substitution (default)
+template <int KL, int NBB = SPB, class IN, class OUT>
 __device__ __forceinline__ void stream_backward(const Band& B, int N, IN&& in, OUT&& out) {
+  constexpr int SPB = NBB;
   using V = decltype(in(0));
   constexpr int K2 = 2 * KL;
   V w[K2 + 1];  // w[t] = pending y(c - t)
@@ -657,7 +658,14 @@ __device__ __forceinline__ void forward_gen(const Band& B, int N, GEN& gen, OUT&
 }
 
 // the job of grid row y: POL kernels take the poloidal velocity alone, the others the
-// remaining fields (two kernels, so that each holds only its own path's registers)
+// remaining fields (two kernels, so that each holds only its own path's registers).  The
+// poloidal velocity's chain is the longest (two solves per column) and its kernel has
+// the fewest threads: it runs beside the other kernel (a stream of its own, forked and
+// joined) with 8-row batches and the whole register file; the other kernel, with five
+// times the threads, uses 4-row batches at four CTAs per SM.
+template <bool POL> struct SolveBatch {
+  static constexpr int fwd = POL ? 8 : SPF_FUSED, bwd = POL ? 8 : SPB, ctas = POL ? 1 : 4;
+};
 __device__ __forceinline__ int solve_job(bool pol, int y) {
   return pol ? J_VPOL : (y == 0 ? J_VTOR : y == 1 ? J_COD : y == 2 ? J_MTOR : y == 3 ? J_MPOL : J_COMP);
 }
@@ -666,7 +674,7 @@ constexpr int SOLVE_JOBS_OTHER = J_NJOB - 1;
 // Predictor (velocity.F90:369-395, codensity.F90:224-234, magnetic.F90:370-408).
 // grid (ceil(2 H / threads), 1) for POL, (ceil(2 H / threads), SOLVE_JOBS_OTHER) otherwise.
 template <int KL, bool POL>
-__global__ void __launch_bounds__(SOLVE_THREADS, 4) k_predictor(StepArgs a) {
+__global__ void __launch_bounds__(SOLVE_THREADS, SolveBatch<POL>::ctas) k_predictor(StepArgs a) {
   const int job = solve_job(POL, blockIdx.y);
   if (job == J_COMP && !a.comp) return;
   if ((job == J_MTOR || job == J_MPOL) && a.Nic > 1) return;  // k_mag_ic
@@ -702,13 +710,13 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 4) k_predictor(StepArgs a) {
       }
       return;
     }
-    RhsGen<KL, false, false, true> g1{nullptr, L, nullptr, v.Nn, v.S, rst, N, 0.0, 0.0, 0.0, {}};
+    RhsGen<KL, false, false, true, SolveBatch<POL>::fwd> g1{nullptr, L, nullptr, v.Nn, v.S, rst, N, 0.0, 0.0, 0.0, {}};
     forward_gen<KL>(v.B2, N, g1, w1);
-    stream_backward<KL>(v.B2, N, r1, [&](int c, double x) { v.W2[(size_t)c * rst] = x; });
-    RhsGen<KL, true, false, false> g2{v.y1, L, v.X, v.W2, nullptr, rst, N, 0.0, 0.0, 0.0, {}};
+    stream_backward<KL, SolveBatch<POL>::bwd>(v.B2, N, r1, [&](int c, double x) { v.W2[(size_t)c * rst] = x; });
+    RhsGen<KL, true, false, false, SolveBatch<POL>::fwd> g2{v.y1, L, v.X, v.W2, nullptr, rst, N, 0.0, 0.0, 0.0, {}};
     forward_gen<KL>(v.B1, N, g2, w1);
     double x0 = 0.0, xN = 0.0;
-    stream_backward<KL>(v.B1, N, r1, [&](int c, double x) {
+    stream_backward<KL, SolveBatch<POL>::bwd>(v.B1, N, r1, [&](int c, double x) {
       v.W2[(size_t)c * rst] = x;
       if (c == N - 1) xN = x;
       if (c == 0) x0 = x;
@@ -729,9 +737,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 4) k_predictor(StepArgs a) {
     }
     return;
   }
-  RhsGen<KL, true, false, true> g{v.y1, L, v.X, v.Nn, v.S, rst, N, 0.0, bc0, bcN, {}};
+  RhsGen<KL, true, false, true, SolveBatch<POL>::fwd> g{v.y1, L, v.X, v.Nn, v.S, rst, N, 0.0, bc0, bcN, {}};
   forward_gen<KL>(v.B1, N, g, w1);
-  stream_backward<KL>(v.B1, N, r1, [&](int c, double x) { v.X[(size_t)c * rst] = x; });
+  stream_backward<KL, SolveBatch<POL>::bwd>(v.B1, N, r1, [&](int c, double x) { v.X[(size_t)c * rst] = x; });
   }
 }
 
@@ -760,7 +768,7 @@ __global__ void k_cgce_sums(const double* part, int nwarp, double* red) {
 // back substitution produces them (n decreasing), per warp by a fixed shuffle tree and
 // across warps by k_cgce_sums in a fixed order.  grid as k_predictor's.
 template <int KL, bool POL>
-__global__ void __launch_bounds__(SOLVE_THREADS, 4) k_corrector(StepArgs a) {
+__global__ void __launch_bounds__(SOLVE_THREADS, SolveBatch<POL>::ctas) k_corrector(StepArgs a) {
   const int job = solve_job(POL, blockIdx.y);
   if (job == J_COMP && !a.comp) return;
   if ((job == J_MTOR || job == J_MPOL) && a.Nic > 1) return;  // k_mag_ic
@@ -797,13 +805,13 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 4) k_corrector(StepArgs a) {
       if (l == 0) {
         unsolved(0.0);
       } else {
-        RhsGen<KL, false, true, true> g1{nullptr, L, nullptr, v.Nn, v.S, rst, N, c, 0.0, 0.0, {}};
+        RhsGen<KL, false, true, true, SolveBatch<POL>::fwd> g1{nullptr, L, nullptr, v.Nn, v.S, rst, N, c, 0.0, 0.0, {}};
         forward_gen<KL>(v.B2, N, g1, w1);
-        stream_backward<KL>(v.B2, N, r1, [&](int cc, double x) { v.W2[(size_t)cc * rst] = x; });
+        stream_backward<KL, SolveBatch<POL>::bwd>(v.B2, N, r1, [&](int cc, double x) { v.W2[(size_t)cc * rst] = x; });
         auto inD = [&](int n) { return (n == 0 || n == N - 1) ? 0.0 : v.W2[(size_t)n * rst]; };
         double xN = 0.0;
         stream_forward<KL>(v.B1, N, inD, w1);
-        stream_backward<KL>(v.B1, N, r1, [&](int cc, double x) {
+        stream_backward<KL, SolveBatch<POL>::bwd>(v.B1, N, r1, [&](int cc, double x) {
           v.W2[(size_t)cc * rst] = x;
           if (cc == N - 1) xN = x;
           if (cc == 0) x0 = x;
@@ -817,9 +825,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 4) k_corrector(StepArgs a) {
       }
     } else {
       if (l != 0 || zero) {
-        RhsGen<KL, false, true, true> g{nullptr, L, nullptr, v.Nn, v.S, rst, N, c, bc0, 0.0, {}};
+        RhsGen<KL, false, true, true, SolveBatch<POL>::fwd> g{nullptr, L, nullptr, v.Nn, v.S, rst, N, c, bc0, 0.0, {}};
         forward_gen<KL>(v.B1, N, g, w1);
-        stream_backward<KL>(v.B1, N, r1, [&](int cc, double x) { addcorr(cc, x); if (cc == 0) x0 = x; });
+        stream_backward<KL, SolveBatch<POL>::bwd>(v.B1, N, r1, [&](int cc, double x) { addcorr(cc, x); if (cc == 0) x0 = x; });
       } else {
         unsolved(bc0);
       }
@@ -1221,13 +1229,18 @@ template <int KL>
 void launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
   const int T = ctx->solve_threads;
   const dim3 gp(ceil_div(2 * ctx->H, T), 1), go(ceil_div(2 * ctx->H, T), SOLVE_JOBS_OTHER);  // a real column each
+  // the poloidal velocity's kernel on the auxiliary stream, beside the others
+  cudaEventRecord(ctx->ev_fork, ctx->stream);
+  cudaStreamWaitEvent(ctx->aux_stream, ctx->ev_fork, 0);
   if (corr) {
-    k_corrector<KL, true><<<gp, T, 0, ctx->stream>>>(a);
+    k_corrector<KL, true><<<gp, T, 0, ctx->aux_stream>>>(a);
     k_corrector<KL, false><<<go, T, 0, ctx->stream>>>(a);
   } else {
-    k_predictor<KL, true><<<gp, T, 0, ctx->stream>>>(a);
+    k_predictor<KL, true><<<gp, T, 0, ctx->aux_stream>>>(a);
     k_predictor<KL, false><<<go, T, 0, ctx->stream>>>(a);
   }
+  cudaEventRecord(ctx->ev_join, ctx->aux_stream);
+  cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
   ctx->launches++;
   if (ctx->Nic > 1) {  // the field coupled to the inner core
     dim3 gi(ceil_div(ctx->H, T), 2);
