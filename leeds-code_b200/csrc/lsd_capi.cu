@@ -54,7 +54,8 @@ void free_ctx(lsd_ctx* ctx) {
     if (ctx->ev_committed[k]) cudaEventDestroy(ctx->ev_committed[k]);
   }
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
-  if (ctx->aux_stream) { cudaStreamSynchronize(ctx->aux_stream); cudaStreamDestroy(ctx->aux_stream); }
+  for (cudaStream_t as : ctx->aux_stream)
+    if (as) { cudaStreamSynchronize(as); cudaStreamDestroy(as); }
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->stream && ctx->owns_stream) cudaStreamDestroy(ctx->stream);
@@ -561,7 +562,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   CTRY(cudaSetDevice(ctx->dev));
   CTRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   ctx->owns_stream = true;
-  CTRY(cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking));
+  for (cudaStream_t& as : ctx->aux_stream) CTRY(cudaStreamCreateWithFlags(&as, cudaStreamNonBlocking));
   CTRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
   CTRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   CTRY(cudaEventCreate(&ctx->ev0));

@@ -1225,22 +1225,30 @@ namespace {
 // threads per CTA: ctx->solve_threads (a multiple of 32, at most SOLVE_THREADS; the
 // autotuner's choice); one thread per harmonic whatever the CTA size, so the results and
 // the per-warp corrector partials do not depend on it
+// the auxiliary stream beside the stream work is queued on now (see lsd_ctx::aux_stream)
+cudaStream_t aux_for(const lsd_ctx* ctx) {
+  if (ctx->stream == ctx->cap_stream[0]) return ctx->aux_stream[1];
+  if (ctx->stream == ctx->cap_stream[1]) return ctx->aux_stream[2];
+  return ctx->aux_stream[0];
+}
+
 template <int KL>
-void launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
+int launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
   const int T = ctx->solve_threads;
   const dim3 gp(ceil_div(2 * ctx->H, T), 1), go(ceil_div(2 * ctx->H, T), SOLVE_JOBS_OTHER);  // a real column each
   // the poloidal velocity's kernel on the auxiliary stream, beside the others
-  cudaEventRecord(ctx->ev_fork, ctx->stream);
-  cudaStreamWaitEvent(ctx->aux_stream, ctx->ev_fork, 0);
+  const cudaStream_t aux = aux_for(ctx);
+  CUDA_TRY(cudaEventRecord(ctx->ev_fork, ctx->stream));
+  CUDA_TRY(cudaStreamWaitEvent(aux, ctx->ev_fork, 0));
   if (corr) {
-    k_corrector<KL, true><<<gp, T, 0, ctx->aux_stream>>>(a);
+    k_corrector<KL, true><<<gp, T, 0, aux>>>(a);
     k_corrector<KL, false><<<go, T, 0, ctx->stream>>>(a);
   } else {
-    k_predictor<KL, true><<<gp, T, 0, ctx->aux_stream>>>(a);
+    k_predictor<KL, true><<<gp, T, 0, aux>>>(a);
     k_predictor<KL, false><<<go, T, 0, ctx->stream>>>(a);
   }
-  cudaEventRecord(ctx->ev_join, ctx->aux_stream);
-  cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
+  CUDA_TRY(cudaEventRecord(ctx->ev_join, aux));
+  CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
   ctx->launches++;
   if (ctx->Nic > 1) {  // the field coupled to the inner core
     dim3 gi(ceil_div(ctx->H, T), 2);
@@ -1248,6 +1256,7 @@ void launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
     else k_mag_ic<KL, false><<<gi, T, 0, ctx->stream>>>(a);
     ctx->launches++;
   }
+  return LSD_OK;
 }
 
 // rot_predictor / rot_corrector before the solves (main.F90:136, 148)
@@ -1263,14 +1272,13 @@ void launch_rot(lsd_ctx* ctx, bool corr) {
 
 int launch_step_kernel(lsd_ctx* ctx, const StepArgs& a, bool corr) {
   switch (ctx->KL) {
-    case 2: launch_pred<2>(ctx, a, corr); break;
-    case 3: launch_pred<3>(ctx, a, corr); break;
-    case 4: launch_pred<4>(ctx, a, corr); break;
-    case 5: launch_pred<5>(ctx, a, corr); break;
-    case 6: launch_pred<6>(ctx, a, corr); break;
+    case 2: return launch_pred<2>(ctx, a, corr);
+    case 3: return launch_pred<3>(ctx, a, corr);
+    case 4: return launch_pred<4>(ctx, a, corr);
+    case 5: return launch_pred<5>(ctx, a, corr);
+    case 6: return launch_pred<6>(ctx, a, corr);
     default: return lsd_fail(ctx, LSD_EARG, "stencil half-width KL must be 2..6 for the step kernels");
   }
-  return LSD_OK;
 }
 }  // namespace
 
