@@ -69,9 +69,24 @@ int dalloc(lsd_ctx* ctx, T** p, size_t count) {
   return LSD_OK;
 }
 
+// Host-to-device copies that kernels on the context's stream read go on that stream: a
+// plain cudaMemcpy runs on the legacy default stream, which a non-blocking stream does not
+// wait for, and from pageable memory it returns once the data is staged, before its DMA
+// has landed.  cudaMemcpyAsync from pageable memory also stages before returning, so the
+// host buffer may be reused at once.
 template <class T>
 int upload(lsd_ctx* ctx, T* d, const std::vector<T>& h) {
-  CUDA_TRY(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, ctx->stream));
+  return LSD_OK;
+}
+int h2d(lsd_ctx* ctx, void* d, const void* h, size_t bytes) {
+  CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  return LSD_OK;
+}
+// device-to-host after the stream's work: queued on it, then waited for
+int d2h(lsd_ctx* ctx, void* h, const void* d, size_t bytes) {
+  CUDA_TRY(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return LSD_OK;
 }
 
@@ -676,11 +691,11 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
     TRY(upload(ctx, ctx->d_icref, ref));
     TRY(dalloc(ctx, &ctx->d_icyt, (size_t)2 * Ni * (2 * KL + 1) * L));
     TRY(dalloc(ctx, &ctx->d_icstate, (size_t)2 * Ni * H)); TRY(dalloc(ctx, &ctx->d_icsv, (size_t)2 * Ni * H));
-    CTRY(cudaMemset(ctx->d_icstate, 0, sizeof(cplx) * 2 * Ni * H));
-    CTRY(cudaMemset(ctx->d_icsv, 0, sizeof(cplx) * 2 * Ni * H));
+    CTRY(cudaMemsetAsync(ctx->d_icstate, 0, sizeof(cplx) * 2 * Ni * H, ctx->stream));
+    CTRY(cudaMemsetAsync(ctx->d_icsv, 0, sizeof(cplx) * 2 * Ni * H, ctx->stream));
   }
   TRY(dalloc(ctx, &ctx->d_rot, (size_t)ROT_NSLOT + 4 * ctx->HB));  // + the torque sums per half-row
-  CTRY(cudaMemset(ctx->d_rot, 0, sizeof(double) * (ROT_NSLOT + 4 * ctx->HB)));
+  CTRY(cudaMemsetAsync(ctx->d_rot, 0, sizeof(double) * (ROT_NSLOT + 4 * ctx->HB), ctx->stream));
   TRY(dalloc(ctx, &ctx->d_gwP0, Th));
   {  // rot_precompute (rotation.F90:20-33): 8 pi / 15 r_i^5, r_i = rratio / (1 - rratio)
     const double ri = c.rratio / (1.0 - c.rratio), r2 = ri * ri, r4 = r2 * r2;
@@ -693,9 +708,9 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   const size_t F = (size_t)N * H;
   TRY(dalloc(ctx, &ctx->d_state, LSD_NFIELD * F)); TRY(dalloc(ctx, &ctx->d_nl, LSD_NFIELD * F));
   TRY(dalloc(ctx, &ctx->d_sv, LSD_NFIELD * F));
-  CTRY(cudaMemset(ctx->d_state, 0, sizeof(cplx) * LSD_NFIELD * F));
-  CTRY(cudaMemset(ctx->d_nl, 0, sizeof(cplx) * LSD_NFIELD * F));
-  CTRY(cudaMemset(ctx->d_sv, 0, sizeof(cplx) * LSD_NFIELD * F));
+  CTRY(cudaMemsetAsync(ctx->d_state, 0, sizeof(cplx) * LSD_NFIELD * F, ctx->stream));
+  CTRY(cudaMemsetAsync(ctx->d_nl, 0, sizeof(cplx) * LSD_NFIELD * F, ctx->stream));
+  CTRY(cudaMemsetAsync(ctx->d_sv, 0, sizeof(cplx) * LSD_NFIELD * F, ctx->stream));
   // 12 solve work columns / evaluation slots + dC + dComp (+ dr q, dr s, dr t, anelastic)
   ctx->nspec = c.boussinesq ? 14 : 17;
   TRY(dalloc(ctx, &ctx->d_spec, (size_t)ctx->nspec * F));
@@ -719,7 +734,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   TRY(dalloc(ctx, &ctx->d_pc, 1));
   TRY(dalloc(ctx, &ctx->d_opfail, 1));
   CTRY(cudaMallocHost((void**)&ctx->h_pc, sizeof(PcDev)));
-  CTRY(cudaMemset(ctx->d_pc, 0, sizeof(PcDev)));
+  CTRY(cudaMemsetAsync(ctx->d_pc, 0, sizeof(PcDev), ctx->stream));
   TRY(lsd_build_tables(ctx));
   TRY(lsd_build_operators(ctx));
   if (c.precision == LSD_PREC_OZAKI) TRY(lsd_ozaki_setup(ctx));
@@ -1007,7 +1022,7 @@ int lsd_tra_spec2phys(lsd_ctx* ctx, const double* s_re, const double* s_im, doub
   if ((rc = lsd_launch_synth(ctx, &g, 1))) return rc;
   if ((rc = lsd_launch_c2r(ctx, ctx->d_four, ctx->d_phys, 1))) return rc;
   if ((rc = time_end(ctx))) return rc;
-  CUDA_TRY(cudaMemcpy(p, ctx->d_phys, sizeof(double) * phys_count(ctx), cudaMemcpyDeviceToHost));
+  if ((rc = d2h(ctx, p, ctx->d_phys, sizeof(double) * phys_count(ctx)))) return rc;
   return LSD_OK;
 }
 
@@ -1016,7 +1031,7 @@ int lsd_tra_phys2spec(lsd_ctx* ctx, const double* p, double* s_re, double* s_im)
   CUDA_TRY(cudaSetDevice(ctx->dev));
   int rc;
   if ((rc = ensure_phys(ctx, 3))) return rc;
-  CUDA_TRY(cudaMemcpy(ctx->d_phys, p, sizeof(double) * phys_count(ctx), cudaMemcpyHostToDevice));
+  if ((rc = h2d(ctx, ctx->d_phys, p, sizeof(double) * phys_count(ctx)))) return rc;
   AnalGroup g;
   g.kind = AK_SCALAR;
   g.in[0] = ctx->d_four; g.in[1] = g.in[2] = nullptr;
@@ -1044,9 +1059,9 @@ int lsd_tra_qst2rtp(lsd_ctx* ctx, const double* q_re, const double* q_im, const 
   if ((rc = lsd_launch_c2r(ctx, ctx->d_four, ctx->d_phys, 3))) return rc;
   if ((rc = time_end(ctx))) return rc;
   size_t P = phys_count(ctx);
-  CUDA_TRY(cudaMemcpy(r, ctx->d_phys, sizeof(double) * P, cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(th, ctx->d_phys + P, sizeof(double) * P, cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(ph, ctx->d_phys + 2 * P, sizeof(double) * P, cudaMemcpyDeviceToHost));
+  if ((rc = d2h(ctx, r, ctx->d_phys, sizeof(double) * P))) return rc;
+  if ((rc = d2h(ctx, th, ctx->d_phys + P, sizeof(double) * P))) return rc;
+  if ((rc = d2h(ctx, ph, ctx->d_phys + 2 * P, sizeof(double) * P))) return rc;
   return LSD_OK;
 }
 
@@ -1057,9 +1072,9 @@ int lsd_tra_rtp2qst(lsd_ctx* ctx, const double* r, const double* th, const doubl
   int rc;
   if ((rc = ensure_phys(ctx, 3))) return rc;
   size_t P = phys_count(ctx);
-  CUDA_TRY(cudaMemcpy(ctx->d_phys, r, sizeof(double) * P, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(ctx->d_phys + P, th, sizeof(double) * P, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(ctx->d_phys + 2 * P, ph, sizeof(double) * P, cudaMemcpyHostToDevice));
+  if ((rc = h2d(ctx, ctx->d_phys, r, sizeof(double) * P))) return rc;
+  if ((rc = h2d(ctx, ctx->d_phys + P, th, sizeof(double) * P))) return rc;
+  if ((rc = h2d(ctx, ctx->d_phys + 2 * P, ph, sizeof(double) * P))) return rc;
   const size_t F = (size_t)ctx->N * ctx->H, FF = (size_t)ctx->N * ctx->HB * ctx->NM * 4;
   AnalGroup g;
   g.kind = AK_VECTOR;
@@ -1088,8 +1103,8 @@ int lsd_tra_grad(lsd_ctx* ctx, const double* s_re, const double* s_im, double* t
   if ((rc = lsd_launch_c2r(ctx, ctx->d_four, ctx->d_phys, 2))) return rc;
   if ((rc = time_end(ctx))) return rc;
   size_t P = phys_count(ctx);
-  CUDA_TRY(cudaMemcpy(th, ctx->d_phys, sizeof(double) * P, cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(ph, ctx->d_phys + P, sizeof(double) * P, cudaMemcpyDeviceToHost));
+  if ((rc = d2h(ctx, th, ctx->d_phys, sizeof(double) * P))) return rc;
+  if ((rc = d2h(ctx, ph, ctx->d_phys + P, sizeof(double) * P))) return rc;
   return LSD_OK;
 }
 
@@ -1112,7 +1127,7 @@ int lsd_tra_dth(lsd_ctx* ctx, const double* s_re, const double* s_im, double* p)
   if (rc) return rc;
   if ((rc = lsd_launch_c2r(ctx, ctx->d_four, ctx->d_phys, 1))) return rc;
   if ((rc = time_end(ctx))) return rc;
-  CUDA_TRY(cudaMemcpy(p, ctx->d_phys, sizeof(double) * phys_count(ctx), cudaMemcpyDeviceToHost));
+  if ((rc = d2h(ctx, p, ctx->d_phys, sizeof(double) * phys_count(ctx)))) return rc;
   return LSD_OK;
 }
 
@@ -1151,7 +1166,8 @@ int lsd_tra_qst2rtp_vel(lsd_ctx* ctx, const double* q_re, const double* q_im, co
   if ((rc = lsd_launch_c2r(ctx, fo, ctx->d_phys, 8))) return rc;
   if ((rc = time_end(ctx))) return rc;
   size_t P = phys_count(ctx);
-  for (int k = 0; k < 8; ++k) CUDA_TRY(cudaMemcpy(out[k], ctx->d_phys + k * P, sizeof(double) * P, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 8; ++k)
+    if ((rc = d2h(ctx, out[k], ctx->d_phys + k * P, sizeof(double) * P))) return rc;
   return LSD_OK;
 }
 

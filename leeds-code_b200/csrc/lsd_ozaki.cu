@@ -92,10 +92,12 @@ int lsd_umma_selftest(lsd_ctx* ctx, double* maxerr) {
   CUDA_TRY(cudaMalloc(&dB, B.size()));
   CUDA_TRY(cudaMalloc(&dD, sizeof(int32_t) * 128 * 32));
   CUDA_TRY(cudaMalloc(&dErr, sizeof(int)));
-  CUDA_TRY(cudaMemcpy(dA, A.data(), A.size(), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(dB, B.data(), B.size(), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemset(dD, 0, sizeof(int32_t) * 128 * 32));
-  CUDA_TRY(cudaMemset(dErr, 0, sizeof(int)));
+  // on the context's stream, which the kernel below runs on (a plain cudaMemcpy from
+  // pageable memory may return before its DMA lands, and is not ordered with that stream)
+  CUDA_TRY(cudaMemcpyAsync(dA, A.data(), A.size(), cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(dB, B.data(), B.size(), cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(dD, 0, sizeof(int32_t) * 128 * 32, ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(dErr, 0, sizeof(int), ctx->stream));
   k_umma_selftest<<<1, 128, 0, ctx->stream>>>(dA, dB, dD, dErr);
   ctx->launches++;
   CUDA_TRY(cudaGetLastError());
@@ -839,11 +841,12 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
   if (kidx.empty()) kidx.push_back(0);
   if (nhl.empty()) nhl.push_back(0);
   CUDA_TRY(cudaMalloc(&o->d_probs, sizeof(OzProb) * probs.size()));
-  CUDA_TRY(cudaMemcpy(o->d_probs, probs.data(), sizeof(OzProb) * probs.size(), cudaMemcpyHostToDevice));
+  // uploads on the context's stream, which the table kernels below run on
+  CUDA_TRY(cudaMemcpyAsync(o->d_probs, probs.data(), sizeof(OzProb) * probs.size(), cudaMemcpyHostToDevice, ctx->stream));
   CUDA_TRY(cudaMalloc(&o->d_kidx, sizeof(int) * kidx.size()));
-  CUDA_TRY(cudaMemcpy(o->d_kidx, kidx.data(), sizeof(int) * kidx.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpyAsync(o->d_kidx, kidx.data(), sizeof(int) * kidx.size(), cudaMemcpyHostToDevice, ctx->stream));
   CUDA_TRY(cudaMalloc(&o->d_nh, sizeof(int) * nhl.size()));
-  CUDA_TRY(cudaMemcpy(o->d_nh, nhl.data(), sizeof(int) * nhl.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpyAsync(o->d_nh, nhl.data(), sizeof(int) * nhl.size(), cudaMemcpyHostToDevice, ctx->stream));
   CUDA_TRY(cudaMalloc(&o->d_B, std::max<long long>(bbytes, 16)));
   CUDA_TRY(cudaMalloc(&o->d_fexp, sizeof(int) * (size_t)std::max(fofs, 1)));
   CUDA_TRY(cudaMalloc(&o->d_A, std::max<long long>(abytes_max, 16)));
@@ -851,7 +854,7 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
   for (int type = 0; type < OZ_NTYPE; ++type) max_rows = std::max(max_rows, o->nzb_max[type] * 128);
   CUDA_TRY(cudaMalloc(&o->d_erow, sizeof(int) * (size_t)NM * max_rows));
   CUDA_TRY(cudaMalloc(&o->d_err, sizeof(int)));
-  CUDA_TRY(cudaMemset(o->d_err, 0, sizeof(int)));
+  CUDA_TRY(cudaMemsetAsync(o->d_err, 0, sizeof(int), ctx->stream));
   OzTabArgs ta;
   ta.leg = ctx->d_leg; ta.H = ctx->H; ta.Th2 = Th2; ta.S = S; ta.NM = NM;
   ta.probs = o->d_probs; ta.kidx = o->d_kidx; ta.nhlist = o->d_nh; ta.B = o->d_B; ta.fexp = o->d_fexp;
@@ -1019,7 +1022,8 @@ int lsd_ozaki_set_tiles(lsd_ctx* ctx, int nst, int ctas) {
 int lsd_ozaki_check(lsd_ctx* ctx) {
   OzState* o = (OzState*)ctx->oz;
   int err = 0;
-  CUDA_TRY(cudaMemcpy(&err, o->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpyAsync(&err, o->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   if (err) return lsd_fail(ctx, LSD_ECUDA, "tensor-core Legendre contraction: an mbarrier wait timed out");
   return LSD_OK;
 }

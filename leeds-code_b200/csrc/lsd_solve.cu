@@ -1766,8 +1766,9 @@ int lsd_diagnostics_device(lsd_ctx* ctx, double* sc, double* spec, double* prof)
     for (int k = 0; k < 8; ++k) sc[LSD_D_MICPART + k] = v8[k];
   }
   {  // rot_torque.dat
-    double rot[ROT_NSLOT];
-    CUDA_TRY(cudaMemcpy(rot, ctx->d_rot, sizeof(rot), cudaMemcpyDeviceToHost));
+    double rot[ROT_NSLOT];  // after the work queued on the context's stream
+    CUDA_TRY(cudaMemcpyAsync(rot, ctx->d_rot, sizeof(rot), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     sc[LSD_D_ROT + 0] = rot[ROT_OMEGA]; sc[LSD_D_ROT + 1] = rot[ROT_VEL]; sc[LSD_D_ROT + 2] = rot[ROT_MAG];
   }
   // ---- mag_cmb (io.F90:2036-2145): var_coll_norm_orig of q, s zeroed below the outer shell

@@ -144,7 +144,8 @@ int lsd_autotune(lsd_ctx* ctx) {
   const size_t Fi = (size_t)ctx->Nic * ctx->H;
   // keep the rotation slots; fill the state with the pattern
   std::vector<double> rot(ROT_NSLOT, 0.0);
-  CUDA_TRY(cudaMemcpy(rot.data(), ctx->d_rot, sizeof(double) * ROT_NSLOT, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpyAsync(rot.data(), ctx->d_rot, sizeof(double) * ROT_NSLOT, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   k_tune_fill<<<592, 256, 0, ctx->stream>>>((double*)ctx->d_state, 2 * nstate * F);
   CUDA_TRY(cudaGetLastError());
   const int reps = 3;
