@@ -83,12 +83,7 @@ int h2d(lsd_ctx* ctx, void* d, const void* h, size_t bytes) {
   CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
   return LSD_OK;
 }
-// device-to-host after the stream's work: queued on it, then waited for
-int d2h(lsd_ctx* ctx, void* h, const void* d, size_t bytes) {
-  CUDA_TRY(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  return LSD_OK;
-}
+
 
 // harmonic layout: _loop_setlm (parallel.h_template:54-80), _loop_sumth (:85-100)
 void build_layout(lsd_ctx* c) {
