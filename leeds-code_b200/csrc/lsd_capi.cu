@@ -54,10 +54,6 @@ void free_ctx(lsd_ctx* ctx) {
     if (ctx->ev_committed[k]) cudaEventDestroy(ctx->ev_committed[k]);
   }
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
-  for (cudaStream_t as : ctx->aux_stream)
-    if (as) { cudaStreamSynchronize(as); cudaStreamDestroy(as); }
-  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
-  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->stream && ctx->owns_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -572,9 +568,6 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   CTRY(cudaSetDevice(ctx->dev));
   CTRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   ctx->owns_stream = true;
-  for (cudaStream_t& as : ctx->aux_stream) CTRY(cudaStreamCreateWithFlags(&as, cudaStreamNonBlocking));
-  CTRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
-  CTRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   CTRY(cudaEventCreate(&ctx->ev0));
   CTRY(cudaEventCreate(&ctx->ev1));
   build_layout(ctx);
@@ -719,7 +712,7 @@ int lsd_create(const lsd_config* cfg, lsd_ctx** out) {
   }
   TRY(dalloc(ctx, &ctx->d_four, (size_t)ctx->nfour * N * ctx->HB * NM * 4));
   TRY(dalloc(ctx, &ctx->d_red, (size_t)128 + 48 * N));
-  TRY(dalloc(ctx, &ctx->d_cpart, (size_t)8 * ((2 * H + 31) / 32)));
+  TRY(dalloc(ctx, &ctx->d_cpart, (size_t)8 * ((H + 31) / 32)));
   TRY(dalloc(ctx, &ctx->d_cfl, (size_t)2 * N + 1));
   CTRY(cudaMallocHost((void**)&ctx->h_red, sizeof(double) * 64));
   // pinned staging: three spectral fields, and at least the host staging of the energy

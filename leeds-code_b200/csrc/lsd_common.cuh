@@ -192,13 +192,6 @@ struct lsd_ctx {
   cudaStream_t cap_stream[2] = {nullptr, nullptr};
   long long k_begin = 0, k_loop = 0, k_rebuild = 0, k_corr = 0;
   void* oz = nullptr;  // tensor-core path state (lsd_ozaki.cu)
-  // streams for work that runs beside the main stream's, forked from and joined to it
-  // with the two events (inside a graph capture: a fork and a join).  One per capture
-  // level -- [0] beside the context's stream, [1] beside cap_stream[0], [2] beside
-  // cap_stream[1] -- because a stream that joined a capture stays in it until that
-  // capture ends, and the corrector loop's body is captured inside the step loop's.
-  cudaStream_t aux_stream[3] = {nullptr, nullptr, nullptr};
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // tunables besides fftE / fftG and the GEMM tiles (lsd_tune.cu)
   int solve_threads = 128;
   lsd_tuning tuning{};

@@ -231,7 +231,7 @@ struct StepArgs {
   int comp;
   double* red;  // corrector: [8] sums of squares
   double* cpart;  // corrector: the per-warp sums [8][nwarp] that k_cgce_sums adds up
-  int nwarp;      // ceil(2 H / 32): warps of the predictor / corrector grid
+  int nwarp;      // ceil(H / 32)
   int NL;       // rows per operator in lus / ipivs (N + Nic - 1)
   int Nic;      // inner-core points (> 1: conducting, the field families are coupled)
   cplx* icstate;       // [2][Nic][H] mag_icTor, mag_icPol
@@ -246,7 +246,6 @@ enum SolveJob { J_VTOR = 0, J_VPOL, J_COD, J_MTOR, J_MPOL, J_COMP, J_NJOB };
 
 constexpr int SOLVE_THREADS = 128;
 constexpr int SPF = 8;  // right-hand-side rows fetched ahead, so that their loads overlap
-constexpr int SPF_FUSED = 4;  // rows per batch of the fused right-hand side (forward_gen)
 
 __device__ __forceinline__ int job_field(int job) {
   return job == J_VTOR ? LSD_VEL_TOR : job == J_VPOL ? LSD_VEL_POL : job == J_COD ? LSD_COD_C
@@ -270,31 +269,18 @@ __device__ __forceinline__ double2 axpy2(double2 y, double a, double2 x) {  // y
   return make_double2(y.x + a * x.x, y.y + a * x.y);
 }
 
-// value helpers for one complex column (double2) or one real column (double)
-__device__ __forceinline__ double2 axpyv(double2 y, double a, double2 x) { return axpy2(y, a, x); }
-__device__ __forceinline__ double axpyv(double y, double a, double x) { return y + a * x; }
-__device__ __forceinline__ double2 negv(double2 x) { return make_double2(-x.x, -x.y); }
-__device__ __forceinline__ double negv(double x) { return -x; }
-__device__ __forceinline__ double2 divv(double2 x, double d) { return make_double2(x.x / d, x.y / d); }
-__device__ __forceinline__ double divv(double x, double d) { return x / d; }
-template <class V> __device__ __forceinline__ V zerov();
-template <> __device__ __forceinline__ double2 zerov<double2>() { return make_double2(0.0, 0.0); }
-template <> __device__ __forceinline__ double zerov<double>() { return 0.0; }
-
 // dgbtrs forward part (LAPACK order): for c = 0..N-2 swap rows c and piv(c), then
 // x(c+i) -= L(c+i, c) x(c), i <= KL.  in(n) supplies right-hand-side rows in increasing
 // n (each once); out(c, y) receives the finished rows.  The right-hand-side rows and the
-// factors of a batch of SPF rows are loaded before its arithmetic.  Values: double2 (a
-// complex column) or double (one real column), as in() returns.
+// factors of a batch of SPF rows are loaded before its arithmetic.
 template <int KL, class IN, class OUT>
 __device__ __forceinline__ void stream_forward(const Band& B, int N, IN&& in, OUT&& out) {
-  using V = decltype(in(0));
   constexpr int KD = 2 * KL + 1;
-  V w[KL + 1];
+  double2 w[KL + 1];
 #pragma unroll
-  for (int i = 0; i <= KL; ++i) w[i] = i < N ? in(i) : zerov<V>();
+  for (int i = 0; i <= KL; ++i) w[i] = i < N ? in(i) : make_double2(0.0, 0.0);
   for (int c0 = 0; c0 < N; c0 += SPF) {
-    V buf[SPF];  // rows c0 + KL + 1 + u, requested in increasing order
+    double2 buf[SPF];  // rows c0 + KL + 1 + u, requested in increasing order
     int pv[SPF];
     double lf[SPF][KL];
 #pragma unroll
@@ -305,7 +291,7 @@ __device__ __forceinline__ void stream_forward(const Band& B, int N, IN&& in, OU
       for (int i = 0; i < KL; ++i) lf[u][i] = B.at(KD + i, c);
     }
 #pragma unroll
-    for (int u = 0; u < SPF; ++u) buf[u] = c0 + KL + 1 + u < N ? in(c0 + KL + 1 + u) : zerov<V>();
+    for (int u = 0; u < SPF; ++u) buf[u] = c0 + KL + 1 + u < N ? in(c0 + KL + 1 + u) : make_double2(0.0, 0.0);
 #pragma unroll
     for (int u = 0; u < SPF; ++u) {
       const int c = c0 + u;
@@ -314,11 +300,11 @@ __device__ __forceinline__ void stream_forward(const Band& B, int N, IN&& in, OU
         const int p = pv[u] - 1 - c;  // 0..KL
 #pragma unroll
         for (int i = 1; i <= KL; ++i)
-          if (p == i) { const V t = w[0]; w[0] = w[i]; w[i] = t; }
-        const V temp = negv(w[0]);
+          if (p == i) { const double2 t = w[0]; w[0] = w[i]; w[i] = t; }
+        const double2 temp = make_double2(-w[0].x, -w[0].y);
 #pragma unroll
         for (int i = 1; i <= KL; ++i)
-          if (c + i < N) w[i] = axpyv(w[i], lf[u][i - 1], temp);
+          if (c + i < N) w[i] = axpy2(w[i], lf[u][i - 1], temp);
       }
       out(c, w[0]);
 #pragma unroll
@@ -331,17 +317,15 @@ __device__ __forceinline__ void stream_forward(const Band& B, int N, IN&& in, OU
 // dtbsv (upper, non-unit, bandwidth 2KL; LAPACK column order) on the forward result:
 // for c = N-1..0: x(c) = y(c) / U(c, c); x(c-t) -= x(c) U(c-t, c), t <= 2KL.
 // in(n) supplies y rows in decreasing n; out(c, x) receives x(c) in decreasing c.
-constexpr int SPB = 4;  // rows per batch of the back substitution (default)
-template <int KL, int NBB = SPB, class IN, class OUT>
+constexpr int SPB = 8;  // rows per batch of the back substitution
+template <int KL, class IN, class OUT>
 __device__ __forceinline__ void stream_backward(const Band& B, int N, IN&& in, OUT&& out) {
-  constexpr int SPB = NBB;
-  using V = decltype(in(0));
   constexpr int K2 = 2 * KL;
-  V w[K2 + 1];  // w[t] = pending y(c - t)
+  double2 w[K2 + 1];  // w[t] = pending y(c - t)
 #pragma unroll
-  for (int t = 0; t <= K2; ++t) w[t] = N - 1 - t >= 0 ? in(N - 1 - t) : zerov<V>();
+  for (int t = 0; t <= K2; ++t) w[t] = N - 1 - t >= 0 ? in(N - 1 - t) : make_double2(0.0, 0.0);
   for (int c0 = N - 1; c0 >= 0; c0 -= SPB) {
-    V buf[SPB];  // rows c0 - K2 - 1 - u
+    double2 buf[SPB];  // rows c0 - K2 - 1 - u
     double uf[SPB][K2 + 1];
 #pragma unroll
     for (int u = 0; u < SPB; ++u) {
@@ -350,16 +334,17 @@ __device__ __forceinline__ void stream_backward(const Band& B, int N, IN&& in, O
       for (int t = 0; t <= K2; ++t) uf[u][t] = B.at(K2 - t, c);  // uf[u][0] = U(c, c)
     }
 #pragma unroll
-    for (int u = 0; u < SPB; ++u) buf[u] = c0 - K2 - 1 - u >= 0 ? in(c0 - K2 - 1 - u) : zerov<V>();
+    for (int u = 0; u < SPB; ++u) buf[u] = c0 - K2 - 1 - u >= 0 ? in(c0 - K2 - 1 - u) : make_double2(0.0, 0.0);
 #pragma unroll
     for (int u = 0; u < SPB; ++u) {
       const int c = c0 - u;
       if (c < 0) break;
-      const V xc = divv(w[0], uf[u][0]);
+      const double d = uf[u][0];
+      const double2 xc = make_double2(w[0].x / d, w[0].y / d);
       out(c, xc);
-      const V mx = negv(xc);
+      const double2 mx = make_double2(-xc.x, -xc.y);
 #pragma unroll
-      for (int t = 1; t <= K2; ++t) w[t] = axpyv(w[t], uf[u][t], mx);
+      for (int t = 1; t <= K2; ++t) w[t] = axpy2(w[t], uf[u][t], mx);
 #pragma unroll
       for (int t = 0; t < K2; ++t) w[t] = w[t + 1];
       w[K2] = buf[u];
@@ -486,209 +471,23 @@ __device__ __forceinline__ void diff_terms(const double2* Nn, double2* S, double
   }
 }
 
-// ---- the predictor and corrector solves, one real column per thread ---------------------
-// Thread t of a job row takes harmonic t / 2 and part t % 2 (0 = Re, 1 = Im): lanes 2i and
-// 2i + 1 read the two halves of one complex value (a warp covers 16 harmonics, 512
-// contiguous bytes of a row) and share the factors of their degree (one load, broadcast).
-// Twice the threads of one-harmonic-per-thread, half the registers of each.  The
-// right-hand side (tim_multY, tim_nlincorr, tim_zerobc) is formed inside the forward
-// elimination, batch by batch, and the save of the nonlinear terms rides along, so a
-// column makes one forward and one backward pass per solve.
-
-// one real column of a field: element n at p[n * rst], rst = 2 H doubles
-struct RView {
-  double *X, *S, *W1, *W2;
-  const double* Nn;
-  size_t rst;
-  Band B1, B2;       // main operator; Green's operator (poloidal velocity)
-  const double* y1;  // Y band of the main family
-  const double* g;   // Green's functions: element (n, k) at g[(n 2 + k) L]
-  double iG[4];
-};
-
-template <int KL>
-__device__ RView rview(const StepArgs& a, int job, int nh, int part, int l) {
-  const ColView c = col_view<KL>(a, job, nh, l);
-  RView v;
-  v.X = (double*)c.X + part;
-  v.S = (double*)c.S + part;
-  v.W1 = (double*)c.W1 + part;
-  v.W2 = (double*)c.W2 + part;
-  v.Nn = (const double*)c.Nn + part;
-  v.rst = 2 * c.rst;
-  v.B1 = c.B1;
-  v.B2 = c.B2;
-  v.y1 = c.y1;
-  v.g = c.g;
-  for (int i = 0; i < 4; ++i) v.iG[i] = c.iG[i];
-  return v;
-}
-
-// The right-hand side of a forward elimination, SPF rows per batch (rows >= N are zero):
-// interior rows R(r) (MULTY: + (Y X)(r), tim_multY; DIFF: c (R(r) - S(r)), tim_nlincorr),
-// bc0 / bcN on the wall rows (tim_zerobc / the boundary values); SAVE: S(r) := R(r).
-// A batch issues every load (its X rows, R and S rows, Y band values) before its stores.
-template <int KL, bool MULTY, bool DIFF, bool SAVE, int NB = SPF_FUSED>
-struct RhsGen {
-  const double* y;  // Y band [n][2KL+1][L] at this degree (MULTY)
-  int L;
-  const double* X;  // the state column (MULTY)
-  const double* R;  // nonlinear terms, or the previous solve's result
-  double* S;        // saved nonlinear terms (DIFF reads the old ones, SAVE writes the new)
-  size_t rst;
-  int N;
-  double c;         // d_implicit (DIFF)
-  double bc0, bcN;
-  double xw[2 * KL + NB];  // X rows r0 - KL .. r0 + NB - 1 + KL (MULTY)
-  static constexpr int nb = NB;
-
-  __device__ __forceinline__ void batch(int r0, bool first, double* v) {
-    constexpr int LDM = 2 * KL + 1, SPF = NB;
-    double nv[SPF], sv[SPF];
-    double yb[MULTY ? SPF : 1][LDM];
-    if constexpr (MULTY) {
-      if (first) {
-#pragma unroll
-        for (int t = 0; t < 2 * KL; ++t) {
-          const int j = t - KL;
-          xw[t] = (j >= 0 && j < N) ? X[(size_t)j * rst] : 0.0;
-        }
-      } else {
-#pragma unroll
-        for (int t = 0; t < 2 * KL; ++t) xw[t] = xw[t + SPF];
-      }
-#pragma unroll
-      for (int u = 0; u < SPF; ++u) {
-        const int j = r0 + KL + u;
-        xw[2 * KL + u] = j < N ? X[(size_t)j * rst] : 0.0;
-      }
-#pragma unroll
-      for (int u = 0; u < SPF; ++u) {
-        const int r = r0 + u;
-#pragma unroll
-        for (int t = 0; t < LDM; ++t) {
-          const int jj = r - KL + t;
-          yb[u][t] = (r < N && jj >= 0 && jj < N) ? __ldg(y + ((size_t)jj * LDM + (LDM - 1 - t)) * L) : 0.0;
-        }
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < SPF; ++u) {
-      const int r = r0 + u;
-      nv[u] = r < N ? R[(size_t)r * rst] : 0.0;
-      if constexpr (DIFF) sv[u] = r < N ? S[(size_t)r * rst] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < SPF; ++u) {
-      const int r = r0 + u;
-      double acc = DIFF ? c * (nv[u] - sv[u]) : nv[u];
-      if constexpr (MULTY) {
-#pragma unroll
-        for (int t = 0; t < LDM; ++t) acc = acc + yb[u][t] * xw[u + t];
-      }
-      v[u] = r == 0 ? bc0 : r == N - 1 ? bcN : r < N ? acc : 0.0;
-    }
-    if constexpr (SAVE) {
-#pragma unroll
-      for (int u = 0; u < SPF; ++u)
-        if (r0 + u < N) S[(size_t)(r0 + u) * rst] = nv[u];
-    }
-  }
-};
-
-// The forward part of dgbtrs (as stream_forward) fed by gen: right-hand-side row c + KL + 1
-// enters when column c is eliminated; batch b brings rows SPF b .. SPF b + SPF - 1 and
-// finishes columns SPF b - KL - 1 .. SPF b + SPF - KL - 2 (the factors of those columns
-// loaded with it).
-template <int KL, class GEN, class OUT>
-__device__ __forceinline__ void forward_gen(const Band& B, int N, GEN& gen, OUT&& out) {
-  constexpr int SPF = GEN::nb;
-  constexpr int KD = 2 * KL + 1;
-  double w[KL + 1], v[SPF], lf[SPF][KL];
-  int pv[SPF];
-  auto factors = [&](int r0) {
-#pragma unroll
-    for (int u = 0; u < SPF; ++u) {
-      const int c = min(max(r0 + u - KL - 1, 0), N - 1);
-      pv[u] = B.pivot(c);
-#pragma unroll
-      for (int i = 0; i < KL; ++i) lf[u][i] = B.at(KD + i, c);
-    }
-  };
-  auto step = [&](int c, int u) {  // eliminate column c, then row c + KL + 1 (v[u]) enters
-    if (c < N - 1) {
-      const int p = pv[u] - 1 - c;  // 0..KL
-#pragma unroll
-      for (int i = 1; i <= KL; ++i)
-        if (p == i) { const double t = w[0]; w[0] = w[i]; w[i] = t; }
-      const double temp = -w[0];
-#pragma unroll
-      for (int i = 1; i <= KL; ++i)
-        if (c + i < N) w[i] = w[i] + lf[u][i - 1] * temp;
-    }
-    out(c, w[0]);
-#pragma unroll
-    for (int i = 0; i < KL; ++i) w[i] = w[i + 1];
-    w[KL] = v[u];
-  };
-  // the first batches fill the window (rows 0..KL; compile-time positions), the rest of
-  // the last of them already finishes columns
-  constexpr int FILL = (KL + 1 + SPF - 1) / SPF;  // batches that rows 0..KL span
-#pragma unroll
-  for (int b = 0; b < FILL; ++b) {
-    factors(b * SPF);
-    gen.batch(b * SPF, b == 0, v);
-#pragma unroll
-    for (int u = 0; u < SPF; ++u) {
-      const int r = b * SPF + u;
-      if (r <= KL) w[r] = v[u];
-      else if (r - KL - 1 < N) step(r - KL - 1, u);
-    }
-  }
-  for (int r0 = FILL * SPF; r0 - KL - 1 < N; r0 += SPF) {
-    factors(r0);
-    gen.batch(r0, false, v);
-#pragma unroll
-    for (int u = 0; u < SPF; ++u) {
-      const int c = r0 + u - KL - 1;
-      if (c >= N) break;
-      step(c, u);
-    }
-  }
-}
-
-// the job of grid row y: POL kernels take the poloidal velocity alone, the others the
-// remaining fields (two kernels, so that each holds only its own path's registers).  The
-// poloidal velocity's chain is the longest (two solves per column) and its kernel has
-// the fewest threads: it runs beside the other kernel (a stream of its own, forked and
-// joined) with 8-row batches and the whole register file; the other kernel, with five
-// times the threads, uses 4-row batches at four CTAs per SM.
-template <bool POL> struct SolveBatch {
-  static constexpr int fwd = POL ? 8 : SPF_FUSED, bwd = POL ? 8 : SPB, ctas = POL ? 1 : 4;
-};
-__device__ __forceinline__ int solve_job(bool pol, int y) {
-  return pol ? J_VPOL : (y == 0 ? J_VTOR : y == 1 ? J_COD : y == 2 ? J_MTOR : y == 3 ? J_MPOL : J_COMP);
-}
-constexpr int SOLVE_JOBS_OTHER = J_NJOB - 1;
-
 // Predictor (velocity.F90:369-395, codensity.F90:224-234, magnetic.F90:370-408).
-// grid (ceil(2 H / threads), 1) for POL, (ceil(2 H / threads), SOLVE_JOBS_OTHER) otherwise.
-template <int KL, bool POL>
-__global__ void __launch_bounds__(SOLVE_THREADS, SolveBatch<POL>::ctas) k_predictor(StepArgs a) {
-  const int job = solve_job(POL, blockIdx.y);
+// grid (ceil(H / SOLVE_THREADS), J_NJOB).
+template <int KL>
+__global__ void __launch_bounds__(SOLVE_THREADS) k_predictor(StepArgs a) {
+  const int job = blockIdx.y;
   if (job == J_COMP && !a.comp) return;
   if ((job == J_MTOR || job == J_MPOL) && a.Nic > 1) return;  // k_mag_ic
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nh = gt >> 1, part = gt & 1;
+  const int nh = blockIdx.x * blockDim.x + threadIdx.x;
   if (nh >= a.H) return;
   const int l = a.hl[nh], N = a.N, L = a.L;
   const bool zero = (job == J_COD || job == J_COMP);
-  const RView v = rview<KL>(a, job, nh, part, l);
+  const ColView v = col_view<KL>(a, job, nh, l);
   const size_t rst = v.rst;
-  // boundary rows of the right-hand side (tim_zerobc; cod_setbc / comp_setbc for l = 0),
-  // real: the imaginary part's are zero
+  const double2 z2 = make_double2(0.0, 0.0);
+  // boundary rows of the right-hand side (tim_zerobc; cod_setbc / comp_setbc for l = 0)
   double bc0 = 0.0, bcN = 0.0;
-  if (zero && nh == 0 && part == 0) {
+  if (zero && nh == 0) {
     const int bc = job == J_COD ? a.cod_bc : a.comp_bc;
     const double qi = job == J_COD ? a.qi : a.qi_comp, qo = job == J_COD ? a.qo : a.qo_comp;
     if (bc == 1 || bc == 2) bc0 = 1.0;
@@ -696,51 +495,59 @@ __global__ void __launch_bounds__(SOLVE_THREADS, SolveBatch<POL>::ctas) k_predic
     bcN = (bc == 2 || bc == 4) ? qo : 0.0;
   }
   // vel_setbc_Tor (velocity.F90:291-300): the no-slip inner wall turns with the inner core
-  if (job == J_VTOR && l == 1 && a.hm[nh] == 0 && a.vel_bc <= 2 && part == 0) bc0 = a.rot[ROT_OMEGA] * a.rtor10[0];
-  auto w1 = [&](int c, double x) { v.W1[(size_t)c * rst] = x; };
+  if (job == J_VTOR && l == 1 && a.hm[nh] == 0 && a.vel_bc <= 2) bc0 = a.rot[ROT_OMEGA] * a.rtor10[0];
+  auto w1 = [&](int c, double2 x) { v.W1[(size_t)c * rst] = x; };
   auto r1 = [&](int n) { return v.W1[(size_t)n * rst]; };
-  if constexpr (POL) {
+  if (job == J_VPOL) {
     // Pol := NPol ; zerobc ; invX(XGre) ; Pol := YPol vel_Pol + Pol ; zerobc ; invX(XPol) ;
     // vel_gre_adjust (velocity.F90:369-395, 445-465)
+    save_terms(v.Nn, v.S, rst, N);
+    auto inA = [&](int n) {
+      const double2 x = __ldg(v.Nn + (size_t)n * rst);
+      return (n == 0 || n == N - 1) ? z2 : x;
+    };
     if (l == 0) {
-      for (int n = 0; n < N; ++n) {
-        const double x = __ldg(v.Nn + (size_t)n * rst);
-        v.S[(size_t)n * rst] = x;
-        v.X[(size_t)n * rst] = (n == 0 || n == N - 1) ? 0.0 : x;
-      }
+      for (int n = 0; n < N; ++n) v.X[(size_t)n * rst] = inA(n);
       return;
     }
-    RhsGen<KL, false, false, true, SolveBatch<POL>::fwd> g1{nullptr, L, nullptr, v.Nn, v.S, rst, N, 0.0, 0.0, 0.0, {}};
-    forward_gen<KL>(v.B2, N, g1, w1);
-    stream_backward<KL, SolveBatch<POL>::bwd>(v.B2, N, r1, [&](int c, double x) { v.W2[(size_t)c * rst] = x; });
-    RhsGen<KL, true, false, false, SolveBatch<POL>::fwd> g2{v.y1, L, v.X, v.W2, nullptr, rst, N, 0.0, 0.0, 0.0, {}};
-    forward_gen<KL>(v.B1, N, g2, w1);
-    double x0 = 0.0, xN = 0.0;
-    stream_backward<KL, SolveBatch<POL>::bwd>(v.B1, N, r1, [&](int c, double x) {
+    stream_forward<KL>(v.B2, N, inA, w1);
+    stream_backward<KL>(v.B2, N, r1, [&](int c, double2 x) { v.W2[(size_t)c * rst] = x; });
+    multy_rows<KL>(v.y1, L, v.X, v.W2, v.W2, rst, N);  // YPol vel_Pol + Pol, in place
+    auto inB = [&](int n) { return (n == 0 || n == N - 1) ? z2 : v.W2[(size_t)n * rst]; };
+    double2 x0 = z2, xN = z2;
+    stream_forward<KL>(v.B1, N, inB, w1);
+    stream_backward<KL>(v.B1, N, r1, [&](int c, double2 x) {
       v.W2[(size_t)c * rst] = x;
       if (c == N - 1) xN = x;
       if (c == 0) x0 = x;
     });
-    const double ca = v.iG[0] * x0 + v.iG[2] * xN, cb = v.iG[1] * x0 + v.iG[3] * xN;
+    double2 ca, cb;
+    gre_coeffs(v.iG, x0, xN, ca, cb);
 #pragma unroll 8
     for (int n = 0; n < N; ++n) {
-      const double g1n = __ldg(v.g + (size_t)(2 * n) * L), g2n = __ldg(v.g + (size_t)(2 * n + 1) * L);
-      v.X[(size_t)n * rst] = v.W2[(size_t)n * rst] - ca * g1n - cb * g2n;
-    }
-  } else {
-  // other fields: X := Y X + N ; zerobc (+ setbc) ; invX
-  if (l == 0 && !zero) {
-    for (int n = 0; n < N; ++n) {
-      const double x = __ldg(v.Nn + (size_t)n * rst);
-      v.S[(size_t)n * rst] = x;
-      v.X[(size_t)n * rst] = n == 0 ? bc0 : n == N - 1 ? bcN : x;
+      const double g1 = __ldg(v.g + (size_t)(2 * n) * L), g2 = __ldg(v.g + (size_t)(2 * n + 1) * L);
+      const double2 x = v.W2[(size_t)n * rst];
+      v.X[(size_t)n * rst] = make_double2(x.x - ca.x * g1 - cb.x * g2, x.y - ca.y * g1 - cb.y * g2);
     }
     return;
   }
-  RhsGen<KL, true, false, true, SolveBatch<POL>::fwd> g{v.y1, L, v.X, v.Nn, v.S, rst, N, 0.0, bc0, bcN, {}};
-  forward_gen<KL>(v.B1, N, g, w1);
-  stream_backward<KL, SolveBatch<POL>::bwd>(v.B1, N, r1, [&](int c, double x) { v.X[(size_t)c * rst] = x; });
+  // other fields: X := Y X + N ; zerobc (+ setbc) ; invX
+  const bool solve = (l != 0 || zero);
+  save_terms(v.Nn, v.S, rst, N);
+  if (!solve) {
+    for (int n = 0; n < N; ++n)
+      v.X[(size_t)n * rst] = n == 0 ? make_double2(bc0, 0.0) : n == N - 1 ? make_double2(bcN, 0.0)
+                                                                         : __ldg(v.Nn + (size_t)n * rst);
+    return;
   }
+  multy_rows<KL>(v.y1, L, v.X, v.Nn, v.W1, rst, N);  // Y X + N into W1 (solved in place)
+  auto inC = [&](int n) {
+    if (n == 0) return make_double2(bc0, 0.0);
+    if (n == N - 1) return make_double2(bcN, 0.0);
+    return v.W1[(size_t)n * rst];
+  };
+  stream_forward<KL>(v.B1, N, inC, w1);
+  stream_backward<KL>(v.B1, N, r1, [&](int c, double2 x) { v.X[(size_t)c * rst] = x; });
 }
 
 // the warp's sum of v (harmonics 32 w .. 32 w + 31) into its own slot of the corrector's
@@ -764,75 +571,72 @@ __global__ void k_cgce_sums(const double* part, int nwarp, double* red) {
 
 // Corrector (velocity.F90:413-439, codensity.F90:240-259, magnetic.F90:414-461)
 // red[] slots: 0 vTor, 1 vPol, 2 cod, 3 comp, 4 bTor, 5 bicTor, 6 bPol, 7 bicPol.
-// The sum of squares of the corrections is accumulated per real column in the order the
-// back substitution produces them (n decreasing), per warp by a fixed shuffle tree and
-// across warps by k_cgce_sums in a fixed order.  grid as k_predictor's.
-template <int KL, bool POL>
-__global__ void __launch_bounds__(SOLVE_THREADS, SolveBatch<POL>::ctas) k_corrector(StepArgs a) {
-  const int job = solve_job(POL, blockIdx.y);
+// The sum of squares of the corrections is accumulated per harmonic in the order the
+// back substitution produces them (n decreasing) and across harmonics by atomics.
+template <int KL>
+__global__ void __launch_bounds__(SOLVE_THREADS) k_corrector(StepArgs a) {
+  const int job = blockIdx.y;
   if (job == J_COMP && !a.comp) return;
   if ((job == J_MTOR || job == J_MPOL) && a.Nic > 1) return;  // k_mag_ic
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nh = gt >> 1, part = gt & 1;
+  const int nh = blockIdx.x * blockDim.x + threadIdx.x;
   double ss = 0.0, ssic = 0.0;
   if (nh < a.H) {
     const int l = a.hl[nh], N = a.N, L = a.L;
-    const RView v = rview<KL>(a, job, nh, part, l);
+    const ColView v = col_view<KL>(a, job, nh, l);
     const size_t rst = v.rst;
+    const double2 z2 = make_double2(0.0, 0.0);
     const double c = a.implicit;
     // nc = c (N - N_saved) ; N_saved = N ; zerobc (tim_nlincorr, timestep.F90:696-715)
     // vel_setbc_Tor (Re part; velocity.F90:291-299): only no-slip walls (i_vel_bc <= 2)
-    const bool tor10 = job == J_VTOR && l == 1 && a.hm[nh] == 0 && a.vel_bc <= 2 && part == 0;
-    const double bc0 = tor10 ? a.rot[ROT_OMEGA] * a.rtor10[0] - v.X[0] : 0.0;
+    const bool tor10 = job == J_VTOR && l == 1 && a.hm[nh] == 0 && a.vel_bc <= 2;
+    const double wr = tor10 ? a.rot[ROT_OMEGA] * a.rtor10[0] : 0.0;
+    // the right-hand side in W1 (the forward pass then overwrites it row by row, in place)
+    diff_terms(v.Nn, v.S, v.W1, rst, N, c);
+    auto inC = [&](int n) {
+      if (n == 0) return tor10 ? make_double2(wr - v.X[0].x, 0.0) : z2;
+      if (n == N - 1) return z2;
+      return v.W1[(size_t)n * rst];
+    };
     // x += d ; dterr sum of d^2 (tim_addcorr, timestep.F90:717-737)
-    auto addcorr = [&](int n, double d) {
-      v.X[(size_t)n * rst] = v.X[(size_t)n * rst] + d;
-      ss = ss + d * d;
+    auto addcorr = [&](int n, double2 d) {
+      const double2 x = v.X[(size_t)n * rst];
+      v.X[(size_t)n * rst] = make_double2(x.x + d.x, x.y + d.y);
+      ss = ss + d.x * d.x + d.y * d.y;
     };
-    auto w1 = [&](int cc, double x) { v.W1[(size_t)cc * rst] = x; };
+    auto w1 = [&](int cc, double2 x) { v.W1[(size_t)cc * rst] = x; };
     auto r1 = [&](int n) { return v.W1[(size_t)n * rst]; };
-    // the right-hand side and the save, row by row (columns that are not solved)
-    auto unsolved = [&](double b0) {
-      for (int n = 0; n < N; ++n) {
-        const double x = __ldg(v.Nn + (size_t)n * rst), p = v.S[(size_t)n * rst];
-        v.S[(size_t)n * rst] = x;
-        addcorr(n, n == 0 ? b0 : n == N - 1 ? 0.0 : c * (x - p));
-      }
-    };
     const bool zero = (job == J_COD || job == J_COMP);
-    double x0 = 0.0;
-    if constexpr (POL) {
+    double2 x0 = z2;
+    if (job == J_VPOL) {
       if (l == 0) {
-        unsolved(0.0);
+        for (int n = 0; n < N; ++n) addcorr(n, inC(n));
       } else {
-        RhsGen<KL, false, true, true, SolveBatch<POL>::fwd> g1{nullptr, L, nullptr, v.Nn, v.S, rst, N, c, 0.0, 0.0, {}};
-        forward_gen<KL>(v.B2, N, g1, w1);
-        stream_backward<KL, SolveBatch<POL>::bwd>(v.B2, N, r1, [&](int cc, double x) { v.W2[(size_t)cc * rst] = x; });
-        auto inD = [&](int n) { return (n == 0 || n == N - 1) ? 0.0 : v.W2[(size_t)n * rst]; };
-        double xN = 0.0;
+        stream_forward<KL>(v.B2, N, inC, w1);
+        stream_backward<KL>(v.B2, N, r1, [&](int cc, double2 x) { v.W2[(size_t)cc * rst] = x; });
+        auto inD = [&](int n) { return (n == 0 || n == N - 1) ? z2 : v.W2[(size_t)n * rst]; };
+        double2 xN = z2;
         stream_forward<KL>(v.B1, N, inD, w1);
-        stream_backward<KL, SolveBatch<POL>::bwd>(v.B1, N, r1, [&](int cc, double x) {
+        stream_backward<KL>(v.B1, N, r1, [&](int cc, double2 x) {
           v.W2[(size_t)cc * rst] = x;
           if (cc == N - 1) xN = x;
           if (cc == 0) x0 = x;
         });
-        const double ca = v.iG[0] * x0 + v.iG[2] * xN, cb = v.iG[1] * x0 + v.iG[3] * xN;
+        double2 ca, cb;
+        gre_coeffs(v.iG, x0, xN, ca, cb);
 #pragma unroll 8
         for (int n = 0; n < N; ++n) {
-          const double g1n = __ldg(v.g + (size_t)(2 * n) * L), g2n = __ldg(v.g + (size_t)(2 * n + 1) * L);
-          addcorr(n, v.W2[(size_t)n * rst] - ca * g1n - cb * g2n);
+          const double g1 = __ldg(v.g + (size_t)(2 * n) * L), g2 = __ldg(v.g + (size_t)(2 * n + 1) * L);
+          const double2 x = v.W2[(size_t)n * rst];
+          addcorr(n, make_double2(x.x - ca.x * g1 - cb.x * g2, x.y - ca.y * g1 - cb.y * g2));
         }
       }
+    } else if (l != 0 || zero) {
+      stream_forward<KL>(v.B1, N, inC, w1);
+      stream_backward<KL>(v.B1, N, r1, [&](int cc, double2 x) { addcorr(cc, x); if (cc == 0) x0 = x; });
     } else {
-      if (l != 0 || zero) {
-        RhsGen<KL, false, true, true, SolveBatch<POL>::fwd> g{nullptr, L, nullptr, v.Nn, v.S, rst, N, c, bc0, 0.0, {}};
-        forward_gen<KL>(v.B1, N, g, w1);
-        stream_backward<KL, SolveBatch<POL>::bwd>(v.B1, N, r1, [&](int cc, double x) { addcorr(cc, x); if (cc == 0) x0 = x; });
-      } else {
-        unsolved(bc0);
-      }
+      for (int n = 0; n < N; ++n) addcorr(n, inC(n));
     }
-    if ((job == J_MTOR || job == J_MPOL) && l != 0) ssic = x0 * x0;  // inner-core copy (Ni = 1)
+    if ((job == J_MTOR || job == J_MPOL) && l != 0) ssic = x0.x * x0.x + x0.y * x0.y;  // inner-core copy (Ni = 1)
   }
   int slot = job == J_VTOR ? 0 : job == J_VPOL ? 1 : job == J_COD ? 2 : job == J_COMP ? 3 : job == J_MTOR ? 4 : 6;
   warp_partial(ss, a, slot);
@@ -1104,7 +908,7 @@ StepArgs step_args(lsd_ctx* ctx) {
   a.qi = ctx->cfg.qi; a.qo = ctx->cfg.qo; a.qi_comp = ctx->cfg.qi_comp; a.qo_comp = ctx->cfg.qo_comp;
   a.comp = ctx->cfg.comp_tstep;
   a.red = ctx->d_red;
-  a.cpart = ctx->d_cpart; a.nwarp = (2 * ctx->H + 31) / 32;  // warps of the real-column grid
+  a.cpart = ctx->d_cpart; a.nwarp = (ctx->H + 31) / 32;
   a.NL = ctx->NL; a.Nic = ctx->Nic;
   a.icstate = ctx->d_icstate; a.icsv = ctx->d_icsv; a.icyt = ctx->d_icyt;
   a.rot = ctx->d_rot;
@@ -1225,38 +1029,18 @@ namespace {
 // threads per CTA: ctx->solve_threads (a multiple of 32, at most SOLVE_THREADS; the
 // autotuner's choice); one thread per harmonic whatever the CTA size, so the results and
 // the per-warp corrector partials do not depend on it
-// the auxiliary stream beside the stream work is queued on now (see lsd_ctx::aux_stream)
-cudaStream_t aux_for(const lsd_ctx* ctx) {
-  if (ctx->stream == ctx->cap_stream[0]) return ctx->aux_stream[1];
-  if (ctx->stream == ctx->cap_stream[1]) return ctx->aux_stream[2];
-  return ctx->aux_stream[0];
-}
-
 template <int KL>
-int launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
+void launch_pred(lsd_ctx* ctx, const StepArgs& a, bool corr) {
   const int T = ctx->solve_threads;
-  const dim3 gp(ceil_div(2 * ctx->H, T), 1), go(ceil_div(2 * ctx->H, T), SOLVE_JOBS_OTHER);  // a real column each
-  // the poloidal velocity's kernel on the auxiliary stream, beside the others
-  const cudaStream_t aux = aux_for(ctx);
-  CUDA_TRY(cudaEventRecord(ctx->ev_fork, ctx->stream));
-  CUDA_TRY(cudaStreamWaitEvent(aux, ctx->ev_fork, 0));
-  if (corr) {
-    k_corrector<KL, true><<<gp, T, 0, aux>>>(a);
-    k_corrector<KL, false><<<go, T, 0, ctx->stream>>>(a);
-  } else {
-    k_predictor<KL, true><<<gp, T, 0, aux>>>(a);
-    k_predictor<KL, false><<<go, T, 0, ctx->stream>>>(a);
-  }
-  CUDA_TRY(cudaEventRecord(ctx->ev_join, aux));
-  CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
-  ctx->launches++;
+  dim3 g(ceil_div(ctx->H, T), J_NJOB);
+  if (corr) k_corrector<KL><<<g, T, 0, ctx->stream>>>(a);
+  else k_predictor<KL><<<g, T, 0, ctx->stream>>>(a);
   if (ctx->Nic > 1) {  // the field coupled to the inner core
     dim3 gi(ceil_div(ctx->H, T), 2);
     if (corr) k_mag_ic<KL, true><<<gi, T, 0, ctx->stream>>>(a);
     else k_mag_ic<KL, false><<<gi, T, 0, ctx->stream>>>(a);
     ctx->launches++;
   }
-  return LSD_OK;
 }
 
 // rot_predictor / rot_corrector before the solves (main.F90:136, 148)
@@ -1272,13 +1056,14 @@ void launch_rot(lsd_ctx* ctx, bool corr) {
 
 int launch_step_kernel(lsd_ctx* ctx, const StepArgs& a, bool corr) {
   switch (ctx->KL) {
-    case 2: return launch_pred<2>(ctx, a, corr);
-    case 3: return launch_pred<3>(ctx, a, corr);
-    case 4: return launch_pred<4>(ctx, a, corr);
-    case 5: return launch_pred<5>(ctx, a, corr);
-    case 6: return launch_pred<6>(ctx, a, corr);
+    case 2: launch_pred<2>(ctx, a, corr); break;
+    case 3: launch_pred<3>(ctx, a, corr); break;
+    case 4: launch_pred<4>(ctx, a, corr); break;
+    case 5: launch_pred<5>(ctx, a, corr); break;
+    case 6: launch_pred<6>(ctx, a, corr); break;
     default: return lsd_fail(ctx, LSD_EARG, "stencil half-width KL must be 2..6 for the step kernels");
   }
+  return LSD_OK;
 }
 }  // namespace
 
