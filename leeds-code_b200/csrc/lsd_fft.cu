@@ -476,7 +476,7 @@ constexpr int PROD_THREADS = 256;
 
 template <int E, int G, int PS>
 __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int N, ProdConst pc,
-                                                              const cplx* four_in, cplx* four_out, int fpr) {
+                                                              const cplx* four_in, cplx* four_out) {
   constexpr int RS = E * (G + 1), P2 = E * G;
   constexpr int NF_IN = PSet<PS>::in, NDER = PSet<PS>::deriv, NF = NF_IN + NDER, NF_OUT = PSet<PS>::out;
   extern __shared__ __align__(16) unsigned char psm[];
@@ -509,68 +509,32 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
     rows[(size_t)row * RS + ppos<G>(k)] = c2r_pack(k, yk, ym, pl);
     if (k != 0 && 2 * k != P2) rows[(size_t)row * RS + ppos<G>(P2 - k)] = c2r_pack(P2 - k, ym, yk, pl);
   };
-  if constexpr (NDER == 0) {
-    // Coalesced gather, fpr fields per round: consecutive threads read consecutive
-    // (counter, E/O) values of this half-row (16 of every 32 bytes of the half-row pair's
-    // block, the whole block in a few wide requests instead of one request per bin pair),
-    // neighbouring lanes hold the E and the O of one counter and exchange them, the
-    // southern (E + O) and northern (E - O) bins go to a staging area by bin, and the
-    // packing reads bins k and P2 - k from there.
-    double2* stage = (double2*)((unsigned char*)tabs.thm + sizeof(int) * (size_t)((NM + 3) & ~3));
-    const int NE = 2 * NM;                                          // (c, p) values of a field
-    for (int f0 = 0; f0 < NF_IN; f0 += fpr) {
-      const int nfr = min(fpr, NF_IN - f0);
-      const int nld = ((nfr * NE + 31) / 32) * 32;                  // whole warps: the exchange
-      for (int it = tid; it < nld; it += PROD_THREADS) {
-        const int fl = it / NE, e = it - fl * NE;
-        const bool live = it < nfr * NE;
-        double2 x = make_double2(0.0, 0.0);
-        if (live) x = four_in[(size_t)pc.fin[f0 + fl] * fstride + boff + 2 * e];
-        const double2 y = make_double2(__shfl_xor_sync(0xffffffffu, x.x, 1), __shfl_xor_sync(0xffffffffu, x.y, 1));
-        if (live) {
-          const int c = e >> 1, side = e & 1;                       // E lane: south, O lane: north
-          stage[(fl * 2 + side) * M + tabs.thm[c]] = side ? sub2(y, x) : add2(x, y);
+  for (int it0 = tid; it0 < NITEM; it0 += U * PROD_THREADS) {
+    double2 e0[U], o0[U], e1[U], o1[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int it = it0 + u * PROD_THREADS;
+      e0[u] = o0[u] = e1[u] = o1[u] = make_double2(0.0, 0.0);
+      if (it < NITEM) {
+        const int f = it / KH, k = it - f * KH, km = k == 0 ? P2 : P2 - k;
+        const cplx* src = four_in + (size_t)pc.fin[f] * fstride + boff;
+        if (k < M) {
+          const int c = __ldg(pc.bin2c + k);
+          e0[u] = src[4 * c]; o0[u] = src[4 * c + 2];
+        }
+        if (km < M) {
+          const int c = __ldg(pc.bin2c + km);
+          e1[u] = src[4 * c]; o1[u] = src[4 * c + 2];
         }
       }
-      __syncthreads();
-      for (int it = tid; it < nfr * 2 * KH; it += PROD_THREADS) {
-        const int fl = it / (2 * KH), rem = it - fl * 2 * KH, side = rem / KH, k = rem - side * KH;
-        const int km = k == 0 ? P2 : P2 - k;
-        const double2* sy = stage + (fl * 2 + side) * M;
-        const double2 yk = k < M ? sy[k] : make_double2(0.0, 0.0);
-        const double2 ym = km < M ? sy[km] : make_double2(0.0, 0.0);
-        put((f0 + fl) * 2 + side, k, yk, ym);
-      }
-      __syncthreads();  // the staging area is refilled by the next round
     }
-  } else {  // bin pairs straight from HBM (the sets with derived rows)
-    for (int it0 = tid; it0 < NITEM; it0 += U * PROD_THREADS) {
-      double2 e0[U], o0[U], e1[U], o1[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int it = it0 + u * PROD_THREADS;
-        e0[u] = o0[u] = e1[u] = o1[u] = make_double2(0.0, 0.0);
-        if (it < NITEM) {
-          const int f = it / KH, k = it - f * KH, km = k == 0 ? P2 : P2 - k;
-          const cplx* src = four_in + (size_t)pc.fin[f] * fstride + boff;
-          if (k < M) {
-            const int c = __ldg(pc.bin2c + k);
-            e0[u] = src[4 * c]; o0[u] = src[4 * c + 2];
-          }
-          if (km < M) {
-            const int c = __ldg(pc.bin2c + km);
-            e1[u] = src[4 * c]; o1[u] = src[4 * c + 2];
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int it = it0 + u * PROD_THREADS;
-        if (it < NITEM) {
-          const int f = it / KH, k = it - f * KH;
-          put(f * 2, k, add2(e0[u], o0[u]), add2(e1[u], o1[u]));
-          put(f * 2 + 1, k, sub2(e0[u], o0[u]), sub2(e1[u], o1[u]));
-        }
+    for (int u = 0; u < U; ++u) {
+      const int it = it0 + u * PROD_THREADS;
+      if (it < NITEM) {
+        const int f = it / KH, k = it - f * KH;
+        put(f * 2, k, add2(e0[u], o0[u]), add2(e1[u], o1[u]));
+        put(f * 2 + 1, k, sub2(e0[u], o0[u]), sub2(e1[u], o1[u]));
       }
     }
   }
@@ -836,9 +800,7 @@ bool lsd_fft_compiled(int E, int G) { return dispatch_EG(E, G, [](auto, auto) { 
 
 // shared memory of the products kernel with the plan (E, G) for nfields staged rows
 size_t lsd_products_smem_for(int nfields, int P2, int E, int G, int NM) {
-  // + one field of the gather's staging area (2 x M bins; M <= NM)
-  return sizeof(double2) * ((size_t)nfields * 2 * E * (G + 1)) + fft_tab_bytes(P2, E, G, NM) +
-         sizeof(double2) * 2 * (size_t)NM;
+  return sizeof(double2) * ((size_t)nfields * 2 * E * (G + 1)) + fft_tab_bytes(P2, E, G, NM);
 }
 size_t lsd_products_smem_eg(const lsd_ctx* ctx, int E, int G) {
   const bool comp = ctx->cfg.comp_tstep != 0;
@@ -898,20 +860,14 @@ template <int PS>
 int launch_products_set(lsd_ctx* ctx, const ProdConst& pc, const cplx* four_in, cplx* four_out) {
   FFTPlanDev pl = make_plan(ctx);
   constexpr int NF = PSet<PS>::in + PSet<PS>::deriv;
-  const size_t base = sizeof(double2) * ((size_t)NF * 2 * ctx->fftE * (ctx->fftG + 1)) +
+  const size_t smem = sizeof(double2) * ((size_t)NF * 2 * ctx->fftE * (ctx->fftG + 1)) +
                       fft_tab_bytes(ctx->P2, ctx->fftE, ctx->fftG, ctx->NM);
-  // the coalesced gather's staging area: two fields per round where that keeps the CTAs
-  // per SM (two below 112 KB each), else one
-  const size_t per_field = PSet<PS>::deriv == 0 ? sizeof(double2) * 2 * (size_t)ctx->M : 0;
-  const size_t half = 112 * 1024, full = 224 * 1024;
-  const int fpr = (base + 2 * per_field <= half || (base > half && base + 2 * per_field <= full)) ? 2 : 1;
-  const size_t smem = base + fpr * per_field;
-  if (smem > full) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
+  if (smem > 224 * 1024) return lsd_fail(ctx, LSD_EARG, "products: FFT rows do not fit in shared memory");
   dim3 grid(2 * ctx->HB, ctx->N);
   int rc = dispatch_EG(ctx->fftE, ctx->fftG, [&](auto e, auto g) {
     constexpr int E = decltype(e)::value, G = decltype(g)::value;
     cudaFuncSetAttribute(k_products<E, G, PS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_products<E, G, PS><<<grid, PROD_THREADS, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out, fpr);
+    k_products<E, G, PS><<<grid, PROD_THREADS, smem, ctx->stream>>>(pl, ctx->N, pc, four_in, four_out);
     return 0;
   });
   if (rc) return lsd_fail(ctx, LSD_EARG, "FFT length not supported");
