@@ -144,7 +144,6 @@ constexpr int OZ_MAXSTAGES = 4;  // bulk-copy ring: up to 4 stages, as many as l
 constexpr int OZ_EPI = 256;      // epilogue threads: warps 0-7 (warp w: TMEM lane quarter w % 4,
                                  // column half w / 4 of a chunk)
 constexpr int OZ_THREADS = OZ_EPI + 64;  // + warp 8 (bulk copies) and warp 9 (MMA issue)
-constexpr int OZ_STG = OZ_NC + 1;  // epilogue staging row (doubles)
 constexpr int OZ_MAXG = 8;       // groups (output fields) of one launch
 
 enum { OZ_VEC = 0, OZ_P = 1, OZ_GRAD = 2, OZ_ST = 3, OZ_Q = 4, OZ_NTYPE = 5 };
@@ -517,8 +516,36 @@ struct OzGemmArgs {
   const int* nhlist; const int* hm;
   cplx* out0[OZ_MAXG]; cplx* out1[OZ_MAXG]; int zero_m0_im[OZ_MAXG];
   int* err;
-  int nst;  // stages of the bulk-copy ring
+  int nst;          // stages of the bulk-copy ring
+  int pair_digits;  // the launch's diagonal bound allows D_2i 256 + D_2i+1 in int32
 };
+
+// The exact integer sum_d D_d 256^(S-1-d) of one accumulator column (|sum| < 2^53, so
+// every partial sum below is exact in FP64).  pair: two diagonals per int32 (D_2i 256 +
+// D_2i+1, which the host has bounded below 2^31), joined in FP64 by 2^16 steps; half as
+// many int32 -> FP64 conversions as one diagonal at a time.
+// one 32-byte store of two complex values (p 32-byte aligned)
+__device__ __forceinline__ void st_global_2c(cplx* p, double2 a, double2 b) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
+               : "memory");
+}
+
+template <int S>
+__device__ __forceinline__ double oz_combine(const int32_t (&v)[S][8], int q, bool pair) {
+  double h;
+  if (pair) {
+    h = (double)(v[0][q] * 256 + v[1][q]);
+#pragma unroll
+    for (int d = 2; d < S; d += 2)
+      if (d + 1 < S) h = fma(h, 65536.0, (double)(v[d][q] * 256 + v[d + 1][q]));
+      else h = fma(h, 256.0, (double)v[d][q]);
+  } else {
+    h = (double)v[0][q];
+#pragma unroll
+    for (int d = 1; d < S; ++d) h = fma(h, 256.0, (double)v[d][q]);
+  }
+  return h;
+}
 
 __device__ __forceinline__ bool oz_wait(uint64_t* mbar, uint32_t parity, int* err) {
   if (umma::mbar_wait(mbar, parity, WAIT_ITERS)) return true;
@@ -531,21 +558,17 @@ __device__ __forceinline__ bool oz_wait(uint64_t* mbar, uint32_t parity, int* er
 // issue and the tensor-memory handshakes run on counters over all of the CTA's tiles, so
 // the pipeline does not drain between tiles.  Two CTAs per SM (256 tensor-memory columns
 // each).
-template <int TYPE>
+template <int TYPE, int S>
 __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb) {
   constexpr int PER = OzT<TYPE>::per;
   extern __shared__ __align__(1024) uint8_t oz_smem[];
   __shared__ __align__(8) uint64_t full[OZ_MAXSTAGES], empty[OZ_MAXSTAGES], accf, tfree, fin;
   __shared__ uint32_t tbase;
-  __shared__ cplx* pbase[64];  // output base of each (re, im) row pair of the z-block
-  __shared__ int pzero[64];    // analysis: drop the imaginary part of m = 0 for this pair
-  __shared__ double csc[OZ_NC];  // column scales 2^fexp of the current chunk
+  __shared__ double csc[2][OZ_NC];  // column scales 2^fexp of a chunk (chunk parity)
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int S = a.S;
   const int ntile = a.NM * 2 * nzb;
   const uint32_t stage_bytes = (uint32_t)S * 5120;  // A: S x 4096, B: S x 1024
   const int nst = a.nst;
-  double* stg = (double*)(oz_smem + (size_t)nst * stage_bytes);  // [128][OZ_STG]
   if (tid == 0) {
     for (int i = 0; i < nst; ++i) { umma::mbar_init(&full[i], 1); umma::mbar_init(&empty[i], 1); }
     umma::mbar_init(&accf, 1);
@@ -636,8 +659,15 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
     umma::mbar_wait(&fin, 0, WAIT_ITERS);
   } else if (tid < OZ_EPI) {
     // ---- epilogue: row (tid mod 128) of each z-block, columns 16 (tid / 128) .. + 15 of a
-    // chunk
-    const int row = tid & 127, half = tid >> 7;
+    // chunk, in two groups of 8.  Per group the thread reads its S x 8 accumulator words,
+    // forms the 8 values and trades half of them with the neighbouring lane (rows 2i and
+    // 2i + 1 are Re and Im of one output: the even lane keeps the group's columns 0-3, the
+    // odd lane 4-7).  The tensor memory goes back once the second group's words are in
+    // registers (the MMAs of the next chunk run while the thread converts and stores);
+    // the 8 complex values go straight to HBM.
+    const int row = tid & 127, half = tid >> 7, odd = row & 1;
+    const uint32_t tlane = (uint32_t)(32 * (warp & 3)) << 16;
+    const bool pair = a.pair_digits != 0;
     int cc = 0;
     OzProb nxt = prob(blockIdx.x);
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
@@ -646,27 +676,23 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
       const OzProb pr = nxt;
       nxt = prob(t + gridDim.x);
       if (pr.nchunk == 0) continue;  // no harmonics of this parity: nothing to write
-      if (tid < 64) {
-        const int Rr = zb * 128 + 2 * tid;
-        cplx* base = nullptr;
-        int zero = 0;
-        if (Rr < a.nrows) {
-          const int g = Rr / a.rows_per_group, n = (Rr % a.rows_per_group) / PER, comp = Rr % PER;
-          cplx* out = (comp < 2) ? a.out0[g] : a.out1[g];
-          base = OzT<TYPE>::anal ? out + (size_t)n * a.H : out + four_off(n, c, p, 0, a.NM, a.HB);
-          zero = TYPE == OZ_ST || a.zero_m0_im[g];
-        }
-        pbase[tid] = base;
-        pzero[tid] = zero;
-      }
-      const int R = zb * 128 + row;
+      const int R = zb * 128 + row, Rp = R & ~1;  // rows come in (Re, Im) pairs: nrows is even
       const bool live = R < a.nrows;
+      cplx* base = nullptr;  // this lane pair's output
+      bool zero = false;     // analysis: drop the imaginary part of m = 0
+      if (Rp < a.nrows) {
+        const int g = Rp / a.rows_per_group, n = (Rp % a.rows_per_group) / PER, comp = Rp % PER;
+        cplx* out = (comp < 2) ? a.out0[g] : a.out1[g];
+        base = OzT<TYPE>::anal ? out + (size_t)n * a.H : out + four_off(n, c, p, 0, a.NM, a.HB);
+        zero = TYPE == OZ_ST || a.zero_m0_im[g];
+      }
       // x y = 2^(ea + eb + 4) sum_d D_d 2^(-8(d+2)) = 2^(ea + eb + 4 - 8(S+1)) H with
       // H = Horner over d in 2^8; the power of two and the row scale 2^erow are one factor
       const double rsc = live ? pow2i(a.erow[(size_t)c * a.nrows + R] + 4 - 8 * (S + 1)) : 0.0;
       bool ok = true;
       for (int ch = 0; ch < pr.nchunk; ++ch, ++cc) {
-        if (tid < OZ_NC) csc[tid] = pow2i(a.fexp[pr.fofs + ch * OZ_NC + tid]);
+        // csc[cc & 1] was last read in chunk cc - 2, before every thread's barrier of cc - 1
+        if (tid < OZ_NC) csc[cc & 1][tid] = pow2i(a.fexp[pr.fofs + ch * OZ_NC + tid]);
         const bool got = umma::mbar_wait(&accf, cc & 1, WAIT_ITERS);
         if (!umma::bar_and(1, OZ_EPI, got)) {  // uniform over the epilogue threads
           if (tid == 0) atomicExch(a.err, 1);
@@ -674,46 +700,58 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
           break;
         }
         umma::fence_after_sync();
+        const double* cs = csc[cc & 1] + 16 * half;
+        double2 o[2][4];
 #pragma unroll
-        for (int c0 = 16 * half; c0 < 16 * half + 16; c0 += 4) {
-          int32_t v[OZ_MAXS][4];
+        for (int g8 = 0; g8 < 2; ++g8) {
+          int32_t v[S][8];
 #pragma unroll
-          for (int d = 0; d < OZ_MAXS; ++d)
-            if (d < S) umma::tmem_ld4(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * OZ_NC + c0), v[d]);
+          for (int d = 0; d < S; ++d)
+            umma::tmem_ld8(tmem + tlane + (uint32_t)(d * OZ_NC + 16 * half + 8 * g8), v[d]);
           umma::tmem_wait_ld();
+          if (g8 == 1) {  // all words of this chunk are in registers
+            umma::fence_before_sync();
+            umma::mbar_arrive(&tfree);
+          }
+          double h[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) h[q] = oz_combine<S>(v, q, pair) * (rsc * cs[8 * g8 + q]);
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            double hsum = (double)v[0][q];
-#pragma unroll
-            for (int d = 1; d < OZ_MAXS; ++d)
-              if (d < S) hsum = fma(hsum, 256.0, (double)v[d][q]);
-            stg[row * OZ_STG + c0 + q] = hsum * (rsc * csc[c0 + q]);
+            const double r = __shfl_xor_sync(0xffffffffu, odd ? h[q] : h[q + 4], 1);
+            o[g8][q] = odd ? make_double2(r, h[q + 4]) : make_double2(h[q], r);
           }
         }
-        umma::fence_before_sync();
-        umma::mbar_arrive(&tfree);  // tensor memory may take the next chunk
-        umma::bar_sync(1, OZ_EPI);
-        // coalesced stores: row pairs (re, im) x 32 columns
-        for (int idx = tid; idx < 64 * OZ_NC; idx += OZ_EPI) {
-          const int pair = idx / OZ_NC, q = idx % OZ_NC;
-          cplx* base = pbase[pair];
-          if (!base) continue;
-          double2 val = make_double2(stg[(2 * pair) * OZ_STG + q], stg[(2 * pair + 1) * OZ_STG + q]);
-          if (!OzT<TYPE>::anal) {
-            const int j = ch * OZ_NC + q;
-            if (j < a.Th2) base[(size_t)(j >> 1) * a.NM * 4 + (j & 1)] = val;
-          } else {
-            const int k = ch * OZ_NC + q;
-            if (k < pr.nk) {
-              const int nh = a.nhlist[pr.nhofs + k];
-              // m = 0: s, t (and a scalar) keep no imaginary part; q keeps its own
-              // (transform.fftw3.F90:599, 869, 902, 908)
-              if (pzero[pair] && a.hm[nh] == 0) val.y = 0.0;
-              base[nh] = val;
+        if (base) {
+#pragma unroll
+          for (int g8 = 0; g8 < 2; ++g8) {
+            const int k0 = ch * OZ_NC + 16 * half + 8 * g8 + 4 * odd;
+            if (!OzT<TYPE>::anal) {
+              // theta rows j, j + 1 (j even) of one half-row pair are neighbours in four_off:
+              // one 32-byte store (the field bases are 32-byte aligned)
+#pragma unroll
+              for (int q = 0; q < 4; q += 2) {
+                const int j = k0 + q;
+                cplx* dst = base + (size_t)(j >> 1) * a.NM * 4;
+                if (j + 1 < a.Th2) st_global_2c(dst, o[g8][q], o[g8][q + 1]);
+                else if (j < a.Th2) *dst = o[g8][q];
+              }
+            } else {
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int k = k0 + q;
+                if (k < pr.nk) {
+                  const int nh = a.nhlist[pr.nhofs + k];
+                  double2 val = o[g8][q];
+                  // m = 0: s, t (and a scalar) keep no imaginary part; q keeps its own
+                  // (transform.fftw3.F90:599, 869, 902, 908)
+                  if (zero && a.hm[nh] == 0) val.y = 0.0;
+                  base[nh] = val;
+                }
+              }
             }
           }
         }
-        umma::bar_sync(1, OZ_EPI);
       }
       if (!ok) break;
     }
@@ -743,14 +781,30 @@ struct OzState {
   int nst = 2;           // GEMM ring stages
   int ctas = 2;          // persistent GEMM CTAs per SM
   int srow[2] = {1, 1};  // pre-pass stage row length (odd, in complex): synthesis, analysis
+  int pair[OZ_NTYPE] = {};  // per type: the epilogue may join diagonals in pairs (oz_combine)
 };
 
 namespace {
 constexpr int OZ_MAXG_SYNTH = OZ_MAXG, OZ_MAXG_ANAL = 4;  // groups per launch
 
+// f(k_oz_gemm<TYPE, S>) for the runtime slice count S
+template <int TYPE, class F>
+void oz_gemm_dispatch(int S, F&& f) {
+  switch (S) {
+    case 2: f(k_oz_gemm<TYPE, 2>); break;
+    case 3: f(k_oz_gemm<TYPE, 3>); break;
+    case 4: f(k_oz_gemm<TYPE, 4>); break;
+    case 5: f(k_oz_gemm<TYPE, 5>); break;
+    case 6: f(k_oz_gemm<TYPE, 6>); break;
+    case 7: f(k_oz_gemm<TYPE, 7>); break;
+    default: f(k_oz_gemm<TYPE, 8>); break;
+  }
+}
 template <int TYPE>
-void oz_set_smem(size_t smem) {
-  cudaFuncSetAttribute(k_oz_gemm<TYPE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+void oz_set_smem(int S, size_t smem) {
+  oz_gemm_dispatch<TYPE>(S, [&](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
 }
 }  // namespace
 
@@ -826,10 +880,26 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
         probs[((size_t)type * NM + c) * 2 + p] = pr;
       }
     abytes_max = std::max(abytes_max, abytes);
+    // digit products bound the diagonals: |D_d| <= K sum_{s+t=d} m_s m_t with m_0 = 65 (the
+    // top digit) and m_s = 128 below it; pairs need 256 |D_2i| + |D_2i+1| < 2^31
+    long long kmax = 0;
+    for (int c = 0; c < NM; ++c)
+      for (int p = 0; p < 2; ++p) kmax = std::max(kmax, 32LL * probs[((size_t)type * NM + c) * 2 + p].nks);
+    auto bound = [&](int d) {
+      long long b = 0;
+      for (int s = 0; s < S; ++s) {
+        const int t = d - s;
+        if (t >= 0 && t < S) b += (long long)(s ? 128 : 65) * (t ? 128 : 65);
+      }
+      return kmax * b;
+    };
+    bool pair_ok = true;
+    for (int d = 0; d + 1 < S; d += 2) pair_ok = pair_ok && 256 * bound(d) + bound(d + 1) < (1LL << 31);
+    o->pair[type] = pair_ok ? 1 : 0;
   }
   // ring stages: as many (2..4) as keep two CTAs per SM (<= 78 KiB of stages each)
   lsd_ozaki_default_tiles(S, &o->nst, &o->ctas);
-  o->smem = (size_t)o->nst * S * 5120 + sizeof(double) * 128 * OZ_STG;
+  o->smem = (size_t)o->nst * S * 5120;
   {
     int mx = 1;
     for (int c = 0; c < NM; ++c) mx = std::max(mx, ctx->mlen[c]);
@@ -867,8 +937,8 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
   ctx->launches += 5;
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  oz_set_smem<OZ_VEC>(o->smem); oz_set_smem<OZ_P>(o->smem); oz_set_smem<OZ_GRAD>(o->smem);
-  oz_set_smem<OZ_ST>(o->smem); oz_set_smem<OZ_Q>(o->smem);
+  oz_set_smem<OZ_VEC>(o->S, o->smem); oz_set_smem<OZ_P>(o->S, o->smem); oz_set_smem<OZ_GRAD>(o->S, o->smem);
+  oz_set_smem<OZ_ST>(o->S, o->smem); oz_set_smem<OZ_Q>(o->S, o->smem);
   CUDA_TRY(cudaGetLastError());
   return LSD_OK;
 }
@@ -892,6 +962,7 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   ga.N = ctx->N; ga.H = ctx->H; ga.NM = ctx->NM; ga.Th2 = ctx->Th2; ga.HB = ctx->HB; ga.S = o->S; ga.nrows = nrows;
   ga.rows_per_group = rpg; ga.probs = o->d_probs; ga.A = o->d_A; ga.B = o->d_B; ga.fexp = o->d_fexp;
   ga.erow = o->d_erow; ga.nhlist = o->d_nh; ga.hm = ctx->d_m; ga.err = o->d_err; ga.nst = o->nst;
+  ga.pair_digits = o->pair[TYPE];
   for (int i = 0; i < OZ_MAXG; ++i) {
     const bool on = i < ng;
     pa.in0[i] = on ? gs[i].in0 : nullptr; pa.in1[i] = on ? gs[i].in1 : nullptr;
@@ -917,7 +988,9 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->dev);
   const int ntile = ctx->NM * 2 * nzb;
-  k_oz_gemm<TYPE><<<std::min(ntile, o->ctas * nsm), OZ_THREADS, o->smem, ctx->stream>>>(ga, nzb);
+  oz_gemm_dispatch<TYPE>(o->S, [&](auto kern) {
+    kern<<<std::min(ntile, o->ctas * nsm), OZ_THREADS, o->smem, ctx->stream>>>(ga, nzb);
+  });
   ctx->launches += 2;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return lsd_fail(ctx, LSD_ECUDA, std::string("tensor-core contraction: ") + cudaGetErrorString(e));
@@ -986,17 +1059,19 @@ int lsd_ozaki_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
 int* lsd_ozaki_err_flag(lsd_ctx* ctx) { return ((OzState*)ctx->oz)->d_err; }
 
 // The GEMM's tunable tiles: ring stages and CTAs per SM.  A pair is valid when the
-// stages and the epilogue's staging fit the shared memory of that many CTAs per SM
-// (228 KB per SM, 1 KB reserved per CTA) and leave room for the 256 (ctas = 2) or 512
-// tensor-memory columns.
+// stages (+ 4 KB of static shared memory) fit the shared memory of that many CTAs per SM
+// (228 KB per SM, 1 KB reserved per CTA); 256 (ctas = 2) or 512 tensor-memory columns
+// each.
 bool lsd_ozaki_tiles_ok(int S, int nst, int ctas) {
   if (nst < 2 || nst > OZ_MAXSTAGES || (ctas != 1 && ctas != 2) || S < 2 || S > OZ_MAXS) return false;
-  const size_t smem = (size_t)nst * S * 5120 + sizeof(double) * 128 * OZ_STG + 4096;  // + static
+  const size_t smem = (size_t)nst * S * 5120 + 4096;  // + static
   return smem * ctas <= (size_t)228 * 1024 - 1024 * ctas;
 }
-int lsd_ozaki_default_stages(int S) { return std::max(2, std::min(OZ_MAXSTAGES, 79872 / (S * 5120))); }
-// the default tiles: as many stages (2..4) as leave two CTAs per SM, one CTA per SM when
-// even two stages do not (S = 8), so that the persistent grid is all resident
+// three stages where two CTAs per SM still fit, else two (at lmax 127, five slices: 2 and
+// 3 stages time alike, 4 two per cent slower)
+int lsd_ozaki_default_stages(int S) { return lsd_ozaki_tiles_ok(S, 3, 2) ? 3 : 2; }
+// the default tiles: the default stages, two CTAs per SM where they fit, else one, so that
+// the persistent grid is all resident
 void lsd_ozaki_default_tiles(int S, int* nst, int* ctas) {
   *nst = lsd_ozaki_default_stages(S);
   *ctas = lsd_ozaki_tiles_ok(S, *nst, 2) ? 2 : 1;
@@ -1012,9 +1087,9 @@ int lsd_ozaki_set_tiles(lsd_ctx* ctx, int nst, int ctas) {
   if (!lsd_ozaki_tiles_ok(o->S, nst, ctas)) return lsd_fail(ctx, LSD_EARG, "tensor-core GEMM tiles: invalid stages / CTAs");
   o->nst = nst;
   o->ctas = ctas;
-  o->smem = (size_t)o->nst * o->S * 5120 + sizeof(double) * 128 * OZ_STG;
-  oz_set_smem<OZ_VEC>(o->smem); oz_set_smem<OZ_P>(o->smem); oz_set_smem<OZ_GRAD>(o->smem);
-  oz_set_smem<OZ_ST>(o->smem); oz_set_smem<OZ_Q>(o->smem);
+  o->smem = (size_t)o->nst * o->S * 5120;
+  oz_set_smem<OZ_VEC>(o->S, o->smem); oz_set_smem<OZ_P>(o->S, o->smem); oz_set_smem<OZ_GRAD>(o->S, o->smem);
+  oz_set_smem<OZ_ST>(o->S, o->smem); oz_set_smem<OZ_Q>(o->S, o->smem);
   CUDA_TRY(cudaGetLastError());
   return LSD_OK;
 }

@@ -35,12 +35,13 @@ def test_candidates(L, M, Mp, prec, S):
     assert sp["solve_threads"] == [128, 64, 32]
     if prec == capi.PREC_OZAKI:
         Sx = S or 7
-        default_stages = max(2, min(4, 79872 // (Sx * 5120)))
-        fits2 = default_stages * Sx * 5120 + 8 * 128 * 33 + 4096 <= (228 * 1024 - 2048) // 2
-        assert sp["gemm"][0] == (default_stages, 2 if fits2 else 1)
+
+        def fits(nst, ctas):  # ring stages + 4 KB static, 1 KB reserved per CTA, 228 KB per SM
+            return (nst * Sx * 5120 + 4096) * ctas <= 228 * 1024 - 1024 * ctas
+        default_stages = 3 if fits(3, 2) else 2
+        assert sp["gemm"][0] == (default_stages, 2 if fits(default_stages, 2) else 1)
         for nst, ctas in sp["gemm"]:
-            smem = nst * Sx * 5120 + 8 * 128 * 33 + 4096
-            assert 2 <= nst <= 4 and ctas in (1, 2) and smem * ctas <= 228 * 1024 - 1024 * ctas
+            assert 2 <= nst <= 4 and ctas in (1, 2) and fits(nst, ctas)
         assert len(set(sp["gemm"])) == len(sp["gemm"])
     else:
         assert sp["gemm"] == []
