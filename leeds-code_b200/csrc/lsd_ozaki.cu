@@ -133,14 +133,15 @@ int lsd_umma_selftest(lsd_ctx* ctx, double* maxerr) {
 // Two kernels per contraction: a slicing pre-pass reads the FP64 data once, takes each
 // row's exponent and writes the int8 digits in the tcgen05 shared-memory tile layout; the
 // GEMM streams A and B tiles with bulk copies (a ring of 2-4 stages), issues the int8 MMAs of
-// the S(S+1)/2 digit pairs into S tensor-memory diagonals, and its epilogue warps recombine
-// the diagonals in FP64 and store through shared memory (coalesced).
+// the S(S+1)/2 digit pairs into S tensor-memory diagonals, and its epilogue warps read the
+// diagonals into registers, hand the tensor memory back, recombine them exactly and store
+// straight to HBM.
 // =========================================================================================
 namespace {
 
 constexpr int OZ_MAXS = 8;       // slices per operand
 constexpr int OZ_NC = 32;        // columns per chunk
-constexpr int OZ_MAXSTAGES = 4;  // bulk-copy ring: up to 4 stages, as many as leave two CTAs per SM
+constexpr int OZ_MAXSTAGES = 4;  // bulk-copy ring: up to 4 stages (default 3 where two CTAs per SM fit)
 constexpr int OZ_EPI = 256;      // epilogue threads: warps 0-7 (warp w: TMEM lane quarter w % 4,
                                  // column half w / 4 of a chunk)
 constexpr int OZ_THREADS = OZ_EPI + 64;  // + warp 8 (bulk copies) and warp 9 (MMA issue)
