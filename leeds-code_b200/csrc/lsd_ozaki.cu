@@ -320,7 +320,8 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
   extern __shared__ __align__(16) double2 stg[];  // [2 stages][slot][field][srow]
   __shared__ __align__(8) uint64_t full[2];
   __shared__ int e_slot[NSQ];
-  __shared__ int kx[2][512];  // harmonic lists of the two problems (synthesis), local indices
+  __shared__ __align__(16) int kx[2][512];  // harmonic lists of the two problems (synthesis), local
+                                            // indices, 0 beyond K up to the last K step
   const int c = blockIdx.x, zb = blockIdx.y;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int kbeg = a.mstart[c], klen = a.mlen[c];
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
   if (!OzT<TYPE>::anal)
     for (int p = 0; p < 2; ++p) {
       const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
-      for (int i = tid; i < pr.K && i < 512; i += 256) kx[p][i] = a.kidx[pr.kofs + i] - kbeg;
+      for (int i = tid; i < pr.nks * 32 && i < 512; i += 256) kx[p][i] = i < pr.K ? a.kidx[pr.kofs + i] - kbeg : 0;
     }
   __syncthreads();
   // quarter q -> stage q & 1 (issued by thread 0)
@@ -398,58 +399,51 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
     const int sl = r / PER, comp = R % PER;
     const double sc = live && e_slot[sl] > -1000 ? pow2i(8 * S - 2 - e_slot[sl]) : 0.0;
     const unsigned long long bias = oz_bias(S);
-    const double r1 = (TYPE == OZ_GRAD && live) ? a.rinv[(R % a.rows_per_group) / PER] : 1.0;
-    const double2* row0 = st + (size_t)(sl * NIN) * srow;
-    const double2* row1 = row0 + srow;  // second field (VEC: t, ST: phi)
-    const int rt = q * 32 + r;          // row inside the 128-row tile
-    // the A value of row R, harmonic / theta-row slot k of parity p (0 beyond K)
-    auto value = [&](int p, const OzProb& pr, int k) {
-      double v = 0.0;
-      if (live && k < pr.K) {
-        const bool seg1 = k < pr.len1;
-        if (TYPE == OZ_P) {
-          const double2 x = row0[kx[p][k]];
-          v = comp ? x.y : x.x;
-        } else if (TYPE == OZ_VEC) {
-          // theta: s llP_ (segment 1) + (t.im, -t.re) llsin1mP (segment 2);
-          // phi:   t llP_ + (-s.im, s.re) llsin1mP        (transform.fftw3.F90:746-774)
-          const bool use_t = seg1 ? comp >= 2 : comp < 2;
-          const double2 x = (use_t ? row1 : row0)[kx[p][k]];
-          if (seg1) v = (comp & 1) ? x.y : x.x;
-          else v = comp == 0 ? x.y : comp == 1 ? -x.x : comp == 2 ? -x.y : x.x;
-        } else if (TYPE == OZ_GRAD) {
-          // theta: (C/r) P_ ; phi: i (C/r) sin1mP              (transform.fftw3.F90:955-1000)
-          if (seg1 == (comp < 2)) {
-            const double2 x = row0[kx[p][k]];
-            const double2 cv = make_double2(x.x * r1, x.y * r1);
-            v = comp == 0 ? cv.x : comp == 1 ? cv.y : comp == 2 ? -cv.y : cv.x;
-          }
-        } else if (TYPE == OZ_Q) {
-          const double2 y = row0[2 * k + p];
-          v = comp ? y.y : y.x;
-        } else {  // OZ_ST: segment 1 (gwllP_) on parity 1-p, segment 2 (gwllsin1mP) on parity p
-          const int pp = seg1 ? 1 - p : p;
-          const int j = seg1 ? k : k - pr.len1;
-          // s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re)
-          // (transform.fftw3.F90:866-909)
-          const bool use_ph = seg1 ? comp >= 2 : comp < 2;
-          const double2 y = (use_ph ? row1 : row0)[2 * j + pp];
-          if (seg1) v = (comp & 1) ? y.y : y.x;
-          else v = comp == 0 ? y.y : comp == 1 ? -y.x : comp == 2 ? -y.y : y.x;
-        }
-      }
-      return v;
-    };
+    const double* row0 = (const double*)(st + (size_t)(sl * NIN) * srow);
+    const double* row1 = row0 + 2 * srow;  // second field (VEC: t, ST: phi)
+    const int rt = q * 32 + r;             // row inside the 128-row tile
+    // Per thread and K segment, the value of K slot k is f * src[idx(k)] (a double of the
+    // staged complex rows: component and field fixed by the row's component `comp`), and f
+    // (a sign, 1/r for the gradient, 0 where the segment does not feed this component) is
+    // folded into the power-of-two scale: fl(x f 2^a) = fl(x f) 2^a, so the digits are
+    // those of the value itself.  The reference's recipes:
+    //  VEC theta: s llP_ (segment 1) + (t.im, -t.re) llsin1mP (segment 2);
+    //      phi:   t llP_ + (-s.im, s.re) llsin1mP                      (transform.fftw3.F90:746-774)
+    //  GRAD theta: (C/r) P_ ; phi: i (C/r) sin1mP                     (transform.fftw3.F90:955-1000)
+    //  ST s: Yth gwllP_ + (Yph.im, -Yph.re) gwllsin1mP ; t: Yph gwllP_ + (-Yth.im, Yth.re),
+    //      segment 1 on parity 1 - p, segment 2 on parity p             (transform.fftw3.F90:866-909)
+    const double* src1;  // segment 1 (k < len1)
+    const double* src2;  // segment 2
+    double f1 = 1.0, f2 = 1.0;
+    if (TYPE == OZ_P || TYPE == OZ_Q) {
+      src1 = src2 = row0 + (comp & 1);
+    } else if (TYPE == OZ_VEC || TYPE == OZ_ST) {
+      src1 = (comp >= 2 ? row1 : row0) + (comp & 1);
+      src2 = (comp < 2 ? row1 : row0) + ((comp & 1) ? 0 : 1);
+      f2 = (comp == 1 || comp == 2) ? -1.0 : 1.0;
+    } else {  // OZ_GRAD
+      const double r1 = live ? a.rinv[(R % a.rows_per_group) / PER] : 1.0;
+      src1 = row0 + (comp & 1);
+      src2 = row0 + (comp == 2 ? 1 : 0);
+      f1 = comp < 2 ? r1 : 0.0;
+      f2 = comp >= 2 ? (comp == 2 ? -r1 : r1) : 0.0;
+    }
+    const double sc1 = sc * f1, sc2 = sc * f2;
     if constexpr (OzT<TYPE>::anal) {
       // items (parity, K step, 16-byte half of the step) over the warps; a thread writes one
       // full 16-byte core-matrix row per slice, a warp four whole 128-byte lines (the
-      // analysis has K steps enough for all warps)
+      // analysis has K steps enough for all warps).  Slot k reads complex element 2j + pp
+      // (j = k in segment 1, k - len1 in segment 2; pp = 1 - p, p (ST) or p (Q)), i.e. the
+      // double 4k + const per segment.
       const OzProb pr0 = a.probs[(TYPE * a.NM + c) * 2], pr1 = a.probs[(TYPE * a.NM + c) * 2 + 1];
       const int n0 = pr0.nchunk ? 2 * pr0.nks : 0, n1 = pr1.nchunk ? 2 * pr1.nks : 0;
       for (int i = kq; i < n0 + n1; i += 8) {
         const int p = i < n0 ? 0 : 1;
         const OzProb& pr = p ? pr1 : pr0;
         const int li = i - (p ? n0 : 0), ks = li >> 1, hh = li & 1;
+        const int pp1 = TYPE == OZ_ST ? 1 - p : p;
+        const double* b1 = src1 + 2 * pp1;
+        const double* b2 = src2 + 2 * p - 4 * pr.len1;
         int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
         uint32_t ow[S][4];
 #pragma unroll
@@ -457,7 +451,10 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
           uint32_t hi[4], lo[4];
 #pragma unroll
           for (int u4 = 0; u4 < 4; ++u4) {
-            const unsigned long long Y = oz_biased(value(p, pr, ks * 32 + hh * 16 + b4 * 4 + u4), sc, bias);
+            const int k = ks * 32 + hh * 16 + b4 * 4 + u4;
+            const bool s1 = k < pr.len1;
+            const double x = (live && k < pr.K) ? (s1 ? b1 : b2)[4 * k] : 0.0;
+            const unsigned long long Y = oz_biased(x, s1 ? sc1 : sc2, bias);
             lo[u4] = (uint32_t)Y;
             hi[u4] = (uint32_t)(Y >> 32);
           }
@@ -479,16 +476,22 @@ __global__ void __launch_bounds__(256, 2) k_oz_prep(OzPrepArgs a, int srow) {
       }
     } else {
       // thread (row, K eighth kq): four values of every K step, one 32-bit word per slice
-      // (the synthesis has few K steps per counter)
+      // (the synthesis has few K steps per counter); slot k reads complex element kx[p][k]
       for (int p = 0; p < 2; ++p) {
         const OzProb pr = a.probs[(TYPE * a.NM + c) * 2 + p];
         if (pr.nchunk == 0) continue;
         int8_t* Ablk = a.A + pr.aofs + (size_t)zb * pr.nks * S * 4096;
         for (int ks = 0; ks < pr.nks; ++ks) {
+          const int kb = ks * 32 + kq * 4;
+          const int4 k4 = *(const int4*)&kx[p][kb];
+          const int ke[4] = {k4.x, k4.y, k4.z, k4.w};
           uint32_t hi[4], lo[4];
 #pragma unroll
           for (int u4 = 0; u4 < 4; ++u4) {
-            const unsigned long long Y = oz_biased(value(p, pr, ks * 32 + kq * 4 + u4), sc, bias);
+            const int k = kb + u4;
+            const bool s1 = k < pr.len1;
+            const double x = (live && k < pr.K) ? (s1 ? src1 : src2)[2 * ke[u4]] : 0.0;
+            const unsigned long long Y = oz_biased(x, s1 ? sc1 : sc2, bias);
             lo[u4] = (uint32_t)Y;
             hi[u4] = (uint32_t)(Y >> 32);
           }
