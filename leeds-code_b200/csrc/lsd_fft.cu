@@ -40,6 +40,7 @@ struct FFTPlanDev {
   const double2* tw2;  // e^{+2 pi i k/P2}, k < P2
   const double2* twh;  // e^{+2 pi i k/Ph}, k < Ph
   const int* thm;      // m-counter -> bin
+  const int* bin2c;    // bin -> m-counter (M entries)
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -221,16 +222,21 @@ __device__ __forceinline__ void rdft(double2 (&x)[N], const double2* w) {
 // Per-CTA shared tables of one transform length P2 = E G:
 //   tw[t1 G + k1] = e^{+2 pi i t1 k1 / P2}   column-pass twiddles (read by consecutive k1)
 //   twE[j] = e^{+2 pi i j / E},  twG[j] = e^{+2 pi i j / G}   register-DFT twiddles
-//   thm[c] = FFT bin of m-counter c
+//   twh[k] = e^{+2 pi i k / Ph}, k < P2      real-FFT packing / unpacking twiddles
+//   thm[c] = FFT bin of m-counter c,  b2c[b] = m-counter of bin b < M
+// (in shared memory, so that no load of the packing, gathering or unpacking waits on
+// another global load)
 struct FFTTabs {
   double2* tw;
   double2* twE;
   double2* twG;
+  double2* twh;
   int* thm;
+  int* b2c;
 };
 
 __host__ __device__ __forceinline__ size_t fft_tab_bytes(int P2, int E, int G, int NM) {
-  return sizeof(double2) * ((size_t)P2 + E + G) + sizeof(int) * (size_t)((NM + 3) & ~3);
+  return sizeof(double2) * (2 * (size_t)P2 + E + G) + sizeof(int) * (size_t)(((NM + 3) & ~3) + ((P2 + 3) & ~3));
 }
 
 // carve the tables out of `base` (16-byte aligned) and fill them; ends with a barrier
@@ -240,11 +246,15 @@ __device__ __forceinline__ FFTTabs fft_tabs_init(unsigned char* base, const FFTP
   t.tw = (double2*)base;
   t.twE = t.tw + E * G;
   t.twG = t.twE + E;
-  t.thm = (int*)(t.twG + G);
+  t.twh = t.twG + G;
+  t.thm = (int*)(t.twh + E * G);
+  t.b2c = t.thm + ((pl.NM + 3) & ~3);
   for (int i = threadIdx.x; i < E * G; i += blockDim.x) t.tw[i] = __ldg(&pl.tw2[(i / G) * (i % G)]);
   for (int i = threadIdx.x; i < E; i += blockDim.x) t.twE[i] = __ldg(&pl.tw2[G * i]);
   for (int i = threadIdx.x; i < G; i += blockDim.x) t.twG[i] = __ldg(&pl.tw2[E * i]);
+  for (int i = threadIdx.x; i < E * G; i += blockDim.x) t.twh[i] = __ldg(&pl.twh[i]);
   for (int i = threadIdx.x; i < pl.NM; i += blockDim.x) t.thm[i] = __ldg(&pl.thm[i]);
+  for (int i = threadIdx.x; i < pl.M; i += blockDim.x) t.b2c[i] = __ldg(&pl.bin2c[i]);
   __syncthreads();
   return t;
 }
@@ -297,21 +307,21 @@ __device__ __forceinline__ void row_pass(double2* rows, int nrows, const FFTTabs
 
 // Half-spectrum packing for the c2r: Z[k] from Y[k] and conj(Y[P2-k]) (Y[P2] = Nyquist = 0;
 // the imaginary part of the DC bin is ignored).
-__device__ __forceinline__ double2 c2r_pack(int k, double2 yk, double2 ymk, const FFTPlanDev& pl) {
+__device__ __forceinline__ double2 c2r_pack(int k, double2 yk, double2 ymk, const double2* twh) {
   const double2 yc = conj2(ymk);
   if (k == 0) yk.y = 0.0;
   const double2 s = add2(yk, yc), d = sub2(yk, yc);
-  const double2 wd = cmul(__ldg(&pl.twh[k]), d);
+  const double2 wd = cmul(twh[k], d);
   return make_double2(s.x - wd.y, s.y + wd.x);  // s + i w d
 }
 // Bin k < P2 of the real spectrum from Z[k] and Z[P2-k] (Z[0] for k = 0).
-__device__ __forceinline__ double2 r2c_unpack(int k, double2 zk, double2 zmk, const FFTPlanDev& pl) {
+__device__ __forceinline__ double2 r2c_unpack(int k, double2 zk, double2 zmk, const double2* twh) {
   if (k == 0) return make_double2(zk.x + zk.y, 0.0);
   const double2 zc = conj2(zmk);
   const double2 A = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
   const double2 Bi = make_double2(0.5 * (zk.x - zc.x), 0.5 * (zk.y - zc.y));  // i B
   const double2 B = make_double2(Bi.y, -Bi.x);
-  return add2(A, cmulc(B, __ldg(&pl.twh[k])));
+  return add2(A, cmulc(B, twh[k]));
 }
 
 // theta row of half-row h on side 0 (south) / 1 (north)
@@ -334,8 +344,8 @@ __device__ __forceinline__ void stage_elem(double2* sp, const cplx* blk, const F
 
 // bin b < M of a transformed row (natural order, padded) as a real-spectrum bin
 template <int G>
-__device__ __forceinline__ double2 row_unpack(const double2* row, int b, const FFTPlanDev& pl) {
-  return r2c_unpack(b, row[ppos<G>(b)], row[ppos<G>(b == 0 ? 0 : pl.P2 - b)], pl);
+__device__ __forceinline__ double2 row_unpack(const double2* row, int b, int P2, const double2* twh) {
+  return r2c_unpack(b, row[ppos<G>(b)], row[ppos<G>(b == 0 ? 0 : P2 - b)], twh);
 }
 
 // ---- fused: theta-Fourier inputs -> products -> theta-Fourier outputs ---------------------
@@ -370,7 +380,6 @@ struct ProdConst {
   const double* r;    // [7][N] powers of r
   const double* ref;  // [7][N] reference state (anelastic)
   unsigned long long* cflmax;  // variable dt: per-shell CFL maxima [N][2] (bits of doubles >= 0), or null
-  const int* bin2c;   // FFT bin -> m-counter (M entries)
   double* rotsum;     // inner-core rotation: per half-row h the two torque surface sums of
                       // shell 0 at [2 h], [2 h + 1] (k_rot adds them up), or null
   const double* gwP0; // Gauss weight x P_0^0 / 2 per theta row
@@ -506,8 +515,8 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
   // thread keep their loads in flight.
   constexpr int KH = P2 / 2 + 1, U = 3, NITEM = NF_IN * KH;
   auto put = [&](int row, int k, double2 yk, double2 ym) {
-    rows[(size_t)row * RS + ppos<G>(k)] = c2r_pack(k, yk, ym, pl);
-    if (k != 0 && 2 * k != P2) rows[(size_t)row * RS + ppos<G>(P2 - k)] = c2r_pack(P2 - k, ym, yk, pl);
+    rows[(size_t)row * RS + ppos<G>(k)] = c2r_pack(k, yk, ym, tabs.twh);
+    if (k != 0 && 2 * k != P2) rows[(size_t)row * RS + ppos<G>(P2 - k)] = c2r_pack(P2 - k, ym, yk, tabs.twh);
   };
   for (int it0 = tid; it0 < NITEM; it0 += U * PROD_THREADS) {
     double2 e0[U], o0[U], e1[U], o1[U];
@@ -519,11 +528,11 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
         const int f = it / KH, k = it - f * KH, km = k == 0 ? P2 : P2 - k;
         const cplx* src = four_in + (size_t)pc.fin[f] * fstride + boff;
         if (k < M) {
-          const int c = __ldg(pc.bin2c + k);
+          const int c = tabs.b2c[k];
           e0[u] = src[4 * c]; o0[u] = src[4 * c + 2];
         }
         if (km < M) {
-          const int c = __ldg(pc.bin2c + km);
+          const int c = tabs.b2c[km];
           e1[u] = src[4 * c]; o1[u] = src[4 * c + 2];
         }
       }
@@ -549,7 +558,7 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
         const int b = q ? km : k;
         te[q] = to[q] = pe[q] = po[q] = make_double2(0.0, 0.0);
         if (b < M) {
-          const int c = __ldg(pc.bin2c + b);
+          const int c = tabs.b2c[b];
           te[q] = sth[4 * c]; to[q] = sth[4 * c + 2]; pe[q] = sph[4 * c]; po[q] = sph[4 * c + 2];
         }
       }
@@ -664,8 +673,8 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
   for (int i = tid; i < NF_OUT * NE; i += PROD_THREADS) {
     const int q = i / NE, e = i - q * NE, c = e >> 1, p = e & 1;
     const int b = tabs.thm[c];
-    const double2 xs = row_unpack<G>(rows + (size_t)(q * 2) * RS, b, pl);
-    const double2 xn = row_unpack<G>(rows + (size_t)(q * 2 + 1) * RS, b, pl);
+    const double2 xs = row_unpack<G>(rows + (size_t)(q * 2) * RS, b, P2, tabs.twh);
+    const double2 xn = row_unpack<G>(rows + (size_t)(q * 2 + 1) * RS, b, P2, tabs.twh);
     double2 val = p == 0 ? add2(xs, xn) : sub2(xs, xn);
     if (p == 0 && equator) { val.x *= 0.5; val.y *= 0.5; }
     four_out[(size_t)q * fstride + four_off_a(n, c, p, h, N, Th2)] = val;
@@ -688,7 +697,7 @@ __global__ void __launch_bounds__(128) k_c2r(FFTPlanDev pl, int N, const cplx* f
   __syncthreads();
   for (int i = threadIdx.x; i < 4 * P2; i += blockDim.x) {
     const int r = i / P2, k = i - r * P2;
-    rows[r * RS + ppos<G>(k)] = c2r_pack(k, row_bin(sp, k, r >> 1, r & 1, M), row_bin(sp, k == 0 ? P2 : P2 - k, r >> 1, r & 1, M), pl);
+    rows[r * RS + ppos<G>(k)] = c2r_pack(k, row_bin(sp, k, r >> 1, r & 1, M), row_bin(sp, k == 0 ? P2 : P2 - k, r >> 1, r & 1, M), tabs.twh);
   }
   __syncthreads();
   col_pass<E, G, +1>(rows, 4, tabs);
@@ -737,8 +746,8 @@ __global__ void __launch_bounds__(128) k_r2c(FFTPlanDev pl, int N, const double*
   for (int i = threadIdx.x; i < NM * 2; i += blockDim.x) {
     const int c = i >> 1, q = i & 1, hh = 2 * hb + q, b = tabs.thm[c];
     if (hh >= Th2) continue;
-    const double2 xs = row_unpack<G>(rows + (2 * q) * RS, b, pl);
-    const double2 xn = row_unpack<G>(rows + (2 * q + 1) * RS, b, pl);
+    const double2 xs = row_unpack<G>(rows + (2 * q) * RS, b, P2, tabs.twh);
+    const double2 xn = row_unpack<G>(rows + (2 * q + 1) * RS, b, P2, tabs.twh);
     double2 ev = add2(xs, xn);
     if ((Th & 1) && hh == Th2 - 1) { ev.x *= 0.5; ev.y *= 0.5; }
     fld[four_off_a(n, c, 0, hh, N, Th2)] = ev;
@@ -776,7 +785,7 @@ FFTPlanDev make_plan(lsd_ctx* ctx) {
   FFTPlanDev pl;
   pl.P2 = ctx->P2; pl.Ph = ctx->Ph; pl.M = ctx->M; pl.NM = ctx->NM; pl.Th = ctx->Th; pl.Th2 = ctx->Th2;
   pl.HB = ctx->HB; pl.Mp = ctx->Mp;
-  pl.tw2 = ctx->d_tw2; pl.twh = ctx->d_twh; pl.thm = ctx->d_thm;
+  pl.tw2 = ctx->d_tw2; pl.twh = ctx->d_twh; pl.thm = ctx->d_thm; pl.bin2c = ctx->d_bin2c;
   return pl;
 }
 
@@ -940,7 +949,6 @@ int lsd_launch_products(lsd_ctx* ctx, const cplx* four_in, cplx* four_out) {
   pc.r = ctx->d_r;
   pc.ref = ctx->d_ref;
   pc.L = ctx->L;
-  pc.bin2c = ctx->d_bin2c;
   pc.cflmax = c.timestep < 0 ? (unsigned long long*)ctx->d_cfl : nullptr;
   pc.rotsum = c.rot_tstep ? ctx->d_rot + ROT_NSLOT : nullptr;
   pc.gwP0 = ctx->d_gwP0;
