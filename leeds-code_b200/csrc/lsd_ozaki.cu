@@ -522,20 +522,37 @@ struct OzGemmArgs {
   int* err;
   int nst;          // stages of the bulk-copy ring
   int pair_digits;  // the launch's diagonal bound allows D_2i 256 + D_2i+1 in int32
+  int wide_sum;     // ... and the whole sum over the diagonals in int64 (oz_combine)
 };
 
-// The exact integer sum_d D_d 256^(S-1-d) of one accumulator column (|sum| < 2^53, so
-// every partial sum below is exact in FP64).  pair: two diagonals per int32 (D_2i 256 +
-// D_2i+1, which the host has bounded below 2^31), joined in FP64 by 2^16 steps; half as
-// many int32 -> FP64 conversions as one diagonal at a time.
 // one 32-byte store of two complex values (p 32-byte aligned)
 __device__ __forceinline__ void st_global_2c(cplx* p, double2 a, double2 b) {
   asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
                : "memory");
 }
 
+// The integer sum_d D_d 256^(S-1-d) of one accumulator column.  wide (the host's bound
+// on the sum is below 2^62): formed exactly in int64 and converted once (exact while
+// |sum| < 2^53, one rounding beyond); else a Horner sum in FP64 (exact below 2^53).
+// pair: two diagonals per int32 first (D_2i 256 + D_2i+1, which the host has bounded
+// below 2^31), then 2^16 steps: half the steps, and in FP64 half the conversions.
 template <int S>
-__device__ __forceinline__ double oz_combine(const int32_t (&v)[S][8], int q, bool pair) {
+__device__ __forceinline__ double oz_combine(const int32_t (&v)[S][8], int q, bool pair, bool wide) {
+  if (wide) {
+    long long h;
+    if (pair) {
+      h = (long long)(v[0][q] * 256 + v[1][q]);
+#pragma unroll
+      for (int d = 2; d < S; d += 2)
+        if (d + 1 < S) h = h * 65536 + (long long)(v[d][q] * 256 + v[d + 1][q]);
+        else h = h * 256 + (long long)v[d][q];
+    } else {
+      h = (long long)v[0][q];
+#pragma unroll
+      for (int d = 1; d < S; ++d) h = h * 256 + (long long)v[d][q];
+    }
+    return (double)h;
+  }
   double h;
   if (pair) {
     h = (double)(v[0][q] * 256 + v[1][q]);
@@ -671,7 +688,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
     // the 8 complex values go straight to HBM.
     const int row = tid & 127, half = tid >> 7, odd = row & 1;
     const uint32_t tlane = (uint32_t)(32 * (warp & 3)) << 16;
-    const bool pair = a.pair_digits != 0;
+    const bool pair = a.pair_digits != 0, wide = a.wide_sum != 0;
     int cc = 0;
     OzProb nxt = prob(blockIdx.x);
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
@@ -719,7 +736,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
           }
           double h[8];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) h[q] = oz_combine<S>(v, q, pair) * (rsc * cs[8 * g8 + q]);
+          for (int q = 0; q < 8; ++q) h[q] = oz_combine<S>(v, q, pair, wide) * (rsc * cs[8 * g8 + q]);
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const double r = __shfl_xor_sync(0xffffffffu, odd ? h[q] : h[q + 4], 1);
@@ -786,6 +803,7 @@ struct OzState {
   int ctas = 2;          // persistent GEMM CTAs per SM
   int srow[2] = {1, 1};  // pre-pass stage row length (odd, in complex): synthesis, analysis
   int pair[OZ_NTYPE] = {};  // per type: the epilogue may join diagonals in pairs (oz_combine)
+  int wide[OZ_NTYPE] = {};  // per type: ... and sum them in int64
 };
 
 namespace {
@@ -900,6 +918,9 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
     bool pair_ok = true;
     for (int d = 0; d + 1 < S; d += 2) pair_ok = pair_ok && 256 * bound(d) + bound(d + 1) < (1LL << 31);
     o->pair[type] = pair_ok ? 1 : 0;
+    double total = 0.0;  // bound on |sum_d D_d 256^(S-1-d)|
+    for (int d = 0; d < S; ++d) total += (double)bound(d) * std::ldexp(1.0, 8 * (S - 1 - d));
+    o->wide[type] = total < std::ldexp(1.0, 62) ? 1 : 0;
   }
   // ring stages: as many (2..4) as keep two CTAs per SM (<= 78 KiB of stages each)
   lsd_ozaki_default_tiles(S, &o->nst, &o->ctas);
@@ -967,6 +988,7 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   ga.rows_per_group = rpg; ga.probs = o->d_probs; ga.A = o->d_A; ga.B = o->d_B; ga.fexp = o->d_fexp;
   ga.erow = o->d_erow; ga.nhlist = o->d_nh; ga.hm = ctx->d_m; ga.err = o->d_err; ga.nst = o->nst;
   ga.pair_digits = o->pair[TYPE];
+  ga.wide_sum = o->wide[TYPE];
   for (int i = 0; i < OZ_MAXG; ++i) {
     const bool on = i < ng;
     pa.in0[i] = on ? gs[i].in0 : nullptr; pa.in1[i] = on ? gs[i].in1 : nullptr;
