@@ -324,6 +324,12 @@ __device__ __forceinline__ double2 r2c_unpack(int k, double2 zk, double2 zmk, co
   return add2(A, cmulc(B, twh[k]));
 }
 
+// one 32-byte store of two complex values (p 32-byte aligned)
+__device__ __forceinline__ void st_global_2c(cplx* p, double2 a, double2 b) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
+               : "memory");
+}
+
 // theta row of half-row h on side 0 (south) / 1 (north)
 __device__ __forceinline__ int row_theta(int h, int side, int Th) { return side ? Th - 1 - h : h; }
 
@@ -497,7 +503,7 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
   const int BLK = NM * 4;                        // one field's (n, h/2) block
   const size_t fstride = (size_t)N * pl.HB * BLK;
   const size_t boff = ((size_t)n * pl.HB + hb) * BLK + jj;  // element (c, p) at boff + 2 (2c + p)
-  const int tid = threadIdx.x, NE = NM * 2;                 // (c, p) elements of this half-row
+  const int tid = threadIdx.x;
   ShellC sh{};
   if constexpr (PS >= PS_ANEL_MOM) {
     const double* ref = pc.ref;
@@ -668,16 +674,18 @@ __global__ void __launch_bounds__(PROD_THREADS, 2) k_products(FFTPlanDev pl, int
   __syncthreads();
   col_pass<E, G, -1>(rows, NF_OUT * 2, tabs);
   __syncthreads();
-  // ---- unpack bins, fold south/north into E/O, store
+  // ---- unpack bins, fold south/north into E/O, store: a thread per (output, counter)
+  // unpacks both rows once and writes the (E, O) pair, neighbours in four_off_a, with one
+  // 32-byte store (the field bases are 32-byte aligned)
   const bool equator = (Th & 1) && h == Th2 - 1;  // odd Th: the equator row is counted once
-  for (int i = tid; i < NF_OUT * NE; i += PROD_THREADS) {
-    const int q = i / NE, e = i - q * NE, c = e >> 1, p = e & 1;
+  for (int i = tid; i < NF_OUT * NM; i += PROD_THREADS) {
+    const int q = i / NM, c = i - q * NM;
     const int b = tabs.thm[c];
     const double2 xs = row_unpack<G>(rows + (size_t)(q * 2) * RS, b, P2, tabs.twh);
     const double2 xn = row_unpack<G>(rows + (size_t)(q * 2 + 1) * RS, b, P2, tabs.twh);
-    double2 val = p == 0 ? add2(xs, xn) : sub2(xs, xn);
-    if (p == 0 && equator) { val.x *= 0.5; val.y *= 0.5; }
-    four_out[(size_t)q * fstride + four_off_a(n, c, p, h, N, Th2)] = val;
+    double2 ev = add2(xs, xn);
+    if (equator) { ev.x *= 0.5; ev.y *= 0.5; }
+    st_global_2c(four_out + (size_t)q * fstride + four_off_a(n, c, 0, h, N, Th2), ev, sub2(xs, xn));
   }
 }
 
