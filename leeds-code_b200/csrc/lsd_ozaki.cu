@@ -795,8 +795,17 @@ struct OzState {
   int* d_nh = nullptr;
   int8_t* d_B = nullptr;
   int* d_fexp = nullptr;
-  int8_t* d_A = nullptr;  // data digits, shared by every launch (stream ordered)
-  int* d_erow = nullptr;  // row exponents [c][rows]
+  // data digits and row exponents [c][rows], one buffer per concurrent chain: synthesis
+  // VEC / P / GRAD and analysis ST / Q run as forked branches (buffer 0: VEC, ST; 1: P, Q;
+  // 2: GRAD), the two phases never at once
+  int8_t* d_A[3] = {};
+  int* d_erow[3] = {};
+  // per stream that launches a contraction (the context's stream, or a graph-capture
+  // stream): two more streams and the fork / join events of its branches.  A stream that
+  // joined one capture stays in it until that capture ends, so nested captures need
+  // streams of their own.
+  struct Aux { cudaStream_t origin; cudaStream_t s[2]; cudaEvent_t fork, join[2]; };
+  std::vector<Aux> aux;
   int* d_err = nullptr;
   size_t smem = 0;
   int nst = 2;           // GEMM ring stages
@@ -808,6 +817,9 @@ struct OzState {
 
 namespace {
 constexpr int OZ_MAXG_SYNTH = OZ_MAXG, OZ_MAXG_ANAL = 4;  // groups per launch
+
+// the digit / exponent buffer of each type's chain
+int oz_buf(int type) { return type == OZ_VEC || type == OZ_ST ? 0 : type == OZ_P || type == OZ_Q ? 1 : 2; }
 
 // f(k_oz_gemm<TYPE, S>) for the runtime slice count S
 template <int TYPE, class F>
@@ -833,9 +845,17 @@ void oz_set_smem(int S, size_t smem) {
 void lsd_ozaki_free(lsd_ctx* ctx) {
   OzState* o = (OzState*)ctx->oz;
   if (!o) return;
-  void* ptrs[] = {o->d_probs, o->d_kidx, o->d_nh, o->d_B, o->d_fexp, o->d_A, o->d_erow, o->d_err};
+  void* ptrs[] = {o->d_probs, o->d_kidx, o->d_nh, o->d_B, o->d_fexp, o->d_A[0], o->d_A[1], o->d_A[2],
+                  o->d_erow[0], o->d_erow[1], o->d_erow[2], o->d_err};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  for (OzState::Aux& x : o->aux) {
+    for (int i = 0; i < 2; ++i) {
+      if (x.s[i]) cudaStreamDestroy(x.s[i]);
+      if (x.join[i]) cudaEventDestroy(x.join[i]);
+    }
+    if (x.fork) cudaEventDestroy(x.fork);
+  }
   delete o;
   ctx->oz = nullptr;
 }
@@ -857,7 +877,7 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
     }
   std::vector<int> kidx, nhl;
   std::vector<OzProb> probs((size_t)OZ_NTYPE * NM * 2);
-  long long bbytes = 0, abytes_max = 0;
+  long long bbytes = 0, abytes_t[OZ_NTYPE] = {};
   int fofs = 0;
   for (int type = 0; type < OZ_NTYPE; ++type) {
     const bool anal = type >= OZ_ST;
@@ -901,7 +921,7 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
         if (pr.nchunk) abytes += (long long)o->nzb_max[type] * pr.nks * S * 4096;
         probs[((size_t)type * NM + c) * 2 + p] = pr;
       }
-    abytes_max = std::max(abytes_max, abytes);
+    abytes_t[type] = abytes;
     // digit products bound the diagonals: |D_d| <= K sum_{s+t=d} m_s m_t with m_0 = 65 (the
     // top digit) and m_s = 128 below it; pairs need 256 |D_2i| + |D_2i+1| < 2^31
     long long kmax = 0;
@@ -944,10 +964,17 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
   CUDA_TRY(cudaMemcpyAsync(o->d_nh, nhl.data(), sizeof(int) * nhl.size(), cudaMemcpyHostToDevice, ctx->stream));
   CUDA_TRY(cudaMalloc(&o->d_B, std::max<long long>(bbytes, 16)));
   CUDA_TRY(cudaMalloc(&o->d_fexp, sizeof(int) * (size_t)std::max(fofs, 1)));
-  CUDA_TRY(cudaMalloc(&o->d_A, std::max<long long>(abytes_max, 16)));
-  int max_rows = 0;
-  for (int type = 0; type < OZ_NTYPE; ++type) max_rows = std::max(max_rows, o->nzb_max[type] * 128);
-  CUDA_TRY(cudaMalloc(&o->d_erow, sizeof(int) * (size_t)NM * max_rows));
+  for (int b = 0; b < 3; ++b) {  // the buffers of the chains (oz_buf)
+    long long ab = 16;
+    int rows = 128;
+    for (int type = 0; type < OZ_NTYPE; ++type)
+      if (oz_buf(type) == b) {
+        ab = std::max(ab, abytes_t[type]);
+        rows = std::max(rows, o->nzb_max[type] * 128);
+      }
+    CUDA_TRY(cudaMalloc(&o->d_A[b], ab));
+    CUDA_TRY(cudaMalloc(&o->d_erow[b], sizeof(int) * (size_t)NM * rows));
+  }
   CUDA_TRY(cudaMalloc(&o->d_err, sizeof(int)));
   CUDA_TRY(cudaMemsetAsync(o->d_err, 0, sizeof(int), ctx->stream));
   OzTabArgs ta;
@@ -973,20 +1000,21 @@ namespace {
 struct OzLaunchGroup { const cplx* in0; const cplx* in1; cplx* out0; cplx* out1; int zero_m0_im; };
 
 template <int TYPE>
-int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
+int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng, cudaStream_t stream) {
   OzState* o = (OzState*)ctx->oz;
+  const int buf = oz_buf(TYPE);
   constexpr int PER = OzT<TYPE>::per;
   const int rpg = PER * ctx->N, nrows = ng * rpg, nzb = ceil_div(nrows, 128);
   if (nzb > o->nzb_max[TYPE]) return lsd_fail(ctx, LSD_EARG, "tensor-core contraction: too many groups in one launch");
   OzPrepArgs pa;
   pa.N = ctx->N; pa.H = ctx->H; pa.NM = ctx->NM; pa.Th2 = ctx->Th2; pa.HB = ctx->HB; pa.S = o->S; pa.nrows = nrows;
   pa.rows_per_group = rpg; pa.probs = o->d_probs; pa.kidx = o->d_kidx; pa.mstart = ctx->d_mstart;
-  pa.mlen = ctx->d_mlen; pa.rinv = ctx->d_rinv; pa.A = o->d_A; pa.erow = o->d_erow;
+  pa.mlen = ctx->d_mlen; pa.rinv = ctx->d_rinv; pa.A = o->d_A[buf]; pa.erow = o->d_erow[buf];
   pa.err = o->d_err;
   OzGemmArgs ga;
   ga.N = ctx->N; ga.H = ctx->H; ga.NM = ctx->NM; ga.Th2 = ctx->Th2; ga.HB = ctx->HB; ga.S = o->S; ga.nrows = nrows;
-  ga.rows_per_group = rpg; ga.probs = o->d_probs; ga.A = o->d_A; ga.B = o->d_B; ga.fexp = o->d_fexp;
-  ga.erow = o->d_erow; ga.nhlist = o->d_nh; ga.hm = ctx->d_m; ga.err = o->d_err; ga.nst = o->nst;
+  ga.rows_per_group = rpg; ga.probs = o->d_probs; ga.A = o->d_A[buf]; ga.B = o->d_B; ga.fexp = o->d_fexp;
+  ga.erow = o->d_erow[buf]; ga.nhlist = o->d_nh; ga.hm = ctx->d_m; ga.err = o->d_err; ga.nst = o->nst;
   ga.pair_digits = o->pair[TYPE];
   ga.wide_sum = o->wide[TYPE];
   for (int i = 0; i < OZ_MAXG; ++i) {
@@ -1000,7 +1028,7 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   const size_t psm = oz_prep_smem<TYPE>(srow);
   auto go = [&](auto kern) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm);
-    kern<<<pg, 256, psm, ctx->stream>>>(pa, srow);
+    kern<<<pg, 256, psm, stream>>>(pa, srow);
   };
   switch (o->S) {
     case 2: go(k_oz_prep<TYPE, 2>); break;
@@ -1015,7 +1043,7 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->dev);
   const int ntile = ctx->NM * 2 * nzb;
   oz_gemm_dispatch<TYPE>(o->S, [&](auto kern) {
-    kern<<<std::min(ntile, o->ctas * nsm), OZ_THREADS, o->smem, ctx->stream>>>(ga, nzb);
+    kern<<<std::min(ntile, o->ctas * nsm), OZ_THREADS, o->smem, stream>>>(ga, nzb);
   });
   ctx->launches += 2;
   cudaError_t e = cudaGetLastError();
@@ -1024,11 +1052,53 @@ int oz_run(lsd_ctx* ctx, const OzLaunchGroup* gs, int ng) {
 }
 
 template <int TYPE>
-int oz_run_all(lsd_ctx* ctx, const std::vector<OzLaunchGroup>& gs, int maxg) {
+int oz_run_all(lsd_ctx* ctx, const std::vector<OzLaunchGroup>& gs, int maxg, cudaStream_t stream) {
   for (size_t i = 0; i < gs.size(); i += maxg) {
-    int rc = oz_run<TYPE>(ctx, gs.data() + i, (int)std::min<size_t>(maxg, gs.size() - i));
+    int rc = oz_run<TYPE>(ctx, gs.data() + i, (int)std::min<size_t>(maxg, gs.size() - i), stream);
     if (rc) return rc;
   }
+  return LSD_OK;
+}
+
+// the branch streams of ctx->stream (created on first use)
+OzState::Aux* oz_aux(lsd_ctx* ctx) {
+  OzState* o = (OzState*)ctx->oz;
+  for (OzState::Aux& x : o->aux)
+    if (x.origin == ctx->stream) return &x;
+  OzState::Aux x{};
+  x.origin = ctx->stream;
+  bool ok = cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < 2 && ok; ++i)
+    ok = cudaStreamCreateWithFlags(&x.s[i], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&x.join[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {  // release what was made; the caller reports the failure
+    for (int i = 0; i < 2; ++i) {
+      if (x.s[i]) cudaStreamDestroy(x.s[i]);
+      if (x.join[i]) cudaEventDestroy(x.join[i]);
+    }
+    if (x.fork) cudaEventDestroy(x.fork);
+    return nullptr;
+  }
+  o->aux.push_back(x);  // the pointer below is used before the next push
+  return &o->aux.back();
+}
+
+// fn(main, branch 0, branch 1) launches the chains; the branches start after everything
+// queued on ctx->stream so far, and ctx->stream waits for both at the end
+template <class F>
+int oz_forked(lsd_ctx* ctx, F&& fn) {
+  OzState::Aux* x = oz_aux(ctx);
+  if (!x) return lsd_fail(ctx, LSD_ECUDA, "tensor-core contraction: branch streams");
+  cudaStream_t s0 = ctx->stream;
+  CUDA_TRY(cudaEventRecord(x->fork, s0));
+  for (int i = 0; i < 2; ++i) CUDA_TRY(cudaStreamWaitEvent(x->s[i], x->fork, 0));
+  int rc = fn(s0, x->s[0], x->s[1]);
+  for (int i = 0; i < 2; ++i) {  // join also after an error, so that no branch is left open
+    cudaEventRecord(x->join[i], x->s[i]);
+    cudaStreamWaitEvent(s0, x->join[i], 0);
+  }
+  if (rc) return rc;
+  CUDA_TRY(cudaGetLastError());
   return LSD_OK;
 }
 
@@ -1058,11 +1128,13 @@ int lsd_ozaki_launch_synth(lsd_ctx* ctx, const SynthGroup* groups, int ngroups) 
         break;
     }
   }
-  int rc;
-  if ((rc = oz_run_all<OZ_VEC>(ctx, gv, OZ_MAXG_SYNTH))) return rc;
-  if ((rc = oz_run_all<OZ_P>(ctx, gp, OZ_MAXG_SYNTH))) return rc;
-  if ((rc = oz_run_all<OZ_GRAD>(ctx, gg, OZ_MAXG_SYNTH))) return rc;
-  return LSD_OK;
+  // three independent chains (slicing pass -> GEMM each) on forked branches
+  return oz_forked(ctx, [&](cudaStream_t s0, cudaStream_t s1, cudaStream_t s2) {
+    int rc = oz_run_all<OZ_VEC>(ctx, gv, OZ_MAXG_SYNTH, s0);
+    if (!rc) rc = oz_run_all<OZ_P>(ctx, gp, OZ_MAXG_SYNTH, s1);
+    if (!rc) rc = oz_run_all<OZ_GRAD>(ctx, gg, OZ_MAXG_SYNTH, s2);
+    return rc;
+  });
 }
 
 int lsd_ozaki_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
@@ -1076,10 +1148,11 @@ int lsd_ozaki_launch_anal(lsd_ctx* ctx, const AnalGroup* groups, int ngroups) {
       gq.push_back({G.in[0], nullptr, G.out[0], nullptr, 1});
     }
   }
-  int rc;
-  if ((rc = oz_run_all<OZ_ST>(ctx, gs, OZ_MAXG_ANAL))) return rc;
-  if ((rc = oz_run_all<OZ_Q>(ctx, gq, OZ_MAXG_ANAL))) return rc;
-  return LSD_OK;
+  return oz_forked(ctx, [&](cudaStream_t s0, cudaStream_t s1, cudaStream_t) {
+    int rc = oz_run_all<OZ_ST>(ctx, gs, OZ_MAXG_ANAL, s0);
+    if (!rc) rc = oz_run_all<OZ_Q>(ctx, gq, OZ_MAXG_ANAL, s1);
+    return rc;
+  });
 }
 
 int* lsd_ozaki_err_flag(lsd_ctx* ctx) { return ((OzState*)ctx->oz)->d_err; }
