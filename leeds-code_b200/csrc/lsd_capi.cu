@@ -30,6 +30,13 @@ void free_ctx(lsd_ctx* ctx) {
   if (ctx->g_step) cudaGraphExecDestroy(ctx->g_step);
   for (cudaStream_t cs : ctx->cap_stream)
     if (cs) cudaStreamDestroy(cs);
+  for (lsd_ctx::Aux& x : ctx->eval_aux) {
+    for (int i = 0; i < 2; ++i) {
+      cudaStreamDestroy(x.s[i]);
+      cudaEventDestroy(x.join[i]);
+    }
+    cudaEventDestroy(x.fork);
+  }
   lsd_ozaki_free(ctx);
   void* ptrs[] = {ctx->d_sblk_l, ctx->d_sblk_nh, ctx->d_aperm, ctx->d_l, ctx->d_m, ctx->d_s, ctx->d_mc, ctx->d_mstart, ctx->d_mlen, ctx->d_thm, ctx->d_bin2c, ctx->d_lm2nh,
                   ctx->d_leg, ctx->d_gp, ctx->d_gw, ctx->d_sn, ctx->d_sn1, ctx->d_tw2, ctx->d_twh, ctx->d_r,

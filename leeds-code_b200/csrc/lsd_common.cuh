@@ -190,6 +190,11 @@ struct lsd_ctx {
   int* d_opfail = nullptr;
   cudaGraphExec_t g_step = nullptr;
   cudaStream_t cap_stream[2] = {nullptr, nullptr};
+  // per stream that launches an evaluation (the context's stream, or a graph-capture
+  // stream): two branch streams and the fork / join events of the spectral preparation's
+  // independent chains (a stream that joined one capture stays in it until it ends)
+  struct Aux { cudaStream_t origin; cudaStream_t s[2]; cudaEvent_t fork, join[2]; };
+  std::vector<Aux> eval_aux;
   long long k_begin = 0, k_loop = 0, k_rebuild = 0, k_corr = 0;
   void* oz = nullptr;  // tensor-core path state (lsd_ozaki.cu)
   // tunables besides fftE / fftG and the GEMM tiles (lsd_tune.cu)

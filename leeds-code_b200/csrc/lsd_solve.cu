@@ -921,6 +921,30 @@ StepArgs step_args(lsd_ctx* ctx) {
 // One nonlinear evaluation: main.F90:102-124 for Boussinesq MHD + codensity.
 int lsd_eval(lsd_ctx* ctx) { return lsd_eval_marked(ctx, nullptr); }
 
+namespace {
+// the evaluation's branch streams of ctx->stream (created on first use), or null
+lsd_ctx::Aux* eval_aux(lsd_ctx* ctx) {
+  for (lsd_ctx::Aux& x : ctx->eval_aux)
+    if (x.origin == ctx->stream) return &x;
+  lsd_ctx::Aux x{};
+  x.origin = ctx->stream;
+  bool ok = cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < 2 && ok; ++i)
+    ok = cudaStreamCreateWithFlags(&x.s[i], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&x.join[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    for (int i = 0; i < 2; ++i) {
+      if (x.s[i]) cudaStreamDestroy(x.s[i]);
+      if (x.join[i]) cudaEventDestroy(x.join[i]);
+    }
+    if (x.fork) cudaEventDestroy(x.fork);
+    return nullptr;
+  }
+  ctx->eval_aux.push_back(x);  // the pointer below is used before the next push
+  return &ctx->eval_aux.back();
+}
+}  // namespace
+
 // marks (optional): 5 events recorded after the spectral preparation, the synthesis, the
 // FFT+products, the analysis and the tail
 int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
@@ -937,18 +961,29 @@ int lsd_eval_marked(lsd_ctx* ctx, cudaEvent_t* marks) {
                                anel ? ctx->d_wts : ctx->d_intr2dr, anel ? 1 : 0, st + LSD_VEL_TOR * F);
     ctx->launches++;
   }
+  // three independent chains on forked branches: u (q, s, t and curl) on s, B on branch 0,
+  // the codensity (and composition) derivatives on branch 1; joined before the synthesis
+  lsd_ctx::Aux* x = eval_aux(ctx);
+  if (!x) return lsd_fail(ctx, LSD_ECUDA, "evaluation: branch streams");
+  CUDA_TRY(cudaEventRecord(x->fork, s));
+  for (int i = 0; i < 2; ++i) CUDA_TRY(cudaStreamWaitEvent(x->s[i], x->fork, 0));
   k_qst<<<g, 128, 0, s>>>(sa, anel ? ctx->d_compr1dr : ctx->d_r1dr, st + LSD_VEL_TOR * F, st + LSD_VEL_POL * F,
                           sp + S_VQ * F, sp + S_VS * F, sp + S_VT * F);
-  k_qst<<<g, 128, 0, s>>>(sa, ctx->d_r1dr, st + LSD_MAG_TOR * F, st + LSD_MAG_POL * F, sp + S_BQ * F, sp + S_BS * F,
-                          sp + S_BT * F);
   k_curl<<<g, 128, 0, s>>>(sa, sp + S_VQ * F, sp + S_VS * F, sp + S_VT * F, sp + S_VCQ * F, sp + S_VCS * F, sp + S_VCT * F);
-  k_curl<<<g, 128, 0, s>>>(sa, sp + S_BQ * F, sp + S_BS * F, sp + S_BT * F, sp + S_BCQ * F, sp + S_BCS * F, sp + S_BCT * F);
-  k_drC<<<g, 128, 0, s>>>(sa, st + LSD_COD_C * F, sp + S_DC * F);
+  k_qst<<<g, 128, 0, x->s[0]>>>(sa, ctx->d_r1dr, st + LSD_MAG_TOR * F, st + LSD_MAG_POL * F, sp + S_BQ * F,
+                                sp + S_BS * F, sp + S_BT * F);
+  k_curl<<<g, 128, 0, x->s[0]>>>(sa, sp + S_BQ * F, sp + S_BS * F, sp + S_BT * F, sp + S_BCQ * F, sp + S_BCS * F,
+                                 sp + S_BCT * F);
+  k_drC<<<g, 128, 0, x->s[1]>>>(sa, st + LSD_COD_C * F, sp + S_DC * F);
   ctx->launches += 5;
   const bool comp = ctx->cfg.comp_tstep != 0;
   if (comp) {  // comp_transform (composition.F90:196-212)
-    k_drC<<<g, 128, 0, s>>>(sa, st + LSD_COMP_C * F, sp + S_DCOMP * F);
+    k_drC<<<g, 128, 0, x->s[1]>>>(sa, st + LSD_COMP_C * F, sp + S_DCOMP * F);
     ctx->launches++;
+  }
+  for (int i = 0; i < 2; ++i) {
+    CUDA_TRY(cudaEventRecord(x->join[i], x->s[i]));
+    CUDA_TRY(cudaStreamWaitEvent(s, x->join[i], 0));
   }
   if (anel) {  // dr q, dr s, dr t (var_coll_TorPol2qstderiv, variables.F90:610-660)
     for (int k = 0; k < 3; ++k) k_drC<<<g, 128, 0, s>>>(sa, sp + (S_VQ + k) * F, sp + (S_VDQ + k) * F);
