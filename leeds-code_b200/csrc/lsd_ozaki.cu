@@ -536,8 +536,8 @@ __device__ __forceinline__ void st_global_2c(cplx* p, double2 a, double2 b) {
 // |sum| < 2^53, one rounding beyond); else a Horner sum in FP64 (exact below 2^53).
 // pair: two diagonals per int32 first (D_2i 256 + D_2i+1, which the host has bounded
 // below 2^31), then 2^16 steps: half the steps, and in FP64 half the conversions.
-template <int S>
-__device__ __forceinline__ double oz_combine(const int32_t (&v)[S][8], int q, bool pair, bool wide) {
+template <int S, int W>
+__device__ __forceinline__ double oz_combine(const int32_t (&v)[S][W], int q, bool pair, bool wide) {
   if (wide) {
     long long h;
     if (pair) {
@@ -722,48 +722,54 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
         }
         umma::fence_after_sync();
         const double* cs = csc[cc & 1] + 16 * half;
-        double2 o[2][4];
+        // groups of CW columns (8 up to five slices, 4 above, to bound the registers); per
+        // group the even lane keeps its first HW columns, the odd lane the last HW
+        constexpr int CW = S <= 5 ? 8 : 4, NGR = 16 / CW, HW = CW / 2;
+        double2 o[NGR][HW];
 #pragma unroll
-        for (int g8 = 0; g8 < 2; ++g8) {
-          int32_t v[S][8];
+        for (int gi = 0; gi < NGR; ++gi) {
+          int32_t v[S][CW];
 #pragma unroll
-          for (int d = 0; d < S; ++d)
-            umma::tmem_ld8(tmem + tlane + (uint32_t)(d * OZ_NC + 16 * half + 8 * g8), v[d]);
+          for (int d = 0; d < S; ++d) {
+            const uint32_t ta = tmem + tlane + (uint32_t)(d * OZ_NC + 16 * half + CW * gi);
+            if constexpr (CW == 8) umma::tmem_ld8(ta, v[d]);
+            else umma::tmem_ld4(ta, v[d]);
+          }
           umma::tmem_wait_ld();
-          if (g8 == 1) {  // all words of this chunk are in registers
+          if (gi == NGR - 1) {  // all words of this chunk are in registers
             umma::fence_before_sync();
             umma::mbar_arrive(&tfree);
           }
-          double h[8];
+          double h[CW];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) h[q] = oz_combine<S>(v, q, pair, wide) * (rsc * cs[8 * g8 + q]);
+          for (int q = 0; q < CW; ++q) h[q] = oz_combine<S, CW>(v, q, pair, wide) * (rsc * cs[CW * gi + q]);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const double r = __shfl_xor_sync(0xffffffffu, odd ? h[q] : h[q + 4], 1);
-            o[g8][q] = odd ? make_double2(r, h[q + 4]) : make_double2(h[q], r);
+          for (int q = 0; q < HW; ++q) {
+            const double r = __shfl_xor_sync(0xffffffffu, odd ? h[q] : h[q + HW], 1);
+            o[gi][q] = odd ? make_double2(r, h[q + HW]) : make_double2(h[q], r);
           }
         }
         if (base) {
 #pragma unroll
-          for (int g8 = 0; g8 < 2; ++g8) {
-            const int k0 = ch * OZ_NC + 16 * half + 8 * g8 + 4 * odd;
+          for (int gi = 0; gi < NGR; ++gi) {
+            const int k0 = ch * OZ_NC + 16 * half + CW * gi + HW * odd;
             if (!OzT<TYPE>::anal) {
               // theta rows j, j + 1 (j even) of one half-row pair are neighbours in four_off:
               // one 32-byte store (the field bases are 32-byte aligned)
 #pragma unroll
-              for (int q = 0; q < 4; q += 2) {
+              for (int q = 0; q < HW; q += 2) {
                 const int j = k0 + q;
                 cplx* dst = base + (size_t)(j >> 1) * a.NM * 4;
-                if (j + 1 < a.Th2) st_global_2c(dst, o[g8][q], o[g8][q + 1]);
-                else if (j < a.Th2) *dst = o[g8][q];
+                if (j + 1 < a.Th2) st_global_2c(dst, o[gi][q], o[gi][q + 1]);
+                else if (j < a.Th2) *dst = o[gi][q];
               }
             } else {
 #pragma unroll
-              for (int q = 0; q < 4; ++q) {
+              for (int q = 0; q < HW; ++q) {
                 const int k = k0 + q;
                 if (k < pr.nk) {
                   const int nh = a.nhlist[pr.nhofs + k];
-                  double2 val = o[g8][q];
+                  double2 val = o[gi][q];
                   // m = 0: s, t (and a scalar) keep no imaginary part; q keeps its own
                   // (transform.fftw3.F90:599, 869, 902, 908)
                   if (zero && a.hm[nh] == 0) val.y = 0.0;
