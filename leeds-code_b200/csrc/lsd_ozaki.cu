@@ -140,7 +140,7 @@ int lsd_umma_selftest(lsd_ctx* ctx, double* maxerr) {
 namespace {
 
 constexpr int OZ_MAXS = 8;       // slices per operand
-constexpr int OZ_NC = 32;        // columns per chunk
+constexpr int OZ_NCMAX = 48;     // columns per chunk: 48 or 32 (oz_nc)
 constexpr int OZ_MAXSTAGES = 4;  // bulk-copy ring: up to 4 stages (default 3 where two CTAs per SM fit)
 constexpr int OZ_EPI = 256;      // epilogue threads: warps 0-7 (warp w: TMEM lane quarter w % 4,
                                  // column half w / 4 of a chunk)
@@ -148,6 +148,14 @@ constexpr int OZ_THREADS = OZ_EPI + 64;  // + warp 8 (bulk copies) and warp 9 (M
 constexpr int OZ_MAXG = 8;       // groups (output fields) of one launch
 
 enum { OZ_VEC = 0, OZ_P = 1, OZ_GRAD = 2, OZ_ST = 3, OZ_Q = 4, OZ_NTYPE = 5 };
+
+// Columns per chunk: 48 for the synthesis types while the S diagonals of a chunk fit the
+// CTA's 256 tensor-memory columns (S <= 5; theta rows come in multiples of 48 at lmax 127
+// and 255, and the largest MMA is N = 240), else 32; the analysis types keep 32 (their
+// columns are the <= 64 harmonics of one (m, parity)).  Fewer, wider MMAs per K step.
+__host__ __device__ constexpr int oz_nc(int type, int S) { return type < OZ_ST && S * 48 <= 256 ? 48 : 32; }
+// bytes of one ring stage (A: S x 4096, B: S slices of NC x 32), the widest chunk's
+constexpr size_t oz_stage_bytes(int S) { return (size_t)S * (4096 + oz_nc(OZ_VEC, S) * 32); }
 
 // per (type, m-counter, parity)
 struct OzProb {
@@ -214,7 +222,8 @@ struct OzTabArgs {
 __global__ void k_oz_tab_synth(OzTabArgs a, int type) {
   const int c = blockIdx.x, p = blockIdx.y;
   const OzProb pr = a.probs[(type * a.NM + c) * 2 + p];
-  for (int j = threadIdx.x; j < pr.nchunk * OZ_NC; j += blockDim.x) {
+  const int NC = oz_nc(type, a.S);
+  for (int j = threadIdx.x; j < pr.nchunk * NC; j += blockDim.x) {
     const bool valid = j < a.Th2;
     double mx = 0.0;
     if (valid)
@@ -224,7 +233,7 @@ __global__ void k_oz_tab_synth(OzTabArgs a, int type) {
       }
     const int e = oz_exponent(mx);
     a.fexp[pr.fofs + j] = e;
-    const int ch = j / OZ_NC, r = j % OZ_NC;
+    const int ch = j / NC, r = j % NC;
     for (int k = 0; k < pr.nks * 32; ++k) {
       int8_t d[OZ_MAXS];
       double v = 0.0;
@@ -234,7 +243,7 @@ __global__ void k_oz_tab_synth(OzTabArgs a, int type) {
       }
       oz_digits(v, e, a.S, d);
       for (int s = 0; s < a.S; ++s)
-        a.B[pr.bofs + (((size_t)ch * pr.nks + k / 32) * a.S + s) * 1024 + umma::tile_off(r, k % 32)] = d[s];
+        a.B[pr.bofs + (((size_t)ch * pr.nks + k / 32) * a.S + s) * (NC * 32) + umma::tile_off(r, k % 32)] = d[s];
     }
   }
 }
@@ -243,7 +252,8 @@ __global__ void k_oz_tab_synth(OzTabArgs a, int type) {
 __global__ void k_oz_tab_anal(OzTabArgs a, int type) {
   const int c = blockIdx.x, p = blockIdx.y;
   const OzProb pr = a.probs[(type * a.NM + c) * 2 + p];
-  for (int k = threadIdx.x; k < pr.nchunk * OZ_NC; k += blockDim.x) {
+  const int NC = oz_nc(type, a.S);
+  for (int k = threadIdx.x; k < pr.nchunk * NC; k += blockDim.x) {
     const bool valid = k < pr.nk;
     const int nh = valid ? a.nhlist[pr.nhofs + k] : 0;
     double mx = 0.0;
@@ -255,7 +265,7 @@ __global__ void k_oz_tab_anal(OzTabArgs a, int type) {
       }
     const int e = oz_exponent(mx);
     a.fexp[pr.fofs + k] = e;
-    const int cb = k / OZ_NC, r = k % OZ_NC;
+    const int cb = k / NC, r = k % NC;
     for (int jj = 0; jj < pr.nks * 32; ++jj) {
       int8_t d[OZ_MAXS];
       double v = 0.0;
@@ -266,7 +276,7 @@ __global__ void k_oz_tab_anal(OzTabArgs a, int type) {
       }
       oz_digits(v, e, a.S, d);
       for (int s = 0; s < a.S; ++s)
-        a.B[pr.bofs + (((size_t)cb * pr.nks + jj / 32) * a.S + s) * 1024 + umma::tile_off(r, jj % 32)] = d[s];
+        a.B[pr.bofs + (((size_t)cb * pr.nks + jj / 32) * a.S + s) * (NC * 32) + umma::tile_off(r, jj % 32)] = d[s];
     }
   }
 }
@@ -585,10 +595,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
   extern __shared__ __align__(1024) uint8_t oz_smem[];
   __shared__ __align__(8) uint64_t full[OZ_MAXSTAGES], empty[OZ_MAXSTAGES], accf, tfree, fin;
   __shared__ uint32_t tbase;
-  __shared__ double csc[2][OZ_NC];  // column scales 2^fexp of a chunk (chunk parity)
+  __shared__ double csc[2][OZ_NCMAX];  // column scales 2^fexp of a chunk (chunk parity)
+  constexpr int NC = oz_nc(TYPE, S), BT = NC * 32;  // chunk columns; bytes of one B slice tile
   const int tid = threadIdx.x, warp = tid >> 5;
   const int ntile = a.NM * 2 * nzb;
-  const uint32_t stage_bytes = (uint32_t)S * 5120;  // A: S x 4096, B: S x 1024
+  const uint32_t stage_bytes = (uint32_t)S * (4096 + BT);  // A: S x 4096, B: S x BT
   const int nst = a.nst;
   if (tid == 0) {
     for (int i = 0; i < nst; ++i) { umma::mbar_init(&full[i], 1); umma::mbar_init(&empty[i], 1); }
@@ -638,7 +649,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
         uint8_t* sA = oz_smem + (size_t)st * stage_bytes;
         umma::mbar_expect_tx(&full[st], stage_bytes);
         umma::bulk_g2s(sA, Ablk + (size_t)ks * S * 4096, (uint32_t)S * 4096, &full[st]);
-        umma::bulk_g2s(sA + (size_t)S * 4096, Bblk + ((size_t)ch * pr.nks + ks) * S * 1024, (uint32_t)S * 1024,
+        umma::bulk_g2s(sA + (size_t)S * 4096, Bblk + ((size_t)ch * pr.nks + ks) * S * BT, (uint32_t)S * BT,
                        &full[st]);
       }
     }
@@ -646,10 +657,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
     for (int j = (it > nst ? it - nst : 0); j < it; ++j)
       umma::mbar_wait(&full[j % nst], (j / nst) & 1, WAIT_ITERS);
   } else if (tid == OZ_EPI + 32) {
-    // ---- MMA issuer: the S(S+1)/2 digit pairs of a K step into S diagonals of 32 columns,
+    // ---- MMA issuer: the S(S+1)/2 digit pairs of a K step into S diagonals of NC columns,
     // as S MMAs: A slice sa against B slices 0 .. S-1-sa at once (stacked in the stage, they
-    // are one K-major operand of N = 32 (S - sa) rows), accumulating into the tensor-memory
-    // columns 32 sa .. 32 S - 1, i.e. diagonals d = sa + s
+    // are one K-major operand of N = NC (S - sa) rows), accumulating into the tensor-memory
+    // columns NC sa .. NC S - 1, i.e. diagonals d = sa + s
     int it = 0, cc = 0;
     bool ok = true;
     OzProb nxt = prob(blockIdx.x);
@@ -668,7 +679,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
           const uint64_t bd = umma::desc_kmajor_noswz(sb0, 128, 256);
           for (int sa = 0; sa < S; ++sa) {
             const uint64_t ad = umma::desc_kmajor_noswz(sa0 + (uint32_t)sa * 4096, 128, 256);
-            umma::mma_s8(tmem + (uint32_t)(sa * OZ_NC), ad, bd, umma::idesc_s8(128, OZ_NC * (S - sa)),
+            umma::mma_s8(tmem + (uint32_t)(sa * NC), ad, bd, umma::idesc_s8(128, NC * (S - sa)),
                          (ks > 0 || sa > 0) ? 1 : 0);
           }
           umma::commit(&empty[st]);
@@ -679,13 +690,13 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
     umma::commit(&fin);  // arrives when every MMA issued above has completed
     umma::mbar_wait(&fin, 0, WAIT_ITERS);
   } else if (tid < OZ_EPI) {
-    // ---- epilogue: row (tid mod 128) of each z-block, columns 16 (tid / 128) .. + 15 of a
-    // chunk, in two groups of 8.  Per group the thread reads its S x 8 accumulator words,
-    // forms the 8 values and trades half of them with the neighbouring lane (rows 2i and
-    // 2i + 1 are Re and Im of one output: the even lane keeps the group's columns 0-3, the
-    // odd lane 4-7).  The tensor memory goes back once the second group's words are in
-    // registers (the MMAs of the next chunk run while the thread converts and stores);
-    // the 8 complex values go straight to HBM.
+    // ---- epilogue: row (tid mod 128) of each z-block, the half tid / 128 of a chunk's NC
+    // columns, in groups of CW.  Per group the thread reads its S x CW accumulator words,
+    // forms the CW values, trades half of them with the neighbouring lane (rows 2i and
+    // 2i + 1 are Re and Im of one output: the even lane keeps the group's first CW/2
+    // columns, the odd lane the rest) and stores its complex values straight to HBM.  The
+    // tensor memory goes back once the last group's words are in registers (the MMAs of
+    // the next chunk run while the thread converts and stores).
     const int row = tid & 127, half = tid >> 7, odd = row & 1;
     const uint32_t tlane = (uint32_t)(32 * (warp & 3)) << 16;
     const bool pair = a.pair_digits != 0, wide = a.wide_sum != 0;
@@ -713,7 +724,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
       bool ok = true;
       for (int ch = 0; ch < pr.nchunk; ++ch, ++cc) {
         // csc[cc & 1] was last read in chunk cc - 2, before every thread's barrier of cc - 1
-        if (tid < OZ_NC) csc[cc & 1][tid] = pow2i(a.fexp[pr.fofs + ch * OZ_NC + tid]);
+        if (tid < NC) csc[cc & 1][tid] = pow2i(a.fexp[pr.fofs + ch * NC + tid]);
         const bool got = umma::mbar_wait(&accf, cc & 1, WAIT_ITERS);
         if (!umma::bar_and(1, OZ_EPI, got)) {  // uniform over the epilogue threads
           if (tid == 0) atomicExch(a.err, 1);
@@ -721,17 +732,17 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
           break;
         }
         umma::fence_after_sync();
-        const double* cs = csc[cc & 1] + 16 * half;
+        constexpr int NH = NC / 2;  // columns of a thread's half of the chunk
+        const double* cs = csc[cc & 1] + NH * half;
         // groups of CW columns (8 up to five slices, 4 above, to bound the registers); per
         // group the even lane keeps its first HW columns, the odd lane the last HW
-        constexpr int CW = S <= 5 ? 8 : 4, NGR = 16 / CW, HW = CW / 2;
-        double2 o[NGR][HW];
+        constexpr int CW = S <= 5 ? 8 : 4, NGR = NH / CW, HW = CW / 2;
 #pragma unroll
         for (int gi = 0; gi < NGR; ++gi) {
           int32_t v[S][CW];
 #pragma unroll
           for (int d = 0; d < S; ++d) {
-            const uint32_t ta = tmem + tlane + (uint32_t)(d * OZ_NC + 16 * half + CW * gi);
+            const uint32_t ta = tmem + tlane + (uint32_t)(d * NC + NH * half + CW * gi);
             if constexpr (CW == 8) umma::tmem_ld8(ta, v[d]);
             else umma::tmem_ld4(ta, v[d]);
           }
@@ -743,16 +754,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
           double h[CW];
 #pragma unroll
           for (int q = 0; q < CW; ++q) h[q] = oz_combine<S, CW>(v, q, pair, wide) * (rsc * cs[CW * gi + q]);
+          double2 o[HW];
 #pragma unroll
           for (int q = 0; q < HW; ++q) {
             const double r = __shfl_xor_sync(0xffffffffu, odd ? h[q] : h[q + HW], 1);
-            o[gi][q] = odd ? make_double2(r, h[q + HW]) : make_double2(h[q], r);
+            o[q] = odd ? make_double2(r, h[q + HW]) : make_double2(h[q], r);
           }
-        }
-        if (base) {
-#pragma unroll
-          for (int gi = 0; gi < NGR; ++gi) {
-            const int k0 = ch * OZ_NC + 16 * half + CW * gi + HW * odd;
+          if (base) {  // stored group by group (fewer live registers)
+            const int k0 = ch * NC + NH * half + CW * gi + HW * odd;
             if (!OzT<TYPE>::anal) {
               // theta rows j, j + 1 (j even) of one half-row pair are neighbours in four_off:
               // one 32-byte store (the field bases are 32-byte aligned)
@@ -760,8 +769,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
               for (int q = 0; q < HW; q += 2) {
                 const int j = k0 + q;
                 cplx* dst = base + (size_t)(j >> 1) * a.NM * 4;
-                if (j + 1 < a.Th2) st_global_2c(dst, o[gi][q], o[gi][q + 1]);
-                else if (j < a.Th2) *dst = o[gi][q];
+                if (j + 1 < a.Th2) st_global_2c(dst, o[q], o[q + 1]);
+                else if (j < a.Th2) *dst = o[q];
               }
             } else {
 #pragma unroll
@@ -769,7 +778,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 2) k_oz_gemm(OzGemmArgs a, int nzb
                 const int k = k0 + q;
                 if (k < pr.nk) {
                   const int nh = a.nhlist[pr.nhofs + k];
-                  double2 val = o[gi][q];
+                  double2 val = o[q];
                   // m = 0: s, t (and a scalar) keep no imaginary part; q keeps its own
                   // (transform.fftw3.F90:599, 869, 902, 908)
                   if (zero && a.hm[nh] == 0) val.y = 0.0;
@@ -918,11 +927,12 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
         // analysis: (c, p) without harmonics has no output (nchunk 0); a synthesis output
         // without harmonics is still written (zeros)
         const bool empty = anal && pr.nk == 0;
-        pr.nchunk = empty ? 0 : (anal ? ceil_div(pr.nk, OZ_NC) : ceil_div(Th2, OZ_NC));
+        const int NC = oz_nc(type, S);
+        pr.nchunk = empty ? 0 : (anal ? ceil_div(pr.nk, NC) : ceil_div(Th2, NC));
         pr.fofs = fofs;
-        fofs += pr.nchunk * OZ_NC;
+        fofs += pr.nchunk * NC;
         pr.bofs = bbytes;
-        bbytes += (long long)pr.nchunk * pr.nks * S * 1024;
+        bbytes += (long long)pr.nchunk * pr.nks * S * NC * 32;
         pr.aofs = abytes;
         if (pr.nchunk) abytes += (long long)o->nzb_max[type] * pr.nks * S * 4096;
         probs[((size_t)type * NM + c) * 2 + p] = pr;
@@ -950,7 +960,7 @@ int lsd_ozaki_setup(lsd_ctx* ctx) {
   }
   // ring stages: as many (2..4) as keep two CTAs per SM (<= 78 KiB of stages each)
   lsd_ozaki_default_tiles(S, &o->nst, &o->ctas);
-  o->smem = (size_t)o->nst * S * 5120;
+  o->smem = (size_t)o->nst * oz_stage_bytes(S);
   {
     int mx = 1;
     for (int c = 0; c < NM; ++c) mx = std::max(mx, ctx->mlen[c]);
@@ -1169,7 +1179,7 @@ int* lsd_ozaki_err_flag(lsd_ctx* ctx) { return ((OzState*)ctx->oz)->d_err; }
 // each.
 bool lsd_ozaki_tiles_ok(int S, int nst, int ctas) {
   if (nst < 2 || nst > OZ_MAXSTAGES || (ctas != 1 && ctas != 2) || S < 2 || S > OZ_MAXS) return false;
-  const size_t smem = (size_t)nst * S * 5120 + 4096;  // + static
+  const size_t smem = (size_t)nst * oz_stage_bytes(S) + 4096;  // + static
   return smem * ctas <= (size_t)228 * 1024 - 1024 * ctas;
 }
 // three stages where two CTAs per SM still fit, else two (at lmax 127, five slices: 2 and
@@ -1192,7 +1202,7 @@ int lsd_ozaki_set_tiles(lsd_ctx* ctx, int nst, int ctas) {
   if (!lsd_ozaki_tiles_ok(o->S, nst, ctas)) return lsd_fail(ctx, LSD_EARG, "tensor-core GEMM tiles: invalid stages / CTAs");
   o->nst = nst;
   o->ctas = ctas;
-  o->smem = (size_t)o->nst * o->S * 5120;
+  o->smem = (size_t)o->nst * oz_stage_bytes(o->S);
   oz_set_smem<OZ_VEC>(o->S, o->smem); oz_set_smem<OZ_P>(o->S, o->smem); oz_set_smem<OZ_GRAD>(o->S, o->smem);
   oz_set_smem<OZ_ST>(o->S, o->smem); oz_set_smem<OZ_Q>(o->S, o->smem);
   CUDA_TRY(cudaGetLastError());

@@ -36,8 +36,10 @@ def test_candidates(L, M, Mp, prec, S):
     if prec == capi.PREC_OZAKI:
         Sx = S or 7
 
+        nc = 48 if Sx <= 5 else 32  # the synthesis chunk's columns
+
         def fits(nst, ctas):  # ring stages + 4 KB static, 1 KB reserved per CTA, 228 KB per SM
-            return (nst * Sx * 5120 + 4096) * ctas <= 228 * 1024 - 1024 * ctas
+            return (nst * Sx * (4096 + nc * 32) + 4096) * ctas <= 228 * 1024 - 1024 * ctas
         default_stages = 3 if fits(3, 2) else 2
         assert sp["gemm"][0] == (default_stages, 2 if fits(default_stages, 2) else 1)
         for nst, ctas in sp["gemm"]:
