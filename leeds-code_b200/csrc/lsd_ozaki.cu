@@ -126,7 +126,7 @@ int lsd_umma_selftest(lsd_ctx* ctx, double* maxerr) {
 //   D[row, col] = sum_k A[row, k] B[k, col]
 // rows: the data (group, shell, component re/im of the inputs), 128 per CTA ("z-block");
 // columns: theta rows j of the half grid (synthesis) or the harmonics of (c, p) (analysis),
-// 32 per chunk; k: harmonics of c in two segments (synthesis) or the folded theta rows of
+// NC per chunk (48 or 32, oz_nc); k: harmonics of c in two segments (synthesis) or the folded theta rows of
 // two parities (analysis), 32 per K step.  The sign/parity recipes of the reference's
 // accumulations (transform.fftw3.F90:746-774, 866-909) are folded into the A rows.
 //
