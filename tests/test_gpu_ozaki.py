@@ -4,10 +4,11 @@ Each operand is scaled by a power of two per row (spectral coefficients of one s
 order m) or per column (one theta row, or one harmonic), rounded to an integer of 8S - 2
 bits and split into S balanced base-256 int8 digits; the products of digit pairs whose
 index sum is below S are accumulated exactly in int32 on the tcgen05 tensor cores and
-recombined in FP64.  Rounding costs 2^(1-8S) and the dropped tail about (S + 1) 2^(2-8S)
+recombined exactly (in int64 where the sum's bound allows, else in FP64).  Rounding costs 2^(1-8S) and the dropped tail about (S + 1) 2^(2-8S)
 of (row max) x (column max) per product, so a single transform agrees with the FP64
 oracle to about 1e-14 of the largest output for S >= 7 (FP64 rounding), 1e-11 for S = 6
 and 3e-9 for S = 5.  Tolerances (relative to the largest magnitude of the compared array):
+  single transforms, S = 3, 4    5e-3, 2e-5 (the S = 5 bar times 256 per slice, 4x margin)
   single transforms, S = 5       2e-8
   single transforms, S = 6       1e-10
   single transforms, S = 7, 8    5e-13
@@ -44,7 +45,11 @@ def test_ozaki_slices_are_validated():
 @pytest.mark.gpu
 @pytest.mark.parametrize("LMMp,S,tol", [((32, 32, 1), 7, 5e-13), ((64, 16, 4), 7, 5e-13),
                                          ((24, 8, 2), 7, 5e-13), ((32, 32, 1), 8, 5e-13),
-                                         ((64, 16, 4), 6, 1e-10), ((64, 16, 4), 5, 2e-8)])
+                                         ((64, 16, 4), 6, 1e-10), ((64, 16, 4), 5, 2e-8),
+                                         # 48-column synthesis chunks with 18 theta rows (masked)
+                                         ((24, 8, 2), 5, 2e-8),
+                                         # fewer slices: 256 times per slice, 4x margin
+                                         ((64, 16, 4), 4, 2e-5), ((32, 32, 1), 3, 5e-3)])
 def test_ozaki_transforms(LMMp, S, tol):
     L, M, Mp = LMMp
     cfg = capi.template_config(L=L, M=M, Mp=Mp, N=9, timestep=1e-5, precision=capi.PREC_OZAKI,
